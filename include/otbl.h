@@ -1,0 +1,135 @@
+/*
+ * otbl.h -- C ABI of the B200 RK3 substep of OpenTBL's zero-pressure-gradient
+ * boundary-layer DNS.
+ *
+ * The reference exposes the substep as Fortran external subroutines with
+ * implicit interfaces, called from bl_1.F90:98-119 with every coefficient and
+ * size held in module globals (mod.F90). Here the globals become an explicit
+ * context: the config struct, a packed coefficient buffer (otbl_layout.h) and
+ * the device-resident state. Every entry point returns an int status
+ * (OTBL_OK = 0) and otbl_last_error() gives the message. Calls on one context
+ * are stream-ordered on the context's CUDA stream and are not re-entrant;
+ * different contexts may be driven from different host threads.
+ *
+ * Field arrays use the reference's single-rank plane layout (otbl_layout.h).
+ * Plane indices i, rows j and the recycling plane xout are 1-based, as in the
+ * Fortran.
+ */
+#ifndef OTBL_H
+#define OTBL_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define OTBL_OK 0
+#define OTBL_ERR_ARG 1      /* bad argument (null pointer, bad id, bad size) */
+#define OTBL_ERR_CONFIG 2   /* inconsistent configuration                     */
+#define OTBL_ERR_OOM 3      /* device allocation failed                       */
+#define OTBL_ERR_CUDA 4     /* CUDA runtime error                             */
+#define OTBL_ERR_NAN 5      /* non-finite value detected by the dt reduction  */
+#define OTBL_ERR_NODEV 6    /* no CUDA device / extension not usable          */
+
+/* transposes (change.f90): round the payload to REAL4 as the reference's
+ * MPI_ALLTOALLV(MPI_REAL4) does (change.f90:579,608,641,652,676,686), or
+ * keep full FP64 */
+#define OTBL_XPOSE_NONE 0
+#define OTBL_XPOSE_FP32 1
+
+/* time step: recomputed from the CFL limits at substep 1 of every step
+ * (bl_1.F90:91, rhsp.F90:214-262), or held fixed */
+#define OTBL_DT_ADAPTIVE 0
+#define OTBL_DT_FIXED 1
+
+typedef struct otbl_config {
+  int nx, ny, nz;   /* grid (mod.F90:22); nz1 = 2*(nz/3), nz2 = nz1/2-1     */
+  int xout;         /* recycling plane, 1-based (mod.F90:23)               */
+  int xpose_round;  /* OTBL_XPOSE_*                                        */
+  int dt_mode;      /* OTBL_DT_*                                           */
+  double re, ax, ay, az, cfl; /* input deck, bl_1.F90:207-210              */
+  double y_blend;   /* height that replaces y(119) in genflu.F90:57        */
+  double dt_fixed;  /* dt for OTBL_DT_FIXED; <= 0 freezes the first CFL dt */
+} otbl_config;
+
+/* field ids for otbl_set_field / otbl_get_field / otbl_field_device_ptr */
+enum {
+  OTBL_F_U = 0, OTBL_F_V, OTBL_F_W, OTBL_F_P,
+  OTBL_F_RHSUPA, OTBL_F_RHSVPA, OTBL_F_RHSWPA,
+  OTBL_F_COUNT
+};
+
+/* inflow-recycling state of module genmod (mod.F90:86-93) plus the clock */
+typedef struct otbl_inflow {
+  double tiempo;    /* simulation time (bl_1.F90:128)                      */
+  double timeinit;  /* time origin of the mean-profile filter              */
+  double dt;        /* current time step                                   */
+  double utauout, rthout, dout, gamma1, gamma2, timec; /* genflu outputs   */
+  double umax, wmax, vmax; /* CFL maxima of the last dt reduction          */
+} otbl_inflow;
+
+/* ---- setup (host only; coeft.f90 coef, bl_1.F90 inlet_retheta, boun.f90
+ *      magicnumber) ---- */
+int otbl_config_check(const otbl_config *cfg);
+size_t otbl_coef_count(int nx, int ny, int nz);
+int otbl_coef_offset(int nx, int ny, int nz, int id, size_t *off);
+/* y: y(0:ny+1) (ny+2 values); u0: inlet mean profile u(k=0, 1:ny+1, i=1)
+ * (getstartzy-bg.F90:273). Fills coef[otbl_coef_count()] */
+int otbl_coef_compute(const otbl_config *cfg, const double *y,
+                      const double *u0, double *coef);
+
+/* ---- context ---- */
+typedef struct otbl_ctx otbl_ctx;
+int otbl_ctx_create(const otbl_config *cfg, const double *coef, int device,
+                    otbl_ctx **out);
+void otbl_ctx_destroy(otbl_ctx *ctx);
+const char *otbl_last_error(const otbl_ctx *ctx);
+size_t otbl_device_bytes(const otbl_ctx *ctx);
+
+/* host <-> device copies of the state, reference layout */
+int otbl_set_field(otbl_ctx *ctx, int id, const double *host);
+int otbl_get_field(otbl_ctx *ctx, int id, double *host);
+int otbl_field_device_ptr(otbl_ctx *ctx, int id, double **dptr);
+/* u0 (ny+1), v0 (ny): inlet profiles (getstartzy-bg.F90:273-276);
+ * um (ny+1): filtered mean profile at xout (readheader, getstartzy-bg.F90:578) */
+int otbl_set_inflow(otbl_ctx *ctx, const double *u0, const double *v0,
+                    const double *um, const otbl_inflow *st);
+int otbl_get_inflow(otbl_ctx *ctx, double *um, otbl_inflow *st);
+
+/* ---- the substep, bl_1.F90:94-125 ----
+ * m = RK3 substep 1..3; setstep = 1 recomputes dt (adaptive mode). */
+int otbl_rhsp(otbl_ctx *ctx, int m, int setstep);   /* rhsp.F90:22        */
+int otbl_outflow_correction(otbl_ctx *ctx);         /* boun.f90:63        */
+int otbl_pois(otbl_ctx *ctx, int m);                /* pois.f90:11, with
+                                     varstep = 0.5/dt/rkdv(m), bl_1.F90:117 */
+int otbl_substep(otbl_ctx *ctx, int m, int setstep);
+/* nsteps full RK3 steps, tiempo += dt after each (bl_1.F90:85-128) */
+int otbl_advance(otbl_ctx *ctx, int nsteps);
+int otbl_sync(otbl_ctx *ctx);
+
+/* ---- pieces of the path, on device buffers owned by the caller ---- */
+/* change.f90:224/257: planes (0:nz2, jee, nx) <-> pencils (nx, nz1*jee),
+ * rounding to REAL4 when the context's xpose_round is OTBL_XPOSE_FP32 */
+int otbl_chp2x(otbl_ctx *ctx, const double *plan_dev, double *pen_dev, int jee);
+int otbl_chx2p(otbl_ctx *ctx, const double *pen_dev, double *plan_dev, int jee);
+/* ffts.f90:27 fourxz on nlines z-lines: iopt<0 r2c (phys -> fou, x 1/nz,
+ * modes 0..nz2 kept); iopt>=0 c2r (fou -> phys, modes > nz2 zeroed).
+ * fou: nlines x (nz2+1) complex; phys: nlines x (nz+2) reals */
+int otbl_fourxz(otbl_ctx *ctx, double *fou_dev, double *phys_dev, int iopt,
+                int nlines);
+/* ffts.f90:147 cosftx on nlines x-lines of length nx stored as pencils
+ * c(nx, nlines): transforms c(2:nx, :), iopt<0 REDFT10 x 1/(nx-1),
+ * iopt>=0 REDFT01 x 0.5 */
+int otbl_cosftx(otbl_ctx *ctx, double *c_dev, int nlines, int iopt);
+int otbl_boun(otbl_ctx *ctx);                        /* boun.f90:7         */
+int otbl_genflu(otbl_ctx *ctx);                      /* genflu.F90:3       */
+
+/* kernel launches issued by this context since creation */
+long long otbl_launch_count(const otbl_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
