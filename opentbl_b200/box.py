@@ -1,0 +1,153 @@
+"""Host-side mirror of the reference's substep interface.
+
+``Box`` owns one device context (one boundary-layer box resident in HBM) and
+exposes the reference's subroutine surface with the same meaning and order:
+
+  rhsp(m, setstep)        rhsp.F90:22    RHS, RK3 stage update, implicit y
+  outflow_correction()    boun.f90:63    global mass balance at the outflow
+  pois(m)                 pois.f90:11    pressure Poisson solve + projection
+  substep(m, setstep)     bl_1.F90:98-119 (the three calls above)
+  advance(nsteps)         bl_1.F90:85-128 (3 substeps per step, tiempo += dt)
+  boun(), genflu()        boun.f90:7, genflu.F90:3 (standalone pieces)
+  chp2x/chx2p, fourxz, cosftx   change.f90, ffts.f90 on device buffers
+
+State arrays use the reference's plane layout, as numpy arrays shaped
+(nx, ny+1 or ny, nz1) -- C order of the Fortran (0:nz2, j, i) arrays.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import native
+from .config import BoxConfig
+from .native import FIELDS, UTYPE, OtblError, OtblInflow
+
+
+class Box:
+    def __init__(self, cfg: BoxConfig, init: dict, coef: np.ndarray | None = None,
+                 device: int = 0):
+        self.cfg = cfg
+        self.L = native.lib()
+        self.re = float(init["re"])
+        self.xout = int(init["xout"])
+        self.y = np.asarray(init["y"], dtype=np.float64)
+        if coef is None:
+            coef = native.coef_compute(cfg, self.re, self.xout, self.y, init["u0"])
+        self.coef = np.ascontiguousarray(coef, dtype=np.float64)
+        self.ccfg = native.make_config(cfg, self.re, self.xout)
+        h = ctypes.c_void_p()
+        st = self.L.otbl_ctx_create(ctypes.byref(self.ccfg), native.dptr(self.coef), device,
+                                    ctypes.byref(h))
+        self.h = h
+        if st != native.OTBL_OK:
+            msg = self.L.otbl_last_error(h).decode() if h.value else ""
+            self.close()
+            raise OtblError(f"otbl_ctx_create: {native.ERRORS.get(st, st)} {msg}")
+        for n in FIELDS:
+            self.set_field(n, init[n])
+        inf = OtblInflow()
+        inf.dt = float(init.get("dt", 0.0))
+        inf.tiempo = float(init.get("tiempo", 0.0))
+        inf.timeinit = float(init.get("timeinit", 0.0))
+        self._check(self.L.otbl_set_inflow(
+            self.h, native.dptr(np.ascontiguousarray(init["u0"], dtype=np.float64)),
+            native.dptr(np.ascontiguousarray(init["v0"], dtype=np.float64)),
+            native.dptr(np.ascontiguousarray(init["um"], dtype=np.float64)), ctypes.byref(inf)),
+            "otbl_set_inflow")
+
+    # ---- plumbing ----
+    def _check(self, st, what):
+        if st != native.OTBL_OK:
+            msg = self.L.otbl_last_error(self.h).decode() if self.h else ""
+            raise OtblError(f"{what}: {native.ERRORS.get(st, st)} {msg}")
+
+    def shape(self, name):
+        c = self.cfg
+        return (c.nx, c.ny + 1 if UTYPE[name] else c.ny, c.nz1)
+
+    def set_field(self, name, arr):
+        a = np.ascontiguousarray(np.asarray(arr, dtype=np.float64).reshape(self.shape(name)))
+        self._check(self.L.otbl_set_field(self.h, FIELDS.index(name), native.dptr(a)), "otbl_set_field")
+
+    def field(self, name) -> np.ndarray:
+        a = np.empty(self.shape(name))
+        self._check(self.L.otbl_get_field(self.h, FIELDS.index(name), native.dptr(a)), "otbl_get_field")
+        return a
+
+    def device_ptr(self, name) -> int:
+        p = ctypes.POINTER(ctypes.c_double)()
+        self._check(self.L.otbl_field_device_ptr(self.h, FIELDS.index(name), ctypes.byref(p)),
+                    "otbl_field_device_ptr")
+        return ctypes.cast(p, ctypes.c_void_p).value
+
+    def inflow(self):
+        um = np.zeros(self.cfg.ny + 1)
+        st = OtblInflow()
+        self._check(self.L.otbl_get_inflow(self.h, native.dptr(um), ctypes.byref(st)), "otbl_get_inflow")
+        return um, {n: getattr(st, n) for n, _ in OtblInflow._fields_}
+
+    @property
+    def launches(self) -> int:
+        return int(self.L.otbl_launch_count(self.h))
+
+    @property
+    def device_bytes(self) -> int:
+        return int(self.L.otbl_device_bytes(self.h))
+
+    # ---- the reference's subroutine surface ----
+    def rhsp(self, m: int, setstep: bool):
+        self._check(self.L.otbl_rhsp(self.h, m, int(setstep)), "otbl_rhsp")
+
+    def outflow_correction(self):
+        self._check(self.L.otbl_outflow_correction(self.h), "otbl_outflow_correction")
+
+    def pois(self, m: int):
+        self._check(self.L.otbl_pois(self.h, m), "otbl_pois")
+
+    def substep(self, m: int, setstep: bool):
+        self._check(self.L.otbl_substep(self.h, m, int(setstep)), "otbl_substep")
+
+    def advance(self, nsteps: int):
+        self._check(self.L.otbl_advance(self.h, nsteps), "otbl_advance")
+
+    def sync(self):
+        self._check(self.L.otbl_sync(self.h), "otbl_sync")
+
+    def boun(self):
+        self._check(self.L.otbl_boun(self.h), "otbl_boun")
+
+    def genflu(self):
+        self._check(self.L.otbl_genflu(self.h), "otbl_genflu")
+
+    # device-buffer pieces (pointers are raw device addresses)
+    def chp2x(self, plan_dev: int, pen_dev: int, jee: int):
+        self._check(self.L.otbl_chp2x(self.h, plan_dev, pen_dev, jee), "otbl_chp2x")
+
+    def chx2p(self, pen_dev: int, plan_dev: int, jee: int):
+        self._check(self.L.otbl_chx2p(self.h, pen_dev, plan_dev, jee), "otbl_chx2p")
+
+    def fourxz(self, fou_dev: int, phys_dev: int, iopt: int, nlines: int):
+        self._check(self.L.otbl_fourxz(self.h, fou_dev, phys_dev, iopt, nlines), "otbl_fourxz")
+
+    def cosftx(self, c_dev: int, nlines: int, iopt: int):
+        self._check(self.L.otbl_cosftx(self.h, c_dev, nlines, iopt), "otbl_cosftx")
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.L.otbl_ctx_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def make_box(cfg: BoxConfig, device: int = 0):
+    """Seeded synthetic box (opentbl_b200.synth) resident on the device."""
+    from . import synth
+    init = synth.make_initial(cfg)
+    return Box(cfg, init, device=device), init

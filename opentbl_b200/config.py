@@ -71,12 +71,12 @@ C1 = BoxConfig(nx=257, ny=97, nz=128, lx=60.0, ly=8.0, lz=8.0, re_theta=300.0,
 C2 = BoxConfig(nx=1025, ny=193, nz=512, lx=80.0, ly=10.0, lz=10.0,
                re_theta=1000.0, profile="musker", name="C2-1025x193x512")
 # small box for tests and smoke runs
-TINY = BoxConfig(nx=33, ny=41, nz=24, lx=12.0, ly=6.0, lz=4.0, dy_wall=0.02,
+TINY = BoxConfig(nx=33, ny=41, nz=32, lx=12.0, ly=6.0, lz=4.0, dy_wall=0.02,
                  re_theta=300.0, profile="blasius", y_blend=1.5,
-                 name="tiny-33x41x24")
-SMALL = BoxConfig(nx=65, ny=57, nz=48, lx=24.0, ly=8.0, lz=6.0,
+                 name="tiny-33x41x32")
+SMALL = BoxConfig(nx=65, ny=57, nz=64, lx=24.0, ly=8.0, lz=6.0,
                   dy_wall=0.006, re_theta=300.0, profile="blasius",
-                  name="small-65x57x48")
+                  name="small-65x57x64")
 
 
 def replace(cfg: BoxConfig, **kw) -> BoxConfig:

@@ -1,0 +1,229 @@
+// Hand-written FFT building blocks for the substep (sm_100a, FP64).
+//
+// Spanwise transforms (ffts.f90:27-67 fourxz): a real line of nz points is
+// handled as a complex line of M = nz/2 points (even/odd packing) and
+// transformed by one warp with a Stockham autosort FFT in shared memory
+// (radix 8/4/2 passes, each pass: registers <- smem, small DFT, smem <-
+// registers). Streamwise cosine transforms (ffts.f90:147-181 cosftx) use the
+// same Stockham passes with a whole CTA over a length nx-1 complex line
+// (radices 8/4/2/3/5), with Makhoul's permutation turning a DCT-II/III of
+// length n into one complex FFT of length n.
+//
+// Twiddles come from tables tw[t] = exp(-2 pi i t / N) built on the device by
+// sincospi at context creation.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace otbl {
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+// multiply by i*s (s = +1 or -1)
+__device__ __forceinline__ double2 cmul_i(double2 a, int s) {
+  return s > 0 ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
+}
+
+// In-register DFT of size R; SIGN = -1 forward (e^{-}), +1 backward (e^{+}).
+template <int R, int SIGN>
+__device__ __forceinline__ void dft_small(double2 *v);
+
+template <>
+__device__ __forceinline__ void dft_small<2, -1>(double2 *v) {
+  const double2 a = v[0], b = v[1];
+  v[0] = cadd(a, b);
+  v[1] = csub(a, b);
+}
+template <>
+__device__ __forceinline__ void dft_small<2, 1>(double2 *v) {
+  dft_small<2, -1>(v);
+}
+
+template <int SIGN>
+__device__ __forceinline__ void dft4(double2 &t0, double2 &t1, double2 &t2, double2 &t3) {
+  const double2 a0 = cadd(t0, t2), a1 = csub(t0, t2);
+  const double2 b0 = cadd(t1, t3), b1 = cmul_i(csub(t1, t3), SIGN);
+  t0 = cadd(a0, b0);
+  t1 = cadd(a1, b1);
+  t2 = csub(a0, b0);
+  t3 = csub(a1, b1);
+}
+template <>
+__device__ __forceinline__ void dft_small<4, -1>(double2 *v) {
+  dft4<-1>(v[0], v[1], v[2], v[3]);
+}
+template <>
+__device__ __forceinline__ void dft_small<4, 1>(double2 *v) {
+  dft4<1>(v[0], v[1], v[2], v[3]);
+}
+
+template <int SIGN>
+__device__ __forceinline__ void dft8(double2 *v) {
+  const double c = 0.70710678118654752440;  // cos(pi/4)
+  double2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+  double2 o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+  dft4<SIGN>(e0, e1, e2, e3);
+  dft4<SIGN>(o0, o1, o2, o3);
+  // W8^q = exp(SIGN*2*pi*i*q/8)
+  const double2 w1 = make_double2(c, SIGN * c);
+  const double2 w3 = make_double2(-c, SIGN * c);
+  o1 = cmul(o1, w1);
+  o2 = cmul_i(o2, SIGN);
+  o3 = cmul(o3, w3);
+  v[0] = cadd(e0, o0);
+  v[4] = csub(e0, o0);
+  v[1] = cadd(e1, o1);
+  v[5] = csub(e1, o1);
+  v[2] = cadd(e2, o2);
+  v[6] = csub(e2, o2);
+  v[3] = cadd(e3, o3);
+  v[7] = csub(e3, o3);
+}
+template <>
+__device__ __forceinline__ void dft_small<8, -1>(double2 *v) {
+  dft8<-1>(v);
+}
+template <>
+__device__ __forceinline__ void dft_small<8, 1>(double2 *v) {
+  dft8<1>(v);
+}
+
+template <int SIGN>
+__device__ __forceinline__ void dft3(double2 *v) {
+  const double s3 = 0.86602540378443864676;  // sin(2 pi/3)
+  const double2 a = v[0], b = v[1], cc = v[2];
+  const double2 t1 = cadd(b, cc);
+  const double2 t2 = make_double2(a.x - 0.5 * t1.x, a.y - 0.5 * t1.y);
+  const double2 t3 = cmul_i(csub(b, cc), SIGN);  // i*SIGN*(b-c)
+  v[0] = cadd(a, t1);
+  v[1] = make_double2(t2.x + s3 * t3.x, t2.y + s3 * t3.y);
+  v[2] = make_double2(t2.x - s3 * t3.x, t2.y - s3 * t3.y);
+}
+template <>
+__device__ __forceinline__ void dft_small<3, -1>(double2 *v) {
+  dft3<-1>(v);
+}
+template <>
+__device__ __forceinline__ void dft_small<3, 1>(double2 *v) {
+  dft3<1>(v);
+}
+
+template <int SIGN>
+__device__ __forceinline__ void dft5(double2 *v) {
+  // cos/sin of 2 pi/5 and 4 pi/5
+  const double c1 = 0.30901699437494742410, c2 = -0.80901699437494742410;
+  const double s1 = 0.95105651629515357212, s2 = 0.58778525229247312917;
+  const double2 a = v[0];
+  const double2 b1 = cadd(v[1], v[4]), b2 = cadd(v[2], v[3]);
+  const double2 d1 = csub(v[1], v[4]), d2 = csub(v[2], v[3]);
+  const double2 r1 = make_double2(a.x + c1 * b1.x + c2 * b2.x, a.y + c1 * b1.y + c2 * b2.y);
+  const double2 r2 = make_double2(a.x + c2 * b1.x + c1 * b2.x, a.y + c2 * b1.y + c1 * b2.y);
+  const double2 i1 = cmul_i(make_double2(s1 * d1.x + s2 * d2.x, s1 * d1.y + s2 * d2.y), SIGN);
+  const double2 i2 = cmul_i(make_double2(s2 * d1.x - s1 * d2.x, s2 * d1.y - s1 * d2.y), SIGN);
+  v[0] = cadd(a, cadd(b1, b2));
+  v[1] = cadd(r1, i1);
+  v[4] = csub(r1, i1);
+  v[2] = cadd(r2, i2);
+  v[3] = csub(r2, i2);
+}
+template <>
+__device__ __forceinline__ void dft_small<5, -1>(double2 *v) {
+  dft5<-1>(v);
+}
+template <>
+__device__ __forceinline__ void dft_small<5, 1>(double2 *v) {
+  dft5<1>(v);
+}
+
+// One Stockham pass of radix R over a length-M complex line in shared memory,
+// in place, by a group of G threads (rank t in the group). Pass with span Ns:
+//   item j (0 <= j < M/R), k = j mod Ns:
+//   v[r] = buf[j + r*M/R] * W_{Ns*R}^{r*k};  v = DFT_R(v);
+//   buf[(j/Ns)*Ns*R + k + r*Ns] = v[r]
+// MAXIT bounds the items per thread. SYNC is __syncwarp or __syncthreads.
+template <int R, int SIGN, int MAXIT, bool BLOCK>
+__device__ __forceinline__ void stockham_pass(double2 *buf, int M, int Ns, const double2 *__restrict__ tw,
+                                              int t, int G) {
+  const int nit = M / R;
+  const int stride_tw = M / (Ns * R);
+  double2 v[MAXIT][R];
+#pragma unroll
+  for (int it = 0; it < MAXIT; ++it) {
+    const int j = t + it * G;
+    if (j < nit) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[it][r] = buf[j + r * nit];
+    }
+  }
+  if (BLOCK)
+    __syncthreads();
+  else
+    __syncwarp();
+#pragma unroll
+  for (int it = 0; it < MAXIT; ++it) {
+    const int j = t + it * G;
+    if (j < nit) {
+      const int k = j % Ns;
+      if (Ns > 1) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          double2 w = __ldg(&tw[r * k * stride_tw]);
+          if (SIGN > 0) w.y = -w.y;
+          v[it][r] = cmul(v[it][r], w);
+        }
+      }
+      dft_small<R, SIGN>(v[it]);
+      const int base = (j / Ns) * Ns * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) buf[base + r * Ns] = v[it][r];
+    }
+  }
+  if (BLOCK)
+    __syncthreads();
+  else
+    __syncwarp();
+}
+
+// Warp FFT of a power-of-two length M <= 512 in shared memory (in place).
+template <int SIGN>
+__device__ __forceinline__ void warp_fft(double2 *buf, int M, const double2 *__restrict__ tw, int lane) {
+  int Ns = 1;
+  while (Ns * 8 <= M) {
+    stockham_pass<8, SIGN, 2, false>(buf, M, Ns, tw, lane, 32);
+    Ns *= 8;
+  }
+  if (Ns * 4 <= M) {
+    stockham_pass<4, SIGN, 4, false>(buf, M, Ns, tw, lane, 32);
+    Ns *= 4;
+  }
+  if (Ns * 2 <= M) {
+    stockham_pass<2, SIGN, 8, false>(buf, M, Ns, tw, lane, 32);
+    Ns *= 2;
+  }
+}
+
+// CTA FFT of length n = 2^a 3^b 5^c (n <= 4096) in shared memory; NB lines
+// stored back to back (line l at buf + l*n) are transformed in turn by the
+// 256 threads of the CTA. The twiddle table has n entries.
+template <int R, int SIGN, int NB>
+__device__ __forceinline__ void block_pass(double2 *buf, int n, int Ns, const double2 *__restrict__ tw) {
+  constexpr int MAXIT = (4096 / R + 255) / 256;
+#pragma unroll 1
+  for (int l = 0; l < NB; ++l)
+    stockham_pass<R, SIGN, MAXIT, true>(buf + l * n, n, Ns, tw, threadIdx.x, 256);
+}
+
+template <int SIGN, int NB>
+__device__ __forceinline__ void block_fft(double2 *buf, int n, const double2 *__restrict__ tw) {
+  int Ns = 1, rem = n;
+  while (rem % 8 == 0) { block_pass<8, SIGN, NB>(buf, n, Ns, tw); Ns *= 8; rem /= 8; }
+  while (rem % 4 == 0) { block_pass<4, SIGN, NB>(buf, n, Ns, tw); Ns *= 4; rem /= 4; }
+  while (rem % 2 == 0) { block_pass<2, SIGN, NB>(buf, n, Ns, tw); Ns *= 2; rem /= 2; }
+  while (rem % 3 == 0) { block_pass<3, SIGN, NB>(buf, n, Ns, tw); Ns *= 3; rem /= 3; }
+  while (rem % 5 == 0) { block_pass<5, SIGN, NB>(buf, n, Ns, tw); Ns *= 5; rem /= 5; }
+}
+
+}  // namespace otbl

@@ -1,0 +1,1379 @@
+// CUDA kernels of the RK3 substep (sm_100a, FP64).
+//
+// Stage map (reference routine -> kernel):
+//   interpxx  lip.f90:248   k_interpx     x-lines, compact mid-point interp.
+//   interpyy  lip.f90:359   k_interpy     y-lines in Fourier space
+//   fourxz    ffts.f90:27   k_products    z-lines: 9 c2r + 6 r2c per (i,j)
+//                                          line, the six nonlinear products
+//                                          and the CFL maxima (rhsp.F90:120-171,
+//                                          367-415)
+//   difvisxx  lip.f90:52    k_difvisx     x-lines, d/dx(product) + d2/dx2
+//   dt        rhsp.F90:214  k_dt          dt, RK3 factors, implzy LU factors
+//   genflu    genflu.F90:3  k_genflu      inflow plane + boun of plane 1
+//   rhsp tail rhsp.F90:291-484 k_final    y-lines: pressure gradient, RHS
+//                                          assembly (differzy), boun, vistyy,
+//                                          RK3 combination, implzy
+//   outflow_correction boun.f90:63  k_outflow
+//   pois      pois.f90:11   k_pois_fwd    divergence + DCT-II along x
+//                           k_pois_solve  tridiagonal in y per (x-mode, kz)
+//                           k_pois_bwd    DCT-III along x
+//                           k_project     pressure/velocity update
+// The reference's transposes (change.f90) are not executed on the substep:
+// x-lines are read straight from the plane layout (threads over the
+// contiguous (j, kr) index, a walk over i with the plane stride), and the
+// REAL4 rounding of the transposed payload (OTBL_XPOSE_FP32) is applied at
+// exactly the loads/stores where the reference transposes.
+#include <cfloat>
+
+#include "fft.cuh"
+#include "otbl_internal.cuh"
+
+namespace otbl {
+
+#define A3(a, r, i) (a)[((i)-1) * 3 + (r)-1]
+#define A2(a, r, i) (a)[((i)-1) * 2 + (r)-1]
+#define M4(a, r, cc) (a)[((cc)-1) * 4 + (r)-1]
+#define M5(a, r, cc) (a)[((cc)-1) * 5 + (r)-1]
+#define M2(a, r, cc) (a)[((cc)-1) * 2 + (r)-1]
+
+__device__ __forceinline__ double rnd(double x, int xr) { return xr ? (double)(float)x : x; }
+
+// NaN-propagating maximum of non-negative values
+__device__ __forceinline__ double nmax(double m, double v) {
+  return (m != m) ? m : ((v != v) ? v : fmax(m, v));
+}
+__device__ __forceinline__ double warp_nmax(double m) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = nmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  return m;
+}
+
+// ---------------------------------------------------------------------------
+// x-line kernels: one thread per pencil mp in [0, np), np = nz1*jee. The
+// pencil's value at plane i sits at in[(i-1)*np + mp], so a warp reads 32
+// consecutive doubles per plane.
+// ---------------------------------------------------------------------------
+
+// interpxx, lip.f90:248-300. which 0: u (inxu, cofiux, chi=2, chi2=3);
+// which 1: v,w (inxv, cofivx, chi=1, chi2=4).
+__global__ void __launch_bounds__(128) k_interpx(DCoef c, const double *__restrict__ in,
+                                                 double *__restrict__ out, int which, int np) {
+  const int mp = blockIdx.x * blockDim.x + threadIdx.x;
+  if (mp >= np) return;
+  const int nx = c.nx, xr = c.xround;
+  const size_t S = (size_t)np;
+  const double *icon = which == 0 ? c.inxu : c.inxv;
+  const double *econ = which == 0 ? c.cofiux : c.cofivx;
+  const int chi = which == 0 ? 2 : 1, chi2 = which == 0 ? 3 : 4;
+  const double *ib = c.inbx;
+  const double *g = in + mp;
+  double *o = out + mp;
+  auto G = [&](int i) { return rnd(__ldg(g + (size_t)(i - 1) * S), xr); };
+  double bb = M4(ib, chi2, 1) * G(1) + M4(ib, chi2, 2) * G(2) + M4(ib, chi2, 3) * G(3) + M4(ib, chi2, 4) * G(4);
+  o[0] = bb;
+  double gi = G(2);
+  for (int i = 2; i <= nx - 1; ++i) {
+    const double gn = G(i + 1);
+    const double b = A2(econ, 1, i) * gi + A2(econ, 2, i) * gn;
+    bb = b + A3(icon, 1, i) * bb;
+    o[(size_t)(i - 1) * S] = bb;
+    gi = gn;
+  }
+  {
+    const double b = M4(ib, chi, 1) * G(nx) + M4(ib, chi, 2) * G(nx - 1) + M4(ib, chi, 3) * G(nx - 2) +
+                     M4(ib, chi, 4) * G(nx - 3);
+    bb = b + A3(icon, 1, nx) * bb;
+  }
+  double x = bb * A3(icon, 2, nx);
+  o[(size_t)(nx - 1) * S] = rnd(x, xr);
+  for (int i = nx - 1; i >= 1; --i) {
+    x = (o[(size_t)(i - 1) * S] - A3(icon, 3, i) * x) * A3(icon, 2, i);
+    o[(size_t)(i - 1) * S] = rnd(x, xr);
+  }
+}
+
+// difvisxx, lip.f90:52-142: result = Pade d/dx(gin) + rex * Pade d2/dx2(up),
+// outflow rows replaced as lip.f90:105,132. which 0: u; which 1: v,w.
+// scr holds the viscous forward sweep.
+__global__ void __launch_bounds__(128) k_difvisx(DCoef c, const double *__restrict__ gin,
+                                                 const double *__restrict__ upin, double *__restrict__ out,
+                                                 double *__restrict__ scr, int which, int np) {
+  const int mp = blockIdx.x * blockDim.x + threadIdx.x;
+  if (mp >= np) return;
+  const int nx = c.nx, xr = c.xround;
+  const size_t S = (size_t)np;
+  const double *icon = which == 0 ? c.dcxu : c.dcxv;
+  const double *iconv = which == 0 ? c.vixu : c.vixv;
+  const double *econ = which == 0 ? c.cofcxu : c.cofcxv;
+  const double *econv = which == 0 ? c.cofvxu : c.cofvxv;
+  const int chv = which == 0 ? 1 : 2, chv1 = chv + 2, ic = which == 0 ? 3 : 1;
+  const double *db = c.dcbx, *vb = c.cofvbx;
+  const double rex = c.S[OTBL_S_REX], idx = c.S[OTBL_S_IDX], uinf = c.S[OTBL_S_UINF];
+  const double *g = gin + mp, *up = upin + mp;
+  double *o = out + mp, *s = scr + mp;
+  auto G = [&](int i) { return rnd(__ldg(g + (size_t)(i - 1) * S), xr); };
+  auto U = [&](int i) { return rnd(__ldg(up + (size_t)(i - 1) * S), xr); };
+  double bc = M5(db, chv, 1) * G(1) + M5(db, chv, 2) * G(2) + M5(db, chv, 3) * G(3) + M5(db, chv, 4) * G(4);
+  double bv = M4(vb, ic, 1) * U(1) + M4(vb, ic, 2) * U(2) + M4(vb, ic, 3) * U(3) + M4(vb, ic, 4) * U(4);
+  o[0] = bc;
+  s[0] = bv;
+  double gp = G(1), gi = G(2), um1 = U(1), ui = U(2);
+  for (int i = 2; i <= nx - 1; ++i) {
+    const double un = U(i + 1);
+    const double b = A2(econ, 1, i) * gp + A2(econ, 2, i) * gi;
+    bc = b + A3(icon, 1, i) * bc;
+    o[(size_t)(i - 1) * S] = bc;
+    const double bw = A3(econv, 1, i) * un + A3(econv, 2, i) * ui + A3(econv, 3, i) * um1;
+    bv = bw + A3(iconv, 1, i) * bv;
+    s[(size_t)(i - 1) * S] = bv;
+    gp = gi;
+    gi = G(i + 1);
+    um1 = ui;
+    ui = un;
+  }
+  const double uN = U(nx), uN1 = U(nx - 1), uN2 = U(nx - 2), uN3 = U(nx - 3);
+  {
+    const double b = M5(db, chv1, 1) * G(nx) + M5(db, chv1, 2) * G(nx - 1) + M5(db, chv1, 3) * G(nx - 2) +
+                     M5(db, chv1, 4) * G(nx - 3);
+    bc = b + A3(icon, 1, nx) * bc;
+    const double bw = M4(vb, ic + 1, 1) * uN + M4(vb, ic + 1, 2) * uN1 + M4(vb, ic + 1, 3) * uN2 +
+                      M4(vb, ic + 1, 4) * uN3;
+    bv = bw + A3(iconv, 1, nx) * bv;
+  }
+  double xc = bc * A3(icon, 2, nx);
+  double xv = bv * A3(iconv, 2, nx);
+  o[(size_t)(nx - 1) * S] = rnd(uinf * (uN - uN1) * idx + rex * 0.0, xr);
+  for (int i = nx - 1; i >= 1; --i) {
+    xc = (o[(size_t)(i - 1) * S] - A3(icon, 3, i) * xc) * A3(icon, 2, i);
+    xv = (s[(size_t)(i - 1) * S] - A3(iconv, 3, i) * xv) * A3(iconv, 2, i);
+    o[(size_t)(i - 1) * S] = rnd(xc + rex * xv, xr);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// y-line helpers: one thread per column (i, kr); rows j are nz1 apart.
+// ---------------------------------------------------------------------------
+
+// interpyy, lip.f90:359-440 (not in place); out rows 1..ny.
+__device__ __forceinline__ void col_interpyy(const DCoef &c, const double *g, double *o, int which) {
+  const int ny = c.ny;
+  const size_t S = c.nz1;
+  const double *icon = which == 0 ? c.inyu : c.inyv;
+  const double *econ = which == 0 ? c.cofiuy : c.cofivy;
+  const double *ib = c.inby;
+  auto G = [&](int j) { return g[(size_t)(j - 1) * S]; };
+  double bb;
+  if (which == 0) {
+    bb = 0.0;
+    o[0] = bb;
+    for (int j = 2; j <= ny - 1; ++j) {
+      const double b = A2(econ, 1, j) * G(j) + A2(econ, 2, j) * G(j + 1);
+      bb = b + A3(icon, 1, j) * bb;
+      o[(size_t)(j - 1) * S] = bb;
+    }
+    const double b = M4(ib, 1, 1) * G(ny + 1) + M4(ib, 1, 2) * G(ny) + M4(ib, 1, 3) * G(ny - 1) +
+                     M4(ib, 1, 4) * G(ny - 2);
+    bb = b + A3(icon, 1, ny) * bb;
+  } else {
+    bb = M4(ib, 3, 1) * G(1) + M4(ib, 3, 2) * G(2) + M4(ib, 3, 3) * G(3) + M4(ib, 3, 4) * G(4);
+    o[0] = bb;
+    for (int j = 2; j <= ny - 1; ++j) {
+      const double b = A2(econ, 2, j) * G(j) + A2(econ, 1, j) * G(j - 1);
+      bb = b + A3(icon, 1, j) * bb;
+      o[(size_t)(j - 1) * S] = bb;
+    }
+    const double b = M4(ib, 4, 1) * G(ny) + M4(ib, 4, 2) * G(ny - 1) + M4(ib, 4, 3) * G(ny - 2) +
+                     M4(ib, 4, 4) * G(ny - 3);
+    bb = b + A3(icon, 1, ny) * bb;
+  }
+  double x = bb * A3(icon, 2, ny);
+  o[(size_t)(ny - 1) * S] = x;
+  for (int j = ny - 1; j >= 1; --j) {
+    x = (o[(size_t)(j - 1) * S] - A3(icon, 3, j) * x) * A3(icon, 2, j);
+    o[(size_t)(j - 1) * S] = x;
+  }
+}
+
+// differzy, lip.f90:152-232 (not in place). which 0: u-type (dcyu, cofcyu,
+// chv=3, fwb1=-1, fwb2=0, jee=ny+1); which 1: v-type (dcyv, cofcyv, chv=1,
+// fwb1=0, fwb2=1, jee=ny). Reads rows 1..ny of g.
+__device__ __forceinline__ void col_differzy(const DCoef &c, const double *g, double *r, int which) {
+  const int ny = c.ny;
+  const size_t S = c.nz1;
+  const double *icon = which == 0 ? c.dcyu : c.dcyv;
+  const double *econ = which == 0 ? c.cofcyu : c.cofcyv;
+  const double *db = c.dcby;
+  const int chv = which == 0 ? 3 : 1, cha = chv + 1;
+  const int jee = which == 0 ? ny + 1 : ny;
+  auto G = [&](int j) { return g[(size_t)(j - 1) * S]; };
+  const double bot = M4(db, chv, 1) * G(1) + M4(db, chv, 2) * G(2) + M4(db, chv, 3) * G(3) + M4(db, chv, 4) * G(4);
+  const double top = M4(db, cha, 1) * G(ny) + M4(db, cha, 2) * G(ny - 1) + M4(db, cha, 3) * G(ny - 2) +
+                     M4(db, cha, 4) * G(ny - 3);
+  double x = bot;
+  r[0] = x;
+  for (int j = 2; j <= jee - 1; ++j) {
+    const double b = which == 0 ? A2(econ, 2, j) * G(j) + A2(econ, 1, j) * G(j - 1)
+                                : A2(econ, 2, j) * G(j + 1) + A2(econ, 1, j) * G(j);
+    x = b + A3(icon, 1, j) * x;
+    r[(size_t)(j - 1) * S] = x;
+  }
+  x = top + A3(icon, 1, jee) * x;
+  x = x * A3(icon, 2, jee);
+  r[(size_t)(jee - 1) * S] = x;
+  for (int j = jee - 1; j >= 1; --j) {
+    x = (r[(size_t)(j - 1) * S] - A3(icon, 3, j) * x) * A3(icon, 2, j);
+    r[(size_t)(j - 1) * S] = x;
+  }
+}
+
+// vistyy, lip.f90:447-513. which 0: u,w (viyu, cofvyu, jee=ny+1, ic=3);
+// which 1: v (viyv, cofvyv, jee=ny, ic=1).
+__device__ __forceinline__ void col_vistyy(const DCoef &c, const double *u, double *r, int which) {
+  const int ny = c.ny;
+  const size_t S = c.nz1;
+  const double *icon = which == 0 ? c.viyu : c.viyv;
+  const double *econ = which == 0 ? c.cofvyu : c.cofvyv;
+  const double *vb = c.cofvby;
+  const int jee = which == 0 ? ny + 1 : ny, ic = which == 0 ? 3 : 1;
+  auto U = [&](int j) { return u[(size_t)(j - 1) * S]; };
+  double x = M4(vb, ic, 1) * U(1) + M4(vb, ic, 2) * U(2) + M4(vb, ic, 3) * U(3) + M4(vb, ic, 4) * U(4);
+  r[0] = x;
+  for (int j = 2; j <= jee - 1; ++j) {
+    const double b = A3(econ, 1, j) * U(j + 1) + A3(econ, 2, j) * U(j) + A3(econ, 3, j) * U(j - 1);
+    x = b + A3(icon, 1, j) * x;
+    r[(size_t)(j - 1) * S] = x;
+  }
+  {
+    const double b = M4(vb, ic + 1, 1) * U(jee) + M4(vb, ic + 1, 2) * U(jee - 1) + M4(vb, ic + 1, 3) * U(jee - 2) +
+                     M4(vb, ic + 1, 4) * U(jee - 3);
+    x = b + A3(icon, 1, jee) * x;
+  }
+  x = x * A3(icon, 2, jee);
+  r[(size_t)(jee - 1) * S] = x;
+  for (int j = jee - 1; j >= 1; --j) {
+    x = (r[(size_t)(j - 1) * S] - A3(icon, 3, j) * x) * A3(icon, 2, j);
+    r[(size_t)(j - 1) * S] = x;
+  }
+}
+
+// implzy, lip.f90:528-597, with the LU of (A + var1*B) pre-factored by k_dt
+// into fac (a1,a2,a3 per row; raw a1(2) and a3(jee-1) after the rows).
+// res: right-hand side column (rows 1..jee); u: output column; rows 1 and
+// jee of u take the boundary values ub1 / ubj.
+__device__ __forceinline__ void col_implzy(const DCoef &c, const double *res, double *u, double ub1, double ubj,
+                                           const double *__restrict__ fac, int which) {
+  const int ny = c.ny;
+  const size_t S = c.nz1;
+  const double *icon = which == 0 ? c.vyui : c.vyvi;
+  const int jee = which == 0 ? ny + 1 : ny;
+  auto R = [&](int j) { return res[(size_t)(j - 1) * S]; };
+  const double a1raw = fac[3 * (jee + 1)], a3raw = fac[3 * (jee + 1) + 1];
+  double rm = R(1), r0 = R(2), rp;
+  double x = 0.0;
+  for (int j = 2; j <= jee - 1; ++j) {
+    rp = R(j + 1);
+    double t = A3(icon, 1, j) * rm + A3(icon, 2, j) * r0 + A3(icon, 3, j) * rp;
+    if (j == 2) t = t - a1raw * ub1;
+    if (j == jee - 1) t = t - a3raw * ubj;
+    if (j >= 3) t = t + fac[3 * j + 0] * x;
+    x = t;
+    u[(size_t)(j - 1) * S] = x;
+    rm = r0;
+    r0 = rp;
+  }
+  x = x * fac[3 * (jee - 1) + 1];
+  u[(size_t)(jee - 2) * S] = x;
+  for (int j = jee - 2; j >= 2; --j) {
+    x = (u[(size_t)(j - 1) * S] - fac[3 * j + 2] * x) * fac[3 * j + 1];
+    u[(size_t)(j - 1) * S] = x;
+  }
+  u[0] = ub1;
+  u[(size_t)(jee - 1) * S] = ubj;
+}
+
+// interpyy in Fourier space for u,w (which 0, jin = ny+1) and v (which 1).
+__global__ void __launch_bounds__(128) k_interpy(DCoef c, const double *__restrict__ in,
+                                                 double *__restrict__ out, int which) {
+  const int kr = blockIdx.x * blockDim.x + threadIdx.x;
+  if (kr >= c.nz1) return;
+  const int i = blockIdx.y + 1;
+  const int jin = which == 0 ? c.ny + 1 : c.ny;
+  const double *g = in + ((size_t)(i - 1) * jin) * c.nz1 + kr;
+  double *o = out + ((size_t)(i - 1) * c.ny) * c.nz1 + kr;
+  col_interpyy(c, g, o, which);
+}
+
+// ---------------------------------------------------------------------------
+// z-line transforms (fourxz, ffts.f90:27-67), one warp per line.
+// ---------------------------------------------------------------------------
+struct ZTab {
+  const double2 *tw;   // exp(-2 pi i t/M), t < M
+  const double2 *tw2;  // exp(-2 pi i t/nz), t < M
+  int M, nz, nz2;
+};
+
+// c2r of fou (nz2+1 complex modes, global) into buf (M complex = nz reals)
+__device__ __forceinline__ void line_c2r(const ZTab &z, const double *__restrict__ fou, double2 *buf, int lane) {
+  const int M = z.M, nz2 = z.nz2;
+  const double2 *f2 = reinterpret_cast<const double2 *>(fou);
+  for (int k = lane; k < M; k += 32) {
+    double2 a = k <= nz2 ? __ldg(f2 + k) : make_double2(0.0, 0.0);
+    if (k == 0) a.y = 0.0;  // c2r ignores Im X[0]
+    const int km = M - k;
+    double2 b = km <= nz2 ? __ldg(f2 + km) : make_double2(0.0, 0.0);
+    b.y = -b.y;
+    const double2 s = cadd(a, b), d = csub(a, b);
+    const double2 t = cmul(cconj(__ldg(z.tw2 + k)), d);  // W^{-k} d
+    buf[k] = make_double2(s.x - t.y, s.y + t.x);          // s + i t
+  }
+  __syncwarp();
+  warp_fft<1>(buf, M, z.tw, lane);
+}
+
+// r2c of buf (nz reals packed as M complex) into fou (modes 0..nz2) x 1/nz
+__device__ __forceinline__ void line_r2c(const ZTab &z, double2 *buf, double *__restrict__ fou, int lane) {
+  const int M = z.M, nz2 = z.nz2;
+  warp_fft<-1>(buf, M, z.tw, lane);
+  const double dnf = 1.0 / (double)z.nz;
+  double2 *f2 = reinterpret_cast<double2 *>(fou);
+  for (int k = lane; k <= nz2; k += 32) {
+    const double2 zk = buf[k];
+    const double2 zc = cconj(buf[(M - k) & (M - 1)]);
+    const double2 e = make_double2(0.5 * (zk.x + zc.x), 0.5 * (zk.y + zc.y));
+    const double2 d = csub(zk, zc);
+    const double2 o = make_double2(0.5 * d.y, -0.5 * d.x);  // -i d / 2
+    const double2 xk = cadd(e, cmul(__ldg(z.tw2 + k), o));
+    f2[k] = make_double2(dnf * xk.x, dnf * xk.y);
+  }
+  __syncwarp();
+}
+
+__device__ __forceinline__ void buf_mul(double2 *a, const double2 *b, int M, int lane) {
+  for (int t = lane; t < M; t += 32) {
+    const double2 x = a[t], y = b[t];
+    a[t] = make_double2(x.x * y.x, x.y * y.y);
+  }
+  __syncwarp();
+}
+__device__ __forceinline__ void buf_sq(double2 *a, int M, int lane) {
+  for (int t = lane; t < M; t += 32) {
+    const double2 x = a[t];
+    a[t] = make_double2(x.x * x.x, x.y * x.y);
+  }
+  __syncwarp();
+}
+__device__ __forceinline__ double buf_absmax(const double2 *a, int M, int lane) {
+  double m = 0.0;
+  for (int t = lane; t < M; t += 32) m = nmax(nmax(m, fabs(a[t].x)), fabs(a[t].y));
+  return m;
+}
+
+struct ProdArgs {
+  const double *u, *v, *w, *ux, *vx, *wx, *uy, *wy, *vy;
+  double *uu, *uw, *uv, *vw, *vv, *ww;
+  unsigned long long *vm_bits;
+  DState *st;
+  int setstep;
+};
+
+// rhsp.F90:120-171 (uu, uw, uv and the CFL maxima, all planes) and
+// rhsp.F90:367-415 (vw, vv, ww, planes 2..nx-1); one warp per (i, j) line.
+__global__ void __launch_bounds__(128) k_products(DCoef c, ZTab z, ProdArgs a) {
+  extern __shared__ double2 sm[];
+  const int M = z.M, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int j = blockIdx.x * 4 + wid + 1;
+  const int i = blockIdx.y + 1;
+  const int nx = c.nx, ny = c.ny, nz1 = c.nz1;
+  if (j > ny + 1) return;
+  double2 *A = sm + (size_t)wid * 3 * M, *B = A + M, *P = B + M;
+  const size_t offu = ((size_t)(i - 1) * (ny + 1) + (j - 1)) * nz1;
+  const size_t offv = ((size_t)(i - 1) * ny + (j - 1)) * nz1;
+  double mu = 0.0, mw = 0.0, mv = 0.0;
+  line_c2r(z, a.u + offu, P, lane);
+  if (a.setstep) mu = buf_absmax(P, M, lane);
+  line_c2r(z, a.ux + offu, A, lane);
+  buf_sq(A, M, lane);
+  line_r2c(z, A, a.uu + offu, lane);
+  line_c2r(z, a.wx + offu, A, lane);
+  if (a.setstep) mw = buf_absmax(A, M, lane);
+  buf_mul(A, P, M, lane);
+  line_r2c(z, A, a.uw + offu, lane);
+  if (j <= ny) {
+    line_c2r(z, a.vx + offv, A, lane);
+    if (a.setstep) mv = buf_absmax(A, M, lane);
+    line_c2r(z, a.uy + offv, B, lane);
+    buf_mul(A, B, M, lane);
+    line_r2c(z, A, a.uv + offv, lane);
+    if (i >= 2 && i <= nx - 1) {
+      line_c2r(z, a.v + offv, A, lane);
+      line_c2r(z, a.wy + offv, B, lane);
+      buf_mul(A, B, M, lane);
+      line_r2c(z, A, a.vw + offv, lane);
+      line_c2r(z, a.vy + offv, A, lane);
+      buf_sq(A, M, lane);
+      line_r2c(z, A, a.vv + offv, lane);
+      line_c2r(z, a.w + offu, A, lane);
+      buf_sq(A, M, lane);
+      line_r2c(z, A, a.ww + offv, lane);
+    }
+  }
+  if (a.setstep) {
+    mu = warp_nmax(mu);
+    mw = warp_nmax(mw);
+    mv = warp_nmax(mv);
+    if (lane == 0) {
+      atomicMax(&a.st->umax_bits, (unsigned long long)__double_as_longlong(mu));
+      atomicMax(&a.st->wmax_bits, (unsigned long long)__double_as_longlong(mw));
+      if (j <= ny) atomicMax(&a.vm_bits[j], (unsigned long long)__double_as_longlong(mv));
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// dt (rhsp.F90:214-267), RK3 factors, implzy LU (lip.f90:545-568)
+// ---------------------------------------------------------------------------
+__device__ void implzy_factor(const DCoef &c, double *fac, int which, double var1) {
+  const int ny = c.ny, jee = which == 0 ? ny + 1 : ny;
+  const double *icon = which == 0 ? c.vyui : c.vyvi;
+  const double *econ = which == 0 ? c.cofvyu : c.cofvyv;
+  for (int j = 2; j <= jee - 1; ++j) {
+    fac[3 * j + 0] = A3(icon, 1, j) + var1 * A3(econ, 3, j);
+    fac[3 * j + 1] = A3(icon, 2, j) + var1 * A3(econ, 2, j);
+    fac[3 * j + 2] = A3(icon, 3, j) + var1 * A3(econ, 1, j);
+  }
+  fac[3 * (jee + 1)] = fac[3 * 2 + 0];
+  fac[3 * (jee + 1) + 1] = fac[3 * (jee - 1) + 2];
+  fac[3 * 2 + 0] = 0.0;
+  fac[3 * (jee - 1) + 2] = 0.0;
+  for (int j = 3; j <= jee - 1; ++j) {
+    const double d = 1.0 / fac[3 * (j - 1) + 1];
+    fac[3 * (j - 1) + 1] = d;
+    fac[3 * j + 0] = -fac[3 * j + 0] * d;
+    fac[3 * j + 1] = fac[3 * j + 1] + fac[3 * j + 0] * fac[3 * (j - 1) + 2];
+  }
+  fac[3 * (jee - 1) + 1] = 1.0 / fac[3 * (jee - 1) + 1];
+}
+
+__global__ void k_dt(DCoef c, DState *st, const unsigned long long *vm_bits, double *fac_u, double *fac_v, int m,
+                     int setstep, int dt_mode, double dt_fixed) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double *S = c.S;
+  if (setstep) {
+    const double poco = 1e-7;
+    const double um = __longlong_as_double((long long)st->umax_bits);
+    const double wm = __longlong_as_double((long long)st->wmax_bits);
+    const double dt1 = S[OTBL_S_DXMIN] / fmax(poco, um);
+    const double dt2 = S[OTBL_S_DXMIN] / fmax(poco, wm);
+    double dt3 = DBL_MAX, vmax = 0.0;
+    for (int j = 1; j <= c.ny; ++j) {
+      const double vm = __longlong_as_double((long long)vm_bits[j]);
+      dt3 = fmin(dt3, c.dymin[j - 1] / fmax(poco, vm));
+      vmax = nmax(vmax, vm);
+    }
+    const double dtloc = fmin(fmin(dt1, dt2), fmin(dt3, S[OTBL_S_DTRET]));
+    st->umax = um;
+    st->wmax = wm;
+    st->vmax = vmax;
+    if (!isfinite(um) || !isfinite(wm) || !isfinite(vmax)) st->err = OTBL_ERR_NAN;
+    if (dt_mode == OTBL_DT_ADAPTIVE) {
+      st->dt = dtloc;
+    } else if (!st->dt_frozen) {
+      st->dt = dt_fixed > 0.0 ? dt_fixed : dtloc;
+      st->dt_frozen = 1;
+    }
+  }
+  const double dt = st->dt;
+  if (!(dt > 0.0) || !isfinite(dt)) st->err = OTBL_ERR_NAN;
+  const int q = m - 1;
+  st->var1 = dt * (S[OTBL_S_RKCV + q] + S[OTBL_S_RKDV + q]);
+  st->var2 = dt * S[OTBL_S_REX] * S[OTBL_S_RKCV + q];
+  st->var3 = dt * S[OTBL_S_RKC + q];
+  st->var4 = dt * S[OTBL_S_RKD + q];
+  st->rkk = S[OTBL_S_REX] * dt * S[OTBL_S_RKDV + q];
+  st->varstep = 5e-1 / dt / S[OTBL_S_RKDV + q];
+  implzy_factor(c, fac_u, 0, st->rkk);
+  implzy_factor(c, fac_v, 1, st->rkk);
+}
+
+__global__ void k_reset_max(DState *st, unsigned long long *vm_bits, int ny) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t == 0) {
+    st->umax_bits = 0ull;
+    st->wmax_bits = 0ull;
+  }
+  if (t <= ny) vm_bits[t] = 0ull;
+}
+
+__global__ void k_tiempo(DState *st) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) st->tiempo = st->tiempo + st->dt;
+}
+
+// ---------------------------------------------------------------------------
+// genflu (genflu.F90:3-242, NEWGENFLU) on one CTA, followed by boun on plane
+// 1 (boun.f90:33-55) and rhs*pa(plane 1) = 0 (rhsp.F90:424-426,441-442).
+// ---------------------------------------------------------------------------
+struct GenArgs {
+  double *u, *v, *w, *rhsupa, *rhsvpa, *rhswpa;
+  const double *u0, *v0;
+  double *um;
+  double *wk;  // nz1*(ny+2) scratch
+  DState *st;
+};
+
+__device__ void dobleu_dev(const double *eta, double *www, double *www1, int n) {
+  const double ag = 4.0, bg = 0.2, w1default = (double)0.7895f;
+  const double bg2 = 1.0 - 2.0 * bg, tag = 1.0 / tanh(ag);
+  *www1 = w1default;
+  www[1] = 0.0;
+  for (int i = 2; i <= n; ++i) {
+    const double xxx = 0.5 * (eta[i] + eta[i - 1]);
+    const double yyy = xxx >= 1.0 ? 1.0 : 0.5 * (1.0 + tag * tanh(ag * (xxx - bg) / (bg2 * xxx + bg)));
+    www[i] = www[i - 1] + yyy * (eta[i] - eta[i - 1]);
+    if (eta[i] >= 1.0 && eta[i - 1] < 1.0) *www1 = www[i - 1] + (1.0 - eta[i - 1]) * yyy;
+  }
+}
+
+// profile, genflu.F90:204-242, on plane 1 of a field with n rows
+__device__ void profile_dev(const DCoef &c, double *ut, double *wk, int ntop, const int *kl, const double *fsca,
+                            int n, double ggg) {
+  const int nz1 = c.nz1, ny = c.ny, t = threadIdx.x, T = blockDim.x;
+  const int nk = nz1 - 2;
+  if (n == ny + 1) {
+    for (int e = t; e < ntop * nk; e += T) {
+      const int i = e / nk + 1, k = e % nk + 2, kll = max(kl[i], 1);
+      wk[(size_t)i * nz1 + k] = ut[(size_t)(kll + 1) * nz1 + k] * fsca[i] + ut[(size_t)kll * nz1 + k] * (1 - fsca[i]);
+    }
+    __syncthreads();
+    for (int k = t + 2; k < nz1; k += T) wk[k] = -wk[(size_t)nz1 + k];
+  } else {
+    for (int e = t; e < ntop * nk; e += T) {
+      const int i = e / nk + 1, k = e % nk + 2, kll = max(kl[i], 1);
+      wk[(size_t)(i - 1) * nz1 + k] =
+          ut[(size_t)kll * nz1 + k] * fsca[i] + ut[(size_t)(kll - 1) * nz1 + k] * (1 - fsca[i]);
+    }
+  }
+  __syncthreads();
+  const int i0 = ntop - 2;
+  for (int e = t; e < (n - i0 + 1) * nk; e += T) {
+    const int i = e / nk + i0, k = e % nk + 2;
+    wk[(size_t)(i - 1) * nz1 + k] = wk[(size_t)(ntop - 4) * nz1 + k];
+  }
+  __syncthreads();
+  for (int e = t; e < n * nk; e += T) {
+    const int i = e / nk + 1, k = e % nk + 2;
+    ut[(size_t)(i - 1) * nz1 + k] = wk[(size_t)(i - 1) * nz1 + k] * ggg;
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(512) k_genflu(DCoef c, GenArgs a) {
+  extern __shared__ double gsm[];
+  const int ny = c.ny, nz1 = c.nz1, xout = c.xout, t = threadIdx.x, T = blockDim.x;
+  const size_t PU = (size_t)(ny + 1) * nz1, PV = (size_t)ny * nz1;
+  const double *y = c.y, *dy = c.dy;
+  const double yb = c.S[OTBL_S_YBLEND];
+  double *fsca = gsm;                              // 2*(ny+1)
+  double *ysca = fsca + 2 * (ny + 1);              // ny+1
+  double *wlwa = ysca + (ny + 1);                  // ny+1
+  int *kl = reinterpret_cast<int *>(wlwa + (ny + 1));  // 2*(ny+1)
+  __shared__ int ntop[2];
+  __shared__ double ggg;
+  // plane xout -> plane 1 with the blending of genflu.F90:55-60
+  for (size_t e = t; e < PU; e += T) {
+    const int j = (int)(e / nz1) + 1, kr = (int)(e % nz1);
+    double uv = a.u[(size_t)(xout - 1) * PU + e], wv = a.w[(size_t)(xout - 1) * PU + e];
+    if (kr >= 2) {
+      const double fb = 0.5 * (1 - tanh(y[j] - yb));
+      uv = uv * fb;
+      wv = wv * fb;
+    }
+    a.u[e] = uv;
+    a.w[e] = wv;
+  }
+  for (size_t e = t; e < PV; e += T) a.v[e] = a.v[(size_t)(xout - 1) * PV + e];
+  __syncthreads();
+  if (t == 0) {
+    DState *st = a.st;
+    const double re = c.S[OTBL_S_RE], din = c.S[OTBL_S_DIN], rthin = c.S[OTBL_S_RTHIN];
+    const double dt = st->dt, tloc = st->tiempo - st->timeinit;
+    double timec;
+    if (tloc < 20)
+      timec = 20;
+    else if (tloc < 100)
+      timec = 100;
+    else
+      timec = tloc;
+    st->timec = timec;
+    double *um = a.um - 1;
+    for (int j = 1; j <= ny + 1; ++j) um[j] = (dt / timec) * a.u[(size_t)(j - 1) * nz1] + um[j] * (1.0 - dt / timec);
+    st->utauout = sqrt(fabs((um[2] - um[1]) / (y[2] - y[1]) / re));
+    double uinf = 0.0;
+    for (int j = ny + 1 - 20; j <= ny + 1 - 5; ++j) uinf += um[j];
+    uinf = uinf / 16.0;
+    const double u99 = (double)0.99f * uinf;
+    int jtop = 0;
+    for (int j = 1; j <= ny - 2; ++j) {
+      if (um[j] >= u99) break;
+      jtop = j + 1;
+    }
+    st->dout = y[jtop];
+    double s = 0.0;
+    for (int q = 0; q < jtop + 2; ++q) s += (uinf - um[2 + q]) * um[2 + q] * dy[1 + q];
+    st->rthout = s * re / uinf;
+    st->gamma2 = rthin / st->rthout;
+    st->gamma1 = pow(st->gamma2, 0.125);
+    ggg = 1.0 / st->gamma1;
+    for (int kk = 1; kk <= 2; ++kk) {
+      for (int j = 1; j <= ny; ++j) ysca[j] = kk == 1 ? 5e-1 * (y[j] + y[j + 1]) / din : y[j] / din;
+      double www1;
+      dobleu_dev(ysca, wlwa, &www1, ny);
+      for (int j = 1; j <= ny; ++j)
+        wlwa[j] = ysca[j] / st->gamma1 + (1.0 / st->gamma2 - 1.0 / st->gamma1) / www1 * wlwa[j];
+      int kll = 1;
+      int *klk = kl + (kk - 1) * (ny + 1);
+      double *fk = fsca + (kk - 1) * (ny + 1);
+      ntop[kk - 1] = 0;
+      for (int j = 0; j <= ny; ++j) {
+        klk[j] = 0;
+        fk[j] = 0.0;
+      }
+      for (int i = 1; i <= ny; ++i) {
+        if (wlwa[i] <= ysca[ny]) {
+          ntop[kk - 1] = i;
+          int khh = ny;
+          while (khh - kll > 1) {
+            const int kx = (khh + kll) / 2;
+            if (ysca[kx] >= wlwa[i])
+              khh = kx;
+            else
+              kll = kx;
+          }
+          klk[i] = kll;
+          fk[i] = (wlwa[i] - ysca[kll]) / (ysca[khh] - ysca[kll]);
+        }
+      }
+    }
+  }
+  __syncthreads();
+  // zero mode, genflu.F90:146-150
+  for (int j = t + 1; j <= ny + 1; j += T) {
+    a.u[(size_t)(j - 1) * nz1] = a.u0[j - 1];
+    a.u[(size_t)(j - 1) * nz1 + 1] = 0.0;
+    a.w[(size_t)(j - 1) * nz1] = 0.0;
+    a.w[(size_t)(j - 1) * nz1 + 1] = 0.0;
+    if (j <= ny) {
+      a.v[(size_t)(j - 1) * nz1] = a.v0[j - 1];
+      a.v[(size_t)(j - 1) * nz1 + 1] = 0.0;
+    }
+  }
+  __syncthreads();
+  // a rescaled grid with fewer than 4 points inside the box (only reachable
+  // with non-finite integral quantities) cannot be profiled: flag it
+  if (ntop[0] >= 4 && ntop[1] >= 4) {
+    profile_dev(c, a.u, a.wk, ntop[0], kl, fsca, ny + 1, ggg);
+    profile_dev(c, a.w, a.wk, ntop[0], kl, fsca, ny + 1, ggg);
+    profile_dev(c, a.v, a.wk, ntop[1], kl + (ny + 1), fsca + (ny + 1), ny, ggg);
+  } else if (t == 0) {
+    a.st->err = OTBL_ERR_NAN;
+  }
+  // boun on plane 1 and the plane-1 RHS history
+  const double *ib = c.inby, *cc = c.ccon;
+  for (int kr = t; kr < nz1; kr += T) {
+    a.v[kr] = 0.0;
+    a.v[(size_t)(ny - 1) * nz1 + kr] = kr == 0 ? c.vmagic[0] : 0.0;
+    double *fl[2] = {a.u, a.w};
+    for (int f = 0; f < 2; ++f) {
+      double *q = fl[f] + kr;
+      q[0] = -1.0 / M4(ib, 2, 1) * (M4(ib, 2, 2) * q[nz1] + M4(ib, 2, 3) * q[2 * nz1] + M4(ib, 2, 4) * q[3 * nz1]);
+      q[(size_t)ny * nz1] = -1.0 / M2(cc, 1, 1) *
+                            (M2(cc, 1, 2) * q[(size_t)(ny - 1) * nz1] + M2(cc, 1, 3) * q[(size_t)(ny - 2) * nz1] +
+                             M2(cc, 1, 4) * q[(size_t)(ny - 3) * nz1]);
+    }
+  }
+  for (size_t e = t; e < PU; e += T) {
+    a.rhsupa[e] = 0.0;
+    a.rhswpa[e] = 0.0;
+  }
+  for (size_t e = t; e < PV; e += T) a.rhsvpa[e] = 0.0;
+}
+
+// ---------------------------------------------------------------------------
+// tail of rhsp (rhsp.F90:291-484) for planes 2..nx, one thread per column.
+// ---------------------------------------------------------------------------
+struct FinalArgs {
+  double *u, *v, *w;                 // state: old on entry, new on exit
+  const double *p;
+  double *rhsupa, *rhsvpa, *rhswpa;  // old on entry, new on exit
+  double *cu, *cv, *cw;              // difvisxx outputs; become rhsu/v/w
+  const double *uv, *uw, *vw, *vv, *ww;
+  double *s1, *s2, *s3;
+  const double *fac_u, *fac_v;
+  const DState *st;
+};
+
+__global__ void __launch_bounds__(128) k_final(DCoef c, FinalArgs a) {
+  const int kr = blockIdx.x * blockDim.x + threadIdx.x;
+  if (kr >= c.nz1) return;
+  const int i = blockIdx.y + 2;
+  const int nx = c.nx, ny = c.ny, nz1 = c.nz1;
+  const size_t S = nz1;
+  const int k = kr >> 1, odd = kr & 1, pof = odd ? -1 : 1;
+  const double kz = c.kaz[k], kv = c.kvis[k];
+  const bool last = (i == nx);
+  const size_t bu = (size_t)(i - 1) * (ny + 1) * nz1 + kr, bv = (size_t)(i - 1) * ny * nz1 + kr;
+  const double var1 = a.st->var1, var3 = a.st->var3, var4 = a.st->var4;
+  const double v2 = last ? 0.0 : a.st->var2;
+  const double idxx = c.S[OTBL_S_IDXX];
+  // (x * kaz) for the component kr of a complex column x: kaz = (0, kz)
+  auto kazm = [&](const double *col, int j) {
+    const double q = col[(size_t)(j - 1) * S + pof];
+    return odd ? kz * q : -kz * q;
+  };
+  double *s1 = a.s1 + bu, *s2 = a.s2 + bu, *s3 = a.s3 + bu;
+  double *uc = a.u + bu, *vc = a.v + bv, *wc = a.w + bu;
+  const double *pc = a.p + bv;
+  const double *ib = c.inby, *cc = c.ccon;
+  // ---- rhsv (rows 1..ny) ----
+  double *rv = a.cv + bv;
+  if (!last) col_differzy(c, a.vv + bv, s2, 1);
+  for (int j = 1; j <= ny; ++j) {
+    double r = rv[(j - 1) * S];
+    if (!last) {
+      if (j >= 2 && j <= ny - 1) r = r - vc[(j - 1) * S] * kv;
+      r = r + kazm(a.vw + bv, j);
+      r = r + s2[(j - 1) * S];
+    }
+    if (j == 1 || j == ny) r = 0.0;
+    rv[(j - 1) * S] = r;
+  }
+  // ---- rhsu (rows 1..ny+1) ----
+  double *ru = a.cu + bu;
+  if (!last) col_differzy(c, a.uv + bv, s1, 0);
+  for (int j = 1; j <= ny + 1; ++j) {
+    double r;
+    if (!last) {
+      r = s1[(j - 1) * S] + kazm(a.uw + bu, j);
+      r = r + ru[(j - 1) * S];
+      if (j >= 2 && j <= ny) r = r - uc[(j - 1) * S] * kv;
+    } else {
+      r = ru[(j - 1) * S];
+    }
+    ru[(j - 1) * S] = r;
+  }
+  ru[0] = -1.0 / M4(ib, 2, 1) * (M4(ib, 2, 2) * ru[S] + M4(ib, 2, 3) * ru[2 * S] + M4(ib, 2, 4) * ru[3 * S]);
+  ru[(size_t)ny * S] = 0.0;
+  // ---- rhsw (rows 1..ny+1) ----
+  double *rw = a.cw + bu;
+  if (!last) col_differzy(c, a.vw + bv, s3, 0);
+  for (int j = 1; j <= ny + 1; ++j) {
+    double r = rw[(j - 1) * S];
+    if (!last) {
+      if (j >= 2 && j <= ny) r = r - wc[(j - 1) * S] * kv;
+      r = r + s3[(j - 1) * S];
+      if (j <= ny) r = r + kazm(a.ww + bv, j);
+    }
+    rw[(j - 1) * S] = r;
+  }
+  rw[0] = -1.0 / M4(ib, 2, 1) * (M4(ib, 2, 2) * rw[S] + M4(ib, 2, 3) * rw[2 * S] + M4(ib, 2, 4) * rw[3 * S]);
+  rw[(size_t)ny * S] = 0.0;
+
+  // ---- v: pressure gradient, boun, vistyy, RK3 combination, implzy ----
+  {
+    auto vs = [&](int j) {
+      if (j == 1) return 0.0;
+      if (j == ny) return kr == 0 ? c.vmagic[i - 1] : 0.0;
+      return vc[(j - 1) * S] - var1 * c.idyy[j - 1] * (pc[(size_t)j * S] - pc[(size_t)(j - 1) * S]);
+    };
+    col_vistyy(c, vc, s2, 1);
+    double *hp = a.rhsvpa + bv;
+    for (int j = 1; j <= ny; ++j) {
+      const double wk = vs(j) - (var3 * rv[(j - 1) * S] + v2 * s2[(j - 1) * S] + var4 * hp[(j - 1) * S]);
+      s2[(j - 1) * S] = wk;
+      hp[(j - 1) * S] = rv[(j - 1) * S];
+    }
+    col_implzy(c, s2, vc, 0.0, vs(ny), a.fac_v, 1);
+  }
+  // ---- u ----
+  {
+    const double *pn = pc + (size_t)ny * nz1;  // plane i+1
+    auto us = [&](int j) {
+      const double q = uc[(j - 1) * S];
+      if (last) return q;
+      return q - var1 * idxx * (pn[(size_t)(j - 1) * S] - pc[(size_t)(j - 1) * S]);
+    };
+    const double u2 = us(2), u3 = us(3), u4 = us(4);
+    const double un = us(ny), un1 = us(ny - 1), un2 = us(ny - 2);
+    const double ub1 = -1.0 / M4(ib, 2, 1) * (M4(ib, 2, 2) * u2 + M4(ib, 2, 3) * u3 + M4(ib, 2, 4) * u4);
+    const double ubt = -1.0 / M2(cc, 1, 1) * (M2(cc, 1, 2) * un + M2(cc, 1, 3) * un1 + M2(cc, 1, 4) * un2);
+    col_vistyy(c, uc, s1, 0);
+    double *hp = a.rhsupa + bu;
+    for (int j = 1; j <= ny + 1; ++j) {
+      const double usj = j == 1 ? ub1 : (j == ny + 1 ? ubt : us(j));
+      const double wk = usj - (var3 * ru[(j - 1) * S] + v2 * s1[(j - 1) * S] + var4 * hp[(j - 1) * S]);
+      s1[(j - 1) * S] = wk;
+      hp[(j - 1) * S] = ru[(j - 1) * S];
+    }
+    col_implzy(c, s1, uc, ub1, ubt, a.fac_u, 0);
+  }
+  // ---- w ----
+  {
+    auto ws = [&](int j) {
+      const double q = wc[(j - 1) * S];
+      const double pp = pc[(size_t)(j - 1) * S + pof];
+      const double av = var1 * kz;
+      return q - (odd ? av * pp : -av * pp);
+    };
+    const double w2 = ws(2), w3 = ws(3), w4 = ws(4);
+    const double wn = ws(ny), wn1 = ws(ny - 1), wn2 = ws(ny - 2);
+    const double wb1 = -1.0 / M4(ib, 2, 1) * (M4(ib, 2, 2) * w2 + M4(ib, 2, 3) * w3 + M4(ib, 2, 4) * w4);
+    const double wbt = -1.0 / M2(cc, 1, 1) * (M2(cc, 1, 2) * wn + M2(cc, 1, 3) * wn1 + M2(cc, 1, 4) * wn2);
+    col_vistyy(c, wc, s3, 0);
+    double *hp = a.rhswpa + bu;
+    for (int j = 1; j <= ny + 1; ++j) {
+      const double wsj = j == 1 ? wb1 : (j == ny + 1 ? wbt : ws(j));
+      const double wk = wsj - (var3 * rw[(j - 1) * S] + v2 * s3[(j - 1) * S] + var4 * hp[(j - 1) * S]);
+      s3[(j - 1) * S] = wk;
+      hp[(j - 1) * S] = rw[(j - 1) * S];
+    }
+    col_implzy(c, s3, wc, wb1, wbt, a.fac_u, 0);
+  }
+}
+
+// boun (boun.f90:7-56) on every plane, for the standalone entry point
+__global__ void k_boun(DCoef c, double *u, double *v, double *w) {
+  const int kr = blockIdx.x * blockDim.x + threadIdx.x;
+  if (kr >= c.nz1) return;
+  const int i = blockIdx.y + 1, ny = c.ny, nz1 = c.nz1;
+  const double *ib = c.inby, *cc = c.ccon;
+  double *vc = v + (size_t)(i - 1) * ny * nz1 + kr;
+  vc[0] = 0.0;
+  vc[(size_t)(ny - 1) * nz1] = kr == 0 ? c.vmagic[i - 1] : 0.0;
+  double *fl[2] = {u + (size_t)(i - 1) * (ny + 1) * nz1 + kr, w + (size_t)(i - 1) * (ny + 1) * nz1 + kr};
+  for (int f = 0; f < 2; ++f) {
+    double *q = fl[f];
+    q[0] = -1.0 / M4(ib, 2, 1) * (M4(ib, 2, 2) * q[nz1] + M4(ib, 2, 3) * q[2 * nz1] + M4(ib, 2, 4) * q[3 * nz1]);
+    q[(size_t)ny * nz1] = -1.0 / M2(cc, 1, 1) *
+                          (M2(cc, 1, 2) * q[(size_t)(ny - 1) * nz1] + M2(cc, 1, 3) * q[(size_t)(ny - 2) * nz1] +
+                           M2(cc, 1, 4) * q[(size_t)(ny - 3) * nz1]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// outflow_correction, boun.f90:63-93: one CTA, fixed-order reductions.
+// ---------------------------------------------------------------------------
+__device__ double block_sum(double v, double *red) {
+  const int t = threadIdx.x;
+  red[t] = v;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (t < s) red[t] = red[t] + red[t + s];
+    __syncthreads();
+  }
+  const double r = red[0];
+  __syncthreads();
+  return r;
+}
+
+__global__ void __launch_bounds__(256) k_outflow(DCoef c, double *u, const double *v, double *rhsupa) {
+  __shared__ double red[256];
+  const int t = threadIdx.x, nx = c.nx, ny = c.ny, nz1 = c.nz1;
+  const size_t PU = (size_t)(ny + 1) * nz1, PV = (size_t)ny * nz1;
+  double a = 0.0, b = 0.0, d = 0.0;
+  for (int i = 2 + t; i <= nx; i += 256) a += v[(size_t)(i - 1) * PV + (size_t)(ny - 1) * nz1];
+  for (int j = 2 + t; j <= ny; j += 256) {
+    b += u[(size_t)(j - 1) * nz1] * c.dy[j - 1];
+    d += u[(size_t)(nx - 1) * PU + (size_t)(j - 1) * nz1] * c.dy[j - 1];
+  }
+  const double sv = block_sum(a, red), s1 = block_sum(b, red), s2 = block_sum(d, red);
+  double sumax = sv * c.S[OTBL_S_DX1];
+  sumax = sumax - s1;
+  sumax = sumax + s2;
+  const double alpha = -sumax / (c.y[ny] - c.y[1]);
+  for (int j = 2 + t; j <= ny; j += 256) {
+    double *q = u + (size_t)(nx - 1) * PU + (size_t)(j - 1) * nz1;
+    q[0] = q[0] + alpha;
+    double *h = rhsupa + (size_t)(nx - 1) * PU + (size_t)(j - 1) * nz1;
+    h[0] = h[0] + alpha * c.S[OTBL_S_IDX];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// pois (pois.f90:11-189)
+// ---------------------------------------------------------------------------
+struct XTab {
+  const double2 *tw;   // exp(-2 pi i t/n), t < n
+  const double2 *tw2;  // exp(-i pi t/(2n)), t < n
+  int n;
+};
+
+// divergence (pois.f90:41-54) + DCT-II along x (cosftx iopt=-1) for two
+// spanwise modes (k0, k0+1) of one row j; output phi-hat in plane layout
+// (v-type, plane i = mode index + 2). Mode 0 made real (pois.f90:102).
+__global__ void __launch_bounds__(256) k_pois_fwd(DCoef c, XTab x, const double *__restrict__ u,
+                                                 const double *__restrict__ v, const double *__restrict__ w,
+                                                 double *__restrict__ phi) {
+  extern __shared__ double2 xsm[];
+  const int n = x.n, ny = c.ny, nz1 = c.nz1, nz2 = c.nz2, xr = c.xround;
+  const int j = blockIdx.y + 1;
+  const int k0 = blockIdx.x * 2;
+  const size_t PU = (size_t)(ny + 1) * nz1, PV = (size_t)ny * nz1;
+  const double idx = c.S[OTBL_S_IDX], idy = c.idy[j];
+  for (int e = threadIdx.x; e < 2 * n; e += 256) {
+    const int l = e / n, tt = e % n;
+    const int k = k0 + l;
+    double2 val = make_double2(0.0, 0.0);
+    if (k <= nz2) {
+      const int i = tt + 2;
+      const double kz = c.kaz[k];
+      const double2 wv = *reinterpret_cast<const double2 *>(w + (size_t)(i - 1) * PU + (size_t)j * nz1 + 2 * k);
+      const double2 v1 = *reinterpret_cast<const double2 *>(v + (size_t)(i - 1) * PV + (size_t)j * nz1 + 2 * k);
+      const double2 v0 = *reinterpret_cast<const double2 *>(v + (size_t)(i - 1) * PV + (size_t)(j - 1) * nz1 + 2 * k);
+      const double2 ua = *reinterpret_cast<const double2 *>(u + (size_t)(i - 1) * PU + (size_t)j * nz1 + 2 * k);
+      const double2 ub = *reinterpret_cast<const double2 *>(u + (size_t)(i - 2) * PU + (size_t)j * nz1 + 2 * k);
+      double re = -kz * wv.y + (v1.x - v0.x) * idy;
+      double im = kz * wv.x + (v1.y - v0.y) * idy;
+      re = re + idx * (ua.x - ub.x);
+      im = im + idx * (ua.y - ub.y);
+      val = make_double2(rnd(re, xr), rnd(im, xr));
+    }
+    const int dst = (tt & 1) ? n - 1 - (tt >> 1) : (tt >> 1);
+    xsm[l * n + dst] = val;
+  }
+  __syncthreads();
+  block_fft<-1, 2>(xsm, n, x.tw);
+  const double dnf = 1.0 / (double)n;
+  for (int e = threadIdx.x; e < 2 * n; e += 256) {
+    const int l = e / n, kk = e % n;
+    const int k = k0 + l;
+    if (k > nz2) continue;
+    const double2 V = xsm[l * n + kk], Vm = xsm[l * n + (kk == 0 ? 0 : n - kk)];
+    const double2 wq = __ldg(x.tw2 + kk);
+    const double2 y = cadd(cmul(wq, V), cmul(cconj(wq), Vm));
+    double re = rnd(dnf * y.x, xr), im = rnd(dnf * y.y, xr);
+    if (k == 0) im = 0.0;
+    double *o = phi + (size_t)(kk + 1) * PV + (size_t)(j - 1) * nz1 + 2 * k;
+    o[0] = re;
+    o[1] = im;
+  }
+}
+
+// tridiagonal solve in y per (x-mode, kz), pois.f90:106-117 + soltriy;
+// one thread per column (plane i >= 2, real index kr); dinv scratch.
+__global__ void __launch_bounds__(128) k_pois_solve(DCoef c, double *phi, double *dinv) {
+  const int kr = blockIdx.x * blockDim.x + threadIdx.x;
+  if (kr >= c.nz1) return;
+  const int i = blockIdx.y + 2, ny = c.ny, ny1 = ny - 1, nz1 = c.nz1;
+  const size_t S = nz1;
+  const int k = kr >> 1;
+  double *col = phi + (size_t)(i - 1) * ny * nz1 + kr;
+  double *dv = dinv + (size_t)(i - 1) * ny * nz1 + kr;
+  const double *ayp = c.ayp;
+  const double shift_k = c.kaz2[k], shift_x = c.kmod[i - 2];
+  const bool sing = (i == 2 && k == 0);
+  if (sing) col[(size_t)(ny1 - 1) * S] = 0.0;
+  auto a2 = [&](int j) {
+    if (sing && j == ny1) return 2.0 * A3(ayp, 2, ny1);
+    return A3(ayp, 2, j) - shift_k - shift_x;
+  };
+  double a2p = a2(1);
+  double us = col[0];
+  for (int j = 2; j <= ny1; ++j) {
+    const double d = 1.0 / a2p;
+    dv[(size_t)(j - 2) * S] = d;
+    const double l = -A3(ayp, 1, j) * d;
+    a2p = a2(j) + l * A3(ayp, 3, j - 1);
+    us = col[(size_t)(j - 1) * S] + l * us;
+    col[(size_t)(j - 1) * S] = us;
+  }
+  double xv = us * (1.0 / a2p);
+  col[(size_t)(ny1 - 1) * S] = xv;
+  for (int j = ny1 - 1; j >= 1; --j) {
+    xv = (col[(size_t)(j - 1) * S] - A3(ayp, 3, j) * xv) * dv[(size_t)(j - 1) * S];
+    col[(size_t)(j - 1) * S] = xv;
+  }
+}
+
+// DCT-III along x (cosftx iopt=+1) for two modes of one row j, in place
+__global__ void __launch_bounds__(256) k_pois_bwd(DCoef c, XTab x, double *__restrict__ phi) {
+  extern __shared__ double2 xsm[];
+  const int n = x.n, ny = c.ny, nz1 = c.nz1, nz2 = c.nz2, xr = c.xround;
+  const int j = blockIdx.y + 1;
+  const int k0 = blockIdx.x * 2;
+  const size_t PV = (size_t)ny * nz1;
+  for (int e = threadIdx.x; e < 2 * n; e += 256) {
+    const int l = e / n, kk = e % n;
+    const int k = k0 + l;
+    double2 val = make_double2(0.0, 0.0);
+    if (k <= nz2) {
+      const double *q = phi + (size_t)(kk + 1) * PV + (size_t)(j - 1) * nz1 + 2 * k;
+      const double2 Y = make_double2(rnd(q[0], xr), rnd(q[1], xr));
+      double2 Ym = make_double2(0.0, 0.0);
+      if (kk > 0) {
+        const double *qm = phi + (size_t)(n - kk + 1) * PV + (size_t)(j - 1) * nz1 + 2 * k;
+        Ym = make_double2(rnd(qm[0], xr), rnd(qm[1], xr));
+      }
+      const double2 d = make_double2(Y.x + Ym.y, Y.y - Ym.x);  // Y - i Ym
+      val = cmul(cconj(__ldg(x.tw2 + kk)), d);
+    }
+    xsm[l * n + kk] = val;
+  }
+  __syncthreads();
+  block_fft<1, 2>(xsm, n, x.tw);
+  for (int e = threadIdx.x; e < 2 * n; e += 256) {
+    const int l = e / n, tt = e % n;
+    const int k = k0 + l;
+    if (k > nz2) continue;
+    const double2 V = xsm[l * n + ((tt & 1) ? n - 1 - (tt >> 1) : (tt >> 1))];
+    double *o = phi + (size_t)(tt + 1) * PV + (size_t)(j - 1) * nz1 + 2 * k;
+    o[0] = rnd(0.5 * V.x, xr);
+    o[1] = rnd(0.5 * V.y, xr);
+  }
+}
+
+// projection, pois.f90:144-162; one thread per (i >= 2, j, kr)
+__global__ void __launch_bounds__(128) k_project(DCoef c, const DState *st, const double *__restrict__ phi,
+                                                 double *u, double *v, double *w, double *p) {
+  const int kr = blockIdx.x * blockDim.x + threadIdx.x;
+  if (kr >= c.nz1) return;
+  const int j = blockIdx.y + 1, i = blockIdx.z + 2;
+  const int nx = c.nx, ny = c.ny, nz1 = c.nz1;
+  const size_t PU = (size_t)(ny + 1) * nz1, PV = (size_t)ny * nz1;
+  const int k = kr >> 1, odd = kr & 1, pof = odd ? -1 : 1;
+  const double kz = c.kaz[k];
+  const double *f = phi + (size_t)(i - 1) * PV + kr;  // phi(j, i) at f[(j-1)*nz1]
+  if (j >= 2) {
+    const double fm = f[(size_t)(j - 2) * nz1];
+    double *pq = p + (size_t)(i - 1) * PV + (size_t)(j - 1) * nz1 + kr;
+    *pq = st->varstep * fm + *pq;
+    const double q = f[(size_t)(j - 2) * nz1 + pof];
+    const double kf = odd ? kz * q : -kz * q;
+    double *wq = w + (size_t)(i - 1) * PU + (size_t)(j - 1) * nz1 + kr;
+    *wq = *wq - kf;
+  }
+  if (j >= 2 && j <= ny - 1) {
+    double *vq = v + (size_t)(i - 1) * PV + (size_t)(j - 1) * nz1 + kr;
+    *vq = *vq - c.idyy[j - 1] * (f[(size_t)(j - 1) * nz1] - f[(size_t)(j - 2) * nz1]);
+  }
+  if (j <= ny - 1 && i <= nx - 1) {
+    double *uq = u + (size_t)(i - 1) * PU + (size_t)j * nz1 + kr;
+    *uq = *uq - c.S[OTBL_S_IDXX] * (f[PV + (size_t)(j - 1) * nz1] - f[(size_t)(j - 1) * nz1]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// standalone pieces of the path
+// ---------------------------------------------------------------------------
+// planes [nx][np] <-> pencils [np][nx] (change.f90 chp2x / chx2p), rounded
+__global__ void k_transpose(const double *__restrict__ in, double *__restrict__ out, int rows, int cols, int xr) {
+  __shared__ double tile[32][33];
+  const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += 8) {
+    const int row = by + r, col = bx + threadIdx.x;
+    if (row < rows && col < cols) tile[r][threadIdx.x] = in[(size_t)row * cols + col];
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += 8) {
+    const int orow = bx + r, ocol = by + threadIdx.x;
+    if (orow < cols && ocol < rows) out[(size_t)orow * rows + ocol] = rnd(tile[threadIdx.x][r], xr);
+  }
+}
+
+__global__ void __launch_bounds__(128) k_fourxz(DCoef c, ZTab z, double *fou, double *phys, int iopt,
+                                                int nlines) {
+  extern __shared__ double2 sm[];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int l = blockIdx.x * 4 + wid;
+  if (l >= nlines) return;
+  const int M = z.M;
+  double2 *A = sm + (size_t)wid * M;
+  double *ph = phys + (size_t)l * (z.nz + 2);
+  double *fo = fou + (size_t)l * c.nz1;
+  if (iopt < 0) {
+    for (int t = lane; t < M; t += 32) A[t] = make_double2(ph[2 * t], ph[2 * t + 1]);
+    __syncwarp();
+    line_r2c(z, A, fo, lane);
+  } else {
+    line_c2r(z, fo, A, lane);
+    for (int t = lane; t < M; t += 32) {
+      ph[2 * t] = A[t].x;
+      ph[2 * t + 1] = A[t].y;
+    }
+    for (int t = lane; t < 2; t += 32) ph[z.nz + t] = 0.0;
+  }
+}
+
+// cosftx on pencils c(nx, nlines), elements 2..nx; two real lines per CTA
+__global__ void __launch_bounds__(256) k_cosftx(XTab x, double *cp, int nx, int nlines, int iopt) {
+  extern __shared__ double2 xsm[];
+  const int n = x.n;
+  const int l0 = blockIdx.x * 2;
+  double *la = cp + (size_t)l0 * nx + 1;
+  double *lb = (l0 + 1 < nlines) ? cp + (size_t)(l0 + 1) * nx + 1 : nullptr;
+  if (iopt < 0) {
+    for (int tt = threadIdx.x; tt < n; tt += 256) {
+      const int dst = (tt & 1) ? n - 1 - (tt >> 1) : (tt >> 1);
+      xsm[dst] = make_double2(la[tt], lb ? lb[tt] : 0.0);
+    }
+    __syncthreads();
+    block_fft<-1, 1>(xsm, n, x.tw);
+    const double dnf = 1.0 / (double)n;
+    for (int kk = threadIdx.x; kk < n; kk += 256) {
+      const double2 V = xsm[kk], Vm = xsm[kk == 0 ? 0 : n - kk];
+      const double2 wq = __ldg(x.tw2 + kk);
+      const double2 y = cadd(cmul(wq, V), cmul(cconj(wq), Vm));
+      la[kk] = dnf * y.x;
+      if (lb) lb[kk] = dnf * y.y;
+    }
+  } else {
+    for (int kk = threadIdx.x; kk < n; kk += 256) {
+      const double2 Y = make_double2(la[kk], lb ? lb[kk] : 0.0);
+      const double2 Ym = kk > 0 ? make_double2(la[n - kk], lb ? lb[n - kk] : 0.0) : make_double2(0.0, 0.0);
+      const double2 d = make_double2(Y.x + Ym.y, Y.y - Ym.x);
+      xsm[kk] = cmul(cconj(__ldg(x.tw2 + kk)), d);
+    }
+    __syncthreads();
+    block_fft<1, 1>(xsm, n, x.tw);
+    for (int tt = threadIdx.x; tt < n; tt += 256) {
+      const double2 V = xsm[(tt & 1) ? n - 1 - (tt >> 1) : (tt >> 1)];
+      la[tt] = 0.5 * V.x;
+      if (lb) lb[tt] = 0.5 * V.y;
+    }
+  }
+}
+
+__global__ void k_twiddles(double2 *tw, int n, double2 *tw2, int n2, int mode2) {
+  // tw[t] = exp(-2 pi i t/n); tw2[t] = exp(-2 pi i t/n2) (mode2 = 0) or
+  // exp(-i pi t/(2 n2)) (mode2 = 1), t < count
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) {
+    double s, co;
+    sincospi(-2.0 * (double)t / (double)n, &s, &co);
+    tw[t] = make_double2(co, s);
+  }
+  if (tw2 && t < n2) {
+    double s, co;
+    if (mode2 == 0)
+      sincospi(-2.0 * (double)t / (double)(2 * n2), &s, &co);
+    else
+      sincospi(-(double)t / (2.0 * (double)n2), &s, &co);
+    tw2[t] = make_double2(co, s);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// launch wrappers
+// ---------------------------------------------------------------------------
+static inline ZTab ztab(otbl_ctx *c) {
+  ZTab z;
+  z.tw = reinterpret_cast<const double2 *>(c->w.twz);
+  z.tw2 = reinterpret_cast<const double2 *>(c->w.twz2);
+  z.M = c->cfg.nz / 2;
+  z.nz = c->cfg.nz;
+  z.nz2 = c->dc.nz2;
+  return z;
+}
+static inline XTab xtab(otbl_ctx *c) {
+  XTab x;
+  x.tw = reinterpret_cast<const double2 *>(c->w.twx);
+  x.tw2 = reinterpret_cast<const double2 *>(c->w.twx2);
+  x.n = c->cfg.nx - 1;
+  return x;
+}
+
+cudaError_t launch_twiddles(otbl_ctx *c) {
+  const int M = c->cfg.nz / 2, n = c->cfg.nx - 1;
+  k_twiddles<<<(M + 255) / 256, 256, 0, c->stream>>>(reinterpret_cast<double2 *>(c->w.twz), M,
+                                                     reinterpret_cast<double2 *>(c->w.twz2), M, 0);
+  k_twiddles<<<(n + 255) / 256, 256, 0, c->stream>>>(reinterpret_cast<double2 *>(c->w.twx), n,
+                                                     reinterpret_cast<double2 *>(c->w.twx2), n, 1);
+  c->launches += 2;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_interpx(otbl_ctx *c) {
+  const int nz1 = c->dc.nz1, ny = c->cfg.ny;
+  const int npu = nz1 * (ny + 1), npv = nz1 * ny;
+  k_interpx<<<(npu + 127) / 128, 128, 0, c->stream>>>(c->dc, c->f[OTBL_F_U], c->w.ux, 0, npu);
+  k_interpx<<<(npv + 127) / 128, 128, 0, c->stream>>>(c->dc, c->f[OTBL_F_V], c->w.vx, 1, npv);
+  k_interpx<<<(npu + 127) / 128, 128, 0, c->stream>>>(c->dc, c->f[OTBL_F_W], c->w.wx, 1, npu);
+  c->launches += 3;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_interpy(otbl_ctx *c) {
+  const int nz1 = c->dc.nz1;
+  dim3 g((nz1 + 127) / 128, c->cfg.nx);
+  k_interpy<<<g, 128, 0, c->stream>>>(c->dc, c->f[OTBL_F_U], c->w.uy, 0);
+  k_interpy<<<g, 128, 0, c->stream>>>(c->dc, c->f[OTBL_F_W], c->w.wy, 0);
+  k_interpy<<<g, 128, 0, c->stream>>>(c->dc, c->f[OTBL_F_V], c->w.vy, 1);
+  c->launches += 3;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reset_max(otbl_ctx *c) {
+  k_reset_max<<<(c->cfg.ny + 1 + 255) / 256, 256, 0, c->stream>>>(c->st, c->w.vm_bits, c->cfg.ny);
+  c->launches += 1;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_products(otbl_ctx *c, int setstep) {
+  ProdArgs a;
+  a.u = c->f[OTBL_F_U];
+  a.v = c->f[OTBL_F_V];
+  a.w = c->f[OTBL_F_W];
+  a.ux = c->w.ux;
+  a.vx = c->w.vx;
+  a.wx = c->w.wx;
+  a.uy = c->w.uy;
+  a.wy = c->w.wy;
+  a.vy = c->w.vy;
+  a.uu = c->w.uu;
+  a.uw = c->w.uw;
+  a.uv = c->w.uv;
+  a.vw = c->w.vw;
+  a.vv = c->w.vv;
+  a.ww = c->w.ww;
+  a.vm_bits = c->w.vm_bits;
+  a.st = c->st;
+  a.setstep = setstep;
+  const int M = c->cfg.nz / 2;
+  const size_t smem = (size_t)4 * 3 * M * sizeof(double2);
+  cudaFuncSetAttribute(k_products, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  dim3 g((c->cfg.ny + 1 + 3) / 4, c->cfg.nx);
+  k_products<<<g, 128, smem, c->stream>>>(c->dc, ztab(c), a);
+  c->launches += 1;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_difvisx(otbl_ctx *c) {
+  const int nz1 = c->dc.nz1, ny = c->cfg.ny;
+  const int npu = nz1 * (ny + 1), npv = nz1 * ny;
+  k_difvisx<<<(npu + 127) / 128, 128, 0, c->stream>>>(c->dc, c->w.uu, c->f[OTBL_F_U], c->w.cu, c->w.s1, 0, npu);
+  k_difvisx<<<(npv + 127) / 128, 128, 0, c->stream>>>(c->dc, c->w.uv, c->f[OTBL_F_V], c->w.cv, c->w.s2, 1, npv);
+  k_difvisx<<<(npu + 127) / 128, 128, 0, c->stream>>>(c->dc, c->w.uw, c->f[OTBL_F_W], c->w.cw, c->w.s3, 1, npu);
+  c->launches += 3;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_dt(otbl_ctx *c, int m, int setstep) {
+  k_dt<<<1, 32, 0, c->stream>>>(c->dc, c->st, c->w.vm_bits, c->w.fac_u, c->w.fac_v, m, setstep, c->cfg.dt_mode,
+                                c->cfg.dt_fixed);
+  c->launches += 1;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_genflu(otbl_ctx *c) {
+  GenArgs a;
+  a.u = c->f[OTBL_F_U];
+  a.v = c->f[OTBL_F_V];
+  a.w = c->f[OTBL_F_W];
+  a.rhsupa = c->f[OTBL_F_RHSUPA];
+  a.rhsvpa = c->f[OTBL_F_RHSVPA];
+  a.rhswpa = c->f[OTBL_F_RHSWPA];
+  a.u0 = c->u0;
+  a.v0 = c->v0;
+  a.um = c->um;
+  a.wk = c->w.gf;
+  a.st = c->st;
+  const int ny = c->cfg.ny;
+  const size_t smem = sizeof(double) * (4 * (size_t)(ny + 1)) + sizeof(int) * 2 * (ny + 1);
+  cudaFuncSetAttribute(k_genflu, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_genflu<<<1, 512, smem, c->stream>>>(c->dc, a);
+  c->launches += 1;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_final(otbl_ctx *c) {
+  FinalArgs a;
+  a.u = c->f[OTBL_F_U];
+  a.v = c->f[OTBL_F_V];
+  a.w = c->f[OTBL_F_W];
+  a.p = c->f[OTBL_F_P];
+  a.rhsupa = c->f[OTBL_F_RHSUPA];
+  a.rhsvpa = c->f[OTBL_F_RHSVPA];
+  a.rhswpa = c->f[OTBL_F_RHSWPA];
+  a.cu = c->w.cu;
+  a.cv = c->w.cv;
+  a.cw = c->w.cw;
+  a.uv = c->w.uv;
+  a.uw = c->w.uw;
+  a.vw = c->w.vw;
+  a.vv = c->w.vv;
+  a.ww = c->w.ww;
+  a.s1 = c->w.s1;
+  a.s2 = c->w.s2;
+  a.s3 = c->w.s3;
+  a.fac_u = c->w.fac_u;
+  a.fac_v = c->w.fac_v;
+  a.st = c->st;
+  dim3 g((c->dc.nz1 + 127) / 128, c->cfg.nx - 1);
+  k_final<<<g, 128, 0, c->stream>>>(c->dc, a);
+  c->launches += 1;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_outflow(otbl_ctx *c) {
+  k_outflow<<<1, 256, 0, c->stream>>>(c->dc, c->f[OTBL_F_U], c->f[OTBL_F_V], c->f[OTBL_F_RHSUPA]);
+  c->launches += 1;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pois(otbl_ctx *c, int m) {
+  (void)m;  // varstep for substep m was set by k_dt
+  const int nz2 = c->dc.nz2, ny = c->cfg.ny, nx = c->cfg.nx, nz1 = c->dc.nz1;
+  const int n = nx - 1;
+  const size_t smem = (size_t)2 * n * sizeof(double2);
+  cudaFuncSetAttribute(k_pois_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaFuncSetAttribute(k_pois_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  double *phi = c->w.ux, *dinv = c->w.s1;
+  dim3 gx((nz2 + 1 + 1) / 2, ny - 1);
+  k_pois_fwd<<<gx, 256, smem, c->stream>>>(c->dc, xtab(c), c->f[OTBL_F_U], c->f[OTBL_F_V], c->f[OTBL_F_W], phi);
+  dim3 gs((nz1 + 127) / 128, nx - 1);
+  k_pois_solve<<<gs, 128, 0, c->stream>>>(c->dc, phi, dinv);
+  k_pois_bwd<<<gx, 256, smem, c->stream>>>(c->dc, xtab(c), phi);
+  dim3 gp((nz1 + 127) / 128, ny, nx - 1);
+  k_project<<<gp, 128, 0, c->stream>>>(c->dc, c->st, phi, c->f[OTBL_F_U], c->f[OTBL_F_V], c->f[OTBL_F_W],
+                                       c->f[OTBL_F_P]);
+  c->launches += 4;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_boun_all(otbl_ctx *c) {
+  dim3 g((c->dc.nz1 + 127) / 128, c->cfg.nx);
+  k_boun<<<g, 128, 0, c->stream>>>(c->dc, c->f[OTBL_F_U], c->f[OTBL_F_V], c->f[OTBL_F_W]);
+  c->launches += 1;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tiempo(otbl_ctx *c) {
+  k_tiempo<<<1, 32, 0, c->stream>>>(c->st);
+  c->launches += 1;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_chp2x(otbl_ctx *c, const double *in, double *out, int jee, int to_pen) {
+  const int np = c->dc.nz1 * jee, nx = c->cfg.nx;
+  const int rows = to_pen ? nx : np, cols = to_pen ? np : nx;
+  dim3 g((cols + 31) / 32, (rows + 31) / 32), b(32, 8);
+  k_transpose<<<g, b, 0, c->stream>>>(in, out, rows, cols, c->dc.xround);
+  c->launches += 1;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fourxz(otbl_ctx *c, double *fou, double *phys, int iopt, int nlines) {
+  const int M = c->cfg.nz / 2;
+  const size_t smem = (size_t)4 * M * sizeof(double2);
+  k_fourxz<<<(nlines + 3) / 4, 128, smem, c->stream>>>(c->dc, ztab(c), fou, phys, iopt, nlines);
+  c->launches += 1;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cosftx(otbl_ctx *c, double *cp, int nlines, int iopt) {
+  const int n = c->cfg.nx - 1;
+  const size_t smem = (size_t)n * sizeof(double2);
+  k_cosftx<<<(nlines + 1) / 2, 256, smem, c->stream>>>(xtab(c), cp, c->cfg.nx, nlines, iopt);
+  c->launches += 1;
+  return cudaGetLastError();
+}
+
+}  // namespace otbl

@@ -1,0 +1,389 @@
+// C ABI of the B200 substep (include/otbl.h): context lifetime, state
+// transfer and the stream-ordered orchestration of the kernels in
+// kernels.cu, following the call order of bl_1.F90:94-125.
+#include <cstdio>
+#include <cstring>
+
+#include "otbl_internal.cuh"
+
+using namespace otbl;
+
+namespace {
+
+bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+bool factors_235(int n) {
+  if (n <= 0) return false;
+  for (int p : {2, 3, 5})
+    while (n % p == 0) n /= p;
+  return n == 1;
+}
+
+int fail(otbl_ctx *c, int code, const char *msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+template <typename T>
+int dalloc(otbl_ctx *c, T **p, size_t count) {
+  void *q = nullptr;
+  const size_t bytes = count * sizeof(T);
+  if (cudaMalloc(&q, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    c->err = "cudaMalloc failed (" + std::to_string(bytes) + " bytes)";
+    return OTBL_ERR_OOM;
+  }
+  cudaMemset(q, 0, bytes);
+  c->allocs.push_back(q);
+  c->bytes += bytes;
+  *p = static_cast<T *>(q);
+  return OTBL_OK;
+}
+
+size_t field_len(const otbl_ctx *c, int id) {
+  const int ut = (id == OTBL_F_U || id == OTBL_F_W || id == OTBL_F_RHSUPA || id == OTBL_F_RHSWPA);
+  return otbl_field_len(c->cfg.nx, c->cfg.ny, c->cfg.nz, ut);
+}
+
+int check(otbl_ctx *c, cudaError_t e, const char *where) {
+  if (e != cudaSuccess) {
+    c->err = std::string(where) + ": " + cudaGetErrorString(e);
+    return OTBL_ERR_CUDA;
+  }
+  return OTBL_OK;
+}
+
+}  // namespace
+
+extern "C" int otbl_ctx_create(const otbl_config *cfg, const double *coef, int device, otbl_ctx **out) {
+  if (!cfg || !coef || !out) return OTBL_ERR_ARG;
+  *out = nullptr;
+  int st = otbl_config_check(cfg);
+  if (st != OTBL_OK) return st;
+  if (!is_pow2(cfg->nz / 2) || cfg->nz / 2 > 512 || cfg->nz / 2 < 8) return OTBL_ERR_CONFIG;
+  if (!factors_235(cfg->nx - 1) || cfg->nx - 1 > 4096) return OTBL_ERR_CONFIG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device || device < 0) {
+    cudaGetLastError();
+    return OTBL_ERR_NODEV;
+  }
+  otbl_ctx *c = new otbl_ctx();
+  c->cfg = *cfg;
+  c->device = device;
+  c->bytes = 0;
+  c->launches = 0;
+  c->stream = nullptr;
+  if (cudaSetDevice(device) != cudaSuccess) {
+    delete c;
+    return OTBL_ERR_NODEV;
+  }
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return OTBL_ERR_CUDA;
+  }
+  const int nx = cfg->nx, ny = cfg->ny, nz = cfg->nz;
+  const int nz1 = 2 * (nz / 3);
+  otbl_coef_offsets o;
+  otbl_coef_layout(nx, ny, nz, &o);
+  const size_t ncoef = o.off[OTBL_C_COUNT];
+  c->coef_host.assign(coef, coef + ncoef);
+#define TRY(x)                \
+  do {                        \
+    int s__ = (x);            \
+    if (s__ != OTBL_OK) {     \
+      *out = c;               \
+      return s__;             \
+    }                         \
+  } while (0)
+  TRY(dalloc(c, &c->coef_dev, ncoef));
+  if (cudaMemcpy(c->coef_dev, coef, ncoef * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
+    *out = c;
+    return fail(c, OTBL_ERR_CUDA, "coefficient upload failed");
+  }
+  DCoef &d = c->dc;
+  d.nx = nx;
+  d.ny = ny;
+  d.nz = nz;
+  d.nz1 = nz1;
+  d.nz2 = nz1 / 2 - 1;
+  d.xout = cfg->xout;
+  d.xround = cfg->xpose_round;
+  auto P = [&](int id) { return (const double *)(c->coef_dev + o.off[id]); };
+  d.S = P(OTBL_C_SCAL);
+  d.y = P(OTBL_C_Y);
+  d.dy = P(OTBL_C_DY);
+  d.idy = P(OTBL_C_IDY);
+  d.idyy = P(OTBL_C_IDYY);
+  d.dymin = P(OTBL_C_DYMIN);
+  d.kaz = P(OTBL_C_KAZ);
+  d.kaz2 = P(OTBL_C_KAZ2);
+  d.kvis = P(OTBL_C_KVIS);
+  d.kmod = P(OTBL_C_KMOD);
+  d.ayp = P(OTBL_C_AYP);
+  d.vmagic = P(OTBL_C_VMAGIC);
+  d.inxu = P(OTBL_C_INXU);
+  d.inxv = P(OTBL_C_INXV);
+  d.cofiux = P(OTBL_C_COFIUX);
+  d.cofivx = P(OTBL_C_COFIVX);
+  d.inbx = P(OTBL_C_INBX);
+  d.dcxu = P(OTBL_C_DCXU);
+  d.dcxv = P(OTBL_C_DCXV);
+  d.cofcxu = P(OTBL_C_COFCXU);
+  d.cofcxv = P(OTBL_C_COFCXV);
+  d.dcbx = P(OTBL_C_DCBX);
+  d.vixu = P(OTBL_C_VIXU);
+  d.vixv = P(OTBL_C_VIXV);
+  d.cofvxu = P(OTBL_C_COFVXU);
+  d.cofvxv = P(OTBL_C_COFVXV);
+  d.cofvbx = P(OTBL_C_COFVBX);
+  d.inyu = P(OTBL_C_INYU);
+  d.inyv = P(OTBL_C_INYV);
+  d.cofiuy = P(OTBL_C_COFIUY);
+  d.cofivy = P(OTBL_C_COFIVY);
+  d.inby = P(OTBL_C_INBY);
+  d.dcyu = P(OTBL_C_DCYU);
+  d.dcyv = P(OTBL_C_DCYV);
+  d.cofcyu = P(OTBL_C_COFCYU);
+  d.cofcyv = P(OTBL_C_COFCYV);
+  d.dcby = P(OTBL_C_DCBY);
+  d.viyu = P(OTBL_C_VIYU);
+  d.viyv = P(OTBL_C_VIYV);
+  d.vyui = P(OTBL_C_VYUI);
+  d.vyvi = P(OTBL_C_VYVI);
+  d.cofvyu = P(OTBL_C_COFVYU);
+  d.cofvyv = P(OTBL_C_COFVYV);
+  d.cofvby = P(OTBL_C_COFVBY);
+  d.ccon = P(OTBL_C_CCON);
+
+  const size_t lu = otbl_field_len(nx, ny, nz, 1);
+  for (int id = 0; id < OTBL_F_COUNT; ++id) TRY(dalloc(c, &c->f[id], field_len(c, id)));
+  TRY(dalloc(c, &c->u0, (size_t)ny + 1));
+  TRY(dalloc(c, &c->v0, (size_t)ny + 1));
+  TRY(dalloc(c, &c->um, (size_t)ny + 1));
+  TRY(dalloc(c, &c->st, 1));
+  Work &w = c->w;
+  double **big[] = {&w.ux, &w.vx, &w.wx, &w.uy, &w.wy, &w.vy, &w.uu, &w.uw, &w.uv,
+                    &w.vw, &w.vv, &w.ww, &w.cu, &w.cv, &w.cw, &w.s1, &w.s2, &w.s3};
+  for (double **b : big) TRY(dalloc(c, b, lu));
+  const int M = nz / 2, n = nx - 1;
+  TRY(dalloc(c, &w.twz, 2 * (size_t)M));
+  TRY(dalloc(c, &w.twz2, 2 * (size_t)M));
+  TRY(dalloc(c, &w.twx, 2 * (size_t)n));
+  TRY(dalloc(c, &w.twx2, 2 * (size_t)n));
+  TRY(dalloc(c, &w.vm_bits, (size_t)ny + 1));
+  TRY(dalloc(c, &w.fac_u, 3 * (size_t)(ny + 4)));
+  TRY(dalloc(c, &w.fac_v, 3 * (size_t)(ny + 4)));
+  TRY(dalloc(c, &w.gf, (size_t)nz1 * (ny + 2)));
+#undef TRY
+  if (check(c, launch_twiddles(c), "twiddles") != OTBL_OK || check(c, cudaStreamSynchronize(c->stream), "init")) {
+    *out = c;
+    return OTBL_ERR_CUDA;
+  }
+  *out = c;
+  return OTBL_OK;
+}
+
+extern "C" void otbl_ctx_destroy(otbl_ctx *c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (void *p : c->allocs) cudaFree(p);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+extern "C" const char *otbl_last_error(const otbl_ctx *c) { return c ? c->err.c_str() : "null context"; }
+
+extern "C" size_t otbl_device_bytes(const otbl_ctx *c) { return c ? c->bytes : 0; }
+
+extern "C" long long otbl_launch_count(const otbl_ctx *c) { return c ? c->launches : 0; }
+
+extern "C" int otbl_set_field(otbl_ctx *c, int id, const double *host) {
+  if (!c || !host || id < 0 || id >= OTBL_F_COUNT) return OTBL_ERR_ARG;
+  cudaSetDevice(c->device);
+  OTBL_CUDA_TRY(c, cudaMemcpyAsync(c->f[id], host, field_len(c, id) * sizeof(double), cudaMemcpyHostToDevice,
+                                   c->stream));
+  OTBL_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  return OTBL_OK;
+}
+
+extern "C" int otbl_get_field(otbl_ctx *c, int id, double *host) {
+  if (!c || !host || id < 0 || id >= OTBL_F_COUNT) return OTBL_ERR_ARG;
+  cudaSetDevice(c->device);
+  OTBL_CUDA_TRY(c, cudaMemcpyAsync(host, c->f[id], field_len(c, id) * sizeof(double), cudaMemcpyDeviceToHost,
+                                   c->stream));
+  OTBL_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  return OTBL_OK;
+}
+
+extern "C" int otbl_field_device_ptr(otbl_ctx *c, int id, double **dptr) {
+  if (!c || !dptr || id < 0 || id >= OTBL_F_COUNT) return OTBL_ERR_ARG;
+  *dptr = c->f[id];
+  return OTBL_OK;
+}
+
+extern "C" int otbl_set_inflow(otbl_ctx *c, const double *u0, const double *v0, const double *um,
+                               const otbl_inflow *s) {
+  if (!c || !u0 || !v0 || !um || !s) return OTBL_ERR_ARG;
+  cudaSetDevice(c->device);
+  const int ny = c->cfg.ny;
+  DState h;
+  OTBL_CUDA_TRY(c, cudaMemcpyAsync(&h, c->st, sizeof(DState), cudaMemcpyDeviceToHost, c->stream));
+  OTBL_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  h.tiempo = s->tiempo;
+  h.timeinit = s->timeinit;
+  h.dt = s->dt;
+  h.utauout = s->utauout;
+  h.rthout = s->rthout;
+  h.dout = s->dout;
+  h.gamma1 = s->gamma1;
+  h.gamma2 = s->gamma2;
+  h.timec = s->timec;
+  h.err = 0;
+  OTBL_CUDA_TRY(c, cudaMemcpyAsync(c->st, &h, sizeof(DState), cudaMemcpyHostToDevice, c->stream));
+  OTBL_CUDA_TRY(c, cudaMemcpyAsync(c->u0, u0, sizeof(double) * (ny + 1), cudaMemcpyHostToDevice, c->stream));
+  OTBL_CUDA_TRY(c, cudaMemcpyAsync(c->v0, v0, sizeof(double) * ny, cudaMemcpyHostToDevice, c->stream));
+  OTBL_CUDA_TRY(c, cudaMemcpyAsync(c->um, um, sizeof(double) * (ny + 1), cudaMemcpyHostToDevice, c->stream));
+  OTBL_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  return OTBL_OK;
+}
+
+extern "C" int otbl_get_inflow(otbl_ctx *c, double *um, otbl_inflow *s) {
+  if (!c) return OTBL_ERR_ARG;
+  cudaSetDevice(c->device);
+  DState h;
+  OTBL_CUDA_TRY(c, cudaMemcpyAsync(&h, c->st, sizeof(DState), cudaMemcpyDeviceToHost, c->stream));
+  if (um)
+    OTBL_CUDA_TRY(c, cudaMemcpyAsync(um, c->um, sizeof(double) * (c->cfg.ny + 1), cudaMemcpyDeviceToHost,
+                                     c->stream));
+  OTBL_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  if (s) {
+    s->tiempo = h.tiempo;
+    s->timeinit = h.timeinit;
+    s->dt = h.dt;
+    s->utauout = h.utauout;
+    s->rthout = h.rthout;
+    s->dout = h.dout;
+    s->gamma1 = h.gamma1;
+    s->gamma2 = h.gamma2;
+    s->timec = h.timec;
+    s->umax = h.umax;
+    s->wmax = h.wmax;
+    s->vmax = h.vmax;
+  }
+  if (h.err) {
+    c->err = "non-finite value in the CFL reduction";
+    return h.err;
+  }
+  return OTBL_OK;
+}
+
+#define LAUNCH(c, x)                                       \
+  do {                                                     \
+    int s__ = check((c), (x), #x);                         \
+    if (s__ != OTBL_OK) return s__;                        \
+  } while (0)
+
+extern "C" int otbl_rhsp(otbl_ctx *c, int m, int setstep) {
+  if (!c || m < 1 || m > 3) return OTBL_ERR_ARG;
+  cudaSetDevice(c->device);
+  if (setstep) LAUNCH(c, launch_reset_max(c));
+  LAUNCH(c, launch_interpx(c));
+  LAUNCH(c, launch_interpy(c));
+  LAUNCH(c, launch_products(c, setstep));
+  LAUNCH(c, launch_difvisx(c));
+  LAUNCH(c, launch_dt(c, m, setstep));
+  LAUNCH(c, launch_genflu(c));
+  LAUNCH(c, launch_final(c));
+  return OTBL_OK;
+}
+
+extern "C" int otbl_outflow_correction(otbl_ctx *c) {
+  if (!c) return OTBL_ERR_ARG;
+  cudaSetDevice(c->device);
+  LAUNCH(c, launch_outflow(c));
+  return OTBL_OK;
+}
+
+extern "C" int otbl_pois(otbl_ctx *c, int m) {
+  if (!c || m < 1 || m > 3) return OTBL_ERR_ARG;
+  cudaSetDevice(c->device);
+  LAUNCH(c, launch_pois(c, m));
+  return OTBL_OK;
+}
+
+extern "C" int otbl_substep(otbl_ctx *c, int m, int setstep) {
+  int s = otbl_rhsp(c, m, setstep);
+  if (s != OTBL_OK) return s;
+  s = otbl_outflow_correction(c);
+  if (s != OTBL_OK) return s;
+  return otbl_pois(c, m);
+}
+
+extern "C" int otbl_advance(otbl_ctx *c, int nsteps) {
+  if (!c || nsteps < 0) return OTBL_ERR_ARG;
+  for (int s = 0; s < nsteps; ++s) {
+    for (int m = 1; m <= 3; ++m) {
+      const int r = otbl_substep(c, m, m == 1);
+      if (r != OTBL_OK) return r;
+    }
+    LAUNCH(c, launch_tiempo(c));
+  }
+  return OTBL_OK;
+}
+
+extern "C" int otbl_sync(otbl_ctx *c) {
+  if (!c) return OTBL_ERR_ARG;
+  cudaSetDevice(c->device);
+  OTBL_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  int err = 0;
+  OTBL_CUDA_TRY(c, cudaMemcpy(&err, &c->st->err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err) {
+    c->err = "non-finite value in the CFL reduction";
+    return err;
+  }
+  return OTBL_OK;
+}
+
+extern "C" int otbl_chp2x(otbl_ctx *c, const double *plan, double *pen, int jee) {
+  if (!c || !plan || !pen || (jee != c->cfg.ny && jee != c->cfg.ny + 1)) return OTBL_ERR_ARG;
+  cudaSetDevice(c->device);
+  LAUNCH(c, launch_chp2x(c, plan, pen, jee, 1));
+  return OTBL_OK;
+}
+
+extern "C" int otbl_chx2p(otbl_ctx *c, const double *pen, double *plan, int jee) {
+  if (!c || !plan || !pen || (jee != c->cfg.ny && jee != c->cfg.ny + 1)) return OTBL_ERR_ARG;
+  cudaSetDevice(c->device);
+  LAUNCH(c, launch_chp2x(c, pen, plan, jee, 0));
+  return OTBL_OK;
+}
+
+extern "C" int otbl_fourxz(otbl_ctx *c, double *fou, double *phys, int iopt, int nlines) {
+  if (!c || !fou || !phys || nlines < 0) return OTBL_ERR_ARG;
+  if (nlines == 0) return OTBL_OK;
+  cudaSetDevice(c->device);
+  LAUNCH(c, launch_fourxz(c, fou, phys, iopt, nlines));
+  return OTBL_OK;
+}
+
+extern "C" int otbl_cosftx(otbl_ctx *c, double *cp, int nlines, int iopt) {
+  if (!c || !cp || nlines < 0) return OTBL_ERR_ARG;
+  if (nlines == 0) return OTBL_OK;
+  cudaSetDevice(c->device);
+  LAUNCH(c, launch_cosftx(c, cp, nlines, iopt));
+  return OTBL_OK;
+}
+
+extern "C" int otbl_boun(otbl_ctx *c) {
+  if (!c) return OTBL_ERR_ARG;
+  cudaSetDevice(c->device);
+  LAUNCH(c, launch_boun_all(c));
+  return OTBL_OK;
+}
+
+extern "C" int otbl_genflu(otbl_ctx *c) {
+  if (!c) return OTBL_ERR_ARG;
+  cudaSetDevice(c->device);
+  LAUNCH(c, launch_genflu(c));
+  return OTBL_OK;
+}

@@ -1,0 +1,106 @@
+// Internal declarations of the B200 substep: device view of the coefficient
+// buffer, device scalar state, the context, and launch helpers.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/otbl.h"
+#include "../../include/otbl_layout.h"
+
+namespace otbl {
+
+// Device view of the packed coefficient buffer (include/otbl_layout.h).
+// Passed by value to kernels; every pointer is into one device allocation.
+struct DCoef {
+  int nx, ny, nz, nz1, nz2, xout;
+  int xround;  // OTBL_XPOSE_FP32: round x-line inputs/outputs to REAL4
+  const double *S;
+  const double *y, *dy, *idy, *idyy, *dymin, *kaz, *kaz2, *kvis, *kmod, *ayp, *vmagic;
+  const double *inxu, *inxv, *cofiux, *cofivx, *inbx;
+  const double *dcxu, *dcxv, *cofcxu, *cofcxv, *dcbx;
+  const double *vixu, *vixv, *cofvxu, *cofvxv, *cofvbx;
+  const double *inyu, *inyv, *cofiuy, *cofivy, *inby;
+  const double *dcyu, *dcyv, *cofcyu, *cofcyv, *dcby;
+  const double *viyu, *viyv, *vyui, *vyvi, *cofvyu, *cofvyv, *cofvby, *ccon;
+};
+
+// Scalars that live on the device so that no host synchronisation is needed
+// inside a step (dt is produced by a reduction on the device).
+struct DState {
+  double dt, tiempo, timeinit, timec;
+  double utauout, rthout, dout, gamma1, gamma2;
+  double var1, var2, var3, var4, rkk, varstep;  // RK3 factors of the substep
+  double umax, wmax, vmax;
+  unsigned long long umax_bits, wmax_bits;      // atomicMax targets (>= 0)
+  int err;        // OTBL_ERR_NAN when the dt reduction saw a non-finite value
+  int dt_frozen;  // fixed-dt mode: dt taken
+  int pad[2];
+};
+
+// Device work buffers. Field-sized arrays use the plane layout.
+struct Work {
+  double *ux, *vx, *wx;        // interpxx outputs (u-type, v-type, u-type)
+  double *uy, *wy, *vy;        // interpyy outputs (ny rows each)
+  double *uu, *uw, *uv, *vw, *vv, *ww;  // products (uu, uw u-type; others ny rows)
+  double *cu, *cv, *cw;        // difvisxx outputs
+  double *s1, *s2, *s3;        // line-solve scratch (u-type size)
+  double *twz, *twz2;          // z-FFT twiddles exp(-2 pi i t/M), exp(-2 pi i t/nz)
+  double *twx;                 // x-DCT twiddles for the length nx-1 FFT
+  double *twx2;                // exp(-i pi k/(2n)), k = 0..n-1
+  unsigned long long *vm_bits; // vm(j) maxima, j = 1..ny
+  double *fac_u, *fac_v;       // implzy LU factors for the current dt (3*(ny+1))
+  double *gf;                  // genflu scratch: kl/fsca/ntop + wk plane
+};
+
+}  // namespace otbl
+
+struct otbl_ctx {
+  otbl_config cfg;
+  int device;
+  cudaStream_t stream;
+  otbl::DCoef dc;
+  double *coef_dev;
+  std::vector<double> coef_host;
+  double *f[OTBL_F_COUNT];
+  double *u0, *v0, *um;
+  otbl::DState *st;
+  otbl::Work w;
+  std::vector<void *> allocs;
+  size_t bytes;
+  long long launches;
+  std::string err;
+};
+
+#define OTBL_CUDA_TRY(ctx, call)                                        \
+  do {                                                                  \
+    cudaError_t e__ = (call);                                           \
+    if (e__ != cudaSuccess) {                                           \
+      (ctx)->err = std::string(#call) + ": " + cudaGetErrorString(e__); \
+      return OTBL_ERR_CUDA;                                             \
+    }                                                                   \
+  } while (0)
+
+namespace otbl {
+// kernel launch wrappers (kernels.cu); each returns cudaGetLastError()
+cudaError_t launch_interpx(otbl_ctx *c);
+cudaError_t launch_interpy(otbl_ctx *c);
+cudaError_t launch_products(otbl_ctx *c, int setstep);
+cudaError_t launch_difvisx(otbl_ctx *c);
+cudaError_t launch_dt(otbl_ctx *c, int m, int setstep);
+cudaError_t launch_genflu(otbl_ctx *c);
+cudaError_t launch_final(otbl_ctx *c);
+cudaError_t launch_outflow(otbl_ctx *c);
+cudaError_t launch_pois(otbl_ctx *c, int m);
+cudaError_t launch_reset_max(otbl_ctx *c);
+cudaError_t launch_boun_all(otbl_ctx *c);
+cudaError_t launch_tiempo(otbl_ctx *c);
+cudaError_t launch_twiddles(otbl_ctx *c);
+// standalone pieces
+cudaError_t launch_chp2x(otbl_ctx *c, const double *plan, double *pen, int jee, int to_pen);
+cudaError_t launch_fourxz(otbl_ctx *c, double *fou, double *phys, int iopt, int nlines);
+cudaError_t launch_cosftx(otbl_ctx *c, double *cpen, int nlines, int iopt);
+}  // namespace otbl

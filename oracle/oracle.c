@@ -576,9 +576,11 @@ void orc_genflu(orc_box *b) {
     vj[1] = 0.0;
   }
   double *wk = (double *)calloc((size_t)nz1 * (ny + 2), sizeof(double));
-  profile(b, PL(b, u, ny + 1, 1, 1), wk, ntop[1], kl, fsca, ny + 1);
-  profile(b, PL(b, w, ny + 1, 1, 1), wk, ntop[1], kl, fsca, ny + 1);
-  profile(b, PL(b, v, ny, 1, 1), wk, ntop[2], kl + (ny + 1), fsca + (ny + 1), ny);
+  if (ntop[1] >= 4 && ntop[2] >= 4) { /* guard: degenerate rescaled grids */
+    profile(b, PL(b, u, ny + 1, 1, 1), wk, ntop[1], kl, fsca, ny + 1);
+    profile(b, PL(b, w, ny + 1, 1, 1), wk, ntop[1], kl, fsca, ny + 1);
+    profile(b, PL(b, v, ny, 1, 1), wk, ntop[2], kl + (ny + 1), fsca + (ny + 1), ny);
+  }
   free(wk);
   free(kl);
   free(fsca);

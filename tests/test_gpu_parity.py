@@ -1,0 +1,102 @@
+"""GPU parity: the CUDA substep (through the C ABI) against the CPU oracle on
+the same seeded inputs and coefficient bits.
+
+Tolerances (FP64 path, north-star gates): relative L2 of each field <= 1e-11
+after one substep; <= 1e-9 after several steps; max|div u| after the
+projection <= 1e-12 (absolute, in units of U_inf/delta0) in pure-FP64 mode.
+With REAL4-rounding transposes (xpose_round=1) the same rounding points are
+applied on both sides; agreement is limited by FP32 round-half flips, so the
+bound there is 1e-6.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from opentbl_b200 import Box, config, native
+from opentbl_b200.config import replace
+
+from helpers import divergence_np, oracle_box, rel_l2, setup
+
+pytestmark = pytest.mark.gpu
+
+STATE = ("u", "v", "w", "p", "rhsupa", "rhsvpa", "rhswpa")
+
+
+def _pair(cfg):
+    init, coef = setup(cfg)
+    return Box(cfg, init, coef), oracle_box(cfg, init, coef), init, coef
+
+
+def _compare(gpu, orc, names=STATE):
+    return {n: rel_l2(gpu.field(n), orc.field(n)) for n in names}
+
+
+@pytest.mark.parametrize("name", ["TINY", "SMALL"])
+def test_rhsp_outflow_pois_one_substep(name):
+    cfg = getattr(config, name)
+    g, o, init, coef = _pair(cfg)
+    g.rhsp(1, True)
+    o.rhsp(1, 1)
+    e = _compare(g, o)
+    assert max(e.values()) <= 1e-11, e
+    gi = g.inflow()[1]
+    oi = o.inflow()[1]
+    assert abs(gi["dt"] - oi["dt"]) <= 1e-14 * oi["dt"]
+    for k in ("utauout", "rthout", "gamma1", "gamma2", "dout"):
+        assert abs(gi[k] - oi[k]) <= 1e-12 * max(1.0, abs(oi[k])), (k, gi[k], oi[k])
+    g.outflow_correction()
+    o.outflow_correction()
+    e = _compare(g, o, ("u", "rhsupa"))
+    assert max(e.values()) <= 1e-11, e
+    g.pois(1)
+    o.pois(1)
+    e = _compare(g, o)
+    assert max(e.values()) <= 1e-11, e
+    d = divergence_np(cfg, coef, g.field("u"), g.field("v"), g.field("w"))
+    assert np.abs(d).max() <= 1e-12
+
+
+@pytest.mark.parametrize("name", ["TINY", "SMALL"])
+def test_three_steps(name):
+    cfg = getattr(config, name)
+    g, o, init, coef = _pair(cfg)
+    g.advance(3)
+    o.advance(3)
+    e = _compare(g, o)
+    assert max(e.values()) <= 1e-10, e
+    um_g, gi = g.inflow()
+    um_o, oi = o.inflow()
+    assert rel_l2(um_g, um_o) <= 1e-12
+    assert abs(gi["tiempo"] - oi["tiempo"]) <= 1e-13 * oi["tiempo"]
+
+
+def test_fp32_transposes_one_substep():
+    cfg = replace(config.TINY, xpose_round=1)
+    g, o, init, coef = _pair(cfg)
+    g.substep(1, True)
+    o.substep(1, 1)
+    e = _compare(g, o)
+    assert max(e.values()) <= 1e-6, e
+
+
+def test_fixed_dt_mode():
+    cfg = replace(config.TINY, dt_mode=1, dt_fixed=0.05)
+    g, o, init, coef = _pair(cfg)
+    g.advance(2)
+    o.advance(2)
+    assert abs(g.inflow()[1]["dt"] - 0.05) == 0.0
+    e = _compare(g, o)
+    assert max(e.values()) <= 1e-10, e
+
+
+def test_c1_one_step_and_divergence():
+    """257x97x128 (the reference's CPU-runnable box): one full RK3 step."""
+    cfg = config.C1
+    g, o, init, coef = _pair(cfg)
+    g.advance(1)
+    o.advance(1)
+    e = _compare(g, o)
+    assert max(e.values()) <= 1e-10, e
+    d = divergence_np(cfg, coef, g.field("u"), g.field("v"), g.field("w"))
+    assert np.abs(d).max() <= 1e-12
