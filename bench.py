@@ -1,0 +1,361 @@
+#!/usr/bin/env python
+"""Benchmark of the RK3 substep of OpenTBL's boundary-layer DNS on B200.
+
+Metric: Mpts*RK3-substeps/s = nx*ny*nz * substeps / seconds / 1e6, on the
+1025x193x512 FP64 box (synthetic seeded field, every array resident in HBM).
+One bench "step" is one full RK3 time step (3 substeps, bl_1.F90:94-125);
+`value` counts its 3 substeps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the CPU port of the reference's substep (oracle/,
+OpenMP on all host cores) on the same box, one substep per sample step.
+For N > 1 (torchrun), every rank advances its own independent box (replicas
+only: a box does not shard without the reference's global transposes); the
+time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from opentbl_b200 import config as cfgmod  # noqa: E402
+from opentbl_b200 import native, synth  # noqa: E402
+from opentbl_b200.box import Box  # noqa: E402
+
+WORKLOAD = "C2"
+METRIC = "Mpts·RK3-substeps/s"
+UNIT = "Mpts·substeps/s"
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def algorithmic_bytes(cfg) -> dict:
+    """Bytes each kernel class must move per substep (every input read once,
+    every output written once), and the survey's 55-pass substep figure."""
+    nx, ny, nz1 = cfg.nx, cfg.ny, cfg.nz1
+    U = nx * (ny + 1) * nz1 * 8.0        # one u-type field
+    V = nx * ny * nz1 * 8.0              # one v-type field
+    Vi = (nx - 2) * ny * nz1 * 8.0       # v-type rows on planes 2..nx-1
+    return {
+        "interpx": 2 * (2 * U + V),
+        "interpy": (2 * U + V) + 3 * V,
+        "products": (3 * U + 2 * V + 4 * Vi) + (2 * U + V + 3 * Vi),
+        "difvisx": 2 * (2 * U + V) + (2 * U + V),
+        "final": (3 * U + 2 * V) + 5 * V + (2 * U + V) + V + (2 * U + V) + (2 * U + V) + (2 * U + V),
+        "pois_fwd": (2 * U + V) + V,
+        "pois_solve": 2 * V,
+        "pois_bwd": 2 * V,
+        "project": V + 2 * (2 * U + 2 * V),
+        "substep_survey": 55.0 * U,
+    }
+
+
+def read_traffic(kernel: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "dram_traffic.txt")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        for line in f:
+            parts = line.split()
+            if len(parts) >= 2 and parts[0] == kernel and not line.startswith("#"):
+                try:
+                    return float(parts[1])
+                except ValueError:
+                    return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = f"/tmp/otbl_clocks_{os.getpid()}.csv"
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                p = [x.strip() for x in line.split(",")]
+                if len(p) < 9:
+                    continue
+                try:
+                    sm.append(float(p[1]))
+                    smax = float(p[2])
+                except ValueError:
+                    continue
+                for n, v in zip(names, p[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def dist_max(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(ws: int):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def build_box(cfg, device):
+    init = synth.make_initial(cfg)
+    coef = native.coef_compute(cfg, init["re"], init["xout"], init["y"], init["u0"])
+    return init, coef, Box(cfg, init, coef, device=device)
+
+
+def cpu_baseline(cfg, init, coef, nsub: int):
+    """The CPU port (oracle/) on nsub substeps of the same box, all host threads."""
+    from oracle import pyoracle
+    threads = os.cpu_count() or 1
+    ob = pyoracle.OracleBox(cfg, init, coef, threads=threads)
+    t0 = time.perf_counter()
+    for s in range(nsub):
+        m = s % 3 + 1
+        st = ob.substep(m, 1 if m == 1 else 0)
+        if st != 0:
+            raise RuntimeError(f"oracle substep failed: {st}")
+    dt = time.perf_counter() - t0
+    ob.close()
+    return cfg.mpts * nsub / dt, threads, dt
+
+
+def run_reference(args, cfg, ws, rank):
+    if rank != 0:
+        return
+    init = synth.make_initial(cfg)
+    coef = native.coef_compute(cfg, init["re"], init["xout"], init["y"], init["u0"])
+    from oracle import pyoracle
+    threads = os.cpu_count() or 1
+    ob = pyoracle.OracleBox(cfg, init, coef, threads=threads)
+    warm = min(args.warmup, 1)
+    steps = max(1, min(args.steps, 3))
+    for s in range(warm):
+        ob.substep(s % 3 + 1, 1 if s % 3 == 0 else 0)
+    t0 = time.perf_counter()
+    for s in range(steps):
+        m = (warm + s) % 3 + 1
+        ob.substep(m, 1 if m == 1 else 0)
+    el = time.perf_counter() - t0
+    val = cfg.mpts * steps / el
+    sample = (f"{steps} RK3 substeps of the {cfg.nx}x{cfg.ny}x{cfg.nz} box "
+              f"(after {warm} warm-up), CPU port of rhsp/outflow_correction/pois")
+    out = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": ws,
+           "steps": steps, "warmup": warm, "ms_per_step": 1e3 * el / steps,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic", "config": {"workload": f"rk3_substep {cfg.name} fp64",
+                                           "nx": cfg.nx, "ny": cfg.ny, "nz": cfg.nz},
+           "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port",
+                            "sample": sample},
+           "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default=WORKLOAD)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    cfg = getattr(cfgmod, args.config)
+    ws, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, cfg, ws, rank)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    init, coef, box = build_box(cfg, local)
+    stream = torch.cuda.ExternalStream(box.stream, device=f"cuda:{local}")
+    warm = max(args.warmup, 0)
+    K = max(args.steps, 1)
+    for _ in range(warm):
+        box.advance(1)
+    box.sync()
+
+    # ---- device-timed region: K RK3 steps, CUDA events on the box's stream ----
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    dist_barrier(ws)
+    torch.cuda.synchronize()
+    box.sync()
+    l0 = box.launches
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(K):
+            box.advance(1)
+        ev1.record(stream)
+        ev1.synchronize()
+    box.sync()
+    torch.cuda.synchronize()
+    dist_barrier(ws)
+    launches = box.launches - l0
+    ms = ev0.elapsed_time(ev1)
+    ms = dist_max(ms, ws)
+    sub = 3 * K
+    value = ws * cfg.mpts * sub / (ms / 1e3)
+    clocks = clk.summary()
+
+    # ---- per-kernel timing pass (not part of `value`) ----
+    box.profile(True)
+    box.advance(1)
+    prof = box.profile_read()
+    box.profile(False)
+    per_sub = {k: v[0] / 3.0 for k, v in prof.items()}      # ms per substep
+    dom = max(per_sub, key=per_sub.get)
+    ab = algorithmic_bytes(cfg)
+    peak, peak_kind = peaks()
+    launches_dom = prof[dom][1] / 3.0
+    t_dom = per_sub[dom] / 1e3
+    achieved = ab[dom] / t_dom / 1e9 if dom in ab else None
+    traffic = read_traffic(dom)
+    sub_ms = ms / sub
+    roofline = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                "peak_kind": peak_kind, "algorithmic_bytes_per_launch": ab.get(dom),
+                "launches_per_substep": launches_dom, "ms_per_substep": per_sub[dom]}
+    substep_roofline = {"bytes_per_substep": ab["substep_survey"], "ms_per_substep": sub_ms,
+                        "achieved": ab["substep_survey"] / (sub_ms / 1e3) / 1e9, "peak": peak,
+                        "unit": "GB/s", "frac": ab["substep_survey"] / (sub_ms / 1e3) / 1e9 / peak,
+                        "peak_kind": peak_kind}
+    kernels = {k: round(v, 4) for k, v in sorted(per_sub.items(), key=lambda t: -t[1])}
+
+    # ---- end to end through the public API with host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        names = native.FIELDS
+        pinned = {n: torch.empty(box.shape(n), dtype=torch.float64, pin_memory=True) for n in names}
+        for n in names:
+            pinned[n].numpy()[...] = init[n]
+        D = ctypes.POINTER(ctypes.c_double)
+        um = torch.empty(cfg.ny + 1, dtype=torch.float64, pin_memory=True)
+        inf = native.OtblInflow()
+        L = box.L
+        state_bytes = sum(pinned[n].numel() * 8 for n in names)
+        out_names = ("u", "v", "w", "p")
+        out_bytes = sum(pinned[n].numel() * 8 for n in out_names)
+        box.sync()
+        dist_barrier(ws)
+        t0 = time.perf_counter()
+        for i, n in enumerate(names):   # restart: state from host (getstartzy)
+            L.otbl_set_field(box.h, i, ctypes.cast(pinned[n].data_ptr(), D))
+        for _ in range(K):
+            box.advance(1)
+            # per-step result read-back: dt, u_tau, Re_theta, gamma, um(y)
+            L.otbl_get_inflow(box.h, ctypes.cast(um.data_ptr(), D), ctypes.byref(inf))
+        for n in out_names:             # checkpoint: u, v, w, p to host (escribezy)
+            L.otbl_get_field(box.h, names.index(n), ctypes.cast(pinned[n].data_ptr(), D))
+        el = time.perf_counter() - t0
+        el = dist_max(el, ws)
+        diag_bytes = 8 * (cfg.ny + 1) + 8 * 12
+        e2e = {"value": ws * cfg.mpts * sub / el, "unit": UNIT,
+               "h2d_bytes_per_step": state_bytes / K,
+               "d2h_bytes_per_step": diag_bytes + out_bytes / K,
+               "job": f"restart upload of the 7 state fields, {K} RK3 steps with per-step "
+                      f"diagnostics read-back, checkpoint of u,v,w,p"}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            val, cores, secs = cpu_baseline(cfg, init, coef, 1)
+            cpu = {"value": val, "unit": UNIT, "cores": cores, "kind": "port",
+                   "sample": f"1 RK3 substep of the {cfg.nx}x{cfg.ny}x{cfg.nz} box "
+                             f"({secs:.1f} s), CPU port of rhsp/outflow_correction/pois"}
+        except Exception as e:  # reported, never fatal for the GPU number
+            cpu = {"value": None, "unit": UNIT, "cores": None, "kind": "port", "sample": f"failed: {e}"}
+
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K,
+               "warmup": warm, "ms_per_step": ms / K, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+               "config": {"workload": f"rk3_substep {cfg.name} fp64", "nx": cfg.nx, "ny": cfg.ny,
+                          "nz": cfg.nz, "substeps_per_step": 3,
+                          "l2": "inputs larger than L2 (state %.1f GB per box)" % (
+                              sum(np.prod(box.shape(n)) for n in native.FIELDS) * 8 / 1e9),
+                          "parallelism": f"replicas{ws}"},
+               "roofline": roofline, "substep_roofline": substep_roofline,
+               "kernels_ms_per_substep": kernels,
+               "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks}
+        print(json.dumps(out), flush=True)
+    box.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -129,6 +129,18 @@ int otbl_genflu(otbl_ctx *ctx);                      /* genflu.F90:3       */
 /* kernel launches issued by this context since creation */
 long long otbl_launch_count(const otbl_ctx *ctx);
 
+/* ---- instrumentation (no counterpart in the reference, whose timers are
+ *      the MPI_WTIME accumulators of module temporal, mod.F90:311-322) ---- */
+/* the context's CUDA stream (cudaStream_t), for events recorded by callers */
+int otbl_get_stream(otbl_ctx *ctx, void **stream);
+/* on != 0: record a CUDA event pair around every kernel launch; clears the
+ * records. Timing adds events to the stream; leave it off for throughput. */
+int otbl_profile_enable(otbl_ctx *ctx, int on);
+/* totals per kernel class (kind = 0, 1, ...; OTBL_ERR_ARG past the last):
+ * name, summed device milliseconds and number of launches. Synchronizes. */
+int otbl_profile_read(otbl_ctx *ctx, int kind, const char **name,
+                      double *total_ms, int *count);
+
 #ifdef __cplusplus
 }
 #endif

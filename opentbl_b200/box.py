@@ -89,6 +89,31 @@ class Box:
         return um, {n: getattr(st, n) for n, _ in OtblInflow._fields_}
 
     @property
+    def stream(self) -> int:
+        """Raw cudaStream_t of the context (for torch.cuda.ExternalStream)."""
+        h = ctypes.c_void_p()
+        self._check(self.L.otbl_get_stream(self.h, ctypes.byref(h)), "otbl_get_stream")
+        return h.value or 0
+
+    def profile(self, on: bool):
+        self._check(self.L.otbl_profile_enable(self.h, int(on)), "otbl_profile_enable")
+
+    def profile_read(self) -> dict:
+        """{kernel class: (total device ms, launches)} since profile(True)."""
+        out = {}
+        k = 0
+        while True:
+            name = ctypes.c_char_p()
+            ms = ctypes.c_double()
+            n = ctypes.c_int()
+            if self.L.otbl_profile_read(self.h, k, ctypes.byref(name), ctypes.byref(ms), ctypes.byref(n)) != 0:
+                break
+            if n.value:
+                out[name.value.decode()] = (ms.value, n.value)
+            k += 1
+        return out
+
+    @property
     def launches(self) -> int:
         return int(self.L.otbl_launch_count(self.h))
 

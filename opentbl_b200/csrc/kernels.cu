@@ -1163,6 +1163,37 @@ __global__ void k_twiddles(double2 *tw, int n, double2 *tw2, int n2, int mode2) 
 // ---------------------------------------------------------------------------
 // launch wrappers
 // ---------------------------------------------------------------------------
+const char *const kProfNames[PK_COUNT] = {"interpx", "interpy", "products", "difvisx", "dt",
+                                          "genflu", "final", "outflow", "pois_fwd", "pois_solve",
+                                          "pois_bwd", "project", "misc"};
+
+static cudaEvent_t prof_event(otbl_ctx *c) {
+  if (!c->prof_pool.empty()) {
+    cudaEvent_t e = c->prof_pool.back();
+    c->prof_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  return e;
+}
+
+void prof_begin(otbl_ctx *c, int kind) {
+  if (!c->prof_on) return;
+  otbl_ctx::ProfRec r;
+  r.kind = kind;
+  r.a = prof_event(c);
+  r.b = prof_event(c);
+  cudaEventRecord(r.a, c->stream);
+  c->prof.push_back(r);
+  c->prof_open = (int)c->prof.size() - 1;
+}
+
+void prof_end(otbl_ctx *c) {
+  if (!c->prof_on || c->prof_open < 0) return;
+  cudaEventRecord(c->prof[c->prof_open].b, c->stream);
+  c->prof_open = -1;
+}
 static inline ZTab ztab(otbl_ctx *c) {
   ZTab z;
   z.tw = reinterpret_cast<const double2 *>(c->w.twz);
@@ -1193,9 +1224,11 @@ cudaError_t launch_twiddles(otbl_ctx *c) {
 cudaError_t launch_interpx(otbl_ctx *c) {
   const int nz1 = c->dc.nz1, ny = c->cfg.ny;
   const int npu = nz1 * (ny + 1), npv = nz1 * ny;
+  prof_begin(c, PK_INTERPX);
   k_interpx<<<(npu + 127) / 128, 128, 0, c->stream>>>(c->dc, c->f[OTBL_F_U], c->w.ux, 0, npu);
   k_interpx<<<(npv + 127) / 128, 128, 0, c->stream>>>(c->dc, c->f[OTBL_F_V], c->w.vx, 1, npv);
   k_interpx<<<(npu + 127) / 128, 128, 0, c->stream>>>(c->dc, c->f[OTBL_F_W], c->w.wx, 1, npu);
+  prof_end(c);
   c->launches += 3;
   return cudaGetLastError();
 }
@@ -1203,9 +1236,11 @@ cudaError_t launch_interpx(otbl_ctx *c) {
 cudaError_t launch_interpy(otbl_ctx *c) {
   const int nz1 = c->dc.nz1;
   dim3 g((nz1 + 127) / 128, c->cfg.nx);
+  prof_begin(c, PK_INTERPY);
   k_interpy<<<g, 128, 0, c->stream>>>(c->dc, c->f[OTBL_F_U], c->w.uy, 0);
   k_interpy<<<g, 128, 0, c->stream>>>(c->dc, c->f[OTBL_F_W], c->w.wy, 0);
   k_interpy<<<g, 128, 0, c->stream>>>(c->dc, c->f[OTBL_F_V], c->w.vy, 1);
+  prof_end(c);
   c->launches += 3;
   return cudaGetLastError();
 }
@@ -1240,7 +1275,9 @@ cudaError_t launch_products(otbl_ctx *c, int setstep) {
   const size_t smem = (size_t)4 * 3 * M * sizeof(double2);
   cudaFuncSetAttribute(k_products, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   dim3 g((c->cfg.ny + 1 + 3) / 4, c->cfg.nx);
+  prof_begin(c, PK_PRODUCTS);
   k_products<<<g, 128, smem, c->stream>>>(c->dc, ztab(c), a);
+  prof_end(c);
   c->launches += 1;
   return cudaGetLastError();
 }
@@ -1248,16 +1285,20 @@ cudaError_t launch_products(otbl_ctx *c, int setstep) {
 cudaError_t launch_difvisx(otbl_ctx *c) {
   const int nz1 = c->dc.nz1, ny = c->cfg.ny;
   const int npu = nz1 * (ny + 1), npv = nz1 * ny;
+  prof_begin(c, PK_DIFVISX);
   k_difvisx<<<(npu + 127) / 128, 128, 0, c->stream>>>(c->dc, c->w.uu, c->f[OTBL_F_U], c->w.cu, c->w.s1, 0, npu);
   k_difvisx<<<(npv + 127) / 128, 128, 0, c->stream>>>(c->dc, c->w.uv, c->f[OTBL_F_V], c->w.cv, c->w.s2, 1, npv);
   k_difvisx<<<(npu + 127) / 128, 128, 0, c->stream>>>(c->dc, c->w.uw, c->f[OTBL_F_W], c->w.cw, c->w.s3, 1, npu);
+  prof_end(c);
   c->launches += 3;
   return cudaGetLastError();
 }
 
 cudaError_t launch_dt(otbl_ctx *c, int m, int setstep) {
+  prof_begin(c, PK_DT);
   k_dt<<<1, 32, 0, c->stream>>>(c->dc, c->st, c->w.vm_bits, c->w.fac_u, c->w.fac_v, m, setstep, c->cfg.dt_mode,
                                 c->cfg.dt_fixed);
+  prof_end(c);
   c->launches += 1;
   return cudaGetLastError();
 }
@@ -1278,7 +1319,9 @@ cudaError_t launch_genflu(otbl_ctx *c) {
   const int ny = c->cfg.ny;
   const size_t smem = sizeof(double) * (4 * (size_t)(ny + 1)) + sizeof(int) * 2 * (ny + 1);
   cudaFuncSetAttribute(k_genflu, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  prof_begin(c, PK_GENFLU);
   k_genflu<<<1, 512, smem, c->stream>>>(c->dc, a);
+  prof_end(c);
   c->launches += 1;
   return cudaGetLastError();
 }
@@ -1307,13 +1350,17 @@ cudaError_t launch_final(otbl_ctx *c) {
   a.fac_v = c->w.fac_v;
   a.st = c->st;
   dim3 g((c->dc.nz1 + 127) / 128, c->cfg.nx - 1);
+  prof_begin(c, PK_FINAL);
   k_final<<<g, 128, 0, c->stream>>>(c->dc, a);
+  prof_end(c);
   c->launches += 1;
   return cudaGetLastError();
 }
 
 cudaError_t launch_outflow(otbl_ctx *c) {
+  prof_begin(c, PK_OUTFLOW);
   k_outflow<<<1, 256, 0, c->stream>>>(c->dc, c->f[OTBL_F_U], c->f[OTBL_F_V], c->f[OTBL_F_RHSUPA]);
+  prof_end(c);
   c->launches += 1;
   return cudaGetLastError();
 }
@@ -1327,13 +1374,21 @@ cudaError_t launch_pois(otbl_ctx *c, int m) {
   cudaFuncSetAttribute(k_pois_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   double *phi = c->w.ux, *dinv = c->w.s1;
   dim3 gx((nz2 + 1 + 1) / 2, ny - 1);
+  prof_begin(c, PK_POIS_FWD);
   k_pois_fwd<<<gx, 256, smem, c->stream>>>(c->dc, xtab(c), c->f[OTBL_F_U], c->f[OTBL_F_V], c->f[OTBL_F_W], phi);
+  prof_end(c);
   dim3 gs((nz1 + 127) / 128, nx - 1);
+  prof_begin(c, PK_POIS_SOLVE);
   k_pois_solve<<<gs, 128, 0, c->stream>>>(c->dc, phi, dinv);
+  prof_end(c);
+  prof_begin(c, PK_POIS_BWD);
   k_pois_bwd<<<gx, 256, smem, c->stream>>>(c->dc, xtab(c), phi);
+  prof_end(c);
   dim3 gp((nz1 + 127) / 128, ny, nx - 1);
+  prof_begin(c, PK_PROJECT);
   k_project<<<gp, 128, 0, c->stream>>>(c->dc, c->st, phi, c->f[OTBL_F_U], c->f[OTBL_F_V], c->f[OTBL_F_W],
                                        c->f[OTBL_F_P]);
+  prof_end(c);
   c->launches += 4;
   return cudaGetLastError();
 }

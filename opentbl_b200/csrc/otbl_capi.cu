@@ -186,6 +186,11 @@ extern "C" void otbl_ctx_destroy(otbl_ctx *c) {
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  for (auto &r : c->prof) {
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  for (cudaEvent_t e : c->prof_pool) cudaEventDestroy(e);
   for (void *p : c->allocs) cudaFree(p);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -385,5 +390,45 @@ extern "C" int otbl_genflu(otbl_ctx *c) {
   if (!c) return OTBL_ERR_ARG;
   cudaSetDevice(c->device);
   LAUNCH(c, launch_genflu(c));
+  return OTBL_OK;
+}
+
+extern "C" int otbl_get_stream(otbl_ctx *c, void **stream) {
+  if (!c || !stream) return OTBL_ERR_ARG;
+  *stream = (void *)c->stream;
+  return OTBL_OK;
+}
+
+extern "C" int otbl_profile_enable(otbl_ctx *c, int on) {
+  if (!c) return OTBL_ERR_ARG;
+  cudaSetDevice(c->device);
+  OTBL_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  for (auto &r : c->prof) {
+    c->prof_pool.push_back(r.a);
+    c->prof_pool.push_back(r.b);
+  }
+  c->prof.clear();
+  c->prof_open = -1;
+  c->prof_on = on != 0;
+  return OTBL_OK;
+}
+
+extern "C" int otbl_profile_read(otbl_ctx *c, int kind, const char **name, double *total_ms, int *count) {
+  if (!c || kind < 0 || kind >= PK_COUNT) return OTBL_ERR_ARG;
+  cudaSetDevice(c->device);
+  OTBL_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  double tot = 0.0;
+  int n = 0;
+  for (auto &r : c->prof) {
+    if (r.kind != kind) continue;
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) {
+      tot += ms;
+      ++n;
+    }
+  }
+  if (name) *name = kProfNames[kind];
+  if (total_ms) *total_ms = tot;
+  if (count) *count = n;
   return OTBL_OK;
 }

@@ -73,7 +73,26 @@ struct otbl_ctx {
   size_t bytes;
   long long launches;
   std::string err;
+  // optional per-kernel timing: a CUDA event pair around every launch
+  bool prof_on = false;
+  struct ProfRec {
+    int kind;
+    cudaEvent_t a, b;
+  };
+  std::vector<ProfRec> prof;
+  std::vector<cudaEvent_t> prof_pool;
+  int prof_open = -1;
 };
+
+namespace otbl {
+enum ProfKind {
+  PK_INTERPX = 0, PK_INTERPY, PK_PRODUCTS, PK_DIFVISX, PK_DT, PK_GENFLU, PK_FINAL,
+  PK_OUTFLOW, PK_POIS_FWD, PK_POIS_SOLVE, PK_POIS_BWD, PK_PROJECT, PK_MISC, PK_COUNT
+};
+extern const char *const kProfNames[PK_COUNT];
+void prof_begin(otbl_ctx *c, int kind);
+void prof_end(otbl_ctx *c);
+}  // namespace otbl
 
 #define OTBL_CUDA_TRY(ctx, call)                                        \
   do {                                                                  \

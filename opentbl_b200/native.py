@@ -84,6 +84,9 @@ def _bind(L):
         "otbl_boun": ([P], I),
         "otbl_genflu": ([P], I),
         "otbl_launch_count": ([P], ctypes.c_longlong),
+        "otbl_get_stream": ([P, ctypes.POINTER(P)], I),
+        "otbl_profile_enable": ([P, I], I),
+        "otbl_profile_read": ([P, I, ctypes.POINTER(ctypes.c_char_p), D, ctypes.POINTER(I)], I),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
