@@ -70,6 +70,10 @@ C1 = BoxConfig(nx=257, ny=97, nz=128, lx=60.0, ly=8.0, lz=8.0, re_theta=300.0,
 # 1025x193x512, Re_theta=1000, Lx=80, Ly=10, Lz=10
 C2 = BoxConfig(nx=1025, ny=193, nz=512, lx=80.0, ly=10.0, lz=10.0,
                re_theta=1000.0, profile="musker", name="C2-1025x193x512")
+# medium box for profiling captures: fields of 135 MB (larger than L2),
+# about 3.5 GB on the device
+MED = BoxConfig(nx=513, ny=193, nz=256, lx=40.0, ly=10.0, lz=8.0,
+                re_theta=1000.0, profile="musker", name="MED-513x193x256")
 # small box for tests and smoke runs
 TINY = BoxConfig(nx=33, ny=41, nz=32, lx=12.0, ly=6.0, lz=4.0, dy_wall=0.02,
                  re_theta=300.0, profile="blasius", y_blend=1.5,

@@ -25,282 +25,15 @@
 // exactly the loads/stores where the reference transposes.
 #include <cfloat>
 
+#include "devcommon.cuh"
 #include "fft.cuh"
 #include "otbl_internal.cuh"
 
 namespace otbl {
-
-#define A3(a, r, i) (a)[((i)-1) * 3 + (r)-1]
-#define A2(a, r, i) (a)[((i)-1) * 2 + (r)-1]
-#define M4(a, r, cc) (a)[((cc)-1) * 4 + (r)-1]
-#define M5(a, r, cc) (a)[((cc)-1) * 5 + (r)-1]
-#define M2(a, r, cc) (a)[((cc)-1) * 2 + (r)-1]
-
-__device__ __forceinline__ double rnd(double x, int xr) { return xr ? (double)(float)x : x; }
-
-// NaN-propagating maximum of non-negative values
-__device__ __forceinline__ double nmax(double m, double v) {
-  return (m != m) ? m : ((v != v) ? v : fmax(m, v));
-}
 __device__ __forceinline__ double warp_nmax(double m) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) m = nmax(m, __shfl_xor_sync(0xffffffffu, m, o));
   return m;
-}
-
-// ---------------------------------------------------------------------------
-// x-line kernels: one thread per pencil mp in [0, np), np = nz1*jee. The
-// pencil's value at plane i sits at in[(i-1)*np + mp], so a warp reads 32
-// consecutive doubles per plane.
-// ---------------------------------------------------------------------------
-
-// interpxx, lip.f90:248-300. which 0: u (inxu, cofiux, chi=2, chi2=3);
-// which 1: v,w (inxv, cofivx, chi=1, chi2=4).
-__global__ void __launch_bounds__(128) k_interpx(DCoef c, const double *__restrict__ in,
-                                                 double *__restrict__ out, int which, int np) {
-  const int mp = blockIdx.x * blockDim.x + threadIdx.x;
-  if (mp >= np) return;
-  const int nx = c.nx, xr = c.xround;
-  const size_t S = (size_t)np;
-  const double *icon = which == 0 ? c.inxu : c.inxv;
-  const double *econ = which == 0 ? c.cofiux : c.cofivx;
-  const int chi = which == 0 ? 2 : 1, chi2 = which == 0 ? 3 : 4;
-  const double *ib = c.inbx;
-  const double *g = in + mp;
-  double *o = out + mp;
-  auto G = [&](int i) { return rnd(__ldg(g + (size_t)(i - 1) * S), xr); };
-  double bb = M4(ib, chi2, 1) * G(1) + M4(ib, chi2, 2) * G(2) + M4(ib, chi2, 3) * G(3) + M4(ib, chi2, 4) * G(4);
-  o[0] = bb;
-  double gi = G(2);
-  for (int i = 2; i <= nx - 1; ++i) {
-    const double gn = G(i + 1);
-    const double b = A2(econ, 1, i) * gi + A2(econ, 2, i) * gn;
-    bb = b + A3(icon, 1, i) * bb;
-    o[(size_t)(i - 1) * S] = bb;
-    gi = gn;
-  }
-  {
-    const double b = M4(ib, chi, 1) * G(nx) + M4(ib, chi, 2) * G(nx - 1) + M4(ib, chi, 3) * G(nx - 2) +
-                     M4(ib, chi, 4) * G(nx - 3);
-    bb = b + A3(icon, 1, nx) * bb;
-  }
-  double x = bb * A3(icon, 2, nx);
-  o[(size_t)(nx - 1) * S] = rnd(x, xr);
-  for (int i = nx - 1; i >= 1; --i) {
-    x = (o[(size_t)(i - 1) * S] - A3(icon, 3, i) * x) * A3(icon, 2, i);
-    o[(size_t)(i - 1) * S] = rnd(x, xr);
-  }
-}
-
-// difvisxx, lip.f90:52-142: result = Pade d/dx(gin) + rex * Pade d2/dx2(up),
-// outflow rows replaced as lip.f90:105,132. which 0: u; which 1: v,w.
-// scr holds the viscous forward sweep.
-__global__ void __launch_bounds__(128) k_difvisx(DCoef c, const double *__restrict__ gin,
-                                                 const double *__restrict__ upin, double *__restrict__ out,
-                                                 double *__restrict__ scr, int which, int np) {
-  const int mp = blockIdx.x * blockDim.x + threadIdx.x;
-  if (mp >= np) return;
-  const int nx = c.nx, xr = c.xround;
-  const size_t S = (size_t)np;
-  const double *icon = which == 0 ? c.dcxu : c.dcxv;
-  const double *iconv = which == 0 ? c.vixu : c.vixv;
-  const double *econ = which == 0 ? c.cofcxu : c.cofcxv;
-  const double *econv = which == 0 ? c.cofvxu : c.cofvxv;
-  const int chv = which == 0 ? 1 : 2, chv1 = chv + 2, ic = which == 0 ? 3 : 1;
-  const double *db = c.dcbx, *vb = c.cofvbx;
-  const double rex = c.S[OTBL_S_REX], idx = c.S[OTBL_S_IDX], uinf = c.S[OTBL_S_UINF];
-  const double *g = gin + mp, *up = upin + mp;
-  double *o = out + mp, *s = scr + mp;
-  auto G = [&](int i) { return rnd(__ldg(g + (size_t)(i - 1) * S), xr); };
-  auto U = [&](int i) { return rnd(__ldg(up + (size_t)(i - 1) * S), xr); };
-  double bc = M5(db, chv, 1) * G(1) + M5(db, chv, 2) * G(2) + M5(db, chv, 3) * G(3) + M5(db, chv, 4) * G(4);
-  double bv = M4(vb, ic, 1) * U(1) + M4(vb, ic, 2) * U(2) + M4(vb, ic, 3) * U(3) + M4(vb, ic, 4) * U(4);
-  o[0] = bc;
-  s[0] = bv;
-  double gp = G(1), gi = G(2), um1 = U(1), ui = U(2);
-  for (int i = 2; i <= nx - 1; ++i) {
-    const double un = U(i + 1);
-    const double b = A2(econ, 1, i) * gp + A2(econ, 2, i) * gi;
-    bc = b + A3(icon, 1, i) * bc;
-    o[(size_t)(i - 1) * S] = bc;
-    const double bw = A3(econv, 1, i) * un + A3(econv, 2, i) * ui + A3(econv, 3, i) * um1;
-    bv = bw + A3(iconv, 1, i) * bv;
-    s[(size_t)(i - 1) * S] = bv;
-    gp = gi;
-    gi = G(i + 1);
-    um1 = ui;
-    ui = un;
-  }
-  const double uN = U(nx), uN1 = U(nx - 1), uN2 = U(nx - 2), uN3 = U(nx - 3);
-  {
-    const double b = M5(db, chv1, 1) * G(nx) + M5(db, chv1, 2) * G(nx - 1) + M5(db, chv1, 3) * G(nx - 2) +
-                     M5(db, chv1, 4) * G(nx - 3);
-    bc = b + A3(icon, 1, nx) * bc;
-    const double bw = M4(vb, ic + 1, 1) * uN + M4(vb, ic + 1, 2) * uN1 + M4(vb, ic + 1, 3) * uN2 +
-                      M4(vb, ic + 1, 4) * uN3;
-    bv = bw + A3(iconv, 1, nx) * bv;
-  }
-  double xc = bc * A3(icon, 2, nx);
-  double xv = bv * A3(iconv, 2, nx);
-  o[(size_t)(nx - 1) * S] = rnd(uinf * (uN - uN1) * idx + rex * 0.0, xr);
-  for (int i = nx - 1; i >= 1; --i) {
-    xc = (o[(size_t)(i - 1) * S] - A3(icon, 3, i) * xc) * A3(icon, 2, i);
-    xv = (s[(size_t)(i - 1) * S] - A3(iconv, 3, i) * xv) * A3(iconv, 2, i);
-    o[(size_t)(i - 1) * S] = rnd(xc + rex * xv, xr);
-  }
-}
-
-// ---------------------------------------------------------------------------
-// y-line helpers: one thread per column (i, kr); rows j are nz1 apart.
-// ---------------------------------------------------------------------------
-
-// interpyy, lip.f90:359-440 (not in place); out rows 1..ny.
-__device__ __forceinline__ void col_interpyy(const DCoef &c, const double *g, double *o, int which) {
-  const int ny = c.ny;
-  const size_t S = c.nz1;
-  const double *icon = which == 0 ? c.inyu : c.inyv;
-  const double *econ = which == 0 ? c.cofiuy : c.cofivy;
-  const double *ib = c.inby;
-  auto G = [&](int j) { return g[(size_t)(j - 1) * S]; };
-  double bb;
-  if (which == 0) {
-    bb = 0.0;
-    o[0] = bb;
-    for (int j = 2; j <= ny - 1; ++j) {
-      const double b = A2(econ, 1, j) * G(j) + A2(econ, 2, j) * G(j + 1);
-      bb = b + A3(icon, 1, j) * bb;
-      o[(size_t)(j - 1) * S] = bb;
-    }
-    const double b = M4(ib, 1, 1) * G(ny + 1) + M4(ib, 1, 2) * G(ny) + M4(ib, 1, 3) * G(ny - 1) +
-                     M4(ib, 1, 4) * G(ny - 2);
-    bb = b + A3(icon, 1, ny) * bb;
-  } else {
-    bb = M4(ib, 3, 1) * G(1) + M4(ib, 3, 2) * G(2) + M4(ib, 3, 3) * G(3) + M4(ib, 3, 4) * G(4);
-    o[0] = bb;
-    for (int j = 2; j <= ny - 1; ++j) {
-      const double b = A2(econ, 2, j) * G(j) + A2(econ, 1, j) * G(j - 1);
-      bb = b + A3(icon, 1, j) * bb;
-      o[(size_t)(j - 1) * S] = bb;
-    }
-    const double b = M4(ib, 4, 1) * G(ny) + M4(ib, 4, 2) * G(ny - 1) + M4(ib, 4, 3) * G(ny - 2) +
-                     M4(ib, 4, 4) * G(ny - 3);
-    bb = b + A3(icon, 1, ny) * bb;
-  }
-  double x = bb * A3(icon, 2, ny);
-  o[(size_t)(ny - 1) * S] = x;
-  for (int j = ny - 1; j >= 1; --j) {
-    x = (o[(size_t)(j - 1) * S] - A3(icon, 3, j) * x) * A3(icon, 2, j);
-    o[(size_t)(j - 1) * S] = x;
-  }
-}
-
-// differzy, lip.f90:152-232 (not in place). which 0: u-type (dcyu, cofcyu,
-// chv=3, fwb1=-1, fwb2=0, jee=ny+1); which 1: v-type (dcyv, cofcyv, chv=1,
-// fwb1=0, fwb2=1, jee=ny). Reads rows 1..ny of g.
-__device__ __forceinline__ void col_differzy(const DCoef &c, const double *g, double *r, int which) {
-  const int ny = c.ny;
-  const size_t S = c.nz1;
-  const double *icon = which == 0 ? c.dcyu : c.dcyv;
-  const double *econ = which == 0 ? c.cofcyu : c.cofcyv;
-  const double *db = c.dcby;
-  const int chv = which == 0 ? 3 : 1, cha = chv + 1;
-  const int jee = which == 0 ? ny + 1 : ny;
-  auto G = [&](int j) { return g[(size_t)(j - 1) * S]; };
-  const double bot = M4(db, chv, 1) * G(1) + M4(db, chv, 2) * G(2) + M4(db, chv, 3) * G(3) + M4(db, chv, 4) * G(4);
-  const double top = M4(db, cha, 1) * G(ny) + M4(db, cha, 2) * G(ny - 1) + M4(db, cha, 3) * G(ny - 2) +
-                     M4(db, cha, 4) * G(ny - 3);
-  double x = bot;
-  r[0] = x;
-  for (int j = 2; j <= jee - 1; ++j) {
-    const double b = which == 0 ? A2(econ, 2, j) * G(j) + A2(econ, 1, j) * G(j - 1)
-                                : A2(econ, 2, j) * G(j + 1) + A2(econ, 1, j) * G(j);
-    x = b + A3(icon, 1, j) * x;
-    r[(size_t)(j - 1) * S] = x;
-  }
-  x = top + A3(icon, 1, jee) * x;
-  x = x * A3(icon, 2, jee);
-  r[(size_t)(jee - 1) * S] = x;
-  for (int j = jee - 1; j >= 1; --j) {
-    x = (r[(size_t)(j - 1) * S] - A3(icon, 3, j) * x) * A3(icon, 2, j);
-    r[(size_t)(j - 1) * S] = x;
-  }
-}
-
-// vistyy, lip.f90:447-513. which 0: u,w (viyu, cofvyu, jee=ny+1, ic=3);
-// which 1: v (viyv, cofvyv, jee=ny, ic=1).
-__device__ __forceinline__ void col_vistyy(const DCoef &c, const double *u, double *r, int which) {
-  const int ny = c.ny;
-  const size_t S = c.nz1;
-  const double *icon = which == 0 ? c.viyu : c.viyv;
-  const double *econ = which == 0 ? c.cofvyu : c.cofvyv;
-  const double *vb = c.cofvby;
-  const int jee = which == 0 ? ny + 1 : ny, ic = which == 0 ? 3 : 1;
-  auto U = [&](int j) { return u[(size_t)(j - 1) * S]; };
-  double x = M4(vb, ic, 1) * U(1) + M4(vb, ic, 2) * U(2) + M4(vb, ic, 3) * U(3) + M4(vb, ic, 4) * U(4);
-  r[0] = x;
-  for (int j = 2; j <= jee - 1; ++j) {
-    const double b = A3(econ, 1, j) * U(j + 1) + A3(econ, 2, j) * U(j) + A3(econ, 3, j) * U(j - 1);
-    x = b + A3(icon, 1, j) * x;
-    r[(size_t)(j - 1) * S] = x;
-  }
-  {
-    const double b = M4(vb, ic + 1, 1) * U(jee) + M4(vb, ic + 1, 2) * U(jee - 1) + M4(vb, ic + 1, 3) * U(jee - 2) +
-                     M4(vb, ic + 1, 4) * U(jee - 3);
-    x = b + A3(icon, 1, jee) * x;
-  }
-  x = x * A3(icon, 2, jee);
-  r[(size_t)(jee - 1) * S] = x;
-  for (int j = jee - 1; j >= 1; --j) {
-    x = (r[(size_t)(j - 1) * S] - A3(icon, 3, j) * x) * A3(icon, 2, j);
-    r[(size_t)(j - 1) * S] = x;
-  }
-}
-
-// implzy, lip.f90:528-597, with the LU of (A + var1*B) pre-factored by k_dt
-// into fac (a1,a2,a3 per row; raw a1(2) and a3(jee-1) after the rows).
-// res: right-hand side column (rows 1..jee); u: output column; rows 1 and
-// jee of u take the boundary values ub1 / ubj.
-__device__ __forceinline__ void col_implzy(const DCoef &c, const double *res, double *u, double ub1, double ubj,
-                                           const double *__restrict__ fac, int which) {
-  const int ny = c.ny;
-  const size_t S = c.nz1;
-  const double *icon = which == 0 ? c.vyui : c.vyvi;
-  const int jee = which == 0 ? ny + 1 : ny;
-  auto R = [&](int j) { return res[(size_t)(j - 1) * S]; };
-  const double a1raw = fac[3 * (jee + 1)], a3raw = fac[3 * (jee + 1) + 1];
-  double rm = R(1), r0 = R(2), rp;
-  double x = 0.0;
-  for (int j = 2; j <= jee - 1; ++j) {
-    rp = R(j + 1);
-    double t = A3(icon, 1, j) * rm + A3(icon, 2, j) * r0 + A3(icon, 3, j) * rp;
-    if (j == 2) t = t - a1raw * ub1;
-    if (j == jee - 1) t = t - a3raw * ubj;
-    if (j >= 3) t = t + fac[3 * j + 0] * x;
-    x = t;
-    u[(size_t)(j - 1) * S] = x;
-    rm = r0;
-    r0 = rp;
-  }
-  x = x * fac[3 * (jee - 1) + 1];
-  u[(size_t)(jee - 2) * S] = x;
-  for (int j = jee - 2; j >= 2; --j) {
-    x = (u[(size_t)(j - 1) * S] - fac[3 * j + 2] * x) * fac[3 * j + 1];
-    u[(size_t)(j - 1) * S] = x;
-  }
-  u[0] = ub1;
-  u[(size_t)(jee - 1) * S] = ubj;
-}
-
-// interpyy in Fourier space for u,w (which 0, jin = ny+1) and v (which 1).
-__global__ void __launch_bounds__(128) k_interpy(DCoef c, const double *__restrict__ in,
-                                                 double *__restrict__ out, int which) {
-  const int kr = blockIdx.x * blockDim.x + threadIdx.x;
-  if (kr >= c.nz1) return;
-  const int i = blockIdx.y + 1;
-  const int jin = which == 0 ? c.ny + 1 : c.ny;
-  const double *g = in + ((size_t)(i - 1) * jin) * c.nz1 + kr;
-  double *o = out + ((size_t)(i - 1) * c.ny) * c.nz1 + kr;
-  col_interpyy(c, g, o, which);
 }
 
 // ---------------------------------------------------------------------------
@@ -697,148 +430,6 @@ __global__ void __launch_bounds__(512) k_genflu(DCoef c, GenArgs a) {
   for (size_t e = t; e < PV; e += T) a.rhsvpa[e] = 0.0;
 }
 
-// ---------------------------------------------------------------------------
-// tail of rhsp (rhsp.F90:291-484) for planes 2..nx, one thread per column.
-// ---------------------------------------------------------------------------
-struct FinalArgs {
-  double *u, *v, *w;                 // state: old on entry, new on exit
-  const double *p;
-  double *rhsupa, *rhsvpa, *rhswpa;  // old on entry, new on exit
-  double *cu, *cv, *cw;              // difvisxx outputs; become rhsu/v/w
-  const double *uv, *uw, *vw, *vv, *ww;
-  double *s1, *s2, *s3;
-  const double *fac_u, *fac_v;
-  const DState *st;
-};
-
-__global__ void __launch_bounds__(128) k_final(DCoef c, FinalArgs a) {
-  const int kr = blockIdx.x * blockDim.x + threadIdx.x;
-  if (kr >= c.nz1) return;
-  const int i = blockIdx.y + 2;
-  const int nx = c.nx, ny = c.ny, nz1 = c.nz1;
-  const size_t S = nz1;
-  const int k = kr >> 1, odd = kr & 1, pof = odd ? -1 : 1;
-  const double kz = c.kaz[k], kv = c.kvis[k];
-  const bool last = (i == nx);
-  const size_t bu = (size_t)(i - 1) * (ny + 1) * nz1 + kr, bv = (size_t)(i - 1) * ny * nz1 + kr;
-  const double var1 = a.st->var1, var3 = a.st->var3, var4 = a.st->var4;
-  const double v2 = last ? 0.0 : a.st->var2;
-  const double idxx = c.S[OTBL_S_IDXX];
-  // (x * kaz) for the component kr of a complex column x: kaz = (0, kz)
-  auto kazm = [&](const double *col, int j) {
-    const double q = col[(size_t)(j - 1) * S + pof];
-    return odd ? kz * q : -kz * q;
-  };
-  double *s1 = a.s1 + bu, *s2 = a.s2 + bu, *s3 = a.s3 + bu;
-  double *uc = a.u + bu, *vc = a.v + bv, *wc = a.w + bu;
-  const double *pc = a.p + bv;
-  const double *ib = c.inby, *cc = c.ccon;
-  // ---- rhsv (rows 1..ny) ----
-  double *rv = a.cv + bv;
-  if (!last) col_differzy(c, a.vv + bv, s2, 1);
-  for (int j = 1; j <= ny; ++j) {
-    double r = rv[(j - 1) * S];
-    if (!last) {
-      if (j >= 2 && j <= ny - 1) r = r - vc[(j - 1) * S] * kv;
-      r = r + kazm(a.vw + bv, j);
-      r = r + s2[(j - 1) * S];
-    }
-    if (j == 1 || j == ny) r = 0.0;
-    rv[(j - 1) * S] = r;
-  }
-  // ---- rhsu (rows 1..ny+1) ----
-  double *ru = a.cu + bu;
-  if (!last) col_differzy(c, a.uv + bv, s1, 0);
-  for (int j = 1; j <= ny + 1; ++j) {
-    double r;
-    if (!last) {
-      r = s1[(j - 1) * S] + kazm(a.uw + bu, j);
-      r = r + ru[(j - 1) * S];
-      if (j >= 2 && j <= ny) r = r - uc[(j - 1) * S] * kv;
-    } else {
-      r = ru[(j - 1) * S];
-    }
-    ru[(j - 1) * S] = r;
-  }
-  ru[0] = -1.0 / M4(ib, 2, 1) * (M4(ib, 2, 2) * ru[S] + M4(ib, 2, 3) * ru[2 * S] + M4(ib, 2, 4) * ru[3 * S]);
-  ru[(size_t)ny * S] = 0.0;
-  // ---- rhsw (rows 1..ny+1) ----
-  double *rw = a.cw + bu;
-  if (!last) col_differzy(c, a.vw + bv, s3, 0);
-  for (int j = 1; j <= ny + 1; ++j) {
-    double r = rw[(j - 1) * S];
-    if (!last) {
-      if (j >= 2 && j <= ny) r = r - wc[(j - 1) * S] * kv;
-      r = r + s3[(j - 1) * S];
-      if (j <= ny) r = r + kazm(a.ww + bv, j);
-    }
-    rw[(j - 1) * S] = r;
-  }
-  rw[0] = -1.0 / M4(ib, 2, 1) * (M4(ib, 2, 2) * rw[S] + M4(ib, 2, 3) * rw[2 * S] + M4(ib, 2, 4) * rw[3 * S]);
-  rw[(size_t)ny * S] = 0.0;
-
-  // ---- v: pressure gradient, boun, vistyy, RK3 combination, implzy ----
-  {
-    auto vs = [&](int j) {
-      if (j == 1) return 0.0;
-      if (j == ny) return kr == 0 ? c.vmagic[i - 1] : 0.0;
-      return vc[(j - 1) * S] - var1 * c.idyy[j - 1] * (pc[(size_t)j * S] - pc[(size_t)(j - 1) * S]);
-    };
-    col_vistyy(c, vc, s2, 1);
-    double *hp = a.rhsvpa + bv;
-    for (int j = 1; j <= ny; ++j) {
-      const double wk = vs(j) - (var3 * rv[(j - 1) * S] + v2 * s2[(j - 1) * S] + var4 * hp[(j - 1) * S]);
-      s2[(j - 1) * S] = wk;
-      hp[(j - 1) * S] = rv[(j - 1) * S];
-    }
-    col_implzy(c, s2, vc, 0.0, vs(ny), a.fac_v, 1);
-  }
-  // ---- u ----
-  {
-    const double *pn = pc + (size_t)ny * nz1;  // plane i+1
-    auto us = [&](int j) {
-      const double q = uc[(j - 1) * S];
-      if (last) return q;
-      return q - var1 * idxx * (pn[(size_t)(j - 1) * S] - pc[(size_t)(j - 1) * S]);
-    };
-    const double u2 = us(2), u3 = us(3), u4 = us(4);
-    const double un = us(ny), un1 = us(ny - 1), un2 = us(ny - 2);
-    const double ub1 = -1.0 / M4(ib, 2, 1) * (M4(ib, 2, 2) * u2 + M4(ib, 2, 3) * u3 + M4(ib, 2, 4) * u4);
-    const double ubt = -1.0 / M2(cc, 1, 1) * (M2(cc, 1, 2) * un + M2(cc, 1, 3) * un1 + M2(cc, 1, 4) * un2);
-    col_vistyy(c, uc, s1, 0);
-    double *hp = a.rhsupa + bu;
-    for (int j = 1; j <= ny + 1; ++j) {
-      const double usj = j == 1 ? ub1 : (j == ny + 1 ? ubt : us(j));
-      const double wk = usj - (var3 * ru[(j - 1) * S] + v2 * s1[(j - 1) * S] + var4 * hp[(j - 1) * S]);
-      s1[(j - 1) * S] = wk;
-      hp[(j - 1) * S] = ru[(j - 1) * S];
-    }
-    col_implzy(c, s1, uc, ub1, ubt, a.fac_u, 0);
-  }
-  // ---- w ----
-  {
-    auto ws = [&](int j) {
-      const double q = wc[(j - 1) * S];
-      const double pp = pc[(size_t)(j - 1) * S + pof];
-      const double av = var1 * kz;
-      return q - (odd ? av * pp : -av * pp);
-    };
-    const double w2 = ws(2), w3 = ws(3), w4 = ws(4);
-    const double wn = ws(ny), wn1 = ws(ny - 1), wn2 = ws(ny - 2);
-    const double wb1 = -1.0 / M4(ib, 2, 1) * (M4(ib, 2, 2) * w2 + M4(ib, 2, 3) * w3 + M4(ib, 2, 4) * w4);
-    const double wbt = -1.0 / M2(cc, 1, 1) * (M2(cc, 1, 2) * wn + M2(cc, 1, 3) * wn1 + M2(cc, 1, 4) * wn2);
-    col_vistyy(c, wc, s3, 0);
-    double *hp = a.rhswpa + bu;
-    for (int j = 1; j <= ny + 1; ++j) {
-      const double wsj = j == 1 ? wb1 : (j == ny + 1 ? wbt : ws(j));
-      const double wk = wsj - (var3 * rw[(j - 1) * S] + v2 * s3[(j - 1) * S] + var4 * hp[(j - 1) * S]);
-      s3[(j - 1) * S] = wk;
-      hp[(j - 1) * S] = rw[(j - 1) * S];
-    }
-    col_implzy(c, s3, wc, wb1, wbt, a.fac_u, 0);
-  }
-}
-
 // boun (boun.f90:7-56) on every plane, for the standalone entry point
 __global__ void k_boun(DCoef c, double *u, double *v, double *w) {
   const int kr = blockIdx.x * blockDim.x + threadIdx.x;
@@ -954,42 +545,6 @@ __global__ void __launch_bounds__(256) k_pois_fwd(DCoef c, XTab x, const double 
     double *o = phi + (size_t)(kk + 1) * PV + (size_t)(j - 1) * nz1 + 2 * k;
     o[0] = re;
     o[1] = im;
-  }
-}
-
-// tridiagonal solve in y per (x-mode, kz), pois.f90:106-117 + soltriy;
-// one thread per column (plane i >= 2, real index kr); dinv scratch.
-__global__ void __launch_bounds__(128) k_pois_solve(DCoef c, double *phi, double *dinv) {
-  const int kr = blockIdx.x * blockDim.x + threadIdx.x;
-  if (kr >= c.nz1) return;
-  const int i = blockIdx.y + 2, ny = c.ny, ny1 = ny - 1, nz1 = c.nz1;
-  const size_t S = nz1;
-  const int k = kr >> 1;
-  double *col = phi + (size_t)(i - 1) * ny * nz1 + kr;
-  double *dv = dinv + (size_t)(i - 1) * ny * nz1 + kr;
-  const double *ayp = c.ayp;
-  const double shift_k = c.kaz2[k], shift_x = c.kmod[i - 2];
-  const bool sing = (i == 2 && k == 0);
-  if (sing) col[(size_t)(ny1 - 1) * S] = 0.0;
-  auto a2 = [&](int j) {
-    if (sing && j == ny1) return 2.0 * A3(ayp, 2, ny1);
-    return A3(ayp, 2, j) - shift_k - shift_x;
-  };
-  double a2p = a2(1);
-  double us = col[0];
-  for (int j = 2; j <= ny1; ++j) {
-    const double d = 1.0 / a2p;
-    dv[(size_t)(j - 2) * S] = d;
-    const double l = -A3(ayp, 1, j) * d;
-    a2p = a2(j) + l * A3(ayp, 3, j - 1);
-    us = col[(size_t)(j - 1) * S] + l * us;
-    col[(size_t)(j - 1) * S] = us;
-  }
-  double xv = us * (1.0 / a2p);
-  col[(size_t)(ny1 - 1) * S] = xv;
-  for (int j = ny1 - 1; j >= 1; --j) {
-    xv = (col[(size_t)(j - 1) * S] - A3(ayp, 3, j) * xv) * dv[(size_t)(j - 1) * S];
-    col[(size_t)(j - 1) * S] = xv;
   }
 }
 
@@ -1221,30 +776,6 @@ cudaError_t launch_twiddles(otbl_ctx *c) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_interpx(otbl_ctx *c) {
-  const int nz1 = c->dc.nz1, ny = c->cfg.ny;
-  const int npu = nz1 * (ny + 1), npv = nz1 * ny;
-  prof_begin(c, PK_INTERPX);
-  k_interpx<<<(npu + 127) / 128, 128, 0, c->stream>>>(c->dc, c->f[OTBL_F_U], c->w.ux, 0, npu);
-  k_interpx<<<(npv + 127) / 128, 128, 0, c->stream>>>(c->dc, c->f[OTBL_F_V], c->w.vx, 1, npv);
-  k_interpx<<<(npu + 127) / 128, 128, 0, c->stream>>>(c->dc, c->f[OTBL_F_W], c->w.wx, 1, npu);
-  prof_end(c);
-  c->launches += 3;
-  return cudaGetLastError();
-}
-
-cudaError_t launch_interpy(otbl_ctx *c) {
-  const int nz1 = c->dc.nz1;
-  dim3 g((nz1 + 127) / 128, c->cfg.nx);
-  prof_begin(c, PK_INTERPY);
-  k_interpy<<<g, 128, 0, c->stream>>>(c->dc, c->f[OTBL_F_U], c->w.uy, 0);
-  k_interpy<<<g, 128, 0, c->stream>>>(c->dc, c->f[OTBL_F_W], c->w.wy, 0);
-  k_interpy<<<g, 128, 0, c->stream>>>(c->dc, c->f[OTBL_F_V], c->w.vy, 1);
-  prof_end(c);
-  c->launches += 3;
-  return cudaGetLastError();
-}
-
 cudaError_t launch_reset_max(otbl_ctx *c) {
   k_reset_max<<<(c->cfg.ny + 1 + 255) / 256, 256, 0, c->stream>>>(c->st, c->w.vm_bits, c->cfg.ny);
   c->launches += 1;
@@ -1282,18 +813,6 @@ cudaError_t launch_products(otbl_ctx *c, int setstep) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_difvisx(otbl_ctx *c) {
-  const int nz1 = c->dc.nz1, ny = c->cfg.ny;
-  const int npu = nz1 * (ny + 1), npv = nz1 * ny;
-  prof_begin(c, PK_DIFVISX);
-  k_difvisx<<<(npu + 127) / 128, 128, 0, c->stream>>>(c->dc, c->w.uu, c->f[OTBL_F_U], c->w.cu, c->w.s1, 0, npu);
-  k_difvisx<<<(npv + 127) / 128, 128, 0, c->stream>>>(c->dc, c->w.uv, c->f[OTBL_F_V], c->w.cv, c->w.s2, 1, npv);
-  k_difvisx<<<(npu + 127) / 128, 128, 0, c->stream>>>(c->dc, c->w.uw, c->f[OTBL_F_W], c->w.cw, c->w.s3, 1, npu);
-  prof_end(c);
-  c->launches += 3;
-  return cudaGetLastError();
-}
-
 cudaError_t launch_dt(otbl_ctx *c, int m, int setstep) {
   prof_begin(c, PK_DT);
   k_dt<<<1, 32, 0, c->stream>>>(c->dc, c->st, c->w.vm_bits, c->w.fac_u, c->w.fac_v, m, setstep, c->cfg.dt_mode,
@@ -1326,37 +845,6 @@ cudaError_t launch_genflu(otbl_ctx *c) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_final(otbl_ctx *c) {
-  FinalArgs a;
-  a.u = c->f[OTBL_F_U];
-  a.v = c->f[OTBL_F_V];
-  a.w = c->f[OTBL_F_W];
-  a.p = c->f[OTBL_F_P];
-  a.rhsupa = c->f[OTBL_F_RHSUPA];
-  a.rhsvpa = c->f[OTBL_F_RHSVPA];
-  a.rhswpa = c->f[OTBL_F_RHSWPA];
-  a.cu = c->w.cu;
-  a.cv = c->w.cv;
-  a.cw = c->w.cw;
-  a.uv = c->w.uv;
-  a.uw = c->w.uw;
-  a.vw = c->w.vw;
-  a.vv = c->w.vv;
-  a.ww = c->w.ww;
-  a.s1 = c->w.s1;
-  a.s2 = c->w.s2;
-  a.s3 = c->w.s3;
-  a.fac_u = c->w.fac_u;
-  a.fac_v = c->w.fac_v;
-  a.st = c->st;
-  dim3 g((c->dc.nz1 + 127) / 128, c->cfg.nx - 1);
-  prof_begin(c, PK_FINAL);
-  k_final<<<g, 128, 0, c->stream>>>(c->dc, a);
-  prof_end(c);
-  c->launches += 1;
-  return cudaGetLastError();
-}
-
 cudaError_t launch_outflow(otbl_ctx *c) {
   prof_begin(c, PK_OUTFLOW);
   k_outflow<<<1, 256, 0, c->stream>>>(c->dc, c->f[OTBL_F_U], c->f[OTBL_F_V], c->f[OTBL_F_RHSUPA]);
@@ -1372,15 +860,13 @@ cudaError_t launch_pois(otbl_ctx *c, int m) {
   const size_t smem = (size_t)2 * n * sizeof(double2);
   cudaFuncSetAttribute(k_pois_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   cudaFuncSetAttribute(k_pois_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  double *phi = c->w.ux, *dinv = c->w.s1;
+  double *phi = c->w.ux;
   dim3 gx((nz2 + 1 + 1) / 2, ny - 1);
   prof_begin(c, PK_POIS_FWD);
   k_pois_fwd<<<gx, 256, smem, c->stream>>>(c->dc, xtab(c), c->f[OTBL_F_U], c->f[OTBL_F_V], c->f[OTBL_F_W], phi);
   prof_end(c);
-  dim3 gs((nz1 + 127) / 128, nx - 1);
-  prof_begin(c, PK_POIS_SOLVE);
-  k_pois_solve<<<gs, 128, 0, c->stream>>>(c->dc, phi, dinv);
-  prof_end(c);
+  cudaError_t e = launch_pois_solve(c, phi);
+  if (e != cudaSuccess) return e;
   prof_begin(c, PK_POIS_BWD);
   k_pois_bwd<<<gx, 256, smem, c->stream>>>(c->dc, xtab(c), phi);
   prof_end(c);
@@ -1389,7 +875,7 @@ cudaError_t launch_pois(otbl_ctx *c, int m) {
   k_project<<<gp, 128, 0, c->stream>>>(c->dc, c->st, phi, c->f[OTBL_F_U], c->f[OTBL_F_V], c->f[OTBL_F_W],
                                        c->f[OTBL_F_P]);
   prof_end(c);
-  c->launches += 4;
+  c->launches += 3;
   return cudaGetLastError();
 }
 

@@ -173,8 +173,9 @@ extern "C" int otbl_ctx_create(const otbl_config *cfg, const double *coef, int d
   TRY(dalloc(c, &w.fac_u, 3 * (size_t)(ny + 4)));
   TRY(dalloc(c, &w.fac_v, 3 * (size_t)(ny + 4)));
   TRY(dalloc(c, &w.gf, (size_t)nz1 * (ny + 2)));
+  TRY(dalloc(c, &w.pois_dinv, (size_t)nx * ny * (nz1 / 2)));
 #undef TRY
-  if (check(c, launch_twiddles(c), "twiddles") != OTBL_OK || check(c, cudaStreamSynchronize(c->stream), "init")) {
+  if (check(c, launch_twiddles(c), "twiddles") != OTBL_OK || check(c, launch_pois_lu(c), "pois_lu") != OTBL_OK || check(c, cudaStreamSynchronize(c->stream), "init")) {
     *out = c;
     return OTBL_ERR_CUDA;
   }

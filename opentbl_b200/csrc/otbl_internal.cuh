@@ -54,6 +54,7 @@ struct Work {
   unsigned long long *vm_bits; // vm(j) maxima, j = 1..ny
   double *fac_u, *fac_v;       // implzy LU factors for the current dt (3*(ny+1))
   double *gf;                  // genflu scratch: kl/fsca/ntop + wk plane
+  double *pois_dinv;           // pivots of the (x-mode, kz) y-systems, [i][j][k]
 };
 
 }  // namespace otbl
@@ -118,6 +119,8 @@ cudaError_t launch_reset_max(otbl_ctx *c);
 cudaError_t launch_boun_all(otbl_ctx *c);
 cudaError_t launch_tiempo(otbl_ctx *c);
 cudaError_t launch_twiddles(otbl_ctx *c);
+cudaError_t launch_pois_lu(otbl_ctx *c);
+cudaError_t launch_pois_solve(otbl_ctx *c, double *phi);
 // standalone pieces
 cudaError_t launch_chp2x(otbl_ctx *c, const double *plan, double *pen, int jee, int to_pen);
 cudaError_t launch_fourxz(otbl_ctx *c, double *fou, double *phys, int iopt, int nlines);
