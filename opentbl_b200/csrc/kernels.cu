@@ -242,15 +242,21 @@ __global__ void k_tiempo(DState *st) {
 }
 
 // ---------------------------------------------------------------------------
-// genflu (genflu.F90:3-242, NEWGENFLU) on one CTA, followed by boun on plane
-// 1 (boun.f90:33-55) and rhs*pa(plane 1) = 0 (rhsp.F90:424-426,441-442).
+// genflu (genflu.F90:3-242, NEWGENFLU) on one CTA. Inside the substep
+// (tail = 1) it is followed by boun on plane 1 (boun.f90:33-55) and
+// rhs*pa(plane 1) = 0 (rhsp.F90:424-426,441-442); plane 1 is not touched by
+// the rest of rhsp.
 // ---------------------------------------------------------------------------
 struct GenArgs {
   double *u, *v, *w, *rhsupa, *rhsvpa, *rhswpa;
   const double *u0, *v0;
   double *um;
   double *wk;  // nz1*(ny+2) scratch
-  DState *st;
+  // scalars: inputs dt, tiempo, timeinit; outputs of genflu.F90:67-93
+  const double *dt, *tiempo, *timeinit;
+  double *timec, *utauout, *rthout, *dout, *gamma1, *gamma2;
+  int *err;  // set to OTBL_ERR_NAN for a degenerate rescaled grid; may be null
+  int tail;
 };
 
 __device__ void dobleu_dev(const double *eta, double *www, double *www1, int n) {
@@ -326,9 +332,8 @@ __global__ void __launch_bounds__(512) k_genflu(DCoef c, GenArgs a) {
   for (size_t e = t; e < PV; e += T) a.v[e] = a.v[(size_t)(xout - 1) * PV + e];
   __syncthreads();
   if (t == 0) {
-    DState *st = a.st;
     const double re = c.S[OTBL_S_RE], din = c.S[OTBL_S_DIN], rthin = c.S[OTBL_S_RTHIN];
-    const double dt = st->dt, tloc = st->tiempo - st->timeinit;
+    const double dt = *a.dt, tloc = *a.tiempo - *a.timeinit;
     double timec;
     if (tloc < 20)
       timec = 20;
@@ -336,10 +341,10 @@ __global__ void __launch_bounds__(512) k_genflu(DCoef c, GenArgs a) {
       timec = 100;
     else
       timec = tloc;
-    st->timec = timec;
+    *a.timec = timec;
     double *um = a.um - 1;
     for (int j = 1; j <= ny + 1; ++j) um[j] = (dt / timec) * a.u[(size_t)(j - 1) * nz1] + um[j] * (1.0 - dt / timec);
-    st->utauout = sqrt(fabs((um[2] - um[1]) / (y[2] - y[1]) / re));
+    *a.utauout = sqrt(fabs((um[2] - um[1]) / (y[2] - y[1]) / re));
     double uinf = 0.0;
     for (int j = ny + 1 - 20; j <= ny + 1 - 5; ++j) uinf += um[j];
     uinf = uinf / 16.0;
@@ -349,19 +354,22 @@ __global__ void __launch_bounds__(512) k_genflu(DCoef c, GenArgs a) {
       if (um[j] >= u99) break;
       jtop = j + 1;
     }
-    st->dout = y[jtop];
+    *a.dout = y[jtop];
     double s = 0.0;
     for (int q = 0; q < jtop + 2; ++q) s += (uinf - um[2 + q]) * um[2 + q] * dy[1 + q];
-    st->rthout = s * re / uinf;
-    st->gamma2 = rthin / st->rthout;
-    st->gamma1 = pow(st->gamma2, 0.125);
-    ggg = 1.0 / st->gamma1;
+    const double rthout = s * re / uinf;
+    *a.rthout = rthout;
+    const double gamma2 = rthin / rthout;
+    const double gamma1 = pow(gamma2, 0.125);
+    *a.gamma2 = gamma2;
+    *a.gamma1 = gamma1;
+    ggg = 1.0 / gamma1;
     for (int kk = 1; kk <= 2; ++kk) {
       for (int j = 1; j <= ny; ++j) ysca[j] = kk == 1 ? 5e-1 * (y[j] + y[j + 1]) / din : y[j] / din;
       double www1;
       dobleu_dev(ysca, wlwa, &www1, ny);
       for (int j = 1; j <= ny; ++j)
-        wlwa[j] = ysca[j] / st->gamma1 + (1.0 / st->gamma2 - 1.0 / st->gamma1) / www1 * wlwa[j];
+        wlwa[j] = ysca[j] / gamma1 + (1.0 / gamma2 - 1.0 / gamma1) / www1 * wlwa[j];
       int kll = 1;
       int *klk = kl + (kk - 1) * (ny + 1);
       double *fk = fsca + (kk - 1) * (ny + 1);
@@ -406,10 +414,12 @@ __global__ void __launch_bounds__(512) k_genflu(DCoef c, GenArgs a) {
     profile_dev(c, a.u, a.wk, ntop[0], kl, fsca, ny + 1, ggg);
     profile_dev(c, a.w, a.wk, ntop[0], kl, fsca, ny + 1, ggg);
     profile_dev(c, a.v, a.wk, ntop[1], kl + (ny + 1), fsca + (ny + 1), ny, ggg);
-  } else if (t == 0) {
-    a.st->err = OTBL_ERR_NAN;
+  } else if (t == 0 && a.err) {
+    *a.err = OTBL_ERR_NAN;
   }
+  if (!a.tail) return;
   // boun on plane 1 and the plane-1 RHS history
+  __syncthreads();
   const double *ib = c.inby, *cc = c.ccon;
   for (int kr = t; kr < nz1; kr += T) {
     a.v[kr] = 0.0;
@@ -581,7 +591,10 @@ __global__ void __launch_bounds__(256) k_pois_bwd(DCoef c, XTab x, double *__res
     const double2 V = xsm[l * n + ((tt & 1) ? n - 1 - (tt >> 1) : (tt >> 1))];
     double *o = phi + (size_t)(tt + 1) * PV + (size_t)(j - 1) * nz1 + 2 * k;
     o[0] = rnd(0.5 * V.x, xr);
-    o[1] = rnd(0.5 * V.y, xr);
+    // mode 0 is real (pois.f90:102): its imaginary pencil is identically zero
+    // in the reference's real transforms, while the complex line transform
+    // used here leaves rounding-level values there
+    o[1] = k == 0 ? 0.0 : rnd(0.5 * V.y, xr);
   }
 }
 
@@ -822,7 +835,7 @@ cudaError_t launch_dt(otbl_ctx *c, int m, int setstep) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_genflu(otbl_ctx *c) {
+cudaError_t launch_genflu(otbl_ctx *c, int tail) {
   GenArgs a;
   a.u = c->f[OTBL_F_U];
   a.v = c->f[OTBL_F_V];
@@ -834,7 +847,18 @@ cudaError_t launch_genflu(otbl_ctx *c) {
   a.v0 = c->v0;
   a.um = c->um;
   a.wk = c->w.gf;
-  a.st = c->st;
+  DState *st = c->st;
+  a.dt = &st->dt;
+  a.tiempo = &st->tiempo;
+  a.timeinit = &st->timeinit;
+  a.timec = &st->timec;
+  a.utauout = &st->utauout;
+  a.rthout = &st->rthout;
+  a.dout = &st->dout;
+  a.gamma1 = &st->gamma1;
+  a.gamma2 = &st->gamma2;
+  a.err = &st->err;
+  a.tail = tail;
   const int ny = c->cfg.ny;
   const size_t smem = sizeof(double) * (4 * (size_t)(ny + 1)) + sizeof(int) * 2 * (ny + 1);
   cudaFuncSetAttribute(k_genflu, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -298,7 +298,7 @@ extern "C" int otbl_rhsp(otbl_ctx *c, int m, int setstep) {
   LAUNCH(c, launch_products(c, setstep));
   LAUNCH(c, launch_difvisx(c));
   LAUNCH(c, launch_dt(c, m, setstep));
-  LAUNCH(c, launch_genflu(c));
+  LAUNCH(c, launch_genflu(c, 1));
   LAUNCH(c, launch_final(c));
   return OTBL_OK;
 }
@@ -390,7 +390,7 @@ extern "C" int otbl_boun(otbl_ctx *c) {
 extern "C" int otbl_genflu(otbl_ctx *c) {
   if (!c) return OTBL_ERR_ARG;
   cudaSetDevice(c->device);
-  LAUNCH(c, launch_genflu(c));
+  LAUNCH(c, launch_genflu(c, 0));
   return OTBL_OK;
 }
 

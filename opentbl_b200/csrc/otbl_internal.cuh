@@ -111,7 +111,7 @@ cudaError_t launch_interpy(otbl_ctx *c);
 cudaError_t launch_products(otbl_ctx *c, int setstep);
 cudaError_t launch_difvisx(otbl_ctx *c);
 cudaError_t launch_dt(otbl_ctx *c, int m, int setstep);
-cudaError_t launch_genflu(otbl_ctx *c);
+cudaError_t launch_genflu(otbl_ctx *c, int tail);
 cudaError_t launch_final(otbl_ctx *c);
 cudaError_t launch_outflow(otbl_ctx *c);
 cudaError_t launch_pois(otbl_ctx *c, int m);

@@ -136,3 +136,32 @@ def test_c1_divergence_after_transient():
     dg = np.abs(divergence_np(cfg, coef, g.field("u"), g.field("v"), g.field("w"))).max()
     print("C1 after 3 steps: max|div| gpu", dg)
     assert dg <= 1e-12
+
+
+def test_genflu_standalone():
+    """otbl_genflu (genflu.F90:3-167) against the oracle on the same state:
+    plane xout recycled into plane 1, the filtered mean um and the integral
+    quantities u_tau, Re_theta, delta_99, gamma."""
+    from oracle import pyoracle
+    cfg = config.SMALL
+    g, o, init, coef = _pair(cfg)
+    u0 = np.ascontiguousarray(init["u0"])
+    v0 = np.ascontiguousarray(init["v0"])
+    um = np.ascontiguousarray(init["um"])
+    sg = native.OtblInflow()
+    so = pyoracle.OtblInflow()
+    for s in (sg, so):
+        s.dt, s.tiempo, s.timeinit = 0.05, 3.0, 0.0
+    g.L.otbl_set_inflow(g.h, native.dptr(u0), native.dptr(v0), native.dptr(um), ctypes.byref(sg))
+    o.L.orc_set_inflow(o.h, pyoracle.dptr(u0), pyoracle.dptr(v0), pyoracle.dptr(um), ctypes.byref(so))
+    for _ in range(2):
+        g.genflu()
+        o.L.orc_genflu(o.h)
+    for n in ("u", "v", "w"):
+        assert rel_l2(g.field(n)[0], o.field(n)[0]) <= 1e-13, n
+        assert np.array_equal(g.field(n)[1:], o.field(n)[1:]), n
+    um_g, gi = g.inflow()
+    um_o, oi = o.inflow()
+    assert rel_l2(um_g, um_o) <= 1e-15
+    for k in ("utauout", "rthout", "dout", "gamma1", "gamma2", "timec"):
+        assert abs(gi[k] - oi[k]) <= 1e-13 * max(1.0, abs(oi[k])), (k, gi[k], oi[k])
