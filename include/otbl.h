@@ -126,6 +126,40 @@ int otbl_cosftx(otbl_ctx *ctx, double *c_dev, int nlines, int iopt);
 int otbl_boun(otbl_ctx *ctx);                        /* boun.f90:7         */
 int otbl_genflu(otbl_ctx *ctx);                      /* genflu.F90:3       */
 
+/* ---- genflu without allocation (no counterpart in the reference, whose
+ *      genflu works on module arrays that exist for the whole run) ----
+ * genflu.F90:3 as otbl_genflu, on device buffers owned by the caller: u_dev,
+ * w_dev (nx, ny+1, nz1) and v_dev (nx, ny, nz1) in the plane layout (plane
+ * xout is read, plane 1 written), u0_dev (ny+1), v0_dev (ny), um_dev (ny+1,
+ * updated), scal_dev (OTBL_GF_COUNT doubles, slots below), err_dev (one int,
+ * may be NULL; set to OTBL_ERR_NAN when the rescaled grid cannot be
+ * profiled, never cleared: start it at 0). Only the context's coefficients
+ * and stream are used; the launch is ordered on that stream.
+ *
+ * It is for callers that cannot allocate device memory at call time, e.g. a
+ * host that keeps the fields in its own allocations and has given the rest
+ * of HBM to its own pool, or one whose time loop must not be stalled by the
+ * device-wide synchronisation of cudaMalloc/cudaFree. The profile scratch
+ * plane, nz1*(ny+2) doubles, is a static device array of
+ * OTBL_GENFLU_SCRATCH_MAX doubles in this library; larger grids are refused
+ * with OTBL_ERR_CONFIG. The first call on each device looks up the array's
+ * address (and may load the library's device module): make that call before
+ * any stream capture. The scratch need not start at zero. All calls on one
+ * device share the array: calls that can run at the same time (different
+ * streams, contexts or host threads without ordering) race. No device or
+ * host memory is allocated on the success path. */
+enum {
+  OTBL_GF_DT = 0, OTBL_GF_TIEMPO, OTBL_GF_TIMEINIT,           /* inputs  */
+  OTBL_GF_TIMEC, OTBL_GF_UTAUOUT, OTBL_GF_RTHOUT, OTBL_GF_DOUT,
+  OTBL_GF_GAMMA1, OTBL_GF_GAMMA2,                              /* outputs */
+  OTBL_GF_COUNT
+};
+#define OTBL_GENFLU_SCRATCH_MAX 131072 /* doubles (1 MiB) per device */
+int otbl_genflu_noalloc(otbl_ctx *ctx, double *u_dev, double *v_dev,
+                        double *w_dev, const double *u0_dev,
+                        const double *v0_dev, double *um_dev,
+                        double *scal_dev, int *err_dev);
+
 /* kernel launches issued by this context since creation */
 long long otbl_launch_count(const otbl_ctx *ctx);
 

@@ -24,6 +24,7 @@
 // REAL4 rounding of the transposed payload (OTBL_XPOSE_FP32) is applied at
 // exactly the loads/stores where the reference transposes.
 #include <cfloat>
+#include <mutex>
 
 #include "devcommon.cuh"
 #include "fft.cuh"
@@ -865,6 +866,75 @@ cudaError_t launch_genflu(otbl_ctx *c, int tail) {
   prof_begin(c, PK_GENFLU);
   k_genflu<<<1, 512, smem, c->stream>>>(c->dc, a);
   prof_end(c);
+  c->launches += 1;
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// genflu on caller-owned buffers, with its profile scratch plane in a static
+// device array instead of a context allocation. Callers that cannot allocate
+// device memory at call time use it: a host that owns the fields in its own
+// device allocations and has handed the rest of HBM to its own pool has no
+// room for a scratch buffer mid-run, and a cudaMalloc/cudaFree pair would
+// also synchronise the device inside its stream-ordered time loop.
+//
+// The array is part of this module's data, so it comes into existence when
+// the module is loaded on a device; the first call on each device looks its
+// address up (cudaGetSymbolAddress, which may load the module) and caches
+// it. Nothing in it needs to start at zero: k_genflu writes every row of the
+// plane that it reads earlier in the same launch. All calls on one device
+// share the one array, so two calls whose launches overlap (different
+// streams, contexts or host threads without ordering between them) race.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) double g_genflu_scratch[OTBL_GENFLU_SCRATCH_MAX];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mu;
+double *g_scratch_addr[kMaxDevices] = {};
+}  // namespace
+
+size_t genflu_smem_bytes(int ny) { return sizeof(double) * (4 * (size_t)(ny + 1)) + sizeof(int) * 2 * (ny + 1); }
+
+// The caller has made `device` current.
+cudaError_t genflu_scratch_addr(int device, double **p) {
+  if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(g_scratch_mu);
+  if (!g_scratch_addr[device]) {
+    void *q = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&q, g_genflu_scratch);
+    if (e != cudaSuccess) return e;
+    g_scratch_addr[device] = static_cast<double *>(q);
+  }
+  *p = g_scratch_addr[device];
+  return cudaSuccess;
+}
+
+cudaError_t launch_genflu_noalloc(otbl_ctx *c, double *wk, double *u, double *v, double *w, const double *u0,
+                                  const double *v0, double *um, double *scal, int *err) {
+  GenArgs a;
+  a.u = u;
+  a.v = v;
+  a.w = w;
+  a.rhsupa = a.rhsvpa = a.rhswpa = nullptr;  // only touched with tail = 1
+  a.u0 = u0;
+  a.v0 = v0;
+  a.um = um;
+  a.wk = wk;
+  a.dt = scal + OTBL_GF_DT;
+  a.tiempo = scal + OTBL_GF_TIEMPO;
+  a.timeinit = scal + OTBL_GF_TIMEINIT;
+  a.timec = scal + OTBL_GF_TIMEC;
+  a.utauout = scal + OTBL_GF_UTAUOUT;
+  a.rthout = scal + OTBL_GF_RTHOUT;
+  a.dout = scal + OTBL_GF_DOUT;
+  a.gamma1 = scal + OTBL_GF_GAMMA1;
+  a.gamma2 = scal + OTBL_GF_GAMMA2;
+  a.err = err;
+  a.tail = 0;
+  // the entry point has checked this against the default 48 KB limit
+  const size_t smem = genflu_smem_bytes(c->cfg.ny);
+  k_genflu<<<1, 512, smem, c->stream>>>(c->dc, a);
   c->launches += 1;
   return cudaGetLastError();
 }

@@ -394,6 +394,27 @@ extern "C" int otbl_genflu(otbl_ctx *c) {
   return OTBL_OK;
 }
 
+// The success path allocates nothing: the scratch plane is the static array
+// of kernels.cu, found once per device (only an error path stores a message
+// string in the context).
+extern "C" int otbl_genflu_noalloc(otbl_ctx *c, double *u, double *v, double *w, const double *u0, const double *v0,
+                                   double *um, double *scal, int *err) {
+  if (!c) return OTBL_ERR_ARG;
+  if (!u || !v || !w || !u0 || !v0 || !um || !scal)
+    return fail(c, OTBL_ERR_ARG, "otbl_genflu_noalloc: null device pointer");
+  const size_t need = (size_t)c->dc.nz1 * (size_t)(c->cfg.ny + 2);
+  if (need > (size_t)OTBL_GENFLU_SCRATCH_MAX)
+    return fail(c, OTBL_ERR_CONFIG,
+                "otbl_genflu_noalloc: the profile plane nz1*(ny+2) exceeds OTBL_GENFLU_SCRATCH_MAX doubles");
+  if (genflu_smem_bytes(c->cfg.ny) > 48 * 1024)
+    return fail(c, OTBL_ERR_CONFIG, "otbl_genflu_noalloc: ny too large for 48 KB of shared memory");
+  OTBL_CUDA_TRY(c, cudaSetDevice(c->device));
+  double *wk = nullptr;
+  OTBL_CUDA_TRY(c, genflu_scratch_addr(c->device, &wk));
+  LAUNCH(c, launch_genflu_noalloc(c, wk, u, v, w, u0, v0, um, scal, err));
+  return OTBL_OK;
+}
+
 extern "C" int otbl_get_stream(otbl_ctx *c, void **stream) {
   if (!c || !stream) return OTBL_ERR_ARG;
   *stream = (void *)c->stream;

@@ -125,4 +125,9 @@ cudaError_t launch_pois_solve(otbl_ctx *c, double *phi);
 cudaError_t launch_chp2x(otbl_ctx *c, const double *plan, double *pen, int jee, int to_pen);
 cudaError_t launch_fourxz(otbl_ctx *c, double *fou, double *phys, int iopt, int nlines);
 cudaError_t launch_cosftx(otbl_ctx *c, double *cpen, int nlines, int iopt);
+// genflu on caller-owned buffers with the static scratch plane (no allocation)
+size_t genflu_smem_bytes(int ny);
+cudaError_t genflu_scratch_addr(int device, double **p);
+cudaError_t launch_genflu_noalloc(otbl_ctx *c, double *wk, double *u, double *v, double *w, const double *u0,
+                                  const double *v0, double *um, double *scal, int *err);
 }  // namespace otbl
