@@ -30,7 +30,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 from opentbl_b200 import config as cfgmod  # noqa: E402
-from opentbl_b200 import native, synth  # noqa: E402
+from opentbl_b200 import native, replicas, synth  # noqa: E402
 from opentbl_b200.box import Box  # noqa: E402
 
 WORKLOAD = "C2"
@@ -138,36 +138,6 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def dist_setup():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if ws > 1:
-        import torch
-        import torch.distributed as dist
-        from datetime import timedelta
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
-    return ws, rank, local
-
-
-def dist_max(x: float, ws: int) -> float:
-    if ws == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
-
-
-def dist_barrier(ws: int):
-    if ws > 1:
-        import torch.distributed as dist
-        dist.barrier()
-
-
 def build_box(cfg, device):
     init = synth.make_initial(cfg)
     coef = native.coef_compute(cfg, init["re"], init["xout"], init["y"], init["u0"])
@@ -232,9 +202,11 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
     cfg = getattr(cfgmod, args.config)
-    ws, rank, local = dist_setup()
+    R = replicas.setup()
+    ws, rank, local = R.world_size, R.rank, R.local_rank
     if args.impl == "reference":
         run_reference(args, cfg, ws, rank)
+        replicas.teardown(R)
         return
 
     import torch
@@ -250,7 +222,7 @@ def main():
     # ---- device-timed region: K RK3 steps, CUDA events on the box's stream ----
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
-    dist_barrier(ws)
+    replicas.barrier(R)
     torch.cuda.synchronize()
     box.sync()
     l0 = box.launches
@@ -262,12 +234,12 @@ def main():
         ev1.synchronize()
     box.sync()
     torch.cuda.synchronize()
-    dist_barrier(ws)
+    replicas.barrier(R)
     launches = box.launches - l0
     ms = ev0.elapsed_time(ev1)
-    ms = dist_max(ms, ws)
+    ms = replicas.max_over_ranks(ms, R)
     sub = 3 * K
-    value = ws * cfg.mpts * sub / (ms / 1e3)
+    value = replicas.aggregate_rate(cfg.mpts * sub, ms / 1e3, R)
     clocks = clk.summary()
 
     # ---- per-kernel timing pass (not part of `value`) ----
@@ -309,7 +281,7 @@ def main():
         out_names = ("u", "v", "w", "p")
         out_bytes = sum(pinned[n].numel() * 8 for n in out_names)
         box.sync()
-        dist_barrier(ws)
+        replicas.barrier(R)
         t0 = time.perf_counter()
         for i, n in enumerate(names):   # restart: state from host (getstartzy)
             L.otbl_set_field(box.h, i, ctypes.cast(pinned[n].data_ptr(), D))
@@ -320,9 +292,9 @@ def main():
         for n in out_names:             # checkpoint: u, v, w, p to host (escribezy)
             L.otbl_get_field(box.h, names.index(n), ctypes.cast(pinned[n].data_ptr(), D))
         el = time.perf_counter() - t0
-        el = dist_max(el, ws)
+        el = replicas.max_over_ranks(el, R)
         diag_bytes = 8 * (cfg.ny + 1) + 8 * 12
-        e2e = {"value": ws * cfg.mpts * sub / el, "unit": UNIT,
+        e2e = {"value": replicas.aggregate_rate(cfg.mpts * sub, el, R), "unit": UNIT,
                "h2d_bytes_per_step": state_bytes / K,
                "d2h_bytes_per_step": diag_bytes + out_bytes / K,
                "job": f"restart upload of the 7 state fields, {K} RK3 steps with per-step "
@@ -352,9 +324,7 @@ def main():
                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks}
         print(json.dumps(out), flush=True)
     box.close()
-    if ws > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    replicas.teardown(R)
 
 
 if __name__ == "__main__":

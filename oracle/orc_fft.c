@@ -118,7 +118,8 @@ void orc_fft_exec(const orc_fft *P, const double *in, double *out, int sign) {
 /* --- fourxz line transforms (ffts.f90:27-67) ---
  * c2r: fou[0..2*nz2+1] (complex modes 0..nz2) -> phys[0..nz-1]
  * r2c: phys[0..nz-1] -> fou (modes 0..nz2) x 1/nz
- * h is the complex FFT of length nz/2; work has room for nz+2 complex. */
+ * h is the complex FFT of length nz/2; work has room for 3*(nz/2)+1
+ * complex (c2r) or nz complex (r2c). */
 void orc_c2r_line(const orc_fft *h, int nz, int nz2, const double *fou,
                   double *phys, double *work) {
   const int M = nz / 2;
