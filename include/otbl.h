@@ -134,19 +134,20 @@ int otbl_genflu(otbl_ctx *ctx);                      /* genflu.F90:3       */
  * updated), scal_dev (OTBL_GF_COUNT doubles, slots below), err_dev (one int,
  * may be NULL; set to OTBL_ERR_NAN when the rescaled grid cannot be
  * profiled, never cleared: start it at 0). Only the context's coefficients
- * and stream are used; the launch is ordered on that stream.
+ * and stream are used; the launches are ordered on that stream.
  *
  * It is for callers that cannot allocate device memory at call time, e.g. a
  * host that keeps the fields in its own allocations and has given the rest
  * of HBM to its own pool, or one whose time loop must not be stalled by the
- * device-wide synchronisation of cudaMalloc/cudaFree. The profile scratch
- * plane, nz1*(ny+2) doubles, is a static device array of
- * OTBL_GENFLU_SCRATCH_MAX doubles in this library; larger grids are refused
- * with OTBL_ERR_CONFIG. The first call on each device looks up the array's
- * address (and may load the library's device module): make that call before
- * any stream capture. The scratch need not start at zero. All calls on one
- * device share the array: calls that can run at the same time (different
- * streams, contexts or host threads without ordering) race. No device or
+ * device-wide synchronisation of cudaMalloc/cudaFree. The scratch that
+ * carries genflu's rescaling tables from one launch to the next,
+ * 3*(ny+1)+2 doubles, is a static device array of OTBL_GENFLU_SCRATCH_MAX
+ * doubles in this library; larger grids are refused with OTBL_ERR_CONFIG.
+ * The first call on each device looks up the array's address (and may load
+ * the library's device module): make that call before any stream capture.
+ * The scratch need not start at zero. All calls on one device share the
+ * array: calls that can run at the same time (different streams, contexts or
+ * host threads without ordering) race. No device or
  * host memory is allocated on the success path. */
 enum {
   OTBL_GF_DT = 0, OTBL_GF_TIEMPO, OTBL_GF_TIMEINIT,           /* inputs  */
@@ -154,7 +155,7 @@ enum {
   OTBL_GF_GAMMA1, OTBL_GF_GAMMA2,                              /* outputs */
   OTBL_GF_COUNT
 };
-#define OTBL_GENFLU_SCRATCH_MAX 131072 /* doubles (1 MiB) per device */
+#define OTBL_GENFLU_SCRATCH_MAX 2048 /* doubles (16 KiB) per device: ny <= 680 */
 int otbl_genflu_noalloc(otbl_ctx *ctx, double *u_dev, double *v_dev,
                         double *w_dev, const double *u0_dev,
                         const double *v0_dev, double *um_dev,

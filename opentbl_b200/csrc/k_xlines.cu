@@ -47,8 +47,9 @@ __device__ __forceinline__ void xtile_store(const double *sm, double *__restrict
 }
 
 // interpxx, lip.f90:248-300. which 0: u (inxu, cofiux, chi=2, chi2=3);
-// which 1: v,w (inxv, cofivx, chi=1, chi2=4).
-__global__ void __launch_bounds__(XT_INTERP * 32) k_interpx(DCoef c, const double *__restrict__ in,
+// which 1: v,w (inxv, cofivx, chi=1, chi2=4). Coefficients of the stencil
+// and the solve come chunk-interleaved (XSet).
+__global__ void __launch_bounds__(XT_INTERP * 32) k_interpx(DCoef c, XSet xs, const double *__restrict__ in,
                                                             double *__restrict__ out, int which, int np, int Lp) {
   extern __shared__ double sm[];
   const int nx = c.nx, xr = c.xround;
@@ -57,10 +58,9 @@ __global__ void __launch_bounds__(XT_INTERP * 32) k_interpx(DCoef c, const doubl
   xtile_wait<XT_INTERP>(sm, 1, nx, Lp, xr);
   const int h = threadIdx.x & 31;
   double *x = sm + (threadIdx.x >> 5) * Lp;
-  const double *icon = which == 0 ? c.inxu : c.inxv;
-  const double *econ = which == 0 ? c.cofiux : c.cofivx;
   const int chi = which == 0 ? 2 : 1, chi2 = which == 0 ? 3 : 4;
   const double *ib = c.inbx;
+  const CCo<32> E1(xs.k[XI_E1], h, xs.CL), E2(xs.k[XI_E2], h, xs.CL);
   int s, e;
   chunk_range<32, false>(nx, h, s, e);
   const double gnext = e < nx ? x[e] : 0.0;
@@ -77,9 +77,9 @@ __global__ void __launch_bounds__(XT_INTERP * 32) k_interpx(DCoef c, const doubl
     for (int b = 0; b <= LB; ++b) gv[b] = r0 + b < e ? x[r0 + b] : gnext;
 #pragma unroll
     for (int b = 0; b < LB; ++b) {
-      const int i = min(max(r0 + b + 1, 2), nx - 1);
-      e1[b] = A2(econ, 1, i);
-      e2[b] = A2(econ, 2, i);
+      const bool ok = r0 + b < e;
+      e1[b] = ok ? E1(r0 + b) : 0.0;
+      e2[b] = ok ? E2(r0 + b) : 0.0;
     }
 #pragma unroll
     for (int b = 0; b < LB; ++b) {
@@ -89,14 +89,15 @@ __global__ void __launch_bounds__(XT_INTERP * 32) k_interpx(DCoef c, const doubl
     }
   }
   __syncwarp();
-  solve_icon<32, false>(x, nx, h, Icon{icon, 0});
+  solve_cco<32, false>(x, nx, h, CCo<32>(xs.k[XI_L], h, xs.CL), CCo<32>(xs.k[XI_D], h, xs.CL),
+                       CCo<32>(xs.k[XI_U], h, xs.CL));
   __syncthreads();
   xtile_store<XT_INTERP>(sm, out, nx, np, mp0, Lp, xr);
 }
 
 // difvisxx, lip.f90:52-142: Pade d/dx(gin) + rex * Pade d2/dx2(upin), with
 // the outflow rows of lip.f90:105,132. which 0: u; which 1: v,w.
-__global__ void __launch_bounds__(XT_DIFVIS * 32) k_difvisx(DCoef c, const double *__restrict__ gin,
+__global__ void __launch_bounds__(XT_DIFVIS * 32) k_difvisx(DCoef c, XSet xs, const double *__restrict__ gin,
                                                             const double *__restrict__ upin,
                                                             double *__restrict__ out, int which, int np, int Lp) {
   extern __shared__ double sm[];
@@ -108,10 +109,9 @@ __global__ void __launch_bounds__(XT_DIFVIS * 32) k_difvisx(DCoef c, const doubl
   xtile_wait<XT_DIFVIS>(sm, 2, nx, Lp, xr);
   const int h = threadIdx.x & 31, wv = threadIdx.x >> 5;
   double *x = smg + wv * Lp, *u = smu + wv * Lp;
-  const double *icon = which == 0 ? c.dcxu : c.dcxv;
-  const double *iconv = which == 0 ? c.vixu : c.vixv;
-  const double *econ = which == 0 ? c.cofcxu : c.cofcxv;
-  const double *econv = which == 0 ? c.cofvxu : c.cofvxv;
+  const int CL = xs.CL;
+  const CCo<32> E1(xs.k[XD_E1], h, CL), E2(xs.k[XD_E2], h, CL);
+  const CCo<32> F1(xs.k[XV_F1], h, CL), F2(xs.k[XV_F2], h, CL), F3(xs.k[XV_F3], h, CL);
   const int chv = which == 0 ? 1 : 2, chv1 = chv + 2, ic = which == 0 ? 3 : 1;
   const double *db = c.dcbx, *vb = c.cofvbx;
   const double rex = c.S[OTBL_S_REX], idx = c.S[OTBL_S_IDX], uinf = c.S[OTBL_S_UINF];
@@ -143,9 +143,9 @@ __global__ void __launch_bounds__(XT_DIFVIS * 32) k_difvisx(DCoef c, const doubl
     for (int b = 0; b <= LB; ++b) gv[b] = r1 - b >= s ? x[r1 - b] : gprev;
 #pragma unroll
     for (int b = 0; b < LB; ++b) {
-      const int i = min(max(r1 - b + 1, 2), nx - 1);
-      e1[b] = A2(econ, 1, i);
-      e2[b] = A2(econ, 2, i);
+      const bool ok = r1 - b >= s;
+      e1[b] = ok ? E1(r1 - b) : 0.0;
+      e2[b] = ok ? E2(r1 - b) : 0.0;
     }
 #pragma unroll
     for (int b = 0; b < LB; ++b) {
@@ -162,10 +162,10 @@ __global__ void __launch_bounds__(XT_DIFVIS * 32) k_difvisx(DCoef c, const doubl
     for (int b = 0; b <= LB; ++b) uv[b + 1] = r0 + b < e ? u[r0 + b] : unext;
 #pragma unroll
     for (int b = 0; b < LB; ++b) {
-      const int i = min(max(r0 + b + 1, 2), nx - 1);
-      f1[b] = A3(econv, 1, i);
-      f2[b] = A3(econv, 2, i);
-      f3[b] = A3(econv, 3, i);
+      const bool ok = r0 + b < e;
+      f1[b] = ok ? F1(r0 + b) : 0.0;
+      f2[b] = ok ? F2(r0 + b) : 0.0;
+      f3[b] = ok ? F3(r0 + b) : 0.0;
     }
 #pragma unroll
     for (int b = 0; b < LB; ++b) {
@@ -176,8 +176,10 @@ __global__ void __launch_bounds__(XT_DIFVIS * 32) k_difvisx(DCoef c, const doubl
     uprev = uv[LB];  // original value of the last row of this batch
   }
   __syncwarp();
-  solve_icon<32, false>(x, nx, h, Icon{icon, 0});
-  solve_icon<32, false>(u, nx, h, Icon{iconv, 0});
+  solve_cco<32, false>(x, nx, h, CCo<32>(xs.k[XD_L], h, CL), CCo<32>(xs.k[XD_D], h, CL),
+                       CCo<32>(xs.k[XD_U], h, CL));
+  solve_cco<32, false>(u, nx, h, CCo<32>(xs.k[XV_L], h, CL), CCo<32>(xs.k[XV_D], h, CL),
+                       CCo<32>(xs.k[XV_U], h, CL));
   for (int r = s; r < e; ++r) x[r] = r == nx - 1 ? uinf * (uN - uN1) * idx + rex * 0.0 : x[r] + rex * u[r];
   __syncthreads();
   xtile_store<XT_DIFVIS>(smg, out, nx, np, mp0, Lp, xr);
@@ -190,12 +192,12 @@ cudaError_t launch_interpx(otbl_ctx *c) {
   const size_t smem = sizeof(double) * XT_INTERP * Lp;
   cudaFuncSetAttribute(k_interpx, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   prof_begin(c, PK_INTERPX);
-  k_interpx<<<(npu + XT_INTERP - 1) / XT_INTERP, XT_INTERP * 32, smem, c->stream>>>(c->dc, c->f[OTBL_F_U], c->w.ux,
-                                                                                   0, npu, Lp);
-  k_interpx<<<(npv + XT_INTERP - 1) / XT_INTERP, XT_INTERP * 32, smem, c->stream>>>(c->dc, c->f[OTBL_F_V], c->w.vx,
-                                                                                   1, npv, Lp);
-  k_interpx<<<(npu + XT_INTERP - 1) / XT_INTERP, XT_INTERP * 32, smem, c->stream>>>(c->dc, c->f[OTBL_F_W], c->w.wx,
-                                                                                   1, npu, Lp);
+  k_interpx<<<(npu + XT_INTERP - 1) / XT_INTERP, XT_INTERP * 32, smem, c->stream>>>(c->dc, xset(c->xco, 0),
+                                                                                   c->f[OTBL_F_U], c->w.ux, 0, npu, Lp);
+  k_interpx<<<(npv + XT_INTERP - 1) / XT_INTERP, XT_INTERP * 32, smem, c->stream>>>(c->dc, xset(c->xco, 1),
+                                                                                   c->f[OTBL_F_V], c->w.vx, 1, npv, Lp);
+  k_interpx<<<(npu + XT_INTERP - 1) / XT_INTERP, XT_INTERP * 32, smem, c->stream>>>(c->dc, xset(c->xco, 1),
+                                                                                   c->f[OTBL_F_W], c->w.wx, 1, npu, Lp);
   prof_end(c);
   c->launches += 3;
   return cudaGetLastError();
@@ -209,11 +211,11 @@ cudaError_t launch_difvisx(otbl_ctx *c) {
   cudaFuncSetAttribute(k_difvisx, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const int T = XT_DIFVIS * 32;
   prof_begin(c, PK_DIFVISX);
-  k_difvisx<<<(npu + XT_DIFVIS - 1) / XT_DIFVIS, T, smem, c->stream>>>(c->dc, c->w.uu, c->f[OTBL_F_U], c->w.cu, 0,
+  k_difvisx<<<(npu + XT_DIFVIS - 1) / XT_DIFVIS, T, smem, c->stream>>>(c->dc, xset(c->xco, 0), c->w.uu, c->f[OTBL_F_U], c->w.cu, 0,
                                                                       npu, Lp);
-  k_difvisx<<<(npv + XT_DIFVIS - 1) / XT_DIFVIS, T, smem, c->stream>>>(c->dc, c->w.uv, c->f[OTBL_F_V], c->w.cv, 1,
+  k_difvisx<<<(npv + XT_DIFVIS - 1) / XT_DIFVIS, T, smem, c->stream>>>(c->dc, xset(c->xco, 1), c->w.uv, c->f[OTBL_F_V], c->w.cv, 1,
                                                                       npv, Lp);
-  k_difvisx<<<(npu + XT_DIFVIS - 1) / XT_DIFVIS, T, smem, c->stream>>>(c->dc, c->w.uw, c->f[OTBL_F_W], c->w.cw, 1,
+  k_difvisx<<<(npu + XT_DIFVIS - 1) / XT_DIFVIS, T, smem, c->stream>>>(c->dc, xset(c->xco, 1), c->w.uw, c->f[OTBL_F_W], c->w.cw, 1,
                                                                       npu, Lp);
   prof_end(c);
   c->launches += 3;

@@ -55,9 +55,10 @@ __device__ __forceinline__ void ytile_load(double *t, const double *__restrict__
 
 // differzy (lip.f90:152-232): which 0 u-type (out rows 0..ny, reads 0..ny-1),
 // which 1 v-type (rows 0..ny-1). Then the solve with dcyu/dcyv.
-__device__ __forceinline__ void y_differzy(const DCoef &c, double *x, int h, int which) {
+__device__ __forceinline__ void y_differzy(const DCoef &c, const YSet &ys, double *x, int h, int which) {
   const int ny = c.ny, jee = which == 0 ? ny + 1 : ny;
-  const double *econ = which == 0 ? c.cofcyu : c.cofcyv;
+  const int CL = chunk_len(jee, YNCH, true);
+  const CCo<YNCH> E1(ys.k[YD_E1], h, CL), E2(ys.k[YD_E2], h, CL);
   const double *db = c.dcby;
   const int chv = which == 0 ? 3 : 1, cha = chv + 1;
   int s, e;
@@ -77,9 +78,9 @@ __device__ __forceinline__ void y_differzy(const DCoef &c, double *x, int h, int
       for (int b = 0; b <= LB; ++b) gv[b] = r1 - b >= s ? x[r1 - b] : gprev;
 #pragma unroll
       for (int b = 0; b < LB; ++b) {
-        const int j = min(max(r1 - b + 1, 2), ny);
-        e1[b] = A2(econ, 1, j);
-        e2[b] = A2(econ, 2, j);
+        const bool ok = r1 - b >= s;
+        e1[b] = ok ? E1(r1 - b) : 0.0;
+        e2[b] = ok ? E2(r1 - b) : 0.0;
       }
 #pragma unroll
       for (int b = 0; b < LB; ++b) {
@@ -97,9 +98,9 @@ __device__ __forceinline__ void y_differzy(const DCoef &c, double *x, int h, int
       for (int b = 0; b <= LB; ++b) gv[b] = r0 + b < e ? x[r0 + b] : gnext;
 #pragma unroll
       for (int b = 0; b < LB; ++b) {
-        const int j = min(max(r0 + b + 1, 2), ny);
-        e1[b] = A2(econ, 1, j);
-        e2[b] = A2(econ, 2, j);
+        const bool ok = r0 + b < e;
+        e1[b] = ok ? E1(r0 + b) : 0.0;
+        e2[b] = ok ? E2(r0 + b) : 0.0;
       }
 #pragma unroll
       for (int b = 0; b < LB; ++b) {
@@ -110,13 +111,15 @@ __device__ __forceinline__ void y_differzy(const DCoef &c, double *x, int h, int
     }
   }
   __syncwarp();
-  solve_icon<YNCH, true>(x, jee, h, Icon{which == 0 ? c.dcyu : c.dcyv, 0});
+  solve_cco<YNCH, true>(x, jee, h, CCo<YNCH>(ys.k[YD_L], h, CL), CCo<YNCH>(ys.k[YD_D], h, CL),
+                        CCo<YNCH>(ys.k[YD_U], h, CL));
 }
 
 // vistyy (lip.f90:447-513): which 0 u,w (jee = ny+1, ic = 3), which 1 v.
-__device__ __forceinline__ void y_vistyy(const DCoef &c, double *x, int h, int which) {
+__device__ __forceinline__ void y_vistyy(const DCoef &c, const YSet &ys, double *x, int h, int which) {
   const int ny = c.ny, jee = which == 0 ? ny + 1 : ny, ic = which == 0 ? 3 : 1;
-  const double *econ = which == 0 ? c.cofvyu : c.cofvyv;
+  const int CL = chunk_len(jee, YNCH, true);
+  const CCo<YNCH> F1(ys.k[YV_F1], h, CL), F2(ys.k[YV_F2], h, CL), F3(ys.k[YV_F3], h, CL);
   const double *vb = c.cofvby;
   int s, e;
   chunk_range<YNCH, true>(jee, h, s, e);
@@ -135,10 +138,10 @@ __device__ __forceinline__ void y_vistyy(const DCoef &c, double *x, int h, int w
     for (int b = 0; b <= LB; ++b) uv[b + 1] = r0 + b < e ? x[r0 + b] : unext;
 #pragma unroll
     for (int b = 0; b < LB; ++b) {
-      const int j = min(max(r0 + b + 1, 2), jee - 1);
-      f1[b] = A3(econ, 1, j);
-      f2[b] = A3(econ, 2, j);
-      f3[b] = A3(econ, 3, j);
+      const bool ok = r0 + b < e;
+      f1[b] = ok ? F1(r0 + b) : 0.0;
+      f2[b] = ok ? F2(r0 + b) : 0.0;
+      f3[b] = ok ? F3(r0 + b) : 0.0;
     }
 #pragma unroll
     for (int b = 0; b < LB; ++b) {
@@ -149,17 +152,20 @@ __device__ __forceinline__ void y_vistyy(const DCoef &c, double *x, int h, int w
     uprev = uv[LB];
   }
   __syncwarp();
-  solve_icon<YNCH, true>(x, jee, h, Icon{which == 0 ? c.viyu : c.viyv, 0});
+  solve_cco<YNCH, true>(x, jee, h, CCo<YNCH>(ys.k[YV_L], h, CL), CCo<YNCH>(ys.k[YV_D], h, CL),
+                        CCo<YNCH>(ys.k[YV_U], h, CL));
 }
 
 // implzy (lip.f90:528-597): right-hand side A*res for rows 2..jee-1 from the
 // column `res` (rows 0..jee-1) into `out` rows 0..jee-3, boundary values
 // ub1 / ubj moved to the right-hand side, then the pre-factored solve of
-// (A + var1*B) (factors from k_dt, fac[3j..3j+2] for row j).
-__device__ __forceinline__ void y_implzy(const DCoef &c, const double *res, double *out, int h, int which,
-                                         double ub1, double ubj, const double *__restrict__ fac) {
+// (A + var1*B) (factors from k_dt, interleaved YM_L/YM_D/YM_U; fac holds the
+// boundary couplings a1raw, a3raw).
+__device__ __forceinline__ void y_implzy(const DCoef &c, const YSet &ys, const double *res, double *out, int h,
+                                         int which, double ub1, double ubj, const double *__restrict__ fac) {
   const int ny = c.ny, jee = which == 0 ? ny + 1 : ny, n = jee - 2;
-  const double *icon = which == 0 ? c.vyui : c.vyvi;
+  const int CL = chunk_len(n, YNCH, true);
+  const CCo<YNCH> F1(ys.k[YM_F1], h, CL), F2(ys.k[YM_F2], h, CL), F3(ys.k[YM_F3], h, CL);
   const double a1raw = fac[3 * (jee + 1)], a3raw = fac[3 * (jee + 1) + 1];
   int s, e;
   chunk_range<YNCH, true>(n, h, s, e);
@@ -169,10 +175,10 @@ __device__ __forceinline__ void y_implzy(const DCoef &c, const double *res, doub
     for (int b = 0; b < LB + 2; ++b) rv[b] = q0 + b < e + 2 ? res[q0 + b] : 0.0;
 #pragma unroll
     for (int b = 0; b < LB; ++b) {
-      const int j = min(q0 + b + 2, jee - 1);
-      f1[b] = A3(icon, 1, j);
-      f2[b] = A3(icon, 2, j);
-      f3[b] = A3(icon, 3, j);
+      const bool ok = q0 + b < e;
+      f1[b] = ok ? F1(q0 + b) : 0.0;
+      f2[b] = ok ? F2(q0 + b) : 0.0;
+      f3[b] = ok ? F3(q0 + b) : 0.0;
     }
 #pragma unroll
     for (int b = 0; b < LB; ++b) {
@@ -186,13 +192,14 @@ __device__ __forceinline__ void y_implzy(const DCoef &c, const double *res, doub
     }
   }
   __syncwarp();
-  solve_icon<YNCH, true>(out, n, h, Icon{fac, 2});
+  solve_cco<YNCH, true>(out, n, h, CCo<YNCH>(ys.k[YM_L], h, CL), CCo<YNCH>(ys.k[YM_D], h, CL),
+                        CCo<YNCH>(ys.k[YM_U], h, CL));
 }
 
 // interpyy (lip.f90:359-440) in Fourier space: which 0 u,w (in rows ny+1),
 // which 1 v (in rows ny); out rows 1..ny.
-__global__ void __launch_bounds__(YTHREADS) k_interpy(DCoef c, const double *__restrict__ in, double *__restrict__ out,
-                                                      int which, int Lp) {
+__global__ void __launch_bounds__(YTHREADS) k_interpy(DCoef c, YSet ys, const double *__restrict__ in,
+                                                      double *__restrict__ out, int which, int Lp) {
   extern __shared__ double sm[];
   const int ny = c.ny, nz1 = c.nz1, jin = which == 0 ? ny + 1 : ny;
   const int i = blockIdx.y + 1, kr0 = blockIdx.x * YT;
@@ -201,7 +208,8 @@ __global__ void __launch_bounds__(YTHREADS) k_interpy(DCoef c, const double *__r
   __syncthreads();
   const YIdx q = yidx(nz1);
   double *x = sm + q.col * Lp;
-  const double *econ = which == 0 ? c.cofiuy : c.cofivy;
+  const int CL = chunk_len(ny, YNCH, true);
+  const CCo<YNCH> E1(ys.k[YI_E1], q.h, CL), E2(ys.k[YI_E2], q.h, CL);
   const double *ib = c.inby;
   int s, e;
   chunk_range<YNCH, true>(ny, q.h, s, e);
@@ -217,9 +225,9 @@ __global__ void __launch_bounds__(YTHREADS) k_interpy(DCoef c, const double *__r
       for (int b = 0; b <= LB; ++b) gv[b] = r0 + b < e ? x[r0 + b] : gnext;
 #pragma unroll
       for (int b = 0; b < LB; ++b) {
-        const int j = min(max(r0 + b + 1, 2), ny - 1);
-        e1[b] = A2(econ, 1, j);
-        e2[b] = A2(econ, 2, j);
+        const bool ok = r0 + b < e;
+        e1[b] = ok ? E1(r0 + b) : 0.0;
+        e2[b] = ok ? E2(r0 + b) : 0.0;
       }
 #pragma unroll
       for (int b = 0; b < LB; ++b) {
@@ -241,9 +249,9 @@ __global__ void __launch_bounds__(YTHREADS) k_interpy(DCoef c, const double *__r
       for (int b = 0; b <= LB; ++b) gv[b] = r1 - b >= s ? x[r1 - b] : gprev;
 #pragma unroll
       for (int b = 0; b < LB; ++b) {
-        const int j = min(max(r1 - b + 1, 2), ny - 1);
-        e1[b] = A2(econ, 1, j);
-        e2[b] = A2(econ, 2, j);
+        const bool ok = r1 - b >= s;
+        e1[b] = ok ? E1(r1 - b) : 0.0;
+        e2[b] = ok ? E2(r1 - b) : 0.0;
       }
 #pragma unroll
       for (int b = 0; b < LB; ++b) {
@@ -254,7 +262,8 @@ __global__ void __launch_bounds__(YTHREADS) k_interpy(DCoef c, const double *__r
     }
   }
   __syncwarp();
-  solve_icon<YNCH, true>(x, ny, q.h, Icon{which == 0 ? c.inyu : c.inyv, 0});
+  solve_cco<YNCH, true>(x, ny, q.h, CCo<YNCH>(ys.k[YI_L], q.h, CL), CCo<YNCH>(ys.k[YI_D], q.h, CL),
+                        CCo<YNCH>(ys.k[YI_U], q.h, CL));
   __syncthreads();
   double *o = out + (size_t)(i - 1) * ny * nz1;
   for (int t = threadIdx.x; t < ny * YT; t += YTHREADS) {
@@ -279,7 +288,7 @@ struct FinalArgs {
 };
 
 template <int COMP>  // 0: u, 1: v, 2: w
-__global__ void __launch_bounds__(YTHREADS) k_final(DCoef c, FinalArgs a, int Lp) {
+__global__ void __launch_bounds__(YTHREADS) k_final(DCoef c, YSet ys, FinalArgs a, int Lp) {
   extern __shared__ double sm[];
   __shared__ double ub1s[YT], ubts[YT];
   const int nx = c.nx, ny = c.ny, nz1 = c.nz1;
@@ -316,7 +325,8 @@ __global__ void __launch_bounds__(YTHREADS) k_final(DCoef c, FinalArgs a, int Lp
   int s, e;
   chunk_range<YNCH, true>(jee, q.h, s, e);
   // ---- RHS into tile 1 (rhsp.F90:164-169, 181-204, 351-418, 423-445)
-  if (!last) y_differzy(c, x1, q.h, COMP == 1 ? 1 : 0);
+  if (!last) y_differzy(c, ys, x1, q.h, COMP == 1 ? 1 : 0);
+  const CCo<YNCH> IDYY(ys.k[Y_IDYY], q.h, chunk_len(ny, YNCH, true));
   for (int r0 = s; r0 < e; r0 += YB) {
     double cxv[YB], kpv[YB];
 #pragma unroll
@@ -367,7 +377,7 @@ __global__ void __launch_bounds__(YTHREADS) k_final(DCoef c, FinalArgs a, int Lp
       if (last) return o;
       return o - var1 * idxx * (__ldg(pc + PV + (size_t)r * nz1) - __ldg(pc + (size_t)r * nz1));
     } else if (COMP == 1) {
-      return o - var1 * c.idyy[r] * (__ldg(pc + (size_t)(r + 1) * nz1) - __ldg(pc + (size_t)r * nz1));
+      return o - var1 * IDYY(r) * (__ldg(pc + (size_t)(r + 1) * nz1) - __ldg(pc + (size_t)r * nz1));
     } else {
       const double pp = __ldg(pc + (size_t)r * nz1 + (q.valid ? q.pof : 1));
       const double av = var1 * kz;
@@ -393,7 +403,7 @@ __global__ void __launch_bounds__(YTHREADS) k_final(DCoef c, FinalArgs a, int Lp
   // its final store.
   __syncthreads();
   // ---- explicit y-viscous term of the old velocity into tile 2
-  y_vistyy(c, x2, q.h, COMP == 1 ? 1 : 0);
+  y_vistyy(c, ys, x2, q.h, COMP == 1 ? 1 : 0);
   // ---- RK3 combination into tile 2 and the new RHS history (rhsp.F90:448-475)
   const double ub1 = ub1s[q.col], ubt = ubts[q.col];
   for (int r0 = s; r0 < e; r0 += YB) {
@@ -416,7 +426,7 @@ __global__ void __launch_bounds__(YTHREADS) k_final(DCoef c, FinalArgs a, int Lp
   }
   __syncwarp();
   // ---- implicit y-viscous step (rhsp.F90:479-484) into tile 1 rows 0..jee-3
-  y_implzy(c, x2, x1, q.h, COMP == 1 ? 1 : 0, ub1, ubt, COMP == 1 ? a.fac_v : a.fac_u);
+  y_implzy(c, ys, x2, x1, q.h, COMP == 1 ? 1 : 0, ub1, ubt, COMP == 1 ? a.fac_v : a.fac_u);
   __syncthreads();
   for (int t = threadIdx.x; t < jee * YT; t += YTHREADS) {
     const int j0 = t / YT, col = t - j0 * YT, kr = kr0 + col;
@@ -455,8 +465,8 @@ __global__ void k_pois_lu(DCoef c, double *dinv) {
 
 // The pivots of the CTA's 16 modes are staged in shared memory next to the
 // right-hand-side tile (column c uses pivot column c/2).
-__global__ void __launch_bounds__(YTHREADS) k_pois_solve(DCoef c, double *phi, const double *__restrict__ dinv,
-                                                         int Lp) {
+__global__ void __launch_bounds__(YTHREADS) k_pois_solve(DCoef c, YSet ys, double *phi,
+                                                         const double *__restrict__ dinv, int Lp) {
   extern __shared__ double sm[];
   const int ny = c.ny, ny1 = ny - 1, nz1 = c.nz1, nm = c.nz2 + 1;
   const int i = blockIdx.y + 2, kr0 = blockIdx.x * YT, k0 = kr0 / 2;
@@ -476,10 +486,11 @@ __global__ void __launch_bounds__(YTHREADS) k_pois_solve(DCoef c, double *phi, c
   const double *dcol = D + (q.col >> 1) * Lp;
   if (i == 2 && q.k == 0 && q.valid && q.h == 0) x[ny1 - 1] = 0.0;  // pois.f90:113
   __syncwarp();
-  const double *ayp = c.ayp;
+  const int CL = chunk_len(ny1, YNCH, true);
+  const CCo<YNCH> A1(ys.k[YP_A1], q.h, CL), A3c(ys.k[YP_A3], q.h, CL);
   chunk_tri<YNCH, true>(
-      x, ny1, q.h, [&](int r) { return -A3(ayp, 1, r + 1) * dcol[r - 1]; }, [&](int r) { return dcol[r]; },
-      [&](int r) { return A3(ayp, 3, r + 1); });
+      x, ny1, q.h, [&](int r) { return -A1(r) * dcol[r - 1]; }, [&](int r) { return dcol[r]; },
+      [&](int r) { return A3c(r); });
   __syncthreads();
   for (int t = threadIdx.x; t < ny1 * YT; t += YTHREADS) {
     const int j0 = t / YT, col = t - j0 * YT, kr = kr0 + col;
@@ -503,9 +514,9 @@ cudaError_t launch_interpy(otbl_ctx *c) {
   cudaFuncSetAttribute(k_interpy, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   dim3 g((nz1 + YT - 1) / YT, c->cfg.nx);
   prof_begin(c, PK_INTERPY);
-  k_interpy<<<g, YTHREADS, smem, c->stream>>>(c->dc, c->f[OTBL_F_U], c->w.uy, 0, Lp);
-  k_interpy<<<g, YTHREADS, smem, c->stream>>>(c->dc, c->f[OTBL_F_W], c->w.wy, 0, Lp);
-  k_interpy<<<g, YTHREADS, smem, c->stream>>>(c->dc, c->f[OTBL_F_V], c->w.vy, 1, Lp);
+  k_interpy<<<g, YTHREADS, smem, c->stream>>>(c->dc, yset(c->yco, 0), c->f[OTBL_F_U], c->w.uy, 0, Lp);
+  k_interpy<<<g, YTHREADS, smem, c->stream>>>(c->dc, yset(c->yco, 0), c->f[OTBL_F_W], c->w.wy, 0, Lp);
+  k_interpy<<<g, YTHREADS, smem, c->stream>>>(c->dc, yset(c->yco, 1), c->f[OTBL_F_V], c->w.vy, 1, Lp);
   prof_end(c);
   c->launches += 3;
   return cudaGetLastError();
@@ -539,9 +550,9 @@ cudaError_t launch_final(otbl_ctx *c) {
   cudaFuncSetAttribute(k_final<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   dim3 g((c->dc.nz1 + YT - 1) / YT, c->cfg.nx - 1);
   prof_begin(c, PK_FINAL);
-  k_final<1><<<g, YTHREADS, smem, c->stream>>>(c->dc, a, Lp);
-  k_final<0><<<g, YTHREADS, smem, c->stream>>>(c->dc, a, Lp);
-  k_final<2><<<g, YTHREADS, smem, c->stream>>>(c->dc, a, Lp);
+  k_final<1><<<g, YTHREADS, smem, c->stream>>>(c->dc, yset(c->yco, 1), a, Lp);
+  k_final<0><<<g, YTHREADS, smem, c->stream>>>(c->dc, yset(c->yco, 0), a, Lp);
+  k_final<2><<<g, YTHREADS, smem, c->stream>>>(c->dc, yset(c->yco, 0), a, Lp);
   prof_end(c);
   c->launches += 3;
   return cudaGetLastError();
@@ -561,7 +572,7 @@ cudaError_t launch_pois_solve(otbl_ctx *c, double *phi) {
   cudaFuncSetAttribute(k_pois_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   dim3 g((c->dc.nz1 + YT - 1) / YT, c->cfg.nx - 1);
   prof_begin(c, PK_POIS_SOLVE);
-  k_pois_solve<<<g, YTHREADS, smem, c->stream>>>(c->dc, phi, c->w.pois_dinv, Lp);
+  k_pois_solve<<<g, YTHREADS, smem, c->stream>>>(c->dc, yset(c->yco, 0), phi, c->w.pois_dinv, Lp);
   prof_end(c);
   c->launches += 1;
   return cudaGetLastError();

@@ -9,7 +9,8 @@
 //                                          367-415)
 //   difvisxx  lip.f90:52    k_difvisx     x-lines, d/dx(product) + d2/dx2
 //   dt        rhsp.F90:214  k_dt          dt, RK3 factors, implzy LU factors
-//   genflu    genflu.F90:3  k_genflu      inflow plane + boun of plane 1
+//   genflu    genflu.F90:3  k_genflu_tab  integral quantities, rescaling tables
+//                           k_genflu_cols inflow plane + boun of plane 1
 //   rhsp tail rhsp.F90:291-484 k_final    y-lines: pressure gradient, RHS
 //                                          assembly (differzy), boun, vistyy,
 //                                          RK3 combination, implzy
@@ -28,6 +29,7 @@
 
 #include "devcommon.cuh"
 #include "fft.cuh"
+#include "lines.cuh"
 #include "otbl_internal.cuh"
 
 namespace otbl {
@@ -166,67 +168,106 @@ __global__ void __launch_bounds__(128) k_products(DCoef c, ZTab z, ProdArgs a) {
 // ---------------------------------------------------------------------------
 // dt (rhsp.F90:214-267), RK3 factors, implzy LU (lip.f90:545-568)
 // ---------------------------------------------------------------------------
-__device__ void implzy_factor(const DCoef &c, double *fac, int which, double var1) {
-  const int ny = c.ny, jee = which == 0 ? ny + 1 : ny;
+// LU of (A + var1*B) for implzy, lip.f90:545-568, rows j = 2..jee-1, as a
+// register recurrence. The factors go to the chunk-interleaved copy `fi` of
+// the y-line kernels (YM_L, YM_D, YM_U at fi, fi + len, fi + 2 len, row r =
+// j - 2); fac keeps the two boundary couplings that implzy moves to the
+// right-hand side (fac[3*(jee+1)] = a(2), fac[3*(jee+1)+1] = c(jee-1)).
+__device__ void implzy_factor(const DCoef &c, double *fac, double *fi, int which, double var1) {
+  const int ny = c.ny, jee = which == 0 ? ny + 1 : ny, n = jee - 2;
   const double *icon = which == 0 ? c.vyui : c.vyvi;
   const double *econ = which == 0 ? c.cofvyu : c.cofvyv;
-  for (int j = 2; j <= jee - 1; ++j) {
-    fac[3 * j + 0] = A3(icon, 1, j) + var1 * A3(econ, 3, j);
-    fac[3 * j + 1] = A3(icon, 2, j) + var1 * A3(econ, 2, j);
-    fac[3 * j + 2] = A3(icon, 3, j) + var1 * A3(econ, 1, j);
-  }
-  fac[3 * (jee + 1)] = fac[3 * 2 + 0];
-  fac[3 * (jee + 1) + 1] = fac[3 * (jee - 1) + 2];
-  fac[3 * 2 + 0] = 0.0;
-  fac[3 * (jee - 1) + 2] = 0.0;
+  const int CL = chunk_len(n, 8, true);
+  const size_t len = 8 * (size_t)CL;
+  auto at = [&](int j) {
+    const int r = j - 2;
+    return (size_t)(r % CL) * 8 + r / CL;
+  };
+  fac[3 * (jee + 1)] = A3(icon, 1, 2) + var1 * A3(econ, 3, 2);
+  fac[3 * (jee + 1) + 1] = A3(icon, 3, jee - 1) + var1 * A3(econ, 1, jee - 1);
+  double bprev = A3(icon, 2, 2) + var1 * A3(econ, 2, 2);
+  double cprev = jee - 1 == 2 ? 0.0 : A3(icon, 3, 2) + var1 * A3(econ, 1, 2);
+  fi[at(2)] = 0.0;
+  fi[2 * len + at(2)] = cprev;
   for (int j = 3; j <= jee - 1; ++j) {
-    const double d = 1.0 / fac[3 * (j - 1) + 1];
-    fac[3 * (j - 1) + 1] = d;
-    fac[3 * j + 0] = -fac[3 * j + 0] * d;
-    fac[3 * j + 1] = fac[3 * j + 1] + fac[3 * j + 0] * fac[3 * (j - 1) + 2];
+    const double d = 1.0 / bprev;
+    fi[len + at(j - 1)] = d;
+    const double aj = -(A3(icon, 1, j) + var1 * A3(econ, 3, j)) * d;
+    const double bj = (A3(icon, 2, j) + var1 * A3(econ, 2, j)) + aj * cprev;
+    const double cj = j == jee - 1 ? 0.0 : A3(icon, 3, j) + var1 * A3(econ, 1, j);
+    fi[at(j)] = aj;
+    fi[2 * len + at(j)] = cj;
+    bprev = bj;
+    cprev = cj;
   }
-  fac[3 * (jee - 1) + 1] = 1.0 / fac[3 * (jee - 1) + 1];
+  fi[len + at(jee - 1)] = 1.0 / bprev;
 }
 
-__global__ void k_dt(DCoef c, DState *st, const unsigned long long *vm_bits, double *fac_u, double *fac_v, int m,
-                     int setstep, int dt_mode, double dt_fixed) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// One CTA of 64 threads: the CFL reduction over the rows, then dt, the RK3
+// factors and the two implzy factorisations (one warp each).
+__global__ void __launch_bounds__(64) k_dt(DCoef c, DState *st, const unsigned long long *vm_bits, double *fac_u,
+                                           double *fac_v, double *fi_u, double *fi_v, int m, int setstep,
+                                           int dt_mode, double dt_fixed) {
+  __shared__ double s_dt3[2], s_vmax[2];
+  const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
   const double *S = c.S;
+  const double poco = 1e-7;
   if (setstep) {
-    const double poco = 1e-7;
-    const double um = __longlong_as_double((long long)st->umax_bits);
-    const double wm = __longlong_as_double((long long)st->wmax_bits);
-    const double dt1 = S[OTBL_S_DXMIN] / fmax(poco, um);
-    const double dt2 = S[OTBL_S_DXMIN] / fmax(poco, wm);
     double dt3 = DBL_MAX, vmax = 0.0;
-    for (int j = 1; j <= c.ny; ++j) {
+    for (int j = t + 1; j <= c.ny; j += 64) {
       const double vm = __longlong_as_double((long long)vm_bits[j]);
       dt3 = fmin(dt3, c.dymin[j - 1] / fmax(poco, vm));
       vmax = nmax(vmax, vm);
     }
-    const double dtloc = fmin(fmin(dt1, dt2), fmin(dt3, S[OTBL_S_DTRET]));
-    st->umax = um;
-    st->wmax = wm;
-    st->vmax = vmax;
-    if (!isfinite(um) || !isfinite(wm) || !isfinite(vmax)) st->err = OTBL_ERR_NAN;
-    if (dt_mode == OTBL_DT_ADAPTIVE) {
-      st->dt = dtloc;
-    } else if (!st->dt_frozen) {
-      st->dt = dt_fixed > 0.0 ? dt_fixed : dtloc;
-      st->dt_frozen = 1;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      dt3 = fmin(dt3, __shfl_xor_sync(0xffffffffu, dt3, o));
+      vmax = nmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+    }
+    if (lane == 0) {
+      s_dt3[wid] = dt3;
+      s_vmax[wid] = vmax;
     }
   }
-  const double dt = st->dt;
-  if (!(dt > 0.0) || !isfinite(dt)) st->err = OTBL_ERR_NAN;
-  const int q = m - 1;
-  st->var1 = dt * (S[OTBL_S_RKCV + q] + S[OTBL_S_RKDV + q]);
-  st->var2 = dt * S[OTBL_S_REX] * S[OTBL_S_RKCV + q];
-  st->var3 = dt * S[OTBL_S_RKC + q];
-  st->var4 = dt * S[OTBL_S_RKD + q];
-  st->rkk = S[OTBL_S_REX] * dt * S[OTBL_S_RKDV + q];
-  st->varstep = 5e-1 / dt / S[OTBL_S_RKDV + q];
-  implzy_factor(c, fac_u, 0, st->rkk);
-  implzy_factor(c, fac_v, 1, st->rkk);
+  __syncthreads();
+  if (t == 0) {
+    if (setstep) {
+      const double um = __longlong_as_double((long long)st->umax_bits);
+      const double wm = __longlong_as_double((long long)st->wmax_bits);
+      const double dt1 = S[OTBL_S_DXMIN] / fmax(poco, um);
+      const double dt2 = S[OTBL_S_DXMIN] / fmax(poco, wm);
+      const double dt3 = fmin(s_dt3[0], s_dt3[1]);
+      const double vmax = nmax(s_vmax[0], s_vmax[1]);
+      const double dtloc = fmin(fmin(dt1, dt2), fmin(dt3, S[OTBL_S_DTRET]));
+      st->umax = um;
+      st->wmax = wm;
+      st->vmax = vmax;
+      if (!isfinite(um) || !isfinite(wm) || !isfinite(vmax)) st->err = OTBL_ERR_NAN;
+      if (dt_mode == OTBL_DT_ADAPTIVE) {
+        st->dt = dtloc;
+      } else if (!st->dt_frozen) {
+        st->dt = dt_fixed > 0.0 ? dt_fixed : dtloc;
+        st->dt_frozen = 1;
+      }
+    }
+    const double dt = st->dt;
+    if (!(dt > 0.0) || !isfinite(dt)) st->err = OTBL_ERR_NAN;
+    const int q = m - 1;
+    st->var1 = dt * (S[OTBL_S_RKCV + q] + S[OTBL_S_RKDV + q]);
+    st->var2 = dt * S[OTBL_S_REX] * S[OTBL_S_RKCV + q];
+    st->var3 = dt * S[OTBL_S_RKC + q];
+    st->var4 = dt * S[OTBL_S_RKD + q];
+    st->rkk = S[OTBL_S_REX] * dt * S[OTBL_S_RKDV + q];
+    st->varstep = 5e-1 / dt / S[OTBL_S_RKDV + q];
+  }
+  __syncthreads();
+  if (lane == 0) {
+    const double rkk = *(volatile double *)&st->rkk;
+    if (wid == 0)
+      implzy_factor(c, fac_u, fi_u, 0, rkk);
+    else
+      implzy_factor(c, fac_v, fi_v, 1, rkk);
+  }
 }
 
 __global__ void k_reset_max(DState *st, unsigned long long *vm_bits, int ny) {
@@ -243,16 +284,27 @@ __global__ void k_tiempo(DState *st) {
 }
 
 // ---------------------------------------------------------------------------
-// genflu (genflu.F90:3-242, NEWGENFLU) on one CTA. Inside the substep
-// (tail = 1) it is followed by boun on plane 1 (boun.f90:33-55) and
-// rhs*pa(plane 1) = 0 (rhsp.F90:424-426,441-442); plane 1 is not touched by
-// the rest of rhsp.
+// genflu (genflu.F90:3-242, NEWGENFLU) in two launches:
+//   k_genflu_tab  one CTA: the filtered mean um, u_tau, delta99, Re_theta and
+//                 gamma (genflu.F90:67-93), and for the u and the v grid the
+//                 rescaled-grid interpolation tables kl, fsca, ntop of
+//                 genflu.F90:95-140, into the table scratch `tab`;
+//   k_genflu_cols one thread per (component, kr): plane 1 from plane xout,
+//                 i.e. the blending of genflu.F90:55-60, the zero modes of
+//                 :146-150 and profile (:204-242) in closed form (every output
+//                 row is a blend of two rows of the blended input plane).
+// Inside the substep (tail = 1) the column threads then apply boun on plane 1
+// (boun.f90:33-55) and rhs*pa(plane 1) = 0 (rhsp.F90:424-426,441-442); plane
+// 1 is not touched by the rest of rhsp. Sums whose order sets the rounding
+// are taken sequentially in the reference's order; everything else is
+// element-wise with the reference's expressions, so the result is the one
+// of a single sequential pass.
 // ---------------------------------------------------------------------------
 struct GenArgs {
   double *u, *v, *w, *rhsupa, *rhsvpa, *rhswpa;
   const double *u0, *v0;
   double *um;
-  double *wk;  // nz1*(ny+2) scratch
+  double *tab;  // genflu_tab_doubles(ny) doubles of table scratch
   // scalars: inputs dt, tiempo, timeinit; outputs of genflu.F90:67-93
   const double *dt, *tiempo, *timeinit;
   double *timec, *utauout, *rthout, *dout, *gamma1, *gamma2;
@@ -260,101 +312,55 @@ struct GenArgs {
   int tail;
 };
 
-__device__ void dobleu_dev(const double *eta, double *www, double *www1, int n) {
-  const double ag = 4.0, bg = 0.2, w1default = (double)0.7895f;
-  const double bg2 = 1.0 - 2.0 * bg, tag = 1.0 / tanh(ag);
-  *www1 = w1default;
-  www[1] = 0.0;
-  for (int i = 2; i <= n; ++i) {
-    const double xxx = 0.5 * (eta[i] + eta[i - 1]);
-    const double yyy = xxx >= 1.0 ? 1.0 : 0.5 * (1.0 + tag * tanh(ag * (xxx - bg) / (bg2 * xxx + bg)));
-    www[i] = www[i - 1] + yyy * (eta[i] - eta[i - 1]);
-    if (eta[i] >= 1.0 && eta[i - 1] < 1.0) *www1 = www[i - 1] + (1.0 - eta[i - 1]) * yyy;
-  }
+size_t genflu_smem_bytes(int ny) {
+  return sizeof(double) * (6 * (size_t)(ny + 1) + (ny + 2)) + sizeof(int) * 4 * (size_t)(ny + 1) + 64;
 }
 
-// profile, genflu.F90:204-242, on plane 1 of a field with n rows
-__device__ void profile_dev(const DCoef &c, double *ut, double *wk, int ntop, const int *kl, const double *fsca,
-                            int n, double ggg) {
-  const int nz1 = c.nz1, ny = c.ny, t = threadIdx.x, T = blockDim.x;
-  const int nk = nz1 - 2;
-  if (n == ny + 1) {
-    for (int e = t; e < ntop * nk; e += T) {
-      const int i = e / nk + 1, k = e % nk + 2, kll = max(kl[i], 1);
-      wk[(size_t)i * nz1 + k] = ut[(size_t)(kll + 1) * nz1 + k] * fsca[i] + ut[(size_t)kll * nz1 + k] * (1 - fsca[i]);
-    }
-    __syncthreads();
-    for (int k = t + 2; k < nz1; k += T) wk[k] = -wk[(size_t)nz1 + k];
-  } else {
-    for (int e = t; e < ntop * nk; e += T) {
-      const int i = e / nk + 1, k = e % nk + 2, kll = max(kl[i], 1);
-      wk[(size_t)(i - 1) * nz1 + k] =
-          ut[(size_t)kll * nz1 + k] * fsca[i] + ut[(size_t)(kll - 1) * nz1 + k] * (1 - fsca[i]);
-    }
-  }
-  __syncthreads();
-  const int i0 = ntop - 2;
-  for (int e = t; e < (n - i0 + 1) * nk; e += T) {
-    const int i = e / nk + i0, k = e % nk + 2;
-    wk[(size_t)(i - 1) * nz1 + k] = wk[(size_t)(ntop - 4) * nz1 + k];
-  }
-  __syncthreads();
-  for (int e = t; e < n * nk; e += T) {
-    const int i = e / nk + 1, k = e % nk + 2;
-    ut[(size_t)(i - 1) * nz1 + k] = wk[(size_t)(i - 1) * nz1 + k] * ggg;
-  }
-  __syncthreads();
-}
-
-__global__ void __launch_bounds__(512) k_genflu(DCoef c, GenArgs a) {
+__global__ void __launch_bounds__(256) k_genflu_tab(DCoef c, GenArgs a) {
   extern __shared__ double gsm[];
-  const int ny = c.ny, nz1 = c.nz1, xout = c.xout, t = threadIdx.x, T = blockDim.x;
-  const size_t PU = (size_t)(ny + 1) * nz1, PV = (size_t)ny * nz1;
+  const int ny = c.ny, nz1 = c.nz1, t = threadIdx.x, T = blockDim.x;
+  const size_t PU = (size_t)(ny + 1) * nz1;
   const double *y = c.y, *dy = c.dy;
-  const double yb = c.S[OTBL_S_YBLEND];
-  double *fsca = gsm;                              // 2*(ny+1)
-  double *ysca = fsca + 2 * (ny + 1);              // ny+1
-  double *wlwa = ysca + (ny + 1);                  // ny+1
-  int *kl = reinterpret_cast<int *>(wlwa + (ny + 1));  // 2*(ny+1)
-  __shared__ int ntop[2];
-  __shared__ double ggg;
-  // plane xout -> plane 1 with the blending of genflu.F90:55-60
-  for (size_t e = t; e < PU; e += T) {
-    const int j = (int)(e / nz1) + 1, kr = (int)(e % nz1);
-    double uv = a.u[(size_t)(xout - 1) * PU + e], wv = a.w[(size_t)(xout - 1) * PU + e];
-    if (kr >= 2) {
-      const double fb = 0.5 * (1 - tanh(y[j] - yb));
-      uv = uv * fb;
-      wv = wv * fb;
-    }
-    a.u[e] = uv;
-    a.w[e] = wv;
+  const int N1 = ny + 1;
+  double *ysca = gsm;             // [2][ny+1]
+  double *www = ysca + 2 * N1;    // [2][ny+1]: dobleu output, then wlwa
+  double *yyy = www + 2 * N1;     // [2][ny+1]
+  double *um = yyy + 2 * N1;      // um(1..ny+1) at um[1..]
+  int *kf = reinterpret_cast<int *>(um + ny + 2);  // [2][ny+1] fresh bisection, -1 = outside
+  int *kh = kf + 2 * N1;                            // [2][ny+1] its khh
+  __shared__ double s_timec, s_g1, s_g2, s_www1[2];
+  __shared__ int s_jfirst;
+  const double re = c.S[OTBL_S_RE], din = c.S[OTBL_S_DIN], rthin = c.S[OTBL_S_RTHIN];
+  const double dt = *a.dt;
+  if (t == 0) {
+    const double tloc = *a.tiempo - *a.timeinit;
+    s_timec = tloc < 20 ? 20.0 : (tloc < 100 ? 100.0 : tloc);
+    s_jfirst = ny - 1;
   }
-  for (size_t e = t; e < PV; e += T) a.v[e] = a.v[(size_t)(xout - 1) * PV + e];
+  __syncthreads();
+  const double timec = s_timec;
+  // um(j) <- (dt/timec) u(k=0, j, plane 1) + um(j)(1 - dt/timec); plane 1's
+  // mode 0 is plane xout's (the blending leaves modes 0 alone)
+  const double *ux = a.u + (size_t)(c.xout - 1) * PU;
+  for (int j = t + 1; j <= ny + 1; j += T) {
+    const double v = (dt / timec) * ux[(size_t)(j - 1) * nz1] + a.um[j - 1] * (1.0 - dt / timec);
+    um[j] = v;
+    a.um[j - 1] = v;
+  }
+  __syncthreads();
+  double uinf = 0.0;  // every thread, same order
+  for (int j = ny + 1 - 20; j <= ny + 1 - 5; ++j) uinf += um[j];
+  uinf = uinf / 16.0;
+  const double u99 = (double)0.99f * uinf;
+  // jtop: the loop of genflu.F90:80-84 stops at the first um(j) >= u99
+  for (int j = t + 1; j <= ny - 2; j += T)
+    if (um[j] >= u99) atomicMin(&s_jfirst, j);
   __syncthreads();
   if (t == 0) {
-    const double re = c.S[OTBL_S_RE], din = c.S[OTBL_S_DIN], rthin = c.S[OTBL_S_RTHIN];
-    const double dt = *a.dt, tloc = *a.tiempo - *a.timeinit;
-    double timec;
-    if (tloc < 20)
-      timec = 20;
-    else if (tloc < 100)
-      timec = 100;
-    else
-      timec = tloc;
+    const int jf = s_jfirst;
+    const int jtop = jf == 1 ? 0 : jf;
     *a.timec = timec;
-    double *um = a.um - 1;
-    for (int j = 1; j <= ny + 1; ++j) um[j] = (dt / timec) * a.u[(size_t)(j - 1) * nz1] + um[j] * (1.0 - dt / timec);
     *a.utauout = sqrt(fabs((um[2] - um[1]) / (y[2] - y[1]) / re));
-    double uinf = 0.0;
-    for (int j = ny + 1 - 20; j <= ny + 1 - 5; ++j) uinf += um[j];
-    uinf = uinf / 16.0;
-    const double u99 = (double)0.99f * uinf;
-    int jtop = 0;
-    for (int j = 1; j <= ny - 2; ++j) {
-      if (um[j] >= u99) break;
-      jtop = j + 1;
-    }
     *a.dout = y[jtop];
     double s = 0.0;
     for (int q = 0; q < jtop + 2; ++q) s += (uinf - um[2 + q]) * um[2 + q] * dy[1 + q];
@@ -364,81 +370,196 @@ __global__ void __launch_bounds__(512) k_genflu(DCoef c, GenArgs a) {
     const double gamma1 = pow(gamma2, 0.125);
     *a.gamma2 = gamma2;
     *a.gamma1 = gamma1;
-    ggg = 1.0 / gamma1;
-    for (int kk = 1; kk <= 2; ++kk) {
-      for (int j = 1; j <= ny; ++j) ysca[j] = kk == 1 ? 5e-1 * (y[j] + y[j + 1]) / din : y[j] / din;
-      double www1;
-      dobleu_dev(ysca, wlwa, &www1, ny);
-      for (int j = 1; j <= ny; ++j)
-        wlwa[j] = ysca[j] / gamma1 + (1.0 / gamma2 - 1.0 / gamma1) / www1 * wlwa[j];
-      int kll = 1;
-      int *klk = kl + (kk - 1) * (ny + 1);
-      double *fk = fsca + (kk - 1) * (ny + 1);
-      ntop[kk - 1] = 0;
-      for (int j = 0; j <= ny; ++j) {
-        klk[j] = 0;
-        fk[j] = 0.0;
+    s_g1 = gamma1;
+    s_g2 = gamma2;
+    a.tab[3 * N1] = 1.0 / gamma1;  // ggg
+  }
+  // rescaled grids: kk = 0 (u rows, cell centres) and kk = 1 (v rows)
+  for (int e = t; e < 2 * N1; e += T) {
+    const int kk = e / N1, j = e - kk * N1;
+    if (j >= 1) ysca[e] = kk == 0 ? 5e-1 * (y[j] + y[j + 1]) / din : y[j] / din;
+  }
+  __syncthreads();
+  // dobleu (genflu.F90:250-298): the tanh weights element-wise, the running
+  // integral sequentially
+  {
+    const double ag = 4.0, bg = 0.2;
+    const double bg2 = 1.0 - 2.0 * bg, tag = 1.0 / tanh(ag);
+    for (int e = t; e < 2 * N1; e += T) {
+      const int kk = e / N1, i = e - kk * N1;
+      if (i < 2 || i > ny) continue;
+      const double *eta = ysca + kk * N1;
+      const double xxx = 0.5 * (eta[i] + eta[i - 1]);
+      yyy[e] = xxx >= 1.0 ? 1.0 : 0.5 * (1.0 + tag * tanh(ag * (xxx - bg) / (bg2 * xxx + bg)));
+    }
+  }
+  __syncthreads();
+  if (t == 0 || t == 32) {
+    const int kk = t / 32;
+    const double *eta = ysca + kk * N1, *yy = yyy + kk * N1;
+    double *ww = www + kk * N1;
+    double www1 = (double)0.7895f;
+    ww[1] = 0.0;
+    for (int i = 2; i <= ny; ++i) {
+      ww[i] = ww[i - 1] + yy[i] * (eta[i] - eta[i - 1]);
+      if (eta[i] >= 1.0 && eta[i - 1] < 1.0) www1 = ww[i - 1] + (1.0 - eta[i - 1]) * yy[i];
+    }
+    s_www1[kk] = www1;
+  }
+  __syncthreads();
+  const double gamma1 = s_g1, gamma2 = s_g2;
+  double *fsca = a.tab;
+  int *kl = reinterpret_cast<int *>(a.tab + 2 * N1);
+  int *ntop = reinterpret_cast<int *>(a.tab + 3 * N1 + 1);
+  for (int e = t; e < 2 * N1; e += T) {
+    const int kk = e / N1, j = e - kk * N1;
+    if (j >= 1) www[e] = ysca[e] / gamma1 + (1.0 / gamma2 - 1.0 / gamma1) / s_www1[kk] * www[e];
+  }
+  __syncthreads();
+  // bisection of genflu.F90:120-135 for every row from kll = 1, khh = ny
+  for (int e = t; e < 2 * N1; e += T) {
+    const int kk = e / N1, i = e - kk * N1;
+    const double *ys = ysca + kk * N1;
+    const double wl = www[e];
+    kf[e] = -1;
+    if (i >= 1 && wl <= ys[ny]) {
+      int kll = 1, khh = ny;
+      while (khh - kll > 1) {
+        const int kx = (khh + kll) / 2;
+        if (ys[kx] >= wl)
+          khh = kx;
+        else
+          kll = kx;
       }
-      for (int i = 1; i <= ny; ++i) {
-        if (wlwa[i] <= ysca[ny]) {
-          ntop[kk - 1] = i;
-          int khh = ny;
-          while (khh - kll > 1) {
-            const int kx = (khh + kll) / 2;
-            if (ysca[kx] >= wlwa[i])
-              khh = kx;
-            else
-              kll = kx;
-          }
-          klk[i] = kll;
-          fk[i] = (wlwa[i] - ysca[kll]) / (ysca[khh] - ysca[kll]);
+      kf[e] = kll;
+      kh[e] = khh;
+    }
+  }
+  __syncthreads();
+  // the reference carries kll from one row to the next; a bisection started
+  // at the carried kll = lo ends where the fresh one does unless the target
+  // lies at or below ys[lo], where it stays at lo (redone sequentially)
+  if (t == 0 || t == 32) {
+    const int kk = t / 32;
+    const double *ys = ysca + kk * N1, *wl = www + kk * N1;
+    int *kfk = kf + kk * N1, *khk = kh + kk * N1;
+    int lo = 1, nt = 0;
+    for (int i = 1; i <= ny; ++i) {
+      if (kfk[i] < 0) continue;
+      nt = i;
+      if (!(ys[lo] < wl[i])) {
+        int kll = lo, khh = ny;
+        while (khh - kll > 1) {
+          const int kx = (khh + kll) / 2;
+          if (ys[kx] >= wl[i])
+            khh = kx;
+          else
+            kll = kx;
         }
+        kfk[i] = kll;
+        khk[i] = khh;
       }
+      lo = kfk[i];
     }
+    ntop[kk] = nt;
   }
   __syncthreads();
-  // zero mode, genflu.F90:146-150
-  for (int j = t + 1; j <= ny + 1; j += T) {
-    a.u[(size_t)(j - 1) * nz1] = a.u0[j - 1];
-    a.u[(size_t)(j - 1) * nz1 + 1] = 0.0;
-    a.w[(size_t)(j - 1) * nz1] = 0.0;
-    a.w[(size_t)(j - 1) * nz1 + 1] = 0.0;
-    if (j <= ny) {
-      a.v[(size_t)(j - 1) * nz1] = a.v0[j - 1];
-      a.v[(size_t)(j - 1) * nz1 + 1] = 0.0;
+  for (int e = t; e < 2 * N1; e += T) {
+    const int kk = e / N1, i = e - kk * N1;
+    const double *ys = ysca + kk * N1;
+    if (kf[e] < 0 || i == 0) {
+      kl[e] = 0;
+      fsca[e] = 0.0;
+    } else {
+      const int kll = kf[e], khh = kh[e];
+      kl[e] = kll;
+      fsca[e] = (www[e] - ys[kll]) / (ys[khh] - ys[kll]);
     }
   }
-  __syncthreads();
-  // a rescaled grid with fewer than 4 points inside the box (only reachable
-  // with non-finite integral quantities) cannot be profiled: flag it
-  if (ntop[0] >= 4 && ntop[1] >= 4) {
-    profile_dev(c, a.u, a.wk, ntop[0], kl, fsca, ny + 1, ggg);
-    profile_dev(c, a.w, a.wk, ntop[0], kl, fsca, ny + 1, ggg);
-    profile_dev(c, a.v, a.wk, ntop[1], kl + (ny + 1), fsca + (ny + 1), ny, ggg);
-  } else if (t == 0 && a.err) {
-    *a.err = OTBL_ERR_NAN;
+}
+
+// One thread per (kr, component); blockIdx.y = 0 u, 1 w, 2 v.
+__global__ void __launch_bounds__(128) k_genflu_cols(DCoef c, GenArgs a) {
+  const int ny = c.ny, nz1 = c.nz1, xout = c.xout;
+  const int kr = blockIdx.x * blockDim.x + threadIdx.x;
+  const int comp = blockIdx.y;
+  if (kr >= nz1) return;
+  const bool vt = comp == 2;
+  const int rows = vt ? ny : ny + 1;
+  const size_t P = (size_t)rows * nz1;
+  double *f = comp == 0 ? a.u : (comp == 1 ? a.w : a.v);
+  const double *in = f + (size_t)(xout - 1) * P + kr;
+  double *out = f + kr;
+  const int N1 = ny + 1;
+  const double *fsca = a.tab + (vt ? N1 : 0);
+  const int *kl = reinterpret_cast<const int *>(a.tab + 2 * N1) + (vt ? N1 : 0);
+  const int *ntp = reinterpret_cast<const int *>(a.tab + 3 * N1 + 1);
+  const int nt = vt ? ntp[1] : ntp[0];
+  const bool prof = ntp[0] >= 4 && ntp[1] >= 4;
+  const double ggg = a.tab[3 * N1];
+  const double yb = c.S[OTBL_S_YBLEND];
+  // input row r (0-based) of the blended plane: genflu.F90:55-60 (modes >= 1)
+  auto inp = [&](int r) -> double {
+    const double v = in[(size_t)r * nz1];
+    if (vt || kr < 2) return v;
+    const double fb = 0.5 * (1 - tanh(c.y[r + 1] - yb));
+    return v * fb;
+  };
+  if (kr < 2) {  // zero mode, genflu.F90:146-150
+    for (int r = 0; r < rows; ++r) {
+      double v = 0.0;
+      if (kr == 0 && comp == 0) v = a.u0[r];
+      if (kr == 0 && comp == 2) v = a.v0[r];
+      out[(size_t)r * nz1] = v;
+    }
+  } else if (!prof) {  // degenerate rescaled grid: blended copy, flagged
+    for (int r = 0; r < rows; ++r) out[(size_t)r * nz1] = inp(r);
+    if (kr == 2 && comp == 0 && a.err) *a.err = OTBL_ERR_NAN;
+  } else if (!vt) {  // profile, u-type rows 0..ny
+    auto W = [&](int i) {
+      const int kll = max(kl[i], 1);
+      return inp(kll + 1) * fsca[i] + inp(kll) * (1 - fsca[i]);
+    };
+    const double w1 = W(1);
+    for (int r = 0; r <= ny; ++r) {
+      const int rr = r >= nt - 3 ? nt - 4 : r;
+      const double wv = rr == 0 ? -w1 : W(rr);
+      out[(size_t)r * nz1] = wv * ggg;
+    }
+  } else {  // profile, v-type rows 0..ny-1
+    for (int r = 0; r < ny; ++r) {
+      const int i = (r >= nt - 3 ? nt - 4 : r) + 1;
+      const int kll = max(kl[i], 1);
+      out[(size_t)r * nz1] = (inp(kll) * fsca[i] + inp(kll - 1) * (1 - fsca[i])) * ggg;
+    }
   }
   if (!a.tail) return;
-  // boun on plane 1 and the plane-1 RHS history
-  __syncthreads();
-  const double *ib = c.inby, *cc = c.ccon;
-  for (int kr = t; kr < nz1; kr += T) {
-    a.v[kr] = 0.0;
-    a.v[(size_t)(ny - 1) * nz1 + kr] = kr == 0 ? c.vmagic[0] : 0.0;
-    double *fl[2] = {a.u, a.w};
-    for (int f = 0; f < 2; ++f) {
-      double *q = fl[f] + kr;
-      q[0] = -1.0 / M4(ib, 2, 1) * (M4(ib, 2, 2) * q[nz1] + M4(ib, 2, 3) * q[2 * nz1] + M4(ib, 2, 4) * q[3 * nz1]);
-      q[(size_t)ny * nz1] = -1.0 / M2(cc, 1, 1) *
-                            (M2(cc, 1, 2) * q[(size_t)(ny - 1) * nz1] + M2(cc, 1, 3) * q[(size_t)(ny - 2) * nz1] +
-                             M2(cc, 1, 4) * q[(size_t)(ny - 3) * nz1]);
-    }
+  // boun on plane 1 (this thread wrote the whole column) and the plane-1
+  // RHS history
+  if (vt) {
+    out[0] = 0.0;
+    out[(size_t)(ny - 1) * nz1] = kr == 0 ? c.vmagic[0] : 0.0;
+    for (int r = 0; r < ny; ++r) a.rhsvpa[(size_t)r * nz1 + kr] = 0.0;
+  } else {
+    const double *ib = c.inby, *cc = c.ccon;
+    double *q = out;
+    q[0] = -1.0 / M4(ib, 2, 1) * (M4(ib, 2, 2) * q[nz1] + M4(ib, 2, 3) * q[2 * nz1] + M4(ib, 2, 4) * q[3 * nz1]);
+    q[(size_t)ny * nz1] = -1.0 / M2(cc, 1, 1) *
+                          (M2(cc, 1, 2) * q[(size_t)(ny - 1) * nz1] + M2(cc, 1, 3) * q[(size_t)(ny - 2) * nz1] +
+                           M2(cc, 1, 4) * q[(size_t)(ny - 3) * nz1]);
+    double *h = comp == 0 ? a.rhsupa : a.rhswpa;
+    for (int r = 0; r <= ny; ++r) h[(size_t)r * nz1 + kr] = 0.0;
   }
-  for (size_t e = t; e < PU; e += T) {
-    a.rhsupa[e] = 0.0;
-    a.rhswpa[e] = 0.0;
-  }
-  for (size_t e = t; e < PV; e += T) a.rhsvpa[e] = 0.0;
+}
+
+cudaError_t genflu_launch(otbl_ctx *c, const GenArgs &a) {
+  const size_t smem = genflu_smem_bytes(c->cfg.ny);
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k_genflu_tab, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_genflu_tab<<<1, 256, smem, c->stream>>>(c->dc, a);
+  dim3 g((c->dc.nz1 + 127) / 128, 3);
+  k_genflu_cols<<<g, 128, 0, c->stream>>>(c->dc, a);
+  c->launches += 2;
+  return cudaGetLastError();
 }
 
 // boun (boun.f90:7-56) on every plane, for the standalone entry point
@@ -829,8 +950,8 @@ cudaError_t launch_products(otbl_ctx *c, int setstep) {
 
 cudaError_t launch_dt(otbl_ctx *c, int m, int setstep) {
   prof_begin(c, PK_DT);
-  k_dt<<<1, 32, 0, c->stream>>>(c->dc, c->st, c->w.vm_bits, c->w.fac_u, c->w.fac_v, m, setstep, c->cfg.dt_mode,
-                                c->cfg.dt_fixed);
+  k_dt<<<1, 64, 0, c->stream>>>(c->dc, c->st, c->w.vm_bits, c->w.fac_u, c->w.fac_v, c->yco.fac[0],
+                                c->yco.fac[1], m, setstep, c->cfg.dt_mode, c->cfg.dt_fixed);
   prof_end(c);
   c->launches += 1;
   return cudaGetLastError();
@@ -847,7 +968,7 @@ cudaError_t launch_genflu(otbl_ctx *c, int tail) {
   a.u0 = c->u0;
   a.v0 = c->v0;
   a.um = c->um;
-  a.wk = c->w.gf;
+  a.tab = c->w.gf;
   DState *st = c->st;
   a.dt = &st->dt;
   a.tiempo = &st->tiempo;
@@ -860,19 +981,15 @@ cudaError_t launch_genflu(otbl_ctx *c, int tail) {
   a.gamma2 = &st->gamma2;
   a.err = &st->err;
   a.tail = tail;
-  const int ny = c->cfg.ny;
-  const size_t smem = sizeof(double) * (4 * (size_t)(ny + 1)) + sizeof(int) * 2 * (ny + 1);
-  cudaFuncSetAttribute(k_genflu, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   prof_begin(c, PK_GENFLU);
-  k_genflu<<<1, 512, smem, c->stream>>>(c->dc, a);
+  const cudaError_t e = genflu_launch(c, a);
   prof_end(c);
-  c->launches += 1;
-  return cudaGetLastError();
+  return e;
 }
 
 // ---------------------------------------------------------------------------
-// genflu on caller-owned buffers, with its profile scratch plane in a static
-// device array instead of a context allocation. Callers that cannot allocate
+// genflu on caller-owned buffers, with its table scratch in a static device
+// array instead of a context allocation. Callers that cannot allocate
 // device memory at call time use it: a host that owns the fields in its own
 // device allocations and has handed the rest of HBM to its own pool has no
 // room for a scratch buffer mid-run, and a cudaMalloc/cudaFree pair would
@@ -881,8 +998,8 @@ cudaError_t launch_genflu(otbl_ctx *c, int tail) {
 // The array is part of this module's data, so it comes into existence when
 // the module is loaded on a device; the first call on each device looks its
 // address up (cudaGetSymbolAddress, which may load the module) and caches
-// it. Nothing in it needs to start at zero: k_genflu writes every row of the
-// plane that it reads earlier in the same launch. All calls on one device
+// it. Nothing in it needs to start at zero: k_genflu_tab writes every table
+// entry that k_genflu_cols reads, earlier on the same stream. All calls on one device
 // share the one array, so two calls whose launches overlap (different
 // streams, contexts or host threads without ordering between them) race.
 // ---------------------------------------------------------------------------
@@ -893,8 +1010,6 @@ constexpr int kMaxDevices = 64;
 std::mutex g_scratch_mu;
 double *g_scratch_addr[kMaxDevices] = {};
 }  // namespace
-
-size_t genflu_smem_bytes(int ny) { return sizeof(double) * (4 * (size_t)(ny + 1)) + sizeof(int) * 2 * (ny + 1); }
 
 // The caller has made `device` current.
 cudaError_t genflu_scratch_addr(int device, double **p) {
@@ -920,7 +1035,7 @@ cudaError_t launch_genflu_noalloc(otbl_ctx *c, double *wk, double *u, double *v,
   a.u0 = u0;
   a.v0 = v0;
   a.um = um;
-  a.wk = wk;
+  a.tab = wk;
   a.dt = scal + OTBL_GF_DT;
   a.tiempo = scal + OTBL_GF_TIEMPO;
   a.timeinit = scal + OTBL_GF_TIMEINIT;
@@ -932,11 +1047,7 @@ cudaError_t launch_genflu_noalloc(otbl_ctx *c, double *wk, double *u, double *v,
   a.gamma2 = scal + OTBL_GF_GAMMA2;
   a.err = err;
   a.tail = 0;
-  // the entry point has checked this against the default 48 KB limit
-  const size_t smem = genflu_smem_bytes(c->cfg.ny);
-  k_genflu<<<1, 512, smem, c->stream>>>(c->dc, a);
-  c->launches += 1;
-  return cudaGetLastError();
+  return genflu_launch(c, a);
 }
 
 cudaError_t launch_outflow(otbl_ctx *c) {

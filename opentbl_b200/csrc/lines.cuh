@@ -24,10 +24,15 @@ constexpr int LB = 4;  // rows per batch in the sequential passes
 // length is rounded up to 2 mod 4: eight chunk starts then fall in eight
 // distinct even banks, and with an odd column pitch the neighbouring column
 // takes the odd banks (a conflict-free half-warp of 2 columns x 8 chunks).
+__host__ __device__ inline int chunk_len(int n, int nch, bool even) {
+  int CL = (n + nch - 1) / nch;
+  if (even) CL += (6 - (CL & 3)) & 3;
+  return CL;
+}
+
 template <int NCH, bool EVEN>
 __device__ __forceinline__ void chunk_range(int n, int h, int &s, int &e) {
-  int CL = (n + NCH - 1) / NCH;
-  if (EVEN) CL += (6 - (CL & 3)) & 3;
+  const int CL = chunk_len(n, NCH, EVEN);
   s = min(n, h * CL);
   e = min(n, s + CL);
 }
@@ -155,6 +160,24 @@ template <int NCH, bool EVEN>
 __device__ __forceinline__ void solve_icon(double *x, int n, int h, Icon ic) {
   chunk_tri<NCH, EVEN>(
       x, n, h, [&](int r) { return ic.l(r); }, [&](int r) { return ic.d(r); }, [&](int r) { return ic.u(r); });
+}
+
+// A per-row coefficient in chunk-interleaved order: the value for row r of
+// chunk h (rows [h*CL, (h+1)*CL)) sits at (r - h*CL)*NCH + h. The lanes of a
+// warp step through their chunks in lockstep, so one warp request reads NCH
+// consecutive doubles instead of NCH rows spread over as many cache lines.
+// The host builds these copies with the CL of chunk_len().
+template <int NCH>
+struct CCo {
+  const double *a;
+  int base;
+  __device__ __forceinline__ CCo(const double *p, int h, int CL) : a(p), base(h - h * CL * NCH) {}
+  __device__ __forceinline__ double operator()(int r) const { return __ldg(a + r * NCH + base); }
+};
+
+template <int NCH, bool EVEN>
+__device__ __forceinline__ void solve_cco(double *x, int n, int h, CCo<NCH> L, CCo<NCH> D, CCo<NCH> U) {
+  chunk_tri<NCH, EVEN>(x, n, h, L, D, U);
 }
 
 }  // namespace otbl

@@ -1,9 +1,11 @@
 // C ABI of the B200 substep (include/otbl.h): context lifetime, state
 // transfer and the stream-ordered orchestration of the kernels in
 // kernels.cu, following the call order of bl_1.F90:94-125.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 
+#include "lines.cuh"
 #include "otbl_internal.cuh"
 
 using namespace otbl;
@@ -42,6 +44,127 @@ int dalloc(otbl_ctx *c, T **p, size_t count) {
 size_t field_len(const otbl_ctx *c, int id) {
   const int ut = (id == OTBL_F_U || id == OTBL_F_W || id == OTBL_F_RHSUPA || id == OTBL_F_RHSWPA);
   return otbl_field_len(c->cfg.nx, c->cfg.ny, c->cfg.nz, ut);
+}
+
+// Chunk-interleaved copy (lines.cuh CCo) of f(r), r = 0..n-1, for nch lanes
+// per line; rows past n are 0 and never read.
+template <class F>
+void interleave(double *dst, int n, int nch, bool even, F f) {
+  const int CL = chunk_len(n, nch, even);
+  for (int h = 0; h < nch; ++h)
+    for (int t = 0; t < CL; ++t) {
+      const int r = h * CL + t;
+      dst[(size_t)t * nch + h] = r < n ? f(r) : 0.0;
+    }
+}
+
+// The x-line coefficients of lip.f90 (interpxx, difvisxx) in the
+// chunk-interleaved order of the x-line kernels (32 lanes per line).
+int build_xco(otbl_ctx *c, const otbl_coef_offsets &o) {
+  const int nx = c->cfg.nx;
+  const int CL = chunk_len(nx, 32, false);
+  const size_t len = (size_t)CL * 32;
+  double *dev = nullptr;
+  int st = dalloc(c, &dev, 2 * (size_t)XCO_N * len);
+  if (st != OTBL_OK) return st;
+  std::vector<double> h(2 * (size_t)XCO_N * len);
+  const double *H = c->coef_host.data();
+  auto F = [&](int id) { return H + o.off[id]; };
+  auto ci = [&](int r) { return std::min(std::max(r + 1, 2), nx - 1); };  // stencil row, 1-based
+  for (int which = 0; which < 2; ++which) {
+    const double *inx = F(which == 0 ? OTBL_C_INXU : OTBL_C_INXV);
+    const double *cofi = F(which == 0 ? OTBL_C_COFIUX : OTBL_C_COFIVX);
+    const double *dcx = F(which == 0 ? OTBL_C_DCXU : OTBL_C_DCXV);
+    const double *vix = F(which == 0 ? OTBL_C_VIXU : OTBL_C_VIXV);
+    const double *cofc = F(which == 0 ? OTBL_C_COFCXU : OTBL_C_COFCXV);
+    const double *cofv = F(which == 0 ? OTBL_C_COFVXU : OTBL_C_COFVXV);
+    double *base = h.data() + (size_t)which * XCO_N * len;
+    auto put = [&](int kind, auto f) { interleave(base + (size_t)kind * len, nx, 32, false, f); };
+    // solves: row r (0-based) uses Fortran column r + 1 of the (3, nx) array
+    for (int q = 0; q < 3; ++q) {
+      put(XI_L + q, [&](int r) { return inx[(size_t)r * 3 + q]; });
+      put(XD_L + q, [&](int r) { return dcx[(size_t)r * 3 + q]; });
+      put(XV_L + q, [&](int r) { return vix[(size_t)r * 3 + q]; });
+      put(XV_F1 + q, [&](int r) { return cofv[(size_t)(ci(r) - 1) * 3 + q]; });
+    }
+    for (int q = 0; q < 2; ++q) {
+      put(XI_E1 + q, [&](int r) { return cofi[(size_t)(ci(r) - 1) * 2 + q]; });
+      put(XD_E1 + q, [&](int r) { return cofc[(size_t)(ci(r) - 1) * 2 + q]; });
+    }
+    for (int k = 0; k < XCO_N; ++k) c->xco.k[which][k] = dev + ((size_t)which * XCO_N + k) * len;
+  }
+  c->xco.CL = CL;
+  if (cudaMemcpy(dev, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
+    c->err = "coefficient upload failed";
+    return OTBL_ERR_CUDA;
+  }
+  return OTBL_OK;
+}
+
+// rows of each y-line operator (YCoKind) for which 0 (u,w) / 1 (v)
+int yco_rows(int kind, int which, int ny) {
+  const int jee = which == 0 ? ny + 1 : ny;
+  if (kind <= YI_E2) return ny;
+  if (kind <= YV_F3) return jee;
+  if (kind <= YM_U) return jee - 2;
+  if (kind <= YP_A3) return ny - 1;
+  return ny;
+}
+
+// The y-line coefficients of lip.f90 (interpyy, differzy, vistyy, implzy),
+// of the Poisson operator (pois.f90, ayp) and idyy, in the chunk-interleaved
+// order of the y-line kernels (8 lanes per column). The implzy factors are
+// rewritten by k_dt every substep.
+int build_yco(otbl_ctx *c, const otbl_coef_offsets &o) {
+  const int ny = c->cfg.ny;
+  size_t off[2][YCO_N], total = 0;
+  for (int which = 0; which < 2; ++which)
+    for (int k = 0; k < YCO_N; ++k) {
+      off[which][k] = total;
+      total += 8 * (size_t)chunk_len(yco_rows(k, which, ny), 8, true);
+    }
+  double *dev = nullptr;
+  int st = dalloc(c, &dev, total);
+  if (st != OTBL_OK) return st;
+  std::vector<double> h(total, 0.0);
+  const double *H = c->coef_host.data();
+  auto F = [&](int id) { return H + o.off[id]; };
+  auto cl = [](int v, int lo, int hi) { return std::min(std::max(v, lo), hi); };
+  for (int which = 0; which < 2; ++which) {
+    const int jee = which == 0 ? ny + 1 : ny;
+    const double *iny = F(which == 0 ? OTBL_C_INYU : OTBL_C_INYV);
+    const double *cofi = F(which == 0 ? OTBL_C_COFIUY : OTBL_C_COFIVY);
+    const double *dcy = F(which == 0 ? OTBL_C_DCYU : OTBL_C_DCYV);
+    const double *cofc = F(which == 0 ? OTBL_C_COFCYU : OTBL_C_COFCYV);
+    const double *viy = F(which == 0 ? OTBL_C_VIYU : OTBL_C_VIYV);
+    const double *cofv = F(which == 0 ? OTBL_C_COFVYU : OTBL_C_COFVYV);
+    const double *vyi = F(which == 0 ? OTBL_C_VYUI : OTBL_C_VYVI);
+    const double *ayp = F(OTBL_C_AYP), *idyy = F(OTBL_C_IDYY);
+    auto put = [&](int kind, auto f) {
+      interleave(h.data() + off[which][kind], yco_rows(kind, which, ny), 8, true, f);
+    };
+    for (int q = 0; q < 3; ++q) {
+      put(YI_L + q, [&](int r) { return iny[(size_t)r * 3 + q]; });
+      put(YD_L + q, [&](int r) { return dcy[(size_t)r * 3 + q]; });
+      put(YV_L + q, [&](int r) { return viy[(size_t)r * 3 + q]; });
+      put(YV_F1 + q, [&](int r) { return cofv[(size_t)(cl(r + 1, 2, jee - 1) - 1) * 3 + q]; });
+      put(YM_F1 + q, [&](int r) { return vyi[(size_t)(std::min(r + 2, jee - 1) - 1) * 3 + q]; });
+    }
+    for (int q = 0; q < 2; ++q) {
+      put(YI_E1 + q, [&](int r) { return cofi[(size_t)(cl(r + 1, 2, ny - 1) - 1) * 2 + q]; });
+      put(YD_E1 + q, [&](int r) { return cofc[(size_t)(cl(r + 1, 2, ny) - 1) * 2 + q]; });
+    }
+    put(YP_A1, [&](int r) { return ayp[(size_t)r * 3 + 0]; });
+    put(YP_A3, [&](int r) { return ayp[(size_t)r * 3 + 2]; });
+    put(Y_IDYY, [&](int r) { return idyy[r]; });
+    for (int k = 0; k < YCO_N; ++k) c->yco.k[which][k] = dev + off[which][k];
+    c->yco.fac[which] = dev + off[which][YM_L];
+  }
+  if (cudaMemcpy(dev, h.data(), total * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
+    c->err = "coefficient upload failed";
+    return OTBL_ERR_CUDA;
+  }
+  return OTBL_OK;
 }
 
 int check(otbl_ctx *c, cudaError_t e, const char *where) {
@@ -172,8 +295,10 @@ extern "C" int otbl_ctx_create(const otbl_config *cfg, const double *coef, int d
   TRY(dalloc(c, &w.vm_bits, (size_t)ny + 1));
   TRY(dalloc(c, &w.fac_u, 3 * (size_t)(ny + 4)));
   TRY(dalloc(c, &w.fac_v, 3 * (size_t)(ny + 4)));
-  TRY(dalloc(c, &w.gf, (size_t)nz1 * (ny + 2)));
+  TRY(dalloc(c, &w.gf, genflu_tab_doubles(ny)));
   TRY(dalloc(c, &w.pois_dinv, (size_t)nx * ny * (nz1 / 2)));
+  TRY(build_xco(c, o));
+  TRY(build_yco(c, o));
 #undef TRY
   if (check(c, launch_twiddles(c), "twiddles") != OTBL_OK || check(c, launch_pois_lu(c), "pois_lu") != OTBL_OK || check(c, cudaStreamSynchronize(c->stream), "init")) {
     *out = c;
@@ -394,7 +519,7 @@ extern "C" int otbl_genflu(otbl_ctx *c) {
   return OTBL_OK;
 }
 
-// The success path allocates nothing: the scratch plane is the static array
+// The success path allocates nothing: the table scratch is the static array
 // of kernels.cu, found once per device (only an error path stores a message
 // string in the context).
 extern "C" int otbl_genflu_noalloc(otbl_ctx *c, double *u, double *v, double *w, const double *u0, const double *v0,
@@ -402,10 +527,9 @@ extern "C" int otbl_genflu_noalloc(otbl_ctx *c, double *u, double *v, double *w,
   if (!c) return OTBL_ERR_ARG;
   if (!u || !v || !w || !u0 || !v0 || !um || !scal)
     return fail(c, OTBL_ERR_ARG, "otbl_genflu_noalloc: null device pointer");
-  const size_t need = (size_t)c->dc.nz1 * (size_t)(c->cfg.ny + 2);
-  if (need > (size_t)OTBL_GENFLU_SCRATCH_MAX)
+  if (genflu_tab_doubles(c->cfg.ny) > (size_t)OTBL_GENFLU_SCRATCH_MAX)
     return fail(c, OTBL_ERR_CONFIG,
-                "otbl_genflu_noalloc: the profile plane nz1*(ny+2) exceeds OTBL_GENFLU_SCRATCH_MAX doubles");
+                "otbl_genflu_noalloc: the tables, 3*(ny+1)+2 doubles, exceed OTBL_GENFLU_SCRATCH_MAX");
   if (genflu_smem_bytes(c->cfg.ny) > 48 * 1024)
     return fail(c, OTBL_ERR_CONFIG, "otbl_genflu_noalloc: ny too large for 48 KB of shared memory");
   OTBL_CUDA_TRY(c, cudaSetDevice(c->device));

@@ -28,6 +28,64 @@ struct DCoef {
   const double *viyu, *viyv, *vyui, *vyvi, *cofvyu, *cofvyv, *cofvby, *ccon;
 };
 
+// Chunk-interleaved copies (lines.cuh CCo) of the x-line coefficients, for
+// 32 lanes per line and CL = chunk_len(nx, 32, false). Index [which][kind]:
+// which 0 = u, 1 = v,w (lip.f90 chi/chv selections).
+enum XCoKind {
+  XI_L, XI_D, XI_U,          // interpxx solve: inxu / inxv
+  XI_E1, XI_E2,              // interpxx stencil: cofiux / cofivx at row clamp(r+1, 2, nx-1)
+  XD_L, XD_D, XD_U,          // difvisxx first derivative solve: dcxu / dcxv
+  XV_L, XV_D, XV_U,          // difvisxx second derivative solve: vixu / vixv
+  XD_E1, XD_E2,              // cofcxu / cofcxv at clamp(r+1, 2, nx-1)
+  XV_F1, XV_F2, XV_F3,       // cofvxu / cofvxv at clamp(r+1, 2, nx-1)
+  XCO_N
+};
+struct XCo {
+  const double *k[2][XCO_N];
+  int CL;
+};
+// the set of one `which`, passed by value to a kernel
+struct XSet {
+  const double *k[XCO_N];
+  int CL;
+};
+inline XSet xset(const XCo &x, int which) {
+  XSet s;
+  for (int q = 0; q < XCO_N; ++q) s.k[q] = x.k[which][q];
+  s.CL = x.CL;
+  return s;
+}
+
+// Chunk-interleaved copies of the y-line coefficients, for 8 lanes per
+// column and CL = chunk_len(n, 8, true) with the n of each operator (jee =
+// ny+1 for u-type, ny for v-type). Index [which][kind]: which 0 = u,w,
+// 1 = v (interpyy: 0 = u,w input, 1 = v input).
+enum YCoKind {
+  YI_L, YI_D, YI_U,           // interpyy solve: inyu / inyv, n = ny
+  YI_E1, YI_E2,               // cofiuy / cofivy at clamp(r+1, 2, ny-1)
+  YD_L, YD_D, YD_U,           // differzy solve: dcyu / dcyv, n = jee
+  YD_E1, YD_E2,               // cofcyu / cofcyv at clamp(r+1, 2, ny)
+  YV_L, YV_D, YV_U,           // vistyy solve: viyu / viyv, n = jee
+  YV_F1, YV_F2, YV_F3,        // cofvyu / cofvyv at clamp(r+1, 2, jee-1)
+  YM_F1, YM_F2, YM_F3,        // implzy stencil: vyui / vyvi at min(r+2, jee-1), n = jee-2
+  YM_L, YM_D, YM_U,           // implzy factors of the current dt (k_dt), n = jee-2
+  YP_A1, YP_A3,               // pois y operator: ayp(1, r+1), ayp(3, r+1), n = ny-1
+  Y_IDYY,                     // idyy(r+1), n = ny
+  YCO_N
+};
+struct YCo {
+  const double *k[2][YCO_N];
+  double *fac[2];  // YM_L of each which; YM_D, YM_U follow at +len, +2 len
+};
+struct YSet {
+  const double *k[YCO_N];
+};
+inline YSet yset(const YCo &y, int which) {
+  YSet s;
+  for (int q = 0; q < YCO_N; ++q) s.k[q] = y.k[which][q];
+  return s;
+}
+
 // Scalars that live on the device so that no host synchronisation is needed
 // inside a step (dt is produced by a reduction on the device).
 struct DState {
@@ -53,7 +111,7 @@ struct Work {
   double *twx2;                // exp(-i pi k/(2n)), k = 0..n-1
   unsigned long long *vm_bits; // vm(j) maxima, j = 1..ny
   double *fac_u, *fac_v;       // implzy LU factors for the current dt (3*(ny+1))
-  double *gf;                  // genflu scratch: kl/fsca/ntop + wk plane
+  double *gf;                  // genflu tables (genflu_tab_doubles)
   double *pois_dinv;           // pivots of the (x-mode, kz) y-systems, [i][j][k]
 };
 
@@ -64,6 +122,8 @@ struct otbl_ctx {
   int device;
   cudaStream_t stream;
   otbl::DCoef dc;
+  otbl::XCo xco;
+  otbl::YCo yco;
   double *coef_dev;
   std::vector<double> coef_host;
   double *f[OTBL_F_COUNT];
@@ -125,7 +185,9 @@ cudaError_t launch_pois_solve(otbl_ctx *c, double *phi);
 cudaError_t launch_chp2x(otbl_ctx *c, const double *plan, double *pen, int jee, int to_pen);
 cudaError_t launch_fourxz(otbl_ctx *c, double *fou, double *phys, int iopt, int nlines);
 cudaError_t launch_cosftx(otbl_ctx *c, double *cpen, int nlines, int iopt);
-// genflu on caller-owned buffers with the static scratch plane (no allocation)
+// genflu table scratch: fsca[2][ny+1] | kl[2][ny+1] (int) | ggg | ntop[2] (int)
+inline size_t genflu_tab_doubles(int ny) { return 3 * (size_t)(ny + 1) + 2; }
+// genflu on caller-owned buffers with the static table scratch (no allocation)
 size_t genflu_smem_bytes(int ny);
 cudaError_t genflu_scratch_addr(int device, double **p);
 cudaError_t launch_genflu_noalloc(otbl_ctx *c, double *wk, double *u, double *v, double *w, const double *u0,
