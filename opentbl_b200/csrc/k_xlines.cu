@@ -11,8 +11,14 @@
 
 namespace otbl {
 
-constexpr int XT_INTERP = 8;  // pencils per CTA for interpxx (1 tile)
-constexpr int XT_DIFVIS = 4;  // pencils per CTA for difvisxx (2 tiles)
+#ifndef OTBL_XT_INTERP
+#define OTBL_XT_INTERP 8
+#endif
+#ifndef OTBL_XT_DIFVIS
+#define OTBL_XT_DIFVIS 4
+#endif
+constexpr int XT_INTERP = OTBL_XT_INTERP;  // pencils per CTA for interpxx (1 tile)
+constexpr int XT_DIFVIS = OTBL_XT_DIFVIS;  // pencils per CTA for difvisxx (2 tiles)
 
 // Issues the asynchronous copies of a tile (nx planes x XT pencils); the
 // caller waits with xtile_wait.
@@ -62,7 +68,7 @@ __global__ void __launch_bounds__(XT_INTERP * 32) k_interpx(DCoef c, XSet xs, co
   const double *ib = c.inbx;
   const CCo<32> E1(xs.k[XI_E1], h, xs.CL), E2(xs.k[XI_E2], h, xs.CL);
   int s, e;
-  chunk_range<32, false>(nx, h, s, e);
+  chunk_range(nx, h, xs.CL, s, e);
   const double gnext = e < nx ? x[e] : 0.0;
   double b0 = 0.0, bN = 0.0;
   if (s == 0 && e > s)
@@ -89,7 +95,7 @@ __global__ void __launch_bounds__(XT_INTERP * 32) k_interpx(DCoef c, XSet xs, co
     }
   }
   __syncwarp();
-  solve_cco<32, false>(x, nx, h, CCo<32>(xs.k[XI_L], h, xs.CL), CCo<32>(xs.k[XI_D], h, xs.CL),
+  solve_cco<32>(x, nx, h, xs.CL, CCo<32>(xs.k[XI_L], h, xs.CL), CCo<32>(xs.k[XI_D], h, xs.CL),
                        CCo<32>(xs.k[XI_U], h, xs.CL));
   __syncthreads();
   xtile_store<XT_INTERP>(sm, out, nx, np, mp0, Lp, xr);
@@ -116,7 +122,7 @@ __global__ void __launch_bounds__(XT_DIFVIS * 32) k_difvisx(DCoef c, XSet xs, co
   const double *db = c.dcbx, *vb = c.cofvbx;
   const double rex = c.S[OTBL_S_REX], idx = c.S[OTBL_S_IDX], uinf = c.S[OTBL_S_UINF];
   int s, e;
-  chunk_range<32, false>(nx, h, s, e);
+  chunk_range(nx, h, xs.CL, s, e);
   // halos and boundary stencils, read before anything is overwritten
   const double gprev = s > 0 ? x[s - 1] : 0.0;
   double uprev = s > 0 ? u[s - 1] : 0.0;
@@ -176,9 +182,9 @@ __global__ void __launch_bounds__(XT_DIFVIS * 32) k_difvisx(DCoef c, XSet xs, co
     uprev = uv[LB];  // original value of the last row of this batch
   }
   __syncwarp();
-  solve_cco<32, false>(x, nx, h, CCo<32>(xs.k[XD_L], h, CL), CCo<32>(xs.k[XD_D], h, CL),
+  solve_cco<32>(x, nx, h, xs.CL, CCo<32>(xs.k[XD_L], h, CL), CCo<32>(xs.k[XD_D], h, CL),
                        CCo<32>(xs.k[XD_U], h, CL));
-  solve_cco<32, false>(u, nx, h, CCo<32>(xs.k[XV_L], h, CL), CCo<32>(xs.k[XV_D], h, CL),
+  solve_cco<32>(u, nx, h, xs.CL, CCo<32>(xs.k[XV_L], h, CL), CCo<32>(xs.k[XV_D], h, CL),
                        CCo<32>(xs.k[XV_U], h, CL));
   for (int r = s; r < e; ++r) x[r] = r == nx - 1 ? uinf * (uN - uN1) * idx + rex * 0.0 : x[r] + rex * u[r];
   __syncthreads();
@@ -190,14 +196,13 @@ cudaError_t launch_interpx(otbl_ctx *c) {
   const int npu = nz1 * (ny + 1), npv = nz1 * ny;
   const int Lp = nx | 1;
   const size_t smem = sizeof(double) * XT_INTERP * Lp;
-  cudaFuncSetAttribute(k_interpx, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const dim3 gu((npu + XT_INTERP - 1) / XT_INTERP), gv((npv + XT_INTERP - 1) / XT_INTERP);
+  const XSet x0 = xset(c->xco, 0), x1 = xset(c->xco, 1);
   prof_begin(c, PK_INTERPX);
-  k_interpx<<<(npu + XT_INTERP - 1) / XT_INTERP, XT_INTERP * 32, smem, c->stream>>>(c->dc, xset(c->xco, 0),
-                                                                                   c->f[OTBL_F_U], c->w.ux, 0, npu, Lp);
-  k_interpx<<<(npv + XT_INTERP - 1) / XT_INTERP, XT_INTERP * 32, smem, c->stream>>>(c->dc, xset(c->xco, 1),
-                                                                                   c->f[OTBL_F_V], c->w.vx, 1, npv, Lp);
-  k_interpx<<<(npu + XT_INTERP - 1) / XT_INTERP, XT_INTERP * 32, smem, c->stream>>>(c->dc, xset(c->xco, 1),
-                                                                                   c->f[OTBL_F_W], c->w.wx, 1, npu, Lp);
+  cudaFuncSetAttribute(k_interpx, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_interpx<<<gu, XT_INTERP * 32, smem, c->stream>>>(c->dc, x0, c->f[OTBL_F_U], c->w.ux, 0, npu, Lp);
+  k_interpx<<<gv, XT_INTERP * 32, smem, c->stream>>>(c->dc, x1, c->f[OTBL_F_V], c->w.vx, 1, npv, Lp);
+  k_interpx<<<gu, XT_INTERP * 32, smem, c->stream>>>(c->dc, x1, c->f[OTBL_F_W], c->w.wx, 1, npu, Lp);
   prof_end(c);
   c->launches += 3;
   return cudaGetLastError();
@@ -208,15 +213,14 @@ cudaError_t launch_difvisx(otbl_ctx *c) {
   const int npu = nz1 * (ny + 1), npv = nz1 * ny;
   const int Lp = nx | 1;
   const size_t smem = sizeof(double) * 2 * XT_DIFVIS * Lp;
-  cudaFuncSetAttribute(k_difvisx, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const int T = XT_DIFVIS * 32;
+  const dim3 gu((npu + XT_DIFVIS - 1) / XT_DIFVIS), gv((npv + XT_DIFVIS - 1) / XT_DIFVIS);
+  const XSet x0 = xset(c->xco, 0), x1 = xset(c->xco, 1);
   prof_begin(c, PK_DIFVISX);
-  k_difvisx<<<(npu + XT_DIFVIS - 1) / XT_DIFVIS, T, smem, c->stream>>>(c->dc, xset(c->xco, 0), c->w.uu, c->f[OTBL_F_U], c->w.cu, 0,
-                                                                      npu, Lp);
-  k_difvisx<<<(npv + XT_DIFVIS - 1) / XT_DIFVIS, T, smem, c->stream>>>(c->dc, xset(c->xco, 1), c->w.uv, c->f[OTBL_F_V], c->w.cv, 1,
-                                                                      npv, Lp);
-  k_difvisx<<<(npu + XT_DIFVIS - 1) / XT_DIFVIS, T, smem, c->stream>>>(c->dc, xset(c->xco, 1), c->w.uw, c->f[OTBL_F_W], c->w.cw, 1,
-                                                                      npu, Lp);
+  cudaFuncSetAttribute(k_difvisx, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_difvisx<<<gu, T, smem, c->stream>>>(c->dc, x0, c->w.uu, c->f[OTBL_F_U], c->w.cu, 0, npu, Lp);
+  k_difvisx<<<gv, T, smem, c->stream>>>(c->dc, x1, c->w.uv, c->f[OTBL_F_V], c->w.cv, 1, npv, Lp);
+  k_difvisx<<<gu, T, smem, c->stream>>>(c->dc, x1, c->w.uw, c->f[OTBL_F_W], c->w.cw, 1, npu, Lp);
   prof_end(c);
   c->launches += 3;
   return cudaGetLastError();

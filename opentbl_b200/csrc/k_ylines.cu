@@ -1,6 +1,6 @@
 // Wall-normal (y) line operators and the tail of rhsp on shared-memory tiles.
 //
-// A CTA owns one streamwise plane i and YT = 32 consecutive real indices kr
+// A CTA owns one streamwise plane i and YT consecutive real indices kr
 // (16 spanwise modes, re/im interleaved), all rows j. Eight lanes of a warp
 // share one column (chunked Thomas sweeps, lines.cuh); a warp holds four
 // columns. Tiles are filled with cp.async (every copy of a thread in flight
@@ -12,9 +12,12 @@
 
 namespace otbl {
 
-constexpr int YT = 32;      // columns per CTA
-constexpr int YNCH = 8;     // lanes per column
-constexpr int YTHREADS = 256;
+#ifndef OTBL_YT
+#define OTBL_YT 32
+#endif
+constexpr int YT = OTBL_YT;  // columns per CTA (a multiple of 4)
+constexpr int YNCH = 8;      // lanes per column
+constexpr int YTHREADS = YT * YNCH;
 constexpr int YB = 4;       // rows per batch of global reads
 
 struct YIdx {
@@ -57,12 +60,12 @@ __device__ __forceinline__ void ytile_load(double *t, const double *__restrict__
 // which 1 v-type (rows 0..ny-1). Then the solve with dcyu/dcyv.
 __device__ __forceinline__ void y_differzy(const DCoef &c, const YSet &ys, double *x, int h, int which) {
   const int ny = c.ny, jee = which == 0 ? ny + 1 : ny;
-  const int CL = chunk_len(jee, YNCH, true);
+  const int CL = ys.CL;
   const CCo<YNCH> E1(ys.k[YD_E1], h, CL), E2(ys.k[YD_E2], h, CL);
   const double *db = c.dcby;
   const int chv = which == 0 ? 3 : 1, cha = chv + 1;
   int s, e;
-  chunk_range<YNCH, true>(jee, h, s, e);
+  chunk_range(jee, h, ys.CL, s, e);
   double bot = 0.0, top = 0.0;
   if (s == 0 && e > s)
     bot = M4(db, chv, 1) * x[0] + M4(db, chv, 2) * x[1] + M4(db, chv, 3) * x[2] + M4(db, chv, 4) * x[3];
@@ -111,18 +114,18 @@ __device__ __forceinline__ void y_differzy(const DCoef &c, const YSet &ys, doubl
     }
   }
   __syncwarp();
-  solve_cco<YNCH, true>(x, jee, h, CCo<YNCH>(ys.k[YD_L], h, CL), CCo<YNCH>(ys.k[YD_D], h, CL),
+  solve_cco<YNCH>(x, jee, h, ys.CL, CCo<YNCH>(ys.k[YD_L], h, CL), CCo<YNCH>(ys.k[YD_D], h, CL),
                         CCo<YNCH>(ys.k[YD_U], h, CL));
 }
 
 // vistyy (lip.f90:447-513): which 0 u,w (jee = ny+1, ic = 3), which 1 v.
 __device__ __forceinline__ void y_vistyy(const DCoef &c, const YSet &ys, double *x, int h, int which) {
   const int ny = c.ny, jee = which == 0 ? ny + 1 : ny, ic = which == 0 ? 3 : 1;
-  const int CL = chunk_len(jee, YNCH, true);
+  const int CL = ys.CL;
   const CCo<YNCH> F1(ys.k[YV_F1], h, CL), F2(ys.k[YV_F2], h, CL), F3(ys.k[YV_F3], h, CL);
   const double *vb = c.cofvby;
   int s, e;
-  chunk_range<YNCH, true>(jee, h, s, e);
+  chunk_range(jee, h, ys.CL, s, e);
   double uprev = s > 0 ? x[s - 1] : 0.0;
   const double unext = e < jee ? x[e] : 0.0;
   double b0 = 0.0, bN = 0.0;
@@ -152,7 +155,7 @@ __device__ __forceinline__ void y_vistyy(const DCoef &c, const YSet &ys, double 
     uprev = uv[LB];
   }
   __syncwarp();
-  solve_cco<YNCH, true>(x, jee, h, CCo<YNCH>(ys.k[YV_L], h, CL), CCo<YNCH>(ys.k[YV_D], h, CL),
+  solve_cco<YNCH>(x, jee, h, ys.CL, CCo<YNCH>(ys.k[YV_L], h, CL), CCo<YNCH>(ys.k[YV_D], h, CL),
                         CCo<YNCH>(ys.k[YV_U], h, CL));
 }
 
@@ -164,11 +167,11 @@ __device__ __forceinline__ void y_vistyy(const DCoef &c, const YSet &ys, double 
 __device__ __forceinline__ void y_implzy(const DCoef &c, const YSet &ys, const double *res, double *out, int h,
                                          int which, double ub1, double ubj, const double *__restrict__ fac) {
   const int ny = c.ny, jee = which == 0 ? ny + 1 : ny, n = jee - 2;
-  const int CL = chunk_len(n, YNCH, true);
+  const int CL = ys.CL;
   const CCo<YNCH> F1(ys.k[YM_F1], h, CL), F2(ys.k[YM_F2], h, CL), F3(ys.k[YM_F3], h, CL);
   const double a1raw = fac[3 * (jee + 1)], a3raw = fac[3 * (jee + 1) + 1];
   int s, e;
-  chunk_range<YNCH, true>(n, h, s, e);
+  chunk_range(n, h, ys.CL, s, e);
   for (int q0 = s; q0 < e; q0 += LB) {
     double rv[LB + 2], f1[LB], f2[LB], f3[LB];
 #pragma unroll
@@ -192,7 +195,7 @@ __device__ __forceinline__ void y_implzy(const DCoef &c, const YSet &ys, const d
     }
   }
   __syncwarp();
-  solve_cco<YNCH, true>(out, n, h, CCo<YNCH>(ys.k[YM_L], h, CL), CCo<YNCH>(ys.k[YM_D], h, CL),
+  solve_cco<YNCH>(out, n, h, ys.CL, CCo<YNCH>(ys.k[YM_L], h, CL), CCo<YNCH>(ys.k[YM_D], h, CL),
                         CCo<YNCH>(ys.k[YM_U], h, CL));
 }
 
@@ -208,11 +211,11 @@ __global__ void __launch_bounds__(YTHREADS) k_interpy(DCoef c, YSet ys, const do
   __syncthreads();
   const YIdx q = yidx(nz1);
   double *x = sm + q.col * Lp;
-  const int CL = chunk_len(ny, YNCH, true);
+  const int CL = ys.CL;
   const CCo<YNCH> E1(ys.k[YI_E1], q.h, CL), E2(ys.k[YI_E2], q.h, CL);
   const double *ib = c.inby;
   int s, e;
-  chunk_range<YNCH, true>(ny, q.h, s, e);
+  chunk_range(ny, q.h, ys.CL, s, e);
   if (which == 0) {  // result(j) = e1(j) g(j) + e2(j) g(j+1), ascending
     const double gnext = x[e];  // e <= ny < jin
     double bN = 0.0;
@@ -262,7 +265,7 @@ __global__ void __launch_bounds__(YTHREADS) k_interpy(DCoef c, YSet ys, const do
     }
   }
   __syncwarp();
-  solve_cco<YNCH, true>(x, ny, q.h, CCo<YNCH>(ys.k[YI_L], q.h, CL), CCo<YNCH>(ys.k[YI_D], q.h, CL),
+  solve_cco<YNCH>(x, ny, q.h, ys.CL, CCo<YNCH>(ys.k[YI_L], q.h, CL), CCo<YNCH>(ys.k[YI_D], q.h, CL),
                         CCo<YNCH>(ys.k[YI_U], q.h, CL));
   __syncthreads();
   double *o = out + (size_t)(i - 1) * ny * nz1;
@@ -323,10 +326,10 @@ __global__ void __launch_bounds__(YTHREADS) k_final(DCoef c, YSet ys, FinalArgs 
   const double sgn = q.odd ? 1.0 : -1.0;  // (x * kaz) component = sgn * kz * x[partner]
 
   int s, e;
-  chunk_range<YNCH, true>(jee, q.h, s, e);
+  chunk_range(jee, q.h, ys.CL, s, e);
   // ---- RHS into tile 1 (rhsp.F90:164-169, 181-204, 351-418, 423-445)
   if (!last) y_differzy(c, ys, x1, q.h, COMP == 1 ? 1 : 0);
-  const CCo<YNCH> IDYY(ys.k[Y_IDYY], q.h, chunk_len(ny, YNCH, true));
+  const CCo<YNCH> IDYY(ys.k[Y_IDYY], q.h, ys.CL);
   for (int r0 = s; r0 < e; r0 += YB) {
     double cxv[YB], kpv[YB];
 #pragma unroll
@@ -486,10 +489,10 @@ __global__ void __launch_bounds__(YTHREADS) k_pois_solve(DCoef c, YSet ys, doubl
   const double *dcol = D + (q.col >> 1) * Lp;
   if (i == 2 && q.k == 0 && q.valid && q.h == 0) x[ny1 - 1] = 0.0;  // pois.f90:113
   __syncwarp();
-  const int CL = chunk_len(ny1, YNCH, true);
+  const int CL = ys.CL;
   const CCo<YNCH> A1(ys.k[YP_A1], q.h, CL), A3c(ys.k[YP_A3], q.h, CL);
-  chunk_tri<YNCH, true>(
-      x, ny1, q.h, [&](int r) { return -A1(r) * dcol[r - 1]; }, [&](int r) { return dcol[r]; },
+  chunk_tri<YNCH>(
+      x, ny1, q.h, CL, [&](int r) { return -A1(r) * dcol[r - 1]; }, [&](int r) { return dcol[r]; },
       [&](int r) { return A3c(r); });
   __syncthreads();
   for (int t = threadIdx.x; t < ny1 * YT; t += YTHREADS) {
@@ -503,7 +506,7 @@ __global__ void __launch_bounds__(YTHREADS) k_pois_solve(DCoef c, YSet ys, doubl
 // ---------------------------------------------------------------------------
 // Column pitch: odd, so 16 consecutive columns of one row fall in distinct
 // 8-byte banks (tile loads/stores), and, with chunk lengths = 2 mod 4
-// (chunk_range<.., true>), the 2-column x 8-chunk half-warp pattern of the
+// (chunk_len(.., true)), the 2-column x 8-chunk half-warp pattern of the
 // sweeps is conflict-free as well.
 static int ypitch(int rows) { return rows | 1; }
 

@@ -173,11 +173,10 @@ __global__ void __launch_bounds__(128) k_products(DCoef c, ZTab z, ProdArgs a) {
 // the y-line kernels (YM_L, YM_D, YM_U at fi, fi + len, fi + 2 len, row r =
 // j - 2); fac keeps the two boundary couplings that implzy moves to the
 // right-hand side (fac[3*(jee+1)] = a(2), fac[3*(jee+1)+1] = c(jee-1)).
-__device__ void implzy_factor(const DCoef &c, double *fac, double *fi, int which, double var1) {
-  const int ny = c.ny, jee = which == 0 ? ny + 1 : ny, n = jee - 2;
+__device__ void implzy_factor(const DCoef &c, double *fac, double *fi, int which, double var1, int CL) {
+  const int ny = c.ny, jee = which == 0 ? ny + 1 : ny;
   const double *icon = which == 0 ? c.vyui : c.vyvi;
   const double *econ = which == 0 ? c.cofvyu : c.cofvyv;
-  const int CL = chunk_len(n, 8, true);
   const size_t len = 8 * (size_t)CL;
   auto at = [&](int j) {
     const int r = j - 2;
@@ -206,8 +205,8 @@ __device__ void implzy_factor(const DCoef &c, double *fac, double *fi, int which
 // One CTA of 64 threads: the CFL reduction over the rows, then dt, the RK3
 // factors and the two implzy factorisations (one warp each).
 __global__ void __launch_bounds__(64) k_dt(DCoef c, DState *st, const unsigned long long *vm_bits, double *fac_u,
-                                           double *fac_v, double *fi_u, double *fi_v, int m, int setstep,
-                                           int dt_mode, double dt_fixed) {
+                                           double *fac_v, double *fi_u, double *fi_v, int ycl, int m,
+                                           int setstep, int dt_mode, double dt_fixed) {
   __shared__ double s_dt3[2], s_vmax[2];
   const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
   const double *S = c.S;
@@ -264,9 +263,9 @@ __global__ void __launch_bounds__(64) k_dt(DCoef c, DState *st, const unsigned l
   if (lane == 0) {
     const double rkk = *(volatile double *)&st->rkk;
     if (wid == 0)
-      implzy_factor(c, fac_u, fi_u, 0, rkk);
+      implzy_factor(c, fac_u, fi_u, 0, rkk, ycl);
     else
-      implzy_factor(c, fac_v, fi_v, 1, rkk);
+      implzy_factor(c, fac_v, fi_v, 1, rkk, ycl);
   }
 }
 
@@ -951,7 +950,7 @@ cudaError_t launch_products(otbl_ctx *c, int setstep) {
 cudaError_t launch_dt(otbl_ctx *c, int m, int setstep) {
   prof_begin(c, PK_DT);
   k_dt<<<1, 64, 0, c->stream>>>(c->dc, c->st, c->w.vm_bits, c->w.fac_u, c->w.fac_v, c->yco.fac[0],
-                                c->yco.fac[1], m, setstep, c->cfg.dt_mode, c->cfg.dt_fixed);
+                                c->yco.fac[1], c->yco.CL, m, setstep, c->cfg.dt_mode, c->cfg.dt_fixed);
   prof_end(c);
   c->launches += 1;
   return cudaGetLastError();

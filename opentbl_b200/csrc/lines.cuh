@@ -20,19 +20,20 @@ namespace otbl {
 
 constexpr int LB = 4;  // rows per batch in the sequential passes
 
-// Rows [s, e) of an n-row line owned by rank h of NCH. With EVEN the chunk
-// length is rounded up to 2 mod 4: eight chunk starts then fall in eight
-// distinct even banks, and with an odd column pitch the neighbouring column
-// takes the odd banks (a conflict-free half-warp of 2 columns x 8 chunks).
+// Chunk length for n rows over nch lanes. With `even` it is rounded up to
+// 2 mod 4: eight chunk starts then fall in eight distinct even banks, and
+// with an odd column pitch the neighbouring column takes the odd banks (a
+// conflict-free half-warp of 2 columns x 8 chunks).
 __host__ __device__ inline int chunk_len(int n, int nch, bool even) {
   int CL = (n + nch - 1) / nch;
   if (even) CL += (6 - (CL & 3)) & 3;
   return CL;
 }
 
-template <int NCH, bool EVEN>
-__device__ __forceinline__ void chunk_range(int n, int h, int &s, int &e) {
-  const int CL = chunk_len(n, NCH, EVEN);
+// Rows [s, e) of an n-row line owned by rank h when chunks are CL rows long
+// (one CL serves every operator of a kernel, so that all of them share the
+// chunk-interleaved coefficient layout).
+__device__ __forceinline__ void chunk_range(int n, int h, int CL, int &s, int &e) {
   s = min(n, h * CL);
   e = min(n, s + CL);
 }
@@ -41,10 +42,10 @@ __device__ __forceinline__ void chunk_range(int n, int h, int &s, int &e) {
 //   forward  y_0 = b_0,  y_r = b_r + A(r) y_{r-1}
 //   backward x_{n-1} = C(n-1) y_{n-1},  x_r = C(r) (y_r - U(r) x_{r+1})
 // All 32 lanes of the warp must call this (shuffles use the full mask).
-template <int NCH, bool EVEN, class FA, class FC, class FU>
-__device__ __forceinline__ void chunk_tri(double *x, int n, int h, FA A, FC C, FU U) {
+template <int NCH, class FA, class FC, class FU>
+__device__ __forceinline__ void chunk_tri(double *x, int n, int h, int CL, FA A, FC C, FU U) {
   int s, e;
-  chunk_range<NCH, EVEN>(n, h, s, e);
+  chunk_range(n, h, CL, s, e);
   // ---- forward, local (y_{s-1} = 0)
   double z = 0.0, G = (h == 0) ? 0.0 : 1.0;
   for (int r0 = s; r0 < e; r0 += LB) {
@@ -146,27 +147,11 @@ __device__ __forceinline__ void chunk_tri(double *x, int n, int h, FA A, FC C, F
   }
 }
 
-// Pre-factored Fortran (3, n) coefficient array, rows 1-based: local row r
-// is Fortran row r + 1 + off.
-struct Icon {
-  const double *a;
-  int off;
-  __device__ __forceinline__ double l(int r) const { return __ldg(a + (size_t)(r + off) * 3 + 0); }
-  __device__ __forceinline__ double d(int r) const { return __ldg(a + (size_t)(r + off) * 3 + 1); }
-  __device__ __forceinline__ double u(int r) const { return __ldg(a + (size_t)(r + off) * 3 + 2); }
-};
-
-template <int NCH, bool EVEN>
-__device__ __forceinline__ void solve_icon(double *x, int n, int h, Icon ic) {
-  chunk_tri<NCH, EVEN>(
-      x, n, h, [&](int r) { return ic.l(r); }, [&](int r) { return ic.d(r); }, [&](int r) { return ic.u(r); });
-}
-
 // A per-row coefficient in chunk-interleaved order: the value for row r of
 // chunk h (rows [h*CL, (h+1)*CL)) sits at (r - h*CL)*NCH + h. The lanes of a
 // warp step through their chunks in lockstep, so one warp request reads NCH
 // consecutive doubles instead of NCH rows spread over as many cache lines.
-// The host builds these copies with the CL of chunk_len().
+// The host builds these copies with the kernel's CL.
 template <int NCH>
 struct CCo {
   const double *a;
@@ -175,9 +160,9 @@ struct CCo {
   __device__ __forceinline__ double operator()(int r) const { return __ldg(a + r * NCH + base); }
 };
 
-template <int NCH, bool EVEN>
-__device__ __forceinline__ void solve_cco(double *x, int n, int h, CCo<NCH> L, CCo<NCH> D, CCo<NCH> U) {
-  chunk_tri<NCH, EVEN>(x, n, h, L, D, U);
+template <int NCH>
+__device__ __forceinline__ void solve_cco(double *x, int n, int h, int CL, CCo<NCH> L, CCo<NCH> D, CCo<NCH> U) {
+  chunk_tri<NCH>(x, n, h, CL, L, D, U);
 }
 
 }  // namespace otbl

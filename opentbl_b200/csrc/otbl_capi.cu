@@ -47,10 +47,9 @@ size_t field_len(const otbl_ctx *c, int id) {
 }
 
 // Chunk-interleaved copy (lines.cuh CCo) of f(r), r = 0..n-1, for nch lanes
-// per line; rows past n are 0 and never read.
+// per line and chunks of CL rows; rows past n are 0 and never read.
 template <class F>
-void interleave(double *dst, int n, int nch, bool even, F f) {
-  const int CL = chunk_len(n, nch, even);
+void interleave(double *dst, int n, int nch, int CL, F f) {
   for (int h = 0; h < nch; ++h)
     for (int t = 0; t < CL; ++t) {
       const int r = h * CL + t;
@@ -62,7 +61,7 @@ void interleave(double *dst, int n, int nch, bool even, F f) {
 // chunk-interleaved order of the x-line kernels (32 lanes per line).
 int build_xco(otbl_ctx *c, const otbl_coef_offsets &o) {
   const int nx = c->cfg.nx;
-  const int CL = chunk_len(nx, 32, false);
+  const int CL = xline_cl(nx);
   const size_t len = (size_t)CL * 32;
   double *dev = nullptr;
   int st = dalloc(c, &dev, 2 * (size_t)XCO_N * len);
@@ -79,7 +78,7 @@ int build_xco(otbl_ctx *c, const otbl_coef_offsets &o) {
     const double *cofc = F(which == 0 ? OTBL_C_COFCXU : OTBL_C_COFCXV);
     const double *cofv = F(which == 0 ? OTBL_C_COFVXU : OTBL_C_COFVXV);
     double *base = h.data() + (size_t)which * XCO_N * len;
-    auto put = [&](int kind, auto f) { interleave(base + (size_t)kind * len, nx, 32, false, f); };
+    auto put = [&](int kind, auto f) { interleave(base + (size_t)kind * len, nx, 32, CL, f); };
     // solves: row r (0-based) uses Fortran column r + 1 of the (3, nx) array
     for (int q = 0; q < 3; ++q) {
       put(XI_L + q, [&](int r) { return inx[(size_t)r * 3 + q]; });
@@ -117,11 +116,12 @@ int yco_rows(int kind, int which, int ny) {
 // rewritten by k_dt every substep.
 int build_yco(otbl_ctx *c, const otbl_coef_offsets &o) {
   const int ny = c->cfg.ny;
+  const int CL = yline_cl(ny);
   size_t off[2][YCO_N], total = 0;
   for (int which = 0; which < 2; ++which)
     for (int k = 0; k < YCO_N; ++k) {
       off[which][k] = total;
-      total += 8 * (size_t)chunk_len(yco_rows(k, which, ny), 8, true);
+      total += 8 * (size_t)CL;
     }
   double *dev = nullptr;
   int st = dalloc(c, &dev, total);
@@ -141,7 +141,7 @@ int build_yco(otbl_ctx *c, const otbl_coef_offsets &o) {
     const double *vyi = F(which == 0 ? OTBL_C_VYUI : OTBL_C_VYVI);
     const double *ayp = F(OTBL_C_AYP), *idyy = F(OTBL_C_IDYY);
     auto put = [&](int kind, auto f) {
-      interleave(h.data() + off[which][kind], yco_rows(kind, which, ny), 8, true, f);
+      interleave(h.data() + off[which][kind], yco_rows(kind, which, ny), 8, CL, f);
     };
     for (int q = 0; q < 3; ++q) {
       put(YI_L + q, [&](int r) { return iny[(size_t)r * 3 + q]; });
@@ -160,6 +160,7 @@ int build_yco(otbl_ctx *c, const otbl_coef_offsets &o) {
     for (int k = 0; k < YCO_N; ++k) c->yco.k[which][k] = dev + off[which][k];
     c->yco.fac[which] = dev + off[which][YM_L];
   }
+  c->yco.CL = CL;
   if (cudaMemcpy(dev, h.data(), total * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
     c->err = "coefficient upload failed";
     return OTBL_ERR_CUDA;

@@ -29,7 +29,7 @@ struct DCoef {
 };
 
 // Chunk-interleaved copies (lines.cuh CCo) of the x-line coefficients, for
-// 32 lanes per line and CL = chunk_len(nx, 32, false). Index [which][kind]:
+// 32 lanes per line and chunks of CL rows (xline_cl). Index [which][kind]:
 // which 0 = u, 1 = v,w (lip.f90 chi/chv selections).
 enum XCoKind {
   XI_L, XI_D, XI_U,          // interpxx solve: inxu / inxv
@@ -57,9 +57,10 @@ inline XSet xset(const XCo &x, int which) {
 }
 
 // Chunk-interleaved copies of the y-line coefficients, for 8 lanes per
-// column and CL = chunk_len(n, 8, true) with the n of each operator (jee =
-// ny+1 for u-type, ny for v-type). Index [which][kind]: which 0 = u,w,
-// 1 = v (interpyy: 0 = u,w input, 1 = v input).
+// column and one chunk length CL = yline_cl(ny) for every operator (the
+// operators have ny-1 .. ny+1 rows; jee = ny+1 for u-type, ny for v-type).
+// Index [which][kind]: which 0 = u,w, 1 = v (interpyy: 0 = u,w input,
+// 1 = v input).
 enum YCoKind {
   YI_L, YI_D, YI_U,           // interpyy solve: inyu / inyv, n = ny
   YI_E1, YI_E2,               // cofiuy / cofivy at clamp(r+1, 2, ny-1)
@@ -75,15 +76,27 @@ enum YCoKind {
 };
 struct YCo {
   const double *k[2][YCO_N];
-  double *fac[2];  // YM_L of each which; YM_D, YM_U follow at +len, +2 len
+  double *fac[2];  // YM_L of each which; YM_D, YM_U follow at +8 CL, +16 CL
+  int CL;
 };
 struct YSet {
   const double *k[YCO_N];
+  int CL;
 };
 inline YSet yset(const YCo &y, int which) {
   YSet s;
   for (int q = 0; q < YCO_N; ++q) s.k[q] = y.k[which][q];
+  s.CL = y.CL;
   return s;
+}
+
+// Chunk lengths: 32 lanes per x-line; 8 lanes per y-column with one length
+// for all y operators, rounded to 2 mod 4 (lines.cuh chunk_len).
+inline int xline_cl(int nx) { return (nx + 31) / 32; }
+inline int yline_cl(int ny) {  // 8 lanes, rows up to ny+1, 2 mod 4
+  int c = (ny + 1 + 7) / 8;
+  c += (6 - (c & 3)) & 3;
+  return c;
 }
 
 // Scalars that live on the device so that no host synchronisation is needed

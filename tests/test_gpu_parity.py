@@ -138,6 +138,20 @@ def test_c1_divergence_after_transient():
     assert dg <= 1e-12
 
 
+@pytest.mark.parametrize("cfg", [
+    replace(config.TINY, nx=17, ny=300, name="tall-17x300x32"),     # y chunks of 38 rows
+    replace(config.TINY, nx=1081, name="long-1081x41x32"),          # x chunks of 34 rows
+], ids=lambda c: c.name)
+def test_shared_memory_fallback_paths(cfg):
+    """Grids whose line chunks are longer than the register kernels are
+    compiled for take the shared-memory sweeps; same bound as the main path."""
+    g, o, init, coef = _pair(cfg)
+    g.substep(1, True)
+    o.substep(1, 1)
+    e = _compare(g, o)
+    assert max(e.values()) <= 1e-11, e
+
+
 def test_genflu_standalone():
     """otbl_genflu (genflu.F90:3-167) against the oracle on the same state:
     plane xout recycled into plane 1, the filtered mean um and the integral
