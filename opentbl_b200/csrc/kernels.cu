@@ -166,6 +166,226 @@ __global__ void __launch_bounds__(128) k_products(DCoef c, ZTab z, ProdArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// k_products for M = nz/2 = 256 (nz = 512): the transforms and products of
+// k_products with each line kept in registers between the inverse
+// transform's last Stockham pass and the forward transform's first one.
+// Register layout L: lane t holds complex element n = t + 32 m in v[m],
+// m < E = M/32. Passes: radix 8 (Ns = 1), radix 8 (Ns = 8), radix R3
+// (Ns = 64); the first reads L, the last writes L, the two in between go
+// through a per-warp shared buffer whose index i is stored at i + i/8, which
+// makes every pass conflict-free. The arithmetic is warp_fft's, operation
+// for operation.
+// ---------------------------------------------------------------------------
+template <int M>
+struct ZPlan {
+  static constexpr int E = M / 32;
+  static constexpr int R3 = 4;  // 256 = 8 x 8 x 4
+};
+__device__ __forceinline__ int zpad(int i) { return i + (i >> 3); }
+
+// inverse (SIGN = +1) or forward (SIGN = -1) FFT of a line in layout L
+template <int M, int SIGN>
+__device__ __forceinline__ void zfft_regs(double2 (&L)[M / 32], double2 *buf, const double2 *__restrict__ tw,
+                                          int t) {
+  constexpr int E = M / 32, R3 = ZPlan<M>::R3;
+  constexpr int IA = E / 8;  // radix-8 items per lane in the first two passes
+  // pass A: radix 8, Ns = 1, input from registers
+#pragma unroll
+  for (int it = 0; it < IA; ++it) {
+    double2 v[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) v[r] = L[it + r * IA];
+    dft_small<8, SIGN>(v);
+    const int j = t + 32 * it;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) buf[zpad(j * 8 + r)] = v[r];
+  }
+  __syncwarp();
+  // pass B: radix 8, Ns = 8
+  {
+    double2 v[IA][8];
+#pragma unroll
+    for (int it = 0; it < IA; ++it) {
+      const int j = t + 32 * it;
+#pragma unroll
+      for (int r = 0; r < 8; ++r) v[it][r] = buf[zpad(j + r * (M / 8))];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int it = 0; it < IA; ++it) {
+      const int j = t + 32 * it, k = j % 8;
+#pragma unroll
+      for (int r = 1; r < 8; ++r) {
+        double2 w = __ldg(&tw[r * k * (M / 64)]);
+        if (SIGN > 0) w.y = -w.y;
+        v[it][r] = cmul(v[it][r], w);
+      }
+      dft_small<8, SIGN>(v[it]);
+      const int base = (j / 8) * 64 + k;
+#pragma unroll
+      for (int r = 0; r < 8; ++r) buf[zpad(base + r * 8)] = v[it][r];
+    }
+  }
+  __syncwarp();
+  // pass C: radix R3, Ns = 64 (= M/R3), output to registers
+  {
+    constexpr int IC = (M / R3) / 32;
+    double2 v[IC][R3];
+#pragma unroll
+    for (int it = 0; it < IC; ++it) {
+      const int j = t + 32 * it;
+#pragma unroll
+      for (int r = 0; r < R3; ++r) v[it][r] = buf[zpad(j + r * (M / R3))];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int it = 0; it < IC; ++it) {
+      const int j = t + 32 * it;  // k = j mod 64 = j, twiddle stride M/(64 R3) = 1
+#pragma unroll
+      for (int r = 1; r < R3; ++r) {
+        double2 w = __ldg(&tw[r * j]);
+        if (SIGN > 0) w.y = -w.y;
+        v[it][r] = cmul(v[it][r], w);
+      }
+      dft_small<R3, SIGN>(v[it]);
+#pragma unroll
+      for (int r = 0; r < R3; ++r) L[it + r * IC] = v[it][r];
+    }
+  }
+}
+
+// c2r of fou (modes 0..nz2, global) into layout L (physical values packed
+// as complex), the line_c2r pre-step followed by the inverse FFT
+template <int M>
+__device__ __forceinline__ void zc2r_regs(const ZTab &z, const double *__restrict__ fou, double2 (&L)[M / 32],
+                                          double2 *buf, int t) {
+  constexpr int E = M / 32;
+  const int nz2 = z.nz2;
+  const double2 *f2 = reinterpret_cast<const double2 *>(fou);
+  double2 a[E], b[E];
+#pragma unroll
+  for (int m = 0; m < E; ++m) {
+    const int k = t + 32 * m, km = M - k;
+    a[m] = __ldg(f2 + min(k, nz2));
+    b[m] = __ldg(f2 + min(km, nz2));
+  }
+#pragma unroll
+  for (int m = 0; m < E; ++m) {
+    const int k = t + 32 * m, km = M - k;
+    double2 aa = k <= nz2 ? a[m] : make_double2(0.0, 0.0);
+    if (k == 0) aa.y = 0.0;  // c2r ignores Im X[0]
+    double2 bb = km <= nz2 ? b[m] : make_double2(0.0, 0.0);
+    bb.y = -bb.y;
+    const double2 s = cadd(aa, bb), d = csub(aa, bb);
+    const double2 tt = cmul(cconj(__ldg(z.tw2 + k)), d);  // W^{-k} d
+    L[m] = make_double2(s.x - tt.y, s.y + tt.x);          // s + i t
+  }
+  zfft_regs<M, 1>(L, buf, z.tw, t);
+}
+
+// r2c of layout L (physical values packed as complex) into fou (modes
+// 0..nz2) x 1/nz: forward FFT, then the line_r2c post-step
+template <int M>
+__device__ __forceinline__ void zr2c_regs(const ZTab &z, double2 (&L)[M / 32], double *__restrict__ fou,
+                                          double2 *buf, int t) {
+  constexpr int E = M / 32;
+  zfft_regs<M, -1>(L, buf, z.tw, t);
+  __syncwarp();
+#pragma unroll
+  for (int m = 0; m < E; ++m) buf[zpad(t + 32 * m)] = L[m];
+  __syncwarp();
+  const int nz2 = z.nz2;
+  const double dnf = 1.0 / (double)z.nz;
+  double2 *f2 = reinterpret_cast<double2 *>(fou);
+#pragma unroll
+  for (int m = 0; m < E; ++m) {
+    const int k = t + 32 * m;
+    if (k <= nz2) {
+      const double2 zk = L[m];
+      const double2 zc = cconj(buf[zpad((M - k) & (M - 1))]);
+      const double2 e = make_double2(0.5 * (zk.x + zc.x), 0.5 * (zk.y + zc.y));
+      const double2 d = csub(zk, zc);
+      const double2 o = make_double2(0.5 * d.y, -0.5 * d.x);  // -i d / 2
+      const double2 xk = cadd(e, cmul(__ldg(z.tw2 + k), o));
+      f2[k] = make_double2(dnf * xk.x, dnf * xk.y);
+    }
+  }
+  __syncwarp();
+}
+
+template <int E>
+__device__ __forceinline__ void regs_mul(double2 (&a)[E], const double2 (&b)[E]) {
+#pragma unroll
+  for (int m = 0; m < E; ++m) a[m] = make_double2(a[m].x * b[m].x, a[m].y * b[m].y);
+}
+template <int E>
+__device__ __forceinline__ void regs_sq(double2 (&a)[E]) {
+#pragma unroll
+  for (int m = 0; m < E; ++m) a[m] = make_double2(a[m].x * a[m].x, a[m].y * a[m].y);
+}
+template <int E>
+__device__ __forceinline__ double regs_absmax(const double2 (&a)[E]) {
+  double mx = 0.0;
+#pragma unroll
+  for (int m = 0; m < E; ++m) mx = nmax(nmax(mx, fabs(a[m].x)), fabs(a[m].y));
+  return mx;
+}
+
+template <int M>
+__global__ void __launch_bounds__(128) k_products_r(DCoef c, ZTab z, ProdArgs a) {
+  extern __shared__ double2 sm[];
+  constexpr int E = M / 32;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int j = blockIdx.x * 4 + wid + 1;
+  const int i = blockIdx.y + 1;
+  const int nx = c.nx, ny = c.ny, nz1 = c.nz1;
+  if (j > ny + 1) return;
+  double2 *buf = sm + (size_t)wid * (M + M / 8);
+  const size_t offu = ((size_t)(i - 1) * (ny + 1) + (j - 1)) * nz1;
+  const size_t offv = ((size_t)(i - 1) * ny + (j - 1)) * nz1;
+  double mu = 0.0, mw = 0.0, mv = 0.0;
+  double2 A[E], B[E];
+  zc2r_regs<M>(z, a.ux + offu, A, buf, lane);  // uu = ux^2
+  regs_sq<E>(A);
+  zr2c_regs<M>(z, A, a.uu + offu, buf, lane);
+  zc2r_regs<M>(z, a.u + offu, B, buf, lane);   // uw = wx u
+  if (a.setstep) mu = regs_absmax<E>(B);
+  zc2r_regs<M>(z, a.wx + offu, A, buf, lane);
+  if (a.setstep) mw = regs_absmax<E>(A);
+  regs_mul<E>(A, B);
+  zr2c_regs<M>(z, A, a.uw + offu, buf, lane);
+  if (j <= ny) {
+    zc2r_regs<M>(z, a.vx + offv, A, buf, lane);  // uv = vx uy
+    if (a.setstep) mv = regs_absmax<E>(A);
+    zc2r_regs<M>(z, a.uy + offv, B, buf, lane);
+    regs_mul<E>(A, B);
+    zr2c_regs<M>(z, A, a.uv + offv, buf, lane);
+    if (i >= 2 && i <= nx - 1) {
+      zc2r_regs<M>(z, a.v + offv, A, buf, lane);  // vw = v wy
+      zc2r_regs<M>(z, a.wy + offv, B, buf, lane);
+      regs_mul<E>(A, B);
+      zr2c_regs<M>(z, A, a.vw + offv, buf, lane);
+      zc2r_regs<M>(z, a.vy + offv, A, buf, lane);  // vv = vy^2
+      regs_sq<E>(A);
+      zr2c_regs<M>(z, A, a.vv + offv, buf, lane);
+      zc2r_regs<M>(z, a.w + offu, A, buf, lane);  // ww = w^2
+      regs_sq<E>(A);
+      zr2c_regs<M>(z, A, a.ww + offv, buf, lane);
+    }
+  }
+  if (a.setstep) {
+    mu = warp_nmax(mu);
+    mw = warp_nmax(mw);
+    mv = warp_nmax(mv);
+    if (lane == 0) {
+      atomicMax(&a.st->umax_bits, (unsigned long long)__double_as_longlong(mu));
+      atomicMax(&a.st->wmax_bits, (unsigned long long)__double_as_longlong(mw));
+      if (j <= ny) atomicMax(&a.vm_bits[j], (unsigned long long)__double_as_longlong(mv));
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // dt (rhsp.F90:214-267), RK3 factors, implzy LU (lip.f90:545-568)
 // ---------------------------------------------------------------------------
 // LU of (A + var1*B) for implzy, lip.f90:545-568, rows j = 2..jee-1, as a
@@ -937,11 +1157,16 @@ cudaError_t launch_products(otbl_ctx *c, int setstep) {
   a.st = c->st;
   a.setstep = setstep;
   const int M = c->cfg.nz / 2;
-  const size_t smem = (size_t)4 * 3 * M * sizeof(double2);
-  cudaFuncSetAttribute(k_products, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   dim3 g((c->cfg.ny + 1 + 3) / 4, c->cfg.nx);
   prof_begin(c, PK_PRODUCTS);
-  k_products<<<g, 128, smem, c->stream>>>(c->dc, ztab(c), a);
+  if (M == 256) {
+    const size_t smem = (size_t)4 * (M + M / 8) * sizeof(double2);
+    k_products_r<256><<<g, 128, smem, c->stream>>>(c->dc, ztab(c), a);
+  } else {
+    const size_t smem = (size_t)4 * 3 * M * sizeof(double2);
+    cudaFuncSetAttribute(k_products, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_products<<<g, 128, smem, c->stream>>>(c->dc, ztab(c), a);
+  }
   prof_end(c);
   c->launches += 1;
   return cudaGetLastError();

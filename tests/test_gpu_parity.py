@@ -152,6 +152,24 @@ def test_shared_memory_fallback_paths(cfg):
     assert max(e.values()) <= 1e-11, e
 
 
+def test_register_products_path():
+    """nz = 512 (M = nz/2 = 256) runs the register-pipelined spanwise
+    transforms of k_products; one substep and one step against the oracle."""
+    cfg = replace(config.TINY, nx=17, nz=512, name="wide-17x41x512")
+    g, o, init, coef = _pair(cfg)
+    g.substep(1, True)
+    o.substep(1, 1)
+    e = _compare(g, o)
+    assert max(e.values()) <= 1e-11, e
+    g.substep(2, False)
+    g.substep(3, False)
+    o.substep(2, 0)
+    o.substep(3, 0)
+    e = _compare(g, o)
+    assert max(e.values()) <= 1e-10, e
+    assert abs(g.inflow()[1]["umax"] - o.inflow()[1]["umax"]) <= 1e-14 * o.inflow()[1]["umax"]
+
+
 def test_genflu_standalone():
     """otbl_genflu (genflu.F90:3-167) against the oracle on the same state:
     plane xout recycled into plane 1, the filtered mean um and the integral
