@@ -7,6 +7,8 @@
 // at once); global reads that feed element-wise steps are issued four rows
 // at a time.
 #include "devcommon.cuh"
+#include <type_traits>
+
 #include "lines.cuh"
 #include "otbl_internal.cuh"
 
@@ -19,6 +21,14 @@ constexpr int YT = OTBL_YT;  // columns per CTA (a multiple of 4)
 constexpr int YNCH = 8;      // lanes per column
 constexpr int YTHREADS = YT * YNCH;
 constexpr int YB = 4;       // rows per batch of global reads
+
+// a chunk-interleaved coefficient (lines.cuh CCo) addressed by the chunk
+// offset t of lane h: entry t*YNCH + h
+struct RCo8 {
+  const double *p;
+  __device__ __forceinline__ RCo8(const double *a, int h) : p(a + h) {}
+  __device__ __forceinline__ double operator()(int t) const { return __ldg(p + t * YNCH); }
+};
 
 struct YIdx {
   int col, h, kr, k, odd, pof;
@@ -440,6 +450,308 @@ __global__ void __launch_bounds__(YTHREADS) k_final(DCoef c, YSet ys, FinalArgs 
 }
 
 // ---------------------------------------------------------------------------
+// Fixed-length chunks (CL a compile-time constant, one of kYFixCL). Columns
+// are padded to YNCH*CL rows; rows past an operator's n hold zeros and have
+// zero coefficients (A of row 0 and U of row n-1 are stored as 0 too), so
+// every lane runs exactly CL unrolled steps with constant shared-memory
+// offsets and no per-row predicate. Each operator's right-hand side is formed
+// inside its forward sweep, the forward fix-up is applied inside the
+// backward sweep (prefix products g[] in registers), and the backward fix-up
+// inside the pass that consumes the result (suffix products hh[]), so a
+// stencil + solve is three passes over the column instead of five. The
+// arithmetic is chunk_tri's, step for step.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void scan_up8(double &z, double &G, int h) {
+#pragma unroll
+  for (int d = 1; d < YNCH; d <<= 1) {
+    const double zp = __shfl_up_sync(0xffffffffu, z, d, YNCH);
+    const double Gp = __shfl_up_sync(0xffffffffu, G, d, YNCH);
+    if (h >= d) {
+      z = z + G * zp;
+      G = G * Gp;
+    }
+  }
+}
+__device__ __forceinline__ void scan_down8(double &w, double &H, int h) {
+#pragma unroll
+  for (int d = 1; d < YNCH; d <<= 1) {
+    const double wn = __shfl_down_sync(0xffffffffu, w, d, YNCH);
+    const double Hn = __shfl_down_sync(0xffffffffu, H, d, YNCH);
+    if (h + d < YNCH) {
+      w = w + H * wn;
+      H = H * Hn;
+    }
+  }
+}
+
+// rows [0, YNCH*CL) of the YT columns at kr0; rows past `rows` (and columns
+// past nz1) are zero-filled
+template <int CL>
+__device__ __forceinline__ void ytile_load_pad(double *t, const double *__restrict__ g, int rows, int nz1, int kr0,
+                                               int Lp) {
+  for (int e = threadIdx.x; e < YNCH * CL * YT; e += YTHREADS) {
+    const int j0 = e / YT, col = e - j0 * YT, kr = kr0 + col;
+    const bool ok = kr < nz1 && j0 < rows;
+    cp_async8(t + col * Lp + j0, ok ? g + (size_t)j0 * nz1 + kr : g, ok);
+  }
+}
+
+// Forward sweep of the chunk at x (rows s..s+CL-1) with the right-hand side
+// rhs(t, x[t-1], x[t], x[t+1]) of the original values; z_t = rhs + A(t)
+// z_{t-1}. Leaves the local z in x, the prefix products in g and the carried
+// value Yp of the preceding chunks.
+template <int CL, class FS, class FA>
+__device__ __forceinline__ void fx_forward(double *x, int h, FS rhs, FA A, double (&g)[CL], double &Yp) {
+  const double xm = h > 0 ? x[-1] : 0.0;
+  const double xp = h < YNCH - 1 ? x[CL] : 0.0;
+  __syncwarp();
+  double prv = xm, z = 0.0, G = h == 0 ? 0.0 : 1.0;
+#pragma unroll
+  for (int t = 0; t < CL; ++t) {
+    const double cur = x[t];
+    const double nxt = t + 1 < CL ? x[t + 1 < CL ? t + 1 : t] : xp;
+    const double b = rhs(t, prv, cur, nxt);
+    const double a = A(t);
+    z = b + a * z;
+    G = G * a;
+    g[t] = G;
+    x[t] = z;
+    prv = cur;
+  }
+  scan_up8(z, G, h);
+  Yp = __shfl_up_sync(0xffffffffu, z, 1, YNCH);
+  if (h == 0) Yp = 0.0;
+}
+
+// Backward sweep with the forward fix-up y = z + g Yp folded in; leaves the
+// local w in x, the suffix products in hh and the carried Xn: the solution
+// of row t is x[t] + hh[t] * Xn.
+template <int CL, class FC, class FU>
+__device__ __forceinline__ void fx_backward(double *x, int h, const double (&g)[CL], double Yp, FC C, FU U,
+                                            double (&hh)[CL], double &Xn) {
+  double w = 0.0, H = 1.0;
+#pragma unroll
+  for (int t = CL - 1; t >= 0; --t) {
+    const double y = x[t] + g[t] * Yp;
+    const double cv = C(t);
+    const double m = cv * (-U(t));
+    w = cv * y + m * w;
+    H = H * m;
+    hh[t] = H;
+    x[t] = w;
+  }
+  scan_down8(w, H, h);
+  Xn = __shfl_down_sync(0xffffffffu, w, 1, YNCH);
+  if (h == YNCH - 1) Xn = 0.0;
+}
+
+template <int COMP, int CL>  // 0: u, 1: v, 2: w
+__global__ void __launch_bounds__(YTHREADS, 2) k_final_f(DCoef c, YSet ys, FinalArgs a, int Lp) {
+  extern __shared__ double sm[];
+  const int nx = c.nx, ny = c.ny, nz1 = c.nz1;
+  const int i = blockIdx.y + 2, kr0 = blockIdx.x * YT;
+  const bool last = i == nx;
+  const YIdx q = yidx(nz1);
+  const int h = q.h, s = h * CL;
+  const int jee = COMP == 1 ? ny : ny + 1;
+  const size_t PU = (size_t)(ny + 1) * nz1, PV = (size_t)ny * nz1;
+  const size_t pl = (size_t)(i - 1) * (COMP == 1 ? PV : PU);
+  const size_t plv = (size_t)(i - 1) * PV;
+  double *T1 = sm, *T2 = sm + YT * Lp;
+  const double *prod = COMP == 0 ? a.uv : (COMP == 1 ? a.vv : a.vw);
+  const double *kprod = COMP == 0 ? a.uw : (COMP == 1 ? a.vw : a.ww);
+  const int krows = COMP == 0 ? ny + 1 : ny;
+  double *vel = COMP == 0 ? a.u : (COMP == 1 ? a.v : a.w);
+  if (!last) ytile_load_pad<CL>(T1, prod + plv, ny, nz1, kr0, Lp);
+  ytile_load_pad<CL>(T2, vel + pl, jee, nz1, kr0, Lp);
+  cp_async_wait_all();
+  __syncthreads();
+  double *c1 = T1 + q.col * Lp, *c2 = T2 + q.col * Lp;
+  double *x1 = c1 + s, *x2 = c2 + s;
+  const int kc = q.valid ? q.kr : 0;
+  const double *cX = (COMP == 0 ? a.cu : (COMP == 1 ? a.cv : a.cw)) + pl + kc;
+  const double *kp = kprod + (COMP == 0 ? pl : plv) + kc + (q.valid ? q.pof : 1);
+  double *hp = (COMP == 0 ? a.rhsupa : (COMP == 1 ? a.rhsvpa : a.rhswpa)) + pl + kc;
+  const double *velg = vel + pl + kc;
+  const double *pc = a.p + plv + kc;
+  const double kz = c.kaz[q.k], kv = c.kvis[q.k];
+  const double var1 = a.st->var1, var3 = a.st->var3, var4 = a.st->var4;
+  const double v2 = last ? 0.0 : a.st->var2;
+  const double idxx = c.S[OTBL_S_IDXX];
+  const double *ib = c.inby, *cc = c.ccon;
+  const double sgn = q.odd ? 1.0 : -1.0;  // (x * kaz) component = sgn * kz * x[partner]
+  const int ppof = q.valid ? q.pof : 1;
+  const size_t pnext = last ? 0 : PV;
+  double g[CL], hh[CL];
+  double Yp = 0.0, Xn = 0.0;
+  // ---- differzy of the product (lip.f90:152-232) into x1
+  if (!last) {
+    const int which = COMP == 1 ? 1 : 0;
+    const double *db = c.dcby;
+    const int chv = which == 0 ? 3 : 1, cha = chv + 1;
+    const double bot = M4(db, chv, 1) * c1[0] + M4(db, chv, 2) * c1[1] + M4(db, chv, 3) * c1[2] + M4(db, chv, 4) * c1[3];
+    const double top = M4(db, cha, 1) * c1[ny - 1] + M4(db, cha, 2) * c1[ny - 2] + M4(db, cha, 3) * c1[ny - 3] +
+                       M4(db, cha, 4) * c1[ny - 4];
+    const RCo8 E1(ys.k[YD_E1], h), E2(ys.k[YD_E2], h);
+    fx_forward<CL>(
+        x1, h,
+        [&](int t, double pv, double cu, double nx_) {
+          const int r = s + t;
+          const double in = which == 0 ? E2(t) * cu + E1(t) * pv : E2(t) * nx_ + E1(t) * cu;
+          return r == 0 ? bot : (r == jee - 1 ? top : (r < jee ? in : 0.0));
+        },
+        RCo8(ys.k[YD_L], h), g, Yp);
+    fx_backward<CL>(x1, h, g, Yp, RCo8(ys.k[YD_D], h), RCo8(ys.k[YD_U], h), hh, Xn);
+  }
+  // ---- RHS assembly (rhsp.F90:164-169, 181-204, 351-418, 423-445) with the
+  // differzy fix-up folded in
+#pragma unroll
+  for (int t = 0; t < CL; ++t) {
+    const int r = s + t, rr = min(r, jee - 1), j = r + 1;
+    const double d1 = last ? 0.0 : x1[t] + hh[t] * Xn;
+    double R = __ldg(cX + (size_t)rr * nz1);
+    const double kpv = (!last && (COMP != 2 || r < ny)) ? __ldg(kp + (size_t)min(rr, krows - 1) * nz1) : 0.0;
+    const double kzt = sgn * kz * kpv;
+    if (COMP == 0) {
+      if (!last) {
+        R = (d1 + kzt) + R;
+        if (j >= 2 && j <= ny) R = R - x2[t] * kv;
+      }
+    } else if (COMP == 1) {
+      if (!last) {
+        if (j >= 2 && j <= ny - 1) R = R - x2[t] * kv;
+        R = R + kzt;
+        R = R + d1;
+      }
+      if (j == 1 || j == ny) R = 0.0;
+    } else {
+      if (!last) {
+        if (j >= 2 && j <= ny) R = R - x2[t] * kv;
+        R = R + d1;
+        if (j <= ny) R = R + kzt;
+      }
+    }
+    if (COMP != 1 && r == jee - 1) R = 0.0;  // top row of the u,w RHS (rhsp.F90:441-442)
+    x1[t] = (q.valid && r < jee) ? R : 0.0;
+  }
+  if (COMP != 1 && h == 0)  // wall row of the u,w RHS (rhsp.F90:438-440)
+    x1[0] = -1.0 / M4(ib, 2, 1) * (M4(ib, 2, 2) * x1[1] + M4(ib, 2, 3) * x1[2] + M4(ib, 2, 4) * x1[3]);
+  // ---- velocity after the pressure gradient (rhsp.F90:291-339)
+  auto star = [&](int r, double o, double idyy) -> double {
+    if (COMP == 0) {
+      if (last) return o;
+      const int rp = min(r, ny - 1);  // p has ny rows; rows past them are padding
+      return o - var1 * idxx * (__ldg(pc + pnext + (size_t)rp * nz1) - __ldg(pc + (size_t)rp * nz1));
+    } else if (COMP == 1) {
+      const int rp = min(r, ny - 1);
+      return o - var1 * idyy * (__ldg(pc + (size_t)min(r + 1, ny - 1) * nz1) - __ldg(pc + (size_t)rp * nz1));
+    } else {
+      const double pp = __ldg(pc + (size_t)min(r, ny - 1) * nz1 + ppof);
+      const double av = var1 * kz;
+      return o - (q.odd ? av * pp : -av * pp);
+    }
+  };
+  // boun rows 1 and jee of the updated velocity (boun.f90:37-52), from the
+  // old velocity still in the tile
+  double ub1 = 0.0, ubt = 0.0;
+  if (COMP == 1) {
+    ubt = q.kr == 0 ? c.vmagic[i - 1] : 0.0;
+  } else {
+    if (h == 0 && q.valid) {
+      const double s2 = star(1, c2[1], 0.0), s3 = star(2, c2[2], 0.0), s4 = star(3, c2[3], 0.0);
+      const double sn = star(ny - 1, c2[ny - 1], 0.0), sn1 = star(ny - 2, c2[ny - 2], 0.0);
+      const double sn2 = star(ny - 3, c2[ny - 3], 0.0);
+      ub1 = -1.0 / M4(ib, 2, 1) * (M4(ib, 2, 2) * s2 + M4(ib, 2, 3) * s3 + M4(ib, 2, 4) * s4);
+      ubt = -1.0 / M2(cc, 1, 1) * (M2(cc, 1, 2) * sn + M2(cc, 1, 3) * sn1 + M2(cc, 1, 4) * sn2);
+    }
+    ub1 = __shfl_sync(0xffffffffu, ub1, 0, YNCH);
+    ubt = __shfl_sync(0xffffffffu, ubt, 0, YNCH);
+  }
+  // ---- vistyy of the old velocity (lip.f90:447-513) in x2
+  {
+    const int which = COMP == 1 ? 1 : 0, ic = which == 0 ? 3 : 1;
+    const double *vb = c.cofvby;
+    const double b0 = M4(vb, ic, 1) * c2[0] + M4(vb, ic, 2) * c2[1] + M4(vb, ic, 3) * c2[2] + M4(vb, ic, 4) * c2[3];
+    const double bN = M4(vb, ic + 1, 1) * c2[jee - 1] + M4(vb, ic + 1, 2) * c2[jee - 2] +
+                      M4(vb, ic + 1, 3) * c2[jee - 3] + M4(vb, ic + 1, 4) * c2[jee - 4];
+    const RCo8 F1(ys.k[YV_F1], h), F2(ys.k[YV_F2], h), F3(ys.k[YV_F3], h);
+    fx_forward<CL>(
+        x2, h,
+        [&](int t, double pv, double cu, double nx_) {
+          const int r = s + t;
+          const double in = F1(t) * nx_ + F2(t) * cu + F3(t) * pv;
+          return r == 0 ? b0 : (r == jee - 1 ? bN : (r < jee ? in : 0.0));
+        },
+        RCo8(ys.k[YV_L], h), g, Yp);
+    fx_backward<CL>(x2, h, g, Yp, RCo8(ys.k[YV_D], h), RCo8(ys.k[YV_U], h), hh, Xn);
+  }
+  // ---- RK3 combination and the new RHS history (rhsp.F90:448-475), with the
+  // vistyy fix-up folded in
+  {
+    const RCo8 IDYY(ys.k[Y_IDYY], h);
+#pragma unroll
+    for (int t = 0; t < CL; ++t) {
+      const int r = s + t, rr = min(r, jee - 1);
+      const double vis = x2[t] + hh[t] * Xn;
+      const double ov = __ldg(velg + (size_t)rr * nz1);
+      const double hv = __ldg(hp + (size_t)rr * nz1);
+      const double st = r == 0 ? ub1 : (r == jee - 1 ? ubt : star(rr, ov, COMP == 1 ? IDYY(t) : 0.0));
+      const double nv = st - (var3 * x1[t] + v2 * vis + var4 * hv);
+      x2[t] = (q.valid && r < jee) ? nv : 0.0;
+      if (q.valid && r < jee) hp[(size_t)r * nz1] = x1[t];
+    }
+  }
+  // ---- implzy (lip.f90:528-597): rows qq = 0..jee-3 from rows qq..qq+2 of
+  // x2, into x1; the fix-up is folded into the store
+  {
+    const int n = jee - 2;
+    const double *fac = COMP == 1 ? a.fac_v : a.fac_u;
+    const double a1raw = fac[3 * (jee + 1)], a3raw = fac[3 * (jee + 1) + 1];
+    const RCo8 F1(ys.k[YM_F1], h), F2(ys.k[YM_F2], h), F3(ys.k[YM_F3], h);
+    fx_forward<CL>(
+        x1, h,
+        [&](int t, double, double, double) {
+          const int qq = s + t;
+          double v = F1(t) * x2[t] + F2(t) * x2[t + 1] + F3(t) * x2[t + 2];
+          if (qq == 0) v = v - a1raw * ub1;
+          if (qq == n - 1) v = v - a3raw * ubt;
+          return qq < n ? v : 0.0;
+        },
+        RCo8(ys.k[YM_L], h), g, Yp);
+    fx_backward<CL>(x1, h, g, Yp, RCo8(ys.k[YM_D], h), RCo8(ys.k[YM_U], h), hh, Xn);
+    if (q.valid) {
+      double *o = vel + pl + q.kr;
+#pragma unroll
+      for (int t = 0; t < CL; ++t) {
+        const int qq = s + t;
+        if (qq < n) o[(size_t)(qq + 1) * nz1] = x1[t] + hh[t] * Xn;
+      }
+      if (h == 0) {
+        o[0] = ub1;
+        o[(size_t)(jee - 1) * nz1] = ubt;
+      }
+    }
+  }
+}
+
+// Runs f(std::integral_constant<int, CL>) when the fixed-length kernels are
+// compiled for CL.
+template <class F>
+bool with_yfix(int CL, F f) {
+  switch (CL) {
+    case 6: f(std::integral_constant<int, 6>{}); return true;
+    case 10: f(std::integral_constant<int, 10>{}); return true;
+    case 14: f(std::integral_constant<int, 14>{}); return true;
+    case 18: f(std::integral_constant<int, 18>{}); return true;
+    case 22: f(std::integral_constant<int, 22>{}); return true;
+    case 26: f(std::integral_constant<int, 26>{}); return true;
+    case 30: f(std::integral_constant<int, 30>{}); return true;
+    case 34: f(std::integral_constant<int, 34>{}); return true;
+    default: return false;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // pois.f90:106-117 + soltriy: tridiagonal in y per (x-mode, kz). The LU of
 // each (i, k) system depends only on the grid, so its pivots are computed
 // once (k_pois_lu) and every substep runs the pre-factored tile solve.
@@ -553,9 +865,25 @@ cudaError_t launch_final(otbl_ctx *c) {
   cudaFuncSetAttribute(k_final<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   dim3 g((c->dc.nz1 + YT - 1) / YT, c->cfg.nx - 1);
   prof_begin(c, PK_FINAL);
-  k_final<1><<<g, YTHREADS, smem, c->stream>>>(c->dc, yset(c->yco, 1), a, Lp);
-  k_final<0><<<g, YTHREADS, smem, c->stream>>>(c->dc, yset(c->yco, 0), a, Lp);
-  k_final<2><<<g, YTHREADS, smem, c->stream>>>(c->dc, yset(c->yco, 0), a, Lp);
+  const int CL = c->yco.CL;
+  const bool fixed = with_yfix(CL, [&](auto cl) {
+    constexpr int C = decltype(cl)::value;
+    // padded column plus two rows read by the implzy stencil past the last
+    // chunk (they feed only padded output rows); odd pitch
+    const int Lpf = YNCH * C + 3;
+    const size_t smf = sizeof(double) * 2 * YT * Lpf;
+    cudaFuncSetAttribute(k_final_f<0, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smf);
+    cudaFuncSetAttribute(k_final_f<1, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smf);
+    cudaFuncSetAttribute(k_final_f<2, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smf);
+    k_final_f<1, C><<<g, YTHREADS, smf, c->stream>>>(c->dc, yset(c->yco, 1), a, Lpf);
+    k_final_f<0, C><<<g, YTHREADS, smf, c->stream>>>(c->dc, yset(c->yco, 0), a, Lpf);
+    k_final_f<2, C><<<g, YTHREADS, smf, c->stream>>>(c->dc, yset(c->yco, 0), a, Lpf);
+  });
+  if (!fixed) {
+    k_final<1><<<g, YTHREADS, smem, c->stream>>>(c->dc, yset(c->yco, 1), a, Lp);
+    k_final<0><<<g, YTHREADS, smem, c->stream>>>(c->dc, yset(c->yco, 0), a, Lp);
+    k_final<2><<<g, YTHREADS, smem, c->stream>>>(c->dc, yset(c->yco, 0), a, Lp);
+  }
   prof_end(c);
   c->launches += 3;
   return cudaGetLastError();

@@ -143,10 +143,16 @@ int build_yco(otbl_ctx *c, const otbl_coef_offsets &o) {
     auto put = [&](int kind, auto f) {
       interleave(h.data() + off[which][kind], yco_rows(kind, which, ny), 8, CL, f);
     };
+    // solves: A of row 0 and U of the last row do not enter the sweeps and
+    // are stored as 0, so that padded fixed-length sweeps need no predicate
+    auto solve_coef = [](const double *a, int r, int q, int n) {
+      if ((q == 0 && r == 0) || (q == 2 && r == n - 1)) return 0.0;
+      return a[(size_t)r * 3 + q];
+    };
     for (int q = 0; q < 3; ++q) {
-      put(YI_L + q, [&](int r) { return iny[(size_t)r * 3 + q]; });
-      put(YD_L + q, [&](int r) { return dcy[(size_t)r * 3 + q]; });
-      put(YV_L + q, [&](int r) { return viy[(size_t)r * 3 + q]; });
+      put(YI_L + q, [&](int r) { return solve_coef(iny, r, q, ny); });
+      put(YD_L + q, [&](int r) { return solve_coef(dcy, r, q, jee); });
+      put(YV_L + q, [&](int r) { return solve_coef(viy, r, q, jee); });
       put(YV_F1 + q, [&](int r) { return cofv[(size_t)(cl(r + 1, 2, jee - 1) - 1) * 3 + q]; });
       put(YM_F1 + q, [&](int r) { return vyi[(size_t)(std::min(r + 2, jee - 1) - 1) * 3 + q]; });
     }
@@ -154,8 +160,8 @@ int build_yco(otbl_ctx *c, const otbl_coef_offsets &o) {
       put(YI_E1 + q, [&](int r) { return cofi[(size_t)(cl(r + 1, 2, ny - 1) - 1) * 2 + q]; });
       put(YD_E1 + q, [&](int r) { return cofc[(size_t)(cl(r + 1, 2, ny) - 1) * 2 + q]; });
     }
-    put(YP_A1, [&](int r) { return ayp[(size_t)r * 3 + 0]; });
-    put(YP_A3, [&](int r) { return ayp[(size_t)r * 3 + 2]; });
+    put(YP_A1, [&](int r) { return r > 0 ? ayp[(size_t)r * 3 + 0] : 0.0; });
+    put(YP_A3, [&](int r) { return r < ny - 2 ? ayp[(size_t)r * 3 + 2] : 0.0; });
     put(Y_IDYY, [&](int r) { return idyy[r]; });
     for (int k = 0; k < YCO_N; ++k) c->yco.k[which][k] = dev + off[which][k];
     c->yco.fac[which] = dev + off[which][YM_L];
