@@ -74,6 +74,11 @@ C2 = BoxConfig(nx=1025, ny=193, nz=512, lx=80.0, ly=10.0, lz=10.0,
 # about 3.5 GB on the device
 MED = BoxConfig(nx=513, ny=193, nz=256, lx=40.0, ly=10.0, lz=8.0,
                 re_theta=1000.0, profile="musker", name="MED-513x193x256")
+# a quarter of the 1025x193x512 box in x, same y and z sizes (every kernel
+# takes the code path of the full box): fields of 135 MB, about 3.5 GB on the
+# device, for profiling captures
+SLAB = BoxConfig(nx=257, ny=193, nz=512, lx=20.0, ly=10.0, lz=10.0,
+                 re_theta=1000.0, profile="musker", name="SLAB-257x193x512")
 # small box for tests and smoke runs
 TINY = BoxConfig(nx=33, ny=41, nz=32, lx=12.0, ly=6.0, lz=4.0, dy_wall=0.02,
                  re_theta=300.0, profile="blasius", y_blend=1.5,

@@ -603,53 +603,75 @@ __global__ void __launch_bounds__(YTHREADS, 2) k_final_f(DCoef c, YSet ys, Final
         RCo8(ys.k[YD_L], h), g, Yp);
     fx_backward<CL>(x1, h, g, Yp, RCo8(ys.k[YD_D], h), RCo8(ys.k[YD_U], h), hh, Xn);
   }
-  // ---- RHS assembly (rhsp.F90:164-169, 181-204, 351-418, 423-445) with the
-  // differzy fix-up folded in
+  // ---- RHS assembly (rhsp.F90:164-169, 181-204, 351-418, 423-445). The
+  // differzy fix-up is applied first (freeing its products), so that the
+  // global loads of each batch of rows are all in flight before the
+  // arithmetic that uses them.
+  if (!last) {
 #pragma unroll
-  for (int t = 0; t < CL; ++t) {
-    const int r = s + t, rr = min(r, jee - 1), j = r + 1;
-    const double d1 = last ? 0.0 : x1[t] + hh[t] * Xn;
-    double R = __ldg(cX + (size_t)rr * nz1);
-    const double kpv = (!last && (COMP != 2 || r < ny)) ? __ldg(kp + (size_t)min(rr, krows - 1) * nz1) : 0.0;
-    const double kzt = sgn * kz * kpv;
-    if (COMP == 0) {
-      if (!last) {
-        R = (d1 + kzt) + R;
-        if (j >= 2 && j <= ny) R = R - x2[t] * kv;
+    for (int t = 0; t < CL; ++t) x1[t] = x1[t] + hh[t] * Xn;
+  }
+#pragma unroll
+  for (int t0 = 0; t0 < CL; t0 += 8) {
+    double cxv[8], kpv[8];
+#pragma unroll
+    for (int b = 0; b < 8; ++b)
+      if (t0 + b < CL) {
+        const int rr = min(s + t0 + b, jee - 1);
+        cxv[b] = __ldg(cX + (size_t)rr * nz1);
+        kpv[b] = last ? 0.0 : __ldg(kp + (size_t)min(rr, krows - 1) * nz1);
       }
-    } else if (COMP == 1) {
-      if (!last) {
-        if (j >= 2 && j <= ny - 1) R = R - x2[t] * kv;
-        R = R + kzt;
-        R = R + d1;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      const int t = t0 + b;
+      if (t >= CL) break;
+      const int r = s + t, j = r + 1;
+      const double d1 = last ? 0.0 : x1[t];
+      double R = cxv[b];
+      const double kzt = sgn * kz * ((COMP != 2 || r < ny) ? kpv[b] : 0.0);
+      if (COMP == 0) {
+        if (!last) {
+          R = (d1 + kzt) + R;
+          if (j >= 2 && j <= ny) R = R - x2[t] * kv;
+        }
+      } else if (COMP == 1) {
+        if (!last) {
+          if (j >= 2 && j <= ny - 1) R = R - x2[t] * kv;
+          R = R + kzt;
+          R = R + d1;
+        }
+        if (j == 1 || j == ny) R = 0.0;
+      } else {
+        if (!last) {
+          if (j >= 2 && j <= ny) R = R - x2[t] * kv;
+          R = R + d1;
+          if (j <= ny) R = R + kzt;
+        }
       }
-      if (j == 1 || j == ny) R = 0.0;
-    } else {
-      if (!last) {
-        if (j >= 2 && j <= ny) R = R - x2[t] * kv;
-        R = R + d1;
-        if (j <= ny) R = R + kzt;
-      }
+      if (COMP != 1 && r == jee - 1) R = 0.0;  // top row of the u,w RHS (rhsp.F90:441-442)
+      x1[t] = (q.valid && r < jee) ? R : 0.0;
     }
-    if (COMP != 1 && r == jee - 1) R = 0.0;  // top row of the u,w RHS (rhsp.F90:441-442)
-    x1[t] = (q.valid && r < jee) ? R : 0.0;
   }
   if (COMP != 1 && h == 0)  // wall row of the u,w RHS (rhsp.F90:438-440)
     x1[0] = -1.0 / M4(ib, 2, 1) * (M4(ib, 2, 2) * x1[1] + M4(ib, 2, 3) * x1[2] + M4(ib, 2, 4) * x1[3]);
-  // ---- velocity after the pressure gradient (rhsp.F90:291-339)
+  // ---- velocity after the pressure gradient (rhsp.F90:291-339). P0(r),
+  // P1(r) are the pressure values row r needs (p has ny rows; rows past
+  // them are padding and read row ny-1)
+  auto P0 = [&](int r) {  // p(r) for u and v, the partner component for w
+    return __ldg(pc + (size_t)min(r, ny - 1) * nz1 + (COMP == 2 ? ppof : 0));
+  };
+  auto P1 = [&](int r) {  // p of plane i+1 (u) or of row r+1 (v)
+    if (COMP == 0) return last ? 0.0 : __ldg(pc + pnext + (size_t)min(r, ny - 1) * nz1);
+    return __ldg(pc + (size_t)min(r + 1, ny - 1) * nz1);
+  };
+  auto star_v = [&](double o, double p0, double p1, double idyy) -> double {
+    if (COMP == 0) return last ? o : o - var1 * idxx * (p1 - p0);
+    if (COMP == 1) return o - var1 * idyy * (p1 - p0);
+    const double av = var1 * kz;
+    return o - (q.odd ? av * p0 : -av * p0);
+  };
   auto star = [&](int r, double o, double idyy) -> double {
-    if (COMP == 0) {
-      if (last) return o;
-      const int rp = min(r, ny - 1);  // p has ny rows; rows past them are padding
-      return o - var1 * idxx * (__ldg(pc + pnext + (size_t)rp * nz1) - __ldg(pc + (size_t)rp * nz1));
-    } else if (COMP == 1) {
-      const int rp = min(r, ny - 1);
-      return o - var1 * idyy * (__ldg(pc + (size_t)min(r + 1, ny - 1) * nz1) - __ldg(pc + (size_t)rp * nz1));
-    } else {
-      const double pp = __ldg(pc + (size_t)min(r, ny - 1) * nz1 + ppof);
-      const double av = var1 * kz;
-      return o - (q.odd ? av * pp : -av * pp);
-    }
+    return star_v(o, P0(r), COMP == 2 ? 0.0 : P1(r), idyy);
   };
   // boun rows 1 and jee of the updated velocity (boun.f90:37-52), from the
   // old velocity still in the tile
@@ -685,20 +707,35 @@ __global__ void __launch_bounds__(YTHREADS, 2) k_final_f(DCoef c, YSet ys, Final
         RCo8(ys.k[YV_L], h), g, Yp);
     fx_backward<CL>(x2, h, g, Yp, RCo8(ys.k[YV_D], h), RCo8(ys.k[YV_U], h), hh, Xn);
   }
-  // ---- RK3 combination and the new RHS history (rhsp.F90:448-475), with the
-  // vistyy fix-up folded in
+  // ---- RK3 combination and the new RHS history (rhsp.F90:448-475): the
+  // vistyy fix-up first, then batches of rows with their loads in flight
+#pragma unroll
+  for (int t = 0; t < CL; ++t) x2[t] = x2[t] + hh[t] * Xn;
   {
     const RCo8 IDYY(ys.k[Y_IDYY], h);
 #pragma unroll
-    for (int t = 0; t < CL; ++t) {
-      const int r = s + t, rr = min(r, jee - 1);
-      const double vis = x2[t] + hh[t] * Xn;
-      const double ov = __ldg(velg + (size_t)rr * nz1);
-      const double hv = __ldg(hp + (size_t)rr * nz1);
-      const double st = r == 0 ? ub1 : (r == jee - 1 ? ubt : star(rr, ov, COMP == 1 ? IDYY(t) : 0.0));
-      const double nv = st - (var3 * x1[t] + v2 * vis + var4 * hv);
-      x2[t] = (q.valid && r < jee) ? nv : 0.0;
-      if (q.valid && r < jee) hp[(size_t)r * nz1] = x1[t];
+    for (int t0 = 0; t0 < CL; t0 += 4) {
+      double ov[4], hv[4], p0[4], p1[4], iy[4];
+#pragma unroll
+      for (int b = 0; b < 4; ++b)
+        if (t0 + b < CL) {
+          const int rr = min(s + t0 + b, jee - 1);
+          ov[b] = __ldg(velg + (size_t)rr * nz1);
+          hv[b] = __ldg(hp + (size_t)rr * nz1);
+          p0[b] = P0(rr);
+          p1[b] = COMP == 2 ? 0.0 : P1(rr);
+          iy[b] = COMP == 1 ? IDYY(t0 + b) : 0.0;
+        }
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const int t = t0 + b;
+        if (t >= CL) break;
+        const int r = s + t;
+        const double st = r == 0 ? ub1 : (r == jee - 1 ? ubt : star_v(ov[b], p0[b], p1[b], iy[b]));
+        const double nv = st - (var3 * x1[t] + v2 * x2[t] + var4 * hv[b]);
+        x2[t] = (q.valid && r < jee) ? nv : 0.0;
+        if (q.valid && r < jee) hp[(size_t)r * nz1] = x1[t];
+      }
     }
   }
   // ---- implzy (lip.f90:528-597): rows qq = 0..jee-3 from rows qq..qq+2 of
