@@ -1,228 +1,220 @@
-// Streamwise (x) line operators of lip.f90 on shared-memory tiles.
-//
-// A CTA owns XT consecutive pencils (contiguous (j, kr) indices of the plane
-// layout) over all nx planes. Loads read XT consecutive doubles per plane
-// (the reference's chp2x transpose is replaced by this gather; its REAL4
-// rounding is applied at the same points when OTBL_XPOSE_FP32 is set). One
-// warp solves one pencil: 32 lanes own contiguous chunks of planes.
+// Streamwise (x) line operators of lip.f90 (interpxx, difvisxx), one thread
+// per line. A line is a fixed (j, kr) of the plane layout; its nx values are
+// read with the plane stride, so the reference's chp2x transpose is replaced
+// by these strided, warp-coalesced loads (its REAL4 rounding is applied at
+// the same points when OTBL_XPOSE_FP32 is set).
 #include "devcommon.cuh"
-#include "lines.cuh"
 #include "otbl_internal.cuh"
 
 namespace otbl {
 
-#ifndef OTBL_XT_INTERP
-#define OTBL_XT_INTERP 8
-#endif
-#ifndef OTBL_XT_DIFVIS
-#define OTBL_XT_DIFVIS 4
-#endif
-constexpr int XT_INTERP = OTBL_XT_INTERP;  // pencils per CTA for interpxx (1 tile)
-constexpr int XT_DIFVIS = OTBL_XT_DIFVIS;  // pencils per CTA for difvisxx (2 tiles)
+// ---------------------------------------------------------------------------
+// x-lines streamed through registers: one thread per line (pencil), the
+// threads of a warp on consecutive (j, kr), so every row access is a
+// coalesced 256-byte request and every coefficient a broadcast. The forward
+// sweep y_i = b_i + l_i y_{i-1} (b the explicit stencil) leaves a checkpoint
+// of y every K rows in scratch; the backward sweep x_i = (y_i - u_i x_{i+1})
+// d_i walks the segments from the last one, recomputing each segment's y in
+// registers from its checkpoint. This is the serial Thomas of lip.f90 in the
+// reference's order; the traffic is about 1.5x the minimum (inputs read
+// twice) with no shared memory and no scan.
+// ---------------------------------------------------------------------------
+struct XStream {
+  const double *in[3], *in2[3];  // in2: the second input of difvisxx (velocity)
+  double *out[3], *ck[3];        // ck: checkpoint scratch of each line set
+  int which[3], np[3];
+};
 
-// Issues the asynchronous copies of a tile (nx planes x XT pencils); the
-// caller waits with xtile_wait.
-template <int XT>
-__device__ __forceinline__ void xtile_load(double *sm, const double *__restrict__ in, int nx, int np, int mp0,
-                                           int Lp) {
-  for (int e = threadIdx.x; e < nx * XT; e += XT * 32) {
-    const int i0 = e / XT, col = e - i0 * XT, mp = mp0 + col;
-    const bool ok = mp < np;
-    cp_async8(sm + col * Lp + i0, ok ? in + (size_t)i0 * np + mp : in, ok);
-  }
-}
+constexpr int KXI = 16;  // interpxx segment
+constexpr int KXD = 16;  // difvisxx segment (two recurrences)
 
-// Completes the copies; with REAL4 transposes, rounds the tile in place.
-template <int XT>
-__device__ __forceinline__ void xtile_wait(double *sm, int ntiles, int nx, int Lp, int xr) {
-  cp_async_wait_all();
-  __syncthreads();
-  if (xr) {
-    for (int e = threadIdx.x; e < ntiles * XT * Lp; e += XT * 32) sm[e] = rnd(sm[e], 1);
-    __syncthreads();
-  }
-}
-
-template <int XT>
-__device__ __forceinline__ void xtile_store(const double *sm, double *__restrict__ out, int nx, int np, int mp0,
-                                            int Lp, int xr) {
-  for (int e = threadIdx.x; e < nx * XT; e += XT * 32) {
-    const int i0 = e / XT, col = e - i0 * XT, mp = mp0 + col;
-    if (mp < np) out[(size_t)i0 * np + mp] = rnd(sm[col * Lp + i0], xr);
-  }
-}
-
-// interpxx, lip.f90:248-300. which 0: u (inxu, cofiux, chi=2, chi2=3);
-// which 1: v,w (inxv, cofivx, chi=1, chi2=4). Coefficients of the stencil
-// and the solve come chunk-interleaved (XSet).
-__global__ void __launch_bounds__(XT_INTERP * 32) k_interpx(DCoef c, XSet xs, const double *__restrict__ in,
-                                                            double *__restrict__ out, int which, int np, int Lp) {
-  extern __shared__ double sm[];
-  const int nx = c.nx, xr = c.xround;
-  const int mp0 = blockIdx.x * XT_INTERP;
-  xtile_load<XT_INTERP>(sm, in, nx, np, mp0, Lp);
-  xtile_wait<XT_INTERP>(sm, 1, nx, Lp, xr);
-  const int h = threadIdx.x & 31;
-  double *x = sm + (threadIdx.x >> 5) * Lp;
+__global__ void __launch_bounds__(128) k_interpx(DCoef c, XStream a) {
+  const int f = blockIdx.y, np = a.np[f];
+  const int mp = blockIdx.x * blockDim.x + threadIdx.x;
+  if (mp >= np) return;
+  const int nx = c.nx, xr = c.xround, which = a.which[f];
+  const double *in = a.in[f] + mp;
+  double *out = a.out[f] + mp, *ck = a.ck[f] + mp;
+  const double *icon = which == 0 ? c.inxu : c.inxv;
+  const double *econ = which == 0 ? c.cofiux : c.cofivx;
   const int chi = which == 0 ? 2 : 1, chi2 = which == 0 ? 3 : 4;
   const double *ib = c.inbx;
-  const CCo<32> E1(xs.k[XI_E1], h, xs.CL), E2(xs.k[XI_E2], h, xs.CL);
-  int s, e;
-  chunk_range(nx, h, xs.CL, s, e);
-  const double gnext = e < nx ? x[e] : 0.0;
-  double b0 = 0.0, bN = 0.0;
-  if (s == 0 && e > s)
-    b0 = M4(ib, chi2, 1) * x[0] + M4(ib, chi2, 2) * x[1] + M4(ib, chi2, 3) * x[2] + M4(ib, chi2, 4) * x[3];
-  if (e == nx && e > s)
-    bN = M4(ib, chi, 1) * x[nx - 1] + M4(ib, chi, 2) * x[nx - 2] + M4(ib, chi, 3) * x[nx - 3] +
-         M4(ib, chi, 4) * x[nx - 4];
-  __syncwarp();
-  for (int r0 = s; r0 < e; r0 += LB) {  // ascending; a batch reads rows r0..r0+LB first
-    double gv[LB + 1], e1[LB], e2[LB];
+  auto G = [&](int i) { return rnd(__ldg(in + (size_t)i * np), xr); };
+  const double b0 = M4(ib, chi2, 1) * G(0) + M4(ib, chi2, 2) * G(1) + M4(ib, chi2, 3) * G(2) + M4(ib, chi2, 4) * G(3);
+  const double bN = M4(ib, chi, 1) * G(nx - 1) + M4(ib, chi, 2) * G(nx - 2) + M4(ib, chi, 3) * G(nx - 3) +
+                    M4(ib, chi, 4) * G(nx - 4);
+  // right-hand side of row i from g_i, g_{i+1} (interior: lip.f90 stencil)
+  auto rhs = [&](int i, double gi, double gi1) {
+    return i == 0 ? b0 : (i == nx - 1 ? bN : __ldg(econ + 2 * i) * gi + __ldg(econ + 2 * i + 1) * gi1);
+  };
+  const int nseg = (nx + KXI - 1) / KXI;
+  double y = 0.0;
+  for (int sg = 0; sg < nseg; ++sg) {
+    const int s = sg * KXI;
+    ck[(size_t)sg * np] = y;  // y of row s-1
+    double gv[KXI + 1];
 #pragma unroll
-    for (int b = 0; b <= LB; ++b) gv[b] = r0 + b < e ? x[r0 + b] : gnext;
+    for (int b = 0; b <= KXI; ++b) gv[b] = G(min(s + b, nx - 1));
 #pragma unroll
-    for (int b = 0; b < LB; ++b) {
-      const bool ok = r0 + b < e;
-      e1[b] = ok ? E1(r0 + b) : 0.0;
-      e2[b] = ok ? E2(r0 + b) : 0.0;
-    }
-#pragma unroll
-    for (int b = 0; b < LB; ++b) {
-      const int r = r0 + b;
-      if (r >= e) break;
-      x[r] = r == 0 ? b0 : (r == nx - 1 ? bN : e1[b] * gv[b] + e2[b] * gv[b + 1]);
+    for (int b = 0; b < KXI; ++b) {
+      const int i = s + b;
+      if (i < nx) y = rhs(i, gv[b], gv[b + 1]) + (i > 0 ? __ldg(icon + 3 * i) : 0.0) * y;
     }
   }
-  __syncwarp();
-  solve_cco<32>(x, nx, h, xs.CL, CCo<32>(xs.k[XI_L], h, xs.CL), CCo<32>(xs.k[XI_D], h, xs.CL),
-                       CCo<32>(xs.k[XI_U], h, xs.CL));
-  __syncthreads();
-  xtile_store<XT_INTERP>(sm, out, nx, np, mp0, Lp, xr);
+  double xn = 0.0;
+  for (int sg = nseg - 1; sg >= 0; --sg) {
+    const int s = sg * KXI;
+    double gv[KXI + 1], yv[KXI];
+#pragma unroll
+    for (int b = 0; b <= KXI; ++b) gv[b] = G(min(s + b, nx - 1));
+    double yy = ck[(size_t)sg * np];
+#pragma unroll
+    for (int b = 0; b < KXI; ++b) {
+      const int i = s + b;
+      if (i < nx) yy = rhs(i, gv[b], gv[b + 1]) + (i > 0 ? __ldg(icon + 3 * i) : 0.0) * yy;
+      yv[b] = yy;
+    }
+#pragma unroll
+    for (int b = KXI - 1; b >= 0; --b) {
+      const int i = s + b;
+      if (i < nx) {
+        xn = (yv[b] - __ldg(icon + 3 * i + 2) * xn) * __ldg(icon + 3 * i + 1);
+        out[(size_t)i * np] = rnd(xn, xr);
+      }
+    }
+  }
 }
 
-// difvisxx, lip.f90:52-142: Pade d/dx(gin) + rex * Pade d2/dx2(upin), with
-// the outflow rows of lip.f90:105,132. which 0: u; which 1: v,w.
-__global__ void __launch_bounds__(XT_DIFVIS * 32) k_difvisx(DCoef c, XSet xs, const double *__restrict__ gin,
-                                                            const double *__restrict__ upin,
-                                                            double *__restrict__ out, int which, int np, int Lp) {
-  extern __shared__ double sm[];
-  const int nx = c.nx, xr = c.xround;
-  const int mp0 = blockIdx.x * XT_DIFVIS;
-  double *smg = sm, *smu = sm + XT_DIFVIS * Lp;
-  xtile_load<XT_DIFVIS>(smg, gin, nx, np, mp0, Lp);
-  xtile_load<XT_DIFVIS>(smu, upin, nx, np, mp0, Lp);
-  xtile_wait<XT_DIFVIS>(sm, 2, nx, Lp, xr);
-  const int h = threadIdx.x & 31, wv = threadIdx.x >> 5;
-  double *x = smg + wv * Lp, *u = smu + wv * Lp;
-  const int CL = xs.CL;
-  const CCo<32> E1(xs.k[XD_E1], h, CL), E2(xs.k[XD_E2], h, CL);
-  const CCo<32> F1(xs.k[XV_F1], h, CL), F2(xs.k[XV_F2], h, CL), F3(xs.k[XV_F3], h, CL);
+__global__ void __launch_bounds__(128) k_difvisx(DCoef c, XStream a) {
+  const int f = blockIdx.y, np = a.np[f];
+  const int mp = blockIdx.x * blockDim.x + threadIdx.x;
+  if (mp >= np) return;
+  const int nx = c.nx, xr = c.xround, which = a.which[f];
+  const double *gin = a.in[f] + mp, *uin = a.in2[f] + mp;
+  double *out = a.out[f] + mp, *ck = a.ck[f] + mp;
+  const double *icon = which == 0 ? c.dcxu : c.dcxv;
+  const double *iconv = which == 0 ? c.vixu : c.vixv;
+  const double *econ = which == 0 ? c.cofcxu : c.cofcxv;
+  const double *econv = which == 0 ? c.cofvxu : c.cofvxv;
   const int chv = which == 0 ? 1 : 2, chv1 = chv + 2, ic = which == 0 ? 3 : 1;
   const double *db = c.dcbx, *vb = c.cofvbx;
   const double rex = c.S[OTBL_S_REX], idx = c.S[OTBL_S_IDX], uinf = c.S[OTBL_S_UINF];
-  int s, e;
-  chunk_range(nx, h, xs.CL, s, e);
-  // halos and boundary stencils, read before anything is overwritten
-  const double gprev = s > 0 ? x[s - 1] : 0.0;
-  double uprev = s > 0 ? u[s - 1] : 0.0;
-  const double unext = e < nx ? u[e] : 0.0;
-  double gb0 = 0.0, gbN = 0.0, ub0 = 0.0, ubN = 0.0, uN = 0.0, uN1 = 0.0;
-  if (s == 0 && e > s) {
-    gb0 = M5(db, chv, 1) * x[0] + M5(db, chv, 2) * x[1] + M5(db, chv, 3) * x[2] + M5(db, chv, 4) * x[3];
-    ub0 = M4(vb, ic, 1) * u[0] + M4(vb, ic, 2) * u[1] + M4(vb, ic, 3) * u[2] + M4(vb, ic, 4) * u[3];
-  }
-  if (e == nx && e > s) {
-    gbN = M5(db, chv1, 1) * x[nx - 1] + M5(db, chv1, 2) * x[nx - 2] + M5(db, chv1, 3) * x[nx - 3] +
-          M5(db, chv1, 4) * x[nx - 4];
-    ubN = M4(vb, ic + 1, 1) * u[nx - 1] + M4(vb, ic + 1, 2) * u[nx - 2] + M4(vb, ic + 1, 3) * u[nx - 3] +
-          M4(vb, ic + 1, 4) * u[nx - 4];
-    uN = u[nx - 1];
-    uN1 = u[nx - 2];
-  }
-  __syncwarp();
-  // convective right-hand side, descending in place; a batch reads rows
-  // r1-LB..r1 before writing r1-LB+1..r1
-  for (int r1 = e - 1; r1 >= s; r1 -= LB) {
-    double gv[LB + 1], e1[LB], e2[LB];
+  auto G = [&](int i) { return rnd(__ldg(gin + (size_t)i * np), xr); };
+  auto U = [&](int i) { return rnd(__ldg(uin + (size_t)i * np), xr); };
+  const double gb0 = M5(db, chv, 1) * G(0) + M5(db, chv, 2) * G(1) + M5(db, chv, 3) * G(2) + M5(db, chv, 4) * G(3);
+  const double ub0 = M4(vb, ic, 1) * U(0) + M4(vb, ic, 2) * U(1) + M4(vb, ic, 3) * U(2) + M4(vb, ic, 4) * U(3);
+  const double gbN = M5(db, chv1, 1) * G(nx - 1) + M5(db, chv1, 2) * G(nx - 2) + M5(db, chv1, 3) * G(nx - 3) +
+                     M5(db, chv1, 4) * G(nx - 4);
+  const double uN = U(nx - 1), uN1 = U(nx - 2);
+  const double ubN = M4(vb, ic + 1, 1) * uN + M4(vb, ic + 1, 2) * uN1 + M4(vb, ic + 1, 3) * U(nx - 3) +
+                     M4(vb, ic + 1, 4) * U(nx - 4);
+  // right-hand sides of row i: convective e1 g_{i-1} + e2 g_i, viscous
+  // f1 u_{i+1} + f2 u_i + f3 u_{i-1} (lip.f90:52-142)
+  auto rg = [&](int i, double gm, double g0) {
+    return i == 0 ? gb0 : (i == nx - 1 ? gbN : __ldg(econ + 2 * i) * gm + __ldg(econ + 2 * i + 1) * g0);
+  };
+  auto ru = [&](int i, double um, double u0, double up) {
+    return i == 0 ? ub0
+                  : (i == nx - 1 ? ubN
+                                 : __ldg(econv + 3 * i) * up + __ldg(econv + 3 * i + 1) * u0 +
+                                       __ldg(econv + 3 * i + 2) * um);
+  };
+  const int nseg = (nx + KXD - 1) / KXD;
+  double yg = 0.0, yu = 0.0;
+  for (int sg = 0; sg < nseg; ++sg) {
+    const int s = sg * KXD;
+    ck[(size_t)(2 * sg) * np] = yg;
+    ck[(size_t)(2 * sg + 1) * np] = yu;
+    double gv[KXD + 1], uv[KXD + 2];  // rows s-1 .. s+K-1 (g), s-1 .. s+K (u)
 #pragma unroll
-    for (int b = 0; b <= LB; ++b) gv[b] = r1 - b >= s ? x[r1 - b] : gprev;
+    for (int b = 0; b <= KXD; ++b) gv[b] = G(min(max(s + b - 1, 0), nx - 1));
 #pragma unroll
-    for (int b = 0; b < LB; ++b) {
-      const bool ok = r1 - b >= s;
-      e1[b] = ok ? E1(r1 - b) : 0.0;
-      e2[b] = ok ? E2(r1 - b) : 0.0;
+    for (int b = 0; b <= KXD + 1; ++b) uv[b] = U(min(max(s + b - 1, 0), nx - 1));
+#pragma unroll
+    for (int b = 0; b < KXD; ++b) {
+      const int i = s + b;
+      if (i < nx) {
+        yg = rg(i, gv[b], gv[b + 1]) + (i > 0 ? __ldg(icon + 3 * i) : 0.0) * yg;
+        yu = ru(i, uv[b], uv[b + 1], uv[b + 2]) + (i > 0 ? __ldg(iconv + 3 * i) : 0.0) * yu;
+      }
+    }
+  }
+  double xg = 0.0, xu = 0.0;
+  for (int sg = nseg - 1; sg >= 0; --sg) {
+    const int s = sg * KXD;
+    double gv[KXD + 1], uv[KXD + 2], ygv[KXD], yuv[KXD];
+#pragma unroll
+    for (int b = 0; b <= KXD; ++b) gv[b] = G(min(max(s + b - 1, 0), nx - 1));
+#pragma unroll
+    for (int b = 0; b <= KXD + 1; ++b) uv[b] = U(min(max(s + b - 1, 0), nx - 1));
+    double a1 = ck[(size_t)(2 * sg) * np], a2 = ck[(size_t)(2 * sg + 1) * np];
+#pragma unroll
+    for (int b = 0; b < KXD; ++b) {
+      const int i = s + b;
+      if (i < nx) {
+        a1 = rg(i, gv[b], gv[b + 1]) + (i > 0 ? __ldg(icon + 3 * i) : 0.0) * a1;
+        a2 = ru(i, uv[b], uv[b + 1], uv[b + 2]) + (i > 0 ? __ldg(iconv + 3 * i) : 0.0) * a2;
+      }
+      ygv[b] = a1;
+      yuv[b] = a2;
     }
 #pragma unroll
-    for (int b = 0; b < LB; ++b) {
-      const int r = r1 - b;
-      if (r < s) break;
-      x[r] = r == 0 ? gb0 : (r == nx - 1 ? gbN : e1[b] * gv[b + 1] + e2[b] * gv[b]);
+    for (int b = KXD - 1; b >= 0; --b) {
+      const int i = s + b;
+      if (i < nx) {
+        xg = (ygv[b] - __ldg(icon + 3 * i + 2) * xg) * __ldg(icon + 3 * i + 1);
+        xu = (yuv[b] - __ldg(iconv + 3 * i + 2) * xu) * __ldg(iconv + 3 * i + 1);
+        const double v = i == nx - 1 ? uinf * (uN - uN1) * idx + rex * 0.0 : xg + rex * xu;
+        out[(size_t)i * np] = rnd(v, xr);
+      }
     }
   }
-  // viscous right-hand side, ascending in place
-  for (int r0 = s; r0 < e; r0 += LB) {
-    double uv[LB + 2], f1[LB], f2[LB], f3[LB];
-    uv[0] = uprev;  // original value of row r0-1
-#pragma unroll
-    for (int b = 0; b <= LB; ++b) uv[b + 1] = r0 + b < e ? u[r0 + b] : unext;
-#pragma unroll
-    for (int b = 0; b < LB; ++b) {
-      const bool ok = r0 + b < e;
-      f1[b] = ok ? F1(r0 + b) : 0.0;
-      f2[b] = ok ? F2(r0 + b) : 0.0;
-      f3[b] = ok ? F3(r0 + b) : 0.0;
-    }
-#pragma unroll
-    for (int b = 0; b < LB; ++b) {
-      const int r = r0 + b;
-      if (r >= e) break;
-      u[r] = r == 0 ? ub0 : (r == nx - 1 ? ubN : f1[b] * uv[b + 2] + f2[b] * uv[b + 1] + f3[b] * uv[b]);
-    }
-    uprev = uv[LB];  // original value of the last row of this batch
-  }
-  __syncwarp();
-  solve_cco<32>(x, nx, h, xs.CL, CCo<32>(xs.k[XD_L], h, CL), CCo<32>(xs.k[XD_D], h, CL),
-                       CCo<32>(xs.k[XD_U], h, CL));
-  solve_cco<32>(u, nx, h, xs.CL, CCo<32>(xs.k[XV_L], h, CL), CCo<32>(xs.k[XV_D], h, CL),
-                       CCo<32>(xs.k[XV_U], h, CL));
-  for (int r = s; r < e; ++r) x[r] = r == nx - 1 ? uinf * (uN - uN1) * idx + rex * 0.0 : x[r] + rex * u[r];
-  __syncthreads();
-  xtile_store<XT_DIFVIS>(smg, out, nx, np, mp0, Lp, xr);
 }
 
 cudaError_t launch_interpx(otbl_ctx *c) {
-  const int nz1 = c->dc.nz1, ny = c->cfg.ny, nx = c->cfg.nx;
+  const int nz1 = c->dc.nz1, ny = c->cfg.ny;
   const int npu = nz1 * (ny + 1), npv = nz1 * ny;
-  const int Lp = nx | 1;
-  const size_t smem = sizeof(double) * XT_INTERP * Lp;
-  const dim3 gu((npu + XT_INTERP - 1) / XT_INTERP), gv((npv + XT_INTERP - 1) / XT_INTERP);
-  const XSet x0 = xset(c->xco, 0), x1 = xset(c->xco, 1);
+  XStream a;
+  const double *ins[3] = {c->f[OTBL_F_U], c->f[OTBL_F_V], c->f[OTBL_F_W]};
+  double *outs[3] = {c->w.ux, c->w.vx, c->w.wx};
+  double *cks[3] = {c->w.s1, c->w.s2, c->w.s3};
+  const int which[3] = {0, 1, 1}, np[3] = {npu, npv, npu};
+  for (int f = 0; f < 3; ++f) {
+    a.in[f] = ins[f];
+    a.in2[f] = nullptr;
+    a.out[f] = outs[f];
+    a.ck[f] = cks[f];
+    a.which[f] = which[f];
+    a.np[f] = np[f];
+  }
   prof_begin(c, PK_INTERPX);
-  cudaFuncSetAttribute(k_interpx, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_interpx<<<gu, XT_INTERP * 32, smem, c->stream>>>(c->dc, x0, c->f[OTBL_F_U], c->w.ux, 0, npu, Lp);
-  k_interpx<<<gv, XT_INTERP * 32, smem, c->stream>>>(c->dc, x1, c->f[OTBL_F_V], c->w.vx, 1, npv, Lp);
-  k_interpx<<<gu, XT_INTERP * 32, smem, c->stream>>>(c->dc, x1, c->f[OTBL_F_W], c->w.wx, 1, npu, Lp);
+  k_interpx<<<dim3((npu + 127) / 128, 3), 128, 0, c->stream>>>(c->dc, a);
   prof_end(c);
-  c->launches += 3;
+  c->launches += 1;
   return cudaGetLastError();
 }
 
 cudaError_t launch_difvisx(otbl_ctx *c) {
-  const int nz1 = c->dc.nz1, ny = c->cfg.ny, nx = c->cfg.nx;
+  const int nz1 = c->dc.nz1, ny = c->cfg.ny;
   const int npu = nz1 * (ny + 1), npv = nz1 * ny;
-  const int Lp = nx | 1;
-  const size_t smem = sizeof(double) * 2 * XT_DIFVIS * Lp;
-  const int T = XT_DIFVIS * 32;
-  const dim3 gu((npu + XT_DIFVIS - 1) / XT_DIFVIS), gv((npv + XT_DIFVIS - 1) / XT_DIFVIS);
-  const XSet x0 = xset(c->xco, 0), x1 = xset(c->xco, 1);
+  XStream a;
+  const double *gins[3] = {c->w.uu, c->w.uv, c->w.uw};
+  const double *uins[3] = {c->f[OTBL_F_U], c->f[OTBL_F_V], c->f[OTBL_F_W]};
+  double *outs[3] = {c->w.cu, c->w.cv, c->w.cw};
+  double *cks[3] = {c->w.s1, c->w.s2, c->w.s3};
+  const int which[3] = {0, 1, 1}, np[3] = {npu, npv, npu};
+  for (int f = 0; f < 3; ++f) {
+    a.in[f] = gins[f];
+    a.in2[f] = uins[f];
+    a.out[f] = outs[f];
+    a.ck[f] = cks[f];
+    a.which[f] = which[f];
+    a.np[f] = np[f];
+  }
   prof_begin(c, PK_DIFVISX);
-  cudaFuncSetAttribute(k_difvisx, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_difvisx<<<gu, T, smem, c->stream>>>(c->dc, x0, c->w.uu, c->f[OTBL_F_U], c->w.cu, 0, npu, Lp);
-  k_difvisx<<<gv, T, smem, c->stream>>>(c->dc, x1, c->w.uv, c->f[OTBL_F_V], c->w.cv, 1, npv, Lp);
-  k_difvisx<<<gu, T, smem, c->stream>>>(c->dc, x1, c->w.uw, c->f[OTBL_F_W], c->w.cw, 1, npu, Lp);
+  k_difvisx<<<dim3((npu + 127) / 128, 3), 128, 0, c->stream>>>(c->dc, a);
   prof_end(c);
-  c->launches += 3;
+  c->launches += 1;
   return cudaGetLastError();
 }
 

@@ -1,13 +1,13 @@
 // CUDA kernels of the RK3 substep (sm_100a, FP64).
 //
 // Stage map (reference routine -> kernel):
-//   interpxx  lip.f90:248   k_interpx     x-lines, compact mid-point interp.
+//   interpxx  lip.f90:248   k_interpx     x-lines (one thread per line), mid-point interp.
 //   interpyy  lip.f90:359   k_interpy     y-lines in Fourier space
 //   fourxz    ffts.f90:27   k_products    z-lines: 9 c2r + 6 r2c per (i,j)
 //                                          line, the six nonlinear products
 //                                          and the CFL maxima (rhsp.F90:120-171,
 //                                          367-415)
-//   difvisxx  lip.f90:52    k_difvisx     x-lines, d/dx(product) + d2/dx2
+//   difvisxx  lip.f90:52    k_difvisx     x-lines (one thread per line), d/dx + d2/dx2
 //   dt        rhsp.F90:214  k_dt          dt, RK3 factors, implzy LU factors
 //   genflu    genflu.F90:3  k_genflu_tab  integral quantities, rescaling tables
 //                           k_genflu_cols inflow plane + boun of plane 1

@@ -57,49 +57,6 @@ void interleave(double *dst, int n, int nch, int CL, F f) {
     }
 }
 
-// The x-line coefficients of lip.f90 (interpxx, difvisxx) in the
-// chunk-interleaved order of the x-line kernels (32 lanes per line).
-int build_xco(otbl_ctx *c, const otbl_coef_offsets &o) {
-  const int nx = c->cfg.nx;
-  const int CL = xline_cl(nx);
-  const size_t len = (size_t)CL * 32;
-  double *dev = nullptr;
-  int st = dalloc(c, &dev, 2 * (size_t)XCO_N * len);
-  if (st != OTBL_OK) return st;
-  std::vector<double> h(2 * (size_t)XCO_N * len);
-  const double *H = c->coef_host.data();
-  auto F = [&](int id) { return H + o.off[id]; };
-  auto ci = [&](int r) { return std::min(std::max(r + 1, 2), nx - 1); };  // stencil row, 1-based
-  for (int which = 0; which < 2; ++which) {
-    const double *inx = F(which == 0 ? OTBL_C_INXU : OTBL_C_INXV);
-    const double *cofi = F(which == 0 ? OTBL_C_COFIUX : OTBL_C_COFIVX);
-    const double *dcx = F(which == 0 ? OTBL_C_DCXU : OTBL_C_DCXV);
-    const double *vix = F(which == 0 ? OTBL_C_VIXU : OTBL_C_VIXV);
-    const double *cofc = F(which == 0 ? OTBL_C_COFCXU : OTBL_C_COFCXV);
-    const double *cofv = F(which == 0 ? OTBL_C_COFVXU : OTBL_C_COFVXV);
-    double *base = h.data() + (size_t)which * XCO_N * len;
-    auto put = [&](int kind, auto f) { interleave(base + (size_t)kind * len, nx, 32, CL, f); };
-    // solves: row r (0-based) uses Fortran column r + 1 of the (3, nx) array
-    for (int q = 0; q < 3; ++q) {
-      put(XI_L + q, [&](int r) { return inx[(size_t)r * 3 + q]; });
-      put(XD_L + q, [&](int r) { return dcx[(size_t)r * 3 + q]; });
-      put(XV_L + q, [&](int r) { return vix[(size_t)r * 3 + q]; });
-      put(XV_F1 + q, [&](int r) { return cofv[(size_t)(ci(r) - 1) * 3 + q]; });
-    }
-    for (int q = 0; q < 2; ++q) {
-      put(XI_E1 + q, [&](int r) { return cofi[(size_t)(ci(r) - 1) * 2 + q]; });
-      put(XD_E1 + q, [&](int r) { return cofc[(size_t)(ci(r) - 1) * 2 + q]; });
-    }
-    for (int k = 0; k < XCO_N; ++k) c->xco.k[which][k] = dev + ((size_t)which * XCO_N + k) * len;
-  }
-  c->xco.CL = CL;
-  if (cudaMemcpy(dev, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
-    c->err = "coefficient upload failed";
-    return OTBL_ERR_CUDA;
-  }
-  return OTBL_OK;
-}
-
 // rows of each y-line operator (YCoKind) for which 0 (u,w) / 1 (v)
 int yco_rows(int kind, int which, int ny) {
   const int jee = which == 0 ? ny + 1 : ny;
@@ -304,7 +261,6 @@ extern "C" int otbl_ctx_create(const otbl_config *cfg, const double *coef, int d
   TRY(dalloc(c, &w.fac_v, 3 * (size_t)(ny + 4)));
   TRY(dalloc(c, &w.gf, genflu_tab_doubles(ny)));
   TRY(dalloc(c, &w.pois_dinv, (size_t)nx * ny * (nz1 / 2)));
-  TRY(build_xco(c, o));
   TRY(build_yco(c, o));
 #undef TRY
   if (check(c, launch_twiddles(c), "twiddles") != OTBL_OK || check(c, launch_pois_lu(c), "pois_lu") != OTBL_OK || check(c, cudaStreamSynchronize(c->stream), "init")) {

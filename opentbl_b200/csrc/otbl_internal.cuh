@@ -28,34 +28,6 @@ struct DCoef {
   const double *viyu, *viyv, *vyui, *vyvi, *cofvyu, *cofvyv, *cofvby, *ccon;
 };
 
-// Chunk-interleaved copies (lines.cuh CCo) of the x-line coefficients, for
-// 32 lanes per line and chunks of CL rows (xline_cl). Index [which][kind]:
-// which 0 = u, 1 = v,w (lip.f90 chi/chv selections).
-enum XCoKind {
-  XI_L, XI_D, XI_U,          // interpxx solve: inxu / inxv
-  XI_E1, XI_E2,              // interpxx stencil: cofiux / cofivx at row clamp(r+1, 2, nx-1)
-  XD_L, XD_D, XD_U,          // difvisxx first derivative solve: dcxu / dcxv
-  XV_L, XV_D, XV_U,          // difvisxx second derivative solve: vixu / vixv
-  XD_E1, XD_E2,              // cofcxu / cofcxv at clamp(r+1, 2, nx-1)
-  XV_F1, XV_F2, XV_F3,       // cofvxu / cofvxv at clamp(r+1, 2, nx-1)
-  XCO_N
-};
-struct XCo {
-  const double *k[2][XCO_N];
-  int CL;
-};
-// the set of one `which`, passed by value to a kernel
-struct XSet {
-  const double *k[XCO_N];
-  int CL;
-};
-inline XSet xset(const XCo &x, int which) {
-  XSet s;
-  for (int q = 0; q < XCO_N; ++q) s.k[q] = x.k[which][q];
-  s.CL = x.CL;
-  return s;
-}
-
 // Chunk-interleaved copies of the y-line coefficients, for 8 lanes per
 // column and one chunk length CL = yline_cl(ny) for every operator (the
 // operators have ny-1 .. ny+1 rows; jee = ny+1 for u-type, ny for v-type).
@@ -90,9 +62,8 @@ inline YSet yset(const YCo &y, int which) {
   return s;
 }
 
-// Chunk lengths: 32 lanes per x-line; 8 lanes per y-column with one length
-// for all y operators, rounded to 2 mod 4 (lines.cuh chunk_len).
-inline int xline_cl(int nx) { return (nx + 31) / 32; }
+// Chunk length of the y-line kernels: 8 lanes per column, one length for
+// all y operators, rounded to 2 mod 4 (lines.cuh chunk_len).
 inline int yline_cl(int ny) {  // 8 lanes, rows up to ny+1, 2 mod 4
   int c = (ny + 1 + 7) / 8;
   c += (6 - (c & 3)) & 3;
@@ -135,7 +106,6 @@ struct otbl_ctx {
   int device;
   cudaStream_t stream;
   otbl::DCoef dc;
-  otbl::XCo xco;
   otbl::YCo yco;
   double *coef_dev;
   std::vector<double> coef_host;
