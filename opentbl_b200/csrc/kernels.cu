@@ -29,7 +29,6 @@
 
 #include "devcommon.cuh"
 #include "fft.cuh"
-#include "lines.cuh"
 #include "otbl_internal.cuh"
 
 namespace otbl {
@@ -389,44 +388,38 @@ __global__ void __launch_bounds__(128) k_products_r(DCoef c, ZTab z, ProdArgs a)
 // dt (rhsp.F90:214-267), RK3 factors, implzy LU (lip.f90:545-568)
 // ---------------------------------------------------------------------------
 // LU of (A + var1*B) for implzy, lip.f90:545-568, rows j = 2..jee-1, as a
-// register recurrence. The factors go to the chunk-interleaved copy `fi` of
-// the y-line kernels (YM_L, YM_D, YM_U at fi, fi + len, fi + 2 len, row r =
-// j - 2); fac keeps the two boundary couplings that implzy moves to the
-// right-hand side (fac[3*(jee+1)] = a(2), fac[3*(jee+1)+1] = c(jee-1)).
-__device__ void implzy_factor(const DCoef &c, double *fac, double *fi, int which, double var1, int CL) {
+// register recurrence: fac[3j], fac[3j+1], fac[3j+2] = lower, inverse pivot,
+// upper of row j (lower of row 2 and upper of row jee-1 are 0), and the two
+// boundary couplings that implzy moves to the right-hand side,
+// fac[3*(jee+1)] = a(2), fac[3*(jee+1)+1] = c(jee-1).
+__device__ void implzy_factor(const DCoef &c, double *fac, int which, double var1) {
   const int ny = c.ny, jee = which == 0 ? ny + 1 : ny;
   const double *icon = which == 0 ? c.vyui : c.vyvi;
   const double *econ = which == 0 ? c.cofvyu : c.cofvyv;
-  const size_t len = 8 * (size_t)CL;
-  auto at = [&](int j) {
-    const int r = j - 2;
-    return (size_t)(r % CL) * 8 + r / CL;
-  };
   fac[3 * (jee + 1)] = A3(icon, 1, 2) + var1 * A3(econ, 3, 2);
   fac[3 * (jee + 1) + 1] = A3(icon, 3, jee - 1) + var1 * A3(econ, 1, jee - 1);
   double bprev = A3(icon, 2, 2) + var1 * A3(econ, 2, 2);
   double cprev = jee - 1 == 2 ? 0.0 : A3(icon, 3, 2) + var1 * A3(econ, 1, 2);
-  fi[at(2)] = 0.0;
-  fi[2 * len + at(2)] = cprev;
+  fac[3 * 2] = 0.0;
+  fac[3 * 2 + 2] = cprev;
   for (int j = 3; j <= jee - 1; ++j) {
     const double d = 1.0 / bprev;
-    fi[len + at(j - 1)] = d;
+    fac[3 * (j - 1) + 1] = d;
     const double aj = -(A3(icon, 1, j) + var1 * A3(econ, 3, j)) * d;
     const double bj = (A3(icon, 2, j) + var1 * A3(econ, 2, j)) + aj * cprev;
     const double cj = j == jee - 1 ? 0.0 : A3(icon, 3, j) + var1 * A3(econ, 1, j);
-    fi[at(j)] = aj;
-    fi[2 * len + at(j)] = cj;
+    fac[3 * j] = aj;
+    fac[3 * j + 2] = cj;
     bprev = bj;
     cprev = cj;
   }
-  fi[len + at(jee - 1)] = 1.0 / bprev;
+  fac[3 * (jee - 1) + 1] = 1.0 / bprev;
 }
 
 // One CTA of 64 threads: the CFL reduction over the rows, then dt, the RK3
 // factors and the two implzy factorisations (one warp each).
 __global__ void __launch_bounds__(64) k_dt(DCoef c, DState *st, const unsigned long long *vm_bits, double *fac_u,
-                                           double *fac_v, double *fi_u, double *fi_v, int ycl, int m,
-                                           int setstep, int dt_mode, double dt_fixed) {
+                                           double *fac_v, int m, int setstep, int dt_mode, double dt_fixed) {
   __shared__ double s_dt3[2], s_vmax[2];
   const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
   const double *S = c.S;
@@ -483,9 +476,9 @@ __global__ void __launch_bounds__(64) k_dt(DCoef c, DState *st, const unsigned l
   if (lane == 0) {
     const double rkk = *(volatile double *)&st->rkk;
     if (wid == 0)
-      implzy_factor(c, fac_u, fi_u, 0, rkk, ycl);
+      implzy_factor(c, fac_u, 0, rkk);
     else
-      implzy_factor(c, fac_v, fi_v, 1, rkk, ycl);
+      implzy_factor(c, fac_v, 1, rkk);
   }
 }
 
@@ -1174,8 +1167,8 @@ cudaError_t launch_products(otbl_ctx *c, int setstep) {
 
 cudaError_t launch_dt(otbl_ctx *c, int m, int setstep) {
   prof_begin(c, PK_DT);
-  k_dt<<<1, 64, 0, c->stream>>>(c->dc, c->st, c->w.vm_bits, c->w.fac_u, c->w.fac_v, c->yco.fac[0],
-                                c->yco.fac[1], c->yco.CL, m, setstep, c->cfg.dt_mode, c->cfg.dt_fixed);
+  k_dt<<<1, 64, 0, c->stream>>>(c->dc, c->st, c->w.vm_bits, c->w.fac_u, c->w.fac_v, m, setstep,
+                                c->cfg.dt_mode, c->cfg.dt_fixed);
   prof_end(c);
   c->launches += 1;
   return cudaGetLastError();

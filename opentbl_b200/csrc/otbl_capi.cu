@@ -5,7 +5,6 @@
 #include <cstdio>
 #include <cstring>
 
-#include "lines.cuh"
 #include "otbl_internal.cuh"
 
 using namespace otbl;
@@ -44,91 +43,6 @@ int dalloc(otbl_ctx *c, T **p, size_t count) {
 size_t field_len(const otbl_ctx *c, int id) {
   const int ut = (id == OTBL_F_U || id == OTBL_F_W || id == OTBL_F_RHSUPA || id == OTBL_F_RHSWPA);
   return otbl_field_len(c->cfg.nx, c->cfg.ny, c->cfg.nz, ut);
-}
-
-// Chunk-interleaved copy (lines.cuh CCo) of f(r), r = 0..n-1, for nch lanes
-// per line and chunks of CL rows; rows past n are 0 and never read.
-template <class F>
-void interleave(double *dst, int n, int nch, int CL, F f) {
-  for (int h = 0; h < nch; ++h)
-    for (int t = 0; t < CL; ++t) {
-      const int r = h * CL + t;
-      dst[(size_t)t * nch + h] = r < n ? f(r) : 0.0;
-    }
-}
-
-// rows of each y-line operator (YCoKind) for which 0 (u,w) / 1 (v)
-int yco_rows(int kind, int which, int ny) {
-  const int jee = which == 0 ? ny + 1 : ny;
-  if (kind <= YI_E2) return ny;
-  if (kind <= YV_F3) return jee;
-  if (kind <= YM_U) return jee - 2;
-  if (kind <= YP_A3) return ny - 1;
-  return ny;
-}
-
-// The y-line coefficients of lip.f90 (interpyy, differzy, vistyy, implzy),
-// of the Poisson operator (pois.f90, ayp) and idyy, in the chunk-interleaved
-// order of the y-line kernels (8 lanes per column). The implzy factors are
-// rewritten by k_dt every substep.
-int build_yco(otbl_ctx *c, const otbl_coef_offsets &o) {
-  const int ny = c->cfg.ny;
-  const int CL = yline_cl(ny);
-  size_t off[2][YCO_N], total = 0;
-  for (int which = 0; which < 2; ++which)
-    for (int k = 0; k < YCO_N; ++k) {
-      off[which][k] = total;
-      total += 8 * (size_t)CL;
-    }
-  double *dev = nullptr;
-  int st = dalloc(c, &dev, total);
-  if (st != OTBL_OK) return st;
-  std::vector<double> h(total, 0.0);
-  const double *H = c->coef_host.data();
-  auto F = [&](int id) { return H + o.off[id]; };
-  auto cl = [](int v, int lo, int hi) { return std::min(std::max(v, lo), hi); };
-  for (int which = 0; which < 2; ++which) {
-    const int jee = which == 0 ? ny + 1 : ny;
-    const double *iny = F(which == 0 ? OTBL_C_INYU : OTBL_C_INYV);
-    const double *cofi = F(which == 0 ? OTBL_C_COFIUY : OTBL_C_COFIVY);
-    const double *dcy = F(which == 0 ? OTBL_C_DCYU : OTBL_C_DCYV);
-    const double *cofc = F(which == 0 ? OTBL_C_COFCYU : OTBL_C_COFCYV);
-    const double *viy = F(which == 0 ? OTBL_C_VIYU : OTBL_C_VIYV);
-    const double *cofv = F(which == 0 ? OTBL_C_COFVYU : OTBL_C_COFVYV);
-    const double *vyi = F(which == 0 ? OTBL_C_VYUI : OTBL_C_VYVI);
-    const double *ayp = F(OTBL_C_AYP), *idyy = F(OTBL_C_IDYY);
-    auto put = [&](int kind, auto f) {
-      interleave(h.data() + off[which][kind], yco_rows(kind, which, ny), 8, CL, f);
-    };
-    // solves: A of row 0 and U of the last row do not enter the sweeps and
-    // are stored as 0, so that padded fixed-length sweeps need no predicate
-    auto solve_coef = [](const double *a, int r, int q, int n) {
-      if ((q == 0 && r == 0) || (q == 2 && r == n - 1)) return 0.0;
-      return a[(size_t)r * 3 + q];
-    };
-    for (int q = 0; q < 3; ++q) {
-      put(YI_L + q, [&](int r) { return solve_coef(iny, r, q, ny); });
-      put(YD_L + q, [&](int r) { return solve_coef(dcy, r, q, jee); });
-      put(YV_L + q, [&](int r) { return solve_coef(viy, r, q, jee); });
-      put(YV_F1 + q, [&](int r) { return cofv[(size_t)(cl(r + 1, 2, jee - 1) - 1) * 3 + q]; });
-      put(YM_F1 + q, [&](int r) { return vyi[(size_t)(std::min(r + 2, jee - 1) - 1) * 3 + q]; });
-    }
-    for (int q = 0; q < 2; ++q) {
-      put(YI_E1 + q, [&](int r) { return cofi[(size_t)(cl(r + 1, 2, ny - 1) - 1) * 2 + q]; });
-      put(YD_E1 + q, [&](int r) { return cofc[(size_t)(cl(r + 1, 2, ny) - 1) * 2 + q]; });
-    }
-    put(YP_A1, [&](int r) { return r > 0 ? ayp[(size_t)r * 3 + 0] : 0.0; });
-    put(YP_A3, [&](int r) { return r < ny - 2 ? ayp[(size_t)r * 3 + 2] : 0.0; });
-    put(Y_IDYY, [&](int r) { return idyy[r]; });
-    for (int k = 0; k < YCO_N; ++k) c->yco.k[which][k] = dev + off[which][k];
-    c->yco.fac[which] = dev + off[which][YM_L];
-  }
-  c->yco.CL = CL;
-  if (cudaMemcpy(dev, h.data(), total * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
-    c->err = "coefficient upload failed";
-    return OTBL_ERR_CUDA;
-  }
-  return OTBL_OK;
 }
 
 int check(otbl_ctx *c, cudaError_t e, const char *where) {
@@ -261,7 +175,6 @@ extern "C" int otbl_ctx_create(const otbl_config *cfg, const double *coef, int d
   TRY(dalloc(c, &w.fac_v, 3 * (size_t)(ny + 4)));
   TRY(dalloc(c, &w.gf, genflu_tab_doubles(ny)));
   TRY(dalloc(c, &w.pois_dinv, (size_t)nx * ny * (nz1 / 2)));
-  TRY(build_yco(c, o));
 #undef TRY
   if (check(c, launch_twiddles(c), "twiddles") != OTBL_OK || check(c, launch_pois_lu(c), "pois_lu") != OTBL_OK || check(c, cudaStreamSynchronize(c->stream), "init")) {
     *out = c;

@@ -28,48 +28,6 @@ struct DCoef {
   const double *viyu, *viyv, *vyui, *vyvi, *cofvyu, *cofvyv, *cofvby, *ccon;
 };
 
-// Chunk-interleaved copies of the y-line coefficients, for 8 lanes per
-// column and one chunk length CL = yline_cl(ny) for every operator (the
-// operators have ny-1 .. ny+1 rows; jee = ny+1 for u-type, ny for v-type).
-// Index [which][kind]: which 0 = u,w, 1 = v (interpyy: 0 = u,w input,
-// 1 = v input).
-enum YCoKind {
-  YI_L, YI_D, YI_U,           // interpyy solve: inyu / inyv, n = ny
-  YI_E1, YI_E2,               // cofiuy / cofivy at clamp(r+1, 2, ny-1)
-  YD_L, YD_D, YD_U,           // differzy solve: dcyu / dcyv, n = jee
-  YD_E1, YD_E2,               // cofcyu / cofcyv at clamp(r+1, 2, ny)
-  YV_L, YV_D, YV_U,           // vistyy solve: viyu / viyv, n = jee
-  YV_F1, YV_F2, YV_F3,        // cofvyu / cofvyv at clamp(r+1, 2, jee-1)
-  YM_F1, YM_F2, YM_F3,        // implzy stencil: vyui / vyvi at min(r+2, jee-1), n = jee-2
-  YM_L, YM_D, YM_U,           // implzy factors of the current dt (k_dt), n = jee-2
-  YP_A1, YP_A3,               // pois y operator: ayp(1, r+1), ayp(3, r+1), n = ny-1
-  Y_IDYY,                     // idyy(r+1), n = ny
-  YCO_N
-};
-struct YCo {
-  const double *k[2][YCO_N];
-  double *fac[2];  // YM_L of each which; YM_D, YM_U follow at +8 CL, +16 CL
-  int CL;
-};
-struct YSet {
-  const double *k[YCO_N];
-  int CL;
-};
-inline YSet yset(const YCo &y, int which) {
-  YSet s;
-  for (int q = 0; q < YCO_N; ++q) s.k[q] = y.k[which][q];
-  s.CL = y.CL;
-  return s;
-}
-
-// Chunk length of the y-line kernels: 8 lanes per column, one length for
-// all y operators, rounded to 2 mod 4 (lines.cuh chunk_len).
-inline int yline_cl(int ny) {  // 8 lanes, rows up to ny+1, 2 mod 4
-  int c = (ny + 1 + 7) / 8;
-  c += (6 - (c & 3)) & 3;
-  return c;
-}
-
 // Scalars that live on the device so that no host synchronisation is needed
 // inside a step (dt is produced by a reduction on the device).
 struct DState {
@@ -106,7 +64,6 @@ struct otbl_ctx {
   int device;
   cudaStream_t stream;
   otbl::DCoef dc;
-  otbl::YCo yco;
   double *coef_dev;
   std::vector<double> coef_host;
   double *f[OTBL_F_COUNT];

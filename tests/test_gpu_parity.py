@@ -139,12 +139,13 @@ def test_c1_divergence_after_transient():
 
 
 @pytest.mark.parametrize("cfg", [
-    replace(config.TINY, nx=17, ny=300, name="tall-17x300x32"),     # y chunks of 38 rows
-    replace(config.TINY, nx=1081, name="long-1081x41x32"),          # x chunks of 34 rows
+    replace(config.TINY, nx=17, ny=300, name="tall-17x300x32"),
+    replace(config.TINY, nx=1081, name="long-1081x41x32"),
 ], ids=lambda c: c.name)
-def test_shared_memory_fallback_paths(cfg):
-    """Grids whose line chunks are longer than the register kernels are
-    compiled for take the shared-memory sweeps; same bound as the main path."""
+def test_long_lines(cfg):
+    """Lines much longer than the default boxes' (300 rows in y, 1081 planes
+    in x): many checkpoint segments per line in the streaming Thomas sweeps
+    and a ragged last segment; same bound as the main path."""
     g, o, init, coef = _pair(cfg)
     g.substep(1, True)
     o.substep(1, 1)
