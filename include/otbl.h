@@ -97,6 +97,13 @@ int otbl_field_device_ptr(otbl_ctx *ctx, int id, double **dptr);
 int otbl_set_inflow(otbl_ctx *ctx, const double *u0, const double *v0,
                     const double *um, const otbl_inflow *st);
 int otbl_get_inflow(otbl_ctx *ctx, double *um, otbl_inflow *st);
+/* ener(1:15) of module statistics (mod.F90:264) as rhsp leaves it: set by
+ * energies at substep m = 1 (rhsp.F90:116, rhsp.F90:493-509 with ministats,
+ * stotf.F90:395-440) from the state rhsp was called on, ener(13:15) zeroed
+ * at the end of rhsp (rhsp.F90:487). One context holds every plane, so the
+ * values are those of plane nx/2 (its branch of ministats overwrites the
+ * plane-1 branch's ener(1:3)). Zero before the first rhsp(m = 1). */
+int otbl_get_energies(otbl_ctx *ctx, double *ener);
 
 /* ---- the substep, bl_1.F90:94-125 ----
  * m = RK3 substep 1..3; setstep = 1 recomputes dt (adaptive mode). */

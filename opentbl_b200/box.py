@@ -88,6 +88,13 @@ class Box:
         self._check(self.L.otbl_get_inflow(self.h, native.dptr(um), ctypes.byref(st)), "otbl_get_inflow")
         return um, {n: getattr(st, n) for n, _ in OtblInflow._fields_}
 
+    def energies(self):
+        """ener(1:15) as rhsp leaves it (rhsp.F90:116,487): energy integrals
+        and wall-row values of plane nx/2 from the last substep m = 1."""
+        e = np.zeros(15)
+        self._check(self.L.otbl_get_energies(self.h, native.dptr(e)), "otbl_get_energies")
+        return e
+
     @property
     def stream(self) -> int:
         """Raw cudaStream_t of the context (for torch.cuda.ExternalStream)."""

@@ -491,6 +491,53 @@ __global__ void k_reset_max(DState *st, unsigned long long *vm_bits, int ny) {
   if (t <= ny) vm_bits[t] = 0ull;
 }
 
+// energies + ministats (rhsp.F90:493-509, stotf.F90:395-440) when one
+// context holds every plane: ministats' plane-1 branch sets uner(1:3) and its
+// plane-nx/2 branch, later in the same loop over planes, overwrites them, so
+// the result is that of plane nx/2 alone, including the reference's addition
+// of Re u(k=0, j=1)^2 to every row of aux (stotf.F90:433-435). rhsp zeroes
+// ener(13:15) before it returns (rhsp.F90:487); so does this kernel.
+// One CTA; warp w takes rows j = w, w+32, ..., lanes the modes k = 1..nz2;
+// the per-warp partial integrals are added in warp order.
+__global__ void __launch_bounds__(1024) k_energies(DCoef c, DState *st, const double *u, const double *v,
+                                                  const double *w) {
+  __shared__ double part[3][32], row2[3][2];
+  const int ny = c.ny, nz1 = c.nz1, i = c.nx / 2;
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+  for (int f = 0; f < 3; ++f) {
+    const int jee = f == 1 ? ny : ny + 1;
+    const double *g = (f == 0 ? u : (f == 1 ? v : w)) + (size_t)(i - 1) * jee * nz1;
+    const double r1 = g[0];
+    double acc = 0.0;
+    for (int j = wp; j < jee; j += 32) {
+      double s = 0.0;
+      for (int kr = 2 + lane; kr < nz1; kr += 32) {
+        const double x = g[(size_t)j * nz1 + kr];
+        s += x * x;
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      const double a = 2.0 * s;
+      if (j < 2 && lane == 0) row2[f][j] = a;
+      acc += (a + r1 * r1) * c.hy[j];
+    }
+    if (lane == 0) part[f][wp] = acc;
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    const int f = threadIdx.x, jee = f == 1 ? ny : ny + 1;
+    const double *g = (f == 0 ? u : (f == 1 ? v : w)) + (size_t)(i - 1) * jee * nz1;
+    double e = 0.0;
+    for (int q = 0; q < 32; ++q) e += part[f][q];
+    st->ener[f] = e;
+    const double q4[4] = {g[0], g[nz1], row2[f][0], row2[f][1]};
+    for (int q = 0; q < 4; ++q) {
+      const int n = 3 + 4 * f + q;
+      st->ener[n] = n >= 12 ? 0.0 : q4[q];
+    }
+  }
+}
+
 __global__ void k_tiempo(DState *st) {
   if (threadIdx.x == 0 && blockIdx.x == 0) st->tiempo = st->tiempo + st->dt;
 }
@@ -1304,6 +1351,12 @@ cudaError_t launch_pois(otbl_ctx *c, int m) {
 cudaError_t launch_boun_all(otbl_ctx *c) {
   dim3 g((c->dc.nz1 + 127) / 128, c->cfg.nx);
   k_boun<<<g, 128, 0, c->stream>>>(c->dc, c->f[OTBL_F_U], c->f[OTBL_F_V], c->f[OTBL_F_W]);
+  c->launches += 1;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_energies(otbl_ctx *c) {
+  k_energies<<<1, 1024, 0, c->stream>>>(c->dc, c->st, c->f[OTBL_F_U], c->f[OTBL_F_V], c->f[OTBL_F_W]);
   c->launches += 1;
   return cudaGetLastError();
 }

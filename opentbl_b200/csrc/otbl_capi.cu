@@ -121,6 +121,7 @@ extern "C" int otbl_ctx_create(const otbl_config *cfg, const double *coef, int d
   d.kmod = P(OTBL_C_KMOD);
   d.ayp = P(OTBL_C_AYP);
   d.vmagic = P(OTBL_C_VMAGIC);
+  d.hy = P(OTBL_C_HY);
   d.inxu = P(OTBL_C_INXU);
   d.inxv = P(OTBL_C_INXV);
   d.cofiux = P(OTBL_C_COFIUX);
@@ -284,6 +285,14 @@ extern "C" int otbl_get_inflow(otbl_ctx *c, double *um, otbl_inflow *s) {
   return OTBL_OK;
 }
 
+extern "C" int otbl_get_energies(otbl_ctx *c, double *ener) {
+  if (!c || !ener) return OTBL_ERR_ARG;
+  cudaSetDevice(c->device);
+  OTBL_CUDA_TRY(c, cudaMemcpyAsync(ener, c->st->ener, sizeof(double) * 15, cudaMemcpyDeviceToHost, c->stream));
+  OTBL_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  return OTBL_OK;
+}
+
 #define LAUNCH(c, x)                                       \
   do {                                                     \
     int s__ = check((c), (x), #x);                         \
@@ -293,6 +302,7 @@ extern "C" int otbl_get_inflow(otbl_ctx *c, double *um, otbl_inflow *s) {
 extern "C" int otbl_rhsp(otbl_ctx *c, int m, int setstep) {
   if (!c || m < 1 || m > 3) return OTBL_ERR_ARG;
   cudaSetDevice(c->device);
+  if (m == 1) LAUNCH(c, launch_energies(c));
   if (setstep) LAUNCH(c, launch_reset_max(c));
   LAUNCH(c, launch_interpx(c));
   LAUNCH(c, launch_interpy(c));

@@ -19,7 +19,7 @@ struct DCoef {
   int nx, ny, nz, nz1, nz2, xout;
   int xround;  // OTBL_XPOSE_FP32: round x-line inputs/outputs to REAL4
   const double *S;
-  const double *y, *dy, *idy, *idyy, *dymin, *kaz, *kaz2, *kvis, *kmod, *ayp, *vmagic;
+  const double *y, *dy, *idy, *idyy, *dymin, *kaz, *kaz2, *kvis, *kmod, *ayp, *vmagic, *hy;
   const double *inxu, *inxv, *cofiux, *cofivx, *inbx;
   const double *dcxu, *dcxv, *cofcxu, *cofcxv, *dcbx;
   const double *vixu, *vixv, *cofvxu, *cofvxv, *cofvbx;
@@ -35,6 +35,7 @@ struct DState {
   double utauout, rthout, dout, gamma1, gamma2;
   double var1, var2, var3, var4, rkk, varstep;  // RK3 factors of the substep
   double umax, wmax, vmax;
+  double ener[15];  // energies of rhsp.F90:116 (module statistics, mod.F90:264)
   unsigned long long umax_bits, wmax_bits;      // atomicMax targets (>= 0)
   int err;        // OTBL_ERR_NAN when the dt reduction saw a non-finite value
   int dt_frozen;  // fixed-dt mode: dt taken
@@ -118,6 +119,7 @@ cudaError_t launch_pois(otbl_ctx *c, int m);
 cudaError_t launch_reset_max(otbl_ctx *c);
 cudaError_t launch_boun_all(otbl_ctx *c);
 cudaError_t launch_tiempo(otbl_ctx *c);
+cudaError_t launch_energies(otbl_ctx *c);
 cudaError_t launch_twiddles(otbl_ctx *c);
 cudaError_t launch_pois_lu(otbl_ctx *c);
 cudaError_t launch_pois_solve(otbl_ctx *c, double *phi);

@@ -71,6 +71,7 @@ def _bind(L):
         "otbl_field_device_ptr": ([P, I, ctypes.POINTER(D)], I),
         "otbl_set_inflow": ([P, D, D, D, ctypes.POINTER(OtblInflow)], I),
         "otbl_get_inflow": ([P, D, ctypes.POINTER(OtblInflow)], I),
+        "otbl_get_energies": ([P, D], I),
         "otbl_rhsp": ([P, I, I], I),
         "otbl_outflow_correction": ([P], I),
         "otbl_pois": ([P, I], I),

@@ -26,6 +26,7 @@ struct orc_box {
   double *um, *u0, *v0;
   double tiempo, timeinit, dt, utauout, rthout, dout, gamma1, gamma2, timec;
   double umax, wmax, vmax;
+  double ener[15]; /* module statistics, mod.F90:264 */
   int dt_frozen;
   /* planes */
   double *resu, *resv, *resw, *rhsu, *rhsv, *rhsw, *wk1, *wk2, *wk3;
@@ -595,6 +596,54 @@ static inline void cmul_kaz(double kz, const double *a, double *out_re, double *
   *out_im = a[0] * kz;
 }
 
+/* energies (rhsp.F90:493-509): ministats (stotf.F90:395-440) on every
+ * plane in order, here the whole box in one domain, so the allreduce is the
+ * identity. Plane 1 sets uner(1:3); plane nx/2 (integer division) sets
+ * uner(4:15) and then overwrites uner(1:3), each row of aux adding
+ * Re(u(0,1))^2 as written at stotf.F90:433-435. Sums run over j in order. */
+static void orc_energies(orc_box *b) {
+  const int nx = b->nx, ny = b->ny, nz1 = b->nz1, nz2 = b->nz2;
+  const double *hy = CF(b, HY);
+  double uner[15] = {0};
+  for (int i = 1; i <= nx; ++i) {
+    if (i != 1 && i != nx / 2) continue;
+    for (int f = 0; f < 3; ++f) {
+      const int jee = f == 1 ? ny : ny + 1;
+      const double *g = b->f[f == 0 ? OTBL_F_U : (f == 1 ? OTBL_F_V : OTBL_F_W)] + (size_t)(i - 1) * jee * nz1;
+      if (i == 1) { /* stotf.F90:406-414 */
+        double e = 0.0;
+        for (int j = 0; j < jee; ++j) {
+          double a = 0.0;
+          for (int k = 0; k <= nz2; ++k) a += g[(size_t)j * nz1 + 2 * k] * g[(size_t)j * nz1 + 2 * k] +
+                                            g[(size_t)j * nz1 + 2 * k + 1] * g[(size_t)j * nz1 + 2 * k + 1];
+          e += a * hy[j];
+        }
+        uner[f] = e;
+      }
+      if (i == nx / 2) { /* stotf.F90:417-438 */
+        const double r1 = g[0];
+        double e = 0.0, a01[2] = {0.0, 0.0};
+        for (int j = 0; j < jee; ++j) {
+          double s = 0.0;
+          for (int k = 1; k <= nz2; ++k) s += g[(size_t)j * nz1 + 2 * k] * g[(size_t)j * nz1 + 2 * k] +
+                                            g[(size_t)j * nz1 + 2 * k + 1] * g[(size_t)j * nz1 + 2 * k + 1];
+          const double a = 2.0 * s;
+          if (j < 2) a01[j] = a;
+          e += (a + r1 * r1) * hy[j];
+        }
+        uner[3 + 4 * f] = g[0];
+        uner[4 + 4 * f] = g[nz1];
+        uner[5 + 4 * f] = a01[0];
+        uner[6 + 4 * f] = a01[1];
+        uner[f] = e;
+      }
+    }
+  }
+  memcpy(b->ener, uner, sizeof uner);
+}
+
+void orc_get_energies(orc_box *b, double *ener) { memcpy(ener, b->ener, sizeof(double) * 15); }
+
 int orc_rhsp(orc_box *b, int m, int setstep) {
   const int nx = b->nx, ny = b->ny, nz = b->nz, nz1 = b->nz1, nz2 = b->nz2;
   const int mpu = nz1 * (ny + 1), mpv = nz1 * ny;
@@ -606,6 +655,8 @@ int orc_rhsp(orc_box *b, int m, int setstep) {
   const double *idyy = CF(b, IDYY), *dymin = CF(b, DYMIN);
   const double *inby = CF(b, INBY);
   const int nth = orc_get_threads();
+
+  if (m == 1) orc_energies(b); /* rhsp.F90:116, on the state rhsp was called on */
 
   /* planes -> pencils and x-interpolation, rhsp.F90:67-69,105-112 */
   orc_chp2x(b, b->penu, u, ny + 1);
@@ -923,6 +974,7 @@ int orc_rhsp(orc_box *b, int m, int setstep) {
     orc_implzy(b, PL(b, v, ny, i, 1), PL(b, wk2, ny, i, 1), 1, rkk);
     orc_implzy(b, PL(b, w, ny + 1, i, 1), PL(b, wk3, ny + 1, i, 1), 0, rkk);
   }
+  b->ener[12] = b->ener[13] = b->ener[14] = 0.0; /* rhsp.F90:487 */
   return OTBL_OK;
 }
 

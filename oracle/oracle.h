@@ -53,6 +53,8 @@ void orc_set_inflow(orc_box *b, const double *u0, const double *v0,
 void orc_get_inflow(orc_box *b, double *um, otbl_inflow *st);
 
 int orc_rhsp(orc_box *b, int m, int setstep);
+/* ener(1:15) as rhsp leaves it (rhsp.F90:116,487) */
+void orc_get_energies(orc_box *b, double *ener);
 void orc_outflow_correction(orc_box *b);
 void orc_pois(orc_box *b, int m);
 int orc_substep(orc_box *b, int m, int setstep);

@@ -53,6 +53,7 @@ def lib():
         L.orc_field.argtypes = [P, ctypes.c_int]
         L.orc_set_inflow.argtypes = [P, D, D, D, ctypes.POINTER(OtblInflow)]
         L.orc_get_inflow.argtypes = [P, D, ctypes.POINTER(OtblInflow)]
+        L.orc_get_energies.argtypes = [P, D]
         for n in ("orc_rhsp", "orc_substep"):
             getattr(L, n).argtypes = [P, ctypes.c_int, ctypes.c_int]
             getattr(L, n).restype = ctypes.c_int
@@ -139,6 +140,11 @@ class OracleBox:
         st = OtblInflow()
         self.L.orc_get_inflow(self.h, dptr(um), ctypes.byref(st))
         return um, {n: getattr(st, n) for n, _ in OtblInflow._fields_}
+
+    def energies(self):
+        e = np.zeros(15)
+        self.L.orc_get_energies(self.h, dptr(e))
+        return e
 
     def rhsp(self, m, setstep):
         return self.L.orc_rhsp(self.h, m, setstep)

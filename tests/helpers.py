@@ -19,6 +19,20 @@ def rel_l2(a, b):
     return float(np.linalg.norm((a - b).ravel()) / (nb if nb > 0 else 1.0))
 
 
+def velocity_rel_l2(g, o):
+    """Relative L2 of the velocity over u, v, w together, Parseval-weighted
+    (mode k = 0 counted once, k > 0 twice, as stotf.F90:155); g and o map
+    "u", "v", "w" to (nx, rows, nz1) arrays."""
+    num = den = 0.0
+    for n in "uvw":
+        a, b = np.asarray(g[n]), np.asarray(o[n])
+        wgt = np.full(a.shape[-1], 2.0)
+        wgt[:2] = 1.0
+        num += float((((a - b) ** 2) * wgt).sum())
+        den += float(((b ** 2) * wgt).sum())
+    return (num / den) ** 0.5
+
+
 def max_abs(a):
     return float(np.max(np.abs(a)))
 

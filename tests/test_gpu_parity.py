@@ -16,7 +16,7 @@ import pytest
 from opentbl_b200 import Box, config, native
 from opentbl_b200.config import replace
 
-from helpers import divergence_np, oracle_box, rel_l2, setup
+from helpers import divergence_np, oracle_box, rel_l2, setup, velocity_rel_l2
 
 pytestmark = pytest.mark.gpu
 
@@ -45,6 +45,9 @@ def test_rhsp_outflow_pois_one_substep(name):
     assert abs(gi["dt"] - oi["dt"]) <= 1e-14 * oi["dt"]
     for k in ("utauout", "rthout", "gamma1", "gamma2", "dout"):
         assert abs(gi[k] - oi[k]) <= 1e-12 * max(1.0, abs(oi[k])), (k, gi[k], oi[k])
+    eg, eo = g.energies(), o.energies()
+    assert np.allclose(eg, eo, rtol=1e-13, atol=1e-300), (eg, eo)
+    assert eo[:3].min() > 0 and not eo[12:].any()
     g.outflow_correction()
     o.outflow_correction()
     e = _compare(g, o, ("u", "rhsupa"))
@@ -102,6 +105,33 @@ def test_c1_one_step():
     do = np.abs(divergence_np(cfg, coef, o.field("u"), o.field("v"), o.field("w"))).max()
     print("C1 after 1 step: max|div| gpu", dg, "oracle", do)
     assert dg <= max(1e-12, 4.0 * do)
+
+
+def test_c1_twenty_steps():
+    """257x97x128, 20 RK3 steps against the oracle: velocity relative L2
+    <= 1e-9 (Parseval weights), max|div u| <= 1e-12, the mean profile at
+    xout, Re_theta and C_f = 2 u_tau^2 (genflu.F90:76-87) to 1e-9, and the
+    energies of the last step."""
+    cfg = config.C1
+    g, o, init, coef = _pair(cfg)
+    g.advance(20)
+    o.advance(20)
+    gv = {n: g.field(n) for n in "uvw"}
+    ov = {n: o.field(n) for n in "uvw"}
+    err = velocity_rel_l2(gv, ov)
+    print("C1 after 20 steps: velocity rel L2", err)
+    assert err <= 1e-9
+    dg = np.abs(divergence_np(cfg, coef, gv["u"], gv["v"], gv["w"])).max()
+    assert dg <= 1e-12, dg
+    x = cfg.resolved_xout() - 1
+    assert rel_l2(gv["u"][x, :, 0], ov["u"][x, :, 0]) <= 1e-9
+    um_g, gi = g.inflow()
+    um_o, oi = o.inflow()
+    assert rel_l2(um_g, um_o) <= 1e-9
+    assert abs(gi["rthout"] - oi["rthout"]) <= 1e-9 * oi["rthout"]
+    cf_g, cf_o = 2.0 * gi["utauout"] ** 2, 2.0 * oi["utauout"] ** 2
+    assert abs(cf_g - cf_o) <= 1e-9 * cf_o
+    assert np.allclose(g.energies(), o.energies(), rtol=1e-9, atol=1e-300)
 
 
 def test_c1_pois_divergence_same_input():

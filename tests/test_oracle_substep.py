@@ -88,6 +88,40 @@ def test_genflu_integrals_against_numpy(tiny, tiempo):
     assert np.all(u[0, :, 1] == 0.0)
 
 
+def _energies_numpy(cfg, coef, u, v, w):
+    """energies/ministats (rhsp.F90:493-509, stotf.F90:395-440) for one
+    domain: plane nx/2's branch, which overwrites plane 1's ener(1:3); then
+    ener(13:15) = 0 (rhsp.F90:487)."""
+    o = native.coef_offsets(cfg)
+    hy = coef[o["HY"]:o["HY"] + cfg.ny + 1]
+    i = cfg.nx // 2 - 1
+    e = np.zeros(15)
+    for f, g in enumerate((u[i], v[i], w[i])):
+        c = g[:, 0::2] + 1j * g[:, 1::2]
+        aux = 2.0 * (np.abs(c[:, 1:]) ** 2).sum(axis=1) + c[0, 0].real ** 2
+        e[f] = (aux * hy[:len(aux)]).sum()
+        e[3 + 4 * f:7 + 4 * f] = (c[0, 0].real, c[1, 0].real,
+                                  aux[0] - c[0, 0].real ** 2, aux[1] - c[0, 0].real ** 2)
+    e[12:] = 0.0
+    return e
+
+
+def test_energies_against_numpy(tiny):
+    """ener after rhsp(m=1) is computed from the state rhsp was called on;
+    substeps 2 and 3 leave it alone."""
+    init, coef = tiny
+    ob = oracle_box(config.TINY, init, coef, threads=2)
+    assert not ob.energies().any()
+    u, v, w = (ob.field(n).copy() for n in "uvw")
+    ob.substep(1, 1)
+    e = ob.energies()
+    ref = _energies_numpy(config.TINY, coef, u, v, w)
+    assert np.allclose(e, ref, rtol=1e-13, atol=0.0), (e, ref)
+    assert e[0] > 0 and e[1] > 0 and e[2] > 0
+    ob.substep(2, 0)
+    assert np.array_equal(ob.energies(), e)
+
+
 def test_real4_transposes_perturb_at_single_precision(tiny):
     init, coef = tiny
     a = oracle_box(config.TINY, init, coef, threads=1)
