@@ -30,7 +30,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 from opentbl_b200 import config as cfgmod  # noqa: E402
-from opentbl_b200 import native, replicas, synth  # noqa: E402
+from opentbl_b200 import diag, native, replicas, synth  # noqa: E402
 from opentbl_b200.box import Box  # noqa: E402
 
 WORKLOAD = "C2"
@@ -45,6 +45,19 @@ def peaks():
             d = json.load(f)
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+# Mixed path (OTBL_PREC_MIXED): element size of each pass of the 55-pass
+# substep schedule (stages A, B, C, D, P of the FP64 figure). FP64: the
+# state u, v, w, p, the RHS history, phi and the divergence; FP32: the x
+# interpolants, the products and partial right-hand sides, and the x-line
+# right-hand sides.
+#   A  reads phi, u, v, w, p; writes u, v, w, p (9 FP64), u_x, v_x, w_x (3 FP32)
+#   B  reads u, v, w (3 FP64), u_x, v_x, w_x; writes 3 products, 3 partial RHS (9 FP32)
+#   C  reads u, v, w (3 FP64), 3 products, 3 partial RHS; writes 3 RHS (9 FP32)
+#   D  reads 3 RHS (3 FP32), RHS history, u, v, w, p; writes u, v, w, RHS history, div (14 FP64)
+#   P  reads div, writes phi (2 FP64)
+MIXED_MANIFEST = {"fp64_passes": 9 + 3 + 3 + 14 + 2, "fp32_passes": 3 + 9 + 9 + 3}
 
 
 def algorithmic_bytes(cfg) -> dict:
@@ -65,6 +78,7 @@ def algorithmic_bytes(cfg) -> dict:
         "pois_bwd": 2 * V,
         "project": V + 2 * (2 * U + 2 * V),
         "substep_survey": 55.0 * U,
+        "substep_mixed": (MIXED_MANIFEST["fp64_passes"] + MIXED_MANIFEST["fp32_passes"] / 2.0) * U,
     }
 
 
@@ -191,6 +205,56 @@ def run_reference(args, cfg, ws, rank):
     print(json.dumps(out), flush=True)
 
 
+def run_mixed(cfg, init, coef, fbox, device, R, warm, K, fp64_ms_per_step):
+    """The mixed-precision path (OTBL_PREC_MIXED) on the same box: device
+    time of K RK3 steps after `warm`, then its error against the FP64 path
+    after the same steps from the same initial state."""
+    import torch
+    mcfg = cfgmod.replace(cfg, precision=1)
+    mbox = Box(mcfg, init, coef, device=device)
+    stream = torch.cuda.ExternalStream(mbox.stream, device=f"cuda:{device}")
+    for _ in range(warm):
+        mbox.advance(1)
+    mbox.sync()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    replicas.barrier(R)
+    torch.cuda.synchronize()
+    with ClockSampler(device) as clk:
+        ev0.record(stream)
+        for _ in range(K):
+            mbox.advance(1)
+        ev1.record(stream)
+        ev1.synchronize()
+    mbox.sync()
+    replicas.barrier(R)
+    ms = replicas.max_over_ranks(ev0.elapsed_time(ev1), R)
+    sub = 3 * K
+    value = replicas.aggregate_rate(cfg.mpts * sub, ms / 1e3, R)
+    mbox.profile(True)
+    mbox.advance(1)
+    prof = mbox.profile_read()
+    mbox.profile(False)
+    per_sub = {k: round(v[0] / 3.0, 4) for k, v in sorted(prof.items(), key=lambda t: -t[1][0])}
+    peak, peak_kind = peaks()
+    ab = algorithmic_bytes(cfg)
+    sub_s = ms / sub / 1e3
+    # error against the FP64 path after the same number of steps
+    nsteps = warm + K + 1
+    fbox.load(init)
+    fbox.advance(nsteps)
+    err = diag.compare(cfg, coef, mbox, fbox)
+    mbox.close()
+    return {"value": value, "unit": UNIT, "ms_per_step": ms / K, "dtype": "f32 operators, f64 state",
+            "speedup_vs_fp64": (fp64_ms_per_step / (ms / K)),
+            "substep_roofline": {"bytes_per_substep": ab["substep_mixed"], "manifest": MIXED_MANIFEST,
+                                 "achieved": ab["substep_mixed"] / sub_s / 1e9, "peak": peak,
+                                 "unit": "GB/s", "frac": ab["substep_mixed"] / sub_s / 1e9 / peak,
+                                 "peak_kind": peak_kind},
+            "kernels_ms_per_substep": per_sub,
+            "err_vs_fp64": dict(steps=nsteps, **err), "clocks": clk.summary()}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -200,6 +264,7 @@ def main():
     ap.add_argument("--config", default=WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
     args = ap.parse_args()
     cfg = getattr(cfgmod, args.config)
     R = replicas.setup()
@@ -300,6 +365,10 @@ def main():
                "job": f"restart upload of the 7 state fields, {K} RK3 steps with per-step "
                       f"diagnostics read-back, checkpoint of u,v,w,p"}
 
+    mixed = None
+    if not args.no_mixed:
+        mixed = run_mixed(cfg, init, coef, box, local, R, warm, K, ms / K)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:
@@ -321,7 +390,8 @@ def main():
                           "parallelism": f"replicas{ws}"},
                "roofline": roofline, "substep_roofline": substep_roofline,
                "kernels_ms_per_substep": kernels,
-               "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks}
+               "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
+               "mixed": mixed}
         print(json.dumps(out), flush=True)
     box.close()
     replicas.teardown(R)

@@ -44,6 +44,16 @@ extern "C" {
 #define OTBL_DT_ADAPTIVE 0
 #define OTBL_DT_FIXED 1
 
+/* arithmetic of the substep (no counterpart in the reference, which is FP64
+ * throughout). OTBL_PREC_FP64: every operator in FP64. OTBL_PREC_MIXED: the
+ * state (u, v, w, p, rhs*pa), the RK3 combination, implzy, the Poisson solve,
+ * the projection, dt, genflu and the energies stay FP64; the x and y
+ * mid-point interpolations, d/dx of difvisxx, the spanwise FFTs and the
+ * nonlinear products run in FP32, and the fifteen intermediate fields they
+ * exchange are stored in FP32. Not combined with OTBL_XPOSE_FP32. */
+#define OTBL_PREC_FP64 0
+#define OTBL_PREC_MIXED 1
+
 typedef struct otbl_config {
   int nx, ny, nz;   /* grid (mod.F90:22); nz1 = 2*(nz/3), nz2 = nz1/2-1     */
   int xout;         /* recycling plane, 1-based (mod.F90:23)               */
@@ -52,6 +62,8 @@ typedef struct otbl_config {
   double re, ax, ay, az, cfl; /* input deck, bl_1.F90:207-210              */
   double y_blend;   /* height that replaces y(119) in genflu.F90:57        */
   double dt_fixed;  /* dt for OTBL_DT_FIXED; <= 0 freezes the first CFL dt */
+  int precision;    /* OTBL_PREC_*                                         */
+  int reserved;     /* 0                                                   */
 } otbl_config;
 
 /* field ids for otbl_set_field / otbl_get_field / otbl_field_device_ptr */

@@ -45,6 +45,11 @@ class Box:
             msg = self.L.otbl_last_error(h).decode() if h.value else ""
             self.close()
             raise OtblError(f"otbl_ctx_create: {native.ERRORS.get(st, st)} {msg}")
+        self.load(init)
+
+    def load(self, init: dict):
+        """Upload a state: the seven fields and the genmod inflow state
+        (getstartzy-bg.F90:18-297, :490-581)."""
         for n in FIELDS:
             self.set_field(n, init[n])
         inf = OtblInflow()

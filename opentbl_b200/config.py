@@ -29,6 +29,7 @@ class BoxConfig:
     xpose_round: int = 0               # 0 none, 1 fp32 (REAL4 transposes)
     dt_mode: int = 0                   # 0 adaptive (reference), 1 fixed
     dt_fixed: float = 0.0
+    precision: int = 0                 # 0 FP64, 1 mixed (OTBL_PREC_*)
     amp: float = 0.05                  # perturbation amplitude / U_inf
     seed: int = 1234
     name: str = ""

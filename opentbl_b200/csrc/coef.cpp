@@ -247,6 +247,8 @@ extern "C" int otbl_config_check(const otbl_config *cfg) {
     return OTBL_ERR_CONFIG;
   if (cfg->xpose_round != 0 && cfg->xpose_round != 1) return OTBL_ERR_CONFIG;
   if (cfg->dt_mode != 0 && cfg->dt_mode != 1) return OTBL_ERR_CONFIG;
+  if (cfg->precision != OTBL_PREC_FP64 && cfg->precision != OTBL_PREC_MIXED) return OTBL_ERR_CONFIG;
+  if (cfg->precision == OTBL_PREC_MIXED && cfg->xpose_round != 0) return OTBL_ERR_CONFIG;
   return OTBL_OK;
 }
 

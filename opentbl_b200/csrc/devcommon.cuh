@@ -13,6 +13,7 @@ namespace otbl {
 
 // REAL4 rounding of the reference's transposes (change.f90:579,608,...)
 __device__ __forceinline__ double rnd(double x, int xr) { return xr ? (double)(float)x : x; }
+__device__ __forceinline__ float rnd(float x, int) { return x; }
 
 // NaN-propagating maximum of non-negative values
 __device__ __forceinline__ double nmax(double m, double v) {

@@ -1,4 +1,5 @@
-// Hand-written FFT building blocks for the substep (sm_100a, FP64).
+// Hand-written FFT building blocks for the substep (sm_100a), in FP64
+// (double2) or, on the mixed-precision path, FP32 (float2).
 //
 // Spanwise transforms (ffts.f90:27-67 fourxz): a real line of nz points is
 // handled as a complex line of M = nz/2 points (even/odd packing) and
@@ -14,62 +15,82 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 namespace otbl {
 
+// complex type of a real type: V2<double> = double2, V2<float> = float2
+template <typename T>
+struct Vec2;
+template <>
+struct Vec2<double> {
+  using type = double2;
+};
+template <>
+struct Vec2<float> {
+  using type = float2;
+};
+template <typename T>
+using V2 = typename Vec2<T>::type;
+
+// complex arithmetic on double2 (FP64 path) and float2 (mixed path)
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
 // multiply by i*s (s = +1 or -1)
-__device__ __forceinline__ double2 cmul_i(double2 a, int s) {
-  return s > 0 ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
+template <typename V>
+__device__ __forceinline__ V cmul_i(V a, int s) {
+  V r;
+  r.x = s > 0 ? -a.y : a.y;
+  r.y = s > 0 ? a.x : -a.x;
+  return r;
+}
+// a*(x, y) for a real scalar
+template <typename V, typename S>
+__device__ __forceinline__ V cscale(S a, V v) {
+  V r;
+  r.x = a * v.x;
+  r.y = a * v.y;
+  return r;
+}
+template <typename V>
+__device__ __forceinline__ V cmake(decltype(V{}.x) x, decltype(V{}.x) y) {
+  V r;
+  r.x = x;
+  r.y = y;
+  return r;
 }
 
-// In-register DFT of size R; SIGN = -1 forward (e^{-}), +1 backward (e^{+}).
-template <int R, int SIGN>
-__device__ __forceinline__ void dft_small(double2 *v);
-
-template <>
-__device__ __forceinline__ void dft_small<2, -1>(double2 *v) {
-  const double2 a = v[0], b = v[1];
-  v[0] = cadd(a, b);
-  v[1] = csub(a, b);
-}
-template <>
-__device__ __forceinline__ void dft_small<2, 1>(double2 *v) {
-  dft_small<2, -1>(v);
-}
-
-template <int SIGN>
-__device__ __forceinline__ void dft4(double2 &t0, double2 &t1, double2 &t2, double2 &t3) {
-  const double2 a0 = cadd(t0, t2), a1 = csub(t0, t2);
-  const double2 b0 = cadd(t1, t3), b1 = cmul_i(csub(t1, t3), SIGN);
+template <int SIGN, typename V>
+__device__ __forceinline__ void dft4(V &t0, V &t1, V &t2, V &t3) {
+  const V a0 = cadd(t0, t2), a1 = csub(t0, t2);
+  const V b0 = cadd(t1, t3), b1 = cmul_i(csub(t1, t3), SIGN);
   t0 = cadd(a0, b0);
   t1 = cadd(a1, b1);
   t2 = csub(a0, b0);
   t3 = csub(a1, b1);
 }
-template <>
-__device__ __forceinline__ void dft_small<4, -1>(double2 *v) {
-  dft4<-1>(v[0], v[1], v[2], v[3]);
-}
-template <>
-__device__ __forceinline__ void dft_small<4, 1>(double2 *v) {
-  dft4<1>(v[0], v[1], v[2], v[3]);
-}
 
-template <int SIGN>
-__device__ __forceinline__ void dft8(double2 *v) {
-  const double c = 0.70710678118654752440;  // cos(pi/4)
-  double2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
-  double2 o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+template <int SIGN, typename V>
+__device__ __forceinline__ void dft8(V *v) {
+  using S = decltype(V{}.x);
+  const S c = S(0.70710678118654752440);  // cos(pi/4)
+  V e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+  V o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
   dft4<SIGN>(e0, e1, e2, e3);
   dft4<SIGN>(o0, o1, o2, o3);
   // W8^q = exp(SIGN*2*pi*i*q/8)
-  const double2 w1 = make_double2(c, SIGN * c);
-  const double2 w3 = make_double2(-c, SIGN * c);
+  const V w1 = cmake<V>(c, SIGN * c);
+  const V w3 = cmake<V>(-c, SIGN * c);
   o1 = cmul(o1, w1);
   o2 = cmul_i(o2, SIGN);
   o3 = cmul(o3, w3);
@@ -82,60 +103,57 @@ __device__ __forceinline__ void dft8(double2 *v) {
   v[3] = cadd(e3, o3);
   v[7] = csub(e3, o3);
 }
-template <>
-__device__ __forceinline__ void dft_small<8, -1>(double2 *v) {
-  dft8<-1>(v);
-}
-template <>
-__device__ __forceinline__ void dft_small<8, 1>(double2 *v) {
-  dft8<1>(v);
-}
 
-template <int SIGN>
-__device__ __forceinline__ void dft3(double2 *v) {
-  const double s3 = 0.86602540378443864676;  // sin(2 pi/3)
-  const double2 a = v[0], b = v[1], cc = v[2];
-  const double2 t1 = cadd(b, cc);
-  const double2 t2 = make_double2(a.x - 0.5 * t1.x, a.y - 0.5 * t1.y);
-  const double2 t3 = cmul_i(csub(b, cc), SIGN);  // i*SIGN*(b-c)
+template <int SIGN, typename V>
+__device__ __forceinline__ void dft3(V *v) {
+  using S = decltype(V{}.x);
+  const S s3 = S(0.86602540378443864676);  // sin(2 pi/3)
+  const V a = v[0], b = v[1], cc = v[2];
+  const V t1 = cadd(b, cc);
+  const V t2 = cmake<V>(a.x - S(0.5) * t1.x, a.y - S(0.5) * t1.y);
+  const V t3 = cmul_i(csub(b, cc), SIGN);  // i*SIGN*(b-c)
   v[0] = cadd(a, t1);
-  v[1] = make_double2(t2.x + s3 * t3.x, t2.y + s3 * t3.y);
-  v[2] = make_double2(t2.x - s3 * t3.x, t2.y - s3 * t3.y);
-}
-template <>
-__device__ __forceinline__ void dft_small<3, -1>(double2 *v) {
-  dft3<-1>(v);
-}
-template <>
-__device__ __forceinline__ void dft_small<3, 1>(double2 *v) {
-  dft3<1>(v);
+  v[1] = cmake<V>(t2.x + s3 * t3.x, t2.y + s3 * t3.y);
+  v[2] = cmake<V>(t2.x - s3 * t3.x, t2.y - s3 * t3.y);
 }
 
-template <int SIGN>
-__device__ __forceinline__ void dft5(double2 *v) {
+template <int SIGN, typename V>
+__device__ __forceinline__ void dft5(V *v) {
+  using S = decltype(V{}.x);
   // cos/sin of 2 pi/5 and 4 pi/5
-  const double c1 = 0.30901699437494742410, c2 = -0.80901699437494742410;
-  const double s1 = 0.95105651629515357212, s2 = 0.58778525229247312917;
-  const double2 a = v[0];
-  const double2 b1 = cadd(v[1], v[4]), b2 = cadd(v[2], v[3]);
-  const double2 d1 = csub(v[1], v[4]), d2 = csub(v[2], v[3]);
-  const double2 r1 = make_double2(a.x + c1 * b1.x + c2 * b2.x, a.y + c1 * b1.y + c2 * b2.y);
-  const double2 r2 = make_double2(a.x + c2 * b1.x + c1 * b2.x, a.y + c2 * b1.y + c1 * b2.y);
-  const double2 i1 = cmul_i(make_double2(s1 * d1.x + s2 * d2.x, s1 * d1.y + s2 * d2.y), SIGN);
-  const double2 i2 = cmul_i(make_double2(s2 * d1.x - s1 * d2.x, s2 * d1.y - s1 * d2.y), SIGN);
+  const S c1 = S(0.30901699437494742410), c2 = S(-0.80901699437494742410);
+  const S s1 = S(0.95105651629515357212), s2 = S(0.58778525229247312917);
+  const V a = v[0];
+  const V b1 = cadd(v[1], v[4]), b2 = cadd(v[2], v[3]);
+  const V d1 = csub(v[1], v[4]), d2 = csub(v[2], v[3]);
+  const V r1 = cmake<V>(a.x + c1 * b1.x + c2 * b2.x, a.y + c1 * b1.y + c2 * b2.y);
+  const V r2 = cmake<V>(a.x + c2 * b1.x + c1 * b2.x, a.y + c2 * b1.y + c1 * b2.y);
+  const V i1 = cmul_i(cmake<V>(s1 * d1.x + s2 * d2.x, s1 * d1.y + s2 * d2.y), SIGN);
+  const V i2 = cmul_i(cmake<V>(s2 * d1.x - s1 * d2.x, s2 * d1.y - s1 * d2.y), SIGN);
   v[0] = cadd(a, cadd(b1, b2));
   v[1] = cadd(r1, i1);
   v[4] = csub(r1, i1);
   v[2] = cadd(r2, i2);
   v[3] = csub(r2, i2);
 }
-template <>
-__device__ __forceinline__ void dft_small<5, -1>(double2 *v) {
-  dft5<-1>(v);
-}
-template <>
-__device__ __forceinline__ void dft_small<5, 1>(double2 *v) {
-  dft5<1>(v);
+
+// In-register DFT of size R; SIGN = -1 forward (e^{-}), +1 backward (e^{+}).
+template <int R, int SIGN, typename V>
+__device__ __forceinline__ void dft_small(V *v) {
+  if constexpr (R == 2) {
+    const V a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  } else if constexpr (R == 3) {
+    dft3<SIGN>(v);
+  } else if constexpr (R == 4) {
+    dft4<SIGN>(v[0], v[1], v[2], v[3]);
+  } else if constexpr (R == 5) {
+    dft5<SIGN>(v);
+  } else {
+    static_assert(R == 8, "radix 2, 3, 4, 5 or 8");
+    dft8<SIGN>(v);
+  }
 }
 
 // One Stockham pass of radix R over a length-M complex line in shared memory,
@@ -144,12 +162,11 @@ __device__ __forceinline__ void dft_small<5, 1>(double2 *v) {
 //   v[r] = buf[j + r*M/R] * W_{Ns*R}^{r*k};  v = DFT_R(v);
 //   buf[(j/Ns)*Ns*R + k + r*Ns] = v[r]
 // MAXIT bounds the items per thread. SYNC is __syncwarp or __syncthreads.
-template <int R, int SIGN, int MAXIT, bool BLOCK>
-__device__ __forceinline__ void stockham_pass(double2 *buf, int M, int Ns, const double2 *__restrict__ tw,
-                                              int t, int G) {
+template <int R, int SIGN, int MAXIT, bool BLOCK, typename V>
+__device__ __forceinline__ void stockham_pass(V *buf, int M, int Ns, const V *__restrict__ tw, int t, int G) {
   const int nit = M / R;
   const int stride_tw = M / (Ns * R);
-  double2 v[MAXIT][R];
+  V v[MAXIT][R];
 #pragma unroll
   for (int it = 0; it < MAXIT; ++it) {
     const int j = t + it * G;
@@ -170,7 +187,7 @@ __device__ __forceinline__ void stockham_pass(double2 *buf, int M, int Ns, const
       if (Ns > 1) {
 #pragma unroll
         for (int r = 1; r < R; ++r) {
-          double2 w = __ldg(&tw[r * k * stride_tw]);
+          V w = __ldg(&tw[r * k * stride_tw]);
           if (SIGN > 0) w.y = -w.y;
           v[it][r] = cmul(v[it][r], w);
         }
@@ -188,8 +205,8 @@ __device__ __forceinline__ void stockham_pass(double2 *buf, int M, int Ns, const
 }
 
 // Warp FFT of a power-of-two length M <= 512 in shared memory (in place).
-template <int SIGN>
-__device__ __forceinline__ void warp_fft(double2 *buf, int M, const double2 *__restrict__ tw, int lane) {
+template <int SIGN, typename V>
+__device__ __forceinline__ void warp_fft(V *buf, int M, const V *__restrict__ tw, int lane) {
   int Ns = 1;
   while (Ns * 8 <= M) {
     stockham_pass<8, SIGN, 2, false>(buf, M, Ns, tw, lane, 32);
@@ -208,16 +225,16 @@ __device__ __forceinline__ void warp_fft(double2 *buf, int M, const double2 *__r
 // CTA FFT of length n = 2^a 3^b 5^c (n <= 4096) in shared memory; NB lines
 // stored back to back (line l at buf + l*n) are transformed in turn by the
 // 256 threads of the CTA. The twiddle table has n entries.
-template <int R, int SIGN, int NB>
-__device__ __forceinline__ void block_pass(double2 *buf, int n, int Ns, const double2 *__restrict__ tw) {
+template <int R, int SIGN, int NB, typename V>
+__device__ __forceinline__ void block_pass(V *buf, int n, int Ns, const V *__restrict__ tw) {
   constexpr int MAXIT = (4096 / R + 255) / 256;
 #pragma unroll 1
   for (int l = 0; l < NB; ++l)
     stockham_pass<R, SIGN, MAXIT, true>(buf + l * n, n, Ns, tw, threadIdx.x, 256);
 }
 
-template <int SIGN, int NB>
-__device__ __forceinline__ void block_fft(double2 *buf, int n, const double2 *__restrict__ tw) {
+template <int SIGN, int NB, typename V>
+__device__ __forceinline__ void block_fft(V *buf, int n, const V *__restrict__ tw) {
   int Ns = 1, rem = n;
   while (rem % 8 == 0) { block_pass<8, SIGN, NB>(buf, n, Ns, tw); Ns *= 8; rem /= 8; }
   while (rem % 4 == 0) { block_pass<4, SIGN, NB>(buf, n, Ns, tw); Ns *= 4; rem /= 4; }

@@ -18,14 +18,17 @@ namespace otbl {
 constexpr int KY = 8;  // rows per checkpointed segment
 
 // interpyy, which 0: u, w (in rows ny+1), which 1: v (in rows ny); out rows
-// 1..ny. blockIdx.y = field (u, w, v).
+// 1..ny. blockIdx.y = field (u, w, v). T: arithmetic and output type (float
+// on the mixed path, with the FP32 coefficient copy); the state is FP64.
 struct InterpyArgs {
   const double *in[3];
-  double *out[3], *ck[3];
+  void *out[3];
+  double *ck[3];
   int which[3];
 };
 
-__global__ void __launch_bounds__(128) k_interpy(DCoef c, InterpyArgs a) {
+template <typename T>
+__global__ void __launch_bounds__(128) k_interpy(DCoefT<T> c, InterpyArgs a) {
   const int f = blockIdx.y;
   const int ny = c.ny, nz1 = c.nz1, ncol = c.nx * nz1;
   const int col = blockIdx.x * blockDim.x + threadIdx.x;
@@ -34,13 +37,13 @@ __global__ void __launch_bounds__(128) k_interpy(DCoef c, InterpyArgs a) {
   const int i = col / nz1 + 1, kr = col - (i - 1) * nz1;
   const size_t S = nz1;
   const double *g = a.in[f] + (size_t)(i - 1) * jin * nz1 + kr;
-  double *o = a.out[f] + (size_t)(i - 1) * ny * nz1 + kr;
-  double *ck = a.ck[f] + col;
-  const double *iny = which == 0 ? c.inyu : c.inyv;
-  const double *econ = which == 0 ? c.cofiuy : c.cofivy;
-  const double *ib = c.inby;
-  auto G = [&](int r) { return __ldg(g + (size_t)min(max(r, 0), jin - 1) * S); };
-  double b0 = 0.0, bN;
+  T *o = static_cast<T *>(a.out[f]) + (size_t)(i - 1) * ny * nz1 + kr;
+  T *ck = reinterpret_cast<T *>(a.ck[f]) + col;
+  const T *iny = which == 0 ? c.inyu : c.inyv;
+  const T *econ = which == 0 ? c.cofiuy : c.cofivy;
+  const T *ib = c.inby;
+  auto G = [&](int r) { return (T)__ldg(g + (size_t)min(max(r, 0), jin - 1) * S); };
+  T b0 = T(0), bN;
   if (which == 0) {
     bN = M4(ib, 1, 1) * G(ny) + M4(ib, 1, 2) * G(ny - 1) + M4(ib, 1, 3) * G(ny - 2) + M4(ib, 1, 4) * G(ny - 3);
   } else {
@@ -49,36 +52,36 @@ __global__ void __launch_bounds__(128) k_interpy(DCoef c, InterpyArgs a) {
   }
   // right-hand side of output row r from input rows r-1, r, r+1:
   // u,w: e1 g(r) + e2 g(r+1), wall row 0; v: e2 g(r) + e1 g(r-1)
-  auto rhs = [&](int r, double gm, double g0, double gp) {
-    const double e1 = __ldg(econ + 2 * r), e2 = __ldg(econ + 2 * r + 1);
-    const double in = which == 0 ? e1 * g0 + e2 * gp : e2 * g0 + e1 * gm;
+  auto rhs = [&](int r, T gm, T g0, T gp) {
+    const T e1 = __ldg(econ + 2 * r), e2 = __ldg(econ + 2 * r + 1);
+    const T in = which == 0 ? e1 * g0 + e2 * gp : e2 * g0 + e1 * gm;
     return r == 0 ? b0 : (r == ny - 1 ? bN : in);
   };
   const int nseg = (ny + KY - 1) / KY;
-  double y = 0.0;
+  T y = T(0);
   for (int sg = 0; sg < nseg; ++sg) {
     const int s0 = sg * KY;
     ck[(size_t)sg * ncol] = y;
-    double gv[KY + 2];
+    T gv[KY + 2];
 #pragma unroll
     for (int b = 0; b < KY + 2; ++b) gv[b] = G(s0 + b - 1);
 #pragma unroll
     for (int b = 0; b < KY; ++b) {
       const int r = s0 + b;
-      if (r < ny) y = rhs(r, gv[b], gv[b + 1], gv[b + 2]) + (r > 0 ? __ldg(iny + 3 * r) : 0.0) * y;
+      if (r < ny) y = rhs(r, gv[b], gv[b + 1], gv[b + 2]) + (r > 0 ? __ldg(iny + 3 * r) : T(0)) * y;
     }
   }
-  double x = 0.0;
+  T x = T(0);
   for (int sg = nseg - 1; sg >= 0; --sg) {
     const int s0 = sg * KY;
-    double gv[KY + 2], yv[KY];
+    T gv[KY + 2], yv[KY];
 #pragma unroll
     for (int b = 0; b < KY + 2; ++b) gv[b] = G(s0 + b - 1);
-    double yy = ck[(size_t)sg * ncol];
+    T yy = ck[(size_t)sg * ncol];
 #pragma unroll
     for (int b = 0; b < KY; ++b) {
       const int r = s0 + b;
-      if (r < ny) yy = rhs(r, gv[b], gv[b + 1], gv[b + 2]) + (r > 0 ? __ldg(iny + 3 * r) : 0.0) * yy;
+      if (r < ny) yy = rhs(r, gv[b], gv[b + 1], gv[b + 2]) + (r > 0 ? __ldg(iny + 3 * r) : T(0)) * yy;
       yv[b] = yy;
     }
 #pragma unroll
@@ -97,12 +100,15 @@ __global__ void __launch_bounds__(128) k_interpy(DCoef c, InterpyArgs a) {
 // per launch pair: RHS assembly, pressure gradient, boun, vistyy, RK3
 // combination, rhs history, implzy.
 // ---------------------------------------------------------------------------
+// W: element type of the difvisxx outputs and the products (float on the
+// mixed path); the arithmetic is FP64 throughout.
+template <typename W>
 struct FinalArgs {
   double *u, *v, *w;                 // state: old on entry, new on exit
   const double *p;
   double *rhsupa, *rhsvpa, *rhswpa;  // old on entry, new on exit
-  const double *cu, *cv, *cw;        // difvisxx outputs
-  const double *uv, *uw, *vw, *vv, *ww;
+  const W *cu, *cv, *cw;             // difvisxx outputs
+  const W *uv, *uw, *vw, *vv, *ww;
   const double *fac_u, *fac_v;
   const DState *st;
 };
@@ -123,17 +129,18 @@ struct FinalArgs {
 //   k_final_s2: implzy (the same two passes) and the new velocity.
 // The sweeps are the serial Thomas of lip.f90 in the reference's order.
 // ---------------------------------------------------------------------------
+template <typename W>
 struct FinalStream {
-  FinalArgs a;
+  FinalArgs<W> a;
   double *ck;   // checkpoints: [2*seg + op][column]
   double *bq;   // implzy right-hand side: [q][column], q < jee-2
   double *ub;   // ub1, ubt: [2][column]
   double *ck2;  // implzy checkpoints: [seg][column]
 };
 
-template <int COMP>
-__global__ void __launch_bounds__(128, 4) k_final_s1(DCoef c, FinalStream fs) {
-  const FinalArgs &a = fs.a;
+template <int COMP, typename W>
+__global__ void __launch_bounds__(128, 4) k_final_s1(DCoef c, FinalStream<W> fs) {
+  const FinalArgs<W> &a = fs.a;
   const int nx = c.nx, ny = c.ny, nz1 = c.nz1;
   const int ncol = (nx - 1) * nz1;
   const int col = blockIdx.x * blockDim.x + threadIdx.x;
@@ -146,10 +153,10 @@ __global__ void __launch_bounds__(128, 4) k_final_s1(DCoef c, FinalStream fs) {
   const size_t PU = (size_t)(ny + 1) * nz1, PV = (size_t)ny * nz1;
   const size_t pl = (size_t)(i - 1) * (COMP == 1 ? PV : PU), plv = (size_t)(i - 1) * PV;
   const size_t S = nz1;  // row stride
-  const double *prod = (COMP == 0 ? a.uv : (COMP == 1 ? a.vv : a.vw)) + plv + kr;
-  const double *kp = (COMP == 0 ? a.uw : (COMP == 1 ? a.vw : a.ww)) + (COMP == 0 ? pl : plv) + kr + pof;
+  const W *prod = (COMP == 0 ? a.uv : (COMP == 1 ? a.vv : a.vw)) + plv + kr;
+  const W *kp = (COMP == 0 ? a.uw : (COMP == 1 ? a.vw : a.ww)) + (COMP == 0 ? pl : plv) + kr + pof;
   const double *vel = (COMP == 0 ? a.u : (COMP == 1 ? a.v : a.w)) + pl + kr;
-  const double *cX = (COMP == 0 ? a.cu : (COMP == 1 ? a.cv : a.cw)) + pl + kr;
+  const W *cX = (COMP == 0 ? a.cu : (COMP == 1 ? a.cv : a.cw)) + pl + kr;
   double *hp = (COMP == 0 ? a.rhsupa : (COMP == 1 ? a.rhsvpa : a.rhswpa)) + pl + kr;
   const double *pc = a.p + plv + kr;
   const double kz = c.kaz[k], kv = c.kvis[k];
@@ -163,7 +170,7 @@ __global__ void __launch_bounds__(128, 4) k_final_s1(DCoef c, FinalStream fs) {
   const double *viy = which == 0 ? c.viyu : c.viyv, *ecv = which == 0 ? c.cofvyu : c.cofvyv;
   const double *vyi = which == 0 ? c.vyui : c.vyvi;
   const double *fac = COMP == 1 ? a.fac_v : a.fac_u;
-  auto Pg = [&](int r) { return __ldg(prod + (size_t)min(max(r, 0), ny - 1) * S); };
+  auto Pg = [&](int r) { return (double)__ldg(prod + (size_t)min(max(r, 0), ny - 1) * S); };
   auto Vg = [&](int r) { return __ldg(vel + (size_t)min(max(r, 0), jee - 1) * S); };
   // velocity after the pressure gradient (rhsp.F90:291-339) at row r
   auto star = [&](int r, double o) -> double {
@@ -262,8 +269,8 @@ __global__ void __launch_bounds__(128, 4) k_final_s1(DCoef c, FinalStream fs) {
 #pragma unroll
     for (int b = 0; b < KY; ++b) {
       const int rr = min(s0 + b, jee - 1);
-      cxv[b] = __ldg(cX + (size_t)rr * S);
-      kpv[b] = last ? 0.0 : __ldg(kp + (size_t)min(rr, krows - 1) * S);
+      cxv[b] = (double)__ldg(cX + (size_t)rr * S);
+      kpv[b] = last ? 0.0 : (double)__ldg(kp + (size_t)min(rr, krows - 1) * S);
       hv[b] = __ldg(hp + (size_t)rr * S);
     }
 #pragma unroll
@@ -321,9 +328,9 @@ __global__ void __launch_bounds__(128, 4) k_final_s1(DCoef c, FinalStream fs) {
   }
 }
 
-template <int COMP>
-__global__ void __launch_bounds__(128) k_final_s2(DCoef c, FinalStream fs) {
-  const FinalArgs &a = fs.a;
+template <int COMP, typename W>
+__global__ void __launch_bounds__(128) k_final_s2(DCoef c, FinalStream<W> fs) {
+  const FinalArgs<W> &a = fs.a;
   const int nx = c.nx, ny = c.ny, nz1 = c.nz1;
   const int ncol = (nx - 1) * nz1;
   const int col = blockIdx.x * blockDim.x + threadIdx.x;
@@ -470,7 +477,7 @@ __global__ void __launch_bounds__(128) k_pois_solve(DCoef c, double *phi, const 
 cudaError_t launch_interpy(otbl_ctx *c) {
   InterpyArgs a;
   const double *ins[3] = {c->f[OTBL_F_U], c->f[OTBL_F_W], c->f[OTBL_F_V]};
-  double *outs[3] = {c->w.uy, c->w.wy, c->w.vy};
+  void *outs[3] = {c->w.uy, c->w.wy, c->w.vy};
   double *cks[3] = {c->w.s1, c->w.s2, c->w.s3};
   const int which[3] = {0, 0, 1};
   for (int f = 0; f < 3; ++f) {
@@ -481,15 +488,19 @@ cudaError_t launch_interpy(otbl_ctx *c) {
   }
   const int ncol = c->cfg.nx * c->dc.nz1;
   prof_begin(c, PK_INTERPY);
-  k_interpy<<<dim3((ncol + 127) / 128, 3), 128, 0, c->stream>>>(c->dc, a);
+  if (c->mixed)
+    k_interpy<float><<<dim3((ncol + 127) / 128, 3), 128, 0, c->stream>>>(c->dcf, a);
+  else
+    k_interpy<double><<<dim3((ncol + 127) / 128, 3), 128, 0, c->stream>>>(c->dc, a);
   prof_end(c);
   c->launches += 1;
   return cudaGetLastError();
 }
 
-cudaError_t launch_final(otbl_ctx *c) {
-  FinalStream fs;
-  FinalArgs &a = fs.a;
+template <typename W>
+static void final_t(otbl_ctx *c) {
+  FinalStream<W> fs;
+  FinalArgs<W> &a = fs.a;
   a.u = c->f[OTBL_F_U];
   a.v = c->f[OTBL_F_V];
   a.w = c->f[OTBL_F_W];
@@ -497,14 +508,14 @@ cudaError_t launch_final(otbl_ctx *c) {
   a.rhsupa = c->f[OTBL_F_RHSUPA];
   a.rhsvpa = c->f[OTBL_F_RHSVPA];
   a.rhswpa = c->f[OTBL_F_RHSWPA];
-  a.cu = c->w.cu;
-  a.cv = c->w.cv;
-  a.cw = c->w.cw;
-  a.uv = c->w.uv;
-  a.uw = c->w.uw;
-  a.vw = c->w.vw;
-  a.vv = c->w.vv;
-  a.ww = c->w.ww;
+  a.cu = static_cast<const W *>(c->w.cu);
+  a.cv = static_cast<const W *>(c->w.cv);
+  a.cw = static_cast<const W *>(c->w.cw);
+  a.uv = static_cast<const W *>(c->w.uv);
+  a.uw = static_cast<const W *>(c->w.uw);
+  a.vw = static_cast<const W *>(c->w.vw);
+  a.vv = static_cast<const W *>(c->w.vv);
+  a.ww = static_cast<const W *>(c->w.ww);
   a.fac_u = c->w.fac_u;
   a.fac_v = c->w.fac_v;
   a.st = c->st;
@@ -514,13 +525,20 @@ cudaError_t launch_final(otbl_ctx *c) {
   fs.ub = c->w.s3;
   fs.ck2 = c->w.s3 + 2 * (size_t)ncol;
   const dim3 g((ncol + 127) / 128);
+  k_final_s1<1, W><<<g, 128, 0, c->stream>>>(c->dc, fs);
+  k_final_s2<1, W><<<g, 128, 0, c->stream>>>(c->dc, fs);
+  k_final_s1<0, W><<<g, 128, 0, c->stream>>>(c->dc, fs);
+  k_final_s2<0, W><<<g, 128, 0, c->stream>>>(c->dc, fs);
+  k_final_s1<2, W><<<g, 128, 0, c->stream>>>(c->dc, fs);
+  k_final_s2<2, W><<<g, 128, 0, c->stream>>>(c->dc, fs);
+}
+
+cudaError_t launch_final(otbl_ctx *c) {
   prof_begin(c, PK_FINAL);
-  k_final_s1<1><<<g, 128, 0, c->stream>>>(c->dc, fs);
-  k_final_s2<1><<<g, 128, 0, c->stream>>>(c->dc, fs);
-  k_final_s1<0><<<g, 128, 0, c->stream>>>(c->dc, fs);
-  k_final_s2<0><<<g, 128, 0, c->stream>>>(c->dc, fs);
-  k_final_s1<2><<<g, 128, 0, c->stream>>>(c->dc, fs);
-  k_final_s2<2><<<g, 128, 0, c->stream>>>(c->dc, fs);
+  if (c->mixed)
+    final_t<float>(c);
+  else
+    final_t<double>(c);
   prof_end(c);
   c->launches += 6;
   return cudaGetLastError();

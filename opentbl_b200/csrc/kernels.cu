@@ -39,73 +39,97 @@ __device__ __forceinline__ double warp_nmax(double m) {
 }
 
 // ---------------------------------------------------------------------------
-// z-line transforms (fourxz, ffts.f90:27-67), one warp per line.
+// z-line transforms (fourxz, ffts.f90:27-67), one warp per line, in the
+// arithmetic type T (double, or float on the mixed path). Fields of element
+// type TI/TO are read and written with conversion to and from T.
 // ---------------------------------------------------------------------------
-struct ZTab {
-  const double2 *tw;   // exp(-2 pi i t/M), t < M
-  const double2 *tw2;  // exp(-2 pi i t/nz), t < M
+template <typename T>
+struct ZTabT {
+  const V2<T> *tw;   // exp(-2 pi i t/M), t < M
+  const V2<T> *tw2;  // exp(-2 pi i t/nz), t < M
   int M, nz, nz2;
 };
+using ZTab = ZTabT<double>;
+
+// complex element k of a field of element type TI, as V2<T>
+template <typename T, typename TI>
+__device__ __forceinline__ V2<T> ldcx(const TI *__restrict__ f, int k) {
+  const V2<TI> a = __ldg(reinterpret_cast<const V2<TI> *>(f) + k);
+  return cmake<V2<T>>((T)a.x, (T)a.y);
+}
+template <typename TO, typename V>
+__device__ __forceinline__ void stcx(TO *__restrict__ f, int k, V v) {
+  reinterpret_cast<V2<TO> *>(f)[k] = cmake<V2<TO>>((TO)v.x, (TO)v.y);
+}
 
 // c2r of fou (nz2+1 complex modes, global) into buf (M complex = nz reals)
-__device__ __forceinline__ void line_c2r(const ZTab &z, const double *__restrict__ fou, double2 *buf, int lane) {
+template <typename T, typename TI>
+__device__ __forceinline__ void line_c2r(const ZTabT<T> &z, const TI *__restrict__ fou, V2<T> *buf, int lane) {
+  using V = V2<T>;
   const int M = z.M, nz2 = z.nz2;
-  const double2 *f2 = reinterpret_cast<const double2 *>(fou);
   for (int k = lane; k < M; k += 32) {
-    double2 a = k <= nz2 ? __ldg(f2 + k) : make_double2(0.0, 0.0);
-    if (k == 0) a.y = 0.0;  // c2r ignores Im X[0]
+    V a = k <= nz2 ? ldcx<T>(fou, k) : cmake<V>(T(0), T(0));
+    if (k == 0) a.y = T(0);  // c2r ignores Im X[0]
     const int km = M - k;
-    double2 b = km <= nz2 ? __ldg(f2 + km) : make_double2(0.0, 0.0);
+    V b = km <= nz2 ? ldcx<T>(fou, km) : cmake<V>(T(0), T(0));
     b.y = -b.y;
-    const double2 s = cadd(a, b), d = csub(a, b);
-    const double2 t = cmul(cconj(__ldg(z.tw2 + k)), d);  // W^{-k} d
-    buf[k] = make_double2(s.x - t.y, s.y + t.x);          // s + i t
+    const V s = cadd(a, b), d = csub(a, b);
+    const V t = cmul(cconj(__ldg(z.tw2 + k)), d);  // W^{-k} d
+    buf[k] = cmake<V>(s.x - t.y, s.y + t.x);      // s + i t
   }
   __syncwarp();
   warp_fft<1>(buf, M, z.tw, lane);
 }
 
 // r2c of buf (nz reals packed as M complex) into fou (modes 0..nz2) x 1/nz
-__device__ __forceinline__ void line_r2c(const ZTab &z, double2 *buf, double *__restrict__ fou, int lane) {
+template <typename T, typename TO>
+__device__ __forceinline__ void line_r2c(const ZTabT<T> &z, V2<T> *buf, TO *__restrict__ fou, int lane) {
+  using V = V2<T>;
   const int M = z.M, nz2 = z.nz2;
   warp_fft<-1>(buf, M, z.tw, lane);
-  const double dnf = 1.0 / (double)z.nz;
-  double2 *f2 = reinterpret_cast<double2 *>(fou);
+  const T dnf = T(1) / (T)z.nz;
   for (int k = lane; k <= nz2; k += 32) {
-    const double2 zk = buf[k];
-    const double2 zc = cconj(buf[(M - k) & (M - 1)]);
-    const double2 e = make_double2(0.5 * (zk.x + zc.x), 0.5 * (zk.y + zc.y));
-    const double2 d = csub(zk, zc);
-    const double2 o = make_double2(0.5 * d.y, -0.5 * d.x);  // -i d / 2
-    const double2 xk = cadd(e, cmul(__ldg(z.tw2 + k), o));
-    f2[k] = make_double2(dnf * xk.x, dnf * xk.y);
+    const V zk = buf[k];
+    const V zc = cconj(buf[(M - k) & (M - 1)]);
+    const V e = cmake<V>(T(0.5) * (zk.x + zc.x), T(0.5) * (zk.y + zc.y));
+    const V d = csub(zk, zc);
+    const V o = cmake<V>(T(0.5) * d.y, T(-0.5) * d.x);  // -i d / 2
+    const V xk = cadd(e, cmul(__ldg(z.tw2 + k), o));
+    stcx(fou, k, cmake<V>(dnf * xk.x, dnf * xk.y));
   }
   __syncwarp();
 }
 
-__device__ __forceinline__ void buf_mul(double2 *a, const double2 *b, int M, int lane) {
+template <typename V>
+__device__ __forceinline__ void buf_mul(V *a, const V *b, int M, int lane) {
   for (int t = lane; t < M; t += 32) {
-    const double2 x = a[t], y = b[t];
-    a[t] = make_double2(x.x * y.x, x.y * y.y);
+    const V x = a[t], y = b[t];
+    a[t] = cmake<V>(x.x * y.x, x.y * y.y);
   }
   __syncwarp();
 }
-__device__ __forceinline__ void buf_sq(double2 *a, int M, int lane) {
+template <typename V>
+__device__ __forceinline__ void buf_sq(V *a, int M, int lane) {
   for (int t = lane; t < M; t += 32) {
-    const double2 x = a[t];
-    a[t] = make_double2(x.x * x.x, x.y * x.y);
+    const V x = a[t];
+    a[t] = cmake<V>(x.x * x.x, x.y * x.y);
   }
   __syncwarp();
 }
-__device__ __forceinline__ double buf_absmax(const double2 *a, int M, int lane) {
+template <typename V>
+__device__ __forceinline__ double buf_absmax(const V *a, int M, int lane) {
   double m = 0.0;
-  for (int t = lane; t < M; t += 32) m = nmax(nmax(m, fabs(a[t].x)), fabs(a[t].y));
+  for (int t = lane; t < M; t += 32) m = nmax(nmax(m, fabs((double)a[t].x)), fabs((double)a[t].y));
   return m;
 }
 
+// products inputs: the FP64 state u, v, w and the interpolants, outputs the
+// six products (W: element type of the intermediate fields)
+template <typename W>
 struct ProdArgs {
-  const double *u, *v, *w, *ux, *vx, *wx, *uy, *wy, *vy;
-  double *uu, *uw, *uv, *vw, *vv, *ww;
+  const double *u, *v, *w;
+  const W *ux, *vx, *wx, *uy, *wy, *vy;
+  W *uu, *uw, *uv, *vw, *vv, *ww;
   unsigned long long *vm_bits;
   DState *st;
   int setstep;
@@ -113,14 +137,17 @@ struct ProdArgs {
 
 // rhsp.F90:120-171 (uu, uw, uv and the CFL maxima, all planes) and
 // rhsp.F90:367-415 (vw, vv, ww, planes 2..nx-1); one warp per (i, j) line.
-__global__ void __launch_bounds__(128) k_products(DCoef c, ZTab z, ProdArgs a) {
-  extern __shared__ double2 sm[];
+template <typename T>
+__global__ void __launch_bounds__(128) k_products(DCoef c, ZTabT<T> z, ProdArgs<T> a) {
+  using V = V2<T>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  V *sm = reinterpret_cast<V *>(smraw);
   const int M = z.M, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int j = blockIdx.x * 4 + wid + 1;
   const int i = blockIdx.y + 1;
   const int nx = c.nx, ny = c.ny, nz1 = c.nz1;
   if (j > ny + 1) return;
-  double2 *A = sm + (size_t)wid * 3 * M, *B = A + M, *P = B + M;
+  V *A = sm + (size_t)wid * 3 * M, *B = A + M, *P = B + M;
   const size_t offu = ((size_t)(i - 1) * (ny + 1) + (j - 1)) * nz1;
   const size_t offv = ((size_t)(i - 1) * ny + (j - 1)) * nz1;
   double mu = 0.0, mw = 0.0, mv = 0.0;
@@ -183,15 +210,14 @@ struct ZPlan {
 __device__ __forceinline__ int zpad(int i) { return i + (i >> 3); }
 
 // inverse (SIGN = +1) or forward (SIGN = -1) FFT of a line in layout L
-template <int M, int SIGN>
-__device__ __forceinline__ void zfft_regs(double2 (&L)[M / 32], double2 *buf, const double2 *__restrict__ tw,
-                                          int t) {
+template <int M, int SIGN, typename V>
+__device__ __forceinline__ void zfft_regs(V (&L)[M / 32], V *buf, const V *__restrict__ tw, int t) {
   constexpr int E = M / 32, R3 = ZPlan<M>::R3;
   constexpr int IA = E / 8;  // radix-8 items per lane in the first two passes
   // pass A: radix 8, Ns = 1, input from registers
 #pragma unroll
   for (int it = 0; it < IA; ++it) {
-    double2 v[8];
+    V v[8];
 #pragma unroll
     for (int r = 0; r < 8; ++r) v[r] = L[it + r * IA];
     dft_small<8, SIGN>(v);
@@ -202,7 +228,7 @@ __device__ __forceinline__ void zfft_regs(double2 (&L)[M / 32], double2 *buf, co
   __syncwarp();
   // pass B: radix 8, Ns = 8
   {
-    double2 v[IA][8];
+    V v[IA][8];
 #pragma unroll
     for (int it = 0; it < IA; ++it) {
       const int j = t + 32 * it;
@@ -215,7 +241,7 @@ __device__ __forceinline__ void zfft_regs(double2 (&L)[M / 32], double2 *buf, co
       const int j = t + 32 * it, k = j % 8;
 #pragma unroll
       for (int r = 1; r < 8; ++r) {
-        double2 w = __ldg(&tw[r * k * (M / 64)]);
+        V w = __ldg(&tw[r * k * (M / 64)]);
         if (SIGN > 0) w.y = -w.y;
         v[it][r] = cmul(v[it][r], w);
       }
@@ -229,7 +255,7 @@ __device__ __forceinline__ void zfft_regs(double2 (&L)[M / 32], double2 *buf, co
   // pass C: radix R3, Ns = 64 (= M/R3), output to registers
   {
     constexpr int IC = (M / R3) / 32;
-    double2 v[IC][R3];
+    V v[IC][R3];
 #pragma unroll
     for (int it = 0; it < IC; ++it) {
       const int j = t + 32 * it;
@@ -242,7 +268,7 @@ __device__ __forceinline__ void zfft_regs(double2 (&L)[M / 32], double2 *buf, co
       const int j = t + 32 * it;  // k = j mod 64 = j, twiddle stride M/(64 R3) = 1
 #pragma unroll
       for (int r = 1; r < R3; ++r) {
-        double2 w = __ldg(&tw[r * j]);
+        V w = __ldg(&tw[r * j]);
         if (SIGN > 0) w.y = -w.y;
         v[it][r] = cmul(v[it][r], w);
       }
@@ -255,38 +281,39 @@ __device__ __forceinline__ void zfft_regs(double2 (&L)[M / 32], double2 *buf, co
 
 // c2r of fou (modes 0..nz2, global) into layout L (physical values packed
 // as complex), the line_c2r pre-step followed by the inverse FFT
-template <int M>
-__device__ __forceinline__ void zc2r_regs(const ZTab &z, const double *__restrict__ fou, double2 (&L)[M / 32],
-                                          double2 *buf, int t) {
+template <int M, typename T, typename TI>
+__device__ __forceinline__ void zc2r_regs(const ZTabT<T> &z, const TI *__restrict__ fou, V2<T> (&L)[M / 32],
+                                          V2<T> *buf, int t) {
+  using V = V2<T>;
   constexpr int E = M / 32;
   const int nz2 = z.nz2;
-  const double2 *f2 = reinterpret_cast<const double2 *>(fou);
-  double2 a[E], b[E];
+  V a[E], b[E];
 #pragma unroll
   for (int m = 0; m < E; ++m) {
     const int k = t + 32 * m, km = M - k;
-    a[m] = __ldg(f2 + min(k, nz2));
-    b[m] = __ldg(f2 + min(km, nz2));
+    a[m] = ldcx<T>(fou, min(k, nz2));
+    b[m] = ldcx<T>(fou, min(km, nz2));
   }
 #pragma unroll
   for (int m = 0; m < E; ++m) {
     const int k = t + 32 * m, km = M - k;
-    double2 aa = k <= nz2 ? a[m] : make_double2(0.0, 0.0);
-    if (k == 0) aa.y = 0.0;  // c2r ignores Im X[0]
-    double2 bb = km <= nz2 ? b[m] : make_double2(0.0, 0.0);
+    V aa = k <= nz2 ? a[m] : cmake<V>(T(0), T(0));
+    if (k == 0) aa.y = T(0);  // c2r ignores Im X[0]
+    V bb = km <= nz2 ? b[m] : cmake<V>(T(0), T(0));
     bb.y = -bb.y;
-    const double2 s = cadd(aa, bb), d = csub(aa, bb);
-    const double2 tt = cmul(cconj(__ldg(z.tw2 + k)), d);  // W^{-k} d
-    L[m] = make_double2(s.x - tt.y, s.y + tt.x);          // s + i t
+    const V s = cadd(aa, bb), d = csub(aa, bb);
+    const V tt = cmul(cconj(__ldg(z.tw2 + k)), d);  // W^{-k} d
+    L[m] = cmake<V>(s.x - tt.y, s.y + tt.x);       // s + i t
   }
   zfft_regs<M, 1>(L, buf, z.tw, t);
 }
 
 // r2c of layout L (physical values packed as complex) into fou (modes
 // 0..nz2) x 1/nz: forward FFT, then the line_r2c post-step
-template <int M>
-__device__ __forceinline__ void zr2c_regs(const ZTab &z, double2 (&L)[M / 32], double *__restrict__ fou,
-                                          double2 *buf, int t) {
+template <int M, typename T, typename TO>
+__device__ __forceinline__ void zr2c_regs(const ZTabT<T> &z, V2<T> (&L)[M / 32], TO *__restrict__ fou, V2<T> *buf,
+                                          int t) {
+  using V = V2<T>;
   constexpr int E = M / 32;
   zfft_regs<M, -1>(L, buf, z.tw, t);
   __syncwarp();
@@ -294,56 +321,57 @@ __device__ __forceinline__ void zr2c_regs(const ZTab &z, double2 (&L)[M / 32], d
   for (int m = 0; m < E; ++m) buf[zpad(t + 32 * m)] = L[m];
   __syncwarp();
   const int nz2 = z.nz2;
-  const double dnf = 1.0 / (double)z.nz;
-  double2 *f2 = reinterpret_cast<double2 *>(fou);
+  const T dnf = T(1) / (T)z.nz;
 #pragma unroll
   for (int m = 0; m < E; ++m) {
     const int k = t + 32 * m;
     if (k <= nz2) {
-      const double2 zk = L[m];
-      const double2 zc = cconj(buf[zpad((M - k) & (M - 1))]);
-      const double2 e = make_double2(0.5 * (zk.x + zc.x), 0.5 * (zk.y + zc.y));
-      const double2 d = csub(zk, zc);
-      const double2 o = make_double2(0.5 * d.y, -0.5 * d.x);  // -i d / 2
-      const double2 xk = cadd(e, cmul(__ldg(z.tw2 + k), o));
-      f2[k] = make_double2(dnf * xk.x, dnf * xk.y);
+      const V zk = L[m];
+      const V zc = cconj(buf[zpad((M - k) & (M - 1))]);
+      const V e = cmake<V>(T(0.5) * (zk.x + zc.x), T(0.5) * (zk.y + zc.y));
+      const V d = csub(zk, zc);
+      const V o = cmake<V>(T(0.5) * d.y, T(-0.5) * d.x);  // -i d / 2
+      const V xk = cadd(e, cmul(__ldg(z.tw2 + k), o));
+      stcx(fou, k, cmake<V>(dnf * xk.x, dnf * xk.y));
     }
   }
   __syncwarp();
 }
 
-template <int E>
-__device__ __forceinline__ void regs_mul(double2 (&a)[E], const double2 (&b)[E]) {
+template <int E, typename V>
+__device__ __forceinline__ void regs_mul(V (&a)[E], const V (&b)[E]) {
 #pragma unroll
-  for (int m = 0; m < E; ++m) a[m] = make_double2(a[m].x * b[m].x, a[m].y * b[m].y);
+  for (int m = 0; m < E; ++m) a[m] = cmake<V>(a[m].x * b[m].x, a[m].y * b[m].y);
 }
-template <int E>
-__device__ __forceinline__ void regs_sq(double2 (&a)[E]) {
+template <int E, typename V>
+__device__ __forceinline__ void regs_sq(V (&a)[E]) {
 #pragma unroll
-  for (int m = 0; m < E; ++m) a[m] = make_double2(a[m].x * a[m].x, a[m].y * a[m].y);
+  for (int m = 0; m < E; ++m) a[m] = cmake<V>(a[m].x * a[m].x, a[m].y * a[m].y);
 }
-template <int E>
-__device__ __forceinline__ double regs_absmax(const double2 (&a)[E]) {
+template <int E, typename V>
+__device__ __forceinline__ double regs_absmax(const V (&a)[E]) {
   double mx = 0.0;
 #pragma unroll
-  for (int m = 0; m < E; ++m) mx = nmax(nmax(mx, fabs(a[m].x)), fabs(a[m].y));
+  for (int m = 0; m < E; ++m) mx = nmax(nmax(mx, fabs((double)a[m].x)), fabs((double)a[m].y));
   return mx;
 }
 
-template <int M>
-__global__ void __launch_bounds__(128) k_products_r(DCoef c, ZTab z, ProdArgs a) {
-  extern __shared__ double2 sm[];
+template <int M, typename T>
+__global__ void __launch_bounds__(128) k_products_r(DCoef c, ZTabT<T> z, ProdArgs<T> a) {
+  using V = V2<T>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  V *sm = reinterpret_cast<V *>(smraw);
   constexpr int E = M / 32;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int j = blockIdx.x * 4 + wid + 1;
   const int i = blockIdx.y + 1;
   const int nx = c.nx, ny = c.ny, nz1 = c.nz1;
   if (j > ny + 1) return;
-  double2 *buf = sm + (size_t)wid * (M + M / 8);
+  V *buf = sm + (size_t)wid * (M + M / 8);
   const size_t offu = ((size_t)(i - 1) * (ny + 1) + (j - 1)) * nz1;
   const size_t offv = ((size_t)(i - 1) * ny + (j - 1)) * nz1;
   double mu = 0.0, mw = 0.0, mv = 0.0;
-  double2 A[E], B[E];
+  V A[E], B[E];
   zc2r_regs<M>(z, a.ux + offu, A, buf, lane);  // uu = ux^2
   regs_sq<E>(A);
   zr2c_regs<M>(z, A, a.uu + offu, buf, lane);
@@ -1109,6 +1137,12 @@ __global__ void k_twiddles(double2 *tw, int n, double2 *tw2, int n2, int mode2) 
   }
 }
 
+// FP32 copy of an FP64 table (mixed path)
+__global__ void k_round_f32(const double *in, float *out, int n) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) out[t] = (float)in[t];
+}
+
 // ---------------------------------------------------------------------------
 // launch wrappers
 // ---------------------------------------------------------------------------
@@ -1167,6 +1201,11 @@ cudaError_t launch_twiddles(otbl_ctx *c) {
   k_twiddles<<<(n + 255) / 256, 256, 0, c->stream>>>(reinterpret_cast<double2 *>(c->w.twx), n,
                                                      reinterpret_cast<double2 *>(c->w.twx2), n, 1);
   c->launches += 2;
+  if (c->mixed) {
+    k_round_f32<<<(2 * M + 255) / 256, 256, 0, c->stream>>>(c->w.twz, c->w.twzf, 2 * M);
+    k_round_f32<<<(2 * M + 255) / 256, 256, 0, c->stream>>>(c->w.twz2, c->w.twz2f, 2 * M);
+    c->launches += 2;
+  }
   return cudaGetLastError();
 }
 
@@ -1176,40 +1215,57 @@ cudaError_t launch_reset_max(otbl_ctx *c) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_products(otbl_ctx *c, int setstep) {
-  ProdArgs a;
+template <typename T>
+static cudaError_t products_t(otbl_ctx *c, int setstep, const ZTabT<T> &z) {
+  ProdArgs<T> a;
   a.u = c->f[OTBL_F_U];
   a.v = c->f[OTBL_F_V];
   a.w = c->f[OTBL_F_W];
-  a.ux = c->w.ux;
-  a.vx = c->w.vx;
-  a.wx = c->w.wx;
-  a.uy = c->w.uy;
-  a.wy = c->w.wy;
-  a.vy = c->w.vy;
-  a.uu = c->w.uu;
-  a.uw = c->w.uw;
-  a.uv = c->w.uv;
-  a.vw = c->w.vw;
-  a.vv = c->w.vv;
-  a.ww = c->w.ww;
+  a.ux = static_cast<const T *>(c->w.ux);
+  a.vx = static_cast<const T *>(c->w.vx);
+  a.wx = static_cast<const T *>(c->w.wx);
+  a.uy = static_cast<const T *>(c->w.uy);
+  a.wy = static_cast<const T *>(c->w.wy);
+  a.vy = static_cast<const T *>(c->w.vy);
+  a.uu = static_cast<T *>(c->w.uu);
+  a.uw = static_cast<T *>(c->w.uw);
+  a.uv = static_cast<T *>(c->w.uv);
+  a.vw = static_cast<T *>(c->w.vw);
+  a.vv = static_cast<T *>(c->w.vv);
+  a.ww = static_cast<T *>(c->w.ww);
   a.vm_bits = c->w.vm_bits;
   a.st = c->st;
   a.setstep = setstep;
   const int M = c->cfg.nz / 2;
   dim3 g((c->cfg.ny + 1 + 3) / 4, c->cfg.nx);
-  prof_begin(c, PK_PRODUCTS);
   if (M == 256) {
-    const size_t smem = (size_t)4 * (M + M / 8) * sizeof(double2);
-    k_products_r<256><<<g, 128, smem, c->stream>>>(c->dc, ztab(c), a);
+    const size_t smem = (size_t)4 * (M + M / 8) * sizeof(V2<T>);
+    k_products_r<256, T><<<g, 128, smem, c->stream>>>(c->dc, z, a);
   } else {
-    const size_t smem = (size_t)4 * 3 * M * sizeof(double2);
-    cudaFuncSetAttribute(k_products, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_products<<<g, 128, smem, c->stream>>>(c->dc, ztab(c), a);
+    const size_t smem = (size_t)4 * 3 * M * sizeof(V2<T>);
+    cudaFuncSetAttribute(k_products<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_products<T><<<g, 128, smem, c->stream>>>(c->dc, z, a);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_products(otbl_ctx *c, int setstep) {
+  prof_begin(c, PK_PRODUCTS);
+  cudaError_t e;
+  if (c->mixed) {
+    ZTabT<float> z;
+    z.tw = reinterpret_cast<const float2 *>(c->w.twzf);
+    z.tw2 = reinterpret_cast<const float2 *>(c->w.twz2f);
+    z.M = c->cfg.nz / 2;
+    z.nz = c->cfg.nz;
+    z.nz2 = c->dc.nz2;
+    e = products_t<float>(c, setstep, z);
+  } else {
+    e = products_t<double>(c, setstep, ztab(c));
   }
   prof_end(c);
   c->launches += 1;
-  return cudaGetLastError();
+  return e;
 }
 
 cudaError_t launch_dt(otbl_ctx *c, int m, int setstep) {
@@ -1329,7 +1385,7 @@ cudaError_t launch_pois(otbl_ctx *c, int m) {
   const size_t smem = (size_t)2 * n * sizeof(double2);
   cudaFuncSetAttribute(k_pois_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   cudaFuncSetAttribute(k_pois_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  double *phi = c->w.ux;
+  double *phi = c->w.s2;
   dim3 gx((nz2 + 1 + 1) / 2, ny - 1);
   prof_begin(c, PK_POIS_FWD);
   k_pois_fwd<<<gx, 256, smem, c->stream>>>(c->dc, xtab(c), c->f[OTBL_F_U], c->f[OTBL_F_V], c->f[OTBL_F_W], phi);

@@ -45,6 +45,68 @@ size_t field_len(const otbl_ctx *c, int id) {
   return otbl_field_len(c->cfg.nx, c->cfg.ny, c->cfg.nz, ut);
 }
 
+// Device coefficient pointers into a packed buffer of element type T
+// (base == nullptr gives null pointers).
+template <typename T>
+DCoefT<T> make_dcoef(const T *base, const otbl_coef_offsets &o, const otbl_config &cfg) {
+  DCoefT<T> d{};
+  d.nx = cfg.nx;
+  d.ny = cfg.ny;
+  d.nz = cfg.nz;
+  d.nz1 = 2 * (cfg.nz / 3);
+  d.nz2 = d.nz1 / 2 - 1;
+  d.xout = cfg.xout;
+  d.xround = cfg.xpose_round;
+  auto P = [&](int id) { return base ? base + o.off[id] : (const T *)nullptr; };
+  d.S = P(OTBL_C_SCAL);
+  d.y = P(OTBL_C_Y);
+  d.dy = P(OTBL_C_DY);
+  d.idy = P(OTBL_C_IDY);
+  d.idyy = P(OTBL_C_IDYY);
+  d.dymin = P(OTBL_C_DYMIN);
+  d.kaz = P(OTBL_C_KAZ);
+  d.kaz2 = P(OTBL_C_KAZ2);
+  d.kvis = P(OTBL_C_KVIS);
+  d.kmod = P(OTBL_C_KMOD);
+  d.ayp = P(OTBL_C_AYP);
+  d.vmagic = P(OTBL_C_VMAGIC);
+  d.hy = P(OTBL_C_HY);
+  d.inxu = P(OTBL_C_INXU);
+  d.inxv = P(OTBL_C_INXV);
+  d.cofiux = P(OTBL_C_COFIUX);
+  d.cofivx = P(OTBL_C_COFIVX);
+  d.inbx = P(OTBL_C_INBX);
+  d.dcxu = P(OTBL_C_DCXU);
+  d.dcxv = P(OTBL_C_DCXV);
+  d.cofcxu = P(OTBL_C_COFCXU);
+  d.cofcxv = P(OTBL_C_COFCXV);
+  d.dcbx = P(OTBL_C_DCBX);
+  d.vixu = P(OTBL_C_VIXU);
+  d.vixv = P(OTBL_C_VIXV);
+  d.cofvxu = P(OTBL_C_COFVXU);
+  d.cofvxv = P(OTBL_C_COFVXV);
+  d.cofvbx = P(OTBL_C_COFVBX);
+  d.inyu = P(OTBL_C_INYU);
+  d.inyv = P(OTBL_C_INYV);
+  d.cofiuy = P(OTBL_C_COFIUY);
+  d.cofivy = P(OTBL_C_COFIVY);
+  d.inby = P(OTBL_C_INBY);
+  d.dcyu = P(OTBL_C_DCYU);
+  d.dcyv = P(OTBL_C_DCYV);
+  d.cofcyu = P(OTBL_C_COFCYU);
+  d.cofcyv = P(OTBL_C_COFCYV);
+  d.dcby = P(OTBL_C_DCBY);
+  d.viyu = P(OTBL_C_VIYU);
+  d.viyv = P(OTBL_C_VIYV);
+  d.vyui = P(OTBL_C_VYUI);
+  d.vyvi = P(OTBL_C_VYVI);
+  d.cofvyu = P(OTBL_C_COFVYU);
+  d.cofvyv = P(OTBL_C_COFVYV);
+  d.cofvby = P(OTBL_C_COFVBY);
+  d.ccon = P(OTBL_C_CCON);
+  return d;
+}
+
 int check(otbl_ctx *c, cudaError_t e, const char *where) {
   if (e != cudaSuccess) {
     c->err = std::string(where) + ": " + cudaGetErrorString(e);
@@ -100,61 +162,19 @@ extern "C" int otbl_ctx_create(const otbl_config *cfg, const double *coef, int d
     *out = c;
     return fail(c, OTBL_ERR_CUDA, "coefficient upload failed");
   }
-  DCoef &d = c->dc;
-  d.nx = nx;
-  d.ny = ny;
-  d.nz = nz;
-  d.nz1 = nz1;
-  d.nz2 = nz1 / 2 - 1;
-  d.xout = cfg->xout;
-  d.xround = cfg->xpose_round;
-  auto P = [&](int id) { return (const double *)(c->coef_dev + o.off[id]); };
-  d.S = P(OTBL_C_SCAL);
-  d.y = P(OTBL_C_Y);
-  d.dy = P(OTBL_C_DY);
-  d.idy = P(OTBL_C_IDY);
-  d.idyy = P(OTBL_C_IDYY);
-  d.dymin = P(OTBL_C_DYMIN);
-  d.kaz = P(OTBL_C_KAZ);
-  d.kaz2 = P(OTBL_C_KAZ2);
-  d.kvis = P(OTBL_C_KVIS);
-  d.kmod = P(OTBL_C_KMOD);
-  d.ayp = P(OTBL_C_AYP);
-  d.vmagic = P(OTBL_C_VMAGIC);
-  d.hy = P(OTBL_C_HY);
-  d.inxu = P(OTBL_C_INXU);
-  d.inxv = P(OTBL_C_INXV);
-  d.cofiux = P(OTBL_C_COFIUX);
-  d.cofivx = P(OTBL_C_COFIVX);
-  d.inbx = P(OTBL_C_INBX);
-  d.dcxu = P(OTBL_C_DCXU);
-  d.dcxv = P(OTBL_C_DCXV);
-  d.cofcxu = P(OTBL_C_COFCXU);
-  d.cofcxv = P(OTBL_C_COFCXV);
-  d.dcbx = P(OTBL_C_DCBX);
-  d.vixu = P(OTBL_C_VIXU);
-  d.vixv = P(OTBL_C_VIXV);
-  d.cofvxu = P(OTBL_C_COFVXU);
-  d.cofvxv = P(OTBL_C_COFVXV);
-  d.cofvbx = P(OTBL_C_COFVBX);
-  d.inyu = P(OTBL_C_INYU);
-  d.inyv = P(OTBL_C_INYV);
-  d.cofiuy = P(OTBL_C_COFIUY);
-  d.cofivy = P(OTBL_C_COFIVY);
-  d.inby = P(OTBL_C_INBY);
-  d.dcyu = P(OTBL_C_DCYU);
-  d.dcyv = P(OTBL_C_DCYV);
-  d.cofcyu = P(OTBL_C_COFCYU);
-  d.cofcyv = P(OTBL_C_COFCYV);
-  d.dcby = P(OTBL_C_DCBY);
-  d.viyu = P(OTBL_C_VIYU);
-  d.viyv = P(OTBL_C_VIYV);
-  d.vyui = P(OTBL_C_VYUI);
-  d.vyvi = P(OTBL_C_VYVI);
-  d.cofvyu = P(OTBL_C_COFVYU);
-  d.cofvyv = P(OTBL_C_COFVYV);
-  d.cofvby = P(OTBL_C_COFVBY);
-  d.ccon = P(OTBL_C_CCON);
+  c->mixed = cfg->precision == OTBL_PREC_MIXED;
+  c->dc = make_dcoef<double>(c->coef_dev, o, *cfg);
+  c->dcf = make_dcoef<float>(nullptr, o, *cfg);
+  if (c->mixed) {
+    // FP32 copy of the packed coefficients for the FP32 operators
+    std::vector<float> cf(coef, coef + ncoef);
+    TRY(dalloc(c, &c->coef_dev_f, ncoef));
+    if (cudaMemcpy(c->coef_dev_f, cf.data(), ncoef * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) {
+      *out = c;
+      return fail(c, OTBL_ERR_CUDA, "coefficient upload failed");
+    }
+    c->dcf = make_dcoef<float>(c->coef_dev_f, o, *cfg);
+  }
 
   const size_t lu = otbl_field_len(nx, ny, nz, 1);
   for (int id = 0; id < OTBL_F_COUNT; ++id) TRY(dalloc(c, &c->f[id], field_len(c, id)));
@@ -163,12 +183,28 @@ extern "C" int otbl_ctx_create(const otbl_config *cfg, const double *coef, int d
   TRY(dalloc(c, &c->um, (size_t)ny + 1));
   TRY(dalloc(c, &c->st, 1));
   Work &w = c->w;
-  double **big[] = {&w.ux, &w.vx, &w.wx, &w.uy, &w.wy, &w.vy, &w.uu, &w.uw, &w.uv,
-                    &w.vw, &w.vv, &w.ww, &w.cu, &w.cv, &w.cw, &w.s1, &w.s2, &w.s3};
-  for (double **b : big) TRY(dalloc(c, b, lu));
+  void **inter[] = {&w.ux, &w.vx, &w.wx, &w.uy, &w.wy, &w.vy, &w.uu, &w.uw,
+                    &w.uv, &w.vw, &w.vv, &w.ww, &w.cu, &w.cv, &w.cw};
+  for (void **b : inter) {
+    if (c->mixed) {
+      float *q = nullptr;
+      TRY(dalloc(c, &q, lu));
+      *b = q;
+    } else {
+      double *q = nullptr;
+      TRY(dalloc(c, &q, lu));
+      *b = q;
+    }
+  }
+  double **scratch[] = {&w.s1, &w.s2, &w.s3};
+  for (double **b : scratch) TRY(dalloc(c, b, lu));
   const int M = nz / 2, n = nx - 1;
   TRY(dalloc(c, &w.twz, 2 * (size_t)M));
   TRY(dalloc(c, &w.twz2, 2 * (size_t)M));
+  if (c->mixed) {
+    TRY(dalloc(c, &w.twzf, 2 * (size_t)M));
+    TRY(dalloc(c, &w.twz2f, 2 * (size_t)M));
+  }
   TRY(dalloc(c, &w.twx, 2 * (size_t)n));
   TRY(dalloc(c, &w.twx2, 2 * (size_t)n));
   TRY(dalloc(c, &w.vm_bits, (size_t)ny + 1));

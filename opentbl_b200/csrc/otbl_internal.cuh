@@ -15,18 +15,23 @@ namespace otbl {
 
 // Device view of the packed coefficient buffer (include/otbl_layout.h).
 // Passed by value to kernels; every pointer is into one device allocation.
-struct DCoef {
+// Device pointers into a packed coefficient buffer (otbl_layout.h): FP64 for
+// the FP64 path, and an FP32 copy (the same layout, every value rounded) for
+// the FP32 operators of the mixed-precision path.
+template <typename T>
+struct DCoefT {
   int nx, ny, nz, nz1, nz2, xout;
   int xround;  // OTBL_XPOSE_FP32: round x-line inputs/outputs to REAL4
-  const double *S;
-  const double *y, *dy, *idy, *idyy, *dymin, *kaz, *kaz2, *kvis, *kmod, *ayp, *vmagic, *hy;
-  const double *inxu, *inxv, *cofiux, *cofivx, *inbx;
-  const double *dcxu, *dcxv, *cofcxu, *cofcxv, *dcbx;
-  const double *vixu, *vixv, *cofvxu, *cofvxv, *cofvbx;
-  const double *inyu, *inyv, *cofiuy, *cofivy, *inby;
-  const double *dcyu, *dcyv, *cofcyu, *cofcyv, *dcby;
-  const double *viyu, *viyv, *vyui, *vyvi, *cofvyu, *cofvyv, *cofvby, *ccon;
+  const T *S;
+  const T *y, *dy, *idy, *idyy, *dymin, *kaz, *kaz2, *kvis, *kmod, *ayp, *vmagic, *hy;
+  const T *inxu, *inxv, *cofiux, *cofivx, *inbx;
+  const T *dcxu, *dcxv, *cofcxu, *cofcxv, *dcbx;
+  const T *vixu, *vixv, *cofvxu, *cofvxv, *cofvbx;
+  const T *inyu, *inyv, *cofiuy, *cofivy, *inby;
+  const T *dcyu, *dcyv, *cofcyu, *cofcyv, *dcby;
+  const T *viyu, *viyv, *vyui, *vyvi, *cofvyu, *cofvyv, *cofvby, *ccon;
 };
+using DCoef = DCoefT<double>;
 
 // Scalars that live on the device so that no host synchronisation is needed
 // inside a step (dt is produced by a reduction on the device).
@@ -42,14 +47,17 @@ struct DState {
   int pad[2];
 };
 
-// Device work buffers. Field-sized arrays use the plane layout.
+// Device work buffers. Field-sized arrays use the plane layout. The fifteen
+// intermediate fields hold doubles on the FP64 path and floats on the mixed
+// path (OTBL_PREC_MIXED); the kernels cast them to their element type.
 struct Work {
-  double *ux, *vx, *wx;        // interpxx outputs (u-type, v-type, u-type)
-  double *uy, *wy, *vy;        // interpyy outputs (ny rows each)
-  double *uu, *uw, *uv, *vw, *vv, *ww;  // products (uu, uw u-type; others ny rows)
-  double *cu, *cv, *cw;        // difvisxx outputs
-  double *s1, *s2, *s3;        // line-solve scratch (u-type size)
+  void *ux, *vx, *wx;          // interpxx outputs (u-type, v-type, u-type)
+  void *uy, *wy, *vy;          // interpyy outputs (ny rows each)
+  void *uu, *uw, *uv, *vw, *vv, *ww;  // products (uu, uw u-type; others ny rows)
+  void *cu, *cv, *cw;          // difvisxx outputs
+  double *s1, *s2, *s3;        // line-solve scratch and pois' phi (u-type size)
   double *twz, *twz2;          // z-FFT twiddles exp(-2 pi i t/M), exp(-2 pi i t/nz)
+  float *twzf, *twz2f;         // the same rounded to FP32 (mixed path)
   double *twx;                 // x-DCT twiddles for the length nx-1 FFT
   double *twx2;                // exp(-i pi k/(2n)), k = 0..n-1
   unsigned long long *vm_bits; // vm(j) maxima, j = 1..ny
@@ -65,7 +73,10 @@ struct otbl_ctx {
   int device;
   cudaStream_t stream;
   otbl::DCoef dc;
+  otbl::DCoefT<float> dcf;  // FP32 coefficients (mixed path)
+  int mixed;                // cfg.precision == OTBL_PREC_MIXED
   double *coef_dev;
+  float *coef_dev_f;
   std::vector<double> coef_host;
   double *f[OTBL_F_COUNT];
   double *u0, *v0, *um;

@@ -24,7 +24,8 @@ class OtblConfig(ctypes.Structure):
                 ("dt_mode", ctypes.c_int), ("re", ctypes.c_double),
                 ("ax", ctypes.c_double), ("ay", ctypes.c_double),
                 ("az", ctypes.c_double), ("cfl", ctypes.c_double),
-                ("y_blend", ctypes.c_double), ("dt_fixed", ctypes.c_double)]
+                ("y_blend", ctypes.c_double), ("dt_fixed", ctypes.c_double),
+                ("precision", ctypes.c_int), ("reserved", ctypes.c_int)]
 
 
 class OtblInflow(ctypes.Structure):
@@ -98,7 +99,8 @@ UTYPE = {"u": True, "v": False, "w": True, "p": False,
 
 def make_config(cfg, re: float, xout: int) -> OtblConfig:
     return OtblConfig(cfg.nx, cfg.ny, cfg.nz, xout, cfg.xpose_round, cfg.dt_mode,
-                      re, cfg.ax, 0.0, cfg.az, cfg.cfl, cfg.y_blend, cfg.dt_fixed)
+                      re, cfg.ax, 0.0, cfg.az, cfg.cfl, cfg.y_blend, cfg.dt_fixed,
+                      getattr(cfg, "precision", 0), 0)
 
 
 class OracleBox:

@@ -51,10 +51,16 @@ def test_config_check():
     L = native.lib()
     good = native.make_config(config.TINY, 300.0, 10)
     assert L.otbl_config_check(ctypes.byref(good)) == 0
-    for field, bad in (("nx", 3), ("ny", 2), ("nz", 2), ("xout", 0), ("xout", 99), ("re", -1.0)):
+    for field, bad in (("nx", 3), ("ny", 2), ("nz", 2), ("xout", 0), ("xout", 99), ("re", -1.0),
+                       ("precision", 2), ("precision", -1)):
         c = native.make_config(config.TINY, 300.0, 10)
         setattr(c, field, bad)
         assert L.otbl_config_check(ctypes.byref(c)) == 2, field
+    mixed = native.make_config(config.TINY, 300.0, 10)
+    mixed.precision = 1
+    assert L.otbl_config_check(ctypes.byref(mixed)) == 0
+    mixed.xpose_round = 1  # REAL4 transposes are an FP64-path mode
+    assert L.otbl_config_check(ctypes.byref(mixed)) == 2
     assert L.otbl_config_check(None) == 1
 
 

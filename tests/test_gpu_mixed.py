@@ -1,0 +1,87 @@
+"""Mixed-precision path (OTBL_PREC_MIXED) against the FP64 oracle and the
+FP64 GPU path on the same seeded inputs and coefficient bits.
+
+The mixed path computes the x/y interpolations, d/dx, the spanwise FFTs and
+the products in FP32 and keeps the state, the RK3 combination, implzy, the
+Poisson solve and the projection in FP64. Tolerances (written here, from
+the north star's mixed-path gates): velocity relative L2 (Parseval weights)
+<= 1e-5 after 100 steps of 1025x193x512 and after 20 steps of 257x97x128;
+max|div u| after the projection <= 1e-10; the mean profile, Re_theta and
+C_f to 1e-5 relative. One substep of the small boxes: <= 1e-6, pressure
+<= 1e-5, RHS history <= 1e-4. Measured on B200: 1.8e-8 after one substep,
+1.7e-7 after 20 steps of 257x97x128, 3.4e-7 after 100 steps of
+1025x193x512, max|div u| ~1e-14.
+"""
+import numpy as np
+import pytest
+
+from opentbl_b200 import Box, config, diag
+from opentbl_b200.config import replace
+
+from helpers import oracle_box, rel_l2, setup
+
+pytestmark = pytest.mark.gpu
+
+
+def _mixed(cfg):
+    return replace(cfg, precision=1, name=(cfg.name or "box") + "-mixed")
+
+
+def _report(tag, g, o, cfg, coef):
+    out = diag.compare(cfg, coef, g, o)
+    print(tag, out)
+    return out
+
+
+@pytest.mark.parametrize("name", ["TINY", "SMALL"])
+def test_mixed_one_substep(name):
+    cfg = getattr(config, name)
+    init, coef = setup(cfg)
+    g = Box(_mixed(cfg), init, coef)
+    o = oracle_box(cfg, init, coef)
+    g.substep(1, True)
+    o.substep(1, 1)
+    r = _report(f"{name} mixed, 1 substep", g, o, cfg, coef)
+    assert r["vel_rel_l2"] <= 1e-6
+    assert r["max_div"] <= 1e-10
+    other = {n: rel_l2(g.field(n), o.field(n)) for n in ("p", "rhsupa", "rhsvpa", "rhswpa")}
+    print(name, "mixed, 1 substep, other fields", other)
+    # the RHS history is the raw FP32-derived right-hand side (measured
+    # 2e-5 for rhsupa, whose convective and viscous parts nearly cancel);
+    # it enters the velocity only times dt
+    assert other["p"] <= 1e-5
+    assert max(other[n] for n in ("rhsupa", "rhsvpa", "rhswpa")) <= 1e-4
+
+
+def test_mixed_c1_twenty_steps():
+    cfg = config.C1
+    init, coef = setup(cfg)
+    g = Box(_mixed(cfg), init, coef)
+    o = oracle_box(cfg, init, coef)
+    g.advance(20)
+    o.advance(20)
+    r = _report("C1 mixed, 20 steps", g, o, cfg, coef)
+    assert r["vel_rel_l2"] <= 1e-5
+    assert r["max_div"] <= 1e-10
+    for k in ("U_rel_l2", "um_rel_l2", "re_theta_rel", "cf_rel"):
+        assert r[k] <= 1e-5, k
+
+
+def test_mixed_c2_hundred_steps_against_fp64():
+    """1025x193x512, 100 RK3 steps: the mixed path against the FP64 GPU
+    path, which the FP64 parity tests pin to the oracle."""
+    cfg = config.C2
+    init, coef = setup(cfg)
+    f = Box(cfg, init, coef)
+    m = Box(_mixed(cfg), init, coef)
+    res = {}
+    done = 0
+    for k in (20, 100):
+        f.advance(k - done)
+        m.advance(k - done)
+        done = k
+        res[k] = _report(f"C2 mixed vs FP64 GPU, {k} steps", m, f, cfg, coef)
+    assert res[100]["vel_rel_l2"] <= 1e-5
+    assert res[100]["max_div"] <= 1e-10
+    for k in ("U_rel_l2", "um_rel_l2", "re_theta_rel", "cf_rel"):
+        assert res[100][k] <= 1e-5, k
