@@ -30,7 +30,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 from opentbl_b200 import config as cfgmod  # noqa: E402
-from opentbl_b200 import diag, native, replicas, synth  # noqa: E402
+from opentbl_b200 import diag, ensemble, native, replicas, serve, synth  # noqa: E402
 from opentbl_b200.box import Box  # noqa: E402
 
 WORKLOAD = "C2"
@@ -205,6 +205,81 @@ def run_reference(args, cfg, ws, rank):
     print(json.dumps(out), flush=True)
 
 
+def run_ensemble(device, R, steps):
+    """The 24-box sweep (nx in {129..513}, ny in {65, 97, 129}, nz in {64,
+    128, 256}, mixed precision), autotuned, one CUDA graph per RK3 step over
+    all boxes, against the same boxes advanced by plain launches."""
+    import torch
+    cfgs = ensemble.ensemble_configs(24)
+    boxes = []
+    for c in cfgs:
+        init = synth.make_initial(c)
+        boxes.append(Box(c, init, device=device))
+    tuned = [b.autotune() for b in boxes]
+    mpts = sum(c.mpts for c in cfgs)
+    g = ensemble.Graph(boxes, 1)
+    gs = torch.cuda.ExternalStream(g.stream, device=f"cuda:{device}")
+    for _ in range(3):
+        g.launch()
+    g.sync()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    replicas.barrier(R)
+    ev0.record(gs)
+    for _ in range(steps):
+        g.launch()
+    ev1.record(gs)
+    ev1.synchronize()
+    ms_g = replicas.max_over_ranks(ev0.elapsed_time(ev1), R)
+    kernels = g.kernels
+    g.close()
+    # plain launches: every box advanced one step per round, each on its stream
+    for b in boxes:
+        b.sync()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        for b in boxes:
+            b.advance(1)
+    for b in boxes:
+        b.sync()
+    ms_p = replicas.max_over_ranks((time.perf_counter() - t0) * 1e3, R)
+    for b in boxes:
+        b.close()
+    sub = 3 * steps
+    return {"boxes": len(cfgs), "mpts_total": mpts, "steps": steps, "precision": "mixed",
+            "graph": {"value": replicas.aggregate_rate(mpts * sub, ms_g / 1e3, R), "unit": UNIT,
+                      "ms_per_step": ms_g / steps, "kernels_per_launch": kernels,
+                      "launches_per_step": 1, "timing": "CUDA events on the graph stream"},
+            "plain": {"value": replicas.aggregate_rate(mpts * sub, ms_p / 1e3, R), "unit": UNIT,
+                      "ms_per_step": ms_p / steps, "timing": "host clock around synchronised rounds"},
+            "autotuned_cta_sizes": {c.name: t for c, t in zip(cfgs, tuned)}}
+
+
+def run_serve(device, args, ens):
+    """A bounded sample of the serving config: Poisson arrivals sized to
+    `serve_load` of the ensemble's graph throughput, K ~ U[10, kmax], sizes
+    as the ensemble sweep with 10% at 1025x193x256, mixed precision, 150 GB
+    HBM budget."""
+    cap = ens["graph"]["value"] if ens else 4000.0
+    probe = serve.make_requests(args.serve_requests, seed=7, rate=1.0, kmax=args.serve_kmax)
+    work = np.mean([r.cfg.mpts * 3 * r.steps for r in probe])
+    rate = args.serve_load * cap / work
+    reqs = serve.make_requests(args.serve_requests, seed=7, rate=rate, kmax=args.serve_kmax)
+    tpl = serve.Templates()
+    t0 = time.perf_counter()
+    tpl.prepare(reqs)
+    prep = time.perf_counter() - t0
+    srv = serve.Server(device=device, budget_bytes=150e9, chunk=4)
+    res = srv.run(reqs)
+    out = serve.summarize(res, srv.makespan)
+    out.update({"rate_per_s": rate, "offered_load": args.serve_load, "kmax": args.serve_kmax,
+                "budget_gb": 150, "stats": srv.stats, "template_prep_s": prep,
+                "sample": f"{len(reqs)} requests (the full config is 2000 with K in [10, 200])"})
+    srv.close()
+    return out
+
+
 def run_mixed(cfg, init, coef, fbox, device, R, warm, K, fp64_ms_per_step):
     """The mixed-precision path (OTBL_PREC_MIXED) on the same box: device
     time of K RK3 steps after `warm`, then its error against the FP64 path
@@ -265,6 +340,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--ensemble-steps", type=int, default=10)
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=48)
+    ap.add_argument("--serve-kmax", type=int, default=40)
+    ap.add_argument("--serve-load", type=float, default=0.7)
     args = ap.parse_args()
     cfg = getattr(cfgmod, args.config)
     R = replicas.setup()
@@ -369,6 +450,14 @@ def main():
     if not args.no_mixed:
         mixed = run_mixed(cfg, init, coef, box, local, R, warm, K, ms / K)
 
+    ens = None
+    if not args.no_ensemble:
+        box.close()
+        ens = run_ensemble(local, R, args.ensemble_steps)
+    srv = None
+    if not args.no_serve and ws == 1:
+        srv = run_serve(local, args, ens)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:
@@ -391,9 +480,10 @@ def main():
                "roofline": roofline, "substep_roofline": substep_roofline,
                "kernels_ms_per_substep": kernels,
                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
-               "mixed": mixed}
+               "mixed": mixed, "ensemble": ens, "serving": srv}
         print(json.dumps(out), flush=True)
-    box.close()
+    if args.no_ensemble:
+        box.close()
     replicas.teardown(R)
 
 

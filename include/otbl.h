@@ -32,6 +32,7 @@ extern "C" {
 #define OTBL_ERR_CUDA 4     /* CUDA runtime error                             */
 #define OTBL_ERR_NAN 5      /* non-finite value detected by the dt reduction  */
 #define OTBL_ERR_NODEV 6    /* no CUDA device / extension not usable          */
+#define OTBL_BUSY 7         /* otbl_query / otbl_graph_query: work in flight  */
 
 /* transposes (change.f90): round the payload to REAL4 as the reference's
  * MPI_ALLTOALLV(MPI_REAL4) does (change.f90:579,608,641,652,676,686), or
@@ -99,13 +100,23 @@ int otbl_ctx_create(const otbl_config *cfg, const double *coef, int device,
 void otbl_ctx_destroy(otbl_ctx *ctx);
 const char *otbl_last_error(const otbl_ctx *ctx);
 size_t otbl_device_bytes(const otbl_ctx *ctx);
+/* device bytes otbl_ctx_create allocates for cfg (0 if cfg is invalid) */
+size_t otbl_ctx_bytes(const otbl_config *cfg);
+/* re-binds a context to another box of the same nx, ny, nz and precision:
+ * new config values (xout, re, ax, az, cfl, ...) and coefficients, no device
+ * allocation; the state is then uploaded with otbl_set_field and
+ * otbl_set_inflow. For slot reuse by a serving loop (no counterpart in the
+ * reference). Synchronizes. */
+int otbl_ctx_rebind(otbl_ctx *ctx, const otbl_config *cfg, const double *coef);
 
 /* host <-> device copies of the state, reference layout */
 int otbl_set_field(otbl_ctx *ctx, int id, const double *host);
 int otbl_get_field(otbl_ctx *ctx, int id, double *host);
 int otbl_field_device_ptr(otbl_ctx *ctx, int id, double **dptr);
 /* u0 (ny+1), v0 (ny): inlet profiles (getstartzy-bg.F90:273-276);
- * um (ny+1): filtered mean profile at xout (readheader, getstartzy-bg.F90:578) */
+ * um (ny+1): filtered mean profile at xout (readheader, getstartzy-bg.F90:578).
+ * A restart: also clears the error flag, the frozen dt of OTBL_DT_FIXED with
+ * dt_fixed <= 0 and the energies. */
 int otbl_set_inflow(otbl_ctx *ctx, const double *u0, const double *v0,
                     const double *um, const otbl_inflow *st);
 int otbl_get_inflow(otbl_ctx *ctx, double *um, otbl_inflow *st);
@@ -182,6 +193,36 @@ int otbl_genflu_noalloc(otbl_ctx *ctx, double *u_dev, double *v_dev,
 
 /* kernel launches issued by this context since creation */
 long long otbl_launch_count(const otbl_ctx *ctx);
+
+/* ---- CUDA graphs of RK3 steps, ensembles (no counterpart in the reference,
+ *      which advances one box per MPI job) ----
+ * otbl_graph_create captures otbl_advance(ctx[k], nsteps) of n contexts on
+ * one device into one CUDA graph, each context a branch that runs
+ * concurrently with the others. Outstanding work of the members is finished
+ * first. Every otbl_graph_launch then advances every member by nsteps RK3
+ * steps on the graph's own stream (asynchronous); the members must not be
+ * driven through their own entry points while a launch is in flight
+ * (otbl_graph_sync or a finished otbl_graph_query orders them again). The
+ * graph holds the members' device buffers: destroy it before them.
+ * Per-kernel profiling must be off while capturing. */
+typedef struct otbl_graph otbl_graph;
+int otbl_graph_create(otbl_ctx *const *ctxs, int n, int nsteps, otbl_graph **out);
+int otbl_graph_launch(otbl_graph *g);
+int otbl_graph_sync(otbl_graph *g);
+int otbl_graph_query(otbl_graph *g);           /* OTBL_OK done, OTBL_BUSY */
+int otbl_graph_stream(otbl_graph *g, void **stream);
+long long otbl_graph_kernels(const otbl_graph *g); /* kernels per launch */
+void otbl_graph_destroy(otbl_graph *g);
+/* OTBL_OK when every call issued on the context has finished, OTBL_BUSY
+ * while work is in flight (never blocks) */
+int otbl_query(otbl_ctx *ctx);
+/* Autotuner (no counterpart in the reference): times CTA sizes of 32, 64
+ * and 128 threads for the x-interpolation, d/dx and y-interpolation line
+ * kernels on this context's box and precision and keeps the fastest. Those
+ * kernels write only work arrays, so the state is unchanged; the arithmetic
+ * does not depend on the CTA size. choice (3 ints, may be NULL) receives the
+ * sizes picked. Call before otbl_graph_create. Synchronizes. */
+int otbl_autotune(otbl_ctx *ctx, int *choice);
 
 /* ---- instrumentation (no counterpart in the reference, whose timers are
  *      the MPI_WTIME accumulators of module temporal, mod.F90:311-322) ---- */

@@ -47,6 +47,20 @@ class Box:
             raise OtblError(f"otbl_ctx_create: {native.ERRORS.get(st, st)} {msg}")
         self.load(init)
 
+    def rebind(self, cfg: BoxConfig, init: dict, coef: np.ndarray | None = None):
+        """Re-use this context for another box of the same nx, ny, nz and
+        precision (otbl_ctx_rebind), then upload its state."""
+        re, xout = float(init["re"]), int(init["xout"])
+        y = np.asarray(init["y"], dtype=np.float64)
+        if coef is None:
+            coef = native.coef_compute(cfg, re, xout, y, init["u0"])
+        coef = np.ascontiguousarray(coef, dtype=np.float64)
+        ccfg = native.make_config(cfg, re, xout)
+        self._check(self.L.otbl_ctx_rebind(self.h, ctypes.byref(ccfg), native.dptr(coef)),
+                    "otbl_ctx_rebind")
+        self.cfg, self.re, self.xout, self.y, self.coef, self.ccfg = cfg, re, xout, y, coef, ccfg
+        self.load(init)
+
     def load(self, init: dict):
         """Upload a state: the seven fields and the genmod inflow state
         (getstartzy-bg.F90:18-297, :490-581)."""
@@ -151,6 +165,20 @@ class Box:
 
     def sync(self):
         self._check(self.L.otbl_sync(self.h), "otbl_sync")
+
+    def autotune(self) -> tuple:
+        """CTA sizes for k_interpx, k_difvisx, k_interpy picked by timing."""
+        ch = (ctypes.c_int * 3)()
+        self._check(self.L.otbl_autotune(self.h, ch), "otbl_autotune")
+        return tuple(ch)
+
+    def busy(self) -> bool:
+        """True while work issued on the context is in flight (never blocks)."""
+        st = self.L.otbl_query(self.h)
+        if st == native.OTBL_BUSY:
+            return True
+        self._check(st, "otbl_query")
+        return False
 
     def boun(self):
         self._check(self.L.otbl_boun(self.h), "otbl_boun")

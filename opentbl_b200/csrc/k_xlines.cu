@@ -199,11 +199,12 @@ cudaError_t launch_interpx(otbl_ctx *c) {
     a.which[f] = which[f];
     a.np[f] = np[f];
   }
+  const int bs = c->tune_bs[0];
   prof_begin(c, PK_INTERPX);
   if (c->mixed)
-    k_interpx<float><<<dim3((npu + 127) / 128, 3), 128, 0, c->stream>>>(c->dcf, a);
+    k_interpx<float><<<dim3((npu + bs - 1) / bs, 3), bs, 0, c->stream>>>(c->dcf, a);
   else
-    k_interpx<double><<<dim3((npu + 127) / 128, 3), 128, 0, c->stream>>>(c->dc, a);
+    k_interpx<double><<<dim3((npu + bs - 1) / bs, 3), bs, 0, c->stream>>>(c->dc, a);
   prof_end(c);
   c->launches += 1;
   return cudaGetLastError();
@@ -226,11 +227,12 @@ cudaError_t launch_difvisx(otbl_ctx *c) {
     a.which[f] = which[f];
     a.np[f] = np[f];
   }
+  const int bs = c->tune_bs[1];
   prof_begin(c, PK_DIFVISX);
   if (c->mixed)
-    k_difvisx<float><<<dim3((npu + 127) / 128, 3), 128, 0, c->stream>>>(c->dcf, a);
+    k_difvisx<float><<<dim3((npu + bs - 1) / bs, 3), bs, 0, c->stream>>>(c->dcf, a);
   else
-    k_difvisx<double><<<dim3((npu + 127) / 128, 3), 128, 0, c->stream>>>(c->dc, a);
+    k_difvisx<double><<<dim3((npu + bs - 1) / bs, 3), bs, 0, c->stream>>>(c->dc, a);
   prof_end(c);
   c->launches += 1;
   return cudaGetLastError();

@@ -16,6 +16,21 @@
 namespace otbl {
 
 constexpr int KY = 8;  // rows per checkpointed segment
+// Segment length and occupancy of the rhsp tail (k_final_s1/s2), per
+// element type of its FP32-capable inputs; measured on B200 at
+// 1025x193x512 over KF in {4, 6, 8} x CTAs/SM in {3..6}: FP64 4 rows at 4
+// CTAs of 128 threads per SM (7.2 ms per substep, 7.8 at 8 rows), mixed 6
+// rows at 5 CTAs (7.0 ms, 8.4 at 8 rows at 4).
+template <typename W>
+struct FinalTune;
+template <>
+struct FinalTune<double> {
+  static constexpr int kf = 4, minb = 4;
+};
+template <>
+struct FinalTune<float> {
+  static constexpr int kf = 6, minb = 5;
+};
 
 // interpyy, which 0: u, w (in rows ny+1), which 1: v (in rows ny); out rows
 // 1..ny. blockIdx.y = field (u, w, v). T: arithmetic and output type (float
@@ -120,7 +135,7 @@ struct FinalArgs {
 // (nx*nz1) than a GPU has threads, so latency is hidden by occupancy.
 //   k_final_s1, pass A (rows ascending): the forward sweeps of differzy (of
 //     the product) and vistyy (of the old velocity), with a checkpoint every
-//     KY rows.
+//     KF rows (FinalTune).
 //   k_final_s1, pass B (segments descending): both forward sweeps recomputed
 //     from the checkpoints into registers, both back-substitutions, the RHS
 //     assembly, the RK3 combination, the new RHS history, and the
@@ -139,7 +154,8 @@ struct FinalStream {
 };
 
 template <int COMP, typename W>
-__global__ void __launch_bounds__(128, 4) k_final_s1(DCoef c, FinalStream<W> fs) {
+__global__ void __launch_bounds__(128, FinalTune<W>::minb) k_final_s1(DCoef c, FinalStream<W> fs) {
+  constexpr int KF = FinalTune<W>::kf;
   const FinalArgs<W> &a = fs.a;
   const int nx = c.nx, ny = c.ny, nz1 = c.nz1;
   const int ncol = (nx - 1) * nz1;
@@ -217,22 +233,22 @@ __global__ void __launch_bounds__(128, 4) k_final_s1(DCoef c, FinalStream<W> fs)
     const double in = __ldg(ecv + 3 * r) * up + __ldg(ecv + 3 * r + 1) * u0 + __ldg(ecv + 3 * r + 2) * um;
     return r == 0 ? b0 : (r == jee - 1 ? bN : in);
   };
-  const int nseg = (jee + KY - 1) / KY;
+  const int nseg = (jee + KF - 1) / KF;
   double *ck = fs.ck + col;
   // ---- pass A: forward sweeps, checkpoints
   double yd = 0.0, yv = 0.0;
   for (int sg = 0; sg < nseg; ++sg) {
-    const int s0 = sg * KY;
+    const int s0 = sg * KF;
     ck[(size_t)(2 * sg) * ncol] = yd;
     ck[(size_t)(2 * sg + 1) * ncol] = yv;
-    double gv[KY + 2], uv[KY + 2];  // rows s0-1 .. s0+KY
+    double gv[KF + 2], uv[KF + 2];  // rows s0-1 .. s0+KF
 #pragma unroll
-    for (int b = 0; b < KY + 2; ++b) {
+    for (int b = 0; b < KF + 2; ++b) {
       gv[b] = last ? 0.0 : Pg(s0 + b - 1);
       uv[b] = Vg(s0 + b - 1);
     }
 #pragma unroll
-    for (int b = 0; b < KY; ++b) {
+    for (int b = 0; b < KF; ++b) {
       const int r = s0 + b;
       if (r < jee) {
         if (!last) yd = rd(r, gv[b], gv[b + 1], gv[b + 2]) + (r > 0 ? __ldg(dcy + 3 * r) : 0.0) * yd;
@@ -247,16 +263,16 @@ __global__ void __launch_bounds__(128, 4) k_final_s1(DCoef c, FinalStream<W> fs)
   double res1 = 0.0, res2 = 0.0;             // combination of rows r+1, r+2
   double *bq = fs.bq + col;
   for (int sg = nseg - 1; sg >= 0; --sg) {
-    const int s0 = sg * KY;
-    double gv[KY + 2], uv[KY + 2], ydv[KY], yvv[KY];
+    const int s0 = sg * KF;
+    double gv[KF + 2], uv[KF + 2], ydv[KF], yvv[KF];
 #pragma unroll
-    for (int b = 0; b < KY + 2; ++b) {
+    for (int b = 0; b < KF + 2; ++b) {
       gv[b] = last ? 0.0 : Pg(s0 + b - 1);
       uv[b] = Vg(s0 + b - 1);
     }
     double ad = ck[(size_t)(2 * sg) * ncol], av = ck[(size_t)(2 * sg + 1) * ncol];
 #pragma unroll
-    for (int b = 0; b < KY; ++b) {
+    for (int b = 0; b < KF; ++b) {
       const int r = s0 + b;
       if (r < jee) {
         if (!last) ad = rd(r, gv[b], gv[b + 1], gv[b + 2]) + (r > 0 ? __ldg(dcy + 3 * r) : 0.0) * ad;
@@ -265,16 +281,16 @@ __global__ void __launch_bounds__(128, 4) k_final_s1(DCoef c, FinalStream<W> fs)
       ydv[b] = ad;
       yvv[b] = av;
     }
-    double cxv[KY], kpv[KY], hv[KY];
+    double cxv[KF], kpv[KF], hv[KF];
 #pragma unroll
-    for (int b = 0; b < KY; ++b) {
+    for (int b = 0; b < KF; ++b) {
       const int rr = min(s0 + b, jee - 1);
       cxv[b] = (double)__ldg(cX + (size_t)rr * S);
       kpv[b] = last ? 0.0 : (double)__ldg(kp + (size_t)min(rr, krows - 1) * S);
       hv[b] = __ldg(hp + (size_t)rr * S);
     }
 #pragma unroll
-    for (int b = KY - 1; b >= 0; --b) {
+    for (int b = KF - 1; b >= 0; --b) {
       const int r = s0 + b, j = r + 1;
       if (r >= jee) continue;
       if (!last) xd = (ydv[b] - __ldg(dcy + 3 * r + 2) * xd) * __ldg(dcy + 3 * r + 1);
@@ -330,6 +346,7 @@ __global__ void __launch_bounds__(128, 4) k_final_s1(DCoef c, FinalStream<W> fs)
 
 template <int COMP, typename W>
 __global__ void __launch_bounds__(128) k_final_s2(DCoef c, FinalStream<W> fs) {
+  constexpr int KF = FinalTune<W>::kf;
   const FinalArgs<W> &a = fs.a;
   const int nx = c.nx, ny = c.ny, nz1 = c.nz1;
   const int ncol = (nx - 1) * nz1;
@@ -343,35 +360,35 @@ __global__ void __launch_bounds__(128) k_final_s2(DCoef c, FinalStream<W> fs) {
   const double *fac = COMP == 1 ? a.fac_v : a.fac_u;  // row q uses fac[3(q+2)..]
   const double *bq = fs.bq + col;
   double *ck = fs.ck2 + col;
-  const int nseg = (n + KY - 1) / KY;
+  const int nseg = (n + KF - 1) / KF;
   double y = 0.0;
   for (int sg = 0; sg < nseg; ++sg) {
-    const int s0 = sg * KY;
+    const int s0 = sg * KF;
     ck[(size_t)sg * ncol] = y;
-    double bv[KY];
+    double bv[KF];
 #pragma unroll
-    for (int b = 0; b < KY; ++b) bv[b] = bq[(size_t)min(s0 + b, n - 1) * ncol];
+    for (int b = 0; b < KF; ++b) bv[b] = bq[(size_t)min(s0 + b, n - 1) * ncol];
 #pragma unroll
-    for (int b = 0; b < KY; ++b) {
+    for (int b = 0; b < KF; ++b) {
       const int q = s0 + b;
       if (q < n) y = bv[b] + (q > 0 ? __ldg(fac + 3 * (q + 2)) : 0.0) * y;
     }
   }
   double x = 0.0;
   for (int sg = nseg - 1; sg >= 0; --sg) {
-    const int s0 = sg * KY;
-    double bv[KY], yv[KY];
+    const int s0 = sg * KF;
+    double bv[KF], yv[KF];
 #pragma unroll
-    for (int b = 0; b < KY; ++b) bv[b] = bq[(size_t)min(s0 + b, n - 1) * ncol];
+    for (int b = 0; b < KF; ++b) bv[b] = bq[(size_t)min(s0 + b, n - 1) * ncol];
     double yy = ck[(size_t)sg * ncol];
 #pragma unroll
-    for (int b = 0; b < KY; ++b) {
+    for (int b = 0; b < KF; ++b) {
       const int q = s0 + b;
       if (q < n) yy = bv[b] + (q > 0 ? __ldg(fac + 3 * (q + 2)) : 0.0) * yy;
       yv[b] = yy;
     }
 #pragma unroll
-    for (int b = KY - 1; b >= 0; --b) {
+    for (int b = KF - 1; b >= 0; --b) {
       const int q = s0 + b;
       if (q < n) {
         x = (yv[b] - __ldg(fac + 3 * (q + 2) + 2) * x) * __ldg(fac + 3 * (q + 2) + 1);
@@ -488,10 +505,11 @@ cudaError_t launch_interpy(otbl_ctx *c) {
   }
   const int ncol = c->cfg.nx * c->dc.nz1;
   prof_begin(c, PK_INTERPY);
+  const int bs = c->tune_bs[2];
   if (c->mixed)
-    k_interpy<float><<<dim3((ncol + 127) / 128, 3), 128, 0, c->stream>>>(c->dcf, a);
+    k_interpy<float><<<dim3((ncol + bs - 1) / bs, 3), bs, 0, c->stream>>>(c->dcf, a);
   else
-    k_interpy<double><<<dim3((ncol + 127) / 128, 3), 128, 0, c->stream>>>(c->dc, a);
+    k_interpy<double><<<dim3((ncol + bs - 1) / bs, 3), bs, 0, c->stream>>>(c->dc, a);
   prof_end(c);
   c->launches += 1;
   return cudaGetLastError();

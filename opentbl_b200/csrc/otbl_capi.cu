@@ -221,6 +221,49 @@ extern "C" int otbl_ctx_create(const otbl_config *cfg, const double *coef, int d
   return OTBL_OK;
 }
 
+extern "C" size_t otbl_ctx_bytes(const otbl_config *cfg) {
+  if (!cfg || otbl_config_check(cfg) != OTBL_OK) return 0;
+  const int nx = cfg->nx, ny = cfg->ny, nz = cfg->nz, nz1 = 2 * (nz / 3), M = nz / 2, n = nx - 1;
+  const bool mixed = cfg->precision == OTBL_PREC_MIXED;
+  otbl_coef_offsets o;
+  otbl_coef_layout(nx, ny, nz, &o);
+  const size_t ncoef = o.off[OTBL_C_COUNT], lu = otbl_field_len(nx, ny, nz, 1), lv = otbl_field_len(nx, ny, nz, 0);
+  size_t b = ncoef * sizeof(double) + (mixed ? ncoef * sizeof(float) : 0);
+  b += (4 * lu + 3 * lv) * sizeof(double);                       // state
+  b += 3 * (size_t)(ny + 1) * sizeof(double) + sizeof(DState);   // u0, v0, um, scalars
+  b += 15 * lu * (mixed ? sizeof(float) : sizeof(double));       // intermediates
+  b += 3 * lu * sizeof(double);                                  // scratch
+  b += (4 * (size_t)M + 4 * (size_t)n) * sizeof(double) + (mixed ? 4 * (size_t)M * sizeof(float) : 0);
+  b += (size_t)(ny + 1) * 8 + 6 * (size_t)(ny + 4) * sizeof(double) + genflu_tab_doubles(ny) * sizeof(double);
+  b += (size_t)nx * ny * (nz1 / 2) * sizeof(double);             // Poisson pivots
+  return b;
+}
+
+extern "C" int otbl_ctx_rebind(otbl_ctx *c, const otbl_config *cfg, const double *coef) {
+  if (!c || !cfg || !coef) return OTBL_ERR_ARG;
+  int st = otbl_config_check(cfg);
+  if (st != OTBL_OK) return st;
+  if (cfg->nx != c->cfg.nx || cfg->ny != c->cfg.ny || cfg->nz != c->cfg.nz || cfg->precision != c->cfg.precision)
+    return OTBL_ERR_CONFIG;
+  cudaSetDevice(c->device);
+  OTBL_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  otbl_coef_offsets o;
+  otbl_coef_layout(cfg->nx, cfg->ny, cfg->nz, &o);
+  const size_t ncoef = o.off[OTBL_C_COUNT];
+  c->cfg = *cfg;
+  c->coef_host.assign(coef, coef + ncoef);
+  OTBL_CUDA_TRY(c, cudaMemcpy(c->coef_dev, coef, ncoef * sizeof(double), cudaMemcpyHostToDevice));
+  c->dc = make_dcoef<double>(c->coef_dev, o, *cfg);
+  if (c->mixed) {
+    std::vector<float> cf(coef, coef + ncoef);
+    OTBL_CUDA_TRY(c, cudaMemcpy(c->coef_dev_f, cf.data(), ncoef * sizeof(float), cudaMemcpyHostToDevice));
+    c->dcf = make_dcoef<float>(c->coef_dev_f, o, *cfg);
+  }
+  if (check(c, launch_pois_lu(c), "pois_lu") != OTBL_OK) return OTBL_ERR_CUDA;
+  OTBL_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  return OTBL_OK;
+}
+
 extern "C" void otbl_ctx_destroy(otbl_ctx *c) {
   if (!c) return;
   cudaSetDevice(c->device);
@@ -283,6 +326,8 @@ extern "C" int otbl_set_inflow(otbl_ctx *c, const double *u0, const double *v0, 
   h.gamma2 = s->gamma2;
   h.timec = s->timec;
   h.err = 0;
+  h.dt_frozen = 0;  // a restart: the fixed-dt mode takes its dt again
+  for (double &e : h.ener) e = 0.0;
   OTBL_CUDA_TRY(c, cudaMemcpyAsync(c->st, &h, sizeof(DState), cudaMemcpyHostToDevice, c->stream));
   OTBL_CUDA_TRY(c, cudaMemcpyAsync(c->u0, u0, sizeof(double) * (ny + 1), cudaMemcpyHostToDevice, c->stream));
   OTBL_CUDA_TRY(c, cudaMemcpyAsync(c->v0, v0, sizeof(double) * ny, cudaMemcpyHostToDevice, c->stream));

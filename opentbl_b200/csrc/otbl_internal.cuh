@@ -74,6 +74,10 @@ struct otbl_ctx {
   cudaStream_t stream;
   otbl::DCoef dc;
   otbl::DCoefT<float> dcf;  // FP32 coefficients (mixed path)
+  // threads per CTA of the line kernels that otbl_autotune times:
+  // [0] k_interpx, [1] k_difvisx, [2] k_interpy (one thread per line, so the
+  // choice changes the schedule, never the arithmetic)
+  int tune_bs[3] = {128, 128, 128};
   int mixed;                // cfg.precision == OTBL_PREC_MIXED
   double *coef_dev;
   float *coef_dev_f;

@@ -16,6 +16,7 @@ LIB_PATH = os.path.join(_HERE, "libotbl.so")
 _lib = None
 
 OTBL_OK = 0
+OTBL_BUSY = 7
 ERRORS = {1: "bad argument", 2: "bad configuration", 3: "out of device memory",
           4: "CUDA error", 5: "non-finite value", 6: "no CUDA device"}
 FIELDS = ("u", "v", "w", "p", "rhsupa", "rhsvpa", "rhswpa")
@@ -67,6 +68,8 @@ def _bind(L):
         "otbl_ctx_destroy": ([P], None),
         "otbl_last_error": ([P], ctypes.c_char_p),
         "otbl_device_bytes": ([P], ctypes.c_size_t),
+        "otbl_ctx_bytes": ([ctypes.POINTER(OtblConfig)], ctypes.c_size_t),
+        "otbl_ctx_rebind": ([P, ctypes.POINTER(OtblConfig), D], I),
         "otbl_set_field": ([P, I, D], I),
         "otbl_get_field": ([P, I, D], I),
         "otbl_field_device_ptr": ([P, I, ctypes.POINTER(D)], I),
@@ -86,6 +89,15 @@ def _bind(L):
         "otbl_boun": ([P], I),
         "otbl_genflu": ([P], I),
         "otbl_launch_count": ([P], ctypes.c_longlong),
+        "otbl_graph_create": ([ctypes.POINTER(P), I, I, ctypes.POINTER(P)], I),
+        "otbl_graph_launch": ([P], I),
+        "otbl_graph_sync": ([P], I),
+        "otbl_graph_query": ([P], I),
+        "otbl_graph_stream": ([P, ctypes.POINTER(P)], I),
+        "otbl_graph_kernels": ([P], ctypes.c_longlong),
+        "otbl_graph_destroy": ([P], None),
+        "otbl_query": ([P], I),
+        "otbl_autotune": ([P, ctypes.POINTER(ctypes.c_int)], I),
         "otbl_get_stream": ([P, ctypes.POINTER(P)], I),
         "otbl_profile_enable": ([P, I], I),
         "otbl_profile_read": ([P, I, ctypes.POINTER(ctypes.c_char_p), D, ctypes.POINTER(I)], I),

@@ -254,3 +254,15 @@ def make_initial(cfg: BoxConfig) -> dict:
         u0=uu[0, :, 0].copy(), v0=vv[0, :, 0].copy(),
         um=uu[xout - 1, :, 0].copy(),
     )
+
+
+def inlet_state(cfg: BoxConfig, base: dict) -> dict:
+    """The fields of `base` (a state of the same grid size) as the initial
+    state of box `cfg`: the fields and inlet profiles are shared, the
+    Reynolds number, the recycling plane and its mean profile um are the
+    box's own (a restart of a related run, as a serving client uploads it)."""
+    y = y_grid(cfg)
+    xout = cfg.resolved_xout()
+    d = dict(base)
+    d.update(y=y, re=reynolds_for(cfg, y), xout=xout, um=base["u"][xout - 1, :, 0].copy())
+    return d
