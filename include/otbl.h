@@ -223,6 +223,9 @@ int otbl_query(otbl_ctx *ctx);
  * does not depend on the CTA size. choice (3 ints, may be NULL) receives the
  * sizes picked. Call before otbl_graph_create. Synchronizes. */
 int otbl_autotune(otbl_ctx *ctx, int *choice);
+/* sets the three CTA sizes (each 32, 64 or 128) without timing, e.g. those
+ * otbl_autotune picked for another context of the same box size */
+int otbl_set_tuning(otbl_ctx *ctx, const int *bs);
 
 /* ---- instrumentation (no counterpart in the reference, whose timers are
  *      the MPI_WTIME accumulators of module temporal, mod.F90:311-322) ---- */

@@ -172,6 +172,10 @@ class Box:
         self._check(self.L.otbl_autotune(self.h, ch), "otbl_autotune")
         return tuple(ch)
 
+    def set_tuning(self, bs):
+        ch = (ctypes.c_int * 3)(*bs)
+        self._check(self.L.otbl_set_tuning(self.h, ch), "otbl_set_tuning")
+
     def busy(self) -> bool:
         """True while work issued on the context is in flight (never blocks)."""
         st = self.L.otbl_query(self.h)

@@ -209,3 +209,11 @@ extern "C" int otbl_autotune(otbl_ctx *c, int *choice) {
     for (int k = 0; k < 3; ++k) choice[k] = c->tune_bs[k];
   return OTBL_OK;
 }
+
+extern "C" int otbl_set_tuning(otbl_ctx *c, const int *bs) {
+  if (!c || !bs) return OTBL_ERR_ARG;
+  for (int k = 0; k < 3; ++k)
+    if (bs[k] != 32 && bs[k] != 64 && bs[k] != 128) return OTBL_ERR_ARG;
+  for (int k = 0; k < 3; ++k) c->tune_bs[k] = bs[k];
+  return OTBL_OK;
+}

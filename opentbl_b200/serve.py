@@ -146,8 +146,10 @@ class Server:
         self.L = native.lib()
         self.idle = {}
         self.used = 0
+        self.tuning = {}  # CTA sizes picked by the autotuner, per grid size
         self.stats = {"created": 0, "reused": 0, "evicted": 0, "graph_launches": 0,
-                      "direct_steps": 0, "peak_bytes": 0, "peak_active": 0}
+                      "direct_steps": 0, "peak_bytes": 0, "peak_active": 0,
+                      "create_s": 0.0, "rebind_s": 0.0, "capture_s": 0.0}
 
     # ---- slots ----
     def _bytes(self, cfg, init) -> int:
@@ -168,18 +170,25 @@ class Server:
         key = size_key(req.cfg)
         lst = self.idle.get(key)
         if lst:
+            t = time.perf_counter()
             s = lst.pop()
             s.box.rebind(req.cfg, init)
             self.stats["reused"] += 1
+            self.stats["rebind_s"] += time.perf_counter() - t
             return s
         need = self._bytes(req.cfg, init)
         while self.used + need > self.budget and self._evict_one():
             pass
         if self.used + need > self.budget:
             return None
+        t = time.perf_counter()
         box = Box(req.cfg, init, device=self.device)
         if self.autotune:
-            box.autotune()
+            if key in self.tuning:
+                box.set_tuning(self.tuning[key])
+            else:
+                self.tuning[key] = box.autotune()
+        self.stats["create_s"] += time.perf_counter() - t
         s = _Slot(box, need)
         self.used += need
         self.stats["created"] += 1
@@ -242,7 +251,9 @@ class Server:
                 s.req = req
                 s.remaining = req.steps
                 s.chunk = min(self.chunk, req.steps)
+                t = time.perf_counter()
                 s.graph = Graph([s.box], s.chunk) if req.steps >= s.chunk else None
+                self.stats["capture_s"] += time.perf_counter() - t
                 s.admitted = time.perf_counter() - t0
                 active.append(s)
                 self._issue(s)

@@ -132,6 +132,8 @@ void orc_set_inflow(orc_box *b, const double *u0, const double *v0,
   b->gamma1 = st->gamma1;
   b->gamma2 = st->gamma2;
   b->timec = st->timec;
+  b->dt_frozen = 0; /* a restart, as otbl_set_inflow */
+  memset(b->ener, 0, sizeof b->ener);
 }
 
 void orc_get_inflow(orc_box *b, double *um, otbl_inflow *st) {

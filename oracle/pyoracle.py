@@ -118,6 +118,8 @@ class OracleBox:
             self.set_field(n, init[n])
         st = OtblInflow()
         st.dt = init.get("dt", 0.0)
+        st.tiempo = init.get("tiempo", 0.0)
+        st.timeinit = init.get("timeinit", 0.0)
         self.L.orc_set_inflow(self.h, dptr(np.ascontiguousarray(init["u0"])),
                               dptr(np.ascontiguousarray(init["v0"])),
                               dptr(np.ascontiguousarray(init["um"])), ctypes.byref(st))
