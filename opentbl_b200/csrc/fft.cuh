@@ -243,4 +243,61 @@ __device__ __forceinline__ void block_fft(V *buf, int n, const V *__restrict__ t
   while (rem % 5 == 0) { block_pass<5, SIGN, NB>(buf, n, Ns, tw); Ns *= 5; rem /= 5; }
 }
 
+// Padded shared-memory index for the line FFTs below: one double2 of padding
+// every 8, which turns the radix-8, Ns = 1 write stride of 8 elements (128
+// bytes, a 32-way bank conflict) into 9.
+__device__ __forceinline__ int xpad(int i) { return i + (i >> 3); }
+
+// Stockham pass as stockham_pass, on a padded line, by the G threads (rank t)
+// that own this line; every thread of the CTA runs the same passes on its own
+// line, so the barriers are CTA-wide.
+template <int R, int SIGN, int MAXIT, typename V>
+__device__ __forceinline__ void stockham_pass_pad(V *buf, int M, int Ns, const V *__restrict__ tw, int t, int G) {
+  const int nit = M / R;
+  const int stride_tw = M / (Ns * R);
+  V v[MAXIT][R];
+#pragma unroll
+  for (int it = 0; it < MAXIT; ++it) {
+    const int j = t + it * G;
+    if (j < nit) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[it][r] = buf[xpad(j + r * nit)];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int it = 0; it < MAXIT; ++it) {
+    const int j = t + it * G;
+    if (j < nit) {
+      const int k = j % Ns;
+      if (Ns > 1) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          V w = __ldg(&tw[r * k * stride_tw]);
+          if (SIGN > 0) w.y = -w.y;
+          v[it][r] = cmul(v[it][r], w);
+        }
+      }
+      dft_small<R, SIGN>(v[it]);
+      const int base = (j / Ns) * Ns * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) buf[xpad(base + r * Ns)] = v[it][r];
+    }
+  }
+  __syncthreads();
+}
+
+// FFT of length n = 2^a 3^b 5^c of this thread's padded line (n * lines per
+// CTA <= 4096), the radix order of block_fft (8s, 4s, 2s, 3s, 5s), so the
+// arithmetic is block_fft's operation for operation.
+template <int SIGN, typename V>
+__device__ __forceinline__ void block_fft_lines(V *buf, int n, const V *__restrict__ tw, int t, int G) {
+  int Ns = 1, rem = n;
+  while (rem % 8 == 0) { stockham_pass_pad<8, SIGN, 2>(buf, n, Ns, tw, t, G); Ns *= 8; rem /= 8; }
+  while (rem % 4 == 0) { stockham_pass_pad<4, SIGN, 4>(buf, n, Ns, tw, t, G); Ns *= 4; rem /= 4; }
+  while (rem % 2 == 0) { stockham_pass_pad<2, SIGN, 8>(buf, n, Ns, tw, t, G); Ns *= 2; rem /= 2; }
+  while (rem % 3 == 0) { stockham_pass_pad<3, SIGN, 6>(buf, n, Ns, tw, t, G); Ns *= 3; rem /= 3; }
+  while (rem % 5 == 0) { stockham_pass_pad<5, SIGN, 4>(buf, n, Ns, tw, t, G); Ns *= 5; rem /= 5; }
+}
+
 }  // namespace otbl

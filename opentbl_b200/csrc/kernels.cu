@@ -916,20 +916,28 @@ struct XTab {
   int n;
 };
 
-// divergence (pois.f90:41-54) + DCT-II along x (cosftx iopt=-1) for two
-// spanwise modes (k0, k0+1) of one row j; output phi-hat in plane layout
-// (v-type, plane i = mode index + 2). Mode 0 made real (pois.f90:102).
+// The x-line transforms of pois: MB spanwise modes of one row j per CTA of
+// 256 threads. The loads and stores walk the planes with the MB modes of a
+// plane on consecutive threads (MB x 16 contiguous bytes per plane row); the
+// MB complex lines of length n = nx-1 sit in padded shared memory (line
+// stride xpad(n)) and are transformed together, 256/MB threads per line.
+// MB is chosen per n so that n * MB <= 4096 (n = 1024: 4 modes, 74 KB).
+
+// divergence (pois.f90:41-54) + DCT-II along x (cosftx iopt=-1); output
+// phi-hat in plane layout (v-type, plane i = x-mode index + 2). Mode 0 made
+// real (pois.f90:102).
+template <int MB>
 __global__ void __launch_bounds__(256) k_pois_fwd(DCoef c, XTab x, const double *__restrict__ u,
                                                  const double *__restrict__ v, const double *__restrict__ w,
                                                  double *__restrict__ phi) {
   extern __shared__ double2 xsm[];
-  const int n = x.n, ny = c.ny, nz1 = c.nz1, nz2 = c.nz2, xr = c.xround;
+  const int n = x.n, ld = xpad(n), ny = c.ny, nz1 = c.nz1, nz2 = c.nz2, xr = c.xround;
   const int j = blockIdx.y + 1;
-  const int k0 = blockIdx.x * 2;
+  const int k0 = blockIdx.x * MB;
   const size_t PU = (size_t)(ny + 1) * nz1, PV = (size_t)ny * nz1;
   const double idx = c.S[OTBL_S_IDX], idy = c.idy[j];
-  for (int e = threadIdx.x; e < 2 * n; e += 256) {
-    const int l = e / n, tt = e % n;
+  for (int e = threadIdx.x; e < n * MB; e += 256) {
+    const int l = e % MB, tt = e / MB;
     const int k = k0 + l;
     double2 val = make_double2(0.0, 0.0);
     if (k <= nz2) {
@@ -947,63 +955,69 @@ __global__ void __launch_bounds__(256) k_pois_fwd(DCoef c, XTab x, const double 
       val = make_double2(rnd(re, xr), rnd(im, xr));
     }
     const int dst = (tt & 1) ? n - 1 - (tt >> 1) : (tt >> 1);
-    xsm[l * n + dst] = val;
+    xsm[l * ld + xpad(dst)] = val;
   }
   __syncthreads();
-  block_fft<-1, 2>(xsm, n, x.tw);
+  {
+    const int G = 256 / MB, l = threadIdx.x / G;
+    block_fft_lines<-1>(xsm + l * ld, n, x.tw, threadIdx.x % G, G);
+  }
   const double dnf = 1.0 / (double)n;
-  for (int e = threadIdx.x; e < 2 * n; e += 256) {
-    const int l = e / n, kk = e % n;
+  for (int e = threadIdx.x; e < n * MB; e += 256) {
+    const int l = e % MB, kk = e / MB;
     const int k = k0 + l;
     if (k > nz2) continue;
-    const double2 V = xsm[l * n + kk], Vm = xsm[l * n + (kk == 0 ? 0 : n - kk)];
+    const double2 V = xsm[l * ld + xpad(kk)], Vm = xsm[l * ld + xpad(kk == 0 ? 0 : n - kk)];
     const double2 wq = __ldg(x.tw2 + kk);
     const double2 y = cadd(cmul(wq, V), cmul(cconj(wq), Vm));
     double re = rnd(dnf * y.x, xr), im = rnd(dnf * y.y, xr);
     if (k == 0) im = 0.0;
-    double *o = phi + (size_t)(kk + 1) * PV + (size_t)(j - 1) * nz1 + 2 * k;
-    o[0] = re;
-    o[1] = im;
+    *reinterpret_cast<double2 *>(phi + (size_t)(kk + 1) * PV + (size_t)(j - 1) * nz1 + 2 * k) =
+        make_double2(re, im);
   }
 }
 
-// DCT-III along x (cosftx iopt=+1) for two modes of one row j, in place
+// DCT-III along x (cosftx iopt=+1), in place on phi-hat
+template <int MB>
 __global__ void __launch_bounds__(256) k_pois_bwd(DCoef c, XTab x, double *__restrict__ phi) {
   extern __shared__ double2 xsm[];
-  const int n = x.n, ny = c.ny, nz1 = c.nz1, nz2 = c.nz2, xr = c.xround;
+  const int n = x.n, ld = xpad(n), ny = c.ny, nz1 = c.nz1, nz2 = c.nz2, xr = c.xround;
   const int j = blockIdx.y + 1;
-  const int k0 = blockIdx.x * 2;
+  const int k0 = blockIdx.x * MB;
   const size_t PV = (size_t)ny * nz1;
-  for (int e = threadIdx.x; e < 2 * n; e += 256) {
-    const int l = e / n, kk = e % n;
+  for (int e = threadIdx.x; e < n * MB; e += 256) {
+    const int l = e % MB, kk = e / MB;
     const int k = k0 + l;
     double2 val = make_double2(0.0, 0.0);
     if (k <= nz2) {
-      const double *q = phi + (size_t)(kk + 1) * PV + (size_t)(j - 1) * nz1 + 2 * k;
-      const double2 Y = make_double2(rnd(q[0], xr), rnd(q[1], xr));
+      const double2 q = *reinterpret_cast<const double2 *>(phi + (size_t)(kk + 1) * PV + (size_t)(j - 1) * nz1 + 2 * k);
+      const double2 Y = make_double2(rnd(q.x, xr), rnd(q.y, xr));
       double2 Ym = make_double2(0.0, 0.0);
       if (kk > 0) {
-        const double *qm = phi + (size_t)(n - kk + 1) * PV + (size_t)(j - 1) * nz1 + 2 * k;
-        Ym = make_double2(rnd(qm[0], xr), rnd(qm[1], xr));
+        const double2 qm =
+            *reinterpret_cast<const double2 *>(phi + (size_t)(n - kk + 1) * PV + (size_t)(j - 1) * nz1 + 2 * k);
+        Ym = make_double2(rnd(qm.x, xr), rnd(qm.y, xr));
       }
       const double2 d = make_double2(Y.x + Ym.y, Y.y - Ym.x);  // Y - i Ym
       val = cmul(cconj(__ldg(x.tw2 + kk)), d);
     }
-    xsm[l * n + kk] = val;
+    xsm[l * ld + xpad(kk)] = val;
   }
   __syncthreads();
-  block_fft<1, 2>(xsm, n, x.tw);
-  for (int e = threadIdx.x; e < 2 * n; e += 256) {
-    const int l = e / n, tt = e % n;
+  {
+    const int G = 256 / MB, l = threadIdx.x / G;
+    block_fft_lines<1>(xsm + l * ld, n, x.tw, threadIdx.x % G, G);
+  }
+  for (int e = threadIdx.x; e < n * MB; e += 256) {
+    const int l = e % MB, tt = e / MB;
     const int k = k0 + l;
     if (k > nz2) continue;
-    const double2 V = xsm[l * n + ((tt & 1) ? n - 1 - (tt >> 1) : (tt >> 1))];
-    double *o = phi + (size_t)(tt + 1) * PV + (size_t)(j - 1) * nz1 + 2 * k;
-    o[0] = rnd(0.5 * V.x, xr);
+    const double2 V = xsm[l * ld + xpad((tt & 1) ? n - 1 - (tt >> 1) : (tt >> 1))];
     // mode 0 is real (pois.f90:102): its imaginary pencil is identically zero
     // in the reference's real transforms, while the complex line transform
     // used here leaves rounding-level values there
-    o[1] = k == 0 ? 0.0 : rnd(0.5 * V.y, xr);
+    *reinterpret_cast<double2 *>(phi + (size_t)(tt + 1) * PV + (size_t)(j - 1) * nz1 + 2 * k) =
+        make_double2(rnd(0.5 * V.x, xr), k == 0 ? 0.0 : rnd(0.5 * V.y, xr));
   }
 }
 
@@ -1136,6 +1150,8 @@ __global__ void k_twiddles(double2 *tw, int n, double2 *tw2, int n2, int mode2) 
     tw2[t] = make_double2(co, s);
   }
 }
+
+static inline int xpad_host(int i) { return i + (i >> 3); }
 
 // FP32 copy of an FP64 table (mixed path)
 __global__ void k_round_f32(const double *in, float *out, int n) {
@@ -1382,18 +1398,40 @@ cudaError_t launch_pois(otbl_ctx *c, int m) {
   (void)m;  // varstep for substep m was set by k_dt
   const int nz2 = c->dc.nz2, ny = c->cfg.ny, nx = c->cfg.nx, nz1 = c->dc.nz1;
   const int n = nx - 1;
-  const size_t smem = (size_t)2 * n * sizeof(double2);
-  cudaFuncSetAttribute(k_pois_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  cudaFuncSetAttribute(k_pois_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  // modes per CTA: n * MB <= 4096 and at most 8
+  const int MB = n <= 512 ? 8 : (n <= 1024 ? 4 : (n <= 2048 ? 2 : 1));
+  const size_t smem = (size_t)MB * xpad_host(n) * sizeof(double2);
   double *phi = c->w.s2;
-  dim3 gx((nz2 + 1 + 1) / 2, ny - 1);
+  dim3 gx((nz2 + 1 + MB - 1) / MB, ny - 1);
+  auto fwd = [&](auto kf) {
+    cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    kf<<<gx, 256, smem, c->stream>>>(c->dc, xtab(c), c->f[OTBL_F_U], c->f[OTBL_F_V], c->f[OTBL_F_W], phi);
+  };
+  auto bwd = [&](auto kb) {
+    cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    kb<<<gx, 256, smem, c->stream>>>(c->dc, xtab(c), phi);
+  };
   prof_begin(c, PK_POIS_FWD);
-  k_pois_fwd<<<gx, 256, smem, c->stream>>>(c->dc, xtab(c), c->f[OTBL_F_U], c->f[OTBL_F_V], c->f[OTBL_F_W], phi);
+  if (MB == 8)
+    fwd(k_pois_fwd<8>);
+  else if (MB == 4)
+    fwd(k_pois_fwd<4>);
+  else if (MB == 2)
+    fwd(k_pois_fwd<2>);
+  else
+    fwd(k_pois_fwd<1>);
   prof_end(c);
   cudaError_t e = launch_pois_solve(c, phi);
   if (e != cudaSuccess) return e;
   prof_begin(c, PK_POIS_BWD);
-  k_pois_bwd<<<gx, 256, smem, c->stream>>>(c->dc, xtab(c), phi);
+  if (MB == 8)
+    bwd(k_pois_bwd<8>);
+  else if (MB == 4)
+    bwd(k_pois_bwd<4>);
+  else if (MB == 2)
+    bwd(k_pois_bwd<2>);
+  else
+    bwd(k_pois_bwd<1>);
   prof_end(c);
   dim3 gp((nz1 + 127) / 128, ny, nx - 1);
   prof_begin(c, PK_PROJECT);
