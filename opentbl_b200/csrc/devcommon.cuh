@@ -32,4 +32,12 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
 }
 
+// a[f] of a kernel-parameter array with f uniform across the grid's y index,
+// selected without indexing the parameter block (which would copy it to
+// local memory)
+template <typename P>
+__device__ __forceinline__ P pick3(const P (&a)[3], int f) {
+  return f == 0 ? a[0] : (f == 1 ? a[1] : a[2]);
+}
+
 }  // namespace otbl

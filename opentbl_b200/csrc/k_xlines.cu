@@ -32,18 +32,34 @@ struct XStream {
   int which[3], np[3];
 };
 
-constexpr int KXI = 16;  // interpxx segment
-constexpr int KXD = 16;  // difvisxx segment (two recurrences)
+// Segment lengths and occupancy per arithmetic type, measured on B200 at
+// 1025x193x512 over segments of 8-32 rows and 4-8 CTAs of 128 threads per
+// SM: interpxx 16 rows (FP64) / 8 rows (FP32) at >= 8 CTAs per SM; difvisxx
+// 8 rows at >= 6 CTAs per SM (3.16 ms per substep in FP64 against 3.46 for
+// 16 rows at 4 CTAs; 1.78 against 2.50 in FP32). FP32 interpxx runs
+// unbounded (56 registers).
+template <typename T>
+struct XTune;
+template <>
+struct XTune<double> {
+  static constexpr int kxi = 16, kxd = 8, minb_i = 8;
+};
+template <>
+struct XTune<float> {
+  static constexpr int kxi = 8, kxd = 8, minb_i = 1;  // 0.88 ms unbounded, 1.19 at >= 8 CTAs
+};
+
 
 template <typename T>
-__global__ void __launch_bounds__(128) k_interpx(DCoefT<T> c, XStream a) {
-  const int f = blockIdx.y, np = a.np[f];
+__global__ void __launch_bounds__(128, XTune<T>::minb_i) k_interpx(DCoefT<T> c, XStream a) {
+  constexpr int KXI = XTune<T>::kxi;
+  const int f = blockIdx.y, np = pick3(a.np, f);
   const int mp = blockIdx.x * blockDim.x + threadIdx.x;
   if (mp >= np) return;
-  const int nx = c.nx, xr = c.xround, which = a.which[f];
-  const double *in = static_cast<const double *>(a.in[f]) + mp;
-  T *out = static_cast<T *>(a.out[f]) + mp;
-  T *ck = reinterpret_cast<T *>(a.ck[f]) + mp;
+  const int nx = c.nx, xr = c.xround, which = pick3(a.which, f);
+  const double *in = static_cast<const double *>(pick3(a.in, f)) + mp;
+  T *out = static_cast<T *>(pick3(a.out, f)) + mp;
+  T *ck = reinterpret_cast<T *>(pick3(a.ck, f)) + mp;
   const T *icon = which == 0 ? c.inxu : c.inxv;
   const T *econ = which == 0 ? c.cofiux : c.cofivx;
   const int chi = which == 0 ? 2 : 1, chi2 = which == 0 ? 3 : 4;
@@ -95,15 +111,16 @@ __global__ void __launch_bounds__(128) k_interpx(DCoefT<T> c, XStream a) {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(128) k_difvisx(DCoefT<T> c, XStream a) {
-  const int f = blockIdx.y, np = a.np[f];
+__global__ void __launch_bounds__(128, 6) k_difvisx(DCoefT<T> c, XStream a) {
+  constexpr int KXD = XTune<T>::kxd;
+  const int f = blockIdx.y, np = pick3(a.np, f);
   const int mp = blockIdx.x * blockDim.x + threadIdx.x;
   if (mp >= np) return;
-  const int nx = c.nx, xr = c.xround, which = a.which[f];
-  const T *gin = static_cast<const T *>(a.in[f]) + mp;
-  const double *uin = a.in2[f] + mp;
-  T *out = static_cast<T *>(a.out[f]) + mp;
-  T *ck = reinterpret_cast<T *>(a.ck[f]) + mp;
+  const int nx = c.nx, xr = c.xround, which = pick3(a.which, f);
+  const T *gin = static_cast<const T *>(pick3(a.in, f)) + mp;
+  const double *uin = pick3(a.in2, f) + mp;
+  T *out = static_cast<T *>(pick3(a.out, f)) + mp;
+  T *ck = reinterpret_cast<T *>(pick3(a.ck, f)) + mp;
   const T *icon = which == 0 ? c.dcxu : c.dcxv;
   const T *iconv = which == 0 ? c.vixu : c.vixv;
   const T *econ = which == 0 ? c.cofcxu : c.cofcxv;

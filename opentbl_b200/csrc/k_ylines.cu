@@ -48,12 +48,12 @@ __global__ void __launch_bounds__(128) k_interpy(DCoefT<T> c, InterpyArgs a) {
   const int ny = c.ny, nz1 = c.nz1, ncol = c.nx * nz1;
   const int col = blockIdx.x * blockDim.x + threadIdx.x;
   if (col >= ncol) return;
-  const int which = a.which[f], jin = which == 0 ? ny + 1 : ny;
+  const int which = pick3(a.which, f), jin = which == 0 ? ny + 1 : ny;
   const int i = col / nz1 + 1, kr = col - (i - 1) * nz1;
   const size_t S = nz1;
-  const double *g = a.in[f] + (size_t)(i - 1) * jin * nz1 + kr;
-  T *o = static_cast<T *>(a.out[f]) + (size_t)(i - 1) * ny * nz1 + kr;
-  T *ck = reinterpret_cast<T *>(a.ck[f]) + col;
+  const double *g = pick3(a.in, f) + (size_t)(i - 1) * jin * nz1 + kr;
+  T *o = static_cast<T *>(pick3(a.out, f)) + (size_t)(i - 1) * ny * nz1 + kr;
+  T *ck = reinterpret_cast<T *>(pick3(a.ck, f)) + col;
   const T *iny = which == 0 ? c.inyu : c.inyv;
   const T *econ = which == 0 ? c.cofiuy : c.cofivy;
   const T *ib = c.inby;
