@@ -16,20 +16,28 @@
 namespace otbl {
 
 constexpr int KY = 8;  // rows per checkpointed segment
-// Segment length and occupancy of the rhsp tail (k_final_s1/s2), per
+// Segment length and occupancy of the rhsp tail (k_final_s1), per
 // element type of its FP32-capable inputs; measured on B200 at
 // 1025x193x512 over KF in {4, 6, 8} x CTAs/SM in {3..6}: FP64 4 rows at 4
 // CTAs of 128 threads per SM (7.2 ms per substep, 7.8 at 8 rows), mixed 6
 // rows at 5 CTAs (7.0 ms, 8.4 at 8 rows at 4).
 template <typename W>
 struct FinalTune;
+#ifndef OTBL_FT_DK
+#define OTBL_FT_DK 4
+#define OTBL_FT_DM 4
+#endif
+#ifndef OTBL_FT_FK
+#define OTBL_FT_FK 6
+#define OTBL_FT_FM 5
+#endif
 template <>
 struct FinalTune<double> {
-  static constexpr int kf = 4, minb = 4;
+  static constexpr int kf = OTBL_FT_DK, minb = OTBL_FT_DM;
 };
 template <>
 struct FinalTune<float> {
-  static constexpr int kf = 6, minb = 5;
+  static constexpr int kf = OTBL_FT_FK, minb = OTBL_FT_FM;
 };
 
 // interpyy, which 0: u, w (in rows ny+1), which 1: v (in rows ny); out rows
@@ -138,19 +146,22 @@ struct FinalArgs {
 //     KF rows (FinalTune).
 //   k_final_s1, pass B (segments descending): both forward sweeps recomputed
 //     from the checkpoints into registers, both back-substitutions, the RHS
-//     assembly, the RK3 combination, the new RHS history, and the
-//     right-hand side of implzy (rows q..q+2 of the combination), written to
-//     scratch together with the boundary values ub1, ubt.
-//   k_final_s2: implzy (the same two passes) and the new velocity.
-// The sweeps are the serial Thomas of lip.f90 in the reference's order.
+//     assembly, the RK3 combination, the new RHS history, the right-hand
+//     side of implzy (rows q..q+2 of the combination) and, in the same
+//     descending order, its elimination with the top-down factors of k_dt
+//     (implzy_factor), written to scratch.
+//   k_final_s2 (rows ascending): implzy's substitution and the new
+//     velocity, with the boundary values ub1, ubt; a light kernel, so that
+//     this serial sweep runs at high occupancy.
+// differzy and vistyy are the serial Thomas sweeps of lip.f90 in the
+// reference's order; implzy is eliminated from the top row down.
 // ---------------------------------------------------------------------------
 template <typename W>
 struct FinalStream {
   FinalArgs<W> a;
   double *ck;   // checkpoints: [2*seg + op][column]
-  double *bq;   // implzy right-hand side: [q][column], q < jee-2
+  double *yq;   // implzy right-hand side after the descending elimination: [q][column]
   double *ub;   // ub1, ubt: [2][column]
-  double *ck2;  // implzy checkpoints: [seg][column]
 };
 
 template <int COMP, typename W>
@@ -171,7 +182,7 @@ __global__ void __launch_bounds__(128, FinalTune<W>::minb) k_final_s1(DCoef c, F
   const size_t S = nz1;  // row stride
   const W *prod = (COMP == 0 ? a.uv : (COMP == 1 ? a.vv : a.vw)) + plv + kr;
   const W *kp = (COMP == 0 ? a.uw : (COMP == 1 ? a.vw : a.ww)) + (COMP == 0 ? pl : plv) + kr + pof;
-  const double *vel = (COMP == 0 ? a.u : (COMP == 1 ? a.v : a.w)) + pl + kr;
+  double *vel = (COMP == 0 ? a.u : (COMP == 1 ? a.v : a.w)) + pl + kr;
   const W *cX = (COMP == 0 ? a.cu : (COMP == 1 ? a.cv : a.cw)) + pl + kr;
   double *hp = (COMP == 0 ? a.rhsupa : (COMP == 1 ? a.rhsvpa : a.rhswpa)) + pl + kr;
   const double *pc = a.p + plv + kr;
@@ -220,8 +231,6 @@ __global__ void __launch_bounds__(128, FinalTune<W>::minb) k_final_s1(DCoef c, F
     ub1 = -1.0 / M4(ib, 2, 1) * (M4(ib, 2, 2) * s2 + M4(ib, 2, 3) * s3 + M4(ib, 2, 4) * s4);
     ubt = -1.0 / M2(cc, 1, 1) * (M2(cc, 1, 2) * sn + M2(cc, 1, 3) * sn1 + M2(cc, 1, 4) * sn2);
   }
-  fs.ub[col] = ub1;
-  fs.ub[(size_t)ncol + col] = ubt;
   // right-hand sides of row r from rows r-1, r, r+1 of the product (g) and
   // the old velocity (u)
   auto rd = [&](int r, double gm, double g0, double gp) {
@@ -261,7 +270,8 @@ __global__ void __launch_bounds__(128, FinalTune<W>::minb) k_final_s1(DCoef c, F
   double xd = 0.0, xv = 0.0;
   double R1 = 0.0, R2 = 0.0, R3 = 0.0;       // RHS rows 1..3 (wall row of u,w)
   double res1 = 0.0, res2 = 0.0;             // combination of rows r+1, r+2
-  double *bq = fs.bq + col;
+  double *yq = fs.yq + col;
+  double yel = 0.0;  // implzy right-hand side of row q+1 after elimination
   for (int sg = nseg - 1; sg >= 0; --sg) {
     const int s0 = sg * KF;
     double gv[KF + 2], uv[KF + 2], ydv[KF], yvv[KF];
@@ -336,18 +346,24 @@ __global__ void __launch_bounds__(128, FinalTune<W>::minb) k_final_s1(DCoef c, F
                    __ldg(vyi + 3 * (r + 1) + 2) * res2;
         if (r == 0) v = v - a1raw * ub1;
         if (r == n - 1) v = v - a3raw * ubt;
-        bq[(size_t)r * ncol] = v;
+        yel = v + fac[3 * (r + 2) + 2] * yel;
+        yq[(size_t)r * ncol] = yel;
       }
       res2 = res1;
       res1 = res;
     }
   }
+  fs.ub[col] = ub1;
+  fs.ub[(size_t)ncol + col] = ubt;
 }
 
-template <int COMP, typename W>
-__global__ void __launch_bounds__(128) k_final_s2(DCoef c, FinalStream<W> fs) {
-  constexpr int KF = FinalTune<W>::kf;
-  const FinalArgs<W> &a = fs.a;
+// implzy substitution x_q = (y_q - A_q x_{q-1}) / B'_q on the eliminated
+// right-hand side of k_final_s1 (rows q = 0..n-1 are velocity rows q+1),
+// then the boundary rows ub1, ubt
+template <int COMP>
+__global__ void __launch_bounds__(128) k_final_s2(DCoef c, double *u, double *v, double *w, const double *fac_u,
+                                                  const double *fac_v, const double *__restrict__ yqb,
+                                                  const double *__restrict__ ub) {
   const int nx = c.nx, ny = c.ny, nz1 = c.nz1;
   const int ncol = (nx - 1) * nz1;
   const int col = blockIdx.x * blockDim.x + threadIdx.x;
@@ -355,49 +371,26 @@ __global__ void __launch_bounds__(128) k_final_s2(DCoef c, FinalStream<W> fs) {
   const int i = col / nz1 + 2, kr = col - (i - 2) * nz1;
   const int jee = COMP == 1 ? ny : ny + 1, n = jee - 2;
   const size_t PU = (size_t)(ny + 1) * nz1, PV = (size_t)ny * nz1;
-  const size_t pl = (size_t)(i - 1) * (COMP == 1 ? PV : PU);
-  double *vel = (COMP == 0 ? a.u : (COMP == 1 ? a.v : a.w)) + pl + kr;
-  const double *fac = COMP == 1 ? a.fac_v : a.fac_u;  // row q uses fac[3(q+2)..]
-  const double *bq = fs.bq + col;
-  double *ck = fs.ck2 + col;
-  const int nseg = (n + KF - 1) / KF;
-  double y = 0.0;
-  for (int sg = 0; sg < nseg; ++sg) {
-    const int s0 = sg * KF;
-    ck[(size_t)sg * ncol] = y;
-    double bv[KF];
-#pragma unroll
-    for (int b = 0; b < KF; ++b) bv[b] = bq[(size_t)min(s0 + b, n - 1) * ncol];
-#pragma unroll
-    for (int b = 0; b < KF; ++b) {
-      const int q = s0 + b;
-      if (q < n) y = bv[b] + (q > 0 ? __ldg(fac + 3 * (q + 2)) : 0.0) * y;
-    }
-  }
+  double *vel = (COMP == 0 ? u : (COMP == 1 ? v : w)) + (size_t)(i - 1) * (COMP == 1 ? PV : PU) + kr;
+  const double *fac = COMP == 1 ? fac_v : fac_u;
+  const double *yq = yqb + col;
+  constexpr int K = 8;
   double x = 0.0;
-  for (int sg = nseg - 1; sg >= 0; --sg) {
-    const int s0 = sg * KF;
-    double bv[KF], yv[KF];
+  for (int q0 = 0; q0 < n; q0 += K) {
+    double yv[K];
 #pragma unroll
-    for (int b = 0; b < KF; ++b) bv[b] = bq[(size_t)min(s0 + b, n - 1) * ncol];
-    double yy = ck[(size_t)sg * ncol];
+    for (int b = 0; b < K; ++b) yv[b] = yq[(size_t)min(q0 + b, n - 1) * ncol];
 #pragma unroll
-    for (int b = 0; b < KF; ++b) {
-      const int q = s0 + b;
-      if (q < n) yy = bv[b] + (q > 0 ? __ldg(fac + 3 * (q + 2)) : 0.0) * yy;
-      yv[b] = yy;
-    }
-#pragma unroll
-    for (int b = KF - 1; b >= 0; --b) {
-      const int q = s0 + b;
+    for (int b = 0; b < K; ++b) {
+      const int q = q0 + b;
       if (q < n) {
-        x = (yv[b] - __ldg(fac + 3 * (q + 2) + 2) * x) * __ldg(fac + 3 * (q + 2) + 1);
+        x = (yv[b] - __ldg(fac + 3 * (q + 2)) * x) * __ldg(fac + 3 * (q + 2) + 1);
         vel[(size_t)(q + 1) * nz1] = x;
       }
     }
   }
-  vel[0] = fs.ub[col];
-  vel[(size_t)(jee - 1) * nz1] = fs.ub[(size_t)ncol + col];
+  vel[0] = ub[col];
+  vel[(size_t)(jee - 1) * nz1] = ub[(size_t)ncol + col];
 }
 
 // ---------------------------------------------------------------------------
@@ -539,16 +532,16 @@ static void final_t(otbl_ctx *c) {
   a.st = c->st;
   const int ncol = (c->cfg.nx - 1) * c->dc.nz1;
   fs.ck = c->w.s1;
-  fs.bq = c->w.s2;
+  fs.yq = c->w.s2;
   fs.ub = c->w.s3;
-  fs.ck2 = c->w.s3 + 2 * (size_t)ncol;
   const dim3 g((ncol + 127) / 128);
+  double *U = c->f[OTBL_F_U], *V = c->f[OTBL_F_V], *Wv = c->f[OTBL_F_W];
   k_final_s1<1, W><<<g, 128, 0, c->stream>>>(c->dc, fs);
-  k_final_s2<1, W><<<g, 128, 0, c->stream>>>(c->dc, fs);
+  k_final_s2<1><<<g, 128, 0, c->stream>>>(c->dc, U, V, Wv, c->w.fac_u, c->w.fac_v, fs.yq, fs.ub);
   k_final_s1<0, W><<<g, 128, 0, c->stream>>>(c->dc, fs);
-  k_final_s2<0, W><<<g, 128, 0, c->stream>>>(c->dc, fs);
+  k_final_s2<0><<<g, 128, 0, c->stream>>>(c->dc, U, V, Wv, c->w.fac_u, c->w.fac_v, fs.yq, fs.ub);
   k_final_s1<2, W><<<g, 128, 0, c->stream>>>(c->dc, fs);
-  k_final_s2<2, W><<<g, 128, 0, c->stream>>>(c->dc, fs);
+  k_final_s2<2><<<g, 128, 0, c->stream>>>(c->dc, U, V, Wv, c->w.fac_u, c->w.fac_v, fs.yq, fs.ub);
 }
 
 cudaError_t launch_final(otbl_ctx *c) {

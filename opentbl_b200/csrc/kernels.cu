@@ -11,7 +11,7 @@
 //   dt        rhsp.F90:214  k_dt          dt, RK3 factors, implzy LU factors
 //   genflu    genflu.F90:3  k_genflu_tab  integral quantities, rescaling tables
 //                           k_genflu_cols inflow plane + boun of plane 1
-//   rhsp tail rhsp.F90:291-484 k_final    y-lines: pressure gradient, RHS
+//   rhsp tail rhsp.F90:291-484 k_final_s1 y-lines: pressure gradient, RHS
 //                                          assembly (differzy), boun, vistyy,
 //                                          RK3 combination, implzy
 //   outflow_correction boun.f90:63  k_outflow
@@ -415,33 +415,38 @@ __global__ void __launch_bounds__(128) k_products_r(DCoef c, ZTabT<T> z, ProdArg
 // ---------------------------------------------------------------------------
 // dt (rhsp.F90:214-267), RK3 factors, implzy LU (lip.f90:545-568)
 // ---------------------------------------------------------------------------
-// LU of (A + var1*B) for implzy, lip.f90:545-568, rows j = 2..jee-1, as a
-// register recurrence: fac[3j], fac[3j+1], fac[3j+2] = lower, inverse pivot,
-// upper of row j (lower of row 2 and upper of row jee-1 are 0), and the two
-// boundary couplings that implzy moves to the right-hand side,
-// fac[3*(jee+1)] = a(2), fac[3*(jee+1)+1] = c(jee-1).
+// Factors of (A + var1*B) for implzy (lip.f90:545-568, rows j = 2..jee-1),
+// eliminated from the top row down (a UL factorisation; the reference's LU
+// eliminates from the bottom, and both solve the same diagonally dominant
+// system to rounding), so that the rhsp tail, which forms the right-hand
+// side from the top row down, eliminates as it goes. With A_j, B_j, C_j the
+// sub-, main and super-diagonal of row j:
+//   B'_{jee-1} = B_{jee-1},  m_j = C_j / B'_{j+1},  B'_j = B_j - m_j A_{j+1}
+//   fac[3j] = A_j (0 for j = 2), fac[3j+1] = 1/B'_j, fac[3j+2] = -m_j (0 for
+//   j = jee-1); descending y_j = r_j + fac[3j+2] y_{j+1}, ascending
+//   x_j = (y_j - fac[3j] x_{j-1}) fac[3j+1].
+// The two boundary couplings that implzy moves to the right-hand side:
+// fac[3*(jee+1)] = A_2, fac[3*(jee+1)+1] = C_{jee-1}.
 __device__ void implzy_factor(const DCoef &c, double *fac, int which, double var1) {
   const int ny = c.ny, jee = which == 0 ? ny + 1 : ny;
   const double *icon = which == 0 ? c.vyui : c.vyvi;
   const double *econ = which == 0 ? c.cofvyu : c.cofvyv;
-  fac[3 * (jee + 1)] = A3(icon, 1, 2) + var1 * A3(econ, 3, 2);
-  fac[3 * (jee + 1) + 1] = A3(icon, 3, jee - 1) + var1 * A3(econ, 1, jee - 1);
-  double bprev = A3(icon, 2, 2) + var1 * A3(econ, 2, 2);
-  double cprev = jee - 1 == 2 ? 0.0 : A3(icon, 3, 2) + var1 * A3(econ, 1, 2);
-  fac[3 * 2] = 0.0;
-  fac[3 * 2 + 2] = cprev;
-  for (int j = 3; j <= jee - 1; ++j) {
-    const double d = 1.0 / bprev;
-    fac[3 * (j - 1) + 1] = d;
-    const double aj = -(A3(icon, 1, j) + var1 * A3(econ, 3, j)) * d;
-    const double bj = (A3(icon, 2, j) + var1 * A3(econ, 2, j)) + aj * cprev;
-    const double cj = j == jee - 1 ? 0.0 : A3(icon, 3, j) + var1 * A3(econ, 1, j);
-    fac[3 * j] = aj;
-    fac[3 * j + 2] = cj;
-    bprev = bj;
-    cprev = cj;
+  auto Aj = [&](int j) { return A3(icon, 1, j) + var1 * A3(econ, 3, j); };
+  auto Bj = [&](int j) { return A3(icon, 2, j) + var1 * A3(econ, 2, j); };
+  auto Cj = [&](int j) { return A3(icon, 3, j) + var1 * A3(econ, 1, j); };
+  fac[3 * (jee + 1)] = Aj(2);
+  fac[3 * (jee + 1) + 1] = Cj(jee - 1);
+  double bp = Bj(jee - 1);
+  fac[3 * (jee - 1) + 2] = 0.0;
+  for (int j = jee - 1;; --j) {
+    const double ib = 1.0 / bp;
+    fac[3 * j + 1] = ib;
+    fac[3 * j] = j == 2 ? 0.0 : Aj(j);
+    if (j == 2) break;
+    const double m = Cj(j - 1) * ib;  // m_{j-1} = C_{j-1} / B'_j
+    fac[3 * (j - 1) + 2] = -m;
+    bp = Bj(j - 1) - m * Aj(j);
   }
-  fac[3 * (jee - 1) + 1] = 1.0 / bprev;
 }
 
 // One CTA of 64 threads: the CFL reduction over the rows, then dt, the RK3
