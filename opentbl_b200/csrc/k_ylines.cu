@@ -10,6 +10,8 @@
 //   k_final_s1/2 the tail of rhsp (rhsp.F90:291-484)
 //   k_pois_lu    pivots of the (x-mode, kz) y-systems of pois (once)
 //   k_pois_solve their solution every substep (pois.f90:106-117, soltriy)
+#include <type_traits>
+
 #include "devcommon.cuh"
 #include "otbl_internal.cuh"
 
@@ -31,13 +33,17 @@ struct FinalTune;
 #define OTBL_FT_FK 6
 #define OTBL_FT_FM 5
 #endif
+// split: pass A in a kernel of its own (FP32 inputs: 6.69 against 7.09 ms;
+// FP64: 7.18 against 6.84 ms fused)
 template <>
 struct FinalTune<double> {
   static constexpr int kf = OTBL_FT_DK, minb = OTBL_FT_DM;
+  static constexpr bool split = false;
 };
 template <>
 struct FinalTune<float> {
   static constexpr int kf = OTBL_FT_FK, minb = OTBL_FT_FM;
+  static constexpr bool split = true;
 };
 
 // interpyy, which 0: u, w (in rows ny+1), which 1: v (in rows ny); out rows
@@ -141,10 +147,11 @@ struct FinalArgs {
 // consecutive threads on consecutive kr: every row access is a coalesced
 // request, every coefficient a broadcast, and there are far more columns
 // (nx*nz1) than a GPU has threads, so latency is hidden by occupancy.
-//   k_final_s1, pass A (rows ascending): the forward sweeps of differzy (of
-//     the product) and vistyy (of the old velocity), with a checkpoint every
-//     KF rows (FinalTune).
-//   k_final_s1, pass B (segments descending): both forward sweeps recomputed
+//   k_final_s1<.., 1>, pass A (rows ascending): the forward sweeps of
+//     differzy (of the product) and vistyy (of the old velocity), with a
+//     checkpoint every KF rows (FinalTune); a light kernel of its own, at
+//     high occupancy.
+//   k_final_s1<.., 2>, pass B (segments descending): both forward sweeps recomputed
 //     from the checkpoints into registers, both back-substitutions, the RHS
 //     assembly, the RK3 combination, the new RHS history, the right-hand
 //     side of implzy (rows q..q+2 of the combination) and, in the same
@@ -164,8 +171,11 @@ struct FinalStream {
   double *ub;   // ub1, ubt: [2][column]
 };
 
-template <int COMP, typename W>
-__global__ void __launch_bounds__(128, FinalTune<W>::minb) k_final_s1(DCoef c, FinalStream<W> fs) {
+// PASSES: 1 pass A only (k_final_sA, a light kernel at high occupancy),
+// 2 pass B only, 3 both
+template <int COMP, typename W, int PASSES>
+__global__ void __launch_bounds__(128, PASSES == 1 ? 8 : FinalTune<W>::minb)
+    k_final_s1(DCoef c, FinalStream<W> fs) {
   constexpr int KF = FinalTune<W>::kf;
   const FinalArgs<W> &a = fs.a;
   const int nx = c.nx, ny = c.ny, nz1 = c.nz1;
@@ -245,6 +255,7 @@ __global__ void __launch_bounds__(128, FinalTune<W>::minb) k_final_s1(DCoef c, F
   const int nseg = (jee + KF - 1) / KF;
   double *ck = fs.ck + col;
   // ---- pass A: forward sweeps, checkpoints
+  if constexpr ((PASSES & 1) != 0) {
   double yd = 0.0, yv = 0.0;
   for (int sg = 0; sg < nseg; ++sg) {
     const int s0 = sg * KF;
@@ -265,6 +276,8 @@ __global__ void __launch_bounds__(128, FinalTune<W>::minb) k_final_s1(DCoef c, F
       }
     }
   }
+  }
+  if constexpr ((PASSES & 2) == 0) return;
   // ---- pass B: back-substitutions and everything row-local, rows descending
   const double a1raw = fac[3 * (jee + 1)], a3raw = fac[3 * (jee + 1) + 1];
   double xd = 0.0, xv = 0.0;
@@ -509,7 +522,7 @@ cudaError_t launch_interpy(otbl_ctx *c) {
 }
 
 template <typename W>
-static void final_t(otbl_ctx *c) {
+static int final_t(otbl_ctx *c) {
   FinalStream<W> fs;
   FinalArgs<W> &a = fs.a;
   a.u = c->f[OTBL_F_U];
@@ -536,22 +549,27 @@ static void final_t(otbl_ctx *c) {
   fs.ub = c->w.s3;
   const dim3 g((ncol + 127) / 128);
   double *U = c->f[OTBL_F_U], *V = c->f[OTBL_F_V], *Wv = c->f[OTBL_F_W];
-  k_final_s1<1, W><<<g, 128, 0, c->stream>>>(c->dc, fs);
-  k_final_s2<1><<<g, 128, 0, c->stream>>>(c->dc, U, V, Wv, c->w.fac_u, c->w.fac_v, fs.yq, fs.ub);
-  k_final_s1<0, W><<<g, 128, 0, c->stream>>>(c->dc, fs);
-  k_final_s2<0><<<g, 128, 0, c->stream>>>(c->dc, U, V, Wv, c->w.fac_u, c->w.fac_v, fs.yq, fs.ub);
-  k_final_s1<2, W><<<g, 128, 0, c->stream>>>(c->dc, fs);
-  k_final_s2<2><<<g, 128, 0, c->stream>>>(c->dc, U, V, Wv, c->w.fac_u, c->w.fac_v, fs.yq, fs.ub);
+  auto comp = [&](auto C) {
+    constexpr int K = decltype(C)::value;
+    if constexpr (FinalTune<W>::split) {
+      k_final_s1<K, W, 1><<<g, 128, 0, c->stream>>>(c->dc, fs);
+      k_final_s1<K, W, 2><<<g, 128, 0, c->stream>>>(c->dc, fs);
+    } else {
+      k_final_s1<K, W, 3><<<g, 128, 0, c->stream>>>(c->dc, fs);
+    }
+    k_final_s2<K><<<g, 128, 0, c->stream>>>(c->dc, U, V, Wv, c->w.fac_u, c->w.fac_v, fs.yq, fs.ub);
+  };
+  comp(std::integral_constant<int, 1>{});
+  comp(std::integral_constant<int, 0>{});
+  comp(std::integral_constant<int, 2>{});
+  return FinalTune<W>::split ? 9 : 6;
 }
 
 cudaError_t launch_final(otbl_ctx *c) {
   prof_begin(c, PK_FINAL);
-  if (c->mixed)
-    final_t<float>(c);
-  else
-    final_t<double>(c);
+  const int nl = c->mixed ? final_t<float>(c) : final_t<double>(c);
   prof_end(c);
-  c->launches += 6;
+  c->launches += nl;
   return cudaGetLastError();
 }
 

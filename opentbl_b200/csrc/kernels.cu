@@ -289,10 +289,10 @@ __device__ __forceinline__ void zc2r_regs(const ZTabT<T> &z, const TI *__restric
   const int nz2 = z.nz2;
   V a[E], b[E];
 #pragma unroll
-  for (int m = 0; m < E; ++m) {
+  for (int m = 0; m < E; ++m) {  // modes above nz2 are not read (they are 0)
     const int k = t + 32 * m, km = M - k;
-    a[m] = ldcx<T>(fou, min(k, nz2));
-    b[m] = ldcx<T>(fou, min(km, nz2));
+    a[m] = k <= nz2 ? ldcx<T>(fou, k) : cmake<V>(T(0), T(0));
+    b[m] = km <= nz2 ? ldcx<T>(fou, km) : cmake<V>(T(0), T(0));
   }
 #pragma unroll
   for (int m = 0; m < E; ++m) {
@@ -356,8 +356,18 @@ __device__ __forceinline__ double regs_absmax(const V (&a)[E]) {
   return mx;
 }
 
+// CTAs per SM bound: FP64 unbounded (252 registers, 4.49 ms per substep at
+// 1025x193x512; 5.02 at >= 3 CTAs with spills), FP32 >= 3 CTAs (168
+// registers, 2.62 ms; 3.16 unbounded at 185)
+#ifndef OTBL_PR_MB_D
+#define OTBL_PR_MB_D 1
+#endif
+#ifndef OTBL_PR_MB_F
+#define OTBL_PR_MB_F 3
+#endif
 template <int M, typename T>
-__global__ void __launch_bounds__(128) k_products_r(DCoef c, ZTabT<T> z, ProdArgs<T> a) {
+__global__ void __launch_bounds__(128, std::is_same<T, double>::value ? OTBL_PR_MB_D : OTBL_PR_MB_F)
+    k_products_r(DCoef c, ZTabT<T> z, ProdArgs<T> a) {
   using V = V2<T>;
   extern __shared__ __align__(16) unsigned char smraw[];
   V *sm = reinterpret_cast<V *>(smraw);
