@@ -33,6 +33,7 @@ extern "C" {
 #define OTBL_ERR_NAN 5      /* non-finite value detected by the dt reduction  */
 #define OTBL_ERR_NODEV 6    /* no CUDA device / extension not usable          */
 #define OTBL_BUSY 7         /* otbl_query / otbl_graph_query: work in flight  */
+#define OTBL_ERR_TIMEOUT 8  /* a bounded device-side wait gave up             */
 
 /* transposes (change.f90): round the payload to REAL4 as the reference's
  * MPI_ALLTOALLV(MPI_REAL4) does (change.f90:579,608,641,652,676,686), or

@@ -17,7 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libotbl.so")
 SOURCES = ["kernels.cu", "k_xlines.cu", "k_ylines.cu", "otbl_capi.cu", "otbl_graph.cu", "coef.cpp"]
-HEADERS = ["otbl_internal.cuh", "fft.cuh", "devcommon.cuh"]
+HEADERS = ["otbl_internal.cuh", "fft.cuh", "devcommon.cuh", "tma.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

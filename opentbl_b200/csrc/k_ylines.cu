@@ -10,10 +10,13 @@
 //   k_final_s1/2 the tail of rhsp (rhsp.F90:291-484)
 //   k_pois_lu    pivots of the (x-mode, kz) y-systems of pois (once)
 //   k_pois_solve their solution every substep (pois.f90:106-117, soltriy)
+#include <cudaTypedefs.h>
+
 #include <type_traits>
 
 #include "devcommon.cuh"
 #include "otbl_internal.cuh"
+#include "tma.cuh"
 
 namespace otbl {
 
@@ -35,14 +38,20 @@ struct FinalTune;
 #endif
 // split: pass A in a kernel of its own (FP32 inputs: 6.69 against 7.09 ms;
 // FP64: 7.18 against 6.84 ms fused)
+// kf_tma: segment of the TMA-fed pass (k_final_tb) and its pass A; 2 rows
+// measured best (FP64 6.38 ms per substep against 6.49 at 4 rows; mixed
+// 5.53 against 5.94)
+#ifndef OTBL_FT_TK
+#define OTBL_FT_TK 2
+#endif
 template <>
 struct FinalTune<double> {
-  static constexpr int kf = OTBL_FT_DK, minb = OTBL_FT_DM;
+  static constexpr int kf = OTBL_FT_DK, minb = OTBL_FT_DM, kf_tma = OTBL_FT_TK;
   static constexpr bool split = false;
 };
 template <>
 struct FinalTune<float> {
-  static constexpr int kf = OTBL_FT_FK, minb = OTBL_FT_FM;
+  static constexpr int kf = OTBL_FT_FK, minb = OTBL_FT_FM, kf_tma = OTBL_FT_TK;
   static constexpr bool split = true;
 };
 
@@ -173,10 +182,9 @@ struct FinalStream {
 
 // PASSES: 1 pass A only (k_final_sA, a light kernel at high occupancy),
 // 2 pass B only, 3 both
-template <int COMP, typename W, int PASSES>
+template <int COMP, typename W, int PASSES, int KF = FinalTune<W>::kf>
 __global__ void __launch_bounds__(128, PASSES == 1 ? 8 : FinalTune<W>::minb)
     k_final_s1(DCoef c, FinalStream<W> fs) {
-  constexpr int KF = FinalTune<W>::kf;
   const FinalArgs<W> &a = fs.a;
   const int nx = c.nx, ny = c.ny, nz1 = c.nz1;
   const int ncol = (nx - 1) * nz1;
@@ -407,6 +415,252 @@ __global__ void __launch_bounds__(128) k_final_s2(DCoef c, double *u, double *v,
 }
 
 // ---------------------------------------------------------------------------
+// Pass B of the rhsp tail fed by TMA. A CTA owns 128 consecutive kr of one
+// plane i (one column per thread); thread 0 loads, for the next segment of
+// KF rows (descending), one box per field (the product and the velocity on
+// rows s0-1..s0+KF, the difvisxx output, the kz product and the RHS history
+// on rows s0..s0+KF-1, the pressure on rows s0..s0+KF of planes i and i+1)
+// into a two-stage shared-memory ring, counted on one mbarrier per stage,
+// while all threads work on the current segment from shared memory. Element
+// (row b, column t) of a box is at b*128 + t, so each thread's reads are
+// conflict-free. Rows outside the field read as 0 and are not used. The
+// arithmetic is k_final_s1's pass B, operation for operation.
+// ---------------------------------------------------------------------------
+template <typename W>
+struct FinalBox {
+  static constexpr int KF = FinalTune<W>::kf_tma, T = 128;
+  static constexpr int prod = 0;                                            // W (KF+2) rows
+  static constexpr int vel = prod + ((KF + 2) * T * (int)sizeof(W) + 127) / 128 * 128;  // double (KF+2)
+  static constexpr int cx = vel + (KF + 2) * T * 8;                         // W KF rows
+  static constexpr int kp = cx + (KF * T * (int)sizeof(W) + 127) / 128 * 128;  // W KF rows
+  static constexpr int hp = kp + (KF * T * (int)sizeof(W) + 127) / 128 * 128;  // double KF rows
+  static constexpr int p = hp + KF * T * 8;                                 // double (KF+1) x 2 planes
+  static constexpr int stage = p + (KF + 1) * 2 * T * 8;
+  static constexpr unsigned tx = (unsigned)((KF + 2) * T * sizeof(W) + (KF + 2) * T * 8 + 2 * KF * T * sizeof(W) +
+                                            KF * T * 8 + (KF + 1) * 2 * T * 8);
+  static constexpr int smem = 2 * stage + 128;  // two stages and the barriers
+};
+
+template <int COMP, typename W>
+__global__ void __launch_bounds__(128) k_final_tb(DCoef c, FinalStream<W> fs, int *err,
+                                                  const __grid_constant__ FinalMaps maps) {
+  using B = FinalBox<W>;
+  constexpr int KF = B::KF, TB = B::T;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  uint64_t *full = reinterpret_cast<uint64_t *>(smraw + 2 * B::stage);
+  const FinalArgs<W> &a = fs.a;
+  const int nx = c.nx, ny = c.ny, nz1 = c.nz1;
+  const int ncol = (nx - 1) * nz1;
+  const int t = threadIdx.x;
+  const int i = blockIdx.y + 2, kr0 = blockIdx.x * TB, kr = kr0 + t;
+  const bool active = kr < nz1;
+  const int col = (i - 2) * nz1 + kr;
+  const int k = kr >> 1, odd = kr & 1;
+  const bool last = i == nx;
+  const int jee = COMP == 1 ? ny : ny + 1, n = jee - 2;
+  const int nseg = (jee + KF - 1) / KF;
+  // ---- the ring: thread 0 initialises the barriers and loads segment nseg-1
+  auto issue = [&](int stg, int sg) {
+    unsigned char *b = smraw + stg * B::stage;
+    const int s0 = sg * KF;
+    mbar_arrive_expect_tx(&full[stg], B::tx);
+    tma_load_3d(b + B::prod, &maps.prod, kr0, s0 - 1, i - 1, &full[stg]);
+    tma_load_3d(b + B::vel, &maps.vel, kr0, s0 - 1, i - 1, &full[stg]);
+    tma_load_3d(b + B::cx, &maps.cx, kr0, s0, i - 1, &full[stg]);
+    tma_load_3d(b + B::kp, &maps.kp, kr0, s0, i - 1, &full[stg]);
+    tma_load_3d(b + B::hp, &maps.hp, kr0, s0, i - 1, &full[stg]);
+    tma_load_3d(b + B::p, &maps.p, kr0, s0, i - 1, &full[stg]);
+  };
+  if (t == 0) {
+    mbar_init(&full[0], 1);
+    mbar_init(&full[1], 1);
+    mbar_init_fence();
+  }
+  __syncthreads();
+  if (t == 0) issue(0, nseg - 1);
+  // ---- per-column setup (as k_final_s1)
+  const int pof = odd ? -1 : 1;
+  const size_t PU = (size_t)(ny + 1) * nz1, PV = (size_t)ny * nz1;
+  const size_t pl = (size_t)(i - 1) * (COMP == 1 ? PV : PU), plv = (size_t)(i - 1) * PV;
+  const size_t S = nz1;
+  const int krc = active ? kr : 0;  // inactive threads read a valid column and write nothing
+  const W *prod = (COMP == 0 ? a.uv : (COMP == 1 ? a.vv : a.vw)) + plv + krc;
+  const double *vel = (COMP == 0 ? a.u : (COMP == 1 ? a.v : a.w)) + pl + krc;
+  double *hp = (COMP == 0 ? a.rhsupa : (COMP == 1 ? a.rhsvpa : a.rhswpa)) + pl + krc;
+  const double *pc = a.p + plv + krc;
+  const double kz = c.kaz[k], kv = c.kvis[k];
+  const double var1 = a.st->var1, var3 = a.st->var3, var4 = a.st->var4;
+  const double v2 = last ? 0.0 : a.st->var2;
+  const double idxx = c.S[OTBL_S_IDXX];
+  const double *ib = c.inby, *cc = c.ccon;
+  const double sgn = odd ? 1.0 : -1.0;
+  const int which = COMP == 1 ? 1 : 0;
+  const double *dcy = which == 0 ? c.dcyu : c.dcyv, *ecd = which == 0 ? c.cofcyu : c.cofcyv;
+  const double *viy = which == 0 ? c.viyu : c.viyv, *ecv = which == 0 ? c.cofvyu : c.cofvyv;
+  const double *vyi = which == 0 ? c.vyui : c.vyvi;
+  const double *fac = COMP == 1 ? a.fac_v : a.fac_u;
+  auto Pg = [&](int r) { return (double)__ldg(prod + (size_t)min(max(r, 0), ny - 1) * S); };
+  auto Vg = [&](int r) { return __ldg(vel + (size_t)min(max(r, 0), jee - 1) * S); };
+  // velocity after the pressure gradient (rhsp.F90:291-339), from global
+  // memory (boundary rows) ...
+  auto star_g = [&](int r, double o) -> double {
+    const int rp = min(r, ny - 1);
+    if (COMP == 0)
+      return last ? o : o - var1 * idxx * (__ldg(pc + PV + (size_t)rp * S) - __ldg(pc + (size_t)rp * S));
+    if (COMP == 1)
+      return o - var1 * c.idyy[r] * (__ldg(pc + (size_t)min(r + 1, ny - 1) * S) - __ldg(pc + (size_t)rp * S));
+    const double pp = __ldg(pc + (size_t)rp * S + pof);
+    const double av = var1 * kz;
+    return o - (odd ? av * pp : -av * pp);
+  };
+  const int chv = which == 0 ? 3 : 1, cha = chv + 1, ic = which == 0 ? 3 : 1;
+  const double *db = c.dcby, *vb = c.cofvby;
+  double bot = 0.0, top = 0.0;
+  if (!last) {
+    bot = M4(db, chv, 1) * Pg(0) + M4(db, chv, 2) * Pg(1) + M4(db, chv, 3) * Pg(2) + M4(db, chv, 4) * Pg(3);
+    top = M4(db, cha, 1) * Pg(ny - 1) + M4(db, cha, 2) * Pg(ny - 2) + M4(db, cha, 3) * Pg(ny - 3) +
+          M4(db, cha, 4) * Pg(ny - 4);
+  }
+  const double b0 = M4(vb, ic, 1) * Vg(0) + M4(vb, ic, 2) * Vg(1) + M4(vb, ic, 3) * Vg(2) + M4(vb, ic, 4) * Vg(3);
+  const double bN = M4(vb, ic + 1, 1) * Vg(jee - 1) + M4(vb, ic + 1, 2) * Vg(jee - 2) +
+                    M4(vb, ic + 1, 3) * Vg(jee - 3) + M4(vb, ic + 1, 4) * Vg(jee - 4);
+  double ub1 = 0.0, ubt = 0.0;
+  if (COMP == 1) {
+    ubt = kr == 0 ? c.vmagic[i - 1] : 0.0;
+  } else {
+    const double s2 = star_g(1, Vg(1)), s3 = star_g(2, Vg(2)), s4 = star_g(3, Vg(3));
+    const double sn = star_g(ny - 1, Vg(ny - 1)), sn1 = star_g(ny - 2, Vg(ny - 2)), sn2 = star_g(ny - 3, Vg(ny - 3));
+    ub1 = -1.0 / M4(ib, 2, 1) * (M4(ib, 2, 2) * s2 + M4(ib, 2, 3) * s3 + M4(ib, 2, 4) * s4);
+    ubt = -1.0 / M2(cc, 1, 1) * (M2(cc, 1, 2) * sn + M2(cc, 1, 3) * sn1 + M2(cc, 1, 4) * sn2);
+  }
+  auto rd = [&](int r, double gm, double g0, double gp) {
+    const double in = which == 0 ? __ldg(ecd + 2 * r + 1) * g0 + __ldg(ecd + 2 * r) * gm
+                                 : __ldg(ecd + 2 * r + 1) * gp + __ldg(ecd + 2 * r) * g0;
+    return r == 0 ? bot : (r == jee - 1 ? top : in);
+  };
+  auto rv = [&](int r, double um, double u0, double up) {
+    const double in = __ldg(ecv + 3 * r) * up + __ldg(ecv + 3 * r + 1) * u0 + __ldg(ecv + 3 * r + 2) * um;
+    return r == 0 ? b0 : (r == jee - 1 ? bN : in);
+  };
+  const double *ck = fs.ck + (active ? col : 0);
+  double *yq = fs.yq + (active ? col : 0);
+  const double a1raw = fac[3 * (jee + 1)], a3raw = fac[3 * (jee + 1) + 1];
+  double xd = 0.0, xv = 0.0;
+  double R1 = 0.0, R2 = 0.0, R3 = 0.0;
+  double res1 = 0.0, res2 = 0.0;
+  double yel = 0.0;
+  double ckd = ck[(size_t)(2 * (nseg - 1)) * ncol], ckv = ck[(size_t)(2 * (nseg - 1) + 1) * ncol];
+  const int tk = t ^ 1;  // kr+1 for even kr, kr-1 for odd kr (the chunk starts even)
+  for (int sg = nseg - 1, it = 0; sg >= 0; --sg, ++it) {
+    const int stg = it & 1;
+    const bool ok = mbar_wait_bounded(&full[stg], (it >> 1) & 1, 2000000000ull);
+    if (__syncthreads_or(!ok)) {  // stage stg of iteration it-1 is free from here on
+      if (t == 0) atomicExch(err, OTBL_ERR_TIMEOUT);
+      return;
+    }
+    if (t == 0 && sg >= 1) issue(stg ^ 1, sg - 1);
+    const int s0 = sg * KF;
+    const unsigned char *bs = smraw + stg * B::stage;
+    const W *sp = reinterpret_cast<const W *>(bs + B::prod);
+    const double *sv = reinterpret_cast<const double *>(bs + B::vel);
+    const W *sc = reinterpret_cast<const W *>(bs + B::cx);
+    const W *sk = reinterpret_cast<const W *>(bs + B::kp);
+    const double *sh = reinterpret_cast<const double *>(bs + B::hp);
+    const double *spp = reinterpret_cast<const double *>(bs + B::p);
+    double ad = ckd, av = ckv;
+    if (sg >= 1) {  // next segment's checkpoints, ahead of use
+      ckd = ck[(size_t)(2 * (sg - 1)) * ncol];
+      ckv = ck[(size_t)(2 * (sg - 1) + 1) * ncol];
+    }
+    if (!active) continue;
+    double ydv[KF], yvv[KF];
+#pragma unroll
+    for (int b = 0; b < KF; ++b) {
+      const int r = s0 + b;
+      if (r < jee) {
+        if (!last)
+          ad = rd(r, (double)sp[b * TB + t], (double)sp[(b + 1) * TB + t], (double)sp[(b + 2) * TB + t]) +
+               (r > 0 ? __ldg(dcy + 3 * r) : 0.0) * ad;
+        av = rv(r, sv[b * TB + t], sv[(b + 1) * TB + t], sv[(b + 2) * TB + t]) +
+             (r > 0 ? __ldg(viy + 3 * r) : 0.0) * av;
+      }
+      ydv[b] = ad;
+      yvv[b] = av;
+    }
+#pragma unroll
+    for (int b = KF - 1; b >= 0; --b) {
+      const int r = s0 + b, j = r + 1;
+      if (r >= jee) continue;
+      if (!last) xd = (ydv[b] - __ldg(dcy + 3 * r + 2) * xd) * __ldg(dcy + 3 * r + 1);
+      xv = (yvv[b] - __ldg(viy + 3 * r + 2) * xv) * __ldg(viy + 3 * r + 1);
+      // RHS assembly (rhsp.F90:164-169, 181-204, 351-418, 423-445)
+      const double d1 = last ? 0.0 : xd;
+      const double u0 = sv[(b + 1) * TB + t];
+      double R = (double)sc[b * TB + t];
+      const double kzt = sgn * kz * ((!last && (COMP != 2 || r < ny)) ? (double)sk[b * TB + tk] : 0.0);
+      if (COMP == 0) {
+        if (!last) {
+          R = (d1 + kzt) + R;
+          if (j >= 2 && j <= ny) R = R - u0 * kv;
+        }
+      } else if (COMP == 1) {
+        if (!last) {
+          if (j >= 2 && j <= ny - 1) R = R - u0 * kv;
+          R = R + kzt;
+          R = R + d1;
+        }
+        if (j == 1 || j == ny) R = 0.0;
+      } else {
+        if (!last) {
+          if (j >= 2 && j <= ny) R = R - u0 * kv;
+          R = R + d1;
+          if (j <= ny) R = R + kzt;
+        }
+      }
+      if (COMP != 1) {  // wall and top rows of the u,w RHS (rhsp.F90:438-442)
+        if (r == jee - 1) R = 0.0;
+        if (r == 0) R = -1.0 / M4(ib, 2, 1) * (M4(ib, 2, 2) * R1 + M4(ib, 2, 3) * R2 + M4(ib, 2, 4) * R3);
+        if (r == 3) R3 = R;
+        if (r == 2) R2 = R;
+        if (r == 1) R1 = R;
+      }
+      // RK3 combination and the new RHS history (rhsp.F90:448-475); rows
+      // 1..jee-2 of the pressure box (no clamp needed there)
+      double st;
+      if (r == 0) {
+        st = ub1;
+      } else if (r == jee - 1) {
+        st = ubt;
+      } else if (COMP == 0) {
+        st = last ? u0 : u0 - var1 * idxx * (spp[((KF + 1) + b) * TB + t] - spp[b * TB + t]);
+      } else if (COMP == 1) {
+        st = u0 - var1 * c.idyy[r] * (spp[(b + 1) * TB + t] - spp[b * TB + t]);
+      } else {
+        const double pp = spp[b * TB + tk];
+        const double avz = var1 * kz;
+        st = u0 - (odd ? avz * pp : -avz * pp);
+      }
+      const double res = st - (var3 * R + v2 * xv + var4 * sh[b * TB + t]);
+      hp[(size_t)r * S] = R;
+      if (r < n) {
+        double v = __ldg(vyi + 3 * (r + 1)) * res + __ldg(vyi + 3 * (r + 1) + 1) * res1 +
+                   __ldg(vyi + 3 * (r + 1) + 2) * res2;
+        if (r == 0) v = v - a1raw * ub1;
+        if (r == n - 1) v = v - a3raw * ubt;
+        yel = v + fac[3 * (r + 2) + 2] * yel;
+        yq[(size_t)r * ncol] = yel;
+      }
+      res2 = res1;
+      res1 = res;
+    }
+  }
+  if (active) {
+    fs.ub[col] = ub1;
+    fs.ub[(size_t)ncol + col] = ubt;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // pois.f90:106-117 + soltriy: tridiagonal in y per (x-mode, kz). The LU of
 // each (i, k) system depends only on the grid, so its pivots are computed
 // once (k_pois_lu) and every substep runs the pre-factored solve.
@@ -521,6 +775,67 @@ cudaError_t launch_interpy(otbl_ctx *c) {
   return cudaGetLastError();
 }
 
+// ---- TMA descriptors (host) ----
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    cudaGetLastError();
+  }
+  return fn;
+}
+
+// a field [planes][rows][nz1] of element size esz, boxes of 128 x brows x bplanes
+static bool encode_field(CUtensorMap *m, const void *base, size_t esz, int planes, int rows, int nz1, int brows,
+                         int bplanes) {
+  auto fn = tensor_map_encoder();
+  if (!fn || (nz1 * esz) % 16 != 0 || ((uintptr_t)base) % 16 != 0) return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)nz1, (cuuint64_t)rows, (cuuint64_t)planes};
+  const cuuint64_t strides[2] = {(cuuint64_t)nz1 * esz, (cuuint64_t)rows * nz1 * esz};
+  const cuuint32_t box[3] = {128, (cuuint32_t)brows, (cuuint32_t)bplanes};
+  const cuuint32_t es[3] = {1, 1, 1};
+  const CUtensorMapDataType dt = esz == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  return fn(m, dt, 3, const_cast<void *>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <typename W>
+static bool build_maps_t(otbl_ctx *c) {
+  constexpr int KF = FinalTune<W>::kf_tma;
+  const int nx = c->cfg.nx, ny = c->cfg.ny, nz1 = c->dc.nz1;
+  const size_t ew = sizeof(W);
+  bool ok = nz1 >= 2;
+  for (int comp = 0; comp < 3 && ok; ++comp) {
+    FinalMaps &m = c->fmaps[comp];
+    const int jee = comp == 1 ? ny : ny + 1;
+    const void *prod = comp == 0 ? c->w.uv : (comp == 1 ? c->w.vv : c->w.vw);
+    const void *kp = comp == 0 ? c->w.uw : (comp == 1 ? c->w.vw : c->w.ww);
+    const int kprows = comp == 0 ? ny + 1 : ny;
+    const double *vel = c->f[comp == 0 ? OTBL_F_U : (comp == 1 ? OTBL_F_V : OTBL_F_W)];
+    const void *cx = comp == 0 ? c->w.cu : (comp == 1 ? c->w.cv : c->w.cw);
+    const double *hp = c->f[comp == 0 ? OTBL_F_RHSUPA : (comp == 1 ? OTBL_F_RHSVPA : OTBL_F_RHSWPA)];
+    ok = ok && encode_field(&m.prod, prod, ew, nx, ny, nz1, KF + 2, 1);
+    ok = ok && encode_field(&m.kp, kp, ew, nx, kprows, nz1, KF, 1);
+    ok = ok && encode_field(&m.vel, vel, 8, nx, jee, nz1, KF + 2, 1);
+    ok = ok && encode_field(&m.cx, cx, ew, nx, jee, nz1, KF, 1);
+    ok = ok && encode_field(&m.hp, hp, 8, nx, jee, nz1, KF, 1);
+    ok = ok && encode_field(&m.p, c->f[OTBL_F_P], 8, nx, ny, nz1, KF + 1, 2);
+  }
+  return ok;
+}
+
+bool build_final_maps(otbl_ctx *c) {
+  c->fmaps_ok = c->mixed ? build_maps_t<float>(c) : build_maps_t<double>(c);
+  return c->fmaps_ok;
+}
+
 template <typename W>
 static int final_t(otbl_ctx *c) {
   FinalStream<W> fs;
@@ -549,9 +864,17 @@ static int final_t(otbl_ctx *c) {
   fs.ub = c->w.s3;
   const dim3 g((ncol + 127) / 128);
   double *U = c->f[OTBL_F_U], *V = c->f[OTBL_F_V], *Wv = c->f[OTBL_F_W];
+  const bool tma = c->fmaps_ok;
+  const dim3 gt((c->dc.nz1 + 127) / 128, c->cfg.nx - 1);
+  const int smem_t = FinalBox<W>::smem;
   auto comp = [&](auto C) {
     constexpr int K = decltype(C)::value;
-    if constexpr (FinalTune<W>::split) {
+    if (tma) {
+      // pass A, then the TMA-fed pass B
+      k_final_s1<K, W, 1, FinalTune<W>::kf_tma><<<g, 128, 0, c->stream>>>(c->dc, fs);
+      cudaFuncSetAttribute(k_final_tb<K, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_t);
+      k_final_tb<K, W><<<gt, 128, smem_t, c->stream>>>(c->dc, fs, &c->st->err, c->fmaps[K]);
+    } else if constexpr (FinalTune<W>::split) {
       k_final_s1<K, W, 1><<<g, 128, 0, c->stream>>>(c->dc, fs);
       k_final_s1<K, W, 2><<<g, 128, 0, c->stream>>>(c->dc, fs);
     } else {
@@ -562,7 +885,7 @@ static int final_t(otbl_ctx *c) {
   comp(std::integral_constant<int, 1>{});
   comp(std::integral_constant<int, 0>{});
   comp(std::integral_constant<int, 2>{});
-  return FinalTune<W>::split ? 9 : 6;
+  return (tma || FinalTune<W>::split) ? 9 : 6;
 }
 
 cudaError_t launch_final(otbl_ctx *c) {

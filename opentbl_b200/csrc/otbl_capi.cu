@@ -2,6 +2,7 @@
 // transfer and the stream-ordered orchestration of the kernels in
 // kernels.cu, following the call order of bl_1.F90:94-125.
 #include <algorithm>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 
@@ -196,8 +197,11 @@ extern "C" int otbl_ctx_create(const otbl_config *cfg, const double *coef, int d
       *b = q;
     }
   }
-  double **scratch[] = {&w.s1, &w.s2, &w.s3};
-  for (double **b : scratch) TRY(dalloc(c, b, lu));
+  // s1 holds the line kernels' checkpoints; the rhsp tail's, at segments of
+  // 2 rows, take 2*ceil((ny+1)/2) <= ny+2 rows of (nx-1)*nz1 columns
+  TRY(dalloc(c, &w.s1, std::max(lu, (size_t)(ny + 2) * (nx - 1) * nz1)));
+  TRY(dalloc(c, &w.s2, lu));
+  TRY(dalloc(c, &w.s3, lu));
   const int M = nz / 2, n = nx - 1;
   TRY(dalloc(c, &w.twz, 2 * (size_t)M));
   TRY(dalloc(c, &w.twz2, 2 * (size_t)M));
@@ -213,6 +217,7 @@ extern "C" int otbl_ctx_create(const otbl_config *cfg, const double *coef, int d
   TRY(dalloc(c, &w.gf, genflu_tab_doubles(ny)));
   TRY(dalloc(c, &w.pois_dinv, (size_t)nx * ny * (nz1 / 2)));
 #undef TRY
+  if (!getenv("OTBL_NO_TMA")) build_final_maps(c);
   if (check(c, launch_twiddles(c), "twiddles") != OTBL_OK || check(c, launch_pois_lu(c), "pois_lu") != OTBL_OK || check(c, cudaStreamSynchronize(c->stream), "init")) {
     *out = c;
     return OTBL_ERR_CUDA;
@@ -232,7 +237,7 @@ extern "C" size_t otbl_ctx_bytes(const otbl_config *cfg) {
   b += (4 * lu + 3 * lv) * sizeof(double);                       // state
   b += 3 * (size_t)(ny + 1) * sizeof(double) + sizeof(DState);   // u0, v0, um, scalars
   b += 15 * lu * (mixed ? sizeof(float) : sizeof(double));       // intermediates
-  b += 3 * lu * sizeof(double);                                  // scratch
+  b += (std::max(lu, (size_t)(ny + 2) * (nx - 1) * nz1) + 2 * lu) * sizeof(double);  // scratch
   b += (4 * (size_t)M + 4 * (size_t)n) * sizeof(double) + (mixed ? 4 * (size_t)M * sizeof(float) : 0);
   b += (size_t)(ny + 1) * 8 + 6 * (size_t)(ny + 4) * sizeof(double) + genflu_tab_doubles(ny) * sizeof(double);
   b += (size_t)nx * ny * (nz1 / 2) * sizeof(double);             // Poisson pivots
@@ -360,7 +365,8 @@ extern "C" int otbl_get_inflow(otbl_ctx *c, double *um, otbl_inflow *s) {
     s->vmax = h.vmax;
   }
   if (h.err) {
-    c->err = "non-finite value in the CFL reduction";
+    c->err = h.err == OTBL_ERR_TIMEOUT ? "a device-side wait of a kernel timed out"
+                                     : "non-finite value in the CFL reduction";
     return h.err;
   }
   return OTBL_OK;
@@ -436,7 +442,8 @@ extern "C" int otbl_sync(otbl_ctx *c) {
   int err = 0;
   OTBL_CUDA_TRY(c, cudaMemcpy(&err, &c->st->err, sizeof(int), cudaMemcpyDeviceToHost));
   if (err) {
-    c->err = "non-finite value in the CFL reduction";
+    c->err = err == OTBL_ERR_TIMEOUT ? "a device-side wait of a kernel timed out"
+                                     : "non-finite value in the CFL reduction";
     return err;
   }
   return OTBL_OK;

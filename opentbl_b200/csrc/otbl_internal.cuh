@@ -2,6 +2,7 @@
 // buffer, device scalar state, the context, and launch helpers.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -66,6 +67,12 @@ struct Work {
   double *pois_dinv;           // pivots of the (x-mode, kz) y-systems, [i][j][k]
 };
 
+// TMA descriptors (opaque 128-byte CUtensorMap objects) of the fields the
+// rhsp tail's descending pass reads, for one velocity component (k_final_tb)
+struct FinalMaps {
+  CUtensorMap prod, kp, vel, cx, hp, p;
+};
+
 }  // namespace otbl
 
 struct otbl_ctx {
@@ -78,6 +85,9 @@ struct otbl_ctx {
   // [0] k_interpx, [1] k_difvisx, [2] k_interpy (one thread per line, so the
   // choice changes the schedule, never the arithmetic)
   int tune_bs[3] = {128, 128, 128};
+  // TMA descriptors of the rhsp tail's inputs, per velocity component
+  otbl::FinalMaps fmaps[3];
+  bool fmaps_ok = false;
   int mixed;                // cfg.precision == OTBL_PREC_MIXED
   double *coef_dev;
   float *coef_dev_f;
@@ -135,6 +145,9 @@ cudaError_t launch_reset_max(otbl_ctx *c);
 cudaError_t launch_boun_all(otbl_ctx *c);
 cudaError_t launch_tiempo(otbl_ctx *c);
 cudaError_t launch_energies(otbl_ctx *c);
+// builds c->fmaps (false if TMA cannot address the fields, e.g. an FP32 row
+// pitch that is not a multiple of 16 bytes)
+bool build_final_maps(otbl_ctx *c);
 cudaError_t launch_twiddles(otbl_ctx *c);
 cudaError_t launch_pois_lu(otbl_ctx *c);
 cudaError_t launch_pois_solve(otbl_ctx *c, double *phi);

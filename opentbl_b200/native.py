@@ -18,7 +18,8 @@ _lib = None
 OTBL_OK = 0
 OTBL_BUSY = 7
 ERRORS = {1: "bad argument", 2: "bad configuration", 3: "out of device memory",
-          4: "CUDA error", 5: "non-finite value", 6: "no CUDA device"}
+          4: "CUDA error", 5: "non-finite value", 6: "no CUDA device",
+          8: "device wait timed out"}
 FIELDS = ("u", "v", "w", "p", "rhsupa", "rhsvpa", "rhswpa")
 UTYPE = {"u": True, "v": False, "w": True, "p": False,
          "rhsupa": True, "rhsvpa": False, "rhswpa": True}

@@ -171,6 +171,7 @@ def test_c1_divergence_after_transient():
 @pytest.mark.parametrize("cfg", [
     replace(config.TINY, nx=17, ny=300, name="tall-17x300x32"),
     replace(config.TINY, nx=1081, name="long-1081x41x32"),
+    replace(config.TINY, nx=65, ny=40, name="even-ny-65x40x32"),  # rhsp-tail checkpoints: ny+2 rows
 ], ids=lambda c: c.name)
 def test_long_lines(cfg):
     """Lines much longer than the default boxes' (300 rows in y, 1081 planes
