@@ -3,8 +3,13 @@
 // read with the plane stride, so the reference's chp2x transpose is replaced
 // by these strided, warp-coalesced loads (its REAL4 rounding is applied at
 // the same points when OTBL_XPOSE_FP32 is set).
+#include <cudaTypedefs.h>
+
+#include <type_traits>
+
 #include "devcommon.cuh"
 #include "otbl_internal.cuh"
+#include "tma.cuh"
 
 namespace otbl {
 
@@ -40,13 +45,18 @@ struct XStream {
 // unbounded (56 registers).
 template <typename T>
 struct XTune;
+// tma: the TMA-fed kernels (k_xline_t) instead of the register streams; at
+// 1025x193x512 FP32 difvisxx 1.65 ms against 1.79, interpxx 1.04 against
+// 1.18; FP64 difvisxx 4.17 against 3.20 (its stages cap it at 5 CTAs/SM).
 template <>
 struct XTune<double> {
   static constexpr int kxi = 16, kxd = 8, minb_i = 8;
+  static constexpr bool tma = false;
 };
 template <>
 struct XTune<float> {
   static constexpr int kxi = 8, kxd = 8, minb_i = 1;  // 0.88 ms unbounded, 1.19 at >= 8 CTAs
+  static constexpr bool tma = true;
 };
 
 
@@ -200,6 +210,227 @@ __global__ void __launch_bounds__(128, 6) k_difvisx(DCoefT<T> c, XStream a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// The same x-line operators fed by TMA: a CTA owns TB consecutive lines of
+// one field; thread 0 loads, for the next segment of K planes, boxes of 32
+// lines x K+1 (K+2) planes of each input into a two-stage shared-memory ring
+// counted on mbarriers (bounded waits), while every thread runs its line's
+// serial sweeps from shared memory. The sequence of segments is the forward
+// sweep (0..nseg-1) then the backward one (nseg-1..0). DV: difvisxx (inputs:
+// the product, FP32 on the mixed path, and the FP64 velocity) or interpxx
+// (input: the FP64 velocity). The arithmetic is k_interpx / k_difvisx's with
+// segments of K = 8.
+// ---------------------------------------------------------------------------
+template <typename T, bool DV, int TB>
+__global__ void __launch_bounds__(TB) k_xline_t(DCoefT<T> c, XStream a, int *err, const __grid_constant__ XMaps maps) {
+  constexpr int K = 8, NB = TB / 32;
+  using TG = typename std::conditional<DV, T, double>::type;
+  constexpr int GR = K + 1, UR = K + 2;
+  constexpr int GBYTES = NB * GR * 32 * (int)sizeof(TG);
+  constexpr int GB = (GBYTES + 127) / 128 * 128;
+  constexpr int UBYTES = DV ? NB * UR * 32 * 8 : 0;
+  constexpr int STG = GB + UBYTES;
+  constexpr unsigned TX = (unsigned)(GBYTES + UBYTES);
+  extern __shared__ __align__(128) unsigned char smraw[];
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + 2 * STG);
+  const int f = blockIdx.y, np = pick3(a.np, f);
+  const int t = threadIdx.x, mp0 = blockIdx.x * TB;
+  if (mp0 >= np) return;  // the whole CTA lies past this field's lines
+  const int mp = mp0 + t;
+  const bool active = mp < np;
+  const int mpc = active ? mp : np - 1;
+  const CUtensorMap *mg = f == 0 ? &maps.g[0] : (f == 1 ? &maps.g[1] : &maps.g[2]);
+  const CUtensorMap *mu = f == 0 ? &maps.u[0] : (f == 1 ? &maps.u[1] : &maps.u[2]);
+  const int nx = c.nx, xr = c.xround, which = pick3(a.which, f);
+  const int nseg = (nx + K - 1) / K;
+  auto seg_of = [&](int it) { return it < nseg ? it : 2 * nseg - 1 - it; };
+  auto issue = [&](int stg, int sg) {
+    unsigned char *b = smraw + stg * STG;
+    const int s0 = sg * K;
+    mbar_arrive_expect_tx(&bar[stg], TX);
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+      tma_load_2d(b + j * GR * 32 * (int)sizeof(TG), mg, mp0 + 32 * j, DV ? s0 - 1 : s0, &bar[stg]);
+      if (DV) tma_load_2d(b + GB + j * UR * 32 * 8, mu, mp0 + 32 * j, s0 - 1, &bar[stg]);
+    }
+  };
+  if (t == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_init_fence();
+  }
+  __syncthreads();
+  if (t == 0) issue(0, 0);
+  T *out = static_cast<T *>(pick3(a.out, f)) + mpc;
+  T *ck = reinterpret_cast<T *>(pick3(a.ck, f)) + mpc;
+  const int gofs = ((t >> 5) * GR) * 32 + (t & 31), uofs = ((t >> 5) * UR) * 32 + (t & 31);
+  // ---- operator setup (boundary stencils from global memory)
+  const T *icon, *econ, *iconv = nullptr, *econv = nullptr;
+  T gb0, gbN, ub0 = T(0), ubN = T(0), uN = T(0), uN1 = T(0);
+  const T rex = c.S[OTBL_S_REX], idx = c.S[OTBL_S_IDX], uinf = c.S[OTBL_S_UINF];
+  if constexpr (DV) {
+    const TG *gin = static_cast<const TG *>(pick3(a.in, f)) + mpc;
+    const double *uin = pick3(a.in2, f) + mpc;
+    icon = which == 0 ? c.dcxu : c.dcxv;
+    iconv = which == 0 ? c.vixu : c.vixv;
+    econ = which == 0 ? c.cofcxu : c.cofcxv;
+    econv = which == 0 ? c.cofvxu : c.cofvxv;
+    const int chv = which == 0 ? 1 : 2, chv1 = chv + 2, ic = which == 0 ? 3 : 1;
+    const T *db = c.dcbx, *vb = c.cofvbx;
+    auto G = [&](int i) { return (T)rnd(__ldg(gin + (size_t)i * np), xr); };
+    auto U = [&](int i) { return (T)rnd(__ldg(uin + (size_t)i * np), xr); };
+    gb0 = M5(db, chv, 1) * G(0) + M5(db, chv, 2) * G(1) + M5(db, chv, 3) * G(2) + M5(db, chv, 4) * G(3);
+    ub0 = M4(vb, ic, 1) * U(0) + M4(vb, ic, 2) * U(1) + M4(vb, ic, 3) * U(2) + M4(vb, ic, 4) * U(3);
+    gbN = M5(db, chv1, 1) * G(nx - 1) + M5(db, chv1, 2) * G(nx - 2) + M5(db, chv1, 3) * G(nx - 3) +
+          M5(db, chv1, 4) * G(nx - 4);
+    uN = U(nx - 1);
+    uN1 = U(nx - 2);
+    ubN = M4(vb, ic + 1, 1) * uN + M4(vb, ic + 1, 2) * uN1 + M4(vb, ic + 1, 3) * U(nx - 3) +
+          M4(vb, ic + 1, 4) * U(nx - 4);
+  } else {
+    const double *gin = static_cast<const double *>(pick3(a.in, f)) + mpc;
+    icon = which == 0 ? c.inxu : c.inxv;
+    econ = which == 0 ? c.cofiux : c.cofivx;
+    const int chi = which == 0 ? 2 : 1, chi2 = which == 0 ? 3 : 4;
+    const T *ib = c.inbx;
+    auto G = [&](int i) { return (T)rnd(__ldg(gin + (size_t)i * np), xr); };
+    gb0 = M4(ib, chi2, 1) * G(0) + M4(ib, chi2, 2) * G(1) + M4(ib, chi2, 3) * G(2) + M4(ib, chi2, 4) * G(3);
+    gbN = M4(ib, chi, 1) * G(nx - 1) + M4(ib, chi, 2) * G(nx - 2) + M4(ib, chi, 3) * G(nx - 3) +
+          M4(ib, chi, 4) * G(nx - 4);
+  }
+  // right-hand sides: interpxx e1 g_i + e2 g_{i+1}; difvisxx convective
+  // e1 g_{i-1} + e2 g_i and viscous f1 u_{i+1} + f2 u_i + f3 u_{i-1}
+  auto rg = [&](int i, T ga, T gb) {
+    return i == 0 ? gb0 : (i == nx - 1 ? gbN : __ldg(econ + 2 * i) * ga + __ldg(econ + 2 * i + 1) * gb);
+  };
+  auto ru = [&](int i, T um, T u0, T up) {
+    return i == 0 ? ub0
+                  : (i == nx - 1 ? ubN
+                                 : __ldg(econv + 3 * i) * up + __ldg(econv + 3 * i + 1) * u0 +
+                                       __ldg(econv + 3 * i + 2) * um);
+  };
+  T yg = T(0), yu = T(0), xg = T(0), xu = T(0);
+  for (int it = 0; it < 2 * nseg; ++it) {
+    const int stg = it & 1;
+    const bool ok = mbar_wait_bounded(&bar[stg], (it >> 1) & 1, 2000000000ull);
+    if (__syncthreads_or(!ok)) {
+      if (t == 0) atomicExch(err, OTBL_ERR_TIMEOUT);
+      return;
+    }
+    if (t == 0 && it + 1 < 2 * nseg) issue(stg ^ 1, seg_of(it + 1));
+    if (!active) continue;
+    const int sg = seg_of(it), s0 = sg * K;
+    const unsigned char *bs = smraw + stg * STG;
+    const TG *gs = reinterpret_cast<const TG *>(bs) + gofs;
+    const double *us = reinterpret_cast<const double *>(bs + GB) + uofs;
+    auto g = [&](int b) { return (T)rnd(gs[b * 32], xr); };
+    auto u = [&](int b) { return (T)rnd(us[b * 32], xr); };
+    if (it < nseg) {  // forward sweep, checkpoint at the segment start
+      ck[(size_t)((DV ? 2 : 1) * sg) * np] = yg;
+      if (DV) ck[(size_t)(2 * sg + 1) * np] = yu;
+#pragma unroll
+      for (int b = 0; b < K; ++b) {
+        const int i = s0 + b;
+        if (i < nx) {
+          yg = rg(i, g(b), g(b + 1)) + (i > 0 ? __ldg(icon + 3 * i) : T(0)) * yg;
+          if (DV) yu = ru(i, u(b), u(b + 1), u(b + 2)) + (i > 0 ? __ldg(iconv + 3 * i) : T(0)) * yu;
+        }
+      }
+    } else {  // backward sweep: recompute the segment, then substitute
+      T a1 = ck[(size_t)((DV ? 2 : 1) * sg) * np], a2 = DV ? ck[(size_t)(2 * sg + 1) * np] : T(0);
+      T y1[K], y2[K];
+#pragma unroll
+      for (int b = 0; b < K; ++b) {
+        const int i = s0 + b;
+        if (i < nx) {
+          a1 = rg(i, g(b), g(b + 1)) + (i > 0 ? __ldg(icon + 3 * i) : T(0)) * a1;
+          if (DV) a2 = ru(i, u(b), u(b + 1), u(b + 2)) + (i > 0 ? __ldg(iconv + 3 * i) : T(0)) * a2;
+        }
+        y1[b] = a1;
+        y2[b] = a2;
+      }
+#pragma unroll
+      for (int b = K - 1; b >= 0; --b) {
+        const int i = s0 + b;
+        if (i < nx) {
+          xg = (y1[b] - __ldg(icon + 3 * i + 2) * xg) * __ldg(icon + 3 * i + 1);
+          T v = xg;
+          if (DV) {
+            xu = (y2[b] - __ldg(iconv + 3 * i + 2) * xu) * __ldg(iconv + 3 * i + 1);
+            v = i == nx - 1 ? uinf * (uN - uN1) * idx + rex * T(0) : xg + rex * xu;
+          }
+          out[(size_t)i * np] = (T)rnd(v, xr);
+        }
+      }
+    }
+  }
+}
+
+template <typename T, bool DV>
+static void xline_t_launch(otbl_ctx *c, const DCoefT<T> &dc, const XStream &a, const XMaps &m, int npmax) {
+  constexpr int K = 8;
+  using TG = typename std::conditional<DV, T, double>::type;
+  auto smem = [&](int tb) {
+    const int nb = tb / 32;
+    const int gb = (nb * (K + 1) * 32 * (int)sizeof(TG) + 127) / 128 * 128;
+    return 2 * (gb + (DV ? nb * (K + 2) * 32 * 8 : 0)) + 128;
+  };
+  const int bs = c->tune_bs[DV ? 1 : 0];
+  int *err = &c->st->err;
+  if (bs <= 32) {
+    cudaFuncSetAttribute(k_xline_t<T, DV, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem(32));
+    k_xline_t<T, DV, 32><<<dim3((npmax + 31) / 32, 3), 32, smem(32), c->stream>>>(dc, a, err, m);
+  } else if (bs <= 64) {
+    cudaFuncSetAttribute(k_xline_t<T, DV, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem(64));
+    k_xline_t<T, DV, 64><<<dim3((npmax + 63) / 64, 3), 64, smem(64), c->stream>>>(dc, a, err, m);
+  } else {
+    cudaFuncSetAttribute(k_xline_t<T, DV, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem(128));
+    k_xline_t<T, DV, 128><<<dim3((npmax + 127) / 128, 3), 128, smem(128), c->stream>>>(dc, a, err, m);
+  }
+}
+
+// ---- TMA descriptors (host): field [nx][np], boxes of 32 lines x rows
+static bool encode_lines(CUtensorMap *m, const void *base, size_t esz, int nx, int np, int rows) {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    cudaGetLastError();
+  }
+  if (!fn || (np * esz) % 16 != 0 || ((uintptr_t)base) % 16 != 0) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)np, (cuuint64_t)nx};
+  const cuuint64_t strides[1] = {(cuuint64_t)np * esz};
+  const cuuint32_t box[2] = {32, (cuuint32_t)rows};
+  const cuuint32_t es[2] = {1, 1};
+  const CUtensorMapDataType dt = esz == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  return fn(m, dt, 2, const_cast<void *>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+bool build_x_maps(otbl_ctx *c) {
+  constexpr int K = 8;
+  const int nx = c->cfg.nx, nz1 = c->dc.nz1, ny = c->cfg.ny;
+  const int np[3] = {nz1 * (ny + 1), nz1 * ny, nz1 * (ny + 1)};
+  const double *st[3] = {c->f[OTBL_F_U], c->f[OTBL_F_V], c->f[OTBL_F_W]};
+  const void *pr[3] = {c->w.uu, c->w.uv, c->w.uw};
+  const size_t ew = c->mixed ? sizeof(float) : sizeof(double);
+  bool ok = true;
+  for (int f = 0; f < 3 && ok; ++f) {
+    ok = ok && encode_lines(&c->xmi.g[f], st[f], 8, nx, np[f], K + 1);
+    c->xmi.u[f] = c->xmi.g[f];  // unused by interpxx
+    ok = ok && encode_lines(&c->xmd.g[f], pr[f], ew, nx, np[f], K + 1);
+    ok = ok && encode_lines(&c->xmd.u[f], st[f], 8, nx, np[f], K + 2);
+  }
+  c->xmaps_ok = ok;
+  return ok;
+}
+
 cudaError_t launch_interpx(otbl_ctx *c) {
   const int nz1 = c->dc.nz1, ny = c->cfg.ny;
   const int npu = nz1 * (ny + 1), npv = nz1 * ny;
@@ -218,7 +449,12 @@ cudaError_t launch_interpx(otbl_ctx *c) {
   }
   const int bs = c->tune_bs[0];
   prof_begin(c, PK_INTERPX);
-  if (c->mixed)
+  if (c->xmaps_ok && (c->mixed ? XTune<float>::tma : XTune<double>::tma)) {
+    if (c->mixed)
+      xline_t_launch<float, false>(c, c->dcf, a, c->xmi, npu);
+    else
+      xline_t_launch<double, false>(c, c->dc, a, c->xmi, npu);
+  } else if (c->mixed)
     k_interpx<float><<<dim3((npu + bs - 1) / bs, 3), bs, 0, c->stream>>>(c->dcf, a);
   else
     k_interpx<double><<<dim3((npu + bs - 1) / bs, 3), bs, 0, c->stream>>>(c->dc, a);
@@ -246,7 +482,12 @@ cudaError_t launch_difvisx(otbl_ctx *c) {
   }
   const int bs = c->tune_bs[1];
   prof_begin(c, PK_DIFVISX);
-  if (c->mixed)
+  if (c->xmaps_ok && (c->mixed ? XTune<float>::tma : XTune<double>::tma)) {
+    if (c->mixed)
+      xline_t_launch<float, true>(c, c->dcf, a, c->xmd, npu);
+    else
+      xline_t_launch<double, true>(c, c->dc, a, c->xmd, npu);
+  } else if (c->mixed)
     k_difvisx<float><<<dim3((npu + bs - 1) / bs, 3), bs, 0, c->stream>>>(c->dcf, a);
   else
     k_difvisx<double><<<dim3((npu + bs - 1) / bs, 3), bs, 0, c->stream>>>(c->dc, a);

@@ -183,7 +183,7 @@ struct FinalStream {
 // PASSES: 1 pass A only (k_final_sA, a light kernel at high occupancy),
 // 2 pass B only, 3 both
 template <int COMP, typename W, int PASSES, int KF = FinalTune<W>::kf>
-__global__ void __launch_bounds__(128, PASSES == 1 ? 8 : FinalTune<W>::minb)
+__global__ void __launch_bounds__(128, PASSES == 1 ? 6 : FinalTune<W>::minb)
     k_final_s1(DCoef c, FinalStream<W> fs) {
   const FinalArgs<W> &a = fs.a;
   const int nx = c.nx, ny = c.ny, nz1 = c.nz1;
@@ -262,22 +262,26 @@ __global__ void __launch_bounds__(128, PASSES == 1 ? 8 : FinalTune<W>::minb)
   };
   const int nseg = (jee + KF - 1) / KF;
   double *ck = fs.ck + col;
-  // ---- pass A: forward sweeps, checkpoints
+  // ---- pass A: forward sweeps, checkpoints every KF rows; the loads go in
+  // batches of KA >= KF rows (a multiple of KF), so that short checkpoint
+  // segments still keep many loads in flight
   if constexpr ((PASSES & 1) != 0) {
+  constexpr int KA = KF >= 8 ? KF : (8 / KF) * KF;
   double yd = 0.0, yv = 0.0;
-  for (int sg = 0; sg < nseg; ++sg) {
-    const int s0 = sg * KF;
-    ck[(size_t)(2 * sg) * ncol] = yd;
-    ck[(size_t)(2 * sg + 1) * ncol] = yv;
-    double gv[KF + 2], uv[KF + 2];  // rows s0-1 .. s0+KF
+  for (int s0 = 0; s0 < jee; s0 += KA) {
+    double gv[KA + 2], uv[KA + 2];  // rows s0-1 .. s0+KA
 #pragma unroll
-    for (int b = 0; b < KF + 2; ++b) {
+    for (int b = 0; b < KA + 2; ++b) {
       gv[b] = last ? 0.0 : Pg(s0 + b - 1);
       uv[b] = Vg(s0 + b - 1);
     }
 #pragma unroll
-    for (int b = 0; b < KF; ++b) {
+    for (int b = 0; b < KA; ++b) {
       const int r = s0 + b;
+      if (b % KF == 0 && r < jee) {  // y of row r-1 at the start of segment r/KF
+        ck[(size_t)(2 * (r / KF)) * ncol] = yd;
+        ck[(size_t)(2 * (r / KF) + 1) * ncol] = yv;
+      }
       if (r < jee) {
         if (!last) yd = rd(r, gv[b], gv[b + 1], gv[b + 2]) + (r > 0 ? __ldg(dcy + 3 * r) : 0.0) * yd;
         yv = rv(r, uv[b], uv[b + 1], uv[b + 2]) + (r > 0 ? __ldg(viy + 3 * r) : 0.0) * yv;

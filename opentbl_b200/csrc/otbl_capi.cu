@@ -217,7 +217,10 @@ extern "C" int otbl_ctx_create(const otbl_config *cfg, const double *coef, int d
   TRY(dalloc(c, &w.gf, genflu_tab_doubles(ny)));
   TRY(dalloc(c, &w.pois_dinv, (size_t)nx * ny * (nz1 / 2)));
 #undef TRY
-  if (!getenv("OTBL_NO_TMA")) build_final_maps(c);
+  if (!getenv("OTBL_NO_TMA")) {
+    build_final_maps(c);
+    build_x_maps(c);
+  }
   if (check(c, launch_twiddles(c), "twiddles") != OTBL_OK || check(c, launch_pois_lu(c), "pois_lu") != OTBL_OK || check(c, cudaStreamSynchronize(c->stream), "init")) {
     *out = c;
     return OTBL_ERR_CUDA;

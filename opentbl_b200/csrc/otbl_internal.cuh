@@ -73,6 +73,12 @@ struct FinalMaps {
   CUtensorMap prod, kp, vel, cx, hp, p;
 };
 
+// TMA descriptors of the x-line kernels' inputs, per field (u, v, w): 2D
+// tensors [plane][line] with boxes of 32 lines
+struct XMaps {
+  CUtensorMap g[3], u[3];
+};
+
 }  // namespace otbl
 
 struct otbl_ctx {
@@ -88,6 +94,8 @@ struct otbl_ctx {
   // TMA descriptors of the rhsp tail's inputs, per velocity component
   otbl::FinalMaps fmaps[3];
   bool fmaps_ok = false;
+  otbl::XMaps xmi, xmd;  // k_interpx_t (state), k_difvisx_t (products, state)
+  bool xmaps_ok = false;
   int mixed;                // cfg.precision == OTBL_PREC_MIXED
   double *coef_dev;
   float *coef_dev_f;
@@ -148,6 +156,7 @@ cudaError_t launch_energies(otbl_ctx *c);
 // builds c->fmaps (false if TMA cannot address the fields, e.g. an FP32 row
 // pitch that is not a multiple of 16 bytes)
 bool build_final_maps(otbl_ctx *c);
+bool build_x_maps(otbl_ctx *c);
 cudaError_t launch_twiddles(otbl_ctx *c);
 cudaError_t launch_pois_lu(otbl_ctx *c);
 cudaError_t launch_pois_solve(otbl_ctx *c, double *phi);
