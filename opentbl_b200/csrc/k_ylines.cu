@@ -423,32 +423,36 @@ __global__ void __launch_bounds__(128) k_final_s2(DCoef c, double *u, double *v,
 // plane i (one column per thread); thread 0 loads, for the next segment of
 // KF rows (descending), one box per field (the product and the velocity on
 // rows s0-1..s0+KF, the difvisxx output, the kz product and the RHS history
-// on rows s0..s0+KF-1, the pressure on rows s0..s0+KF of planes i and i+1)
+// on rows s0..s0+KF-1, the pressure rows that component's pressure
+// gradient needs)
 // into a two-stage shared-memory ring, counted on one mbarrier per stage,
 // while all threads work on the current segment from shared memory. Element
 // (row b, column t) of a box is at b*128 + t, so each thread's reads are
 // conflict-free. Rows outside the field read as 0 and are not used. The
 // arithmetic is k_final_s1's pass B, operation for operation.
 // ---------------------------------------------------------------------------
-template <typename W>
+template <typename W, int COMP>
 struct FinalBox {
   static constexpr int KF = FinalTune<W>::kf_tma, T = 128;
+  // pressure box: u needs planes i, i+1 on rows s0..s0+KF-1, v rows
+  // s0..s0+KF of plane i, w rows s0..s0+KF-1 of plane i
+  static constexpr int PR = COMP == 1 ? KF + 1 : KF, PP = COMP == 0 ? 2 : 1;
   static constexpr int prod = 0;                                            // W (KF+2) rows
   static constexpr int vel = prod + ((KF + 2) * T * (int)sizeof(W) + 127) / 128 * 128;  // double (KF+2)
   static constexpr int cx = vel + (KF + 2) * T * 8;                         // W KF rows
   static constexpr int kp = cx + (KF * T * (int)sizeof(W) + 127) / 128 * 128;  // W KF rows
   static constexpr int hp = kp + (KF * T * (int)sizeof(W) + 127) / 128 * 128;  // double KF rows
-  static constexpr int p = hp + KF * T * 8;                                 // double (KF+1) x 2 planes
-  static constexpr int stage = p + (KF + 1) * 2 * T * 8;
+  static constexpr int p = hp + KF * T * 8;                                 // double PR x PP
+  static constexpr int stage = p + PR * PP * T * 8;
   static constexpr unsigned tx = (unsigned)((KF + 2) * T * sizeof(W) + (KF + 2) * T * 8 + 2 * KF * T * sizeof(W) +
-                                            KF * T * 8 + (KF + 1) * 2 * T * 8);
+                                            KF * T * 8 + PR * PP * T * 8);
   static constexpr int smem = 2 * stage + 128;  // two stages and the barriers
 };
 
 template <int COMP, typename W>
 __global__ void __launch_bounds__(128) k_final_tb(DCoef c, FinalStream<W> fs, int *err,
                                                   const __grid_constant__ FinalMaps maps) {
-  using B = FinalBox<W>;
+  using B = FinalBox<W, COMP>;
   constexpr int KF = B::KF, TB = B::T;
   extern __shared__ __align__(128) unsigned char smraw[];
   uint64_t *full = reinterpret_cast<uint64_t *>(smraw + 2 * B::stage);
@@ -636,7 +640,7 @@ __global__ void __launch_bounds__(128) k_final_tb(DCoef c, FinalStream<W> fs, in
       } else if (r == jee - 1) {
         st = ubt;
       } else if (COMP == 0) {
-        st = last ? u0 : u0 - var1 * idxx * (spp[((KF + 1) + b) * TB + t] - spp[b * TB + t]);
+        st = last ? u0 : u0 - var1 * idxx * (spp[(B::PR + b) * TB + t] - spp[b * TB + t]);
       } else if (COMP == 1) {
         st = u0 - var1 * c.idyy[r] * (spp[(b + 1) * TB + t] - spp[b * TB + t]);
       } else {
@@ -830,7 +834,7 @@ static bool build_maps_t(otbl_ctx *c) {
     ok = ok && encode_field(&m.vel, vel, 8, nx, jee, nz1, KF + 2, 1);
     ok = ok && encode_field(&m.cx, cx, ew, nx, jee, nz1, KF, 1);
     ok = ok && encode_field(&m.hp, hp, 8, nx, jee, nz1, KF, 1);
-    ok = ok && encode_field(&m.p, c->f[OTBL_F_P], 8, nx, ny, nz1, KF + 1, 2);
+    ok = ok && encode_field(&m.p, c->f[OTBL_F_P], 8, nx, ny, nz1, comp == 1 ? KF + 1 : KF, comp == 0 ? 2 : 1);
   }
   return ok;
 }
@@ -870,9 +874,9 @@ static int final_t(otbl_ctx *c) {
   double *U = c->f[OTBL_F_U], *V = c->f[OTBL_F_V], *Wv = c->f[OTBL_F_W];
   const bool tma = c->fmaps_ok;
   const dim3 gt((c->dc.nz1 + 127) / 128, c->cfg.nx - 1);
-  const int smem_t = FinalBox<W>::smem;
   auto comp = [&](auto C) {
     constexpr int K = decltype(C)::value;
+    const int smem_t = FinalBox<W, K>::smem;
     if (tma) {
       // pass A, then the TMA-fed pass B
       k_final_s1<K, W, 1, FinalTune<W>::kf_tma><<<g, 128, 0, c->stream>>>(c->dc, fs);

@@ -9,9 +9,11 @@ in chunks of RK3 steps, each chunk one CUDA graph launch, so the kernels of
 all admitted requests overlap on the device. Slots are kept when their
 request finishes and re-bound (otbl_ctx_rebind) to the next request of the
 same grid size and precision; idle slots of other sizes are released when
-memory is needed. The host loop never blocks on the device: it polls each
-slot (otbl_query / otbl_graph_query) and issues the next chunk when the last
-one has finished.
+memory is needed. New slots are created (device allocation, coefficient
+upload, autotuning) on a background host thread, so the loop keeps feeding
+the running requests meanwhile. The host loop never blocks on the device:
+it polls each slot (otbl_query / otbl_graph_query) and issues the next chunk
+when the last one has finished.
 
 A request's result does not depend on the mix it ran in: its slot's kernels
 read and write only the slot's buffers, on the slot's stream, and every
@@ -23,6 +25,7 @@ from __future__ import annotations
 import dataclasses
 import time
 from collections import deque
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 
@@ -147,6 +150,8 @@ class Server:
         self.idle = {}
         self.used = 0
         self.tuning = {}  # CTA sizes picked by the autotuner, per grid size
+        self.creator = ThreadPoolExecutor(max_workers=1)
+        self.pending = None  # (request, future of its new slot)
         self.stats = {"created": 0, "reused": 0, "evicted": 0, "graph_launches": 0,
                       "direct_steps": 0, "peak_bytes": 0, "peak_active": 0,
                       "create_s": 0.0, "rebind_s": 0.0, "capture_s": 0.0}
@@ -166,8 +171,32 @@ class Server:
                 return True
         return False
 
+    def _create(self, req: Request, init: dict, need: int, key) -> "_Slot":
+        """Runs on the creation thread: a new context for req, autotuned (or
+        given the CTA sizes already picked for its grid size)."""
+        t = time.perf_counter()
+        box = Box(req.cfg, init, device=self.device)
+        if self.autotune:
+            if key in self.tuning:
+                box.set_tuning(self.tuning[key])
+            else:
+                self.tuning[key] = box.autotune()
+        self.stats["create_s"] += time.perf_counter() - t
+        return _Slot(box, need)
+
     def _acquire(self, req: Request, init: dict):
+        """A slot for the request at the head of the queue: an idle slot of
+        its grid size re-bound at once, or a new one created in the
+        background (None until it is ready, or while memory is short)."""
         key = size_key(req.cfg)
+        if self.pending is not None:
+            preq, fut = self.pending
+            if preq is not req or not fut.done():
+                return None
+            self.pending = None
+            s = fut.result()
+            self.stats["created"] += 1
+            return s
         lst = self.idle.get(key)
         if lst:
             t = time.perf_counter()
@@ -181,19 +210,10 @@ class Server:
             pass
         if self.used + need > self.budget:
             return None
-        t = time.perf_counter()
-        box = Box(req.cfg, init, device=self.device)
-        if self.autotune:
-            if key in self.tuning:
-                box.set_tuning(self.tuning[key])
-            else:
-                self.tuning[key] = box.autotune()
-        self.stats["create_s"] += time.perf_counter() - t
-        s = _Slot(box, need)
         self.used += need
-        self.stats["created"] += 1
         self.stats["peak_bytes"] = max(self.stats["peak_bytes"], self.used)
-        return s
+        self.pending = (req, self.creator.submit(self._create, req, init, need, key))
+        return None
 
     def _issue(self, s: _Slot):
         """Next chunk of the slot's request: a graph launch of `chunk` steps,
@@ -234,6 +254,7 @@ class Server:
         queue = deque()
         active = []
         results = []
+        head = None  # the queue head and its initial state
         t0 = time.perf_counter()
         while pending or queue or active:
             now = time.perf_counter() - t0
@@ -243,7 +264,9 @@ class Server:
             # admission, first come first served
             while queue and len(active) < self.max_active:
                 req = queue[0]
-                init = self.templates.get(req.cfg)
+                if head is None or head[0] is not req:
+                    head = (req, self.templates.get(req.cfg))
+                init = head[1]
                 s = self._acquire(req, init)
                 if s is None:
                     break
@@ -278,6 +301,7 @@ class Server:
         return sorted(results, key=lambda r: r.rid)
 
     def close(self):
+        self.creator.shutdown(wait=True)
         for lst in self.idle.values():
             for s in lst:
                 s.box.close()
