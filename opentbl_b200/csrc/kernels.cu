@@ -358,7 +358,9 @@ __device__ __forceinline__ double regs_absmax(const V (&a)[E]) {
 
 // CTAs per SM bound: FP64 unbounded (252 registers, 4.49 ms per substep at
 // 1025x193x512; 5.02 at >= 3 CTAs with spills), FP32 >= 3 CTAs (168
-// registers, 2.62 ms; 3.16 unbounded at 185)
+// registers, 2.62 ms; 3.16 unbounded at 185). A variant with two warps per
+// line (4 elements per thread, radix-4 passes, named barriers) measured
+// slower in both precisions (4.92 and 3.61 ms) and was dropped.
 #ifndef OTBL_PR_MB_D
 #define OTBL_PR_MB_D 1
 #endif
