@@ -45,17 +45,19 @@ struct XStream {
 // unbounded (56 registers).
 template <typename T>
 struct XTune;
-// tma: the TMA-fed kernels (k_xline_t) instead of the register streams; at
-// 1025x193x512 FP32 difvisxx 1.65 ms against 1.79, interpxx 1.04 against
-// 1.18; FP64 difvisxx 4.17 against 3.20 (its stages cap it at 5 CTAs/SM).
+// tma: the TMA-fed kernels (k_xline_t) instead of the register streams,
+// with segments of kti (interpxx) and ktd (difvisxx) planes; at 1025x193x512:
+// FP64 interpxx 1.17 ms (4 planes; 1.49 register-streamed), difvisxx 3.02
+// (6 planes; 3.18, and 4.17 at 8 planes); FP32 interpxx 0.87 (4 planes;
+// 1.18), difvisxx 1.70 (8 planes; 1.79).
 template <>
 struct XTune<double> {
-  static constexpr int kxi = 16, kxd = 8, minb_i = 8;
-  static constexpr bool tma = false;
+  static constexpr int kxi = 16, kxd = 8, minb_i = 8, kti = 4, ktd = 6;
+  static constexpr bool tma = true;
 };
 template <>
 struct XTune<float> {
-  static constexpr int kxi = 8, kxd = 8, minb_i = 1;  // 0.88 ms unbounded, 1.19 at >= 8 CTAs
+  static constexpr int kxi = 8, kxd = 8, minb_i = 1, kti = 4, ktd = 8;  // minb_i: 0.88 ms unbounded, 1.19 at >= 8
   static constexpr bool tma = true;
 };
 
@@ -218,12 +220,17 @@ __global__ void __launch_bounds__(128, 6) k_difvisx(DCoefT<T> c, XStream a) {
 // serial sweeps from shared memory. The sequence of segments is the forward
 // sweep (0..nseg-1) then the backward one (nseg-1..0). DV: difvisxx (inputs:
 // the product, FP32 on the mixed path, and the FP64 velocity) or interpxx
-// (input: the FP64 velocity). The arithmetic is k_interpx / k_difvisx's with
-// segments of K = 8.
+// (input: the FP64 velocity). The arithmetic is k_interpx / k_difvisx's,
+// with segments of K planes (XTune kti, ktd).
 // ---------------------------------------------------------------------------
+template <typename T, bool DV>
+constexpr int xseg() {
+  return DV ? XTune<T>::ktd : XTune<T>::kti;
+}
+
 template <typename T, bool DV, int TB>
 __global__ void __launch_bounds__(TB) k_xline_t(DCoefT<T> c, XStream a, int *err, const __grid_constant__ XMaps maps) {
-  constexpr int K = 8, NB = TB / 32;
+  constexpr int K = xseg<T, DV>(), NB = TB / 32;
   using TG = typename std::conditional<DV, T, double>::type;
   constexpr int GR = K + 1, UR = K + 2;
   constexpr int GBYTES = NB * GR * 32 * (int)sizeof(TG);
@@ -368,7 +375,7 @@ __global__ void __launch_bounds__(TB) k_xline_t(DCoefT<T> c, XStream a, int *err
 
 template <typename T, bool DV>
 static void xline_t_launch(otbl_ctx *c, const DCoefT<T> &dc, const XStream &a, const XMaps &m, int npmax) {
-  constexpr int K = 8;
+  constexpr int K = xseg<T, DV>();
   using TG = typename std::conditional<DV, T, double>::type;
   auto smem = [&](int tb) {
     const int nb = tb / 32;
@@ -414,7 +421,8 @@ static bool encode_lines(CUtensorMap *m, const void *base, size_t esz, int nx, i
 }
 
 bool build_x_maps(otbl_ctx *c) {
-  constexpr int K = 8;
+  const int KI = c->mixed ? xseg<float, false>() : xseg<double, false>();
+  const int KD = c->mixed ? xseg<float, true>() : xseg<double, true>();
   const int nx = c->cfg.nx, nz1 = c->dc.nz1, ny = c->cfg.ny;
   const int np[3] = {nz1 * (ny + 1), nz1 * ny, nz1 * (ny + 1)};
   const double *st[3] = {c->f[OTBL_F_U], c->f[OTBL_F_V], c->f[OTBL_F_W]};
@@ -422,10 +430,10 @@ bool build_x_maps(otbl_ctx *c) {
   const size_t ew = c->mixed ? sizeof(float) : sizeof(double);
   bool ok = true;
   for (int f = 0; f < 3 && ok; ++f) {
-    ok = ok && encode_lines(&c->xmi.g[f], st[f], 8, nx, np[f], K + 1);
+    ok = ok && encode_lines(&c->xmi.g[f], st[f], 8, nx, np[f], KI + 1);
     c->xmi.u[f] = c->xmi.g[f];  // unused by interpxx
-    ok = ok && encode_lines(&c->xmd.g[f], pr[f], ew, nx, np[f], K + 1);
-    ok = ok && encode_lines(&c->xmd.u[f], st[f], 8, nx, np[f], K + 2);
+    ok = ok && encode_lines(&c->xmd.g[f], pr[f], ew, nx, np[f], KD + 1);
+    ok = ok && encode_lines(&c->xmd.u[f], st[f], 8, nx, np[f], KD + 2);
   }
   c->xmaps_ok = ok;
   return ok;
