@@ -133,6 +133,111 @@ __global__ void __launch_bounds__(128) k_interpy(DCoefT<T> c, InterpyArgs a) {
   }
 }
 
+// interpyy fed by TMA: a CTA owns 128 consecutive kr of one plane of one
+// field; thread 0 loads, for the next segment of KYT rows, a box of 128 kr x
+// KYT+2 rows of the input into a two-stage shared-memory ring on mbarriers
+// (bounded waits); the segments run forward (0..nseg-1), then backward. The
+// arithmetic is k_interpy's with segments of KYT rows.
+template <typename T>
+struct YTune;
+template <>
+struct YTune<double> {
+  static constexpr int kt = 8;
+};
+template <>
+struct YTune<float> {
+  static constexpr int kt = 8;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(128) k_interpy_t(DCoefT<T> c, InterpyArgs a, int *err,
+                                                   const __grid_constant__ YMaps maps) {
+  constexpr int K = YTune<T>::kt, TB = 128, R = K + 2;
+  constexpr int STG = R * TB * 8;
+  constexpr unsigned TX = (unsigned)STG;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + 2 * STG);
+  const int f = blockIdx.z;
+  const int ny = c.ny, nz1 = c.nz1, ncol = c.nx * nz1;
+  const int t = threadIdx.x, kr0 = blockIdx.x * TB, kr = kr0 + t, i = blockIdx.y + 1;
+  const bool active = kr < nz1;
+  const int krc = active ? kr : 0;
+  const int which = pick3(a.which, f), jin = which == 0 ? ny + 1 : ny;
+  const CUtensorMap *mg = f == 0 ? &maps.g[0] : (f == 1 ? &maps.g[1] : &maps.g[2]);
+  const int nseg = (ny + K - 1) / K;
+  auto seg_of = [&](int it) { return it < nseg ? it : 2 * nseg - 1 - it; };
+  auto issue = [&](int stg, int sg) {
+    mbar_arrive_expect_tx(&bar[stg], TX);
+    tma_load_3d(smraw + stg * STG, mg, kr0, sg * K - 1, i - 1, &bar[stg]);
+  };
+  if (t == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_init_fence();
+  }
+  __syncthreads();
+  if (t == 0) issue(0, 0);
+  const size_t S = nz1;
+  const int col = (i - 1) * nz1 + krc;
+  const double *g = pick3(a.in, f) + (size_t)(i - 1) * jin * nz1 + krc;
+  T *o = static_cast<T *>(pick3(a.out, f)) + (size_t)(i - 1) * ny * nz1 + krc;
+  T *ck = reinterpret_cast<T *>(pick3(a.ck, f)) + col;
+  const T *iny = which == 0 ? c.inyu : c.inyv;
+  const T *econ = which == 0 ? c.cofiuy : c.cofivy;
+  const T *ib = c.inby;
+  auto G = [&](int r) { return (T)__ldg(g + (size_t)min(max(r, 0), jin - 1) * S); };
+  T b0 = T(0), bN;
+  if (which == 0) {
+    bN = M4(ib, 1, 1) * G(ny) + M4(ib, 1, 2) * G(ny - 1) + M4(ib, 1, 3) * G(ny - 2) + M4(ib, 1, 4) * G(ny - 3);
+  } else {
+    b0 = M4(ib, 3, 1) * G(0) + M4(ib, 3, 2) * G(1) + M4(ib, 3, 3) * G(2) + M4(ib, 3, 4) * G(3);
+    bN = M4(ib, 4, 1) * G(ny - 1) + M4(ib, 4, 2) * G(ny - 2) + M4(ib, 4, 3) * G(ny - 3) + M4(ib, 4, 4) * G(ny - 4);
+  }
+  auto rhs = [&](int r, T gm, T g0, T gp) {
+    const T e1 = __ldg(econ + 2 * r), e2 = __ldg(econ + 2 * r + 1);
+    const T in = which == 0 ? e1 * g0 + e2 * gp : e2 * g0 + e1 * gm;
+    return r == 0 ? b0 : (r == ny - 1 ? bN : in);
+  };
+  T y = T(0), x = T(0);
+  for (int it = 0; it < 2 * nseg; ++it) {
+    const int stg = it & 1;
+    const bool ok = mbar_wait_bounded(&bar[stg], (it >> 1) & 1, 2000000000ull);
+    if (__syncthreads_or(!ok)) {
+      if (t == 0) atomicExch(err, OTBL_ERR_TIMEOUT);
+      return;
+    }
+    if (t == 0 && it + 1 < 2 * nseg) issue(stg ^ 1, seg_of(it + 1));
+    if (!active) continue;
+    const int sg = seg_of(it), s0 = sg * K;
+    const double *gs = reinterpret_cast<const double *>(smraw + stg * STG) + t;
+    auto gv = [&](int b) { return (T)gs[b * TB]; };  // row s0 - 1 + b
+    if (it < nseg) {
+      ck[(size_t)sg * ncol] = y;
+#pragma unroll
+      for (int b = 0; b < K; ++b) {
+        const int r = s0 + b;
+        if (r < ny) y = rhs(r, gv(b), gv(b + 1), gv(b + 2)) + (r > 0 ? __ldg(iny + 3 * r) : T(0)) * y;
+      }
+    } else {
+      T yy = ck[(size_t)sg * ncol], yv[K];
+#pragma unroll
+      for (int b = 0; b < K; ++b) {
+        const int r = s0 + b;
+        if (r < ny) yy = rhs(r, gv(b), gv(b + 1), gv(b + 2)) + (r > 0 ? __ldg(iny + 3 * r) : T(0)) * yy;
+        yv[b] = yy;
+      }
+#pragma unroll
+      for (int b = K - 1; b >= 0; --b) {
+        const int r = s0 + b;
+        if (r < ny) {
+          x = (yv[b] - __ldg(iny + 3 * r + 2) * x) * __ldg(iny + 3 * r + 1);
+          o[(size_t)r * S] = x;
+        }
+      }
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // tail of rhsp (rhsp.F90:291-484) for planes 2..nx, one velocity component
 // per launch pair: RHS assembly, pressure gradient, boun, vistyy, RK3
@@ -774,7 +879,18 @@ cudaError_t launch_interpy(otbl_ctx *c) {
   const int ncol = c->cfg.nx * c->dc.nz1;
   prof_begin(c, PK_INTERPY);
   const int bs = c->tune_bs[2];
-  if (c->mixed)
+  if (c->ymaps_ok) {
+    const dim3 gt((c->dc.nz1 + 127) / 128, c->cfg.nx, 3);
+    if (c->mixed) {
+      const int sm = 2 * (YTune<float>::kt + 2) * 128 * 8 + 128;
+      cudaFuncSetAttribute(k_interpy_t<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+      k_interpy_t<float><<<gt, 128, sm, c->stream>>>(c->dcf, a, &c->st->err, c->ymi);
+    } else {
+      const int sm = 2 * (YTune<double>::kt + 2) * 128 * 8 + 128;
+      cudaFuncSetAttribute(k_interpy_t<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+      k_interpy_t<double><<<gt, 128, sm, c->stream>>>(c->dc, a, &c->st->err, c->ymi);
+    }
+  } else if (c->mixed)
     k_interpy<float><<<dim3((ncol + bs - 1) / bs, 3), bs, 0, c->stream>>>(c->dcf, a);
   else
     k_interpy<double><<<dim3((ncol + bs - 1) / bs, 3), bs, 0, c->stream>>>(c->dc, a);
@@ -836,6 +952,17 @@ static bool build_maps_t(otbl_ctx *c) {
     ok = ok && encode_field(&m.hp, hp, 8, nx, jee, nz1, KF, 1);
     ok = ok && encode_field(&m.p, c->f[OTBL_F_P], 8, nx, ny, nz1, comp == 1 ? KF + 1 : KF, comp == 0 ? 2 : 1);
   }
+  return ok;
+}
+
+bool build_y_maps(otbl_ctx *c) {
+  const int K = c->mixed ? YTune<float>::kt : YTune<double>::kt;
+  const int nx = c->cfg.nx, ny = c->cfg.ny, nz1 = c->dc.nz1;
+  const double *in[3] = {c->f[OTBL_F_U], c->f[OTBL_F_W], c->f[OTBL_F_V]};
+  const int rows[3] = {ny + 1, ny + 1, ny};
+  bool ok = true;
+  for (int f = 0; f < 3 && ok; ++f) ok = encode_field(&c->ymi.g[f], in[f], 8, nx, rows[f], nz1, K + 2, 1);
+  c->ymaps_ok = ok;
   return ok;
 }
 

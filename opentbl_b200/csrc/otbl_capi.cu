@@ -220,6 +220,7 @@ extern "C" int otbl_ctx_create(const otbl_config *cfg, const double *coef, int d
   if (!getenv("OTBL_NO_TMA")) {
     build_final_maps(c);
     build_x_maps(c);
+    build_y_maps(c);
   }
   if (check(c, launch_twiddles(c), "twiddles") != OTBL_OK || check(c, launch_pois_lu(c), "pois_lu") != OTBL_OK || check(c, cudaStreamSynchronize(c->stream), "init")) {
     *out = c;

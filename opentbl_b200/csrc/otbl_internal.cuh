@@ -73,6 +73,11 @@ struct FinalMaps {
   CUtensorMap prod, kp, vel, cx, hp, p;
 };
 
+// TMA descriptors of interpyy's inputs (u, w, v), boxes of 128 kr x rows
+struct YMaps {
+  CUtensorMap g[3];
+};
+
 // TMA descriptors of the x-line kernels' inputs, per field (u, v, w): 2D
 // tensors [plane][line] with boxes of 32 lines
 struct XMaps {
@@ -96,6 +101,8 @@ struct otbl_ctx {
   bool fmaps_ok = false;
   otbl::XMaps xmi, xmd;  // k_interpx_t (state), k_difvisx_t (products, state)
   bool xmaps_ok = false;
+  otbl::YMaps ymi;       // k_interpy_t
+  bool ymaps_ok = false;
   int mixed;                // cfg.precision == OTBL_PREC_MIXED
   double *coef_dev;
   float *coef_dev_f;
@@ -157,6 +164,7 @@ cudaError_t launch_energies(otbl_ctx *c);
 // pitch that is not a multiple of 16 bytes)
 bool build_final_maps(otbl_ctx *c);
 bool build_x_maps(otbl_ctx *c);
+bool build_y_maps(otbl_ctx *c);
 cudaError_t launch_twiddles(otbl_ctx *c);
 cudaError_t launch_pois_lu(otbl_ctx *c);
 cudaError_t launch_pois_solve(otbl_ctx *c, double *phi);
