@@ -937,7 +937,8 @@ struct XTab {
 // 256 threads. The loads and stores walk the planes with the MB modes of a
 // plane on consecutive threads (MB x 16 contiguous bytes per plane row); the
 // MB complex lines of length n = nx-1 sit in padded shared memory (line
-// stride xpad(n)) and are transformed together, 256/MB threads per line.
+// stride xpad(n) | 1, odd, so that the MB lines of one plane fall in
+// different banks) and are transformed together, 256/MB threads per line.
 // MB is chosen per n so that n * MB <= 4096 (n = 1024: 4 modes, 74 KB).
 
 // divergence (pois.f90:41-54) + DCT-II along x (cosftx iopt=-1); output
@@ -948,7 +949,7 @@ __global__ void __launch_bounds__(256) k_pois_fwd(DCoef c, XTab x, const double 
                                                  const double *__restrict__ v, const double *__restrict__ w,
                                                  double *__restrict__ phi) {
   extern __shared__ double2 xsm[];
-  const int n = x.n, ld = xpad(n), ny = c.ny, nz1 = c.nz1, nz2 = c.nz2, xr = c.xround;
+  const int n = x.n, ld = xpad(n) | 1, ny = c.ny, nz1 = c.nz1, nz2 = c.nz2, xr = c.xround;
   const int j = blockIdx.y + 1;
   const int k0 = blockIdx.x * MB;
   const size_t PU = (size_t)(ny + 1) * nz1, PV = (size_t)ny * nz1;
@@ -998,7 +999,7 @@ __global__ void __launch_bounds__(256) k_pois_fwd(DCoef c, XTab x, const double 
 template <int MB>
 __global__ void __launch_bounds__(256) k_pois_bwd(DCoef c, XTab x, double *__restrict__ phi) {
   extern __shared__ double2 xsm[];
-  const int n = x.n, ld = xpad(n), ny = c.ny, nz1 = c.nz1, nz2 = c.nz2, xr = c.xround;
+  const int n = x.n, ld = xpad(n) | 1, ny = c.ny, nz1 = c.nz1, nz2 = c.nz2, xr = c.xround;
   const int j = blockIdx.y + 1;
   const int k0 = blockIdx.x * MB;
   const size_t PV = (size_t)ny * nz1;
@@ -1417,7 +1418,7 @@ cudaError_t launch_pois(otbl_ctx *c, int m) {
   const int n = nx - 1;
   // modes per CTA: n * MB <= 4096 and at most 8
   const int MB = n <= 512 ? 8 : (n <= 1024 ? 4 : (n <= 2048 ? 2 : 1));
-  const size_t smem = (size_t)MB * xpad_host(n) * sizeof(double2);
+  const size_t smem = (size_t)MB * (xpad_host(n) | 1) * sizeof(double2);
   double *phi = c->w.s2;
   dim3 gx((nz2 + 1 + MB - 1) / MB, ny - 1);
   auto fwd = [&](auto kf) {
