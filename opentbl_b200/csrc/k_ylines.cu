@@ -44,15 +44,17 @@ struct FinalTune;
 #ifndef OTBL_FT_TK
 #define OTBL_FT_TK 2
 #endif
+// tma_a: pass A fed by TMA too (k_final_ta; FP32 inputs 5.25 against 5.33
+// ms; FP64 6.50 against 5.94, so FP64 keeps the register-streamed pass A)
 template <>
 struct FinalTune<double> {
   static constexpr int kf = OTBL_FT_DK, minb = OTBL_FT_DM, kf_tma = OTBL_FT_TK;
-  static constexpr bool split = false;
+  static constexpr bool split = false, tma_a = false;
 };
 template <>
 struct FinalTune<float> {
   static constexpr int kf = OTBL_FT_FK, minb = OTBL_FT_FM, kf_tma = OTBL_FT_TK;
-  static constexpr bool split = true;
+  static constexpr bool split = true, tma_a = true;
 };
 
 // interpyy, which 0: u, w (in rows ny+1), which 1: v (in rows ny); out rows
@@ -773,6 +775,104 @@ __global__ void __launch_bounds__(128) k_final_tb(DCoef c, FinalStream<W> fs, in
   }
 }
 
+// Pass A of the rhsp tail fed by TMA: the same ring as k_final_tb, ascending,
+// with boxes of 128 columns x KA+2 rows of the product and the velocity
+// (KA = 8 rows per stage); the checkpoints are still written every KF rows
+// of k_final_tb's segments. The arithmetic is k_final_s1's pass A.
+template <int COMP, typename W>
+__global__ void __launch_bounds__(128) k_final_ta(DCoef c, FinalStream<W> fs, int *err,
+                                                  const __grid_constant__ FinalMaps maps) {
+  constexpr int KF = FinalTune<W>::kf_tma, KA = 8, TB = 128, R = KA + 2;
+  constexpr int PB = (R * TB * (int)sizeof(W) + 127) / 128 * 128;
+  constexpr int STG = PB + R * TB * 8;
+  constexpr unsigned TX = (unsigned)(R * TB * sizeof(W) + R * TB * 8);
+  extern __shared__ __align__(128) unsigned char smraw[];
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + 2 * STG);
+  const FinalArgs<W> &a = fs.a;
+  const int nx = c.nx, ny = c.ny, nz1 = c.nz1;
+  const int ncol = (nx - 1) * nz1;
+  const int t = threadIdx.x;
+  const int i = blockIdx.y + 2, kr0 = blockIdx.x * TB, kr = kr0 + t;
+  const bool active = kr < nz1;
+  const int krc = active ? kr : 0;
+  const int col = (i - 2) * nz1 + krc;
+  const bool last = i == nx;
+  const int jee = COMP == 1 ? ny : ny + 1;
+  const int nst = (jee + KA - 1) / KA;
+  auto issue = [&](int stg, int sa) {
+    unsigned char *b = smraw + stg * STG;
+    mbar_arrive_expect_tx(&bar[stg], TX);
+    tma_load_3d(b, &maps.prod_a, kr0, sa * KA - 1, i - 1, &bar[stg]);
+    tma_load_3d(b + PB, &maps.vel_a, kr0, sa * KA - 1, i - 1, &bar[stg]);
+  };
+  if (t == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_init_fence();
+  }
+  __syncthreads();
+  if (t == 0) issue(0, 0);
+  const size_t PU = (size_t)(ny + 1) * nz1, PV = (size_t)ny * nz1;
+  const size_t pl = (size_t)(i - 1) * (COMP == 1 ? PV : PU), plv = (size_t)(i - 1) * PV;
+  const size_t S = nz1;
+  const W *prod = (COMP == 0 ? a.uv : (COMP == 1 ? a.vv : a.vw)) + plv + krc;
+  const double *vel = (COMP == 0 ? a.u : (COMP == 1 ? a.v : a.w)) + pl + krc;
+  const int which = COMP == 1 ? 1 : 0;
+  const double *dcy = which == 0 ? c.dcyu : c.dcyv, *ecd = which == 0 ? c.cofcyu : c.cofcyv;
+  const double *viy = which == 0 ? c.viyu : c.viyv, *ecv = which == 0 ? c.cofvyu : c.cofvyv;
+  auto Pg = [&](int r) { return (double)__ldg(prod + (size_t)min(max(r, 0), ny - 1) * S); };
+  auto Vg = [&](int r) { return __ldg(vel + (size_t)min(max(r, 0), jee - 1) * S); };
+  const int chv = which == 0 ? 3 : 1, cha = chv + 1, ic = which == 0 ? 3 : 1;
+  const double *db = c.dcby, *vb = c.cofvby;
+  double bot = 0.0, top = 0.0;
+  if (!last) {
+    bot = M4(db, chv, 1) * Pg(0) + M4(db, chv, 2) * Pg(1) + M4(db, chv, 3) * Pg(2) + M4(db, chv, 4) * Pg(3);
+    top = M4(db, cha, 1) * Pg(ny - 1) + M4(db, cha, 2) * Pg(ny - 2) + M4(db, cha, 3) * Pg(ny - 3) +
+          M4(db, cha, 4) * Pg(ny - 4);
+  }
+  const double b0 = M4(vb, ic, 1) * Vg(0) + M4(vb, ic, 2) * Vg(1) + M4(vb, ic, 3) * Vg(2) + M4(vb, ic, 4) * Vg(3);
+  const double bN = M4(vb, ic + 1, 1) * Vg(jee - 1) + M4(vb, ic + 1, 2) * Vg(jee - 2) +
+                    M4(vb, ic + 1, 3) * Vg(jee - 3) + M4(vb, ic + 1, 4) * Vg(jee - 4);
+  auto rd = [&](int r, double gm, double g0, double gp) {
+    const double in = which == 0 ? __ldg(ecd + 2 * r + 1) * g0 + __ldg(ecd + 2 * r) * gm
+                                 : __ldg(ecd + 2 * r + 1) * gp + __ldg(ecd + 2 * r) * g0;
+    return r == 0 ? bot : (r == jee - 1 ? top : in);
+  };
+  auto rv = [&](int r, double um, double u0, double up) {
+    const double in = __ldg(ecv + 3 * r) * up + __ldg(ecv + 3 * r + 1) * u0 + __ldg(ecv + 3 * r + 2) * um;
+    return r == 0 ? b0 : (r == jee - 1 ? bN : in);
+  };
+  double *ck = fs.ck + col;
+  double yd = 0.0, yv = 0.0;
+  for (int sa = 0; sa < nst; ++sa) {
+    const int stg = sa & 1;
+    const bool ok = mbar_wait_bounded(&bar[stg], (sa >> 1) & 1, 2000000000ull);
+    if (__syncthreads_or(!ok)) {
+      if (t == 0) atomicExch(err, OTBL_ERR_TIMEOUT);
+      return;
+    }
+    if (t == 0 && sa + 1 < nst) issue(stg ^ 1, sa + 1);
+    if (!active) continue;
+    const W *sp = reinterpret_cast<const W *>(smraw + stg * STG) + t;
+    const double *sv = reinterpret_cast<const double *>(smraw + stg * STG + PB) + t;
+    const int s0 = sa * KA;
+#pragma unroll
+    for (int b = 0; b < KA; ++b) {
+      const int r = s0 + b;
+      if (b % KF == 0 && r < jee) {  // y of row r-1 at the start of segment r/KF
+        ck[(size_t)(2 * (r / KF)) * ncol] = yd;
+        ck[(size_t)(2 * (r / KF) + 1) * ncol] = yv;
+      }
+      if (r < jee) {
+        if (!last)
+          yd = rd(r, (double)sp[b * TB], (double)sp[(b + 1) * TB], (double)sp[(b + 2) * TB]) +
+               (r > 0 ? __ldg(dcy + 3 * r) : 0.0) * yd;
+        yv = rv(r, sv[b * TB], sv[(b + 1) * TB], sv[(b + 2) * TB]) + (r > 0 ? __ldg(viy + 3 * r) : 0.0) * yv;
+      }
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // pois.f90:106-117 + soltriy: tridiagonal in y per (x-mode, kz). The LU of
 // each (i, k) system depends only on the grid, so its pivots are computed
@@ -946,6 +1046,8 @@ static bool build_maps_t(otbl_ctx *c) {
     const void *cx = comp == 0 ? c->w.cu : (comp == 1 ? c->w.cv : c->w.cw);
     const double *hp = c->f[comp == 0 ? OTBL_F_RHSUPA : (comp == 1 ? OTBL_F_RHSVPA : OTBL_F_RHSWPA)];
     ok = ok && encode_field(&m.prod, prod, ew, nx, ny, nz1, KF + 2, 1);
+    ok = ok && encode_field(&m.prod_a, prod, ew, nx, ny, nz1, 8 + 2, 1);
+    ok = ok && encode_field(&m.vel_a, vel, 8, nx, jee, nz1, 8 + 2, 1);
     ok = ok && encode_field(&m.kp, kp, ew, nx, kprows, nz1, KF, 1);
     ok = ok && encode_field(&m.vel, vel, 8, nx, jee, nz1, KF + 2, 1);
     ok = ok && encode_field(&m.cx, cx, ew, nx, jee, nz1, KF, 1);
@@ -1005,8 +1107,14 @@ static int final_t(otbl_ctx *c) {
     constexpr int K = decltype(C)::value;
     const int smem_t = FinalBox<W, K>::smem;
     if (tma) {
-      // pass A, then the TMA-fed pass B
-      k_final_s1<K, W, 1, FinalTune<W>::kf_tma><<<g, 128, 0, c->stream>>>(c->dc, fs);
+      // pass A (register-streamed or TMA-fed), then the TMA-fed pass B
+      if constexpr (FinalTune<W>::tma_a) {
+        constexpr int sma = 2 * ((10 * 128 * (int)sizeof(W) + 127) / 128 * 128 + 10 * 128 * 8) + 128;
+        cudaFuncSetAttribute(k_final_ta<K, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, sma);
+        k_final_ta<K, W><<<gt, 128, sma, c->stream>>>(c->dc, fs, &c->st->err, c->fmaps[K]);
+      } else {
+        k_final_s1<K, W, 1, FinalTune<W>::kf_tma><<<g, 128, 0, c->stream>>>(c->dc, fs);
+      }
       cudaFuncSetAttribute(k_final_tb<K, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_t);
       k_final_tb<K, W><<<gt, 128, smem_t, c->stream>>>(c->dc, fs, &c->st->err, c->fmaps[K]);
     } else if constexpr (FinalTune<W>::split) {

@@ -71,6 +71,7 @@ struct Work {
 // rhsp tail's descending pass reads, for one velocity component (k_final_tb)
 struct FinalMaps {
   CUtensorMap prod, kp, vel, cx, hp, p;
+  CUtensorMap prod_a, vel_a;  // pass A: boxes of 8 + 2 rows
 };
 
 // TMA descriptors of interpyy's inputs (u, w, v), boxes of 128 kr x rows
