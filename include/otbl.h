@@ -48,11 +48,14 @@ extern "C" {
 
 /* arithmetic of the substep (no counterpart in the reference, which is FP64
  * throughout). OTBL_PREC_FP64: every operator in FP64. OTBL_PREC_MIXED: the
- * state (u, v, w, p, rhs*pa), the RK3 combination, implzy, the Poisson solve,
- * the projection, dt, genflu and the energies stay FP64; the x and y
- * mid-point interpolations, d/dx of difvisxx, the spanwise FFTs and the
- * nonlinear products run in FP32, and the fifteen intermediate fields they
- * exchange are stored in FP32. Not combined with OTBL_XPOSE_FP32. */
+ * velocity (u, v, w), the RK3 combination, implzy, the Poisson solve, the
+ * projection, dt, genflu and the energies stay FP64; the x and y mid-point
+ * interpolations, d/dx of difvisxx, the spanwise FFTs and the nonlinear
+ * products run in FP32, and the fifteen intermediate fields they exchange,
+ * the pressure p and the RHS history rhs*pa are stored in FP32 (their
+ * updates computed in FP64). otbl_set_field / otbl_get_field convert those
+ * fields from and to the caller's FP64 arrays; otbl_field_device_ptr refuses
+ * them (OTBL_ERR_CONFIG). Not combined with OTBL_XPOSE_FP32. */
 #define OTBL_PREC_FP64 0
 #define OTBL_PREC_MIXED 1
 

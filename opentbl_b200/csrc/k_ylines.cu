@@ -245,13 +245,14 @@ __global__ void __launch_bounds__(128) k_interpy_t(DCoefT<T> c, InterpyArgs a, i
 // per launch pair: RHS assembly, pressure gradient, boun, vistyy, RK3
 // combination, rhs history, implzy.
 // ---------------------------------------------------------------------------
-// W: element type of the difvisxx outputs and the products (float on the
-// mixed path); the arithmetic is FP64 throughout.
+// W: element type of the difvisxx outputs, the products, the pressure and
+// the RHS history (float on the mixed path); the arithmetic is FP64
+// throughout.
 template <typename W>
 struct FinalArgs {
   double *u, *v, *w;                 // state: old on entry, new on exit
-  const double *p;
-  double *rhsupa, *rhsvpa, *rhswpa;  // old on entry, new on exit
+  const W *p;                        // p and the RHS history: W as well
+  W *rhsupa, *rhsvpa, *rhswpa;       // old on entry, new on exit
   const W *cu, *cv, *cw;             // difvisxx outputs
   const W *uv, *uw, *vw, *vv, *ww;
   const double *fac_u, *fac_v;
@@ -309,8 +310,8 @@ __global__ void __launch_bounds__(128, PASSES == 1 ? 6 : FinalTune<W>::minb)
   const W *kp = (COMP == 0 ? a.uw : (COMP == 1 ? a.vw : a.ww)) + (COMP == 0 ? pl : plv) + kr + pof;
   double *vel = (COMP == 0 ? a.u : (COMP == 1 ? a.v : a.w)) + pl + kr;
   const W *cX = (COMP == 0 ? a.cu : (COMP == 1 ? a.cv : a.cw)) + pl + kr;
-  double *hp = (COMP == 0 ? a.rhsupa : (COMP == 1 ? a.rhsvpa : a.rhswpa)) + pl + kr;
-  const double *pc = a.p + plv + kr;
+  W *hp = (COMP == 0 ? a.rhsupa : (COMP == 1 ? a.rhsvpa : a.rhswpa)) + pl + kr;
+  const W *pc = a.p + plv + kr;
   const double kz = c.kaz[k], kv = c.kvis[k];
   const double var1 = a.st->var1, var3 = a.st->var3, var4 = a.st->var4;
   const double v2 = last ? 0.0 : a.st->var2;
@@ -328,10 +329,12 @@ __global__ void __launch_bounds__(128, PASSES == 1 ? 6 : FinalTune<W>::minb)
   auto star = [&](int r, double o) -> double {
     const int rp = min(r, ny - 1);
     if (COMP == 0)
-      return last ? o : o - var1 * idxx * (__ldg(pc + PV + (size_t)rp * S) - __ldg(pc + (size_t)rp * S));
+      return last ? o
+                  : o - var1 * idxx * ((double)__ldg(pc + PV + (size_t)rp * S) - (double)__ldg(pc + (size_t)rp * S));
     if (COMP == 1)
-      return o - var1 * c.idyy[r] * (__ldg(pc + (size_t)min(r + 1, ny - 1) * S) - __ldg(pc + (size_t)rp * S));
-    const double pp = __ldg(pc + (size_t)rp * S + pof);
+      return o - var1 * c.idyy[r] *
+                     ((double)__ldg(pc + (size_t)min(r + 1, ny - 1) * S) - (double)__ldg(pc + (size_t)rp * S));
+    const double pp = (double)__ldg(pc + (size_t)rp * S + pof);
     const double av = var1 * kz;
     return o - (odd ? av * pp : -av * pp);
   };
@@ -429,7 +432,7 @@ __global__ void __launch_bounds__(128, PASSES == 1 ? 6 : FinalTune<W>::minb)
       const int rr = min(s0 + b, jee - 1);
       cxv[b] = (double)__ldg(cX + (size_t)rr * S);
       kpv[b] = last ? 0.0 : (double)__ldg(kp + (size_t)min(rr, krows - 1) * S);
-      hv[b] = __ldg(hp + (size_t)rr * S);
+      hv[b] = (double)__ldg(hp + (size_t)rr * S);
     }
 #pragma unroll
     for (int b = KF - 1; b >= 0; --b) {
@@ -471,7 +474,7 @@ __global__ void __launch_bounds__(128, PASSES == 1 ? 6 : FinalTune<W>::minb)
       // RK3 combination and the new RHS history (rhsp.F90:448-475)
       const double st = r == 0 ? ub1 : (r == jee - 1 ? ubt : star(r, u0));
       const double res = st - (var3 * R + v2 * xv + var4 * hv[b]);
-      hp[(size_t)r * S] = R;
+      hp[(size_t)r * S] = (W)R;
       // implzy right-hand side of row q = r from rows r..r+2 (lip.f90:528-597)
       if (r < n) {
         double v = __ldg(vyi + 3 * (r + 1)) * res + __ldg(vyi + 3 * (r + 1) + 1) * res1 +
@@ -540,19 +543,19 @@ __global__ void __launch_bounds__(128) k_final_s2(DCoef c, double *u, double *v,
 // ---------------------------------------------------------------------------
 template <typename W, int COMP>
 struct FinalBox {
-  static constexpr int KF = FinalTune<W>::kf_tma, T = 128;
+  static constexpr int KF = FinalTune<W>::kf_tma, T = 128, E = (int)sizeof(W);
   // pressure box: u needs planes i, i+1 on rows s0..s0+KF-1, v rows
   // s0..s0+KF of plane i, w rows s0..s0+KF-1 of plane i
   static constexpr int PR = COMP == 1 ? KF + 1 : KF, PP = COMP == 0 ? 2 : 1;
-  static constexpr int prod = 0;                                            // W (KF+2) rows
-  static constexpr int vel = prod + ((KF + 2) * T * (int)sizeof(W) + 127) / 128 * 128;  // double (KF+2)
-  static constexpr int cx = vel + (KF + 2) * T * 8;                         // W KF rows
-  static constexpr int kp = cx + (KF * T * (int)sizeof(W) + 127) / 128 * 128;  // W KF rows
-  static constexpr int hp = kp + (KF * T * (int)sizeof(W) + 127) / 128 * 128;  // double KF rows
-  static constexpr int p = hp + KF * T * 8;                                 // double PR x PP
-  static constexpr int stage = p + PR * PP * T * 8;
-  static constexpr unsigned tx = (unsigned)((KF + 2) * T * sizeof(W) + (KF + 2) * T * 8 + 2 * KF * T * sizeof(W) +
-                                            KF * T * 8 + PR * PP * T * 8);
+  static constexpr int r128(int b) { return (b + 127) / 128 * 128; }
+  static constexpr int prod = 0;                              // W (KF+2) rows
+  static constexpr int vel = prod + r128((KF + 2) * T * E);   // double (KF+2) rows
+  static constexpr int cx = vel + (KF + 2) * T * 8;           // W KF rows
+  static constexpr int kp = cx + r128(KF * T * E);            // W KF rows
+  static constexpr int hp = kp + r128(KF * T * E);            // W KF rows
+  static constexpr int p = hp + r128(KF * T * E);             // W PR x PP
+  static constexpr int stage = p + r128(PR * PP * T * E);
+  static constexpr unsigned tx = (unsigned)((KF + 2) * T * E + (KF + 2) * T * 8 + 3 * KF * T * E + PR * PP * T * E);
   static constexpr int smem = 2 * stage + 128;  // two stages and the barriers
 };
 
@@ -601,8 +604,8 @@ __global__ void __launch_bounds__(128) k_final_tb(DCoef c, FinalStream<W> fs, in
   const int krc = active ? kr : 0;  // inactive threads read a valid column and write nothing
   const W *prod = (COMP == 0 ? a.uv : (COMP == 1 ? a.vv : a.vw)) + plv + krc;
   const double *vel = (COMP == 0 ? a.u : (COMP == 1 ? a.v : a.w)) + pl + krc;
-  double *hp = (COMP == 0 ? a.rhsupa : (COMP == 1 ? a.rhsvpa : a.rhswpa)) + pl + krc;
-  const double *pc = a.p + plv + krc;
+  W *hp = (COMP == 0 ? a.rhsupa : (COMP == 1 ? a.rhsvpa : a.rhswpa)) + pl + krc;
+  const W *pc = a.p + plv + krc;
   const double kz = c.kaz[k], kv = c.kvis[k];
   const double var1 = a.st->var1, var3 = a.st->var3, var4 = a.st->var4;
   const double v2 = last ? 0.0 : a.st->var2;
@@ -621,10 +624,12 @@ __global__ void __launch_bounds__(128) k_final_tb(DCoef c, FinalStream<W> fs, in
   auto star_g = [&](int r, double o) -> double {
     const int rp = min(r, ny - 1);
     if (COMP == 0)
-      return last ? o : o - var1 * idxx * (__ldg(pc + PV + (size_t)rp * S) - __ldg(pc + (size_t)rp * S));
+      return last ? o
+                  : o - var1 * idxx * ((double)__ldg(pc + PV + (size_t)rp * S) - (double)__ldg(pc + (size_t)rp * S));
     if (COMP == 1)
-      return o - var1 * c.idyy[r] * (__ldg(pc + (size_t)min(r + 1, ny - 1) * S) - __ldg(pc + (size_t)rp * S));
-    const double pp = __ldg(pc + (size_t)rp * S + pof);
+      return o - var1 * c.idyy[r] *
+                     ((double)__ldg(pc + (size_t)min(r + 1, ny - 1) * S) - (double)__ldg(pc + (size_t)rp * S));
+    const double pp = (double)__ldg(pc + (size_t)rp * S + pof);
     const double av = var1 * kz;
     return o - (odd ? av * pp : -av * pp);
   };
@@ -680,8 +685,8 @@ __global__ void __launch_bounds__(128) k_final_tb(DCoef c, FinalStream<W> fs, in
     const double *sv = reinterpret_cast<const double *>(bs + B::vel);
     const W *sc = reinterpret_cast<const W *>(bs + B::cx);
     const W *sk = reinterpret_cast<const W *>(bs + B::kp);
-    const double *sh = reinterpret_cast<const double *>(bs + B::hp);
-    const double *spp = reinterpret_cast<const double *>(bs + B::p);
+    const W *sh = reinterpret_cast<const W *>(bs + B::hp);
+    const W *spp = reinterpret_cast<const W *>(bs + B::p);
     double ad = ckd, av = ckv;
     if (sg >= 1) {  // next segment's checkpoints, ahead of use
       ckd = ck[(size_t)(2 * (sg - 1)) * ncol];
@@ -747,16 +752,16 @@ __global__ void __launch_bounds__(128) k_final_tb(DCoef c, FinalStream<W> fs, in
       } else if (r == jee - 1) {
         st = ubt;
       } else if (COMP == 0) {
-        st = last ? u0 : u0 - var1 * idxx * (spp[(B::PR + b) * TB + t] - spp[b * TB + t]);
+        st = last ? u0 : u0 - var1 * idxx * ((double)spp[(B::PR + b) * TB + t] - (double)spp[b * TB + t]);
       } else if (COMP == 1) {
-        st = u0 - var1 * c.idyy[r] * (spp[(b + 1) * TB + t] - spp[b * TB + t]);
+        st = u0 - var1 * c.idyy[r] * ((double)spp[(b + 1) * TB + t] - (double)spp[b * TB + t]);
       } else {
-        const double pp = spp[b * TB + tk];
+        const double pp = (double)spp[b * TB + tk];
         const double avz = var1 * kz;
         st = u0 - (odd ? avz * pp : -avz * pp);
       }
-      const double res = st - (var3 * R + v2 * xv + var4 * sh[b * TB + t]);
-      hp[(size_t)r * S] = R;
+      const double res = st - (var3 * R + v2 * xv + var4 * (double)sh[b * TB + t]);
+      hp[(size_t)r * S] = (W)R;
       if (r < n) {
         double v = __ldg(vyi + 3 * (r + 1)) * res + __ldg(vyi + 3 * (r + 1) + 1) * res1 +
                    __ldg(vyi + 3 * (r + 1) + 2) * res2;
@@ -1044,15 +1049,15 @@ static bool build_maps_t(otbl_ctx *c) {
     const int kprows = comp == 0 ? ny + 1 : ny;
     const double *vel = c->f[comp == 0 ? OTBL_F_U : (comp == 1 ? OTBL_F_V : OTBL_F_W)];
     const void *cx = comp == 0 ? c->w.cu : (comp == 1 ? c->w.cv : c->w.cw);
-    const double *hp = c->f[comp == 0 ? OTBL_F_RHSUPA : (comp == 1 ? OTBL_F_RHSVPA : OTBL_F_RHSWPA)];
+    const void *hp = c->f[comp == 0 ? OTBL_F_RHSUPA : (comp == 1 ? OTBL_F_RHSVPA : OTBL_F_RHSWPA)];
     ok = ok && encode_field(&m.prod, prod, ew, nx, ny, nz1, KF + 2, 1);
     ok = ok && encode_field(&m.prod_a, prod, ew, nx, ny, nz1, 8 + 2, 1);
     ok = ok && encode_field(&m.vel_a, vel, 8, nx, jee, nz1, 8 + 2, 1);
     ok = ok && encode_field(&m.kp, kp, ew, nx, kprows, nz1, KF, 1);
     ok = ok && encode_field(&m.vel, vel, 8, nx, jee, nz1, KF + 2, 1);
     ok = ok && encode_field(&m.cx, cx, ew, nx, jee, nz1, KF, 1);
-    ok = ok && encode_field(&m.hp, hp, 8, nx, jee, nz1, KF, 1);
-    ok = ok && encode_field(&m.p, c->f[OTBL_F_P], 8, nx, ny, nz1, comp == 1 ? KF + 1 : KF, comp == 0 ? 2 : 1);
+    ok = ok && encode_field(&m.hp, hp, ew, nx, jee, nz1, KF, 1);
+    ok = ok && encode_field(&m.p, c->f[OTBL_F_P], ew, nx, ny, nz1, comp == 1 ? KF + 1 : KF, comp == 0 ? 2 : 1);
   }
   return ok;
 }
@@ -1080,10 +1085,10 @@ static int final_t(otbl_ctx *c) {
   a.u = c->f[OTBL_F_U];
   a.v = c->f[OTBL_F_V];
   a.w = c->f[OTBL_F_W];
-  a.p = c->f[OTBL_F_P];
-  a.rhsupa = c->f[OTBL_F_RHSUPA];
-  a.rhsvpa = c->f[OTBL_F_RHSVPA];
-  a.rhswpa = c->f[OTBL_F_RHSWPA];
+  a.p = reinterpret_cast<const W *>(c->f[OTBL_F_P]);
+  a.rhsupa = reinterpret_cast<W *>(c->f[OTBL_F_RHSUPA]);
+  a.rhsvpa = reinterpret_cast<W *>(c->f[OTBL_F_RHSVPA]);
+  a.rhswpa = reinterpret_cast<W *>(c->f[OTBL_F_RHSWPA]);
   a.cu = static_cast<const W *>(c->w.cu);
   a.cv = static_cast<const W *>(c->w.cv);
   a.cw = static_cast<const W *>(c->w.cw);

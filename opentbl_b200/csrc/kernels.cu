@@ -605,7 +605,9 @@ __global__ void k_tiempo(DState *st) {
 // of a single sequential pass.
 // ---------------------------------------------------------------------------
 struct GenArgs {
-  double *u, *v, *w, *rhsupa, *rhsvpa, *rhswpa;
+  double *u, *v, *w;
+  void *rhsupa, *rhsvpa, *rhswpa;  // double, or float when rhs32 (mixed path)
+  int rhs32;
   const double *u0, *v0;
   double *um;
   double *tab;  // genflu_tab_doubles(ny) doubles of table scratch
@@ -843,7 +845,12 @@ __global__ void __launch_bounds__(128) k_genflu_cols(DCoef c, GenArgs a) {
   if (vt) {
     out[0] = 0.0;
     out[(size_t)(ny - 1) * nz1] = kr == 0 ? c.vmagic[0] : 0.0;
-    for (int r = 0; r < ny; ++r) a.rhsvpa[(size_t)r * nz1 + kr] = 0.0;
+    for (int r = 0; r < ny; ++r) {
+      if (a.rhs32)
+        static_cast<float *>(a.rhsvpa)[(size_t)r * nz1 + kr] = 0.0f;
+      else
+        static_cast<double *>(a.rhsvpa)[(size_t)r * nz1 + kr] = 0.0;
+    }
   } else {
     const double *ib = c.inby, *cc = c.ccon;
     double *q = out;
@@ -851,8 +858,13 @@ __global__ void __launch_bounds__(128) k_genflu_cols(DCoef c, GenArgs a) {
     q[(size_t)ny * nz1] = -1.0 / M2(cc, 1, 1) *
                           (M2(cc, 1, 2) * q[(size_t)(ny - 1) * nz1] + M2(cc, 1, 3) * q[(size_t)(ny - 2) * nz1] +
                            M2(cc, 1, 4) * q[(size_t)(ny - 3) * nz1]);
-    double *h = comp == 0 ? a.rhsupa : a.rhswpa;
-    for (int r = 0; r <= ny; ++r) h[(size_t)r * nz1 + kr] = 0.0;
+    void *h = comp == 0 ? a.rhsupa : a.rhswpa;
+    for (int r = 0; r <= ny; ++r) {
+      if (a.rhs32)
+        static_cast<float *>(h)[(size_t)r * nz1 + kr] = 0.0f;
+      else
+        static_cast<double *>(h)[(size_t)r * nz1 + kr] = 0.0;
+    }
   }
 }
 
@@ -901,7 +913,8 @@ __device__ double block_sum(double v, double *red) {
   return r;
 }
 
-__global__ void __launch_bounds__(256) k_outflow(DCoef c, double *u, const double *v, double *rhsupa) {
+template <typename TR>
+__global__ void __launch_bounds__(256) k_outflow(DCoef c, double *u, const double *v, TR *rhsupa) {
   __shared__ double red[256];
   const int t = threadIdx.x, nx = c.nx, ny = c.ny, nz1 = c.nz1;
   const size_t PU = (size_t)(ny + 1) * nz1, PV = (size_t)ny * nz1;
@@ -919,8 +932,8 @@ __global__ void __launch_bounds__(256) k_outflow(DCoef c, double *u, const doubl
   for (int j = 2 + t; j <= ny; j += 256) {
     double *q = u + (size_t)(nx - 1) * PU + (size_t)(j - 1) * nz1;
     q[0] = q[0] + alpha;
-    double *h = rhsupa + (size_t)(nx - 1) * PU + (size_t)(j - 1) * nz1;
-    h[0] = h[0] + alpha * c.S[OTBL_S_IDX];
+    TR *h = rhsupa + (size_t)(nx - 1) * PU + (size_t)(j - 1) * nz1;
+    h[0] = (TR)((double)h[0] + alpha * c.S[OTBL_S_IDX]);
   }
 }
 
@@ -1040,8 +1053,9 @@ __global__ void __launch_bounds__(256) k_pois_bwd(DCoef c, XTab x, double *__res
 }
 
 // projection, pois.f90:144-162; one thread per (i >= 2, j, kr)
+template <typename TP>
 __global__ void __launch_bounds__(128) k_project(DCoef c, const DState *st, const double *__restrict__ phi,
-                                                 double *u, double *v, double *w, double *p) {
+                                                 double *u, double *v, double *w, TP *p) {
   const int kr = blockIdx.x * blockDim.x + threadIdx.x;
   if (kr >= c.nz1) return;
   const int j = blockIdx.y + 1, i = blockIdx.z + 2;
@@ -1052,8 +1066,8 @@ __global__ void __launch_bounds__(128) k_project(DCoef c, const DState *st, cons
   const double *f = phi + (size_t)(i - 1) * PV + kr;  // phi(j, i) at f[(j-1)*nz1]
   if (j >= 2) {
     const double fm = f[(size_t)(j - 2) * nz1];
-    double *pq = p + (size_t)(i - 1) * PV + (size_t)(j - 1) * nz1 + kr;
-    *pq = st->varstep * fm + *pq;
+    TP *pq = p + (size_t)(i - 1) * PV + (size_t)(j - 1) * nz1 + kr;
+    *pq = (TP)(st->varstep * fm + (double)*pq);
     const double q = f[(size_t)(j - 2) * nz1 + pof];
     const double kf = odd ? kz * q : -kz * q;
     double *wq = w + (size_t)(i - 1) * PU + (size_t)(j - 1) * nz1 + kr;
@@ -1319,6 +1333,7 @@ cudaError_t launch_genflu(otbl_ctx *c, int tail) {
   a.rhsupa = c->f[OTBL_F_RHSUPA];
   a.rhsvpa = c->f[OTBL_F_RHSVPA];
   a.rhswpa = c->f[OTBL_F_RHSWPA];
+  a.rhs32 = c->f32[OTBL_F_RHSUPA];
   a.u0 = c->u0;
   a.v0 = c->v0;
   a.um = c->um;
@@ -1386,6 +1401,7 @@ cudaError_t launch_genflu_noalloc(otbl_ctx *c, double *wk, double *u, double *v,
   a.v = v;
   a.w = w;
   a.rhsupa = a.rhsvpa = a.rhswpa = nullptr;  // only touched with tail = 1
+  a.rhs32 = 0;
   a.u0 = u0;
   a.v0 = v0;
   a.um = um;
@@ -1406,7 +1422,11 @@ cudaError_t launch_genflu_noalloc(otbl_ctx *c, double *wk, double *u, double *v,
 
 cudaError_t launch_outflow(otbl_ctx *c) {
   prof_begin(c, PK_OUTFLOW);
-  k_outflow<<<1, 256, 0, c->stream>>>(c->dc, c->f[OTBL_F_U], c->f[OTBL_F_V], c->f[OTBL_F_RHSUPA]);
+  if (c->f32[OTBL_F_RHSUPA])
+    k_outflow<float><<<1, 256, 0, c->stream>>>(c->dc, c->f[OTBL_F_U], c->f[OTBL_F_V],
+                                               reinterpret_cast<float *>(c->f[OTBL_F_RHSUPA]));
+  else
+    k_outflow<double><<<1, 256, 0, c->stream>>>(c->dc, c->f[OTBL_F_U], c->f[OTBL_F_V], c->f[OTBL_F_RHSUPA]);
   prof_end(c);
   c->launches += 1;
   return cudaGetLastError();
@@ -1453,8 +1473,12 @@ cudaError_t launch_pois(otbl_ctx *c, int m) {
   prof_end(c);
   dim3 gp((nz1 + 127) / 128, ny, nx - 1);
   prof_begin(c, PK_PROJECT);
-  k_project<<<gp, 128, 0, c->stream>>>(c->dc, c->st, phi, c->f[OTBL_F_U], c->f[OTBL_F_V], c->f[OTBL_F_W],
-                                       c->f[OTBL_F_P]);
+  if (c->f32[OTBL_F_P])
+    k_project<float><<<gp, 128, 0, c->stream>>>(c->dc, c->st, phi, c->f[OTBL_F_U], c->f[OTBL_F_V],
+                                                c->f[OTBL_F_W], reinterpret_cast<float *>(c->f[OTBL_F_P]));
+  else
+    k_project<double><<<gp, 128, 0, c->stream>>>(c->dc, c->st, phi, c->f[OTBL_F_U], c->f[OTBL_F_V],
+                                                 c->f[OTBL_F_W], c->f[OTBL_F_P]);
   prof_end(c);
   c->launches += 3;
   return cudaGetLastError();

@@ -178,7 +178,16 @@ extern "C" int otbl_ctx_create(const otbl_config *cfg, const double *coef, int d
   }
 
   const size_t lu = otbl_field_len(nx, ny, nz, 1);
-  for (int id = 0; id < OTBL_F_COUNT; ++id) TRY(dalloc(c, &c->f[id], field_len(c, id)));
+  for (int id = 0; id < OTBL_F_COUNT; ++id) {
+    c->f32[id] = c->mixed && (id == OTBL_F_P || id == OTBL_F_RHSUPA || id == OTBL_F_RHSVPA || id == OTBL_F_RHSWPA);
+    if (c->f32[id]) {
+      float *q = nullptr;
+      TRY(dalloc(c, &q, field_len(c, id)));
+      c->f[id] = reinterpret_cast<double *>(q);
+    } else {
+      TRY(dalloc(c, &c->f[id], field_len(c, id)));
+    }
+  }
   TRY(dalloc(c, &c->u0, (size_t)ny + 1));
   TRY(dalloc(c, &c->v0, (size_t)ny + 1));
   TRY(dalloc(c, &c->um, (size_t)ny + 1));
@@ -238,7 +247,7 @@ extern "C" size_t otbl_ctx_bytes(const otbl_config *cfg) {
   otbl_coef_layout(nx, ny, nz, &o);
   const size_t ncoef = o.off[OTBL_C_COUNT], lu = otbl_field_len(nx, ny, nz, 1), lv = otbl_field_len(nx, ny, nz, 0);
   size_t b = ncoef * sizeof(double) + (mixed ? ncoef * sizeof(float) : 0);
-  b += (4 * lu + 3 * lv) * sizeof(double);                       // state
+  b += (2 * lu + lv) * sizeof(double) + (2 * lu + 2 * lv) * (mixed ? sizeof(float) : sizeof(double));  // state
   b += 3 * (size_t)(ny + 1) * sizeof(double) + sizeof(DState);   // u0, v0, um, scalars
   b += 15 * lu * (mixed ? sizeof(float) : sizeof(double));       // intermediates
   b += (std::max(lu, (size_t)(ny + 2) * (nx - 1) * nz1) + 2 * lu) * sizeof(double);  // scratch
@@ -296,8 +305,14 @@ extern "C" long long otbl_launch_count(const otbl_ctx *c) { return c ? c->launch
 extern "C" int otbl_set_field(otbl_ctx *c, int id, const double *host) {
   if (!c || !host || id < 0 || id >= OTBL_F_COUNT) return OTBL_ERR_ARG;
   cudaSetDevice(c->device);
-  OTBL_CUDA_TRY(c, cudaMemcpyAsync(c->f[id], host, field_len(c, id) * sizeof(double), cudaMemcpyHostToDevice,
-                                   c->stream));
+  const size_t n = field_len(c, id);
+  if (c->f32[id]) {  // FP32 storage on the mixed path: round on the host
+    std::vector<float> tmp(host, host + n);
+    OTBL_CUDA_TRY(c, cudaMemcpyAsync(c->f[id], tmp.data(), n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    OTBL_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return OTBL_OK;
+  }
+  OTBL_CUDA_TRY(c, cudaMemcpyAsync(c->f[id], host, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   OTBL_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   return OTBL_OK;
 }
@@ -305,14 +320,25 @@ extern "C" int otbl_set_field(otbl_ctx *c, int id, const double *host) {
 extern "C" int otbl_get_field(otbl_ctx *c, int id, double *host) {
   if (!c || !host || id < 0 || id >= OTBL_F_COUNT) return OTBL_ERR_ARG;
   cudaSetDevice(c->device);
-  OTBL_CUDA_TRY(c, cudaMemcpyAsync(host, c->f[id], field_len(c, id) * sizeof(double), cudaMemcpyDeviceToHost,
-                                   c->stream));
+  const size_t n = field_len(c, id);
+  if (c->f32[id]) {
+    std::vector<float> tmp(n);
+    OTBL_CUDA_TRY(c, cudaMemcpyAsync(tmp.data(), c->f[id], n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    OTBL_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    std::copy(tmp.begin(), tmp.end(), host);
+    return OTBL_OK;
+  }
+  OTBL_CUDA_TRY(c, cudaMemcpyAsync(host, c->f[id], n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   OTBL_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   return OTBL_OK;
 }
 
 extern "C" int otbl_field_device_ptr(otbl_ctx *c, int id, double **dptr) {
   if (!c || !dptr || id < 0 || id >= OTBL_F_COUNT) return OTBL_ERR_ARG;
+  if (c->f32[id]) {
+    c->err = "field is stored in FP32 on the mixed-precision path";
+    return OTBL_ERR_CONFIG;
+  }
   *dptr = c->f[id];
   return OTBL_OK;
 }

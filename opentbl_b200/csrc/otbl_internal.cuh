@@ -108,7 +108,10 @@ struct otbl_ctx {
   double *coef_dev;
   float *coef_dev_f;
   std::vector<double> coef_host;
+  // state fields; on the mixed path p and the RHS history are stored as
+  // float (f32[id]) behind the same pointer, u, v, w always as double
   double *f[OTBL_F_COUNT];
+  bool f32[OTBL_F_COUNT] = {false, false, false, false, false, false, false};
   double *u0, *v0, *um;
   otbl::DState *st;
   otbl::Work w;
