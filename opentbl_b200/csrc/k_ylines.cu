@@ -560,7 +560,7 @@ struct FinalBox {
 };
 
 template <int COMP, typename W>
-__global__ void __launch_bounds__(128) k_final_tb(DCoef c, FinalStream<W> fs, int *err,
+__global__ void __launch_bounds__(128) k_final_tb(DCoef c, DCoefT<W> cw, FinalStream<W> fs, int *err,
                                                   const __grid_constant__ FinalMaps maps) {
   using B = FinalBox<W, COMP>;
   constexpr int KF = B::KF, TB = B::T;
@@ -613,8 +613,10 @@ __global__ void __launch_bounds__(128) k_final_tb(DCoef c, FinalStream<W> fs, in
   const double *ib = c.inby, *cc = c.ccon;
   const double sgn = odd ? 1.0 : -1.0;
   const int which = COMP == 1 ? 1 : 0;
-  const double *dcy = which == 0 ? c.dcyu : c.dcyv, *ecd = which == 0 ? c.cofcyu : c.cofcyv;
-  const double *viy = which == 0 ? c.viyu : c.viyv, *ecv = which == 0 ? c.cofvyu : c.cofvyv;
+  // differzy and vistyy run in W on the coefficient copy cw (FP32 on the
+  // mixed path); the RHS assembly, RK3 combination and implzy in FP64
+  const W *dcy = which == 0 ? cw.dcyu : cw.dcyv, *ecd = which == 0 ? cw.cofcyu : cw.cofcyv;
+  const W *viy = which == 0 ? cw.viyu : cw.viyv, *ecv = which == 0 ? cw.cofvyu : cw.cofvyv;
   const double *vyi = which == 0 ? c.vyui : c.vyvi;
   const double *fac = COMP == 1 ? a.fac_v : a.fac_u;
   auto Pg = [&](int r) { return (double)__ldg(prod + (size_t)min(max(r, 0), ny - 1) * S); };
@@ -634,16 +636,16 @@ __global__ void __launch_bounds__(128) k_final_tb(DCoef c, FinalStream<W> fs, in
     return o - (odd ? av * pp : -av * pp);
   };
   const int chv = which == 0 ? 3 : 1, cha = chv + 1, ic = which == 0 ? 3 : 1;
-  const double *db = c.dcby, *vb = c.cofvby;
-  double bot = 0.0, top = 0.0;
+  const W *db = cw.dcby, *vb = cw.cofvby;
+  W bot = W(0), top = W(0);
   if (!last) {
-    bot = M4(db, chv, 1) * Pg(0) + M4(db, chv, 2) * Pg(1) + M4(db, chv, 3) * Pg(2) + M4(db, chv, 4) * Pg(3);
-    top = M4(db, cha, 1) * Pg(ny - 1) + M4(db, cha, 2) * Pg(ny - 2) + M4(db, cha, 3) * Pg(ny - 3) +
-          M4(db, cha, 4) * Pg(ny - 4);
+    bot = M4(db, chv, 1) * (W)Pg(0) + M4(db, chv, 2) * (W)Pg(1) + M4(db, chv, 3) * (W)Pg(2) + M4(db, chv, 4) * (W)Pg(3);
+    top = M4(db, cha, 1) * (W)Pg(ny - 1) + M4(db, cha, 2) * (W)Pg(ny - 2) + M4(db, cha, 3) * (W)Pg(ny - 3) +
+          M4(db, cha, 4) * (W)Pg(ny - 4);
   }
-  const double b0 = M4(vb, ic, 1) * Vg(0) + M4(vb, ic, 2) * Vg(1) + M4(vb, ic, 3) * Vg(2) + M4(vb, ic, 4) * Vg(3);
-  const double bN = M4(vb, ic + 1, 1) * Vg(jee - 1) + M4(vb, ic + 1, 2) * Vg(jee - 2) +
-                    M4(vb, ic + 1, 3) * Vg(jee - 3) + M4(vb, ic + 1, 4) * Vg(jee - 4);
+  const W b0 = M4(vb, ic, 1) * (W)Vg(0) + M4(vb, ic, 2) * (W)Vg(1) + M4(vb, ic, 3) * (W)Vg(2) + M4(vb, ic, 4) * (W)Vg(3);
+  const W bN = M4(vb, ic + 1, 1) * (W)Vg(jee - 1) + M4(vb, ic + 1, 2) * (W)Vg(jee - 2) +
+               M4(vb, ic + 1, 3) * (W)Vg(jee - 3) + M4(vb, ic + 1, 4) * (W)Vg(jee - 4);
   double ub1 = 0.0, ubt = 0.0;
   if (COMP == 1) {
     ubt = kr == 0 ? c.vmagic[i - 1] : 0.0;
@@ -653,23 +655,23 @@ __global__ void __launch_bounds__(128) k_final_tb(DCoef c, FinalStream<W> fs, in
     ub1 = -1.0 / M4(ib, 2, 1) * (M4(ib, 2, 2) * s2 + M4(ib, 2, 3) * s3 + M4(ib, 2, 4) * s4);
     ubt = -1.0 / M2(cc, 1, 1) * (M2(cc, 1, 2) * sn + M2(cc, 1, 3) * sn1 + M2(cc, 1, 4) * sn2);
   }
-  auto rd = [&](int r, double gm, double g0, double gp) {
-    const double in = which == 0 ? __ldg(ecd + 2 * r + 1) * g0 + __ldg(ecd + 2 * r) * gm
-                                 : __ldg(ecd + 2 * r + 1) * gp + __ldg(ecd + 2 * r) * g0;
+  auto rd = [&](int r, W gm, W g0, W gp) {
+    const W in = which == 0 ? __ldg(ecd + 2 * r + 1) * g0 + __ldg(ecd + 2 * r) * gm
+                            : __ldg(ecd + 2 * r + 1) * gp + __ldg(ecd + 2 * r) * g0;
     return r == 0 ? bot : (r == jee - 1 ? top : in);
   };
-  auto rv = [&](int r, double um, double u0, double up) {
-    const double in = __ldg(ecv + 3 * r) * up + __ldg(ecv + 3 * r + 1) * u0 + __ldg(ecv + 3 * r + 2) * um;
+  auto rv = [&](int r, W um, W u0, W up) {
+    const W in = __ldg(ecv + 3 * r) * up + __ldg(ecv + 3 * r + 1) * u0 + __ldg(ecv + 3 * r + 2) * um;
     return r == 0 ? b0 : (r == jee - 1 ? bN : in);
   };
-  const double *ck = fs.ck + (active ? col : 0);
+  const W *ck = reinterpret_cast<const W *>(fs.ck) + (active ? col : 0);
   double *yq = fs.yq + (active ? col : 0);
   const double a1raw = fac[3 * (jee + 1)], a3raw = fac[3 * (jee + 1) + 1];
-  double xd = 0.0, xv = 0.0;
+  W xd = W(0), xv = W(0);
   double R1 = 0.0, R2 = 0.0, R3 = 0.0;
   double res1 = 0.0, res2 = 0.0;
   double yel = 0.0;
-  double ckd = ck[(size_t)(2 * (nseg - 1)) * ncol], ckv = ck[(size_t)(2 * (nseg - 1) + 1) * ncol];
+  W ckd = ck[(size_t)(2 * (nseg - 1)) * ncol], ckv = ck[(size_t)(2 * (nseg - 1) + 1) * ncol];
   const int tk = t ^ 1;  // kr+1 for even kr, kr-1 for odd kr (the chunk starts even)
   for (int sg = nseg - 1, it = 0; sg >= 0; --sg, ++it) {
     const int stg = it & 1;
@@ -687,22 +689,22 @@ __global__ void __launch_bounds__(128) k_final_tb(DCoef c, FinalStream<W> fs, in
     const W *sk = reinterpret_cast<const W *>(bs + B::kp);
     const W *sh = reinterpret_cast<const W *>(bs + B::hp);
     const W *spp = reinterpret_cast<const W *>(bs + B::p);
-    double ad = ckd, av = ckv;
+    W ad = ckd, av = ckv;
     if (sg >= 1) {  // next segment's checkpoints, ahead of use
       ckd = ck[(size_t)(2 * (sg - 1)) * ncol];
       ckv = ck[(size_t)(2 * (sg - 1) + 1) * ncol];
     }
     if (!active) continue;
-    double ydv[KF], yvv[KF];
+    W ydv[KF], yvv[KF];
 #pragma unroll
     for (int b = 0; b < KF; ++b) {
       const int r = s0 + b;
       if (r < jee) {
         if (!last)
-          ad = rd(r, (double)sp[b * TB + t], (double)sp[(b + 1) * TB + t], (double)sp[(b + 2) * TB + t]) +
-               (r > 0 ? __ldg(dcy + 3 * r) : 0.0) * ad;
-        av = rv(r, sv[b * TB + t], sv[(b + 1) * TB + t], sv[(b + 2) * TB + t]) +
-             (r > 0 ? __ldg(viy + 3 * r) : 0.0) * av;
+          ad = rd(r, sp[b * TB + t], sp[(b + 1) * TB + t], sp[(b + 2) * TB + t]) +
+               (r > 0 ? __ldg(dcy + 3 * r) : W(0)) * ad;
+        av = rv(r, (W)sv[b * TB + t], (W)sv[(b + 1) * TB + t], (W)sv[(b + 2) * TB + t]) +
+             (r > 0 ? __ldg(viy + 3 * r) : W(0)) * av;
       }
       ydv[b] = ad;
       yvv[b] = av;
@@ -714,7 +716,7 @@ __global__ void __launch_bounds__(128) k_final_tb(DCoef c, FinalStream<W> fs, in
       if (!last) xd = (ydv[b] - __ldg(dcy + 3 * r + 2) * xd) * __ldg(dcy + 3 * r + 1);
       xv = (yvv[b] - __ldg(viy + 3 * r + 2) * xv) * __ldg(viy + 3 * r + 1);
       // RHS assembly (rhsp.F90:164-169, 181-204, 351-418, 423-445)
-      const double d1 = last ? 0.0 : xd;
+      const double d1 = last ? 0.0 : (double)xd;
       const double u0 = sv[(b + 1) * TB + t];
       double R = (double)sc[b * TB + t];
       const double kzt = sgn * kz * ((!last && (COMP != 2 || r < ny)) ? (double)sk[b * TB + tk] : 0.0);
@@ -760,7 +762,7 @@ __global__ void __launch_bounds__(128) k_final_tb(DCoef c, FinalStream<W> fs, in
         const double avz = var1 * kz;
         st = u0 - (odd ? avz * pp : -avz * pp);
       }
-      const double res = st - (var3 * R + v2 * xv + var4 * (double)sh[b * TB + t]);
+      const double res = st - (var3 * R + v2 * (double)xv + var4 * (double)sh[b * TB + t]);
       hp[(size_t)r * S] = (W)R;
       if (r < n) {
         double v = __ldg(vyi + 3 * (r + 1)) * res + __ldg(vyi + 3 * (r + 1) + 1) * res1 +
@@ -785,7 +787,7 @@ __global__ void __launch_bounds__(128) k_final_tb(DCoef c, FinalStream<W> fs, in
 // (KA = 8 rows per stage); the checkpoints are still written every KF rows
 // of k_final_tb's segments. The arithmetic is k_final_s1's pass A.
 template <int COMP, typename W>
-__global__ void __launch_bounds__(128) k_final_ta(DCoef c, FinalStream<W> fs, int *err,
+__global__ void __launch_bounds__(128) k_final_ta(DCoef c, DCoefT<W> cw, FinalStream<W> fs, int *err,
                                                   const __grid_constant__ FinalMaps maps) {
   constexpr int KF = FinalTune<W>::kf_tma, KA = 8, TB = 128, R = KA + 2;
   constexpr int PB = (R * TB * (int)sizeof(W) + 127) / 128 * 128;
@@ -823,32 +825,33 @@ __global__ void __launch_bounds__(128) k_final_ta(DCoef c, FinalStream<W> fs, in
   const W *prod = (COMP == 0 ? a.uv : (COMP == 1 ? a.vv : a.vw)) + plv + krc;
   const double *vel = (COMP == 0 ? a.u : (COMP == 1 ? a.v : a.w)) + pl + krc;
   const int which = COMP == 1 ? 1 : 0;
-  const double *dcy = which == 0 ? c.dcyu : c.dcyv, *ecd = which == 0 ? c.cofcyu : c.cofcyv;
-  const double *viy = which == 0 ? c.viyu : c.viyv, *ecv = which == 0 ? c.cofvyu : c.cofvyv;
-  auto Pg = [&](int r) { return (double)__ldg(prod + (size_t)min(max(r, 0), ny - 1) * S); };
-  auto Vg = [&](int r) { return __ldg(vel + (size_t)min(max(r, 0), jee - 1) * S); };
+  // the sweeps run in W on the coefficient copy cw (FP32 on the mixed path)
+  const W *dcy = which == 0 ? cw.dcyu : cw.dcyv, *ecd = which == 0 ? cw.cofcyu : cw.cofcyv;
+  const W *viy = which == 0 ? cw.viyu : cw.viyv, *ecv = which == 0 ? cw.cofvyu : cw.cofvyv;
+  auto Pg = [&](int r) { return (W)__ldg(prod + (size_t)min(max(r, 0), ny - 1) * S); };
+  auto Vg = [&](int r) { return (W)__ldg(vel + (size_t)min(max(r, 0), jee - 1) * S); };
   const int chv = which == 0 ? 3 : 1, cha = chv + 1, ic = which == 0 ? 3 : 1;
-  const double *db = c.dcby, *vb = c.cofvby;
-  double bot = 0.0, top = 0.0;
+  const W *db = cw.dcby, *vb = cw.cofvby;
+  W bot = W(0), top = W(0);
   if (!last) {
     bot = M4(db, chv, 1) * Pg(0) + M4(db, chv, 2) * Pg(1) + M4(db, chv, 3) * Pg(2) + M4(db, chv, 4) * Pg(3);
     top = M4(db, cha, 1) * Pg(ny - 1) + M4(db, cha, 2) * Pg(ny - 2) + M4(db, cha, 3) * Pg(ny - 3) +
           M4(db, cha, 4) * Pg(ny - 4);
   }
-  const double b0 = M4(vb, ic, 1) * Vg(0) + M4(vb, ic, 2) * Vg(1) + M4(vb, ic, 3) * Vg(2) + M4(vb, ic, 4) * Vg(3);
-  const double bN = M4(vb, ic + 1, 1) * Vg(jee - 1) + M4(vb, ic + 1, 2) * Vg(jee - 2) +
-                    M4(vb, ic + 1, 3) * Vg(jee - 3) + M4(vb, ic + 1, 4) * Vg(jee - 4);
-  auto rd = [&](int r, double gm, double g0, double gp) {
-    const double in = which == 0 ? __ldg(ecd + 2 * r + 1) * g0 + __ldg(ecd + 2 * r) * gm
-                                 : __ldg(ecd + 2 * r + 1) * gp + __ldg(ecd + 2 * r) * g0;
+  const W b0 = M4(vb, ic, 1) * Vg(0) + M4(vb, ic, 2) * Vg(1) + M4(vb, ic, 3) * Vg(2) + M4(vb, ic, 4) * Vg(3);
+  const W bN = M4(vb, ic + 1, 1) * Vg(jee - 1) + M4(vb, ic + 1, 2) * Vg(jee - 2) +
+               M4(vb, ic + 1, 3) * Vg(jee - 3) + M4(vb, ic + 1, 4) * Vg(jee - 4);
+  auto rd = [&](int r, W gm, W g0, W gp) {
+    const W in = which == 0 ? __ldg(ecd + 2 * r + 1) * g0 + __ldg(ecd + 2 * r) * gm
+                            : __ldg(ecd + 2 * r + 1) * gp + __ldg(ecd + 2 * r) * g0;
     return r == 0 ? bot : (r == jee - 1 ? top : in);
   };
-  auto rv = [&](int r, double um, double u0, double up) {
-    const double in = __ldg(ecv + 3 * r) * up + __ldg(ecv + 3 * r + 1) * u0 + __ldg(ecv + 3 * r + 2) * um;
+  auto rv = [&](int r, W um, W u0, W up) {
+    const W in = __ldg(ecv + 3 * r) * up + __ldg(ecv + 3 * r + 1) * u0 + __ldg(ecv + 3 * r + 2) * um;
     return r == 0 ? b0 : (r == jee - 1 ? bN : in);
   };
-  double *ck = fs.ck + col;
-  double yd = 0.0, yv = 0.0;
+  W *ck = reinterpret_cast<W *>(fs.ck) + col;  // checkpoints in W, read back by k_final_tb
+  W yd = W(0), yv = W(0);
   for (int sa = 0; sa < nst; ++sa) {
     const int stg = sa & 1;
     const bool ok = mbar_wait_bounded(&bar[stg], (sa >> 1) & 1, 2000000000ull);
@@ -869,10 +872,8 @@ __global__ void __launch_bounds__(128) k_final_ta(DCoef c, FinalStream<W> fs, in
         ck[(size_t)(2 * (r / KF) + 1) * ncol] = yv;
       }
       if (r < jee) {
-        if (!last)
-          yd = rd(r, (double)sp[b * TB], (double)sp[(b + 1) * TB], (double)sp[(b + 2) * TB]) +
-               (r > 0 ? __ldg(dcy + 3 * r) : 0.0) * yd;
-        yv = rv(r, sv[b * TB], sv[(b + 1) * TB], sv[(b + 2) * TB]) + (r > 0 ? __ldg(viy + 3 * r) : 0.0) * yv;
+        if (!last) yd = rd(r, sp[b * TB], sp[(b + 1) * TB], sp[(b + 2) * TB]) + (r > 0 ? __ldg(dcy + 3 * r) : W(0)) * yd;
+        yv = rv(r, (W)sv[b * TB], (W)sv[(b + 1) * TB], (W)sv[(b + 2) * TB]) + (r > 0 ? __ldg(viy + 3 * r) : W(0)) * yv;
       }
     }
   }
@@ -1107,6 +1108,11 @@ static int final_t(otbl_ctx *c) {
   const dim3 g((ncol + 127) / 128);
   double *U = c->f[OTBL_F_U], *V = c->f[OTBL_F_V], *Wv = c->f[OTBL_F_W];
   const bool tma = c->fmaps_ok;
+  DCoefT<W> cw;  // the sweeps' coefficients in W
+  if constexpr (std::is_same<W, float>::value)
+    cw = c->dcf;
+  else
+    cw = c->dc;
   const dim3 gt((c->dc.nz1 + 127) / 128, c->cfg.nx - 1);
   auto comp = [&](auto C) {
     constexpr int K = decltype(C)::value;
@@ -1116,12 +1122,12 @@ static int final_t(otbl_ctx *c) {
       if constexpr (FinalTune<W>::tma_a) {
         constexpr int sma = 2 * ((10 * 128 * (int)sizeof(W) + 127) / 128 * 128 + 10 * 128 * 8) + 128;
         cudaFuncSetAttribute(k_final_ta<K, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, sma);
-        k_final_ta<K, W><<<gt, 128, sma, c->stream>>>(c->dc, fs, &c->st->err, c->fmaps[K]);
+        k_final_ta<K, W><<<gt, 128, sma, c->stream>>>(c->dc, cw, fs, &c->st->err, c->fmaps[K]);
       } else {
         k_final_s1<K, W, 1, FinalTune<W>::kf_tma><<<g, 128, 0, c->stream>>>(c->dc, fs);
       }
       cudaFuncSetAttribute(k_final_tb<K, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_t);
-      k_final_tb<K, W><<<gt, 128, smem_t, c->stream>>>(c->dc, fs, &c->st->err, c->fmaps[K]);
+      k_final_tb<K, W><<<gt, 128, smem_t, c->stream>>>(c->dc, cw, fs, &c->st->err, c->fmaps[K]);
     } else if constexpr (FinalTune<W>::split) {
       k_final_s1<K, W, 1><<<g, 128, 0, c->stream>>>(c->dc, fs);
       k_final_s1<K, W, 2><<<g, 128, 0, c->stream>>>(c->dc, fs);
