@@ -230,6 +230,13 @@ int otbl_autotune(otbl_ctx *ctx, int *choice);
 /* sets the three CTA sizes (each 32, 64 or 128) without timing, e.g. those
  * otbl_autotune picked for another context of the same box size */
 int otbl_set_tuning(otbl_ctx *ctx, const int *bs);
+/* failure detection of the device-side waits (no counterpart in the
+ * reference): runs the bounded mbarrier wait of the TMA-fed kernels on a
+ * barrier that never completes, with a 1 ms limit; *status receives
+ * OTBL_ERR_TIMEOUT when the wait gave up and the kernel returned, as the
+ * product kernels do (they record it in the context's error flag, which
+ * otbl_sync and otbl_get_inflow report). Synchronizes. */
+int otbl_selftest_wait(otbl_ctx *ctx, int *status);
 
 /* ---- instrumentation (no counterpart in the reference, whose timers are
  *      the MPI_WTIME accumulators of module temporal, mod.F90:311-322) ---- */

@@ -12,8 +12,31 @@
 #include <vector>
 
 #include "otbl_internal.cuh"
+#include "tma.cuh"
 
 using namespace otbl;
+
+// Self-test of the bounded mbarrier wait that every TMA-fed kernel uses:
+// the barrier is armed for 16 bytes that no copy ever delivers (nothing is
+// issued, so nothing is in flight), every thread waits with a limit of
+// limit_ns and, as the product kernels do on a timeout, the CTA agrees on
+// the failure, records OTBL_ERR_TIMEOUT and returns.
+__global__ void k_wait_selftest(int *status, unsigned long long limit_ns) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_init_fence();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) mbar_arrive_expect_tx(&bar, 16);
+  __syncthreads();
+  const bool ok = mbar_wait_bounded(&bar, 0, limit_ns);
+  if (__syncthreads_or(!ok)) {
+    if (threadIdx.x == 0) atomicExch(status, OTBL_ERR_TIMEOUT);
+    return;
+  }
+  if (threadIdx.x == 0) atomicExch(status, OTBL_OK);
+}
 
 struct otbl_graph {
   int device;
@@ -216,4 +239,19 @@ extern "C" int otbl_set_tuning(otbl_ctx *c, const int *bs) {
     if (bs[k] != 32 && bs[k] != 64 && bs[k] != 128) return OTBL_ERR_ARG;
   for (int k = 0; k < 3; ++k) c->tune_bs[k] = bs[k];
   return OTBL_OK;
+}
+
+extern "C" int otbl_selftest_wait(otbl_ctx *c, int *status) {
+  if (!c || !status) return OTBL_ERR_ARG;
+  cudaSetDevice(c->device);
+  int *d = nullptr;
+  if (cudaMalloc(&d, sizeof(int)) != cudaSuccess) return OTBL_ERR_OOM;
+  const int init = -1;
+  cudaMemcpy(d, &init, sizeof(int), cudaMemcpyHostToDevice);
+  k_wait_selftest<<<1, 64, 0, c->stream>>>(d, 1000000ull);  // 1 ms
+  int st = OTBL_OK;
+  if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(c->stream) != cudaSuccess) st = OTBL_ERR_CUDA;
+  if (st == OTBL_OK && cudaMemcpy(status, d, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) st = OTBL_ERR_CUDA;
+  cudaFree(d);
+  return st;
 }

@@ -100,6 +100,7 @@ def _bind(L):
         "otbl_query": ([P], I),
         "otbl_autotune": ([P, ctypes.POINTER(ctypes.c_int)], I),
         "otbl_set_tuning": ([P, ctypes.POINTER(ctypes.c_int)], I),
+        "otbl_selftest_wait": ([P, ctypes.POINTER(ctypes.c_int)], I),
         "otbl_get_stream": ([P, ctypes.POINTER(P)], I),
         "otbl_profile_enable": ([P, I], I),
         "otbl_profile_read": ([P, I, ctypes.POINTER(ctypes.c_char_p), D, ctypes.POINTER(I)], I),

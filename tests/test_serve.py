@@ -123,3 +123,21 @@ def test_serving_mix_equals_alone():
             assert np.array_equal(res.fields[n], mix[r.rid].fields[n]), (r.rid, n)
     s = serve.summarize(mix, srv.makespan)
     assert s["requests"] == 6 and s["p99_s"] >= s["p50_s"] > 0
+
+
+@pytest.mark.gpu
+def test_bounded_device_wait_reports_timeout():
+    """The bounded mbarrier wait of the TMA-fed kernels on a barrier that
+    never completes: the kernel gives up after 1 ms and reports
+    OTBL_ERR_TIMEOUT; the context keeps working afterwards."""
+    import ctypes
+    cfg = config.TINY
+    init = synth.make_initial(cfg)
+    b = Box(cfg, init)
+    st = ctypes.c_int(0)
+    assert b.L.otbl_selftest_wait(b.h, ctypes.byref(st)) == native.OTBL_OK
+    assert st.value == 8  # OTBL_ERR_TIMEOUT
+    b.advance(1)
+    b.sync()
+    assert np.isfinite(b.field("u")).all()
+    b.close()
