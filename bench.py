@@ -287,6 +287,7 @@ def run_mixed(cfg, init, coef, fbox, device, R, warm, K, fp64_ms_per_step):
     import torch
     mcfg = cfgmod.replace(cfg, precision=1)
     mbox = Box(mcfg, init, coef, device=device)
+    mtuned = mbox.autotune()
     stream = torch.cuda.ExternalStream(mbox.stream, device=f"cuda:{device}")
     for _ in range(warm):
         mbox.advance(1)
@@ -327,7 +328,8 @@ def run_mixed(cfg, init, coef, fbox, device, R, warm, K, fp64_ms_per_step):
                                  "unit": "GB/s", "frac": ab["substep_mixed"] / sub_s / 1e9 / peak,
                                  "peak_kind": peak_kind},
             "kernels_ms_per_substep": per_sub,
-            "err_vs_fp64": dict(steps=nsteps, **err), "clocks": clk.summary()}
+            "err_vs_fp64": dict(steps=nsteps, **err), "clocks": clk.summary(),
+            "autotuned_cta_sizes": list(mtuned)}
 
 
 def main():
@@ -358,6 +360,7 @@ def main():
     import torch
     torch.cuda.set_device(local)
     init, coef, box = build_box(cfg, local)
+    tuned = box.autotune()  # CTA sizes of the line kernels for this box
     stream = torch.cuda.ExternalStream(box.stream, device=f"cuda:{local}")
     warm = max(args.warmup, 0)
     K = max(args.steps, 1)
@@ -476,7 +479,7 @@ def main():
                           "nz": cfg.nz, "substeps_per_step": 3,
                           "l2": "inputs larger than L2 (state %.1f GB per box)" % (
                               sum(np.prod(box.shape(n)) for n in native.FIELDS) * 8 / 1e9),
-                          "parallelism": f"replicas{ws}"},
+                          "parallelism": f"replicas{ws}", "autotuned_cta_sizes": list(tuned)},
                "roofline": roofline, "substep_roofline": substep_roofline,
                "kernels_ms_per_substep": kernels,
                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
