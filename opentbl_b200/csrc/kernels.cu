@@ -788,10 +788,11 @@ __global__ void __launch_bounds__(256) k_genflu_tab(DCoef c, GenArgs a) {
 __global__ void __launch_bounds__(128) k_genflu_cols(DCoef c, GenArgs a) {
   const int ny = c.ny, nz1 = c.nz1, xout = c.xout;
   const int kr = blockIdx.x * blockDim.x + threadIdx.x;
-  const int comp = blockIdx.y;
+  const int comp = blockIdx.y, r = blockIdx.z;  // one thread per (kr, component, row)
   if (kr >= nz1) return;
   const bool vt = comp == 2;
   const int rows = vt ? ny : ny + 1;
+  if (r >= rows) return;
   const size_t P = (size_t)rows * nz1;
   double *f = comp == 0 ? a.u : (comp == 1 ? a.w : a.v);
   const double *in = f + (size_t)(xout - 1) * P + kr;
@@ -804,75 +805,66 @@ __global__ void __launch_bounds__(128) k_genflu_cols(DCoef c, GenArgs a) {
   const bool prof = ntp[0] >= 4 && ntp[1] >= 4;
   const double ggg = a.tab[3 * N1];
   const double yb = c.S[OTBL_S_YBLEND];
-  // input row r (0-based) of the blended plane: genflu.F90:55-60 (modes >= 1)
-  auto inp = [&](int r) -> double {
-    const double v = in[(size_t)r * nz1];
+  // input row q (0-based) of the blended plane: genflu.F90:55-60 (modes >= 1)
+  auto inp = [&](int q) -> double {
+    const double v = in[(size_t)q * nz1];
     if (vt || kr < 2) return v;
-    const double fb = 0.5 * (1 - tanh(c.y[r + 1] - yb));
+    const double fb = 0.5 * (1 - tanh(c.y[q + 1] - yb));
     return v * fb;
   };
-  if (kr < 2) {  // zero mode, genflu.F90:146-150
-    for (int r = 0; r < rows; ++r) {
-      double v = 0.0;
-      if (kr == 0 && comp == 0) v = a.u0[r];
-      if (kr == 0 && comp == 2) v = a.v0[r];
-      out[(size_t)r * nz1] = v;
+  // the new plane-1 value of row q before boun
+  auto val = [&](int q) -> double {
+    if (kr < 2) {  // zero mode, genflu.F90:146-150
+      if (kr == 0 && comp == 0) return a.u0[q];
+      if (kr == 0 && comp == 2) return a.v0[q];
+      return 0.0;
     }
-  } else if (!prof) {  // degenerate rescaled grid: blended copy, flagged
-    for (int r = 0; r < rows; ++r) out[(size_t)r * nz1] = inp(r);
-    if (kr == 2 && comp == 0 && a.err) *a.err = OTBL_ERR_NAN;
-  } else if (!vt) {  // profile, u-type rows 0..ny
-    auto W = [&](int i) {
-      const int kll = max(kl[i], 1);
-      return inp(kll + 1) * fsca[i] + inp(kll) * (1 - fsca[i]);
-    };
-    const double w1 = W(1);
-    for (int r = 0; r <= ny; ++r) {
-      const int rr = r >= nt - 3 ? nt - 4 : r;
-      const double wv = rr == 0 ? -w1 : W(rr);
-      out[(size_t)r * nz1] = wv * ggg;
+    if (!prof) return inp(q);  // degenerate rescaled grid: blended copy, flagged
+    if (!vt) {                 // profile, u-type rows 0..ny
+      auto W = [&](int i) {
+        const int kll = max(kl[i], 1);
+        return inp(kll + 1) * fsca[i] + inp(kll) * (1 - fsca[i]);
+      };
+      const int rr = q >= nt - 3 ? nt - 4 : q;
+      const double wv = rr == 0 ? -W(1) : W(rr);
+      return wv * ggg;
     }
-  } else {  // profile, v-type rows 0..ny-1
-    for (int r = 0; r < ny; ++r) {
-      const int i = (r >= nt - 3 ? nt - 4 : r) + 1;
-      const int kll = max(kl[i], 1);
-      out[(size_t)r * nz1] = (inp(kll) * fsca[i] + inp(kll - 1) * (1 - fsca[i])) * ggg;
-    }
-  }
-  if (!a.tail) return;
-  // boun on plane 1 (this thread wrote the whole column) and the plane-1
-  // RHS history
-  if (vt) {
-    out[0] = 0.0;
-    out[(size_t)(ny - 1) * nz1] = kr == 0 ? c.vmagic[0] : 0.0;
-    for (int r = 0; r < ny; ++r) {
-      if (a.rhs32)
-        static_cast<float *>(a.rhsvpa)[(size_t)r * nz1 + kr] = 0.0f;
-      else
-        static_cast<double *>(a.rhsvpa)[(size_t)r * nz1 + kr] = 0.0;
-    }
+    const int i = (q >= nt - 3 ? nt - 4 : q) + 1;  // profile, v-type rows 0..ny-1
+    const int kll = max(kl[i], 1);
+    return (inp(kll) * fsca[i] + inp(kll - 1) * (1 - fsca[i])) * ggg;
+  };
+  if (kr == 2 && comp == 0 && r == 0 && !prof && a.err) *a.err = OTBL_ERR_NAN;
+  double v;
+  if (!a.tail) {
+    v = val(r);
+  } else if (vt) {  // boun on plane 1 (boun.f90:33-55) and the plane-1 RHS history
+    v = r == 0 ? 0.0 : (r == ny - 1 ? (kr == 0 ? c.vmagic[0] : 0.0) : val(r));
+    if (a.rhs32)
+      static_cast<float *>(a.rhsvpa)[(size_t)r * nz1 + kr] = 0.0f;
+    else
+      static_cast<double *>(a.rhsvpa)[(size_t)r * nz1 + kr] = 0.0;
   } else {
     const double *ib = c.inby, *cc = c.ccon;
-    double *q = out;
-    q[0] = -1.0 / M4(ib, 2, 1) * (M4(ib, 2, 2) * q[nz1] + M4(ib, 2, 3) * q[2 * nz1] + M4(ib, 2, 4) * q[3 * nz1]);
-    q[(size_t)ny * nz1] = -1.0 / M2(cc, 1, 1) *
-                          (M2(cc, 1, 2) * q[(size_t)(ny - 1) * nz1] + M2(cc, 1, 3) * q[(size_t)(ny - 2) * nz1] +
-                           M2(cc, 1, 4) * q[(size_t)(ny - 3) * nz1]);
+    if (r == 0)
+      v = -1.0 / M4(ib, 2, 1) * (M4(ib, 2, 2) * val(1) + M4(ib, 2, 3) * val(2) + M4(ib, 2, 4) * val(3));
+    else if (r == ny)
+      v = -1.0 / M2(cc, 1, 1) * (M2(cc, 1, 2) * val(ny - 1) + M2(cc, 1, 3) * val(ny - 2) + M2(cc, 1, 4) * val(ny - 3));
+    else
+      v = val(r);
     void *h = comp == 0 ? a.rhsupa : a.rhswpa;
-    for (int r = 0; r <= ny; ++r) {
-      if (a.rhs32)
-        static_cast<float *>(h)[(size_t)r * nz1 + kr] = 0.0f;
-      else
-        static_cast<double *>(h)[(size_t)r * nz1 + kr] = 0.0;
-    }
+    if (a.rhs32)
+      static_cast<float *>(h)[(size_t)r * nz1 + kr] = 0.0f;
+    else
+      static_cast<double *>(h)[(size_t)r * nz1 + kr] = 0.0;
   }
+  out[(size_t)r * nz1] = v;
 }
 
 cudaError_t genflu_launch(otbl_ctx *c, const GenArgs &a) {
   const size_t smem = genflu_smem_bytes(c->cfg.ny);
   if (smem > 48 * 1024) cudaFuncSetAttribute(k_genflu_tab, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   k_genflu_tab<<<1, 256, smem, c->stream>>>(c->dc, a);
-  dim3 g((c->dc.nz1 + 127) / 128, 3);
+  dim3 g((c->dc.nz1 + 127) / 128, 3, c->cfg.ny + 1);
   k_genflu_cols<<<g, 128, 0, c->stream>>>(c->dc, a);
   c->launches += 2;
   return cudaGetLastError();

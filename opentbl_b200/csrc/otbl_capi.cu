@@ -140,10 +140,17 @@ extern "C" int otbl_ctx_create(const otbl_config *cfg, const double *coef, int d
     delete c;
     return OTBL_ERR_NODEV;
   }
-  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess) {
+    if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return OTBL_ERR_CUDA;
   }
+  for (cudaEvent_t &e : c->ev)
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+      otbl_ctx_destroy(c);
+      return OTBL_ERR_CUDA;
+    }
   const int nx = cfg->nx, ny = cfg->ny, nz = cfg->nz;
   const int nz1 = 2 * (nz / 3);
   otbl_coef_offsets o;
@@ -291,7 +298,11 @@ extern "C" void otbl_ctx_destroy(otbl_ctx *c) {
     cudaEventDestroy(r.b);
   }
   for (cudaEvent_t e : c->prof_pool) cudaEventDestroy(e);
+  if (c->side) cudaStreamSynchronize(c->side);
   for (void *p : c->allocs) cudaFree(p);
+  for (cudaEvent_t e : c->ev)
+    if (e) cudaEventDestroy(e);
+  if (c->side) cudaStreamDestroy(c->side);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -424,10 +435,28 @@ extern "C" int otbl_rhsp(otbl_ctx *c, int m, int setstep) {
   LAUNCH(c, launch_interpx(c));
   LAUNCH(c, launch_interpy(c));
   LAUNCH(c, launch_products(c, setstep));
+  // k_dt (needs the CFL maxima of the products) beside difvisxx; genflu
+  // (needs dt; writes plane 1 of u, v, w, which difvisxx reads and the rhsp
+  // tail does not touch) beside the tail; joined before outflow_correction
+  cudaStream_t main_s = c->stream;
+  OTBL_CUDA_TRY(c, cudaEventRecord(c->ev[0], main_s));
+  OTBL_CUDA_TRY(c, cudaStreamWaitEvent(c->side, c->ev[0], 0));
+  c->stream = c->side;
+  cudaError_t e = launch_dt(c, m, setstep);
+  c->stream = main_s;
+  if (check(c, e, "launch_dt") != OTBL_OK) return OTBL_ERR_CUDA;
+  OTBL_CUDA_TRY(c, cudaEventRecord(c->ev[1], c->side));
   LAUNCH(c, launch_difvisx(c));
-  LAUNCH(c, launch_dt(c, m, setstep));
-  LAUNCH(c, launch_genflu(c, 1));
+  OTBL_CUDA_TRY(c, cudaEventRecord(c->ev[2], main_s));
+  OTBL_CUDA_TRY(c, cudaStreamWaitEvent(c->side, c->ev[2], 0));
+  c->stream = c->side;
+  e = launch_genflu(c, 1);
+  c->stream = main_s;
+  if (check(c, e, "launch_genflu") != OTBL_OK) return OTBL_ERR_CUDA;
+  OTBL_CUDA_TRY(c, cudaEventRecord(c->ev[3], c->side));
+  OTBL_CUDA_TRY(c, cudaStreamWaitEvent(main_s, c->ev[1], 0));
   LAUNCH(c, launch_final(c));
+  OTBL_CUDA_TRY(c, cudaStreamWaitEvent(main_s, c->ev[3], 0));
   return OTBL_OK;
 }
 

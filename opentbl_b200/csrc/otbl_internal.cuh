@@ -91,6 +91,10 @@ struct otbl_ctx {
   otbl_config cfg;
   int device;
   cudaStream_t stream;
+  // second stream of the substep: k_dt beside difvisxx, genflu beside the
+  // rhsp tail (fork/join by events, so a graph capture records the overlap)
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   otbl::DCoef dc;
   otbl::DCoefT<float> dcf;  // FP32 coefficients (mixed path)
   // threads per CTA of the line kernels that otbl_autotune times:
