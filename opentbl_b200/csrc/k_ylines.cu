@@ -970,11 +970,26 @@ __global__ void __launch_bounds__(128) k_pois_solve(DCoef c, double *phi, const 
 // ---------------------------------------------------------------------------
 // launch wrappers
 // ---------------------------------------------------------------------------
+// Checkpoints of interpyy at the tail of each line scratch, so that
+// interpyy can run beside interpxx (whose checkpoints start at the head);
+// nullptr when the two would overlap.
+double *interpy_ck_tail(otbl_ctx *c, double *s) {
+  const int nx = c->cfg.nx, ny = c->cfg.ny, nz = c->cfg.nz, nz1 = c->dc.nz1;
+  const size_t lu = otbl_field_len(nx, ny, nz, 1);  // doubles in s2, s3 (s1 may be larger)
+  const size_t ncol = (size_t)nx * nz1;
+  const size_t y_need = (size_t)((ny + KY - 1) / KY) * ncol;  // doubles (floats need less)
+  // interpxx: at most one checkpoint per 4 planes per line (4 is its shortest segment)
+  const size_t x_need = (size_t)((nx + 3) / 4) * (size_t)(ny + 1) * nz1;
+  if (x_need + y_need + 64 > lu) return nullptr;
+  return s + ((lu - y_need) & ~(size_t)31);
+}
+
 cudaError_t launch_interpy(otbl_ctx *c) {
   InterpyArgs a;
   const double *ins[3] = {c->f[OTBL_F_U], c->f[OTBL_F_W], c->f[OTBL_F_V]};
   void *outs[3] = {c->w.uy, c->w.wy, c->w.vy};
-  double *cks[3] = {c->w.s1, c->w.s2, c->w.s3};
+  double *tail[3] = {interpy_ck_tail(c, c->w.s1), interpy_ck_tail(c, c->w.s2), interpy_ck_tail(c, c->w.s3)};
+  double *cks[3] = {tail[0] ? tail[0] : c->w.s1, tail[1] ? tail[1] : c->w.s2, tail[2] ? tail[2] : c->w.s3};
   const int which[3] = {0, 0, 1};
   for (int f = 0; f < 3; ++f) {
     a.in[f] = ins[f];

@@ -432,13 +432,28 @@ extern "C" int otbl_rhsp(otbl_ctx *c, int m, int setstep) {
   cudaSetDevice(c->device);
   if (m == 1) LAUNCH(c, launch_energies(c));
   if (setstep) LAUNCH(c, launch_reset_max(c));
-  LAUNCH(c, launch_interpx(c));
-  LAUNCH(c, launch_interpy(c));
+  cudaStream_t main_s = c->stream;
+  // interpyy beside interpxx (both read the state only; their checkpoints
+  // take disjoint parts of the scratch), joined before the products
+  const bool ypar = interpy_ck_tail(c, c->w.s2) != nullptr;
+  if (ypar) {
+    OTBL_CUDA_TRY(c, cudaEventRecord(c->ev[0], main_s));
+    OTBL_CUDA_TRY(c, cudaStreamWaitEvent(c->side, c->ev[0], 0));
+    c->stream = c->side;
+    cudaError_t ey = launch_interpy(c);
+    c->stream = main_s;
+    if (check(c, ey, "launch_interpy") != OTBL_OK) return OTBL_ERR_CUDA;
+    OTBL_CUDA_TRY(c, cudaEventRecord(c->ev[1], c->side));
+    LAUNCH(c, launch_interpx(c));
+    OTBL_CUDA_TRY(c, cudaStreamWaitEvent(main_s, c->ev[1], 0));
+  } else {
+    LAUNCH(c, launch_interpx(c));
+    LAUNCH(c, launch_interpy(c));
+  }
   LAUNCH(c, launch_products(c, setstep));
   // k_dt (needs the CFL maxima of the products) beside difvisxx; genflu
   // (needs dt; writes plane 1 of u, v, w, which difvisxx reads and the rhsp
   // tail does not touch) beside the tail; joined before outflow_correction
-  cudaStream_t main_s = c->stream;
   OTBL_CUDA_TRY(c, cudaEventRecord(c->ev[0], main_s));
   OTBL_CUDA_TRY(c, cudaStreamWaitEvent(c->side, c->ev[0], 0));
   c->stream = c->side;

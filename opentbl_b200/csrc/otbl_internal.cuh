@@ -157,6 +157,9 @@ namespace otbl {
 // kernel launch wrappers (kernels.cu); each returns cudaGetLastError()
 cudaError_t launch_interpx(otbl_ctx *c);
 cudaError_t launch_interpy(otbl_ctx *c);
+// interpyy's checkpoint region in a line scratch when it can run beside
+// interpxx, else nullptr
+double *interpy_ck_tail(otbl_ctx *c, double *s);
 cudaError_t launch_products(otbl_ctx *c, int setstep);
 cudaError_t launch_difvisx(otbl_ctx *c);
 cudaError_t launch_dt(otbl_ctx *c, int m, int setstep);
