@@ -44,16 +44,19 @@ struct FinalTune;
 #ifndef OTBL_FT_TK
 #define OTBL_FT_TK 2
 #endif
+#ifndef OTBL_FT_NS
+#define OTBL_FT_NS 2
+#endif
 // tma_a: pass A fed by TMA too (k_final_ta; FP32 inputs 5.25 against 5.33
 // ms; FP64 6.50 against 5.94, so FP64 keeps the register-streamed pass A)
 template <>
 struct FinalTune<double> {
-  static constexpr int kf = OTBL_FT_DK, minb = OTBL_FT_DM, kf_tma = OTBL_FT_TK;
+  static constexpr int kf = OTBL_FT_DK, minb = OTBL_FT_DM, kf_tma = OTBL_FT_TK, ns_tma = OTBL_FT_NS;
   static constexpr bool split = false, tma_a = false;
 };
 template <>
 struct FinalTune<float> {
-  static constexpr int kf = OTBL_FT_FK, minb = OTBL_FT_FM, kf_tma = OTBL_FT_TK;
+  static constexpr int kf = OTBL_FT_FK, minb = OTBL_FT_FM, kf_tma = OTBL_FT_TK, ns_tma = OTBL_FT_NS;
   static constexpr bool split = true, tma_a = true;
 };
 
@@ -388,7 +391,7 @@ __global__ void __launch_bounds__(128, PASSES == 1 ? 6 : FinalTune<W>::minb)
 #pragma unroll
     for (int b = 0; b < KA; ++b) {
       const int r = s0 + b;
-      if (b % KF == 0 && r < jee) {  // y of row r-1 at the start of segment r/KF
+      if (r % KF == 0 && r < jee) {  // y of row r-1 at the start of segment r/KF
         ck[(size_t)(2 * (r / KF)) * ncol] = yd;
         ck[(size_t)(2 * (r / KF) + 1) * ncol] = yv;
       }
@@ -556,7 +559,8 @@ struct FinalBox {
   static constexpr int p = hp + r128(KF * T * E);             // W PR x PP
   static constexpr int stage = p + r128(PR * PP * T * E);
   static constexpr unsigned tx = (unsigned)((KF + 2) * T * E + (KF + 2) * T * 8 + 3 * KF * T * E + PR * PP * T * E);
-  static constexpr int smem = 2 * stage + 128;  // two stages and the barriers
+  static constexpr int NS = FinalTune<W>::ns_tma;  // ring stages
+  static constexpr int smem = NS * stage + 128;    // the stages and the barriers
 };
 
 template <int COMP, typename W>
@@ -565,7 +569,8 @@ __global__ void __launch_bounds__(128) k_final_tb(DCoef c, DCoefT<W> cw, FinalSt
   using B = FinalBox<W, COMP>;
   constexpr int KF = B::KF, TB = B::T;
   extern __shared__ __align__(128) unsigned char smraw[];
-  uint64_t *full = reinterpret_cast<uint64_t *>(smraw + 2 * B::stage);
+  constexpr int NS = B::NS;
+  uint64_t *full = reinterpret_cast<uint64_t *>(smraw + NS * B::stage);
   const FinalArgs<W> &a = fs.a;
   const int nx = c.nx, ny = c.ny, nz1 = c.nz1;
   const int ncol = (nx - 1) * nz1;
@@ -590,12 +595,12 @@ __global__ void __launch_bounds__(128) k_final_tb(DCoef c, DCoefT<W> cw, FinalSt
     tma_load_3d(b + B::p, &maps.p, kr0, s0, i - 1, &full[stg]);
   };
   if (t == 0) {
-    mbar_init(&full[0], 1);
-    mbar_init(&full[1], 1);
+    for (int q = 0; q < NS; ++q) mbar_init(&full[q], 1);
     mbar_init_fence();
   }
   __syncthreads();
-  if (t == 0) issue(0, nseg - 1);
+  if (t == 0)  // the first NS-1 segments (descending)
+    for (int q = 0; q < NS - 1 && q < nseg; ++q) issue(q, nseg - 1 - q);
   // ---- per-column setup (as k_final_s1)
   const int pof = odd ? -1 : 1;
   const size_t PU = (size_t)(ny + 1) * nz1, PV = (size_t)ny * nz1;
@@ -674,13 +679,13 @@ __global__ void __launch_bounds__(128) k_final_tb(DCoef c, DCoefT<W> cw, FinalSt
   W ckd = ck[(size_t)(2 * (nseg - 1)) * ncol], ckv = ck[(size_t)(2 * (nseg - 1) + 1) * ncol];
   const int tk = t ^ 1;  // kr+1 for even kr, kr-1 for odd kr (the chunk starts even)
   for (int sg = nseg - 1, it = 0; sg >= 0; --sg, ++it) {
-    const int stg = it & 1;
-    const bool ok = mbar_wait_bounded(&full[stg], (it >> 1) & 1, 2000000000ull);
-    if (__syncthreads_or(!ok)) {  // stage stg of iteration it-1 is free from here on
+    const int stg = it % NS;
+    const bool ok = mbar_wait_bounded(&full[stg], (it / NS) & 1, 2000000000ull);
+    if (__syncthreads_or(!ok)) {  // the stage of iteration it-1 is free from here on
       if (t == 0) atomicExch(err, OTBL_ERR_TIMEOUT);
       return;
     }
-    if (t == 0 && sg >= 1) issue(stg ^ 1, sg - 1);
+    if (t == 0 && sg >= NS - 1) issue((it + NS - 1) % NS, sg - (NS - 1));
     const int s0 = sg * KF;
     const unsigned char *bs = smraw + stg * B::stage;
     const W *sp = reinterpret_cast<const W *>(bs + B::prod);
@@ -867,7 +872,7 @@ __global__ void __launch_bounds__(128) k_final_ta(DCoef c, DCoefT<W> cw, FinalSt
 #pragma unroll
     for (int b = 0; b < KA; ++b) {
       const int r = s0 + b;
-      if (b % KF == 0 && r < jee) {  // y of row r-1 at the start of segment r/KF
+      if (r % KF == 0 && r < jee) {  // y of row r-1 at the start of segment r/KF
         ck[(size_t)(2 * (r / KF)) * ncol] = yd;
         ck[(size_t)(2 * (r / KF) + 1) * ncol] = yv;
       }

@@ -8,7 +8,9 @@ the north star's mixed-path gates): velocity relative L2 (Parseval weights)
 <= 1e-5 after 100 steps of 1025x193x512 and after 20 steps of 257x97x128;
 max|div u| after the projection <= 1e-10; the mean profile, Re_theta and
 C_f to 1e-5 relative. One substep of the small boxes: <= 1e-6, pressure
-<= 1e-5, RHS history <= 1e-4. Measured on B200: 1.8e-8 after one substep,
+<= 1e-5, RHS history <= 1e-4. Regression bounds about 5x the measured
+errors are asserted as well (1e-7 after one substep, 1e-6 after 20 steps),
+so that a kernel bug that stays inside the north star's gates still fails. Measured on B200: 1.8e-8 after one substep,
 1.7e-7 after 20 steps of 257x97x128, 3.4e-7 after 100 steps of
 1025x193x512, max|div u| ~1e-14.
 """
@@ -43,6 +45,9 @@ def test_mixed_one_substep(name):
     o.substep(1, 1)
     r = _report(f"{name} mixed, 1 substep", g, o, cfg, coef)
     assert r["vel_rel_l2"] <= 1e-6
+    # regression bound, about 5x the measured 1.8e-8 (TINY: TMA-fed kernels;
+    # SMALL, nz1 % 4 != 0: the register-streamed fallbacks)
+    assert r["vel_rel_l2"] <= 1e-7
     assert r["max_div"] <= 1e-10
     other = {n: rel_l2(g.field(n), o.field(n)) for n in ("p", "rhsupa", "rhsvpa", "rhswpa")}
     print(name, "mixed, 1 substep, other fields", other)
@@ -62,6 +67,7 @@ def test_mixed_c1_twenty_steps():
     o.advance(20)
     r = _report("C1 mixed, 20 steps", g, o, cfg, coef)
     assert r["vel_rel_l2"] <= 1e-5
+    assert r["vel_rel_l2"] <= 1e-6  # regression bound, about 5x the measured 1.7e-7
     assert r["max_div"] <= 1e-10
     for k in ("U_rel_l2", "um_rel_l2", "re_theta_rel", "cf_rel"):
         assert r[k] <= 1e-5, k
