@@ -398,17 +398,7 @@ static void xline_t_launch(otbl_ctx *c, const DCoefT<T> &dc, const XStream &a, c
 
 // ---- TMA descriptors (host): field [nx][np], boxes of 32 lines x rows
 static bool encode_lines(CUtensorMap *m, const void *base, size_t esz, int nx, int np, int rows) {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  static bool tried = false;
-  if (!tried) {
-    tried = true;
-    void *p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    cudaGetLastError();
-  }
+  auto fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(tensor_map_encoder());
   if (!fn || (np * esz) % 16 != 0 || ((uintptr_t)base) % 16 != 0) return false;
   const cuuint64_t dims[2] = {(cuuint64_t)np, (cuuint64_t)nx};
   const cuuint64_t strides[1] = {(cuuint64_t)np * esz};

@@ -1026,25 +1026,25 @@ cudaError_t launch_interpy(otbl_ctx *c) {
 }
 
 // ---- TMA descriptors (host) ----
-static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  static bool tried = false;
-  if (!tried) {
-    tried = true;
+// cuTensorMapEncodeTiled from the driver, looked up once (thread-safe
+// initialisation of a function-local static); nullptr if unavailable
+void *tensor_map_encoder() {
+  static void *const fn = []() -> void * {
     void *p = nullptr;
     cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
     cudaGetLastError();
-  }
+    return p;
+  }();
   return fn;
 }
 
 // a field [planes][rows][nz1] of element size esz, boxes of 128 x brows x bplanes
 static bool encode_field(CUtensorMap *m, const void *base, size_t esz, int planes, int rows, int nz1, int brows,
                          int bplanes) {
-  auto fn = tensor_map_encoder();
+  auto fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(tensor_map_encoder());
   if (!fn || (nz1 * esz) % 16 != 0 || ((uintptr_t)base) % 16 != 0) return false;
   const cuuint64_t dims[3] = {(cuuint64_t)nz1, (cuuint64_t)rows, (cuuint64_t)planes};
   const cuuint64_t strides[2] = {(cuuint64_t)nz1 * esz, (cuuint64_t)rows * nz1 * esz};

@@ -427,9 +427,23 @@ extern "C" int otbl_get_energies(otbl_ctx *c, double *ener) {
     if (s__ != OTBL_OK) return s__;                        \
   } while (0)
 
+static int rhsp_issue(otbl_ctx *c, int m, int setstep);
+
 extern "C" int otbl_rhsp(otbl_ctx *c, int m, int setstep) {
   if (!c || m < 1 || m > 3) return OTBL_ERR_ARG;
   cudaSetDevice(c->device);
+  cudaStream_t main_s = c->stream;
+  const int st = rhsp_issue(c, m, setstep);
+  if (st != OTBL_OK) {
+    // leave no side-stream work unordered behind an error
+    c->stream = main_s;
+    cudaEventRecord(c->ev[3], c->side);
+    cudaStreamWaitEvent(main_s, c->ev[3], 0);
+  }
+  return st;
+}
+
+static int rhsp_issue(otbl_ctx *c, int m, int setstep) {
   if (m == 1) LAUNCH(c, launch_energies(c));
   if (setstep) LAUNCH(c, launch_reset_max(c));
   cudaStream_t main_s = c->stream;

@@ -174,6 +174,8 @@ cudaError_t launch_energies(otbl_ctx *c);
 // builds c->fmaps (false if TMA cannot address the fields, e.g. an FP32 row
 // pitch that is not a multiple of 16 bytes)
 bool build_final_maps(otbl_ctx *c);
+// the driver's cuTensorMapEncodeTiled (as void *), nullptr if unavailable
+void *tensor_map_encoder();
 bool build_x_maps(otbl_ctx *c);
 bool build_y_maps(otbl_ctx *c);
 cudaError_t launch_twiddles(otbl_ctx *c);
