@@ -290,14 +290,18 @@ __device__ __forceinline__ void stockham_pass_pad(V *buf, int M, int Ns, const V
 // FFT of length n = 2^a 3^b 5^c of this thread's padded line (n * lines per
 // CTA <= 4096), the radix order of block_fft (8s, 4s, 2s, 3s, 5s), so the
 // arithmetic is block_fft's operation for operation.
-template <int SIGN, typename V>
+// NT: threads of the CTA (n * lines <= 4096, so a thread has at most
+// 4096 / (NT R) items of a radix-R pass)
+template <int SIGN, int NT = 256, typename V>
 __device__ __forceinline__ void block_fft_lines(V *buf, int n, const V *__restrict__ tw, int t, int G) {
+  constexpr int I8 = (4096 / 8 + NT - 1) / NT, I4 = (4096 / 4 + NT - 1) / NT, I2 = (4096 / 2 + NT - 1) / NT;
+  constexpr int I3 = (4096 / 3 + NT - 1) / NT, I5 = (4096 / 5 + NT - 1) / NT;
   int Ns = 1, rem = n;
-  while (rem % 8 == 0) { stockham_pass_pad<8, SIGN, 2>(buf, n, Ns, tw, t, G); Ns *= 8; rem /= 8; }
-  while (rem % 4 == 0) { stockham_pass_pad<4, SIGN, 4>(buf, n, Ns, tw, t, G); Ns *= 4; rem /= 4; }
-  while (rem % 2 == 0) { stockham_pass_pad<2, SIGN, 8>(buf, n, Ns, tw, t, G); Ns *= 2; rem /= 2; }
-  while (rem % 3 == 0) { stockham_pass_pad<3, SIGN, 6>(buf, n, Ns, tw, t, G); Ns *= 3; rem /= 3; }
-  while (rem % 5 == 0) { stockham_pass_pad<5, SIGN, 4>(buf, n, Ns, tw, t, G); Ns *= 5; rem /= 5; }
+  while (rem % 8 == 0) { stockham_pass_pad<8, SIGN, I8>(buf, n, Ns, tw, t, G); Ns *= 8; rem /= 8; }
+  while (rem % 4 == 0) { stockham_pass_pad<4, SIGN, I4>(buf, n, Ns, tw, t, G); Ns *= 4; rem /= 4; }
+  while (rem % 2 == 0) { stockham_pass_pad<2, SIGN, I2>(buf, n, Ns, tw, t, G); Ns *= 2; rem /= 2; }
+  while (rem % 3 == 0) { stockham_pass_pad<3, SIGN, I3>(buf, n, Ns, tw, t, G); Ns *= 3; rem /= 3; }
+  while (rem % 5 == 0) { stockham_pass_pad<5, SIGN, I5>(buf, n, Ns, tw, t, G); Ns *= 5; rem /= 5; }
 }
 
 }  // namespace otbl

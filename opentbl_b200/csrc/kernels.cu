@@ -949,8 +949,8 @@ struct XTab {
 // divergence (pois.f90:41-54) + DCT-II along x (cosftx iopt=-1); output
 // phi-hat in plane layout (v-type, plane i = x-mode index + 2). Mode 0 made
 // real (pois.f90:102).
-template <int MB>
-__global__ void __launch_bounds__(256) k_pois_fwd(DCoef c, XTab x, const double *__restrict__ u,
+template <int MB, int NT>
+__global__ void __launch_bounds__(NT) k_pois_fwd(DCoef c, XTab x, const double *__restrict__ u,
                                                  const double *__restrict__ v, const double *__restrict__ w,
                                                  double *__restrict__ phi) {
   extern __shared__ double2 xsm[];
@@ -959,7 +959,7 @@ __global__ void __launch_bounds__(256) k_pois_fwd(DCoef c, XTab x, const double 
   const int k0 = blockIdx.x * MB;
   const size_t PU = (size_t)(ny + 1) * nz1, PV = (size_t)ny * nz1;
   const double idx = c.S[OTBL_S_IDX], idy = c.idy[j];
-  for (int e = threadIdx.x; e < n * MB; e += 256) {
+  for (int e = threadIdx.x; e < n * MB; e += NT) {
     const int l = e % MB, tt = e / MB;
     const int k = k0 + l;
     double2 val = make_double2(0.0, 0.0);
@@ -982,11 +982,11 @@ __global__ void __launch_bounds__(256) k_pois_fwd(DCoef c, XTab x, const double 
   }
   __syncthreads();
   {
-    const int G = 256 / MB, l = threadIdx.x / G;
-    block_fft_lines<-1>(xsm + l * ld, n, x.tw, threadIdx.x % G, G);
+    const int G = NT / MB, l = threadIdx.x / G;
+    block_fft_lines<-1, NT>(xsm + l * ld, n, x.tw, threadIdx.x % G, G);
   }
   const double dnf = 1.0 / (double)n;
-  for (int e = threadIdx.x; e < n * MB; e += 256) {
+  for (int e = threadIdx.x; e < n * MB; e += NT) {
     const int l = e % MB, kk = e / MB;
     const int k = k0 + l;
     if (k > nz2) continue;
@@ -1001,14 +1001,14 @@ __global__ void __launch_bounds__(256) k_pois_fwd(DCoef c, XTab x, const double 
 }
 
 // DCT-III along x (cosftx iopt=+1), in place on phi-hat
-template <int MB>
-__global__ void __launch_bounds__(256) k_pois_bwd(DCoef c, XTab x, double *__restrict__ phi) {
+template <int MB, int NT>
+__global__ void __launch_bounds__(NT) k_pois_bwd(DCoef c, XTab x, double *__restrict__ phi) {
   extern __shared__ double2 xsm[];
   const int n = x.n, ld = xpad(n) | 1, ny = c.ny, nz1 = c.nz1, nz2 = c.nz2, xr = c.xround;
   const int j = blockIdx.y + 1;
   const int k0 = blockIdx.x * MB;
   const size_t PV = (size_t)ny * nz1;
-  for (int e = threadIdx.x; e < n * MB; e += 256) {
+  for (int e = threadIdx.x; e < n * MB; e += NT) {
     const int l = e % MB, kk = e / MB;
     const int k = k0 + l;
     double2 val = make_double2(0.0, 0.0);
@@ -1028,10 +1028,10 @@ __global__ void __launch_bounds__(256) k_pois_bwd(DCoef c, XTab x, double *__res
   }
   __syncthreads();
   {
-    const int G = 256 / MB, l = threadIdx.x / G;
-    block_fft_lines<1>(xsm + l * ld, n, x.tw, threadIdx.x % G, G);
+    const int G = NT / MB, l = threadIdx.x / G;
+    block_fft_lines<1, NT>(xsm + l * ld, n, x.tw, threadIdx.x % G, G);
   }
-  for (int e = threadIdx.x; e < n * MB; e += 256) {
+  for (int e = threadIdx.x; e < n * MB; e += NT) {
     const int l = e % MB, tt = e / MB;
     const int k = k0 + l;
     if (k > nz2) continue;
@@ -1176,6 +1176,10 @@ __global__ void k_twiddles(double2 *tw, int n, double2 *tw2, int n2, int mode2) 
 }
 
 static inline int xpad_host(int i) { return i + (i >> 3); }
+#ifndef OTBL_POIS_NT
+#define OTBL_POIS_NT 512
+#endif
+constexpr int POIS_NT_BIG = OTBL_POIS_NT;
 
 // FP32 copy of an FP64 table (mixed path)
 __global__ void k_round_f32(const double *in, float *out, int n) {
@@ -1433,35 +1437,38 @@ cudaError_t launch_pois(otbl_ctx *c, int m) {
   const size_t smem = (size_t)MB * (xpad_host(n) | 1) * sizeof(double2);
   double *phi = c->w.s2;
   dim3 gx((nz2 + 1 + MB - 1) / MB, ny - 1);
+  // threads per CTA: 512 when the CTA holds 2048-4096 points (fewer items
+  // and registers per thread, the same barriers), else 256
+  const int NT = n * MB >= 2048 ? POIS_NT_BIG : 256;
   auto fwd = [&](auto kf) {
     cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    kf<<<gx, 256, smem, c->stream>>>(c->dc, xtab(c), c->f[OTBL_F_U], c->f[OTBL_F_V], c->f[OTBL_F_W], phi);
+    kf<<<gx, NT, smem, c->stream>>>(c->dc, xtab(c), c->f[OTBL_F_U], c->f[OTBL_F_V], c->f[OTBL_F_W], phi);
   };
   auto bwd = [&](auto kb) {
     cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    kb<<<gx, 256, smem, c->stream>>>(c->dc, xtab(c), phi);
+    kb<<<gx, NT, smem, c->stream>>>(c->dc, xtab(c), phi);
   };
   prof_begin(c, PK_POIS_FWD);
   if (MB == 8)
-    fwd(k_pois_fwd<8>);
+    NT == 512 ? fwd(k_pois_fwd<8, 512>) : fwd(k_pois_fwd<8, 256>);
   else if (MB == 4)
-    fwd(k_pois_fwd<4>);
+    NT == 512 ? fwd(k_pois_fwd<4, 512>) : fwd(k_pois_fwd<4, 256>);
   else if (MB == 2)
-    fwd(k_pois_fwd<2>);
+    NT == 512 ? fwd(k_pois_fwd<2, 512>) : fwd(k_pois_fwd<2, 256>);
   else
-    fwd(k_pois_fwd<1>);
+    NT == 512 ? fwd(k_pois_fwd<1, 512>) : fwd(k_pois_fwd<1, 256>);
   prof_end(c);
   cudaError_t e = launch_pois_solve(c, phi);
   if (e != cudaSuccess) return e;
   prof_begin(c, PK_POIS_BWD);
   if (MB == 8)
-    bwd(k_pois_bwd<8>);
+    NT == 512 ? bwd(k_pois_bwd<8, 512>) : bwd(k_pois_bwd<8, 256>);
   else if (MB == 4)
-    bwd(k_pois_bwd<4>);
+    NT == 512 ? bwd(k_pois_bwd<4, 512>) : bwd(k_pois_bwd<4, 256>);
   else if (MB == 2)
-    bwd(k_pois_bwd<2>);
+    NT == 512 ? bwd(k_pois_bwd<2, 512>) : bwd(k_pois_bwd<2, 256>);
   else
-    bwd(k_pois_bwd<1>);
+    NT == 512 ? bwd(k_pois_bwd<1, 512>) : bwd(k_pois_bwd<1, 256>);
   prof_end(c);
   dim3 gp((nz1 + 127) / 128, ny, nx - 1);
   prof_begin(c, PK_PROJECT);
