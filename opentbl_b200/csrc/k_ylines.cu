@@ -1100,7 +1100,7 @@ bool build_final_maps(otbl_ctx *c) {
 }
 
 template <typename W>
-static int final_t(otbl_ctx *c) {
+static int final_t(otbl_ctx *c, unsigned comps, cudaEvent_t before_vel) {
   FinalStream<W> fs;
   FinalArgs<W> &a = fs.a;
   a.u = c->f[OTBL_F_U];
@@ -1154,17 +1154,22 @@ static int final_t(otbl_ctx *c) {
     } else {
       k_final_s1<K, W, 3><<<g, 128, 0, c->stream>>>(c->dc, fs);
     }
+    if (before_vel) {  // the first velocity write waits for this event
+      cudaStreamWaitEvent(c->stream, before_vel, 0);
+      before_vel = nullptr;
+    }
     k_final_s2<K><<<g, 128, 0, c->stream>>>(c->dc, U, V, Wv, c->w.fac_u, c->w.fac_v, fs.yq, fs.ub);
   };
-  comp(std::integral_constant<int, 1>{});
-  comp(std::integral_constant<int, 0>{});
-  comp(std::integral_constant<int, 2>{});
-  return (tma || FinalTune<W>::split) ? 9 : 6;
+  int n = 0;
+  if (comps & 1) comp(std::integral_constant<int, 0>{}), ++n;
+  if (comps & 2) comp(std::integral_constant<int, 1>{}), ++n;
+  if (comps & 4) comp(std::integral_constant<int, 2>{}), ++n;
+  return n * ((tma || FinalTune<W>::split) ? 3 : 2);
 }
 
-cudaError_t launch_final(otbl_ctx *c) {
+cudaError_t launch_final(otbl_ctx *c, unsigned comps, cudaEvent_t before_vel) {
   prof_begin(c, PK_FINAL);
-  const int nl = c->mixed ? final_t<float>(c) : final_t<double>(c);
+  const int nl = c->mixed ? final_t<float>(c, comps, before_vel) : final_t<double>(c, comps, before_vel);
   prof_end(c);
   c->launches += nl;
   return cudaGetLastError();

@@ -135,21 +135,37 @@ struct ProdArgs {
   int setstep;
 };
 
-// rhsp.F90:120-171 (uu, uw, uv and the CFL maxima, all planes) and
-// rhsp.F90:367-415 (vw, vv, ww, planes 2..nx-1); one warp per (i, j) line.
-template <typename T>
+// rhsp.F90:120-171 (PART 0: uu, uw, uv and the CFL maxima, all planes) and
+// rhsp.F90:367-415 (PART 1: vw, vv, ww, planes 2..nx-1 and rows 1..ny); one
+// warp per (i, j) line. The two parts read disjoint inputs and write
+// disjoint products, so the second can run beside difvisxx, which reads
+// only the first's.
+template <typename T, int PART>
 __global__ void __launch_bounds__(128) k_products(DCoef c, ZTabT<T> z, ProdArgs<T> a) {
   using V = V2<T>;
   extern __shared__ __align__(16) unsigned char smraw[];
   V *sm = reinterpret_cast<V *>(smraw);
   const int M = z.M, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int j = blockIdx.x * 4 + wid + 1;
-  const int i = blockIdx.y + 1;
-  const int nx = c.nx, ny = c.ny, nz1 = c.nz1;
-  if (j > ny + 1) return;
+  const int i = blockIdx.y + 1 + PART;
+  const int ny = c.ny, nz1 = c.nz1;
+  if (j > ny + 1 - PART) return;
   V *A = sm + (size_t)wid * 3 * M, *B = A + M, *P = B + M;
   const size_t offu = ((size_t)(i - 1) * (ny + 1) + (j - 1)) * nz1;
   const size_t offv = ((size_t)(i - 1) * ny + (j - 1)) * nz1;
+  if (PART == 1) {
+    line_c2r(z, a.v + offv, A, lane);
+    line_c2r(z, a.wy + offv, B, lane);
+    buf_mul(A, B, M, lane);
+    line_r2c(z, A, a.vw + offv, lane);
+    line_c2r(z, a.vy + offv, A, lane);
+    buf_sq(A, M, lane);
+    line_r2c(z, A, a.vv + offv, lane);
+    line_c2r(z, a.w + offu, A, lane);
+    buf_sq(A, M, lane);
+    line_r2c(z, A, a.ww + offv, lane);
+    return;
+  }
   double mu = 0.0, mw = 0.0, mv = 0.0;
   line_c2r(z, a.u + offu, P, lane);
   if (a.setstep) mu = buf_absmax(P, M, lane);
@@ -166,18 +182,6 @@ __global__ void __launch_bounds__(128) k_products(DCoef c, ZTabT<T> z, ProdArgs<
     line_c2r(z, a.uy + offv, B, lane);
     buf_mul(A, B, M, lane);
     line_r2c(z, A, a.uv + offv, lane);
-    if (i >= 2 && i <= nx - 1) {
-      line_c2r(z, a.v + offv, A, lane);
-      line_c2r(z, a.wy + offv, B, lane);
-      buf_mul(A, B, M, lane);
-      line_r2c(z, A, a.vw + offv, lane);
-      line_c2r(z, a.vy + offv, A, lane);
-      buf_sq(A, M, lane);
-      line_r2c(z, A, a.vv + offv, lane);
-      line_c2r(z, a.w + offu, A, lane);
-      buf_sq(A, M, lane);
-      line_r2c(z, A, a.ww + offv, lane);
-    }
   }
   if (a.setstep) {
     mu = warp_nmax(mu);
@@ -367,7 +371,7 @@ __device__ __forceinline__ double regs_absmax(const V (&a)[E]) {
 #ifndef OTBL_PR_MB_F
 #define OTBL_PR_MB_F 3
 #endif
-template <int M, typename T>
+template <int M, typename T, int PART>
 __global__ void __launch_bounds__(128, std::is_same<T, double>::value ? OTBL_PR_MB_D : OTBL_PR_MB_F)
     k_products_r(DCoef c, ZTabT<T> z, ProdArgs<T> a) {
   using V = V2<T>;
@@ -376,14 +380,27 @@ __global__ void __launch_bounds__(128, std::is_same<T, double>::value ? OTBL_PR_
   constexpr int E = M / 32;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int j = blockIdx.x * 4 + wid + 1;
-  const int i = blockIdx.y + 1;
-  const int nx = c.nx, ny = c.ny, nz1 = c.nz1;
-  if (j > ny + 1) return;
+  const int i = blockIdx.y + 1 + PART;
+  const int ny = c.ny, nz1 = c.nz1;
+  if (j > ny + 1 - PART) return;
   V *buf = sm + (size_t)wid * (M + M / 8);
   const size_t offu = ((size_t)(i - 1) * (ny + 1) + (j - 1)) * nz1;
   const size_t offv = ((size_t)(i - 1) * ny + (j - 1)) * nz1;
-  double mu = 0.0, mw = 0.0, mv = 0.0;
   V A[E], B[E];
+  if (PART == 1) {  // planes 2..nx-1, rows 1..ny
+    zc2r_regs<M>(z, a.v + offv, A, buf, lane);  // vw = v wy
+    zc2r_regs<M>(z, a.wy + offv, B, buf, lane);
+    regs_mul<E>(A, B);
+    zr2c_regs<M>(z, A, a.vw + offv, buf, lane);
+    zc2r_regs<M>(z, a.vy + offv, A, buf, lane);  // vv = vy^2
+    regs_sq<E>(A);
+    zr2c_regs<M>(z, A, a.vv + offv, buf, lane);
+    zc2r_regs<M>(z, a.w + offu, A, buf, lane);  // ww = w^2
+    regs_sq<E>(A);
+    zr2c_regs<M>(z, A, a.ww + offv, buf, lane);
+    return;
+  }
+  double mu = 0.0, mw = 0.0, mv = 0.0;
   zc2r_regs<M>(z, a.ux + offu, A, buf, lane);  // uu = ux^2
   regs_sq<E>(A);
   zr2c_regs<M>(z, A, a.uu + offu, buf, lane);
@@ -399,18 +416,6 @@ __global__ void __launch_bounds__(128, std::is_same<T, double>::value ? OTBL_PR_
     zc2r_regs<M>(z, a.uy + offv, B, buf, lane);
     regs_mul<E>(A, B);
     zr2c_regs<M>(z, A, a.uv + offv, buf, lane);
-    if (i >= 2 && i <= nx - 1) {
-      zc2r_regs<M>(z, a.v + offv, A, buf, lane);  // vw = v wy
-      zc2r_regs<M>(z, a.wy + offv, B, buf, lane);
-      regs_mul<E>(A, B);
-      zr2c_regs<M>(z, A, a.vw + offv, buf, lane);
-      zc2r_regs<M>(z, a.vy + offv, A, buf, lane);  // vv = vy^2
-      regs_sq<E>(A);
-      zr2c_regs<M>(z, A, a.vv + offv, buf, lane);
-      zc2r_regs<M>(z, a.w + offu, A, buf, lane);  // ww = w^2
-      regs_sq<E>(A);
-      zr2c_regs<M>(z, A, a.ww + offv, buf, lane);
-    }
   }
   if (a.setstep) {
     mu = warp_nmax(mu);
@@ -499,7 +504,7 @@ __global__ void __launch_bounds__(64) k_dt(DCoef c, DState *st, const unsigned l
       st->umax = um;
       st->wmax = wm;
       st->vmax = vmax;
-      if (!isfinite(um) || !isfinite(wm) || !isfinite(vmax)) st->err = OTBL_ERR_NAN;
+      if (!isfinite(um) || !isfinite(wm) || !isfinite(vmax)) atomicCAS(&st->err, 0, OTBL_ERR_NAN);
       if (dt_mode == OTBL_DT_ADAPTIVE) {
         st->dt = dtloc;
       } else if (!st->dt_frozen) {
@@ -508,7 +513,7 @@ __global__ void __launch_bounds__(64) k_dt(DCoef c, DState *st, const unsigned l
       }
     }
     const double dt = st->dt;
-    if (!(dt > 0.0) || !isfinite(dt)) st->err = OTBL_ERR_NAN;
+    if (!(dt > 0.0) || !isfinite(dt)) atomicCAS(&st->err, 0, OTBL_ERR_NAN);
     const int q = m - 1;
     st->var1 = dt * (S[OTBL_S_RKCV + q] + S[OTBL_S_RKDV + q]);
     st->var2 = dt * S[OTBL_S_REX] * S[OTBL_S_RKCV + q];
@@ -833,7 +838,7 @@ __global__ void __launch_bounds__(128) k_genflu_cols(DCoef c, GenArgs a) {
     const int kll = max(kl[i], 1);
     return (inp(kll) * fsca[i] + inp(kll - 1) * (1 - fsca[i])) * ggg;
   };
-  if (kr == 2 && comp == 0 && r == 0 && !prof && a.err) *a.err = OTBL_ERR_NAN;
+  if (kr == 2 && comp == 0 && r == 0 && !prof && a.err) atomicCAS(a.err, 0, OTBL_ERR_NAN);
   double v;
   if (!a.tail) {
     v = val(r);
@@ -1260,7 +1265,7 @@ cudaError_t launch_reset_max(otbl_ctx *c) {
 }
 
 template <typename T>
-static cudaError_t products_t(otbl_ctx *c, int setstep, const ZTabT<T> &z) {
+static cudaError_t products_t(otbl_ctx *c, int setstep, int part, const ZTabT<T> &z) {
   ProdArgs<T> a;
   a.u = c->f[OTBL_F_U];
   a.v = c->f[OTBL_F_V];
@@ -1281,19 +1286,25 @@ static cudaError_t products_t(otbl_ctx *c, int setstep, const ZTabT<T> &z) {
   a.st = c->st;
   a.setstep = setstep;
   const int M = c->cfg.nz / 2;
-  dim3 g((c->cfg.ny + 1 + 3) / 4, c->cfg.nx);
+  // part 0: all planes, rows 1..ny+1; part 1: planes 2..nx-1, rows 1..ny
+  const dim3 g((c->cfg.ny + 1 - part + 3) / 4, c->cfg.nx - 2 * part);
   if (M == 256) {
     const size_t smem = (size_t)4 * (M + M / 8) * sizeof(V2<T>);
-    k_products_r<256, T><<<g, 128, smem, c->stream>>>(c->dc, z, a);
+    if (part == 0)
+      k_products_r<256, T, 0><<<g, 128, smem, c->stream>>>(c->dc, z, a);
+    else
+      k_products_r<256, T, 1><<<g, 128, smem, c->stream>>>(c->dc, z, a);
   } else {
     const size_t smem = (size_t)4 * 3 * M * sizeof(V2<T>);
-    cudaFuncSetAttribute(k_products<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_products<T><<<g, 128, smem, c->stream>>>(c->dc, z, a);
+    auto k = part == 0 ? k_products<T, 0> : k_products<T, 1>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k<<<g, 128, smem, c->stream>>>(c->dc, z, a);
   }
   return cudaGetLastError();
 }
 
-cudaError_t launch_products(otbl_ctx *c, int setstep) {
+cudaError_t launch_products(otbl_ctx *c, int setstep, int part) {
+  if (part == 1 && c->cfg.nx <= 2) return cudaSuccess;  // no interior planes
   prof_begin(c, PK_PRODUCTS);
   cudaError_t e;
   if (c->mixed) {
@@ -1303,9 +1314,9 @@ cudaError_t launch_products(otbl_ctx *c, int setstep) {
     z.M = c->cfg.nz / 2;
     z.nz = c->cfg.nz;
     z.nz2 = c->dc.nz2;
-    e = products_t<float>(c, setstep, z);
+    e = products_t<float>(c, setstep, part, z);
   } else {
-    e = products_t<double>(c, setstep, ztab(c));
+    e = products_t<double>(c, setstep, part, ztab(c));
   }
   prof_end(c);
   c->launches += 1;

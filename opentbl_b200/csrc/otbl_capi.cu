@@ -34,7 +34,9 @@ int dalloc(otbl_ctx *c, T **p, size_t count) {
     c->err = "cudaMalloc failed (" + std::to_string(bytes) + " bytes)";
     return OTBL_ERR_OOM;
   }
-  cudaMemset(q, 0, bytes);
+  // on the context stream: the streams are non-blocking, so work on the
+  // legacy default stream would not be ordered before their kernels
+  cudaMemsetAsync(q, 0, bytes, c->stream);
   c->allocs.push_back(q);
   c->bytes += bytes;
   *p = static_cast<T *>(q);
@@ -140,8 +142,16 @@ extern "C" int otbl_ctx_create(const otbl_config *cfg, const double *coef, int d
     delete c;
     return OTBL_ERR_NODEV;
   }
-  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess) {
+  // The context stream and `side` at the greatest priority, `side_lo` at the
+  // least: on B200 at 1025x193x512 the products' second half beside
+  // difvisxx took 52.3 ms per RK3 step this way, 52.9 at equal priorities
+  // and 53.3 with the side stream first.
+  int prio_lo = 0, prio_hi = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+  if (cudaStreamCreateWithPriority(&c->stream, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&c->side, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&c->side_lo, cudaStreamNonBlocking, prio_lo) != cudaSuccess) {
+    if (c->side) cudaStreamDestroy(c->side);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return OTBL_ERR_CUDA;
@@ -166,7 +176,8 @@ extern "C" int otbl_ctx_create(const otbl_config *cfg, const double *coef, int d
     }                         \
   } while (0)
   TRY(dalloc(c, &c->coef_dev, ncoef));
-  if (cudaMemcpy(c->coef_dev, coef, ncoef * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
+  if (cudaMemcpyAsync(c->coef_dev, coef, ncoef * sizeof(double), cudaMemcpyHostToDevice, c->stream) != cudaSuccess ||
+      cudaStreamSynchronize(c->stream) != cudaSuccess) {
     *out = c;
     return fail(c, OTBL_ERR_CUDA, "coefficient upload failed");
   }
@@ -177,7 +188,9 @@ extern "C" int otbl_ctx_create(const otbl_config *cfg, const double *coef, int d
     // FP32 copy of the packed coefficients for the FP32 operators
     std::vector<float> cf(coef, coef + ncoef);
     TRY(dalloc(c, &c->coef_dev_f, ncoef));
-    if (cudaMemcpy(c->coef_dev_f, cf.data(), ncoef * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) {
+    if (cudaMemcpyAsync(c->coef_dev_f, cf.data(), ncoef * sizeof(float), cudaMemcpyHostToDevice, c->stream) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(c->stream) != cudaSuccess) {
       *out = c;
       return fail(c, OTBL_ERR_CUDA, "coefficient upload failed");
     }
@@ -277,11 +290,14 @@ extern "C" int otbl_ctx_rebind(otbl_ctx *c, const otbl_config *cfg, const double
   const size_t ncoef = o.off[OTBL_C_COUNT];
   c->cfg = *cfg;
   c->coef_host.assign(coef, coef + ncoef);
-  OTBL_CUDA_TRY(c, cudaMemcpy(c->coef_dev, coef, ncoef * sizeof(double), cudaMemcpyHostToDevice));
+  OTBL_CUDA_TRY(c, cudaMemcpyAsync(c->coef_dev, coef, ncoef * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  OTBL_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   c->dc = make_dcoef<double>(c->coef_dev, o, *cfg);
   if (c->mixed) {
     std::vector<float> cf(coef, coef + ncoef);
-    OTBL_CUDA_TRY(c, cudaMemcpy(c->coef_dev_f, cf.data(), ncoef * sizeof(float), cudaMemcpyHostToDevice));
+    OTBL_CUDA_TRY(c, cudaMemcpyAsync(c->coef_dev_f, cf.data(), ncoef * sizeof(float), cudaMemcpyHostToDevice,
+                                     c->stream));
+    OTBL_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     c->dcf = make_dcoef<float>(c->coef_dev_f, o, *cfg);
   }
   if (check(c, launch_pois_lu(c), "pois_lu") != OTBL_OK) return OTBL_ERR_CUDA;
@@ -299,9 +315,11 @@ extern "C" void otbl_ctx_destroy(otbl_ctx *c) {
   }
   for (cudaEvent_t e : c->prof_pool) cudaEventDestroy(e);
   if (c->side) cudaStreamSynchronize(c->side);
+  if (c->side_lo) cudaStreamSynchronize(c->side_lo);
   for (void *p : c->allocs) cudaFree(p);
   for (cudaEvent_t e : c->ev)
     if (e) cudaEventDestroy(e);
+  if (c->side_lo) cudaStreamDestroy(c->side_lo);
   if (c->side) cudaStreamDestroy(c->side);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -439,6 +457,8 @@ extern "C" int otbl_rhsp(otbl_ctx *c, int m, int setstep) {
     c->stream = main_s;
     cudaEventRecord(c->ev[3], c->side);
     cudaStreamWaitEvent(main_s, c->ev[3], 0);
+    cudaEventRecord(c->ev[4], c->side_lo);
+    cudaStreamWaitEvent(main_s, c->ev[4], 0);
   }
   return st;
 }
@@ -464,17 +484,26 @@ static int rhsp_issue(otbl_ctx *c, int m, int setstep) {
     LAUNCH(c, launch_interpx(c));
     LAUNCH(c, launch_interpy(c));
   }
-  LAUNCH(c, launch_products(c, setstep));
-  // k_dt (needs the CFL maxima of the products) beside difvisxx; genflu
-  // (needs dt; writes plane 1 of u, v, w, which difvisxx reads and the rhsp
-  // tail does not touch) beside the tail; joined before outflow_correction
+  LAUNCH(c, launch_products(c, setstep, 0));
+  // Beside difvisxx and the u tail: products part 1 (vw, vv, ww: inputs and
+  // outputs disjoint from part 0's, from difvisxx's and from the u tail's)
+  // on side_lo; k_dt (needs the CFL maxima, all from part 0), then genflu
+  // on side. genflu needs dt, writes plane 1 of u, v, w, which difvisxx
+  // reads and the rhsp tail does not touch, and reads plane xout, which the
+  // tail rewrites: it runs once difvisxx is done, and the tail's first
+  // velocity write waits for it. The u tail waits for k_dt, the v and w
+  // tails for part 1.
   OTBL_CUDA_TRY(c, cudaEventRecord(c->ev[0], main_s));
+  OTBL_CUDA_TRY(c, cudaStreamWaitEvent(c->side_lo, c->ev[0], 0));
   OTBL_CUDA_TRY(c, cudaStreamWaitEvent(c->side, c->ev[0], 0));
+  c->stream = c->side_lo;
+  cudaError_t e = launch_products(c, setstep, 1);
+  if (e == cudaSuccess) e = cudaEventRecord(c->ev[4], c->side_lo);
   c->stream = c->side;
-  cudaError_t e = launch_dt(c, m, setstep);
+  if (e == cudaSuccess) e = launch_dt(c, m, setstep);
+  if (e == cudaSuccess) e = cudaEventRecord(c->ev[1], c->side);
   c->stream = main_s;
-  if (check(c, e, "launch_dt") != OTBL_OK) return OTBL_ERR_CUDA;
-  OTBL_CUDA_TRY(c, cudaEventRecord(c->ev[1], c->side));
+  if (check(c, e, "products part 1 / k_dt") != OTBL_OK) return OTBL_ERR_CUDA;
   LAUNCH(c, launch_difvisx(c));
   OTBL_CUDA_TRY(c, cudaEventRecord(c->ev[2], main_s));
   OTBL_CUDA_TRY(c, cudaStreamWaitEvent(c->side, c->ev[2], 0));
@@ -484,8 +513,9 @@ static int rhsp_issue(otbl_ctx *c, int m, int setstep) {
   if (check(c, e, "launch_genflu") != OTBL_OK) return OTBL_ERR_CUDA;
   OTBL_CUDA_TRY(c, cudaEventRecord(c->ev[3], c->side));
   OTBL_CUDA_TRY(c, cudaStreamWaitEvent(main_s, c->ev[1], 0));
-  LAUNCH(c, launch_final(c));
-  OTBL_CUDA_TRY(c, cudaStreamWaitEvent(main_s, c->ev[3], 0));
+  LAUNCH(c, launch_final(c, 1, c->ev[3]));
+  OTBL_CUDA_TRY(c, cudaStreamWaitEvent(main_s, c->ev[4], 0));
+  LAUNCH(c, launch_final(c, 2 | 4));
   return OTBL_OK;
 }
 
@@ -526,9 +556,9 @@ extern "C" int otbl_advance(otbl_ctx *c, int nsteps) {
 extern "C" int otbl_sync(otbl_ctx *c) {
   if (!c) return OTBL_ERR_ARG;
   cudaSetDevice(c->device);
-  OTBL_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   int err = 0;
-  OTBL_CUDA_TRY(c, cudaMemcpy(&err, &c->st->err, sizeof(int), cudaMemcpyDeviceToHost));
+  OTBL_CUDA_TRY(c, cudaMemcpyAsync(&err, &c->st->err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  OTBL_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   if (err) {
     c->err = err == OTBL_ERR_TIMEOUT ? "a device-side wait of a kernel timed out"
                                      : "non-finite value in the CFL reduction";

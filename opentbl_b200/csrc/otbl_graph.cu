@@ -113,7 +113,8 @@ extern "C" int otbl_graph_create(otbl_ctx *const *ctxs, int n, int nsteps, otbl_
     graph_free(g);
     return st != OTBL_OK ? st : OTBL_ERR_CUDA;
   }
-  if (cudaGraphInstantiate(&g->exec, g->graph, 0) != cudaSuccess) {
+  // keep the priorities of the streams the kernels were captured from
+  if (cudaGraphInstantiate(&g->exec, g->graph, cudaGraphInstantiateFlagUseNodePriority) != cudaSuccess) {
     cudaGetLastError();
     graph_free(g);
     return OTBL_ERR_CUDA;
@@ -247,11 +248,13 @@ extern "C" int otbl_selftest_wait(otbl_ctx *c, int *status) {
   int *d = nullptr;
   if (cudaMalloc(&d, sizeof(int)) != cudaSuccess) return OTBL_ERR_OOM;
   const int init = -1;
-  cudaMemcpy(d, &init, sizeof(int), cudaMemcpyHostToDevice);
+  cudaMemcpyAsync(d, &init, sizeof(int), cudaMemcpyHostToDevice, c->stream);
   k_wait_selftest<<<1, 64, 0, c->stream>>>(d, 1000000ull);  // 1 ms
   int st = OTBL_OK;
-  if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(c->stream) != cudaSuccess) st = OTBL_ERR_CUDA;
-  if (st == OTBL_OK && cudaMemcpy(status, d, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) st = OTBL_ERR_CUDA;
+  if (cudaGetLastError() != cudaSuccess) st = OTBL_ERR_CUDA;
+  if (st == OTBL_OK && cudaMemcpyAsync(status, d, sizeof(int), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess)
+    st = OTBL_ERR_CUDA;
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) st = OTBL_ERR_CUDA;
   cudaFree(d);
   return st;
 }

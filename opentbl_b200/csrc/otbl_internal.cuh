@@ -91,10 +91,13 @@ struct otbl_ctx {
   otbl_config cfg;
   int device;
   cudaStream_t stream;
-  // second stream of the substep: k_dt beside difvisxx, genflu beside the
-  // rhsp tail (fork/join by events, so a graph capture records the overlap)
-  cudaStream_t side = nullptr;
-  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  // side streams of the substep (fork/join by events, so a graph capture
+  // records the overlap): `side`, at the context stream's priority, runs
+  // interpyy beside interpxx, k_dt and genflu; `side_lo`, at the lowest
+  // priority, runs the second half of the products beside difvisxx and the
+  // u tail, taking the SM slots those leave free
+  cudaStream_t side = nullptr, side_lo = nullptr;
+  cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   otbl::DCoef dc;
   otbl::DCoefT<float> dcf;  // FP32 coefficients (mixed path)
   // threads per CTA of the line kernels that otbl_autotune times:
@@ -160,11 +163,15 @@ cudaError_t launch_interpy(otbl_ctx *c);
 // interpyy's checkpoint region in a line scratch when it can run beside
 // interpxx, else nullptr
 double *interpy_ck_tail(otbl_ctx *c, double *s);
-cudaError_t launch_products(otbl_ctx *c, int setstep);
+// part 0: uu, uw, uv and the CFL maxima; part 1: vw, vv, ww
+cudaError_t launch_products(otbl_ctx *c, int setstep, int part);
 cudaError_t launch_difvisx(otbl_ctx *c);
 cudaError_t launch_dt(otbl_ctx *c, int m, int setstep);
 cudaError_t launch_genflu(otbl_ctx *c, int tail);
-cudaError_t launch_final(otbl_ctx *c);
+// the rhsp tail of the velocity components in the bit mask comps (1 u, 2 v,
+// 4 w), in that order; the first kernel that writes a velocity component
+// waits for before_vel when it is not null
+cudaError_t launch_final(otbl_ctx *c, unsigned comps, cudaEvent_t before_vel = nullptr);
 cudaError_t launch_outflow(otbl_ctx *c);
 cudaError_t launch_pois(otbl_ctx *c, int m);
 cudaError_t launch_reset_max(otbl_ctx *c);
