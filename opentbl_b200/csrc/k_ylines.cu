@@ -557,8 +557,10 @@ struct FinalBox {
   static constexpr int kp = cx + r128(KF * T * E);            // W KF rows
   static constexpr int hp = kp + r128(KF * T * E);            // W KF rows
   static constexpr int p = hp + r128(KF * T * E);             // W PR x PP
-  static constexpr int stage = p + r128(PR * PP * T * E);
-  static constexpr unsigned tx = (unsigned)((KF + 2) * T * E + (KF + 2) * T * 8 + 3 * KF * T * E + PR * PP * T * E);
+  static constexpr int rc = p + r128(PR * PP * T * E);         // KF coefficient rows
+  static constexpr int stage = rc + KF * 128;
+  static constexpr unsigned tx =
+      (unsigned)((KF + 2) * T * E + (KF + 2) * T * 8 + 3 * KF * T * E + PR * PP * T * E + KF * 128);
   static constexpr int NS = FinalTune<W>::ns_tma;  // ring stages
   static constexpr int smem = NS * stage + 128;    // the stages and the barriers
 };
@@ -593,6 +595,7 @@ __global__ void __launch_bounds__(128) k_final_tb(DCoef c, DCoefT<W> cw, FinalSt
     tma_load_3d(b + B::kp, &maps.kp, kr0, s0, i - 1, &full[stg]);
     tma_load_3d(b + B::hp, &maps.hp, kr0, s0, i - 1, &full[stg]);
     tma_load_3d(b + B::p, &maps.p, kr0, s0, i - 1, &full[stg]);
+    tma_load_2d(b + B::rc, &maps.rc, 0, s0, &full[stg]);
   };
   if (t == 0) {
     for (int q = 0; q < NS; ++q) mbar_init(&full[q], 1);
@@ -620,9 +623,7 @@ __global__ void __launch_bounds__(128) k_final_tb(DCoef c, DCoefT<W> cw, FinalSt
   const int which = COMP == 1 ? 1 : 0;
   // differzy and vistyy run in W on the coefficient copy cw (FP32 on the
   // mixed path); the RHS assembly, RK3 combination and implzy in FP64
-  const W *dcy = which == 0 ? cw.dcyu : cw.dcyv, *ecd = which == 0 ? cw.cofcyu : cw.cofcyv;
-  const W *viy = which == 0 ? cw.viyu : cw.viyv, *ecv = which == 0 ? cw.cofvyu : cw.cofvyv;
-  const double *vyi = which == 0 ? c.vyui : c.vyvi;
+  // (per-row coefficients: k_tail_rows' rows, staged with each segment)
   const double *fac = COMP == 1 ? a.fac_v : a.fac_u;
   auto Pg = [&](int r) { return (double)__ldg(prod + (size_t)min(max(r, 0), ny - 1) * S); };
   auto Vg = [&](int r) { return __ldg(vel + (size_t)min(max(r, 0), jee - 1) * S); };
@@ -660,13 +661,13 @@ __global__ void __launch_bounds__(128) k_final_tb(DCoef c, DCoefT<W> cw, FinalSt
     ub1 = -1.0 / M4(ib, 2, 1) * (M4(ib, 2, 2) * s2 + M4(ib, 2, 3) * s3 + M4(ib, 2, 4) * s4);
     ubt = -1.0 / M2(cc, 1, 1) * (M2(cc, 1, 2) * sn + M2(cc, 1, 3) * sn1 + M2(cc, 1, 4) * sn2);
   }
-  auto rd = [&](int r, W gm, W g0, W gp) {
-    const W in = which == 0 ? __ldg(ecd + 2 * r + 1) * g0 + __ldg(ecd + 2 * r) * gm
-                            : __ldg(ecd + 2 * r + 1) * gp + __ldg(ecd + 2 * r) * g0;
+  // q: the row's W coefficients in shared memory (k_tail_rows' layout)
+  auto rd = [&](int r, const W *q, W gm, W g0, W gp) {
+    const W in = which == 0 ? q[1] * g0 + q[0] * gm : q[1] * gp + q[0] * g0;
     return r == 0 ? bot : (r == jee - 1 ? top : in);
   };
-  auto rv = [&](int r, W um, W u0, W up) {
-    const W in = __ldg(ecv + 3 * r) * up + __ldg(ecv + 3 * r + 1) * u0 + __ldg(ecv + 3 * r + 2) * um;
+  auto rv = [&](int r, const W *q, W um, W u0, W up) {
+    const W in = q[5] * up + q[6] * u0 + q[7] * um;
     return r == 0 ? b0 : (r == jee - 1 ? bN : in);
   };
   const W *ck = reinterpret_cast<const W *>(fs.ck) + (active ? col : 0);
@@ -694,6 +695,7 @@ __global__ void __launch_bounds__(128) k_final_tb(DCoef c, DCoefT<W> cw, FinalSt
     const W *sk = reinterpret_cast<const W *>(bs + B::kp);
     const W *sh = reinterpret_cast<const W *>(bs + B::hp);
     const W *spp = reinterpret_cast<const W *>(bs + B::p);
+    const double *rcs = reinterpret_cast<const double *>(bs + B::rc);
     W ad = ckd, av = ckv;
     if (sg >= 1) {  // next segment's checkpoints, ahead of use
       ckd = ck[(size_t)(2 * (sg - 1)) * ncol];
@@ -704,12 +706,12 @@ __global__ void __launch_bounds__(128) k_final_tb(DCoef c, DCoefT<W> cw, FinalSt
 #pragma unroll
     for (int b = 0; b < KF; ++b) {
       const int r = s0 + b;
+      const W *q = reinterpret_cast<const W *>(rcs + 16 * b + 5);
       if (r < jee) {
         if (!last)
-          ad = rd(r, sp[b * TB + t], sp[(b + 1) * TB + t], sp[(b + 2) * TB + t]) +
-               (r > 0 ? __ldg(dcy + 3 * r) : W(0)) * ad;
-        av = rv(r, (W)sv[b * TB + t], (W)sv[(b + 1) * TB + t], (W)sv[(b + 2) * TB + t]) +
-             (r > 0 ? __ldg(viy + 3 * r) : W(0)) * av;
+          ad = rd(r, q, sp[b * TB + t], sp[(b + 1) * TB + t], sp[(b + 2) * TB + t]) + (r > 0 ? q[2] : W(0)) * ad;
+        av = rv(r, q, (W)sv[b * TB + t], (W)sv[(b + 1) * TB + t], (W)sv[(b + 2) * TB + t]) +
+             (r > 0 ? q[8] : W(0)) * av;
       }
       ydv[b] = ad;
       yvv[b] = av;
@@ -718,8 +720,10 @@ __global__ void __launch_bounds__(128) k_final_tb(DCoef c, DCoefT<W> cw, FinalSt
     for (int b = KF - 1; b >= 0; --b) {
       const int r = s0 + b, j = r + 1;
       if (r >= jee) continue;
-      if (!last) xd = (ydv[b] - __ldg(dcy + 3 * r + 2) * xd) * __ldg(dcy + 3 * r + 1);
-      xv = (yvv[b] - __ldg(viy + 3 * r + 2) * xv) * __ldg(viy + 3 * r + 1);
+      const double *rq = rcs + 16 * b;
+      const W *q = reinterpret_cast<const W *>(rq + 5);
+      if (!last) xd = (ydv[b] - q[4] * xd) * q[3];
+      xv = (yvv[b] - q[10] * xv) * q[9];
       // RHS assembly (rhsp.F90:164-169, 181-204, 351-418, 423-445)
       const double d1 = last ? 0.0 : (double)xd;
       const double u0 = sv[(b + 1) * TB + t];
@@ -761,7 +765,7 @@ __global__ void __launch_bounds__(128) k_final_tb(DCoef c, DCoefT<W> cw, FinalSt
       } else if (COMP == 0) {
         st = last ? u0 : u0 - var1 * idxx * ((double)spp[(B::PR + b) * TB + t] - (double)spp[b * TB + t]);
       } else if (COMP == 1) {
-        st = u0 - var1 * c.idyy[r] * ((double)spp[(b + 1) * TB + t] - (double)spp[b * TB + t]);
+        st = u0 - var1 * rq[4] * ((double)spp[(b + 1) * TB + t] - (double)spp[b * TB + t]);
       } else {
         const double pp = (double)spp[b * TB + tk];
         const double avz = var1 * kz;
@@ -770,11 +774,10 @@ __global__ void __launch_bounds__(128) k_final_tb(DCoef c, DCoefT<W> cw, FinalSt
       const double res = st - (var3 * R + v2 * (double)xv + var4 * (double)sh[b * TB + t]);
       hp[(size_t)r * S] = (W)R;
       if (r < n) {
-        double v = __ldg(vyi + 3 * (r + 1)) * res + __ldg(vyi + 3 * (r + 1) + 1) * res1 +
-                   __ldg(vyi + 3 * (r + 1) + 2) * res2;
+        double v = rq[1] * res + rq[2] * res1 + rq[3] * res2;
         if (r == 0) v = v - a1raw * ub1;
         if (r == n - 1) v = v - a3raw * ubt;
-        yel = v + fac[3 * (r + 2) + 2] * yel;
+        yel = v + rq[0] * yel;
         yq[(size_t)r * ncol] = yel;
       }
       res2 = res1;
@@ -1056,6 +1059,8 @@ static bool encode_field(CUtensorMap *m, const void *base, size_t esz, int plane
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+static bool encode_rows(CUtensorMap *m, const double *base, int rows, int brows);
+
 template <typename W>
 static bool build_maps_t(otbl_ctx *c) {
   constexpr int KF = FinalTune<W>::kf_tma;
@@ -1079,6 +1084,7 @@ static bool build_maps_t(otbl_ctx *c) {
     ok = ok && encode_field(&m.cx, cx, ew, nx, jee, nz1, KF, 1);
     ok = ok && encode_field(&m.hp, hp, ew, nx, jee, nz1, KF, 1);
     ok = ok && encode_field(&m.p, c->f[OTBL_F_P], ew, nx, ny, nz1, comp == 1 ? KF + 1 : KF, comp == 0 ? 2 : 1);
+    ok = ok && encode_rows(&m.rc, c->w.rowc + (comp == 1 ? (size_t)16 * (ny + 2) : 0), ny + 2, KF);
   }
   return ok;
 }
@@ -1092,6 +1098,68 @@ bool build_y_maps(otbl_ctx *c) {
   for (int f = 0; f < 3 && ok; ++f) ok = encode_field(&c->ymi.g[f], in[f], 8, nx, rows[f], nz1, K + 2, 1);
   c->ymaps_ok = ok;
   return ok;
+}
+
+// One 128-byte row per y row r and tail kind (table 0: the u and w tails,
+// u-type coefficients; table 1: the v tail): the FP64 values fac[3(r+2)+2]
+// (the implzy factor of the descending elimination), vyi[3(r+1)+0..2] and
+// idyy[r], then in W ecd[2r+0..1], dcy[3r+0..2], ecv[3r+0..2],
+// viy[3r+0..2] (differzy's and vistyy's right-hand-side and LU
+// coefficients). k_final_tb's ring stages a segment's rows with its field
+// boxes, so its sweeps read them from shared memory as broadcasts. Entries
+// that a row does not use are 0.
+template <typename W>
+__global__ void __launch_bounds__(128) k_tail_rows(DCoef c, DCoefT<W> cw, const double *fac_u, const double *fac_v,
+                                                   double *rowc) {
+  const int ny = c.ny, R = ny + 2;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= 2 * R) return;
+  const int which = e / R, r = e - which * R;
+  const int jee = which == 1 ? ny : ny + 1, n = jee - 2;
+  double *row = rowc + (size_t)e * 16;
+  const double *fac = which == 1 ? fac_v : fac_u;
+  const double *vyi = which == 0 ? c.vyui : c.vyvi;
+  row[0] = r < n ? fac[3 * (r + 2) + 2] : 0.0;
+  for (int q = 0; q < 3; ++q) row[1 + q] = r < n ? vyi[3 * (r + 1) + q] : 0.0;
+  row[4] = (which == 1 && r < ny) ? c.idyy[r] : 0.0;
+  W *q = reinterpret_cast<W *>(row + 5);
+  constexpr int NW = (int)((128 - 5 * sizeof(double)) / sizeof(W));
+  for (int k = 0; k < NW; ++k) q[k] = W(0);
+  if (r < jee) {
+    const W *dcy = which == 0 ? cw.dcyu : cw.dcyv, *ecd = which == 0 ? cw.cofcyu : cw.cofcyv;
+    const W *viy = which == 0 ? cw.viyu : cw.viyv, *ecv = which == 0 ? cw.cofvyu : cw.cofvyv;
+    q[0] = ecd[2 * r];
+    q[1] = ecd[2 * r + 1];
+    for (int k = 0; k < 3; ++k) {
+      q[2 + k] = dcy[3 * r + k];
+      q[5 + k] = ecv[3 * r + k];
+      q[8 + k] = viy[3 * r + k];
+    }
+  }
+}
+
+cudaError_t launch_tail_rows(otbl_ctx *c) {
+  if (!c->fmaps_ok) return cudaSuccess;
+  const int n = 2 * (c->cfg.ny + 2);
+  if (c->mixed)
+    k_tail_rows<float><<<(n + 127) / 128, 128, 0, c->stream>>>(c->dc, c->dcf, c->w.fac_u, c->w.fac_v, c->w.rowc);
+  else
+    k_tail_rows<double><<<(n + 127) / 128, 128, 0, c->stream>>>(c->dc, c->dc, c->w.fac_u, c->w.fac_v, c->w.rowc);
+  c->launches += 1;
+  return cudaGetLastError();
+}
+
+// 2D map of one table of Work::rowc: [ny+2 rows][16 doubles], boxes of KF rows
+static bool encode_rows(CUtensorMap *m, const double *base, int rows, int brows) {
+  auto fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(tensor_map_encoder());
+  if (!fn || ((uintptr_t)base) % 16 != 0) return false;
+  const cuuint64_t dims[2] = {16, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {16 * sizeof(double)};
+  const cuuint32_t box[2] = {16, (cuuint32_t)brows};
+  const cuuint32_t es[2] = {1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double *>(base), dims, strides, box, es,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 bool build_final_maps(otbl_ctx *c) {

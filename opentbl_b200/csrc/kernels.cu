@@ -1327,9 +1327,11 @@ cudaError_t launch_dt(otbl_ctx *c, int m, int setstep) {
   prof_begin(c, PK_DT);
   k_dt<<<1, 64, 0, c->stream>>>(c->dc, c->st, c->w.vm_bits, c->w.fac_u, c->w.fac_v, m, setstep,
                                 c->cfg.dt_mode, c->cfg.dt_fixed);
-  prof_end(c);
   c->launches += 1;
-  return cudaGetLastError();
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = launch_tail_rows(c);
+  prof_end(c);
+  return e;
 }
 
 cudaError_t launch_genflu(otbl_ctx *c, int tail) {

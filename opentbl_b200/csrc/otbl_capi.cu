@@ -243,6 +243,7 @@ extern "C" int otbl_ctx_create(const otbl_config *cfg, const double *coef, int d
   TRY(dalloc(c, &w.vm_bits, (size_t)ny + 1));
   TRY(dalloc(c, &w.fac_u, 3 * (size_t)(ny + 4)));
   TRY(dalloc(c, &w.fac_v, 3 * (size_t)(ny + 4)));
+  TRY(dalloc(c, &w.rowc, 2 * 16 * (size_t)(ny + 2)));
   TRY(dalloc(c, &w.gf, genflu_tab_doubles(ny)));
   TRY(dalloc(c, &w.pois_dinv, (size_t)nx * ny * (nz1 / 2)));
 #undef TRY

@@ -63,6 +63,7 @@ struct Work {
   double *twx2;                // exp(-i pi k/(2n)), k = 0..n-1
   unsigned long long *vm_bits; // vm(j) maxima, j = 1..ny
   double *fac_u, *fac_v;       // implzy LU factors for the current dt (3*(ny+1))
+  double *rowc;                // k_final_tb's per-row coefficients, [2][ny+2][16]
   double *gf;                  // genflu tables (genflu_tab_doubles)
   double *pois_dinv;           // pivots of the (x-mode, kz) y-systems, [i][j][k]
 };
@@ -72,6 +73,7 @@ struct Work {
 struct FinalMaps {
   CUtensorMap prod, kp, vel, cx, hp, p;
   CUtensorMap prod_a, vel_a;  // pass A: boxes of 8 + 2 rows
+  CUtensorMap rc;             // per-row coefficients (Work::rowc)
 };
 
 // TMA descriptors of interpyy's inputs (u, w, v), boxes of 128 kr x rows
@@ -181,6 +183,9 @@ cudaError_t launch_energies(otbl_ctx *c);
 // builds c->fmaps (false if TMA cannot address the fields, e.g. an FP32 row
 // pitch that is not a multiple of 16 bytes)
 bool build_final_maps(otbl_ctx *c);
+// fills Work::rowc from the coefficients and this substep's implzy factors
+// (after k_dt, on the same stream); a no-op without the TMA-fed tail
+cudaError_t launch_tail_rows(otbl_ctx *c);
 // the driver's cuTensorMapEncodeTiled (as void *), nullptr if unavailable
 void *tensor_map_encoder();
 bool build_x_maps(otbl_ctx *c);
