@@ -236,8 +236,9 @@ __global__ void __launch_bounds__(TB) k_xline_t(DCoefT<T> c, XStream a, int *err
   constexpr int GBYTES = NB * GR * 32 * (int)sizeof(TG);
   constexpr int GB = (GBYTES + 127) / 128 * 128;
   constexpr int UBYTES = DV ? NB * UR * 32 * 8 : 0;
-  constexpr int STG = GB + UBYTES;
-  constexpr unsigned TX = (unsigned)(GBYTES + UBYTES);
+  constexpr int RCB = K * 16 * (int)sizeof(T);  // the segment's coefficient rows
+  constexpr int STG = GB + UBYTES + RCB;
+  constexpr unsigned TX = (unsigned)(GBYTES + UBYTES + RCB);
   extern __shared__ __align__(128) unsigned char smraw[];
   uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + 2 * STG);
   const int f = blockIdx.y, np = pick3(a.np, f);
@@ -248,6 +249,7 @@ __global__ void __launch_bounds__(TB) k_xline_t(DCoefT<T> c, XStream a, int *err
   const int mpc = active ? mp : np - 1;
   const CUtensorMap *mg = f == 0 ? &maps.g[0] : (f == 1 ? &maps.g[1] : &maps.g[2]);
   const CUtensorMap *mu = f == 0 ? &maps.u[0] : (f == 1 ? &maps.u[1] : &maps.u[2]);
+  const CUtensorMap *mr = f == 0 ? &maps.r[0] : (f == 1 ? &maps.r[1] : &maps.r[2]);
   const int nx = c.nx, xr = c.xround, which = pick3(a.which, f);
   const int nseg = (nx + K - 1) / K;
   auto seg_of = [&](int it) { return it < nseg ? it : 2 * nseg - 1 - it; };
@@ -260,6 +262,7 @@ __global__ void __launch_bounds__(TB) k_xline_t(DCoefT<T> c, XStream a, int *err
       tma_load_2d(b + j * GR * 32 * (int)sizeof(TG), mg, mp0 + 32 * j, DV ? s0 - 1 : s0, &bar[stg]);
       if (DV) tma_load_2d(b + GB + j * UR * 32 * 8, mu, mp0 + 32 * j, s0 - 1, &bar[stg]);
     }
+    tma_load_2d(b + GB + UBYTES, mr, 0, s0, &bar[stg]);
   };
   if (t == 0) {
     mbar_init(&bar[0], 1);
@@ -272,16 +275,11 @@ __global__ void __launch_bounds__(TB) k_xline_t(DCoefT<T> c, XStream a, int *err
   T *ck = reinterpret_cast<T *>(pick3(a.ck, f)) + mpc;
   const int gofs = ((t >> 5) * GR) * 32 + (t & 31), uofs = ((t >> 5) * UR) * 32 + (t & 31);
   // ---- operator setup (boundary stencils from global memory)
-  const T *icon, *econ, *iconv = nullptr, *econv = nullptr;
   T gb0, gbN, ub0 = T(0), ubN = T(0), uN = T(0), uN1 = T(0);
   const T rex = c.S[OTBL_S_REX], idx = c.S[OTBL_S_IDX], uinf = c.S[OTBL_S_UINF];
   if constexpr (DV) {
     const TG *gin = static_cast<const TG *>(pick3(a.in, f)) + mpc;
     const double *uin = pick3(a.in2, f) + mpc;
-    icon = which == 0 ? c.dcxu : c.dcxv;
-    iconv = which == 0 ? c.vixu : c.vixv;
-    econ = which == 0 ? c.cofcxu : c.cofcxv;
-    econv = which == 0 ? c.cofvxu : c.cofvxv;
     const int chv = which == 0 ? 1 : 2, chv1 = chv + 2, ic = which == 0 ? 3 : 1;
     const T *db = c.dcbx, *vb = c.cofvbx;
     auto G = [&](int i) { return (T)rnd(__ldg(gin + (size_t)i * np), xr); };
@@ -296,8 +294,6 @@ __global__ void __launch_bounds__(TB) k_xline_t(DCoefT<T> c, XStream a, int *err
           M4(vb, ic + 1, 4) * U(nx - 4);
   } else {
     const double *gin = static_cast<const double *>(pick3(a.in, f)) + mpc;
-    icon = which == 0 ? c.inxu : c.inxv;
-    econ = which == 0 ? c.cofiux : c.cofivx;
     const int chi = which == 0 ? 2 : 1, chi2 = which == 0 ? 3 : 4;
     const T *ib = c.inbx;
     auto G = [&](int i) { return (T)rnd(__ldg(gin + (size_t)i * np), xr); };
@@ -306,15 +302,11 @@ __global__ void __launch_bounds__(TB) k_xline_t(DCoefT<T> c, XStream a, int *err
           M4(ib, chi, 4) * G(nx - 4);
   }
   // right-hand sides: interpxx e1 g_i + e2 g_{i+1}; difvisxx convective
-  // e1 g_{i-1} + e2 g_i and viscous f1 u_{i+1} + f2 u_i + f3 u_{i-1}
-  auto rg = [&](int i, T ga, T gb) {
-    return i == 0 ? gb0 : (i == nx - 1 ? gbN : __ldg(econ + 2 * i) * ga + __ldg(econ + 2 * i + 1) * gb);
-  };
-  auto ru = [&](int i, T um, T u0, T up) {
-    return i == 0 ? ub0
-                  : (i == nx - 1 ? ubN
-                                 : __ldg(econv + 3 * i) * up + __ldg(econv + 3 * i + 1) * u0 +
-                                       __ldg(econv + 3 * i + 2) * um);
+  // e1 g_{i-1} + e2 g_i and viscous f1 u_{i+1} + f2 u_i + f3 u_{i-1}; q is
+  // the plane's coefficient row in shared memory (k_x_rows' layout)
+  auto rg = [&](int i, const T *q, T ga, T gb) { return i == 0 ? gb0 : (i == nx - 1 ? gbN : q[0] * ga + q[1] * gb); };
+  auto ru = [&](int i, const T *q, T um, T u0, T up) {
+    return i == 0 ? ub0 : (i == nx - 1 ? ubN : q[5] * up + q[6] * u0 + q[7] * um);
   };
   T yg = T(0), yu = T(0), xg = T(0), xu = T(0);
   for (int it = 0; it < 2 * nseg; ++it) {
@@ -330,6 +322,7 @@ __global__ void __launch_bounds__(TB) k_xline_t(DCoefT<T> c, XStream a, int *err
     const unsigned char *bs = smraw + stg * STG;
     const TG *gs = reinterpret_cast<const TG *>(bs) + gofs;
     const double *us = reinterpret_cast<const double *>(bs + GB) + uofs;
+    const T *rcs = reinterpret_cast<const T *>(bs + GB + UBYTES);
     auto g = [&](int b) { return (T)rnd(gs[b * 32], xr); };
     auto u = [&](int b) { return (T)rnd(us[b * 32], xr); };
     if (it < nseg) {  // forward sweep, checkpoint at the segment start
@@ -338,9 +331,10 @@ __global__ void __launch_bounds__(TB) k_xline_t(DCoefT<T> c, XStream a, int *err
 #pragma unroll
       for (int b = 0; b < K; ++b) {
         const int i = s0 + b;
+        const T *q = rcs + 16 * b;
         if (i < nx) {
-          yg = rg(i, g(b), g(b + 1)) + (i > 0 ? __ldg(icon + 3 * i) : T(0)) * yg;
-          if (DV) yu = ru(i, u(b), u(b + 1), u(b + 2)) + (i > 0 ? __ldg(iconv + 3 * i) : T(0)) * yu;
+          yg = rg(i, q, g(b), g(b + 1)) + (i > 0 ? q[2] : T(0)) * yg;
+          if (DV) yu = ru(i, q, u(b), u(b + 1), u(b + 2)) + (i > 0 ? q[8] : T(0)) * yu;
         }
       }
     } else {  // backward sweep: recompute the segment, then substitute
@@ -349,9 +343,10 @@ __global__ void __launch_bounds__(TB) k_xline_t(DCoefT<T> c, XStream a, int *err
 #pragma unroll
       for (int b = 0; b < K; ++b) {
         const int i = s0 + b;
+        const T *q = rcs + 16 * b;
         if (i < nx) {
-          a1 = rg(i, g(b), g(b + 1)) + (i > 0 ? __ldg(icon + 3 * i) : T(0)) * a1;
-          if (DV) a2 = ru(i, u(b), u(b + 1), u(b + 2)) + (i > 0 ? __ldg(iconv + 3 * i) : T(0)) * a2;
+          a1 = rg(i, q, g(b), g(b + 1)) + (i > 0 ? q[2] : T(0)) * a1;
+          if (DV) a2 = ru(i, q, u(b), u(b + 1), u(b + 2)) + (i > 0 ? q[8] : T(0)) * a2;
         }
         y1[b] = a1;
         y2[b] = a2;
@@ -359,11 +354,12 @@ __global__ void __launch_bounds__(TB) k_xline_t(DCoefT<T> c, XStream a, int *err
 #pragma unroll
       for (int b = K - 1; b >= 0; --b) {
         const int i = s0 + b;
+        const T *q = rcs + 16 * b;
         if (i < nx) {
-          xg = (y1[b] - __ldg(icon + 3 * i + 2) * xg) * __ldg(icon + 3 * i + 1);
+          xg = (y1[b] - q[4] * xg) * q[3];
           T v = xg;
           if (DV) {
-            xu = (y2[b] - __ldg(iconv + 3 * i + 2) * xu) * __ldg(iconv + 3 * i + 1);
+            xu = (y2[b] - q[10] * xu) * q[9];
             v = i == nx - 1 ? uinf * (uN - uN1) * idx + rex * T(0) : xg + rex * xu;
           }
           out[(size_t)i * np] = (T)rnd(v, xr);
@@ -380,7 +376,7 @@ static void xline_t_launch(otbl_ctx *c, const DCoefT<T> &dc, const XStream &a, c
   auto smem = [&](int tb) {
     const int nb = tb / 32;
     const int gb = (nb * (K + 1) * 32 * (int)sizeof(TG) + 127) / 128 * 128;
-    return 2 * (gb + (DV ? nb * (K + 2) * 32 * 8 : 0)) + 128;
+    return 2 * (gb + (DV ? nb * (K + 2) * 32 * 8 : 0) + K * 16 * (int)sizeof(T)) + 128;
   };
   const int bs = c->tune_bs[DV ? 1 : 0];
   int *err = &c->st->err;
@@ -394,6 +390,61 @@ static void xline_t_launch(otbl_ctx *c, const DCoefT<T> &dc, const XStream &a, c
     cudaFuncSetAttribute(k_xline_t<T, DV, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem(128));
     k_xline_t<T, DV, 128><<<dim3((npmax + 127) / 128, 3), 128, smem(128), c->stream>>>(dc, a, err, m);
   }
+}
+
+// One row of 16 T per plane i of each table (dv, which), dv 0 interpxx and
+// 1 difvisxx, which 0 u-type and 1 v-type coefficients: the right-hand-side
+// weights econ[2i], econ[2i+1] and the LU coefficients icon[3i..3i+2], then
+// for difvisxx the viscous operator's econv[3i..3i+2] and iconv[3i..3i+2].
+// k_xline_t's ring stages a segment's rows with its line boxes. Entries a
+// plane does not use are 0.
+template <typename T>
+__global__ void __launch_bounds__(128) k_x_rows(DCoefT<T> c, T *tab) {
+  const int nx = c.nx;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= 4 * nx) return;
+  const int dv = e / (2 * nx), which = (e / nx) & 1, i = e % nx;
+  T *q = tab + (size_t)e * 16;
+  for (int k = 0; k < 16; ++k) q[k] = T(0);
+  const T *icon = dv ? (which == 0 ? c.dcxu : c.dcxv) : (which == 0 ? c.inxu : c.inxv);
+  const T *econ = dv ? (which == 0 ? c.cofcxu : c.cofcxv) : (which == 0 ? c.cofiux : c.cofivx);
+  const bool inner = i > 0 && i < nx - 1;
+  if (inner) {
+    q[0] = econ[2 * i];
+    q[1] = econ[2 * i + 1];
+  }
+  for (int k = 0; k < 3; ++k) q[2 + k] = icon[3 * i + k];
+  if (dv) {
+    const T *iconv = which == 0 ? c.vixu : c.vixv, *econv = which == 0 ? c.cofvxu : c.cofvxv;
+    for (int k = 0; k < 3; ++k) {
+      if (inner) q[5 + k] = econv[3 * i + k];
+      q[8 + k] = iconv[3 * i + k];
+    }
+  }
+}
+
+cudaError_t launch_x_rows(otbl_ctx *c) {
+  const int n = 4 * c->cfg.nx;
+  if (c->mixed)
+    k_x_rows<float><<<(n + 127) / 128, 128, 0, c->stream>>>(c->dcf, static_cast<float *>(c->w.xrowc));
+  else
+    k_x_rows<double><<<(n + 127) / 128, 128, 0, c->stream>>>(c->dc, static_cast<double *>(c->w.xrowc));
+  c->launches += 1;
+  return cudaGetLastError();
+}
+
+// 2D map of one table of Work::xrowc: [nx planes][16 T], boxes of K planes
+static bool encode_xrows(CUtensorMap *m, const void *base, size_t esz, int nx, int k) {
+  auto fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(tensor_map_encoder());
+  if (!fn || ((uintptr_t)base) % 16 != 0) return false;
+  const cuuint64_t dims[2] = {16, (cuuint64_t)nx};
+  const cuuint64_t strides[1] = {16 * esz};
+  const cuuint32_t box[2] = {16, (cuuint32_t)k};
+  const cuuint32_t es[2] = {1, 1};
+  const CUtensorMapDataType dt = esz == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  return fn(m, dt, 2, const_cast<void *>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 // ---- TMA descriptors (host): field [nx][np], boxes of 32 lines x rows
@@ -419,11 +470,16 @@ bool build_x_maps(otbl_ctx *c) {
   const void *pr[3] = {c->w.uu, c->w.uv, c->w.uw};
   const size_t ew = c->mixed ? sizeof(float) : sizeof(double);
   bool ok = true;
+  const int which[3] = {0, 1, 1};  // u-type or v-type operator of each field
+  const char *tab = static_cast<const char *>(c->w.xrowc);
+  auto table = [&](int dv, int wh) { return tab + (size_t)(2 * dv + wh) * nx * 16 * ew; };
   for (int f = 0; f < 3 && ok; ++f) {
     ok = ok && encode_lines(&c->xmi.g[f], st[f], 8, nx, np[f], KI + 1);
     c->xmi.u[f] = c->xmi.g[f];  // unused by interpxx
+    ok = ok && encode_xrows(&c->xmi.r[f], table(0, which[f]), ew, nx, KI);
     ok = ok && encode_lines(&c->xmd.g[f], pr[f], ew, nx, np[f], KD + 1);
     ok = ok && encode_lines(&c->xmd.u[f], st[f], 8, nx, np[f], KD + 2);
+    ok = ok && encode_xrows(&c->xmd.r[f], table(1, which[f]), ew, nx, KD);
   }
   c->xmaps_ok = ok;
   return ok;

@@ -244,6 +244,11 @@ extern "C" int otbl_ctx_create(const otbl_config *cfg, const double *coef, int d
   TRY(dalloc(c, &w.fac_u, 3 * (size_t)(ny + 4)));
   TRY(dalloc(c, &w.fac_v, 3 * (size_t)(ny + 4)));
   TRY(dalloc(c, &w.rowc, 2 * 16 * (size_t)(ny + 2)));
+  {
+    double *q = nullptr;
+    TRY(dalloc(c, &q, 4 * 16 * (size_t)nx));
+    w.xrowc = q;
+  }
   TRY(dalloc(c, &w.gf, genflu_tab_doubles(ny)));
   TRY(dalloc(c, &w.pois_dinv, (size_t)nx * ny * (nz1 / 2)));
 #undef TRY
@@ -252,7 +257,8 @@ extern "C" int otbl_ctx_create(const otbl_config *cfg, const double *coef, int d
     build_x_maps(c);
     build_y_maps(c);
   }
-  if (check(c, launch_twiddles(c), "twiddles") != OTBL_OK || check(c, launch_pois_lu(c), "pois_lu") != OTBL_OK || check(c, cudaStreamSynchronize(c->stream), "init")) {
+  if (check(c, launch_twiddles(c), "twiddles") != OTBL_OK || check(c, launch_pois_lu(c), "pois_lu") != OTBL_OK ||
+      check(c, launch_x_rows(c), "x rows") != OTBL_OK || check(c, cudaStreamSynchronize(c->stream), "init")) {
     *out = c;
     return OTBL_ERR_CUDA;
   }
@@ -302,6 +308,7 @@ extern "C" int otbl_ctx_rebind(otbl_ctx *c, const otbl_config *cfg, const double
     c->dcf = make_dcoef<float>(c->coef_dev_f, o, *cfg);
   }
   if (check(c, launch_pois_lu(c), "pois_lu") != OTBL_OK) return OTBL_ERR_CUDA;
+  if (check(c, launch_x_rows(c), "x rows") != OTBL_OK) return OTBL_ERR_CUDA;
   OTBL_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   return OTBL_OK;
 }

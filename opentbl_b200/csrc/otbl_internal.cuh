@@ -64,6 +64,7 @@ struct Work {
   unsigned long long *vm_bits; // vm(j) maxima, j = 1..ny
   double *fac_u, *fac_v;       // implzy LU factors for the current dt (3*(ny+1))
   double *rowc;                // k_final_tb's per-row coefficients, [2][ny+2][16]
+  void *xrowc;                 // k_xline_t's per-plane coefficients, [2][2][nx][16] (T)
   double *gf;                  // genflu tables (genflu_tab_doubles)
   double *pois_dinv;           // pivots of the (x-mode, kz) y-systems, [i][j][k]
 };
@@ -82,9 +83,10 @@ struct YMaps {
 };
 
 // TMA descriptors of the x-line kernels' inputs, per field (u, v, w): 2D
-// tensors [plane][line] with boxes of 32 lines
+// tensors [plane][line] with boxes of 32 lines, and the per-plane
+// coefficient rows of the field's operator (Work::xrowc)
 struct XMaps {
-  CUtensorMap g[3], u[3];
+  CUtensorMap g[3], u[3], r[3];
 };
 
 }  // namespace otbl
@@ -189,6 +191,8 @@ cudaError_t launch_tail_rows(otbl_ctx *c);
 // the driver's cuTensorMapEncodeTiled (as void *), nullptr if unavailable
 void *tensor_map_encoder();
 bool build_x_maps(otbl_ctx *c);
+// fills Work::xrowc from the coefficients (at creation and on new coefficients)
+cudaError_t launch_x_rows(otbl_ctx *c);
 bool build_y_maps(otbl_ctx *c);
 cudaError_t launch_twiddles(otbl_ctx *c);
 cudaError_t launch_pois_lu(otbl_ctx *c);
