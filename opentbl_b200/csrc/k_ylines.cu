@@ -47,12 +47,14 @@ struct FinalTune;
 #ifndef OTBL_FT_NS
 #define OTBL_FT_NS 2
 #endif
-// tma_a: pass A fed by TMA too (k_final_ta; FP32 inputs 5.25 against 5.33
-// ms; FP64 6.50 against 5.94, so FP64 keeps the register-streamed pass A)
+// tma_a: pass A fed by TMA too (k_final_ta). With the per-row coefficients
+// staged in its ring: FP64 4.00 against 4.76 ms per substep for the
+// register-streamed pass A (before the staging, 6.50 against 5.94); FP32
+// inputs 2.97 ms.
 template <>
 struct FinalTune<double> {
   static constexpr int kf = OTBL_FT_DK, minb = OTBL_FT_DM, kf_tma = OTBL_FT_TK, ns_tma = OTBL_FT_NS;
-  static constexpr bool split = false, tma_a = false;
+  static constexpr bool split = false, tma_a = true;
 };
 template <>
 struct FinalTune<float> {
@@ -158,7 +160,8 @@ template <typename T>
 __global__ void __launch_bounds__(128) k_interpy_t(DCoefT<T> c, InterpyArgs a, int *err,
                                                    const __grid_constant__ YMaps maps) {
   constexpr int K = YTune<T>::kt, TB = 128, R = K + 2;
-  constexpr int STG = R * TB * 8;
+  constexpr int RC = K * 8 * (int)sizeof(T);  // the segment's coefficient rows
+  constexpr int STG = R * TB * 8 + RC;
   constexpr unsigned TX = (unsigned)STG;
   extern __shared__ __align__(128) unsigned char smraw[];
   uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + 2 * STG);
@@ -169,11 +172,13 @@ __global__ void __launch_bounds__(128) k_interpy_t(DCoefT<T> c, InterpyArgs a, i
   const int krc = active ? kr : 0;
   const int which = pick3(a.which, f), jin = which == 0 ? ny + 1 : ny;
   const CUtensorMap *mg = f == 0 ? &maps.g[0] : (f == 1 ? &maps.g[1] : &maps.g[2]);
+  const CUtensorMap *mr = f == 0 ? &maps.r[0] : (f == 1 ? &maps.r[1] : &maps.r[2]);
   const int nseg = (ny + K - 1) / K;
   auto seg_of = [&](int it) { return it < nseg ? it : 2 * nseg - 1 - it; };
   auto issue = [&](int stg, int sg) {
     mbar_arrive_expect_tx(&bar[stg], TX);
     tma_load_3d(smraw + stg * STG, mg, kr0, sg * K - 1, i - 1, &bar[stg]);
+    tma_load_2d(smraw + stg * STG + R * TB * 8, mr, 0, sg * K, &bar[stg]);
   };
   if (t == 0) {
     mbar_init(&bar[0], 1);
@@ -187,8 +192,6 @@ __global__ void __launch_bounds__(128) k_interpy_t(DCoefT<T> c, InterpyArgs a, i
   const double *g = pick3(a.in, f) + (size_t)(i - 1) * jin * nz1 + krc;
   T *o = static_cast<T *>(pick3(a.out, f)) + (size_t)(i - 1) * ny * nz1 + krc;
   T *ck = reinterpret_cast<T *>(pick3(a.ck, f)) + col;
-  const T *iny = which == 0 ? c.inyu : c.inyv;
-  const T *econ = which == 0 ? c.cofiuy : c.cofivy;
   const T *ib = c.inby;
   auto G = [&](int r) { return (T)__ldg(g + (size_t)min(max(r, 0), jin - 1) * S); };
   T b0 = T(0), bN;
@@ -198,8 +201,9 @@ __global__ void __launch_bounds__(128) k_interpy_t(DCoefT<T> c, InterpyArgs a, i
     b0 = M4(ib, 3, 1) * G(0) + M4(ib, 3, 2) * G(1) + M4(ib, 3, 3) * G(2) + M4(ib, 3, 4) * G(3);
     bN = M4(ib, 4, 1) * G(ny - 1) + M4(ib, 4, 2) * G(ny - 2) + M4(ib, 4, 3) * G(ny - 3) + M4(ib, 4, 4) * G(ny - 4);
   }
-  auto rhs = [&](int r, T gm, T g0, T gp) {
-    const T e1 = __ldg(econ + 2 * r), e2 = __ldg(econ + 2 * r + 1);
+  // q: the row's coefficients in shared memory (k_y_rows' layout)
+  auto rhs = [&](int r, const T *q, T gm, T g0, T gp) {
+    const T e1 = q[0], e2 = q[1];
     const T in = which == 0 ? e1 * g0 + e2 * gp : e2 * g0 + e1 * gm;
     return r == 0 ? b0 : (r == ny - 1 ? bN : in);
   };
@@ -215,27 +219,31 @@ __global__ void __launch_bounds__(128) k_interpy_t(DCoefT<T> c, InterpyArgs a, i
     if (!active) continue;
     const int sg = seg_of(it), s0 = sg * K;
     const double *gs = reinterpret_cast<const double *>(smraw + stg * STG) + t;
+    const T *rcs = reinterpret_cast<const T *>(smraw + stg * STG + R * TB * 8);
     auto gv = [&](int b) { return (T)gs[b * TB]; };  // row s0 - 1 + b
     if (it < nseg) {
       ck[(size_t)sg * ncol] = y;
 #pragma unroll
       for (int b = 0; b < K; ++b) {
         const int r = s0 + b;
-        if (r < ny) y = rhs(r, gv(b), gv(b + 1), gv(b + 2)) + (r > 0 ? __ldg(iny + 3 * r) : T(0)) * y;
+        const T *q = rcs + 8 * b;
+        if (r < ny) y = rhs(r, q, gv(b), gv(b + 1), gv(b + 2)) + (r > 0 ? q[2] : T(0)) * y;
       }
     } else {
       T yy = ck[(size_t)sg * ncol], yv[K];
 #pragma unroll
       for (int b = 0; b < K; ++b) {
         const int r = s0 + b;
-        if (r < ny) yy = rhs(r, gv(b), gv(b + 1), gv(b + 2)) + (r > 0 ? __ldg(iny + 3 * r) : T(0)) * yy;
+        const T *q = rcs + 8 * b;
+        if (r < ny) yy = rhs(r, q, gv(b), gv(b + 1), gv(b + 2)) + (r > 0 ? q[2] : T(0)) * yy;
         yv[b] = yy;
       }
 #pragma unroll
       for (int b = K - 1; b >= 0; --b) {
         const int r = s0 + b;
+        const T *q = rcs + 8 * b;
         if (r < ny) {
-          x = (yv[b] - __ldg(iny + 3 * r + 2) * x) * __ldg(iny + 3 * r + 1);
+          x = (yv[b] - q[4] * x) * q[3];
           o[(size_t)r * S] = x;
         }
       }
@@ -799,8 +807,8 @@ __global__ void __launch_bounds__(128) k_final_ta(DCoef c, DCoefT<W> cw, FinalSt
                                                   const __grid_constant__ FinalMaps maps) {
   constexpr int KF = FinalTune<W>::kf_tma, KA = 8, TB = 128, R = KA + 2;
   constexpr int PB = (R * TB * (int)sizeof(W) + 127) / 128 * 128;
-  constexpr int STG = PB + R * TB * 8;
-  constexpr unsigned TX = (unsigned)(R * TB * sizeof(W) + R * TB * 8);
+  constexpr int STG = PB + R * TB * 8 + KA * 128;  // + the KA coefficient rows
+  constexpr unsigned TX = (unsigned)(R * TB * sizeof(W) + R * TB * 8 + KA * 128);
   extern __shared__ __align__(128) unsigned char smraw[];
   uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + 2 * STG);
   const FinalArgs<W> &a = fs.a;
@@ -819,6 +827,7 @@ __global__ void __launch_bounds__(128) k_final_ta(DCoef c, DCoefT<W> cw, FinalSt
     mbar_arrive_expect_tx(&bar[stg], TX);
     tma_load_3d(b, &maps.prod_a, kr0, sa * KA - 1, i - 1, &bar[stg]);
     tma_load_3d(b + PB, &maps.vel_a, kr0, sa * KA - 1, i - 1, &bar[stg]);
+    tma_load_2d(b + PB + R * TB * 8, &maps.rc_a, 0, sa * KA, &bar[stg]);
   };
   if (t == 0) {
     mbar_init(&bar[0], 1);
@@ -833,9 +842,8 @@ __global__ void __launch_bounds__(128) k_final_ta(DCoef c, DCoefT<W> cw, FinalSt
   const W *prod = (COMP == 0 ? a.uv : (COMP == 1 ? a.vv : a.vw)) + plv + krc;
   const double *vel = (COMP == 0 ? a.u : (COMP == 1 ? a.v : a.w)) + pl + krc;
   const int which = COMP == 1 ? 1 : 0;
-  // the sweeps run in W on the coefficient copy cw (FP32 on the mixed path)
-  const W *dcy = which == 0 ? cw.dcyu : cw.dcyv, *ecd = which == 0 ? cw.cofcyu : cw.cofcyv;
-  const W *viy = which == 0 ? cw.viyu : cw.viyv, *ecv = which == 0 ? cw.cofvyu : cw.cofvyv;
+  // the sweeps run in W on the coefficient copy cw (FP32 on the mixed path);
+  // the per-row coefficients come staged with the boxes (k_tail_rows' rows)
   auto Pg = [&](int r) { return (W)__ldg(prod + (size_t)min(max(r, 0), ny - 1) * S); };
   auto Vg = [&](int r) { return (W)__ldg(vel + (size_t)min(max(r, 0), jee - 1) * S); };
   const int chv = which == 0 ? 3 : 1, cha = chv + 1, ic = which == 0 ? 3 : 1;
@@ -849,13 +857,12 @@ __global__ void __launch_bounds__(128) k_final_ta(DCoef c, DCoefT<W> cw, FinalSt
   const W b0 = M4(vb, ic, 1) * Vg(0) + M4(vb, ic, 2) * Vg(1) + M4(vb, ic, 3) * Vg(2) + M4(vb, ic, 4) * Vg(3);
   const W bN = M4(vb, ic + 1, 1) * Vg(jee - 1) + M4(vb, ic + 1, 2) * Vg(jee - 2) +
                M4(vb, ic + 1, 3) * Vg(jee - 3) + M4(vb, ic + 1, 4) * Vg(jee - 4);
-  auto rd = [&](int r, W gm, W g0, W gp) {
-    const W in = which == 0 ? __ldg(ecd + 2 * r + 1) * g0 + __ldg(ecd + 2 * r) * gm
-                            : __ldg(ecd + 2 * r + 1) * gp + __ldg(ecd + 2 * r) * g0;
+  auto rd = [&](int r, const W *q, W gm, W g0, W gp) {
+    const W in = which == 0 ? q[1] * g0 + q[0] * gm : q[1] * gp + q[0] * g0;
     return r == 0 ? bot : (r == jee - 1 ? top : in);
   };
-  auto rv = [&](int r, W um, W u0, W up) {
-    const W in = __ldg(ecv + 3 * r) * up + __ldg(ecv + 3 * r + 1) * u0 + __ldg(ecv + 3 * r + 2) * um;
+  auto rv = [&](int r, const W *q, W um, W u0, W up) {
+    const W in = q[5] * up + q[6] * u0 + q[7] * um;
     return r == 0 ? b0 : (r == jee - 1 ? bN : in);
   };
   W *ck = reinterpret_cast<W *>(fs.ck) + col;  // checkpoints in W, read back by k_final_tb
@@ -871,17 +878,19 @@ __global__ void __launch_bounds__(128) k_final_ta(DCoef c, DCoefT<W> cw, FinalSt
     if (!active) continue;
     const W *sp = reinterpret_cast<const W *>(smraw + stg * STG) + t;
     const double *sv = reinterpret_cast<const double *>(smraw + stg * STG + PB) + t;
+    const double *rcs = reinterpret_cast<const double *>(smraw + stg * STG + PB + R * TB * 8);
     const int s0 = sa * KA;
 #pragma unroll
     for (int b = 0; b < KA; ++b) {
       const int r = s0 + b;
+      const W *q = reinterpret_cast<const W *>(rcs + 16 * b + 5);
       if (r % KF == 0 && r < jee) {  // y of row r-1 at the start of segment r/KF
         ck[(size_t)(2 * (r / KF)) * ncol] = yd;
         ck[(size_t)(2 * (r / KF) + 1) * ncol] = yv;
       }
       if (r < jee) {
-        if (!last) yd = rd(r, sp[b * TB], sp[(b + 1) * TB], sp[(b + 2) * TB]) + (r > 0 ? __ldg(dcy + 3 * r) : W(0)) * yd;
-        yv = rv(r, (W)sv[b * TB], (W)sv[(b + 1) * TB], (W)sv[(b + 2) * TB]) + (r > 0 ? __ldg(viy + 3 * r) : W(0)) * yv;
+        if (!last) yd = rd(r, q, sp[b * TB], sp[(b + 1) * TB], sp[(b + 2) * TB]) + (r > 0 ? q[2] : W(0)) * yd;
+        yv = rv(r, q, (W)sv[b * TB], (W)sv[(b + 1) * TB], (W)sv[(b + 2) * TB]) + (r > 0 ? q[8] : W(0)) * yv;
       }
     }
   }
@@ -1011,11 +1020,11 @@ cudaError_t launch_interpy(otbl_ctx *c) {
   if (c->ymaps_ok) {
     const dim3 gt((c->dc.nz1 + 127) / 128, c->cfg.nx, 3);
     if (c->mixed) {
-      const int sm = 2 * (YTune<float>::kt + 2) * 128 * 8 + 128;
+      const int sm = 2 * ((YTune<float>::kt + 2) * 128 * 8 + YTune<float>::kt * 8 * 4) + 128;
       cudaFuncSetAttribute(k_interpy_t<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
       k_interpy_t<float><<<gt, 128, sm, c->stream>>>(c->dcf, a, &c->st->err, c->ymi);
     } else {
-      const int sm = 2 * (YTune<double>::kt + 2) * 128 * 8 + 128;
+      const int sm = 2 * ((YTune<double>::kt + 2) * 128 * 8 + YTune<double>::kt * 8 * 8) + 128;
       cudaFuncSetAttribute(k_interpy_t<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
       k_interpy_t<double><<<gt, 128, sm, c->stream>>>(c->dc, a, &c->st->err, c->ymi);
     }
@@ -1024,6 +1033,34 @@ cudaError_t launch_interpy(otbl_ctx *c) {
   else
     k_interpy<double><<<dim3((ncol + bs - 1) / bs, 3), bs, 0, c->stream>>>(c->dc, a);
   prof_end(c);
+  c->launches += 1;
+  return cudaGetLastError();
+}
+
+// One row of 8 T per y row r of each table (which 0: u-type input, u and w;
+// 1: v-type input, v): interpyy's right-hand-side weights econ[2r],
+// econ[2r+1] and LU coefficients iny[3r..3r+2]; the rest 0. k_interpy_t's
+// ring stages a segment's rows with its field box.
+template <typename T>
+__global__ void __launch_bounds__(128) k_y_rows(DCoefT<T> c, T *tab) {
+  const int ny = c.ny;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= 2 * ny) return;
+  const int which = e / ny, r = e - which * ny;
+  const T *iny = which == 0 ? c.inyu : c.inyv, *econ = which == 0 ? c.cofiuy : c.cofivy;
+  T *q = tab + (size_t)e * 8;
+  q[0] = econ[2 * r];
+  q[1] = econ[2 * r + 1];
+  for (int k = 0; k < 3; ++k) q[2 + k] = iny[3 * r + k];
+  for (int k = 5; k < 8; ++k) q[k] = T(0);
+}
+
+cudaError_t launch_y_rows(otbl_ctx *c) {
+  const int n = 2 * c->cfg.ny;
+  if (c->mixed)
+    k_y_rows<float><<<(n + 127) / 128, 128, 0, c->stream>>>(c->dcf, static_cast<float *>(c->w.yrowc));
+  else
+    k_y_rows<double><<<(n + 127) / 128, 128, 0, c->stream>>>(c->dc, static_cast<double *>(c->w.yrowc));
   c->launches += 1;
   return cudaGetLastError();
 }
@@ -1061,6 +1098,21 @@ static bool encode_field(CUtensorMap *m, const void *base, size_t esz, int plane
 
 static bool encode_rows(CUtensorMap *m, const double *base, int rows, int brows);
 
+// 2D map of a coefficient table [rows][width elements of esz bytes], boxes
+// of brows full rows
+static bool encode_table(CUtensorMap *m, const void *base, size_t esz, int width, int rows, int brows) {
+  auto fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(tensor_map_encoder());
+  if (!fn || ((uintptr_t)base) % 16 != 0 || (width * esz) % 16 != 0) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)width, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {width * esz};
+  const cuuint32_t box[2] = {(cuuint32_t)width, (cuuint32_t)brows};
+  const cuuint32_t es[2] = {1, 1};
+  const CUtensorMapDataType dt = esz == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  return fn(m, dt, 2, const_cast<void *>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <typename W>
 static bool build_maps_t(otbl_ctx *c) {
   constexpr int KF = FinalTune<W>::kf_tma;
@@ -1085,6 +1137,7 @@ static bool build_maps_t(otbl_ctx *c) {
     ok = ok && encode_field(&m.hp, hp, ew, nx, jee, nz1, KF, 1);
     ok = ok && encode_field(&m.p, c->f[OTBL_F_P], ew, nx, ny, nz1, comp == 1 ? KF + 1 : KF, comp == 0 ? 2 : 1);
     ok = ok && encode_rows(&m.rc, c->w.rowc + (comp == 1 ? (size_t)16 * (ny + 2) : 0), ny + 2, KF);
+    ok = ok && encode_rows(&m.rc_a, c->w.rowc + (comp == 1 ? (size_t)16 * (ny + 2) : 0), ny + 2, 8);
   }
   return ok;
 }
@@ -1095,7 +1148,13 @@ bool build_y_maps(otbl_ctx *c) {
   const double *in[3] = {c->f[OTBL_F_U], c->f[OTBL_F_W], c->f[OTBL_F_V]};
   const int rows[3] = {ny + 1, ny + 1, ny};
   bool ok = true;
-  for (int f = 0; f < 3 && ok; ++f) ok = encode_field(&c->ymi.g[f], in[f], 8, nx, rows[f], nz1, K + 2, 1);
+  const size_t ew = c->mixed ? sizeof(float) : sizeof(double);
+  const int which[3] = {0, 0, 1};
+  for (int f = 0; f < 3 && ok; ++f) {
+    ok = encode_field(&c->ymi.g[f], in[f], 8, nx, rows[f], nz1, K + 2, 1);
+    const char *tab = static_cast<const char *>(c->w.yrowc) + (size_t)which[f] * ny * 8 * ew;
+    ok = ok && encode_table(&c->ymi.r[f], tab, ew, 8, ny, K);
+  }
   c->ymaps_ok = ok;
   return ok;
 }
@@ -1208,7 +1267,7 @@ static int final_t(otbl_ctx *c, unsigned comps, cudaEvent_t before_vel) {
     if (tma) {
       // pass A (register-streamed or TMA-fed), then the TMA-fed pass B
       if constexpr (FinalTune<W>::tma_a) {
-        constexpr int sma = 2 * ((10 * 128 * (int)sizeof(W) + 127) / 128 * 128 + 10 * 128 * 8) + 128;
+        constexpr int sma = 2 * ((10 * 128 * (int)sizeof(W) + 127) / 128 * 128 + 10 * 128 * 8 + 8 * 128) + 128;
         cudaFuncSetAttribute(k_final_ta<K, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, sma);
         k_final_ta<K, W><<<gt, 128, sma, c->stream>>>(c->dc, cw, fs, &c->st->err, c->fmaps[K]);
       } else {

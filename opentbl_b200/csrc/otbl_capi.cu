@@ -248,6 +248,8 @@ extern "C" int otbl_ctx_create(const otbl_config *cfg, const double *coef, int d
     double *q = nullptr;
     TRY(dalloc(c, &q, 4 * 16 * (size_t)nx));
     w.xrowc = q;
+    TRY(dalloc(c, &q, 2 * 8 * (size_t)ny));
+    w.yrowc = q;
   }
   TRY(dalloc(c, &w.gf, genflu_tab_doubles(ny)));
   TRY(dalloc(c, &w.pois_dinv, (size_t)nx * ny * (nz1 / 2)));
@@ -258,7 +260,8 @@ extern "C" int otbl_ctx_create(const otbl_config *cfg, const double *coef, int d
     build_y_maps(c);
   }
   if (check(c, launch_twiddles(c), "twiddles") != OTBL_OK || check(c, launch_pois_lu(c), "pois_lu") != OTBL_OK ||
-      check(c, launch_x_rows(c), "x rows") != OTBL_OK || check(c, cudaStreamSynchronize(c->stream), "init")) {
+      check(c, launch_x_rows(c), "x rows") != OTBL_OK || check(c, launch_y_rows(c), "y rows") != OTBL_OK ||
+      check(c, cudaStreamSynchronize(c->stream), "init")) {
     *out = c;
     return OTBL_ERR_CUDA;
   }
@@ -309,6 +312,7 @@ extern "C" int otbl_ctx_rebind(otbl_ctx *c, const otbl_config *cfg, const double
   }
   if (check(c, launch_pois_lu(c), "pois_lu") != OTBL_OK) return OTBL_ERR_CUDA;
   if (check(c, launch_x_rows(c), "x rows") != OTBL_OK) return OTBL_ERR_CUDA;
+  if (check(c, launch_y_rows(c), "y rows") != OTBL_OK) return OTBL_ERR_CUDA;
   OTBL_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   return OTBL_OK;
 }

@@ -65,6 +65,7 @@ struct Work {
   double *fac_u, *fac_v;       // implzy LU factors for the current dt (3*(ny+1))
   double *rowc;                // k_final_tb's per-row coefficients, [2][ny+2][16]
   void *xrowc;                 // k_xline_t's per-plane coefficients, [2][2][nx][16] (T)
+  void *yrowc;                 // k_interpy_t's per-row coefficients, [2][ny][8] (T)
   double *gf;                  // genflu tables (genflu_tab_doubles)
   double *pois_dinv;           // pivots of the (x-mode, kz) y-systems, [i][j][k]
 };
@@ -74,12 +75,13 @@ struct Work {
 struct FinalMaps {
   CUtensorMap prod, kp, vel, cx, hp, p;
   CUtensorMap prod_a, vel_a;  // pass A: boxes of 8 + 2 rows
-  CUtensorMap rc;             // per-row coefficients (Work::rowc)
+  CUtensorMap rc, rc_a;       // per-row coefficients (Work::rowc), KF / 8 rows
 };
 
-// TMA descriptors of interpyy's inputs (u, w, v), boxes of 128 kr x rows
+// TMA descriptors of interpyy's inputs (u, w, v), boxes of 128 kr x rows,
+// and the per-row coefficient rows of each field's operator (Work::yrowc)
 struct YMaps {
-  CUtensorMap g[3];
+  CUtensorMap g[3], r[3];
 };
 
 // TMA descriptors of the x-line kernels' inputs, per field (u, v, w): 2D
@@ -191,8 +193,10 @@ cudaError_t launch_tail_rows(otbl_ctx *c);
 // the driver's cuTensorMapEncodeTiled (as void *), nullptr if unavailable
 void *tensor_map_encoder();
 bool build_x_maps(otbl_ctx *c);
-// fills Work::xrowc from the coefficients (at creation and on new coefficients)
+// fill Work::xrowc and Work::yrowc from the coefficients (at creation and on
+// new coefficients)
 cudaError_t launch_x_rows(otbl_ctx *c);
+cudaError_t launch_y_rows(otbl_ctx *c);
 bool build_y_maps(otbl_ctx *c);
 cudaError_t launch_twiddles(otbl_ctx *c);
 cudaError_t launch_pois_lu(otbl_ctx *c);
