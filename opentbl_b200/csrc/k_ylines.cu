@@ -1227,7 +1227,7 @@ bool build_final_maps(otbl_ctx *c) {
 }
 
 template <typename W>
-static int final_t(otbl_ctx *c, unsigned comps, cudaEvent_t before_vel) {
+static int final_t(otbl_ctx *c, unsigned comps, cudaEvent_t before_vel, bool second_scratch) {
   FinalStream<W> fs;
   FinalArgs<W> &a = fs.a;
   a.u = c->f[OTBL_F_U];
@@ -1249,9 +1249,9 @@ static int final_t(otbl_ctx *c, unsigned comps, cudaEvent_t before_vel) {
   a.fac_v = c->w.fac_v;
   a.st = c->st;
   const int ncol = (c->cfg.nx - 1) * c->dc.nz1;
-  fs.ck = c->w.s1;
-  fs.yq = c->w.s2;
-  fs.ub = c->w.s3;
+  fs.ck = second_scratch ? c->w.t1 : c->w.s1;
+  fs.yq = second_scratch ? c->w.t2 : c->w.s2;
+  fs.ub = second_scratch ? c->w.t3 : c->w.s3;
   const dim3 g((ncol + 127) / 128);
   double *U = c->f[OTBL_F_U], *V = c->f[OTBL_F_V], *Wv = c->f[OTBL_F_W];
   const bool tma = c->fmaps_ok;
@@ -1294,9 +1294,10 @@ static int final_t(otbl_ctx *c, unsigned comps, cudaEvent_t before_vel) {
   return n * ((tma || FinalTune<W>::split) ? 3 : 2);
 }
 
-cudaError_t launch_final(otbl_ctx *c, unsigned comps, cudaEvent_t before_vel) {
+cudaError_t launch_final(otbl_ctx *c, unsigned comps, cudaEvent_t before_vel, bool second_scratch) {
   prof_begin(c, PK_FINAL);
-  const int nl = c->mixed ? final_t<float>(c, comps, before_vel) : final_t<double>(c, comps, before_vel);
+  const int nl = c->mixed ? final_t<float>(c, comps, before_vel, second_scratch)
+                          : final_t<double>(c, comps, before_vel, second_scratch);
   prof_end(c);
   c->launches += nl;
   return cudaGetLastError();

@@ -231,6 +231,9 @@ extern "C" int otbl_ctx_create(const otbl_config *cfg, const double *coef, int d
   TRY(dalloc(c, &w.s1, std::max(lu, (size_t)(ny + 2) * (nx - 1) * nz1)));
   TRY(dalloc(c, &w.s2, lu));
   TRY(dalloc(c, &w.s3, lu));
+  TRY(dalloc(c, &w.t1, std::max(lu, (size_t)(ny + 2) * (nx - 1) * nz1)));
+  TRY(dalloc(c, &w.t2, lu));
+  TRY(dalloc(c, &w.t3, lu));
   const int M = nz / 2, n = nx - 1;
   TRY(dalloc(c, &w.twz, 2 * (size_t)M));
   TRY(dalloc(c, &w.twz2, 2 * (size_t)M));
@@ -280,10 +283,11 @@ extern "C" size_t otbl_ctx_bytes(const otbl_config *cfg) {
   b += (2 * lu + lv) * sizeof(double) + (2 * lu + 2 * lv) * (mixed ? sizeof(float) : sizeof(double));  // state
   b += 3 * (size_t)(ny + 1) * sizeof(double) + sizeof(DState);   // u0, v0, um, scalars
   b += 15 * lu * (mixed ? sizeof(float) : sizeof(double));       // intermediates
-  b += (std::max(lu, (size_t)(ny + 2) * (nx - 1) * nz1) + 2 * lu) * sizeof(double);  // scratch
+  b += 2 * (std::max(lu, (size_t)(ny + 2) * (nx - 1) * nz1) + 2 * lu) * sizeof(double);  // s1..s3, t1..t3
   b += (4 * (size_t)M + 4 * (size_t)n) * sizeof(double) + (mixed ? 4 * (size_t)M * sizeof(float) : 0);
   b += (size_t)(ny + 1) * 8 + 6 * (size_t)(ny + 4) * sizeof(double) + genflu_tab_doubles(ny) * sizeof(double);
   b += (size_t)nx * ny * (nz1 / 2) * sizeof(double);             // Poisson pivots
+  b += (2 * 16 * (size_t)(ny + 2) + 4 * 16 * (size_t)nx + 2 * 8 * (size_t)ny) * sizeof(double);  // coefficient rows
   return b;
 }
 
@@ -526,8 +530,17 @@ static int rhsp_issue(otbl_ctx *c, int m, int setstep) {
   OTBL_CUDA_TRY(c, cudaEventRecord(c->ev[3], c->side));
   OTBL_CUDA_TRY(c, cudaStreamWaitEvent(main_s, c->ev[1], 0));
   LAUNCH(c, launch_final(c, 1, c->ev[3]));
+  // the v tail here and the w tail on side (its own line scratch t1..t3),
+  // both after part 1; side already follows genflu
+  OTBL_CUDA_TRY(c, cudaStreamWaitEvent(c->side, c->ev[4], 0));
+  c->stream = c->side;
+  e = launch_final(c, 4, nullptr, true);
+  if (e == cudaSuccess) e = cudaEventRecord(c->ev[5], c->side);
+  c->stream = main_s;
+  if (check(c, e, "w tail") != OTBL_OK) return OTBL_ERR_CUDA;
   OTBL_CUDA_TRY(c, cudaStreamWaitEvent(main_s, c->ev[4], 0));
-  LAUNCH(c, launch_final(c, 2 | 4));
+  LAUNCH(c, launch_final(c, 2));
+  OTBL_CUDA_TRY(c, cudaStreamWaitEvent(main_s, c->ev[5], 0));
   return OTBL_OK;
 }
 

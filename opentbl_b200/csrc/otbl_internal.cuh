@@ -57,6 +57,7 @@ struct Work {
   void *uu, *uw, *uv, *vw, *vv, *ww;  // products (uu, uw u-type; others ny rows)
   void *cu, *cv, *cw;          // difvisxx outputs
   double *s1, *s2, *s3;        // line-solve scratch and pois' phi (u-type size)
+  double *t1, *t2, *t3;        // the w tail's scratch (beside the v tail), as s1..s3
   double *twz, *twz2;          // z-FFT twiddles exp(-2 pi i t/M), exp(-2 pi i t/nz)
   float *twzf, *twz2f;         // the same rounded to FP32 (mixed path)
   double *twx;                 // x-DCT twiddles for the length nx-1 FFT
@@ -103,7 +104,7 @@ struct otbl_ctx {
   // priority, runs the second half of the products beside difvisxx and the
   // u tail, taking the SM slots those leave free
   cudaStream_t side = nullptr, side_lo = nullptr;
-  cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   otbl::DCoef dc;
   otbl::DCoefT<float> dcf;  // FP32 coefficients (mixed path)
   // threads per CTA of the line kernels that otbl_autotune times:
@@ -175,9 +176,11 @@ cudaError_t launch_difvisx(otbl_ctx *c);
 cudaError_t launch_dt(otbl_ctx *c, int m, int setstep);
 cudaError_t launch_genflu(otbl_ctx *c, int tail);
 // the rhsp tail of the velocity components in the bit mask comps (1 u, 2 v,
-// 4 w), in that order; the first kernel that writes a velocity component
-// waits for before_vel when it is not null
-cudaError_t launch_final(otbl_ctx *c, unsigned comps, cudaEvent_t before_vel = nullptr);
+// 4 w), in that order, on line scratch s1..s3 (second_scratch: t1..t3); the
+// first kernel that writes a velocity component waits for before_vel when
+// it is not null
+cudaError_t launch_final(otbl_ctx *c, unsigned comps, cudaEvent_t before_vel = nullptr,
+                         bool second_scratch = false);
 cudaError_t launch_outflow(otbl_ctx *c);
 cudaError_t launch_pois(otbl_ctx *c, int m);
 cudaError_t launch_reset_max(otbl_ctx *c);

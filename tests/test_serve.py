@@ -40,9 +40,10 @@ def test_ctx_bytes_grows_with_the_box_and_mixed_is_smaller():
     m = native.make_config(replace(config.C2, precision=1), 1000.0, 100)
     assert 0 < L.otbl_ctx_bytes(a) < L.otbl_ctx_bytes(b)
     assert L.otbl_ctx_bytes(m) < L.otbl_ctx_bytes(b)
-    # 1025x193x512 FP64: 7 state + 15 intermediates + 3 scratch fields
+    # 1025x193x512 FP64: 7 state + 15 intermediates + 6 scratch fields (the
+    # w tail runs beside the v tail on a scratch set of its own)
     nf = 1025 * 194 * 340 * 8
-    assert 25 * nf <= L.otbl_ctx_bytes(b) <= 26.5 * nf
+    assert 28 * nf <= L.otbl_ctx_bytes(b) <= 29.5 * nf
 
 
 class _FakeBox:
@@ -67,6 +68,20 @@ def test_admission_evicts_idle_slots_of_other_sizes():
     assert srv._evict_one() and srv.used == 0
     assert not srv._evict_one()
     assert all(b.box.closed for b in boxes)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [0, 1])
+def test_ctx_bytes_is_what_a_context_allocates(precision):
+    """The admission estimate is exact: otbl_ctx_bytes equals the device
+    bytes a context of that configuration holds."""
+    cfg = replace(config.TINY, precision=precision)
+    init = synth.make_initial(cfg)
+    coef = native.coef_compute(cfg, init["re"], init["xout"], init["y"], init["u0"])
+    b = Box(cfg, init, coef)
+    cc = native.make_config(cfg, init["re"], init["xout"])
+    assert b.device_bytes == native.lib().otbl_ctx_bytes(cc)
+    b.close()
 
 
 @pytest.mark.gpu
