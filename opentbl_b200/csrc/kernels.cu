@@ -135,11 +135,17 @@ struct ProdArgs {
   int setstep;
 };
 
-// rhsp.F90:120-171 (PART 0: uu, uw, uv and the CFL maxima, all planes) and
-// rhsp.F90:367-415 (PART 1: vw, vv, ww, planes 2..nx-1 and rows 1..ny); one
-// warp per (i, j) line. The two parts read disjoint inputs and write
-// disjoint products, so the second can run beside difvisxx, which reads
-// only the first's.
+// rhsp.F90:120-171 and 367-415, one warp per (i, j) line, in three parts
+// with disjoint inputs and outputs: PART 0 uu, uw and the u, w CFL maxima
+// (all planes, rows 1..ny+1; interpxx's outputs only, so it runs beside
+// interpyy), PART 2 uv and the v maxima (all planes, rows 1..ny), PART 1
+// vw, vv, ww (planes 2..nx-1, rows 1..ny; interpyy's outputs only, so it
+// runs beside difvisxx, which reads parts 0 and 2).
+template <int PART>
+struct ProdPart {
+  static constexpr int i0 = PART == 1 ? 2 : 1;      // first plane
+  static constexpr int extra = PART == 0 ? 1 : 0;   // rows ny + extra
+};
 template <typename T, int PART>
 __global__ void __launch_bounds__(128) k_products(DCoef c, ZTabT<T> z, ProdArgs<T> a) {
   using V = V2<T>;
@@ -147,9 +153,9 @@ __global__ void __launch_bounds__(128) k_products(DCoef c, ZTabT<T> z, ProdArgs<
   V *sm = reinterpret_cast<V *>(smraw);
   const int M = z.M, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int j = blockIdx.x * 4 + wid + 1;
-  const int i = blockIdx.y + 1 + PART;
+  const int i = blockIdx.y + ProdPart<PART>::i0;
   const int ny = c.ny, nz1 = c.nz1;
-  if (j > ny + 1 - PART) return;
+  if (j > ny + ProdPart<PART>::extra) return;
   V *A = sm + (size_t)wid * 3 * M, *B = A + M, *P = B + M;
   const size_t offu = ((size_t)(i - 1) * (ny + 1) + (j - 1)) * nz1;
   const size_t offv = ((size_t)(i - 1) * ny + (j - 1)) * nz1;
@@ -166,7 +172,20 @@ __global__ void __launch_bounds__(128) k_products(DCoef c, ZTabT<T> z, ProdArgs<
     line_r2c(z, A, a.ww + offv, lane);
     return;
   }
-  double mu = 0.0, mw = 0.0, mv = 0.0;
+  if (PART == 2) {
+    double mv = 0.0;
+    line_c2r(z, a.vx + offv, A, lane);
+    if (a.setstep) mv = buf_absmax(A, M, lane);
+    line_c2r(z, a.uy + offv, B, lane);
+    buf_mul(A, B, M, lane);
+    line_r2c(z, A, a.uv + offv, lane);
+    if (a.setstep) {
+      mv = warp_nmax(mv);
+      if (lane == 0) atomicMax(&a.vm_bits[j], (unsigned long long)__double_as_longlong(mv));
+    }
+    return;
+  }
+  double mu = 0.0, mw = 0.0;
   line_c2r(z, a.u + offu, P, lane);
   if (a.setstep) mu = buf_absmax(P, M, lane);
   line_c2r(z, a.ux + offu, A, lane);
@@ -176,21 +195,12 @@ __global__ void __launch_bounds__(128) k_products(DCoef c, ZTabT<T> z, ProdArgs<
   if (a.setstep) mw = buf_absmax(A, M, lane);
   buf_mul(A, P, M, lane);
   line_r2c(z, A, a.uw + offu, lane);
-  if (j <= ny) {
-    line_c2r(z, a.vx + offv, A, lane);
-    if (a.setstep) mv = buf_absmax(A, M, lane);
-    line_c2r(z, a.uy + offv, B, lane);
-    buf_mul(A, B, M, lane);
-    line_r2c(z, A, a.uv + offv, lane);
-  }
   if (a.setstep) {
     mu = warp_nmax(mu);
     mw = warp_nmax(mw);
-    mv = warp_nmax(mv);
     if (lane == 0) {
       atomicMax(&a.st->umax_bits, (unsigned long long)__double_as_longlong(mu));
       atomicMax(&a.st->wmax_bits, (unsigned long long)__double_as_longlong(mw));
-      if (j <= ny) atomicMax(&a.vm_bits[j], (unsigned long long)__double_as_longlong(mv));
     }
   }
 }
@@ -380,9 +390,9 @@ __global__ void __launch_bounds__(128, std::is_same<T, double>::value ? OTBL_PR_
   constexpr int E = M / 32;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int j = blockIdx.x * 4 + wid + 1;
-  const int i = blockIdx.y + 1 + PART;
+  const int i = blockIdx.y + ProdPart<PART>::i0;
   const int ny = c.ny, nz1 = c.nz1;
-  if (j > ny + 1 - PART) return;
+  if (j > ny + ProdPart<PART>::extra) return;
   V *buf = sm + (size_t)wid * (M + M / 8);
   const size_t offu = ((size_t)(i - 1) * (ny + 1) + (j - 1)) * nz1;
   const size_t offv = ((size_t)(i - 1) * ny + (j - 1)) * nz1;
@@ -400,31 +410,35 @@ __global__ void __launch_bounds__(128, std::is_same<T, double>::value ? OTBL_PR_
     zr2c_regs<M>(z, A, a.ww + offv, buf, lane);
     return;
   }
-  double mu = 0.0, mw = 0.0, mv = 0.0;
-  zc2r_regs<M>(z, a.ux + offu, A, buf, lane);  // uu = ux^2
-  regs_sq<E>(A);
-  zr2c_regs<M>(z, A, a.uu + offu, buf, lane);
-  zc2r_regs<M>(z, a.u + offu, B, buf, lane);   // uw = wx u
-  if (a.setstep) mu = regs_absmax<E>(B);
-  zc2r_regs<M>(z, a.wx + offu, A, buf, lane);
-  if (a.setstep) mw = regs_absmax<E>(A);
-  regs_mul<E>(A, B);
-  zr2c_regs<M>(z, A, a.uw + offu, buf, lane);
-  if (j <= ny) {
+  if (PART == 2) {  // all planes, rows 1..ny
+    double mv = 0.0;
     zc2r_regs<M>(z, a.vx + offv, A, buf, lane);  // uv = vx uy
     if (a.setstep) mv = regs_absmax<E>(A);
     zc2r_regs<M>(z, a.uy + offv, B, buf, lane);
     regs_mul<E>(A, B);
     zr2c_regs<M>(z, A, a.uv + offv, buf, lane);
+    if (a.setstep) {
+      mv = warp_nmax(mv);
+      if (lane == 0) atomicMax(&a.vm_bits[j], (unsigned long long)__double_as_longlong(mv));
+    }
+    return;
   }
+  double mu = 0.0, mw = 0.0;
+  zc2r_regs<M>(z, a.ux + offu, A, buf, lane);  // uu = ux^2
+  regs_sq<E>(A);
+  zr2c_regs<M>(z, A, a.uu + offu, buf, lane);
+  zc2r_regs<M>(z, a.u + offu, B, buf, lane);  // uw = wx u
+  if (a.setstep) mu = regs_absmax<E>(B);
+  zc2r_regs<M>(z, a.wx + offu, A, buf, lane);
+  if (a.setstep) mw = regs_absmax<E>(A);
+  regs_mul<E>(A, B);
+  zr2c_regs<M>(z, A, a.uw + offu, buf, lane);
   if (a.setstep) {
     mu = warp_nmax(mu);
     mw = warp_nmax(mw);
-    mv = warp_nmax(mv);
     if (lane == 0) {
       atomicMax(&a.st->umax_bits, (unsigned long long)__double_as_longlong(mu));
       atomicMax(&a.st->wmax_bits, (unsigned long long)__double_as_longlong(mw));
-      if (j <= ny) atomicMax(&a.vm_bits[j], (unsigned long long)__double_as_longlong(mv));
     }
   }
 }
@@ -1286,17 +1300,20 @@ static cudaError_t products_t(otbl_ctx *c, int setstep, int part, const ZTabT<T>
   a.st = c->st;
   a.setstep = setstep;
   const int M = c->cfg.nz / 2;
-  // part 0: all planes, rows 1..ny+1; part 1: planes 2..nx-1, rows 1..ny
-  const dim3 g((c->cfg.ny + 1 - part + 3) / 4, c->cfg.nx - 2 * part);
+  // part 0: all planes, rows 1..ny+1; part 2: all planes, rows 1..ny;
+  // part 1: planes 2..nx-1, rows 1..ny
+  const dim3 g((c->cfg.ny + (part == 0 ? 1 : 0) + 3) / 4, c->cfg.nx - (part == 1 ? 2 : 0));
   if (M == 256) {
     const size_t smem = (size_t)4 * (M + M / 8) * sizeof(V2<T>);
     if (part == 0)
       k_products_r<256, T, 0><<<g, 128, smem, c->stream>>>(c->dc, z, a);
-    else
+    else if (part == 1)
       k_products_r<256, T, 1><<<g, 128, smem, c->stream>>>(c->dc, z, a);
+    else
+      k_products_r<256, T, 2><<<g, 128, smem, c->stream>>>(c->dc, z, a);
   } else {
     const size_t smem = (size_t)4 * 3 * M * sizeof(V2<T>);
-    auto k = part == 0 ? k_products<T, 0> : k_products<T, 1>;
+    auto k = part == 0 ? k_products<T, 0> : (part == 1 ? k_products<T, 1> : k_products<T, 2>);
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k<<<g, 128, smem, c->stream>>>(c->dc, z, a);
   }

@@ -483,55 +483,63 @@ static int rhsp_issue(otbl_ctx *c, int m, int setstep) {
   if (m == 1) LAUNCH(c, launch_energies(c));
   if (setstep) LAUNCH(c, launch_reset_max(c));
   cudaStream_t main_s = c->stream;
-  // interpyy beside interpxx (both read the state only; their checkpoints
-  // take disjoint parts of the scratch), joined before the products
+  cudaError_t e = cudaSuccess;
+  // Streams (all forks and joins by events, so a graph capture records them):
+  //   main:    interpxx, products 0 (uu, uw), [interpyy] products 2 (uv),
+  //            difvisxx, [k_dt] u tail ([genflu] before its velocity write),
+  //            [products 1] v tail, [w tail]
+  //   side:    interpyy, [products 0, 2] k_dt, [difvisxx] genflu,
+  //            [products 1] w tail on its own line scratch
+  //   side_lo: [products 2] products 1 (vw, vv, ww)
+  // interpyy and interpxx only read the state (their checkpoints take the
+  // head and the tail of the line scratch); each products part reads and
+  // writes fields no kernel beside it touches; difvisxx reads parts 0 and
+  // 2; k_dt needs the CFL maxima of parts 0 and 2; genflu needs dt, writes
+  // plane 1 of u, v, w after difvisxx has read it and reads plane xout
+  // before a tail rewrites it.
   const bool ypar = interpy_ck_tail(c, c->w.s2) != nullptr;
   if (ypar) {
     OTBL_CUDA_TRY(c, cudaEventRecord(c->ev[0], main_s));
     OTBL_CUDA_TRY(c, cudaStreamWaitEvent(c->side, c->ev[0], 0));
     c->stream = c->side;
-    cudaError_t ey = launch_interpy(c);
+    e = launch_interpy(c);
+    if (e == cudaSuccess) e = cudaEventRecord(c->ev[1], c->side);
     c->stream = main_s;
-    if (check(c, ey, "launch_interpy") != OTBL_OK) return OTBL_ERR_CUDA;
-    OTBL_CUDA_TRY(c, cudaEventRecord(c->ev[1], c->side));
+    if (check(c, e, "launch_interpy") != OTBL_OK) return OTBL_ERR_CUDA;
     LAUNCH(c, launch_interpx(c));
-    OTBL_CUDA_TRY(c, cudaStreamWaitEvent(main_s, c->ev[1], 0));
   } else {
     LAUNCH(c, launch_interpx(c));
     LAUNCH(c, launch_interpy(c));
+    OTBL_CUDA_TRY(c, cudaEventRecord(c->ev[1], main_s));
   }
   LAUNCH(c, launch_products(c, setstep, 0));
-  // Beside difvisxx and the u tail: products part 1 (vw, vv, ww: inputs and
-  // outputs disjoint from part 0's, from difvisxx's and from the u tail's)
-  // on side_lo; k_dt (needs the CFL maxima, all from part 0), then genflu
-  // on side. genflu needs dt, writes plane 1 of u, v, w, which difvisxx
-  // reads and the rhsp tail does not touch, and reads plane xout, which the
-  // tail rewrites: it runs once difvisxx is done, and the tail's first
-  // velocity write waits for it. The u tail waits for k_dt, the v and w
-  // tails for part 1.
+  OTBL_CUDA_TRY(c, cudaStreamWaitEvent(main_s, c->ev[1], 0));
+  LAUNCH(c, launch_products(c, setstep, 2));
   OTBL_CUDA_TRY(c, cudaEventRecord(c->ev[0], main_s));
+  // part 1 needs only interpyy, but started beside parts 0 and 2 it measured
+  // no faster (42.8 against 42.7 ms per FP64 RK3 step), so it follows them
   OTBL_CUDA_TRY(c, cudaStreamWaitEvent(c->side_lo, c->ev[0], 0));
-  OTBL_CUDA_TRY(c, cudaStreamWaitEvent(c->side, c->ev[0], 0));
   c->stream = c->side_lo;
-  cudaError_t e = launch_products(c, setstep, 1);
+  e = launch_products(c, setstep, 1);
   if (e == cudaSuccess) e = cudaEventRecord(c->ev[4], c->side_lo);
+  c->stream = main_s;
+  if (check(c, e, "products part 1") != OTBL_OK) return OTBL_ERR_CUDA;
+  OTBL_CUDA_TRY(c, cudaStreamWaitEvent(c->side, c->ev[0], 0));
   c->stream = c->side;
-  if (e == cudaSuccess) e = launch_dt(c, m, setstep);
+  e = launch_dt(c, m, setstep);
   if (e == cudaSuccess) e = cudaEventRecord(c->ev[1], c->side);
   c->stream = main_s;
-  if (check(c, e, "products part 1 / k_dt") != OTBL_OK) return OTBL_ERR_CUDA;
+  if (check(c, e, "k_dt") != OTBL_OK) return OTBL_ERR_CUDA;
   LAUNCH(c, launch_difvisx(c));
   OTBL_CUDA_TRY(c, cudaEventRecord(c->ev[2], main_s));
   OTBL_CUDA_TRY(c, cudaStreamWaitEvent(c->side, c->ev[2], 0));
   c->stream = c->side;
   e = launch_genflu(c, 1);
+  if (e == cudaSuccess) e = cudaEventRecord(c->ev[3], c->side);
   c->stream = main_s;
   if (check(c, e, "launch_genflu") != OTBL_OK) return OTBL_ERR_CUDA;
-  OTBL_CUDA_TRY(c, cudaEventRecord(c->ev[3], c->side));
   OTBL_CUDA_TRY(c, cudaStreamWaitEvent(main_s, c->ev[1], 0));
   LAUNCH(c, launch_final(c, 1, c->ev[3]));
-  // the v tail here and the w tail on side (its own line scratch t1..t3),
-  // both after part 1; side already follows genflu
   OTBL_CUDA_TRY(c, cudaStreamWaitEvent(c->side, c->ev[4], 0));
   c->stream = c->side;
   e = launch_final(c, 4, nullptr, true);

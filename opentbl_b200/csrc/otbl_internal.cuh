@@ -170,7 +170,8 @@ cudaError_t launch_interpy(otbl_ctx *c);
 // interpyy's checkpoint region in a line scratch when it can run beside
 // interpxx, else nullptr
 double *interpy_ck_tail(otbl_ctx *c, double *s);
-// part 0: uu, uw, uv and the CFL maxima; part 1: vw, vv, ww
+// part 0: uu, uw and the u, w CFL maxima; part 2: uv and the v maxima;
+// part 1: vw, vv, ww
 cudaError_t launch_products(otbl_ctx *c, int setstep, int part);
 cudaError_t launch_difvisx(otbl_ctx *c);
 cudaError_t launch_dt(otbl_ctx *c, int m, int setstep);
