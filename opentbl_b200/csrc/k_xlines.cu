@@ -46,18 +46,33 @@ struct XStream {
 template <typename T>
 struct XTune;
 // tma: the TMA-fed kernels (k_xline_t) instead of the register streams,
-// with segments of kti (interpxx) and ktd (difvisxx) planes; at 1025x193x512:
-// FP64 interpxx 1.17 ms (4 planes; 1.49 register-streamed), difvisxx 3.02
-// (6 planes; 3.18, and 4.17 at 8 planes); FP32 interpxx 0.87 (4 planes;
-// 1.18), difvisxx 1.70 (8 planes; 1.79).
+// with segments of kti (interpxx) and ktd (difvisxx) planes; at 1025x193x512
+// with the coefficient rows staged in the ring, FP64 RK3 step: 42.2 ms at
+// kti 8, 42.5 at 4; ktd 6 against 4 and 8: 42.5, 42.7, 42.7 (FP32 ktd 8
+// against 12: 30.8, 30.9). Before the staging: FP64 interpxx 1.17 ms (4
+// planes; 1.49 register-streamed), difvisxx 3.02 (6 planes; 3.18); FP32
+// interpxx 0.87, difvisxx 1.70.
+#ifndef OTBL_XT_DI
+#define OTBL_XT_DI 8
+#endif
+#ifndef OTBL_XT_DD
+#define OTBL_XT_DD 6
+#endif
+#ifndef OTBL_XT_FI
+#define OTBL_XT_FI 8
+#endif
+#ifndef OTBL_XT_FD
+#define OTBL_XT_FD 8
+#endif
 template <>
 struct XTune<double> {
-  static constexpr int kxi = 16, kxd = 8, minb_i = 8, kti = 4, ktd = 6;
+  static constexpr int kxi = 16, kxd = 8, minb_i = 8, kti = OTBL_XT_DI, ktd = OTBL_XT_DD;
   static constexpr bool tma = true;
 };
 template <>
 struct XTune<float> {
-  static constexpr int kxi = 8, kxd = 8, minb_i = 1, kti = 4, ktd = 8;  // minb_i: 0.88 ms unbounded, 1.19 at >= 8
+  // minb_i: 0.88 ms unbounded, 1.19 at >= 8
+  static constexpr int kxi = 8, kxd = 8, minb_i = 1, kti = OTBL_XT_FI, ktd = OTBL_XT_FD;
   static constexpr bool tma = true;
 };
 

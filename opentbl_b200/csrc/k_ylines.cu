@@ -147,13 +147,16 @@ __global__ void __launch_bounds__(128) k_interpy(DCoefT<T> c, InterpyArgs a) {
 // arithmetic is k_interpy's with segments of KYT rows.
 template <typename T>
 struct YTune;
+#ifndef OTBL_YT
+#define OTBL_YT 8
+#endif
 template <>
 struct YTune<double> {
-  static constexpr int kt = 8;
+  static constexpr int kt = OTBL_YT;
 };
 template <>
 struct YTune<float> {
-  static constexpr int kt = 8;
+  static constexpr int kt = OTBL_YT;
 };
 
 template <typename T>
@@ -994,7 +997,9 @@ double *interpy_ck_tail(otbl_ctx *c, double *s) {
   const int nx = c->cfg.nx, ny = c->cfg.ny, nz = c->cfg.nz, nz1 = c->dc.nz1;
   const size_t lu = otbl_field_len(nx, ny, nz, 1);  // doubles in s2, s3 (s1 may be larger)
   const size_t ncol = (size_t)nx * nz1;
-  const size_t y_need = (size_t)((ny + KY - 1) / KY) * ncol;  // doubles (floats need less)
+  // the shorter of the register-streamed and the TMA-fed segments
+  const int ky = KY < YTune<double>::kt ? KY : YTune<double>::kt;
+  const size_t y_need = (size_t)((ny + ky - 1) / ky) * ncol;  // doubles (floats need less)
   // interpxx: at most one checkpoint per 4 planes per line (4 is its shortest segment)
   const size_t x_need = (size_t)((nx + 3) / 4) * (size_t)(ny + 1) * nz1;
   if (x_need + y_need + 64 > lu) return nullptr;
