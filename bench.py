@@ -482,11 +482,10 @@ def main():
                           "parallelism": f"replicas{ws}", "autotuned_cta_sizes": list(tuned)},
                "roofline": roofline, "substep_roofline": substep_roofline,
                "kernels_ms_per_substep": kernels,
-               "kernels_note": "CUDA events around each kernel class on its stream (products = both "
-                               "halves, final = the u tail plus the v and w tails); interpy, dt, "
-                               "genflu and the products' second half run on side streams beside "
-                               "interpx, difvisx and the u tail, so their times include that overlap "
-                               "and the classes do not add up to ms_per_step/3",
+               "kernels_note": "CUDA events around each kernel class in a separate profiled RK3 step "
+                               "whose kernels run on one stream (products = its three parts, final = "
+                               "the three velocity tails); the timed steps overlap kernels on side "
+                               "streams, so the classes add up to more than ms_per_step/3",
                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
                "mixed": mixed, "ensemble": ens, "serving": srv}
         print(json.dumps(out), flush=True)

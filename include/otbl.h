@@ -243,7 +243,9 @@ int otbl_selftest_wait(otbl_ctx *ctx, int *status);
 /* the context's CUDA stream (cudaStream_t), for events recorded by callers */
 int otbl_get_stream(otbl_ctx *ctx, void **stream);
 /* on != 0: record a CUDA event pair around every kernel launch; clears the
- * records. Timing adds events to the stream; leave it off for throughput. */
+ * records. While on, a substep runs on the context stream alone (none of its
+ * kernels overlap), so each class's time is its own kernels' duration.
+ * Timing adds events and removes the overlap; leave it off for throughput. */
 int otbl_profile_enable(otbl_ctx *ctx, int on);
 /* totals per kernel class (kind = 0, 1, ...; OTBL_ERR_ARG past the last):
  * name, summed device milliseconds and number of launches. Synchronizes. */

@@ -483,6 +483,9 @@ static int rhsp_issue(otbl_ctx *c, int m, int setstep) {
   if (m == 1) LAUNCH(c, launch_energies(c));
   if (setstep) LAUNCH(c, launch_reset_max(c));
   cudaStream_t main_s = c->stream;
+  // with per-kernel timing on, everything runs on the context stream, so
+  // that each event pair brackets its own kernels only
+  cudaStream_t side = c->prof_on ? main_s : c->side, side_lo = c->prof_on ? main_s : c->side_lo;
   cudaError_t e = cudaSuccess;
   // Streams (all forks and joins by events, so a graph capture records them):
   //   main:    interpxx, products 0 (uu, uw), [interpyy] products 2 (uv),
@@ -500,10 +503,10 @@ static int rhsp_issue(otbl_ctx *c, int m, int setstep) {
   const bool ypar = interpy_ck_tail(c, c->w.s2) != nullptr;
   if (ypar) {
     OTBL_CUDA_TRY(c, cudaEventRecord(c->ev[0], main_s));
-    OTBL_CUDA_TRY(c, cudaStreamWaitEvent(c->side, c->ev[0], 0));
-    c->stream = c->side;
+    OTBL_CUDA_TRY(c, cudaStreamWaitEvent(side, c->ev[0], 0));
+    c->stream = side;
     e = launch_interpy(c);
-    if (e == cudaSuccess) e = cudaEventRecord(c->ev[1], c->side);
+    if (e == cudaSuccess) e = cudaEventRecord(c->ev[1], side);
     c->stream = main_s;
     if (check(c, e, "launch_interpy") != OTBL_OK) return OTBL_ERR_CUDA;
     LAUNCH(c, launch_interpx(c));
@@ -518,32 +521,32 @@ static int rhsp_issue(otbl_ctx *c, int m, int setstep) {
   OTBL_CUDA_TRY(c, cudaEventRecord(c->ev[0], main_s));
   // part 1 needs only interpyy, but started beside parts 0 and 2 it measured
   // no faster (42.8 against 42.7 ms per FP64 RK3 step), so it follows them
-  OTBL_CUDA_TRY(c, cudaStreamWaitEvent(c->side_lo, c->ev[0], 0));
-  c->stream = c->side_lo;
+  OTBL_CUDA_TRY(c, cudaStreamWaitEvent(side_lo, c->ev[0], 0));
+  c->stream = side_lo;
   e = launch_products(c, setstep, 1);
-  if (e == cudaSuccess) e = cudaEventRecord(c->ev[4], c->side_lo);
+  if (e == cudaSuccess) e = cudaEventRecord(c->ev[4], side_lo);
   c->stream = main_s;
   if (check(c, e, "products part 1") != OTBL_OK) return OTBL_ERR_CUDA;
-  OTBL_CUDA_TRY(c, cudaStreamWaitEvent(c->side, c->ev[0], 0));
-  c->stream = c->side;
+  OTBL_CUDA_TRY(c, cudaStreamWaitEvent(side, c->ev[0], 0));
+  c->stream = side;
   e = launch_dt(c, m, setstep);
-  if (e == cudaSuccess) e = cudaEventRecord(c->ev[1], c->side);
+  if (e == cudaSuccess) e = cudaEventRecord(c->ev[1], side);
   c->stream = main_s;
   if (check(c, e, "k_dt") != OTBL_OK) return OTBL_ERR_CUDA;
   LAUNCH(c, launch_difvisx(c));
   OTBL_CUDA_TRY(c, cudaEventRecord(c->ev[2], main_s));
-  OTBL_CUDA_TRY(c, cudaStreamWaitEvent(c->side, c->ev[2], 0));
-  c->stream = c->side;
+  OTBL_CUDA_TRY(c, cudaStreamWaitEvent(side, c->ev[2], 0));
+  c->stream = side;
   e = launch_genflu(c, 1);
-  if (e == cudaSuccess) e = cudaEventRecord(c->ev[3], c->side);
+  if (e == cudaSuccess) e = cudaEventRecord(c->ev[3], side);
   c->stream = main_s;
   if (check(c, e, "launch_genflu") != OTBL_OK) return OTBL_ERR_CUDA;
   OTBL_CUDA_TRY(c, cudaStreamWaitEvent(main_s, c->ev[1], 0));
   LAUNCH(c, launch_final(c, 1, c->ev[3]));
-  OTBL_CUDA_TRY(c, cudaStreamWaitEvent(c->side, c->ev[4], 0));
-  c->stream = c->side;
+  OTBL_CUDA_TRY(c, cudaStreamWaitEvent(side, c->ev[4], 0));
+  c->stream = side;
   e = launch_final(c, 4, nullptr, true);
-  if (e == cudaSuccess) e = cudaEventRecord(c->ev[5], c->side);
+  if (e == cudaSuccess) e = cudaEventRecord(c->ev[5], side);
   c->stream = main_s;
   if (check(c, e, "w tail") != OTBL_OK) return OTBL_ERR_CUDA;
   OTBL_CUDA_TRY(c, cudaStreamWaitEvent(main_s, c->ev[4], 0));
