@@ -182,7 +182,9 @@ def run_reference(args, cfg, ws, rank):
     from oracle import pyoracle
     threads = os.cpu_count() or 1
     ob = pyoracle.OracleBox(cfg, init, coef, threads=threads)
-    warm = min(args.warmup, 1)
+    # one step = one substep of the box on the host cores (about 5 s on 16
+    # threads); up to 3 warm-up and 3 timed ones keep the run within a minute
+    warm = min(args.warmup, 3)
     steps = max(1, min(args.steps, 3))
     for s in range(warm):
         ob.substep(s % 3 + 1, 1 if s % 3 == 0 else 0)
