@@ -38,11 +38,13 @@ struct FinalTune;
 #endif
 // split: pass A in a kernel of its own (FP32 inputs: 6.69 against 7.09 ms;
 // FP64: 7.18 against 6.84 ms fused)
-// kf_tma: segment of the TMA-fed pass (k_final_tb) and its pass A; 2 rows
-// measured best (FP64 6.38 ms per substep against 6.49 at 4 rows; mixed
-// 5.53 against 5.94)
+// kf_tma: segment of the TMA-fed pass (k_final_tb) and its pass A. With the
+// coefficient rows staged in the ring, 4 rows: rhsp tail 3.47 ms per FP64
+// substep against 3.73 at 3, 3.90 at 2, 3.71 at 5 and 3.82 at 6 (mixed 2.62,
+// 2.77, 2.87, 2.74, 2.72), and 3.99 with a three-stage ring; before the
+// staging 2 rows were best (6.38 against 6.49 at 4).
 #ifndef OTBL_FT_TK
-#define OTBL_FT_TK 2
+#define OTBL_FT_TK 4
 #endif
 #ifndef OTBL_FT_NS
 #define OTBL_FT_NS 2
