@@ -88,5 +88,6 @@ def test_bench_reference_arm_under_torchrun():
               "cpu_baseline", "e2e"):
         assert k in d, k
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
+    assert d["steps"] == 1 and d["warmup"] == 1  # as asked (each is one substep)
     assert d["cpu_baseline"]["kind"] == "port"
     assert d["e2e"]["h2d_bytes_per_step"] == 0
