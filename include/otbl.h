@@ -9,7 +9,10 @@
  * the device-resident state. Every entry point returns an int status
  * (OTBL_OK = 0) and otbl_last_error() gives the message. Calls on one context
  * are stream-ordered on the context's CUDA stream and are not re-entrant;
- * different contexts may be driven from different host threads.
+ * different contexts may be driven from different host threads. otbl_rhsp
+ * forks part of its kernels onto two internal streams of the context and
+ * joins them back into the context stream before its work ends, so callers
+ * see a single ordered stream (a capture of that stream records the forks).
  *
  * Field arrays use the reference's single-rank plane layout (otbl_layout.h).
  * Plane indices i, rows j and the recycling plane xout are 1-based, as in the
