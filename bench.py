@@ -162,7 +162,7 @@ def cpu_baseline(cfg, init, coef, nsub: int):
     """The CPU port (oracle/) on nsub substeps of the same box, all host threads."""
     from oracle import pyoracle
     threads = os.cpu_count() or 1
-    ob = pyoracle.OracleBox(cfg, init, coef, threads=threads)
+    ob = pyoracle.OracleBox(cfg, init, threads=threads)
     t0 = time.perf_counter()
     for s in range(nsub):
         m = s % 3 + 1
@@ -181,7 +181,7 @@ def run_reference(args, cfg, ws, rank):
     coef = native.coef_compute(cfg, init["re"], init["xout"], init["y"], init["u0"])
     from oracle import pyoracle
     threads = os.cpu_count() or 1
-    ob = pyoracle.OracleBox(cfg, init, coef, threads=threads)
+    ob = pyoracle.OracleBox(cfg, init, threads=threads)
     # one step = one substep of the box on the host cores (about 5 s on 16
     # threads); up to 3 warm-up and 3 timed ones keep the run within a minute
     warm = min(args.warmup, 3)

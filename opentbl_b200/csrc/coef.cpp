@@ -15,9 +15,10 @@
 // The statistics-only arrays of coef (fd_*, l_weight, ldyy) are not built:
 // nothing on the substep reads them.
 //
-// Output is the packed buffer described in include/otbl_layout.h. The same
-// buffer is uploaded to the device and handed to the CPU oracle, so both
-// sides run on bit-identical coefficients.
+// Output is the packed buffer described in include/otbl_layout.h, uploaded
+// to the device by otbl_ctx_create. Fortran semantics are kept where they
+// change bits: integer powers as gfortran expands them, Fortran precedence,
+// and the single-precision kaz of cmplx() without KIND (bl_1.F90:360).
 
 #include <cmath>
 #include <cstring>
@@ -49,7 +50,11 @@ struct Mat {
 
 inline double sq(double a) { return a * a; }
 inline double cu(double a) { return a * a * a; }
-inline double p4(double a) { return a * a * a * a; }
+// x**4 as gfortran expands an integer power: (x*x)*(x*x)
+inline double p4(double a) {
+  const double s = a * a;
+  return s * s;
+}
 
 // ludcmp, coeft.f90:1818-1883 (Numerical Recipes, implicit pivoting).
 // bc is the (np x np) column-major work matrix, n <= np.
@@ -316,8 +321,9 @@ extern "C" int otbl_coef_compute(const otbl_config *cfg, const double *yin,
     daux = std::fmin(daux, dy[i]);
   }
   double dzmin = az * 2 * pi / nz;
-  const double dtrex = re * (cfl * dxmin * dxmin) / 6.0;
-  const double dtrez = re * (cfl * dzmin * dzmin) / (pi * pi);
+  // re*(cfl*dxmin**2)/(6.0d0): the power binds first
+  const double dtrex = re * (cfl * (dxmin * dxmin)) / 6.0;
+  const double dtrez = re * (cfl * (dzmin * dzmin)) / (pi * pi);
   const double dtret = std::fmin(dtrex, dtrez);
   dxmin = dxmin * cfl / std::sqrt(3.0);
   dzmin = dzmin * cfl / pi;
@@ -325,8 +331,12 @@ extern "C" int otbl_coef_compute(const otbl_config *cfg, const double *yin,
 
   // wavenumbers, bl_1.F90:357-366, and kvis, coeft.f90:484-486
   double *kaz = P(OTBL_C_KAZ), *kaz2 = P(OTBL_C_KAZ2), *kvis = P(OTBL_C_KVIS);
+  // kaz(k) = cmplx(0d0, k/az): CMPLX without KIND is a default-kind
+  // (REAL*4) complex, so the imaginary part is k/az rounded to single
+  // precision before it is stored in the complex*16 kaz (the reference's
+  // builds use no default-real promotion flag)
   for (int k = 0; k <= nz2; ++k) {
-    kaz[k] = k / az;             // kaz(k) = cmplx(0, k/az): imaginary part
+    kaz[k] = (double)(float)((double)k / az);
     kaz2[k] = -(-(kaz[k] * kaz[k]));  // -kaz**2 = +k**2/az**2 (real)
     kvis[k] = rex * kaz2[k];
   }

@@ -39,6 +39,12 @@ void orc_r2c_line(const orc_fft *h, int nz, int nz2, const double *phys,
                   double *fou, double *work);
 void orc_dct_line(const orc_fft *p, int n, double *c, int iopt, double *work);
 
+/* the reference's coefficient set-up (coeft.f90 coef, bl_1.F90 wavenumbers
+ * and inlet_retheta, boun.f90 magicnumber) into the packed buffer of
+ * otbl_layout.h, computed by the oracle's own code (orc_coef.c) */
+int orc_coef_compute(const otbl_config *cfg, const double *y, const double *u0,
+                     double *coef);
+
 typedef struct orc_box orc_box;
 
 orc_box *orc_create(const otbl_config *cfg, const double *coef);

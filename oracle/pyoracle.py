@@ -47,6 +47,8 @@ def lib():
         L = ctypes.CDLL(_LIB)
         P = ctypes.c_void_p
         D = ctypes.POINTER(ctypes.c_double)
+        L.orc_coef_compute.argtypes = [ctypes.POINTER(OtblConfig), D, D, D]
+        L.orc_coef_compute.restype = ctypes.c_int
         L.orc_create.restype = P
         L.orc_create.argtypes = [ctypes.POINTER(OtblConfig), D]
         L.orc_destroy.argtypes = [P]
@@ -103,16 +105,42 @@ def make_config(cfg, re: float, xout: int) -> OtblConfig:
                       getattr(cfg, "precision", 0), 0)
 
 
-class OracleBox:
-    """CPU restatement of one box; same state layout as the product."""
+def coef_count(cfg) -> int:
+    """Length of the packed coefficient buffer (include/otbl_layout.h)."""
+    nx, ny, nz2 = cfg.nx, cfg.ny, cfg.nz2
+    lens = [64, ny + 2, ny + 1, ny + 1, ny, ny, ny + 1, nx + 2, nx + 1, nz2 + 1, nz2 + 1,
+            nz2 + 1, nx - 1, 3 * ny, nx, 3 * nx, 3 * nx, 2 * nx, 2 * nx, 16, 3 * nx, 3 * nx,
+            2 * nx, 2 * nx, 20, 3 * nx, 3 * nx, 3 * nx, 3 * nx, 16, 3 * ny, 3 * ny, 2 * ny,
+            2 * ny, 16, 3 * (ny + 1), 3 * ny, 2 * ny, 2 * ny, 16, 3 * (ny + 1), 3 * ny,
+            3 * (ny + 1), 3 * ny, 3 * ny, 3 * ny, 16, 8]
+    return int(sum(lens))
 
-    def __init__(self, cfg, init: dict, coef: np.ndarray, threads: int = 0):
+
+def coef_compute(cfg, re: float, xout: int, y: np.ndarray, u0: np.ndarray) -> np.ndarray:
+    """The oracle's own coefficient set-up (oracle/orc_coef.c: coeft.f90
+    coef, bl_1.F90 wavenumbers and inlet_retheta, boun.f90 magicnumber)."""
+    L = lib()
+    c = make_config(cfg, re, xout)
+    out = np.zeros(coef_count(cfg))
+    st = L.orc_coef_compute(ctypes.byref(c), dptr(np.ascontiguousarray(y, dtype=np.float64)),
+                            dptr(np.ascontiguousarray(u0, dtype=np.float64)), dptr(out))
+    if st != 0:
+        raise RuntimeError(f"orc_coef_compute failed: {st}")
+    return out
+
+
+class OracleBox:
+    """CPU restatement of one box; same state layout as the product. Its
+    coefficients come from the oracle's own set-up (coef_compute) on the
+    box's grid y, inlet profile u0, Re and xout."""
+
+    def __init__(self, cfg, init: dict, threads: int = 0):
         self.cfg = cfg
         self.L = lib()
         if threads:
             self.L.orc_set_threads(threads)
         self.ccfg = make_config(cfg, init["re"], init["xout"])
-        self.coef = np.ascontiguousarray(coef, dtype=np.float64)
+        self.coef = coef_compute(cfg, init["re"], init["xout"], init["y"], init["u0"])
         self.h = self.L.orc_create(ctypes.byref(self.ccfg), dptr(self.coef))
         for i, n in enumerate(FIELDS):
             self.set_field(n, init[n])

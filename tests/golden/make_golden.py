@@ -22,7 +22,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
-from opentbl_b200 import config, native, synth  # noqa: E402
+from opentbl_b200 import config, synth  # noqa: E402
 from opentbl_b200.config import replace  # noqa: E402
 from oracle import pyoracle  # noqa: E402
 
@@ -58,12 +58,11 @@ def make():
     out = {}
     for tag, cfg in cases().items():
         init = synth.make_initial(cfg)
-        coef = native.coef_compute(cfg, init["re"], init["xout"], init["y"], init["u0"])
-        ob = pyoracle.OracleBox(cfg, init, coef, threads=1)
+        ob = pyoracle.OracleBox(cfg, init, threads=1)
         ob.substep(1, 1)
         one = state_fp(ob)
         ob.close()
-        ob = pyoracle.OracleBox(cfg, init, coef, threads=1)
+        ob = pyoracle.OracleBox(cfg, init, threads=1)
         ob.advance(1)
         step = state_fp(ob)
         ob.close()

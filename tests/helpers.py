@@ -20,8 +20,10 @@ def max_abs(a):
     return float(np.max(np.abs(a)))
 
 
-def oracle_box(cfg, init, coef, threads=0):
-    return pyoracle.OracleBox(cfg, init, coef, threads=threads)
+def oracle_box(cfg, init, threads=0):
+    """The oracle on the same seeded input; it computes its coefficients
+    with its own set-up code (oracle/orc_coef.c)."""
+    return pyoracle.OracleBox(cfg, init, threads=threads)
 
 
 divergence_np = diag.divergence

@@ -81,7 +81,7 @@ def test_restart_continues_like_the_oracle(tmp_path):
     h = Box(cfg, r, coef)
     for n in native.FIELDS:
         assert np.array_equal(h.field(n), r[n]), n
-    o = oracle_box(cfg, r, coef)
+    o = oracle_box(cfg, r)
     h.advance(1)
     o.advance(1)
     for n in ("u", "v", "w", "p"):

@@ -44,10 +44,10 @@ def _inputs(tag):
 @pytest.mark.parametrize("tag", ["fp64", "real4"])
 def test_oracle_reproduces_fixtures(tag):
     cfg, init, coef = _inputs(tag)
-    ob = pyoracle.OracleBox(cfg, init, coef, threads=1)
+    ob = pyoracle.OracleBox(cfg, init, threads=1)
     ob.substep(1, 1)
     _check(ob, FIX[tag]["substep1"], 1e-13, 1e-12)
-    ob = pyoracle.OracleBox(cfg, init, coef, threads=1)
+    ob = pyoracle.OracleBox(cfg, init, threads=1)
     ob.advance(1)
     _check(ob, FIX[tag]["step1"], 1e-13, 1e-12)
 

@@ -40,7 +40,7 @@ def test_mixed_one_substep(name):
     cfg = getattr(config, name)
     init, coef = setup(cfg)
     g = Box(_mixed(cfg), init, coef)
-    o = oracle_box(cfg, init, coef)
+    o = oracle_box(cfg, init)
     g.substep(1, True)
     o.substep(1, 1)
     r = _report(f"{name} mixed, 1 substep", g, o, cfg, coef)
@@ -62,7 +62,7 @@ def test_mixed_c1_twenty_steps():
     cfg = config.C1
     init, coef = setup(cfg)
     g = Box(_mixed(cfg), init, coef)
-    o = oracle_box(cfg, init, coef)
+    o = oracle_box(cfg, init)
     g.advance(20)
     o.advance(20)
     r = _report("C1 mixed, 20 steps", g, o, cfg, coef)

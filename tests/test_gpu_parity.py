@@ -25,7 +25,7 @@ STATE = ("u", "v", "w", "p", "rhsupa", "rhsvpa", "rhswpa")
 
 def _pair(cfg):
     init, coef = setup(cfg)
-    return Box(cfg, init, coef), oracle_box(cfg, init, coef), init, coef
+    return Box(cfg, init, coef), oracle_box(cfg, init), init, coef
 
 
 def _compare(gpu, orc, names=STATE):

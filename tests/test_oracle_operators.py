@@ -20,7 +20,7 @@ def tiny():
     cfg = config.TINY
     init = synth.make_initial(cfg)
     coef = native.coef_compute(cfg, init["re"], init["xout"], init["y"], init["u0"])
-    ob = pyoracle.OracleBox(cfg, init, coef, threads=1)
+    ob = pyoracle.OracleBox(cfg, init, threads=1)
     off = native.coef_offsets(cfg)
     yield cfg, init, coef, off, ob
     ob.close()
@@ -189,12 +189,14 @@ def test_implzy_identity_and_constants(tiny, which):
 
 
 # ---------------- coefficient closed forms -----------------------------------
+@pytest.mark.parametrize("source", ["oracle", "product"])
 @pytest.mark.parametrize("name", ["TINY", "C1", "C2"])
-def test_coefficient_closed_forms(name):
+def test_coefficient_closed_forms(name, source):
     cfg = getattr(config, name)
     init = synth.make_initial(cfg)
     y, u0, re, xout = init["y"], init["u0"], init["re"], init["xout"]
-    coef = native.coef_compute(cfg, re, xout, y, u0)
+    compute = pyoracle.coef_compute if source == "oracle" else native.coef_compute
+    coef = compute(cfg, re, xout, y, u0)
     off = native.coef_offsets(cfg)
     S = lambda n: coef[off["SCAL"] + native.SCAL[n]]  # noqa: E731
     nx, nz2 = cfg.nx, cfg.nz2
@@ -211,8 +213,11 @@ def test_coefficient_closed_forms(name):
     kaz = coef[off["KAZ"]:off["KAZ"] + nz2 + 1]
     kaz2 = coef[off["KAZ2"]:off["KAZ2"] + nz2 + 1]
     kvis = coef[off["KVIS"]:off["KVIS"] + nz2 + 1]
-    np.testing.assert_allclose(kaz, k / S("AZ"), rtol=1e-15, atol=0)
-    np.testing.assert_allclose(kaz2, (k / S("AZ")) ** 2, rtol=4e-16, atol=0)
+    # cmplx(0d0, k/az) without KIND is a REAL*4 complex (bl_1.F90:360)
+    kz32 = (k / S("AZ")).astype(np.float32).astype(np.float64)
+    np.testing.assert_array_equal(kaz, kz32)
+    np.testing.assert_allclose(kaz, k / S("AZ"), rtol=1e-7, atol=0)
+    np.testing.assert_array_equal(kaz2, kz32 * kz32)
     np.testing.assert_allclose(kvis, S("REX") * kaz2, rtol=4e-16, atol=0)
     # Poisson eigenvalues in x, coeft.f90:1181-1183
     m = np.arange(1, nx, dtype=float)
@@ -224,4 +229,4 @@ def test_coefficient_closed_forms(name):
     idyy = coef[off["IDYY"]:off["IDYY"] + cfg.ny]
     np.testing.assert_allclose(idyy, 2.0 / (dy[:-1] + dy[1:]), rtol=1e-15)
     # packed buffer is deterministic
-    np.testing.assert_array_equal(coef, native.coef_compute(cfg, re, xout, y, u0))
+    np.testing.assert_array_equal(coef, compute(cfg, re, xout, y, u0))

@@ -26,7 +26,7 @@ def test_projection_is_divergence_free(tiny):
     """pois.f90:11-239: after rhsp + outflow_correction + pois the
     divergence of pois.f90:41-54 is at round-off."""
     init, coef = tiny
-    ob = oracle_box(config.TINY, init, coef, threads=2)
+    ob = oracle_box(config.TINY, init, threads=2)
     d0 = np.abs(ob.divergence()).max()
     ob.substep(1, 1)
     d1 = np.abs(ob.divergence()).max()
@@ -62,7 +62,7 @@ def _genflu_numpy(ucol0, um, y, dy, re, rthin, dt, tloc):
 def test_genflu_integrals_against_numpy(tiny, tiempo):
     init, coef = tiny
     cfg = config.TINY
-    ob = oracle_box(cfg, init, coef, threads=1)
+    ob = oracle_box(cfg, init, threads=1)
     st = pyoracle.OtblInflow()
     st.dt, st.tiempo, st.timeinit = 0.05, tiempo, 0.0
     um0 = np.ascontiguousarray(init["um"])
@@ -110,7 +110,7 @@ def test_energies_against_numpy(tiny):
     """ener after rhsp(m=1) is computed from the state rhsp was called on;
     substeps 2 and 3 leave it alone."""
     init, coef = tiny
-    ob = oracle_box(config.TINY, init, coef, threads=2)
+    ob = oracle_box(config.TINY, init, threads=2)
     assert not ob.energies().any()
     u, v, w = (ob.field(n).copy() for n in "uvw")
     ob.substep(1, 1)
@@ -124,8 +124,8 @@ def test_energies_against_numpy(tiny):
 
 def test_real4_transposes_perturb_at_single_precision(tiny):
     init, coef = tiny
-    a = oracle_box(config.TINY, init, coef, threads=1)
-    b = oracle_box(replace(config.TINY, xpose_round=1), init, coef, threads=1)
+    a = oracle_box(config.TINY, init, threads=1)
+    b = oracle_box(replace(config.TINY, xpose_round=1), init, threads=1)
     a.substep(1, 1)
     b.substep(1, 1)
     e = [rel_l2(b.field(n), a.field(n)) for n in ("u", "v", "w")]
@@ -135,7 +135,7 @@ def test_real4_transposes_perturb_at_single_precision(tiny):
 def test_fixed_dt_mode(tiny):
     init, coef = tiny
     cfg = replace(config.TINY, dt_mode=1, dt_fixed=0.0125)
-    ob = oracle_box(cfg, init, coef, threads=1)
+    ob = oracle_box(cfg, init, threads=1)
     ob.advance(2)
     um, st = ob.inflow()
     assert st["dt"] == 0.0125
@@ -147,7 +147,7 @@ def test_adaptive_dt_is_the_cfl_limit(tiny):
     dtret); with the maxima reported by the oracle the limit is reproduced."""
     init, coef = tiny
     cfg = config.TINY
-    ob = oracle_box(cfg, init, coef, threads=1)
+    ob = oracle_box(cfg, init, threads=1)
     ob.rhsp(1, 1)
     um, st = ob.inflow()
     off = native.coef_offsets(cfg)
@@ -163,7 +163,7 @@ def test_threads_do_not_change_the_result(tiny):
     init, coef = tiny
     res = []
     for t in (1, 4):
-        ob = oracle_box(config.TINY, init, coef, threads=t)
+        ob = oracle_box(config.TINY, init, threads=t)
         ob.advance(1)
         res.append({n: ob.field(n) for n in STATE})
         ob.close()

@@ -36,7 +36,7 @@ def _rank_main(rank, ws, port, q):
     from helpers import oracle_box, setup
     R = replicas.setup("gloo", timeout_s=60)
     init, coef = setup(config.TINY)
-    ob = oracle_box(config.TINY, init, coef, threads=1)
+    ob = oracle_box(config.TINY, init, threads=1)
     replicas.barrier(R)
     t0 = time.perf_counter()
     ob.substep(1, 1)
