@@ -9,7 +9,8 @@ One bench "step" is one full RK3 time step (3 substeps, bl_1.F90:94-125);
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 --impl reference times the CPU port of the reference's substep (oracle/,
-OpenMP on all host cores) on the same box, one substep per sample step.
+its own coefficient set-up and kernels, OpenMP on all host cores) on the same
+box: the requested warm-up and timed steps, each a full RK3 step.
 For N > 1 (torchrun), every rank advances its own independent box (replicas
 only: a box does not shard without the reference's global transposes); the
 time is the max over ranks.
@@ -48,16 +49,30 @@ def peaks():
 
 
 # Mixed path (OTBL_PREC_MIXED): element size of each pass of the 55-pass
-# substep schedule (stages A, B, C, D, P of the FP64 figure). FP64: the
-# state u, v, w, p, the RHS history, phi and the divergence; FP32: the x
-# interpolants, the products and partial right-hand sides, and the x-line
-# right-hand sides.
-#   A  reads phi, u, v, w, p; writes u, v, w, p (9 FP64), u_x, v_x, w_x (3 FP32)
-#   B  reads u, v, w (3 FP64), u_x, v_x, w_x; writes 3 products, 3 partial RHS (9 FP32)
-#   C  reads u, v, w (3 FP64), 3 products, 3 partial RHS; writes 3 RHS (9 FP32)
-#   D  reads 3 RHS (3 FP32), RHS history, u, v, w, p; writes u, v, w, RHS history, div (14 FP64)
-#   P  reads div, writes phi (2 FP64)
-MIXED_MANIFEST = {"fp64_passes": 9 + 3 + 3 + 14 + 2, "fp32_passes": 3 + 9 + 9 + 3}
+# substep schedule (stages A, B, C, D, P of the FP64 figure), as the mixed
+# path stores the fields. FP64: the velocity u, v, w; FP32: the pressure p,
+# the RHS history rhs*pa, the x interpolants, the products and partial
+# right-hand sides, and the x-line right-hand sides. The divergence and phi
+# (four passes) hold the spanwise modes k < 4 in FP64 and the others in
+# FP32, so a fraction 4/(nz2+1) of those passes is FP64.
+#   A  reads phi (div/phi), u, v, w (3 FP64), p (1 FP32);
+#      writes u, v, w (3 FP64), p, u_x, v_x, w_x (4 FP32)         6 + 5 + 1 div/phi
+#   B  reads u, v, w (3 FP64), u_x, v_x, w_x;
+#      writes 3 products, 3 partial RHS (9 FP32)                    3 + 9
+#   C  reads u, v, w (3 FP64), 3 products, 3 partial RHS;
+#      writes 3 RHS (9 FP32)                                        3 + 9
+#   D  reads 3 RHS, 3 RHS history, p (7 FP32), u, v, w (3 FP64);
+#      writes u, v, w (3 FP64), div, 3 RHS history (3 FP32)        6 + 10 + 1 div/phi
+#   P  reads div, writes phi                                        2 div/phi
+MIXED_MANIFEST = {"fp64_passes": 6 + 3 + 3 + 6, "fp32_passes": 5 + 9 + 9 + 10,
+                  "div_phi_passes": 4, "div_phi_fp64_modes": 4}
+
+
+def mixed_passes(cfg):
+    """(FP64 passes, FP32 passes) of the mixed substep for this box."""
+    f64 = min(MIXED_MANIFEST["div_phi_fp64_modes"], cfg.nz2 + 1) / (cfg.nz2 + 1)
+    dp = MIXED_MANIFEST["div_phi_passes"]
+    return (MIXED_MANIFEST["fp64_passes"] + dp * f64, MIXED_MANIFEST["fp32_passes"] + dp * (1 - f64))
 
 
 def algorithmic_bytes(cfg) -> dict:
@@ -78,7 +93,7 @@ def algorithmic_bytes(cfg) -> dict:
         "pois_bwd": 2 * V,
         "project": V + 2 * (2 * U + 2 * V),
         "substep_survey": 55.0 * U,
-        "substep_mixed": (MIXED_MANIFEST["fp64_passes"] + MIXED_MANIFEST["fp32_passes"] / 2.0) * U,
+        "substep_mixed": (mixed_passes(cfg)[0] + mixed_passes(cfg)[1] / 2.0) * U,
     }
 
 
@@ -158,52 +173,94 @@ def build_box(cfg, device):
     return init, coef, Box(cfg, init, coef, device=device)
 
 
-def cpu_baseline(cfg, init, coef, nsub: int):
-    """The CPU port (oracle/) on nsub substeps of the same box, all host threads."""
+def workload_config(cfg, ws):
+    """The `config` of both arms' JSON lines (identical by construction)."""
+    nz1 = 2 * (cfg.nz // 3)
+    state = 8.0 * cfg.nx * nz1 * (4 * (cfg.ny + 1) + 3 * cfg.ny)
+    return {"workload": f"rk3_substep {cfg.name} fp64", "nx": cfg.nx, "ny": cfg.ny,
+            "nz": cfg.nz, "substeps_per_step": 3,
+            "l2": "inputs larger than L2 (state %.1f GB per box)" % (state / 1e9),
+            "parallelism": f"replicas{ws}"}
+
+
+def host_cpu():
+    """CPU model, logical CPUs of the host and CPUs this process may use."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    try:
+        usable = len(os.sched_getaffinity(0))
+    except AttributeError:
+        usable = os.cpu_count() or 1
+    return {"cpu_model": model, "nproc": os.cpu_count(), "usable": usable}
+
+
+def in_tree_libraries():
+    """In-tree shared objects mapped into this process (from /proc/self/maps),
+    as paths relative to the repository root."""
+    found = set()
+    try:
+        with open("/proc/self/maps") as f:
+            for line in f:
+                path = line.split()[-1] if line.strip() else ""
+                if path.endswith(".so") and path.startswith(ROOT + os.sep):
+                    found.add(os.path.relpath(path, ROOT))
+    except OSError:
+        return None
+    return sorted(found)
+
+
+def cpu_baseline(cfg, init, nsteps: int):
+    """The CPU port (oracle/, its own coefficients) on nsteps RK3 steps of the
+    same box, with every usable host thread."""
     from oracle import pyoracle
-    threads = os.cpu_count() or 1
+    threads = host_cpu()["usable"]
     ob = pyoracle.OracleBox(cfg, init, threads=threads)
     t0 = time.perf_counter()
-    for s in range(nsub):
-        m = s % 3 + 1
-        st = ob.substep(m, 1 if m == 1 else 0)
-        if st != 0:
-            raise RuntimeError(f"oracle substep failed: {st}")
+    ob.advance(nsteps)
     dt = time.perf_counter() - t0
     ob.close()
-    return cfg.mpts * nsub / dt, threads, dt
+    return cfg.mpts * 3 * nsteps / dt, threads, dt
 
 
 def run_reference(args, cfg, ws, rank):
+    """The reference arm: the CPU port of the path (oracle/: its own
+    coefficient set-up, operators, FFTs and Poisson solve; nothing of the
+    product is loaded) on the same box, `warmup` untimed and `steps` timed
+    full RK3 steps, every usable host thread. Rank 0 alone runs it."""
     if rank != 0:
         return
     init = synth.make_initial(cfg)
-    coef = native.coef_compute(cfg, init["re"], init["xout"], init["y"], init["u0"])
     from oracle import pyoracle
-    threads = os.cpu_count() or 1
+    cpu = host_cpu()
+    threads = cpu["usable"]
     ob = pyoracle.OracleBox(cfg, init, threads=threads)
-    # one step = one substep of the box on the host cores (about 5 s on 16
-    # threads); up to 3 warm-up and 3 timed ones keep the run within a minute
-    warm = min(args.warmup, 3)
-    steps = max(1, min(args.steps, 3))
-    for s in range(warm):
-        ob.substep(s % 3 + 1, 1 if s % 3 == 0 else 0)
+    warm = max(args.warmup, 0)
+    steps = max(args.steps, 1)
+    if warm:
+        ob.advance(warm)
     t0 = time.perf_counter()
-    for s in range(steps):
-        m = (warm + s) % 3 + 1
-        ob.substep(m, 1 if m == 1 else 0)
+    ob.advance(steps)
     el = time.perf_counter() - t0
-    val = cfg.mpts * steps / el
-    sample = (f"{steps} RK3 substeps of the {cfg.nx}x{cfg.ny}x{cfg.nz} box "
-              f"(after {warm} warm-up), CPU port of rhsp/outflow_correction/pois")
+    ob.close()
+    val = cfg.mpts * 3 * steps / el
+    sample = (f"{steps} RK3 steps ({3 * steps} substeps) of the {cfg.nx}x{cfg.ny}x{cfg.nz} "
+              f"box after {warm} warm-up steps: the CPU port of rhsp/outflow_correction/pois "
+              f"(oracle/, OpenMP, {threads} threads of {cpu['nproc']} on {cpu['cpu_model']})")
     out = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": ws,
            "steps": steps, "warmup": warm, "ms_per_step": 1e3 * el / steps,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-           "data": "synthetic", "config": {"workload": f"rk3_substep {cfg.name} fp64",
-                                           "nx": cfg.nx, "ny": cfg.ny, "nz": cfg.nz},
+           "data": "synthetic", "config": workload_config(cfg, ws),
            "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port",
-                            "sample": sample},
-           "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+                            "sample": sample, **cpu},
+           "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+           "libraries_loaded": in_tree_libraries()}
     print(json.dumps(out), flush=True)
 
 
@@ -325,7 +382,8 @@ def run_mixed(cfg, init, coef, fbox, device, R, warm, K, fp64_ms_per_step):
     mbox.close()
     return {"value": value, "unit": UNIT, "ms_per_step": ms / K, "dtype": "f32 operators, f64 state",
             "speedup_vs_fp64": (fp64_ms_per_step / (ms / K)),
-            "substep_roofline": {"bytes_per_substep": ab["substep_mixed"], "manifest": MIXED_MANIFEST,
+            "substep_roofline": {"bytes_per_substep": ab["substep_mixed"],
+                                 "manifest": dict(MIXED_MANIFEST, passes_fp64_fp32=mixed_passes(cfg)),
                                  "achieved": ab["substep_mixed"] / sub_s / 1e9, "peak": peak,
                                  "unit": "GB/s", "frac": ab["substep_mixed"] / sub_s / 1e9 / peak,
                                  "peak_kind": peak_kind},
@@ -409,8 +467,10 @@ def main():
     sub_ms = ms / sub
     roofline = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                "peak_kind": peak_kind, "algorithmic_bytes_per_launch": ab.get(dom),
-                "launches_per_substep": launches_dom, "ms_per_substep": per_sub[dom]}
+                "peak_kind": peak_kind, "algorithmic_bytes_per_substep": ab.get(dom),
+                "algorithmic_bytes_per_launch": (ab[dom] / launches_dom) if dom in ab else None,
+                "launches_per_substep": launches_dom, "ms_per_substep": per_sub[dom],
+                "ms_per_launch": per_sub[dom] / launches_dom}
     substep_roofline = {"bytes_per_substep": ab["substep_survey"], "ms_per_substep": sub_ms,
                         "achieved": ab["substep_survey"] / (sub_ms / 1e3) / 1e9, "peak": peak,
                         "unit": "GB/s", "frac": ab["substep_survey"] / (sub_ms / 1e3) / 1e9 / peak,
@@ -466,10 +526,13 @@ def main():
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:
-            val, cores, secs = cpu_baseline(cfg, init, coef, 1)
+            val, cores, secs = cpu_baseline(cfg, init, 1)
+            hc = host_cpu()
             cpu = {"value": val, "unit": UNIT, "cores": cores, "kind": "port",
-                   "sample": f"1 RK3 substep of the {cfg.nx}x{cfg.ny}x{cfg.nz} box "
-                             f"({secs:.1f} s), CPU port of rhsp/outflow_correction/pois"}
+                   "sample": f"1 RK3 step (3 substeps) of the {cfg.nx}x{cfg.ny}x{cfg.nz} box "
+                             f"({secs:.1f} s), CPU port of rhsp/outflow_correction/pois "
+                             f"(oracle/, {cores} threads of {hc['nproc']} on {hc['cpu_model']})",
+                   **hc}
         except Exception as e:  # reported, never fatal for the GPU number
             cpu = {"value": None, "unit": UNIT, "cores": None, "kind": "port", "sample": f"failed: {e}"}
 
@@ -477,11 +540,7 @@ def main():
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K,
                "warmup": warm, "ms_per_step": ms / K, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-               "config": {"workload": f"rk3_substep {cfg.name} fp64", "nx": cfg.nx, "ny": cfg.ny,
-                          "nz": cfg.nz, "substeps_per_step": 3,
-                          "l2": "inputs larger than L2 (state %.1f GB per box)" % (
-                              sum(np.prod(box.shape(n)) for n in native.FIELDS) * 8 / 1e9),
-                          "parallelism": f"replicas{ws}", "autotuned_cta_sizes": list(tuned)},
+               "config": workload_config(cfg, ws), "autotuned_cta_sizes": list(tuned),
                "roofline": roofline, "substep_roofline": substep_roofline,
                "kernels_ms_per_substep": kernels,
                "kernels_note": "CUDA events around each kernel class in a separate profiled RK3 step "

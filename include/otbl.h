@@ -33,7 +33,9 @@ extern "C" {
 #define OTBL_ERR_CONFIG 2   /* inconsistent configuration                     */
 #define OTBL_ERR_OOM 3      /* device allocation failed                       */
 #define OTBL_ERR_CUDA 4     /* CUDA runtime error                             */
-#define OTBL_ERR_NAN 5      /* non-finite value detected by the dt reduction  */
+#define OTBL_ERR_NAN 5      /* non-finite value detected by the dt reduction,
+                               or genflu could not profile its rescaled grid
+                               (otbl_last_error tells which)                 */
 #define OTBL_ERR_NODEV 6    /* no CUDA device / extension not usable          */
 #define OTBL_BUSY 7         /* otbl_query / otbl_graph_query: work in flight  */
 #define OTBL_ERR_TIMEOUT 8  /* a bounded device-side wait gave up             */
@@ -51,16 +53,23 @@ extern "C" {
 
 /* arithmetic of the substep (no counterpart in the reference, which is FP64
  * throughout). OTBL_PREC_FP64: every operator in FP64. OTBL_PREC_MIXED: the
- * velocity (u, v, w), the RK3 combination, implzy, the Poisson solve, the
- * projection, dt, genflu and the energies stay FP64; the x and y mid-point
- * interpolations, d/dx of difvisxx, the spanwise FFTs and the nonlinear
- * products run in FP32, and the fifteen intermediate fields they exchange,
- * the pressure p and the RHS history rhs*pa are stored in FP32 (their
- * updates computed in FP64). otbl_set_field / otbl_get_field convert those
+ * velocity (u, v, w), the RK3 combination, implzy, the divergence, the
+ * Poisson solve of spanwise modes 0..3, the projection, dt, genflu and the
+ * energies stay FP64; the x and y mid-point interpolations, d/dx of
+ * difvisxx, the spanwise FFTs, the nonlinear products and the Poisson solve
+ * (x-DCTs and y-systems) of spanwise modes >= 4 run in FP32, and the fifteen
+ * intermediate fields they exchange, the pressure p and the RHS history
+ * rhs*pa are stored in FP32 (their updates computed in FP64). otbl_set_field / otbl_get_field convert those
  * fields from and to the caller's FP64 arrays; otbl_field_device_ptr refuses
  * them (OTBL_ERR_CONFIG). Not combined with OTBL_XPOSE_FP32. */
 #define OTBL_PREC_FP64 0
 #define OTBL_PREC_MIXED 1
+
+/* options (no counterpart in the reference). OTBL_OPT_YDENSE: on the mixed
+ * path, interpyy (lip.f90:359-440) runs as a dense ny x (ny+1) operator on
+ * the tensor cores (tcgen05, TF32 in three parts, FP32 accumulation) in
+ * place of the banded solve; needs OTBL_PREC_MIXED and ny <= 256. */
+#define OTBL_OPT_YDENSE 1
 
 typedef struct otbl_config {
   int nx, ny, nz;   /* grid (mod.F90:22); nz1 = 2*(nz/3), nz2 = nz1/2-1     */
@@ -71,7 +80,7 @@ typedef struct otbl_config {
   double y_blend;   /* height that replaces y(119) in genflu.F90:57        */
   double dt_fixed;  /* dt for OTBL_DT_FIXED; <= 0 freezes the first CFL dt */
   int precision;    /* OTBL_PREC_*                                         */
-  int reserved;     /* 0                                                   */
+  int options;      /* OTBL_OPT_* bits, 0 for none                         */
 } otbl_config;
 
 /* field ids for otbl_set_field / otbl_get_field / otbl_field_device_ptr */
@@ -147,9 +156,12 @@ int otbl_advance(otbl_ctx *ctx, int nsteps);
 int otbl_sync(otbl_ctx *ctx);
 
 /* ---- pieces of the path, on device buffers owned by the caller ---- */
-/* change.f90:224/257: planes (0:nz2, jee, nx) <-> pencils (nx, nz1*jee),
- * rounding to REAL4 when the context's xpose_round is OTBL_XPOSE_FP32 */
-int otbl_chp2x(otbl_ctx *ctx, const double *plan_dev, double *pen_dev, int jee);
+/* change.f90:224/257, in the reference's argument order chp2x(pen, plan,
+ * ...) and chx2p(pen, plan, ...): planes (0:nz2, jee, nx) -> pencils
+ * (nx, nz1*jee) and back, rounding to REAL4 when the context's xpose_round
+ * is OTBL_XPOSE_FP32 (the reference's buf and communicator arguments have no
+ * counterpart: one context holds the whole box) */
+int otbl_chp2x(otbl_ctx *ctx, double *pen_dev, const double *plan_dev, int jee);
 int otbl_chx2p(otbl_ctx *ctx, const double *pen_dev, double *plan_dev, int jee);
 /* ffts.f90:27 fourxz on nlines z-lines: iopt<0 r2c (phys -> fou, x 1/nz,
  * modes 0..nz2 kept); iopt>=0 c2r (fou -> phys, modes > nz2 zeroed).
@@ -161,6 +173,12 @@ int otbl_fourxz(otbl_ctx *ctx, double *fou_dev, double *phys_dev, int iopt,
  * iopt>=0 REDFT01 x 0.5 */
 int otbl_cosftx(otbl_ctx *ctx, double *c_dev, int nlines, int iopt);
 int otbl_boun(otbl_ctx *ctx);                        /* boun.f90:7         */
+/* lip.f90:359-440 interpyy of the context's u, w (u-type input) and v
+ * (v-type input), as rhsp calls it (rhsp.F90:146,367,393), with the
+ * context's operator (banded solve, or the dense tensor-core operator under
+ * OTBL_OPT_YDENSE); the three outputs (nx*ny*nz1 each, plane layout) are
+ * copied to the host as doubles. Synchronizes. */
+int otbl_interpyy(otbl_ctx *ctx, double *uy_host, double *wy_host, double *vy_host);
 int otbl_genflu(otbl_ctx *ctx);                      /* genflu.F90:3       */
 
 /* ---- genflu without allocation (no counterpart in the reference, whose
@@ -182,6 +200,12 @@ int otbl_genflu(otbl_ctx *ctx);                      /* genflu.F90:3       */
  * doubles in this library; larger grids are refused with OTBL_ERR_CONFIG.
  * The first call on each device looks up the array's address (and may load
  * the library's device module): make that call before any stream capture.
+ * The address is kept for the life of the process and belongs to the
+ * device's primary context, the one the CUDA runtime and every context of
+ * this library use (the call makes the context's device current with
+ * cudaSetDevice). A cudaDeviceReset destroys that context, and with it this
+ * address and every otbl_ctx's buffers: after a reset, reload the library
+ * before calling it again.
  * The scratch need not start at zero. All calls on one device share the
  * array: calls that can run at the same time (different streams, contexts or
  * host threads without ordering) race. No device or
@@ -192,11 +216,59 @@ enum {
   OTBL_GF_GAMMA1, OTBL_GF_GAMMA2,                              /* outputs */
   OTBL_GF_COUNT
 };
-#define OTBL_GENFLU_SCRATCH_MAX 2048 /* doubles (16 KiB) per device: ny <= 680 */
+/* doubles (16 KiB) per device. Admitted grids: ny <= 680, where the tables
+ * fit and genflu's shared memory stays within 48 KB; larger ny is refused
+ * with OTBL_ERR_CONFIG */
+#define OTBL_GENFLU_SCRATCH_MAX 2048
 int otbl_genflu_noalloc(otbl_ctx *ctx, double *u_dev, double *v_dev,
                         double *w_dev, const double *u0_dev,
                         const double *v0_dev, double *um_dev,
                         double *scal_dev, int *err_dev);
+
+/* ---- the reference's array surface: the state in the caller's device
+ *      arrays ----
+ * The reference's subroutines take the state as arguments (rhsp.F90:22-27,
+ * pois.f90:11, boun.f90:7,63, genflu.F90:3); these entry points take the
+ * caller's device arrays of the FP64 path in the plane layout of
+ * otbl_layout.h (u, w, rhsupa, rhswpa: nx*(ny+1)*nz1 doubles; v, p, rhsvpa:
+ * nx*ny*nz1), 16-byte aligned. The reference's twin arguments (ut and the
+ * pencil view of the same memory, res/rest, rhsut/rhsut work arrays, wki*,
+ * wkp, wkf, buffers) are one buffer each: a Fortran wrapper passes the
+ * state and drops the work arrays, which live in the context.
+ *
+ * otbl_bind_state points the context's seven state fields at the given
+ * arrays (NULL: the context's own array for that field) and keeps them
+ * bound for every later call on the context, until the next bind. It
+ * re-encodes the TMA descriptors that name the state on the host; it does
+ * not synchronize, and launches already issued keep the arrays they were
+ * given. A CUDA graph (otbl_graph_create) keeps the arrays bound when it was
+ * captured. The caller orders its own writes to the arrays before the call
+ * (see the ordering notes of INTEGRATION.md) and keeps them alive while
+ * bound. OTBL_ERR_CONFIG on the mixed-precision path, which stores p and the
+ * RHS history in FP32.
+ *
+ * Each *_arrays entry point binds the arrays it is given and runs the
+ * context entry point of the same name; with the same arrays bound, the
+ * results are bit for bit those of the context API. */
+int otbl_bind_state(otbl_ctx *ctx, double *u, double *v, double *w, double *p,
+                    double *rhsupa, double *rhsvpa, double *rhswpa);
+/* rhsp(ut,vt,wt,pt,rhsupat,rhsvpat,rhswpat, <work arrays>, dt, m, ...),
+ * rhsp.F90:22-27; dt and the step counters live in the context */
+int otbl_rhsp_arrays(otbl_ctx *ctx, double *u, double *v, double *w, double *p,
+                     double *rhsupa, double *rhsvpa, double *rhswpa, int m,
+                     int setstep);
+/* outflow_correction(ut,vt,rhsupat,communicator), boun.f90:63 */
+int otbl_outflow_correction_arrays(otbl_ctx *ctx, double *u, double *v,
+                                   double *rhsupa);
+/* pois(ut,vt,wt,pt,res,rest,rt,varstep,...), pois.f90:11; res/rest/rt are
+ * the context's scratch and varstep = 0.5/dt/rkdv(m) (bl_1.F90:117) */
+int otbl_pois_arrays(otbl_ctx *ctx, double *u, double *v, double *w, double *p,
+                     int m);
+/* boun(ut,vt,wt), boun.f90:7 */
+int otbl_boun_arrays(otbl_ctx *ctx, double *u, double *v, double *w);
+/* genflu(ut,vt,wt,y,re,dt,tiempo,...), genflu.F90:3; y, re, dt, tiempo and
+ * the genmod state live in the context */
+int otbl_genflu_arrays(otbl_ctx *ctx, double *u, double *v, double *w);
 
 /* kernel launches issued by this context since creation */
 long long otbl_launch_count(const otbl_ctx *ctx);

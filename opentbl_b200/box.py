@@ -190,11 +190,20 @@ class Box:
     def genflu(self):
         self._check(self.L.otbl_genflu(self.h), "otbl_genflu")
 
+    def interpyy(self):
+        """lip.f90:359-440 on the state's u, w, v: (uy, wy, vy), ny rows each."""
+        shp = (self.cfg.nx, self.cfg.ny, self.cfg.nz1)
+        out = [np.zeros(shp) for _ in range(3)]
+        self._check(self.L.otbl_interpyy(self.h, *[native.dptr(a) for a in out]), "otbl_interpyy")
+        return tuple(out)
+
     # device-buffer pieces (pointers are raw device addresses)
-    def chp2x(self, plan_dev: int, pen_dev: int, jee: int):
-        self._check(self.L.otbl_chp2x(self.h, plan_dev, pen_dev, jee), "otbl_chp2x")
+    def chp2x(self, pen_dev: int, plan_dev: int, jee: int):
+        """change.f90:224 chp2x(pen, plan, ...): planes -> pencils."""
+        self._check(self.L.otbl_chp2x(self.h, pen_dev, plan_dev, jee), "otbl_chp2x")
 
     def chx2p(self, pen_dev: int, plan_dev: int, jee: int):
+        """change.f90:257 chx2p(pen, plan, ...): pencils -> planes."""
         self._check(self.L.otbl_chx2p(self.h, pen_dev, plan_dev, jee), "otbl_chx2p")
 
     def fourxz(self, fou_dev: int, phys_dev: int, iopt: int, nlines: int):
@@ -202,6 +211,41 @@ class Box:
 
     def cosftx(self, c_dev: int, nlines: int, iopt: int):
         self._check(self.L.otbl_cosftx(self.h, c_dev, nlines, iopt), "otbl_cosftx")
+
+    # ---- the reference's array surface (caller-owned device arrays, FP64) ----
+    def _ptrs(self, arrays: dict, names):
+        return [ctypes.c_void_p(int(arrays[n])) if arrays.get(n) else None for n in names]
+
+    def bind_state(self, arrays: dict | None = None):
+        """Points the state at caller-owned device arrays {field name: device
+        address}; fields not given go back to the context's own arrays."""
+        p = self._ptrs(arrays or {}, FIELDS)
+        self._check(self.L.otbl_bind_state(self.h, *p), "otbl_bind_state")
+
+    def rhsp_arrays(self, arrays: dict, m: int, setstep: bool):
+        """rhsp(ut,vt,wt,pt,rhsupat,rhsvpat,rhswpat,...), rhsp.F90:22-27."""
+        self._check(self.L.otbl_rhsp_arrays(self.h, *self._ptrs(arrays, FIELDS), m, int(setstep)),
+                    "otbl_rhsp_arrays")
+
+    def outflow_correction_arrays(self, arrays: dict):
+        """outflow_correction(ut,vt,rhsupat,...), boun.f90:63."""
+        self._check(self.L.otbl_outflow_correction_arrays(
+            self.h, *self._ptrs(arrays, ("u", "v", "rhsupa"))), "otbl_outflow_correction_arrays")
+
+    def pois_arrays(self, arrays: dict, m: int):
+        """pois(ut,vt,wt,pt,res,rest,rt,varstep,...), pois.f90:11."""
+        self._check(self.L.otbl_pois_arrays(self.h, *self._ptrs(arrays, ("u", "v", "w", "p")), m),
+                    "otbl_pois_arrays")
+
+    def boun_arrays(self, arrays: dict):
+        """boun(ut,vt,wt), boun.f90:7."""
+        self._check(self.L.otbl_boun_arrays(self.h, *self._ptrs(arrays, ("u", "v", "w"))),
+                    "otbl_boun_arrays")
+
+    def genflu_arrays(self, arrays: dict):
+        """genflu(ut,vt,wt,...), genflu.F90:3."""
+        self._check(self.L.otbl_genflu_arrays(self.h, *self._ptrs(arrays, ("u", "v", "w"))),
+                    "otbl_genflu_arrays")
 
     def close(self):
         if getattr(self, "h", None) is not None and self.h.value:

@@ -16,7 +16,9 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libotbl.so")
-SOURCES = ["kernels.cu", "k_xlines.cu", "k_ylines.cu", "otbl_capi.cu", "otbl_graph.cu", "coef.cpp"]
+DRIVER = os.path.join(HERE, "otbl_driver")
+SOURCES = ["kernels.cu", "k_xlines.cu", "k_ylines.cu", "k_ydense.cu", "otbl_capi.cu", "otbl_graph.cu",
+           "coef.cpp"]
 HEADERS = ["otbl_internal.cuh", "fft.cuh", "devcommon.cuh", "tma.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -35,10 +37,10 @@ def host_compiler() -> list[str]:
 
 
 def stale() -> bool:
-    if not os.path.exists(LIB):
+    if not os.path.exists(LIB) or not os.path.exists(DRIVER):
         return True
     t = os.path.getmtime(LIB)
-    deps = [os.path.join(CSRC, s) for s in SOURCES + HEADERS]
+    deps = [os.path.join(CSRC, s) for s in SOURCES + HEADERS + ["otbl_driver.c"]]
     deps += [os.path.join(HERE, "..", "include", h) for h in ("otbl.h", "otbl_layout.h")]
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
@@ -59,7 +61,21 @@ def build(force: bool = False, verbose: bool = False) -> str:
         raise RuntimeError("nvcc failed building libotbl.so")
     if verbose:
         sys.stderr.write(r.stderr)
+    build_driver()
     return LIB
+
+
+def build_driver() -> str:
+    """The C program csrc/otbl_driver.c, linked against libotbl.so alone
+    (it finds the library next to itself at run time)."""
+    cc = "/usr/bin/gcc" if os.path.exists("/usr/bin/gcc") else (shutil.which("gcc") or "cc")
+    cmd = [cc, "-O2", "-std=c11", "-Wall", "-o", DRIVER, os.path.join(CSRC, "otbl_driver.c"),
+           "-L" + HERE, "-lotbl", "-Wl,-rpath,$ORIGIN", "-lm"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("gcc failed building otbl_driver")
+    return DRIVER
 
 
 if __name__ == "__main__":

@@ -30,6 +30,7 @@ class BoxConfig:
     dt_mode: int = 0                   # 0 adaptive (reference), 1 fixed
     dt_fixed: float = 0.0
     precision: int = 0                 # 0 FP64, 1 mixed (OTBL_PREC_*)
+    options: int = 0                   # OTBL_OPT_* bits (1: interpyy on the tensor cores)
     amp: float = 0.05                  # perturbation amplitude / U_inf
     seed: int = 1234
     name: str = ""

@@ -254,6 +254,9 @@ extern "C" int otbl_config_check(const otbl_config *cfg) {
   if (cfg->dt_mode != 0 && cfg->dt_mode != 1) return OTBL_ERR_CONFIG;
   if (cfg->precision != OTBL_PREC_FP64 && cfg->precision != OTBL_PREC_MIXED) return OTBL_ERR_CONFIG;
   if (cfg->precision == OTBL_PREC_MIXED && cfg->xpose_round != 0) return OTBL_ERR_CONFIG;
+  if (cfg->options & ~OTBL_OPT_YDENSE) return OTBL_ERR_CONFIG;
+  if ((cfg->options & OTBL_OPT_YDENSE) && (cfg->precision != OTBL_PREC_MIXED || cfg->ny > 256))
+    return OTBL_ERR_CONFIG;
   return OTBL_OK;
 }
 

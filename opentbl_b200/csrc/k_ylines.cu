@@ -931,28 +931,32 @@ __global__ void k_pois_lu(DCoef c, double *dinv) {
 // The solve in place on phi rows 0..ny-2 of planes 2..nx, one thread per
 // column: y_r = rhs_r + l_r y_{r-1}, l_r = -ayp(1,r+1) dinv(r-1); then
 // x_r = (y_r - ayp(3,r+1) x_{r+1}) dinv(r). The singular (i = 2, k = 0)
-// system has its last row zeroed first (pois.f90:111-114).
-__global__ void __launch_bounds__(128) k_pois_solve(DCoef c, double *phi, const double *__restrict__ dinv,
-                                                    double *ckbuf) {
+// system has its last row zeroed first (pois.f90:111-114). The launch takes
+// the columns kr0 <= kr < kr0 + nkr of every plane, in T (FP64, or FP32 for
+// the higher spanwise modes of the mixed path, with FP32 coefficients and
+// pivots); phi and the checkpoints hold T.
+template <typename T>
+__global__ void __launch_bounds__(128) k_pois_solve(DCoefT<T> c, T *phi, const T *__restrict__ dinv, T *ckbuf,
+                                                    int kr0, int nkr) {
   const int ny = c.ny, ny1 = ny - 1, nz1 = c.nz1, nm = c.nz2 + 1;
-  const int ncol = (c.nx - 1) * nz1;
+  const int ncol = (c.nx - 1) * nkr;
   const int col = blockIdx.x * blockDim.x + threadIdx.x;
   if (col >= ncol) return;
-  const int i = col / nz1 + 2, kr = col - (i - 2) * nz1, k = kr >> 1;
+  const int i = col / nkr + 2, kr = kr0 + (col - (i - 2) * nkr), k = kr >> 1;
   const size_t S = nz1;
-  double *x = phi + (size_t)(i - 1) * ny * nz1 + kr;
-  const double *dv = dinv + (size_t)(i - 1) * ny * nm + k;
-  double *ck = ckbuf + col;
-  const double *ayp = c.ayp;
+  T *x = phi + (size_t)(i - 1) * ny * nz1 + kr;
+  const T *dv = dinv + (size_t)(i - 1) * ny * nm + k;
+  T *ck = ckbuf + col;
+  const T *ayp = c.ayp;
   const bool sing = i == 2 && k == 0;
-  auto X = [&](int r) { return (sing && r == ny1 - 1) ? 0.0 : x[(size_t)min(r, ny1 - 1) * S]; };
+  auto X = [&](int r) { return (sing && r == ny1 - 1) ? (T)0 : x[(size_t)min(r, ny1 - 1) * S]; };
   auto D = [&](int r) { return __ldg(dv + (size_t)min(max(r, 0), ny1 - 1) * nm); };
   const int nseg = (ny1 + KY - 1) / KY;
-  double y = 0.0;
+  T y = 0;
   for (int sg = 0; sg < nseg; ++sg) {
     const int s0 = sg * KY;
     ck[(size_t)sg * ncol] = y;
-    double bv[KY], dp[KY + 1];
+    T bv[KY], dp[KY + 1];
 #pragma unroll
     for (int b = 0; b < KY; ++b) bv[b] = X(s0 + b);
 #pragma unroll
@@ -960,29 +964,29 @@ __global__ void __launch_bounds__(128) k_pois_solve(DCoef c, double *phi, const 
 #pragma unroll
     for (int b = 0; b < KY; ++b) {
       const int r = s0 + b;
-      if (r < ny1) y = bv[b] + (r > 0 ? -A3(ayp, 1, r + 1) * dp[b] : 0.0) * y;
+      if (r < ny1) y = bv[b] + (r > 0 ? -A3(ayp, 1, r + 1) * dp[b] : (T)0) * y;
     }
   }
-  double xn = 0.0;
+  T xn = 0;
   for (int sg = nseg - 1; sg >= 0; --sg) {
     const int s0 = sg * KY;
-    double bv[KY], dp[KY + 1], yv[KY];
+    T bv[KY], dp[KY + 1], yv[KY];
 #pragma unroll
     for (int b = 0; b < KY; ++b) bv[b] = X(s0 + b);
 #pragma unroll
     for (int b = 0; b <= KY; ++b) dp[b] = D(s0 + b - 1);
-    double yy = ck[(size_t)sg * ncol];
+    T yy = ck[(size_t)sg * ncol];
 #pragma unroll
     for (int b = 0; b < KY; ++b) {
       const int r = s0 + b;
-      if (r < ny1) yy = bv[b] + (r > 0 ? -A3(ayp, 1, r + 1) * dp[b] : 0.0) * yy;
+      if (r < ny1) yy = bv[b] + (r > 0 ? -A3(ayp, 1, r + 1) * dp[b] : (T)0) * yy;
       yv[b] = yy;
     }
 #pragma unroll
     for (int b = KY - 1; b >= 0; --b) {
       const int r = s0 + b;
       if (r < ny1) {
-        xn = (yv[b] - (r < ny1 - 1 ? A3(ayp, 3, r + 1) : 0.0) * xn) * dp[b + 1];
+        xn = (yv[b] - (r < ny1 - 1 ? A3(ayp, 3, r + 1) : (T)0) * xn) * dp[b + 1];
         x[(size_t)r * S] = xn;
       }
     }
@@ -1023,6 +1027,11 @@ cudaError_t launch_interpy(otbl_ctx *c) {
   }
   const int ncol = c->cfg.nx * c->dc.nz1;
   prof_begin(c, PK_INTERPY);
+  if (c->ydense) {
+    const cudaError_t e = launch_interpy_dense(c);
+    prof_end(c);
+    return e;
+  }
   const int bs = c->tune_bs[2];
   if (c->ymaps_ok) {
     const dim3 gt((c->dc.nz1 + 127) / 128, c->cfg.nx, 3);
@@ -1314,15 +1323,29 @@ cudaError_t launch_pois_lu(otbl_ctx *c) {
   dim3 g((c->dc.nz2 + 1 + 127) / 128, c->cfg.nx - 1);
   k_pois_lu<<<g, 128, 0, c->stream>>>(c->dc, c->w.pois_dinv);
   c->launches += 1;
+  if (c->mixed) {
+    const size_t n = (size_t)c->cfg.nx * c->cfg.ny * (c->dc.nz1 / 2);
+    const cudaError_t e = launch_round_f32(c, c->w.pois_dinv, c->w.pois_dinvf, n);
+    if (e != cudaSuccess) return e;
+  }
   return cudaGetLastError();
 }
 
-cudaError_t launch_pois_solve(otbl_ctx *c, double *phi) {
-  const int ncol = (c->cfg.nx - 1) * c->dc.nz1;
-  prof_begin(c, PK_POIS_SOLVE);
-  k_pois_solve<<<(ncol + 127) / 128, 128, 0, c->stream>>>(c->dc, phi, c->w.pois_dinv, c->w.s1);
-  prof_end(c);
+// columns kr0 <= kr < kr0 + nkr of every plane; phi holds T
+template <typename T>
+static void pois_solve_t(otbl_ctx *c, const DCoefT<T> &dc, T *phi, const T *dinv, int kr0, int nkr) {
+  const int ncol = (c->cfg.nx - 1) * nkr;
+  k_pois_solve<T><<<(ncol + 127) / 128, 128, 0, c->stream>>>(dc, phi, dinv, reinterpret_cast<T *>(c->w.s1), kr0,
+                                                            nkr);
   c->launches += 1;
+}
+
+cudaError_t launch_pois_solve(otbl_ctx *c, double *phi64, float *phi32, int kr_split) {
+  const int nz1 = c->dc.nz1;
+  prof_begin(c, PK_POIS_SOLVE);
+  if (kr_split > 0) pois_solve_t<double>(c, c->dc, phi64, c->w.pois_dinv, 0, kr_split);
+  if (kr_split < nz1) pois_solve_t<float>(c, c->dcf, phi32, c->w.pois_dinvf, kr_split, nz1 - kr_split);
+  prof_end(c);
   return cudaGetLastError();
 }
 

@@ -26,6 +26,8 @@
 // exactly the loads/stores where the reference transposes.
 #include <cfloat>
 #include <mutex>
+#include <algorithm>
+#include <type_traits>
 
 #include "devcommon.cuh"
 #include "fft.cuh"
@@ -633,13 +635,10 @@ struct GenArgs {
   // scalars: inputs dt, tiempo, timeinit; outputs of genflu.F90:67-93
   const double *dt, *tiempo, *timeinit;
   double *timec, *utauout, *rthout, *dout, *gamma1, *gamma2;
-  int *err;  // set to OTBL_ERR_NAN for a degenerate rescaled grid; may be null
+  int *err;       // set to err_code for a degenerate rescaled grid; may be null
+  int err_code;   // OTBL_DEVERR_GENFLU_GRID (context flag) or OTBL_ERR_NAN
   int tail;
 };
-
-size_t genflu_smem_bytes(int ny) {
-  return sizeof(double) * (6 * (size_t)(ny + 1) + (ny + 2)) + sizeof(int) * 4 * (size_t)(ny + 1) + 64;
-}
 
 __global__ void __launch_bounds__(256) k_genflu_tab(DCoef c, GenArgs a) {
   extern __shared__ double gsm[];
@@ -852,7 +851,7 @@ __global__ void __launch_bounds__(128) k_genflu_cols(DCoef c, GenArgs a) {
     const int kll = max(kl[i], 1);
     return (inp(kll) * fsca[i] + inp(kll - 1) * (1 - fsca[i])) * ggg;
   };
-  if (kr == 2 && comp == 0 && r == 0 && !prof && a.err) atomicCAS(a.err, 0, OTBL_ERR_NAN);
+  if (kr == 2 && comp == 0 && r == 0 && !prof && a.err) atomicCAS(a.err, 0, a.err_code);
   double v;
   if (!a.tail) {
     v = val(r);
@@ -951,11 +950,13 @@ __global__ void __launch_bounds__(256) k_outflow(DCoef c, double *u, const doubl
 // ---------------------------------------------------------------------------
 // pois (pois.f90:11-189)
 // ---------------------------------------------------------------------------
-struct XTab {
-  const double2 *tw;   // exp(-2 pi i t/n), t < n
-  const double2 *tw2;  // exp(-i pi t/(2n)), t < n
+template <typename T>
+struct XTabT {
+  const V2<T> *tw;   // exp(-2 pi i t/n), t < n
+  const V2<T> *tw2;  // exp(-i pi t/(2n)), t < n
   int n;
 };
+using XTab = XTabT<double>;
 
 // The x-line transforms of pois: MB spanwise modes of one row j per CTA of
 // 256 threads. The loads and stores walk the planes with the MB modes of a
@@ -967,22 +968,29 @@ struct XTab {
 
 // divergence (pois.f90:41-54) + DCT-II along x (cosftx iopt=-1); output
 // phi-hat in plane layout (v-type, plane i = x-mode index + 2). Mode 0 made
-// real (pois.f90:102).
-template <int MB, int NT>
-__global__ void __launch_bounds__(NT) k_pois_fwd(DCoef c, XTab x, const double *__restrict__ u,
+// real (pois.f90:102). The launch covers spanwise modes kbeg..kend, MB per
+// CTA; T is the transform's arithmetic and phi's element type (FP64, or FP32
+// for the higher modes of the mixed path). The divergence itself is formed
+// in FP64 from the FP64 velocity.
+template <typename T, int MB, int NT>
+__global__ void __launch_bounds__(NT) k_pois_fwd(DCoef c, XTabT<T> x, const double *__restrict__ u,
                                                  const double *__restrict__ v, const double *__restrict__ w,
-                                                 double *__restrict__ phi) {
-  extern __shared__ double2 xsm[];
-  const int n = x.n, ld = xpad(n) | 1, ny = c.ny, nz1 = c.nz1, nz2 = c.nz2, xr = c.xround;
+                                                 T *__restrict__ phi, int kbeg, int kend) {
+  using V = V2<T>;
+  extern __shared__ __align__(16) unsigned char xsm_raw[];
+  V *xsm = reinterpret_cast<V *>(xsm_raw);
+  const int n = x.n, ld = xpad(n) | 1, ny = c.ny, nz1 = c.nz1, xr = c.xround;
   const int j = blockIdx.y + 1;
-  const int k0 = blockIdx.x * MB;
+  const int k0 = kbeg + blockIdx.x * MB;
   const size_t PU = (size_t)(ny + 1) * nz1, PV = (size_t)ny * nz1;
   const double idx = c.S[OTBL_S_IDX], idy = c.idy[j];
   for (int e = threadIdx.x; e < n * MB; e += NT) {
     const int l = e % MB, tt = e / MB;
     const int k = k0 + l;
-    double2 val = make_double2(0.0, 0.0);
-    if (k <= nz2) {
+    V val;
+    val.x = 0;
+    val.y = 0;
+    if (k <= kend) {
       const int i = tt + 2;
       const double kz = c.kaz[k];
       const double2 wv = *reinterpret_cast<const double2 *>(w + (size_t)(i - 1) * PU + (size_t)j * nz1 + 2 * k);
@@ -994,7 +1002,8 @@ __global__ void __launch_bounds__(NT) k_pois_fwd(DCoef c, XTab x, const double *
       double im = kz * wv.x + (v1.y - v0.y) * idy;
       re = re + idx * (ua.x - ub.x);
       im = im + idx * (ua.y - ub.y);
-      val = make_double2(rnd(re, xr), rnd(im, xr));
+      val.x = (T)rnd(re, xr);
+      val.y = (T)rnd(im, xr);
     }
     const int dst = (tt & 1) ? n - 1 - (tt >> 1) : (tt >> 1);
     xsm[l * ld + xpad(dst)] = val;
@@ -1004,43 +1013,52 @@ __global__ void __launch_bounds__(NT) k_pois_fwd(DCoef c, XTab x, const double *
     const int G = NT / MB, l = threadIdx.x / G;
     block_fft_lines<-1, NT>(xsm + l * ld, n, x.tw, threadIdx.x % G, G);
   }
-  const double dnf = 1.0 / (double)n;
+  const T dnf = (T)(1.0 / (double)n);
   for (int e = threadIdx.x; e < n * MB; e += NT) {
     const int l = e % MB, kk = e / MB;
     const int k = k0 + l;
-    if (k > nz2) continue;
-    const double2 V = xsm[l * ld + xpad(kk)], Vm = xsm[l * ld + xpad(kk == 0 ? 0 : n - kk)];
-    const double2 wq = __ldg(x.tw2 + kk);
-    const double2 y = cadd(cmul(wq, V), cmul(cconj(wq), Vm));
-    double re = rnd(dnf * y.x, xr), im = rnd(dnf * y.y, xr);
-    if (k == 0) im = 0.0;
-    *reinterpret_cast<double2 *>(phi + (size_t)(kk + 1) * PV + (size_t)(j - 1) * nz1 + 2 * k) =
-        make_double2(re, im);
+    if (k > kend) continue;
+    const V Vv = xsm[l * ld + xpad(kk)], Vm = xsm[l * ld + xpad(kk == 0 ? 0 : n - kk)];
+    const V wq = __ldg(x.tw2 + kk);
+    const V y = cadd(cmul(wq, Vv), cmul(cconj(wq), Vm));
+    V out;
+    out.x = (T)rnd((double)(dnf * y.x), xr);
+    out.y = k == 0 ? (T)0 : (T)rnd((double)(dnf * y.y), xr);
+    *reinterpret_cast<V *>(phi + (size_t)(kk + 1) * PV + (size_t)(j - 1) * nz1 + 2 * k) = out;
   }
 }
 
-// DCT-III along x (cosftx iopt=+1), in place on phi-hat
-template <int MB, int NT>
-__global__ void __launch_bounds__(NT) k_pois_bwd(DCoef c, XTab x, double *__restrict__ phi) {
-  extern __shared__ double2 xsm[];
-  const int n = x.n, ld = xpad(n) | 1, ny = c.ny, nz1 = c.nz1, nz2 = c.nz2, xr = c.xround;
+// DCT-III along x (cosftx iopt=+1), in place on phi-hat, modes kbeg..kend
+template <typename T, int MB, int NT>
+__global__ void __launch_bounds__(NT) k_pois_bwd(DCoef c, XTabT<T> x, T *__restrict__ phi, int kbeg, int kend) {
+  using V = V2<T>;
+  extern __shared__ __align__(16) unsigned char xsm_raw[];
+  V *xsm = reinterpret_cast<V *>(xsm_raw);
+  const int n = x.n, ld = xpad(n) | 1, ny = c.ny, nz1 = c.nz1, xr = c.xround;
   const int j = blockIdx.y + 1;
-  const int k0 = blockIdx.x * MB;
+  const int k0 = kbeg + blockIdx.x * MB;
   const size_t PV = (size_t)ny * nz1;
   for (int e = threadIdx.x; e < n * MB; e += NT) {
     const int l = e % MB, kk = e / MB;
     const int k = k0 + l;
-    double2 val = make_double2(0.0, 0.0);
-    if (k <= nz2) {
-      const double2 q = *reinterpret_cast<const double2 *>(phi + (size_t)(kk + 1) * PV + (size_t)(j - 1) * nz1 + 2 * k);
-      const double2 Y = make_double2(rnd(q.x, xr), rnd(q.y, xr));
-      double2 Ym = make_double2(0.0, 0.0);
+    V val;
+    val.x = 0;
+    val.y = 0;
+    if (k <= kend) {
+      const V q = *reinterpret_cast<const V *>(phi + (size_t)(kk + 1) * PV + (size_t)(j - 1) * nz1 + 2 * k);
+      V Y, Ym;
+      Y.x = (T)rnd((double)q.x, xr);
+      Y.y = (T)rnd((double)q.y, xr);
+      Ym.x = 0;
+      Ym.y = 0;
       if (kk > 0) {
-        const double2 qm =
-            *reinterpret_cast<const double2 *>(phi + (size_t)(n - kk + 1) * PV + (size_t)(j - 1) * nz1 + 2 * k);
-        Ym = make_double2(rnd(qm.x, xr), rnd(qm.y, xr));
+        const V qm = *reinterpret_cast<const V *>(phi + (size_t)(n - kk + 1) * PV + (size_t)(j - 1) * nz1 + 2 * k);
+        Ym.x = (T)rnd((double)qm.x, xr);
+        Ym.y = (T)rnd((double)qm.y, xr);
       }
-      const double2 d = make_double2(Y.x + Ym.y, Y.y - Ym.x);  // Y - i Ym
+      V d;  // Y - i Ym
+      d.x = Y.x + Ym.y;
+      d.y = Y.y - Ym.x;
       val = cmul(cconj(__ldg(x.tw2 + kk)), d);
     }
     xsm[l * ld + xpad(kk)] = val;
@@ -1053,20 +1071,25 @@ __global__ void __launch_bounds__(NT) k_pois_bwd(DCoef c, XTab x, double *__rest
   for (int e = threadIdx.x; e < n * MB; e += NT) {
     const int l = e % MB, tt = e / MB;
     const int k = k0 + l;
-    if (k > nz2) continue;
-    const double2 V = xsm[l * ld + xpad((tt & 1) ? n - 1 - (tt >> 1) : (tt >> 1))];
+    if (k > kend) continue;
+    const V Vv = xsm[l * ld + xpad((tt & 1) ? n - 1 - (tt >> 1) : (tt >> 1))];
     // mode 0 is real (pois.f90:102): its imaginary pencil is identically zero
     // in the reference's real transforms, while the complex line transform
     // used here leaves rounding-level values there
-    *reinterpret_cast<double2 *>(phi + (size_t)(tt + 1) * PV + (size_t)(j - 1) * nz1 + 2 * k) =
-        make_double2(rnd(0.5 * V.x, xr), k == 0 ? 0.0 : rnd(0.5 * V.y, xr));
+    V out;
+    out.x = (T)rnd((double)((T)0.5 * Vv.x), xr);
+    out.y = k == 0 ? (T)0 : (T)rnd((double)((T)0.5 * Vv.y), xr);
+    *reinterpret_cast<V *>(phi + (size_t)(tt + 1) * PV + (size_t)(j - 1) * nz1 + 2 * k) = out;
   }
 }
 
-// projection, pois.f90:144-162; one thread per (i >= 2, j, kr)
+// projection, pois.f90:144-162; one thread per (i >= 2, j, kr). phi holds
+// the columns kr < kr_split in FP64 (phi64) and the others in FP32 (phi32,
+// the mixed path's higher spanwise modes); the update is FP64.
 template <typename TP>
-__global__ void __launch_bounds__(128) k_project(DCoef c, const DState *st, const double *__restrict__ phi,
-                                                 double *u, double *v, double *w, TP *p) {
+__global__ void __launch_bounds__(128) k_project(DCoef c, const DState *st, const double *__restrict__ phi64,
+                                                 const float *__restrict__ phi32, int kr_split, double *u,
+                                                 double *v, double *w, TP *p) {
   const int kr = blockIdx.x * blockDim.x + threadIdx.x;
   if (kr >= c.nz1) return;
   const int j = blockIdx.y + 1, i = blockIdx.z + 2;
@@ -1074,23 +1097,25 @@ __global__ void __launch_bounds__(128) k_project(DCoef c, const DState *st, cons
   const size_t PU = (size_t)(ny + 1) * nz1, PV = (size_t)ny * nz1;
   const int k = kr >> 1, odd = kr & 1, pof = odd ? -1 : 1;
   const double kz = c.kaz[k];
-  const double *f = phi + (size_t)(i - 1) * PV + kr;  // phi(j, i) at f[(j-1)*nz1]
+  const size_t base = (size_t)(i - 1) * PV + kr;  // phi(j, i) at base + (j-1)*nz1
+  const bool lo = kr < kr_split;                  // kr and kr + pof are one mode
+  auto F = [&](long off) { return lo ? phi64[(long)base + off] : (double)phi32[(long)base + off]; };
   if (j >= 2) {
-    const double fm = f[(size_t)(j - 2) * nz1];
+    const double fm = F((long)(j - 2) * nz1);
     TP *pq = p + (size_t)(i - 1) * PV + (size_t)(j - 1) * nz1 + kr;
     *pq = (TP)(st->varstep * fm + (double)*pq);
-    const double q = f[(size_t)(j - 2) * nz1 + pof];
+    const double q = F((long)(j - 2) * nz1 + pof);
     const double kf = odd ? kz * q : -kz * q;
     double *wq = w + (size_t)(i - 1) * PU + (size_t)(j - 1) * nz1 + kr;
     *wq = *wq - kf;
   }
   if (j >= 2 && j <= ny - 1) {
     double *vq = v + (size_t)(i - 1) * PV + (size_t)(j - 1) * nz1 + kr;
-    *vq = *vq - c.idyy[j - 1] * (f[(size_t)(j - 1) * nz1] - f[(size_t)(j - 2) * nz1]);
+    *vq = *vq - c.idyy[j - 1] * (F((long)(j - 1) * nz1) - F((long)(j - 2) * nz1));
   }
   if (j <= ny - 1 && i <= nx - 1) {
     double *uq = u + (size_t)(i - 1) * PU + (size_t)j * nz1 + kr;
-    *uq = *uq - c.S[OTBL_S_IDXX] * (f[PV + (size_t)(j - 1) * nz1] - f[(size_t)(j - 1) * nz1]);
+    *uq = *uq - c.S[OTBL_S_IDXX] * (F((long)PV + (long)(j - 1) * nz1) - F((long)(j - 1) * nz1));
   }
 }
 
@@ -1206,6 +1231,12 @@ __global__ void k_round_f32(const double *in, float *out, int n) {
   if (t < n) out[t] = (float)in[t];
 }
 
+cudaError_t launch_round_f32(otbl_ctx *c, const double *in, float *out, size_t n) {
+  k_round_f32<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(in, out, (int)n);
+  c->launches += 1;
+  return cudaGetLastError();
+}
+
 // ---------------------------------------------------------------------------
 // launch wrappers
 // ---------------------------------------------------------------------------
@@ -1256,6 +1287,13 @@ static inline XTab xtab(otbl_ctx *c) {
   x.n = c->cfg.nx - 1;
   return x;
 }
+static inline XTabT<float> xtabf(otbl_ctx *c) {
+  XTabT<float> x;
+  x.tw = reinterpret_cast<const float2 *>(c->w.twxf);
+  x.tw2 = reinterpret_cast<const float2 *>(c->w.twx2f);
+  x.n = c->cfg.nx - 1;
+  return x;
+}
 
 cudaError_t launch_twiddles(otbl_ctx *c) {
   const int M = c->cfg.nz / 2, n = c->cfg.nx - 1;
@@ -1267,7 +1305,9 @@ cudaError_t launch_twiddles(otbl_ctx *c) {
   if (c->mixed) {
     k_round_f32<<<(2 * M + 255) / 256, 256, 0, c->stream>>>(c->w.twz, c->w.twzf, 2 * M);
     k_round_f32<<<(2 * M + 255) / 256, 256, 0, c->stream>>>(c->w.twz2, c->w.twz2f, 2 * M);
-    c->launches += 2;
+    k_round_f32<<<(2 * n + 255) / 256, 256, 0, c->stream>>>(c->w.twx, c->w.twxf, 2 * n);
+    k_round_f32<<<(2 * n + 255) / 256, 256, 0, c->stream>>>(c->w.twx2, c->w.twx2f, 2 * n);
+    c->launches += 4;
   }
   return cudaGetLastError();
 }
@@ -1375,6 +1415,7 @@ cudaError_t launch_genflu(otbl_ctx *c, int tail) {
   a.gamma1 = &st->gamma1;
   a.gamma2 = &st->gamma2;
   a.err = &st->err;
+  a.err_code = OTBL_DEVERR_GENFLU_GRID;
   a.tail = tail;
   prof_begin(c, PK_GENFLU);
   const cudaError_t e = genflu_launch(c, a);
@@ -1442,6 +1483,7 @@ cudaError_t launch_genflu_noalloc(otbl_ctx *c, double *wk, double *u, double *v,
   a.gamma1 = scal + OTBL_GF_GAMMA1;
   a.gamma2 = scal + OTBL_GF_GAMMA2;
   a.err = err;
+  a.err_code = OTBL_ERR_NAN;
   a.tail = 0;
   return genflu_launch(c, a);
 }
@@ -1458,58 +1500,77 @@ cudaError_t launch_outflow(otbl_ctx *c) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_pois(otbl_ctx *c, int m) {
-  (void)m;  // varstep for substep m was set by k_dt
-  const int nz2 = c->dc.nz2, ny = c->cfg.ny, nx = c->cfg.nx, nz1 = c->dc.nz1;
-  const int n = nx - 1;
+// One x-DCT pass (forward: divergence + DCT-II; backward: DCT-III) over the
+// spanwise modes kbeg..kend in T, MB modes per CTA.
+template <typename T>
+static void pois_xdct(otbl_ctx *c, bool fwd, T *phi, int kbeg, int kend) {
+  if (kend < kbeg) return;
+  const int ny = c->cfg.ny, n = c->cfg.nx - 1;
   // modes per CTA: n * MB <= 4096 and at most 8
   const int MB = n <= 512 ? 8 : (n <= 1024 ? 4 : (n <= 2048 ? 2 : 1));
-  const size_t smem = (size_t)MB * (xpad_host(n) | 1) * sizeof(double2);
-  double *phi = c->w.s2;
-  dim3 gx((nz2 + 1 + MB - 1) / MB, ny - 1);
+  const size_t smem = (size_t)MB * (xpad_host(n) | 1) * sizeof(V2<T>);
+  const dim3 gx((kend - kbeg + 1 + MB - 1) / MB, ny - 1);
   // threads per CTA: 512 when the CTA holds 2048-4096 points (fewer items
   // and registers per thread, the same barriers), else 256
   const int NT = n * MB >= 2048 ? POIS_NT_BIG : 256;
-  auto fwd = [&](auto kf) {
-    cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    kf<<<gx, NT, smem, c->stream>>>(c->dc, xtab(c), c->f[OTBL_F_U], c->f[OTBL_F_V], c->f[OTBL_F_W], phi);
-  };
-  auto bwd = [&](auto kb) {
-    cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    kb<<<gx, NT, smem, c->stream>>>(c->dc, xtab(c), phi);
-  };
-  prof_begin(c, PK_POIS_FWD);
-  if (MB == 8)
-    NT == 512 ? fwd(k_pois_fwd<8, 512>) : fwd(k_pois_fwd<8, 256>);
-  else if (MB == 4)
-    NT == 512 ? fwd(k_pois_fwd<4, 512>) : fwd(k_pois_fwd<4, 256>);
-  else if (MB == 2)
-    NT == 512 ? fwd(k_pois_fwd<2, 512>) : fwd(k_pois_fwd<2, 256>);
+  XTabT<T> xt;
+  if constexpr (std::is_same<T, double>::value)
+    xt = xtab(c);
   else
-    NT == 512 ? fwd(k_pois_fwd<1, 512>) : fwd(k_pois_fwd<1, 256>);
+    xt = xtabf(c);
+  auto go = [&](auto kf, auto kb) {
+    if (fwd) {
+      cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      kf<<<gx, NT, smem, c->stream>>>(c->dc, xt, c->f[OTBL_F_U], c->f[OTBL_F_V], c->f[OTBL_F_W], phi, kbeg, kend);
+    } else {
+      cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      kb<<<gx, NT, smem, c->stream>>>(c->dc, xt, phi, kbeg, kend);
+    }
+  };
+#define OTBL_POIS_GO(MBV, NTV) go(k_pois_fwd<T, MBV, NTV>, k_pois_bwd<T, MBV, NTV>)
+  if (MB == 8)
+    NT == 512 ? OTBL_POIS_GO(8, 512) : OTBL_POIS_GO(8, 256);
+  else if (MB == 4)
+    NT == 512 ? OTBL_POIS_GO(4, 512) : OTBL_POIS_GO(4, 256);
+  else if (MB == 2)
+    NT == 512 ? OTBL_POIS_GO(2, 512) : OTBL_POIS_GO(2, 256);
+  else
+    NT == 512 ? OTBL_POIS_GO(1, 512) : OTBL_POIS_GO(1, 256);
+#undef OTBL_POIS_GO
+  c->launches += 1;
+}
+
+// pois.f90:11-189. FP64 path: every spanwise mode in FP64 on phi = s2. Mixed
+// path: modes k < pois_klo in FP64 (phi64 = s2), the others in FP32 (phi32 =
+// s3, free between the rhsp tails); the projection is FP64 on both.
+cudaError_t launch_pois(otbl_ctx *c, int m) {
+  (void)m;  // varstep for substep m was set by k_dt
+  const int nz2 = c->dc.nz2, ny = c->cfg.ny, nx = c->cfg.nx, nz1 = c->dc.nz1;
+  double *phi64 = c->w.s2;
+  float *phi32 = c->mixed ? reinterpret_cast<float *>(c->w.s3) : nullptr;
+  const int klo = c->mixed ? std::min(c->pois_klo, nz2 + 1) : nz2 + 1;  // modes 0..klo-1 in FP64
+  const int kr_split = 2 * klo;
+  prof_begin(c, PK_POIS_FWD);
+  pois_xdct<double>(c, true, phi64, 0, klo - 1);
+  if (klo <= nz2) pois_xdct<float>(c, true, phi32, klo, nz2);
   prof_end(c);
-  cudaError_t e = launch_pois_solve(c, phi);
+  cudaError_t e = launch_pois_solve(c, phi64, phi32, kr_split);
   if (e != cudaSuccess) return e;
   prof_begin(c, PK_POIS_BWD);
-  if (MB == 8)
-    NT == 512 ? bwd(k_pois_bwd<8, 512>) : bwd(k_pois_bwd<8, 256>);
-  else if (MB == 4)
-    NT == 512 ? bwd(k_pois_bwd<4, 512>) : bwd(k_pois_bwd<4, 256>);
-  else if (MB == 2)
-    NT == 512 ? bwd(k_pois_bwd<2, 512>) : bwd(k_pois_bwd<2, 256>);
-  else
-    NT == 512 ? bwd(k_pois_bwd<1, 512>) : bwd(k_pois_bwd<1, 256>);
+  pois_xdct<double>(c, false, phi64, 0, klo - 1);
+  if (klo <= nz2) pois_xdct<float>(c, false, phi32, klo, nz2);
   prof_end(c);
   dim3 gp((nz1 + 127) / 128, ny, nx - 1);
   prof_begin(c, PK_PROJECT);
   if (c->f32[OTBL_F_P])
-    k_project<float><<<gp, 128, 0, c->stream>>>(c->dc, c->st, phi, c->f[OTBL_F_U], c->f[OTBL_F_V],
-                                                c->f[OTBL_F_W], reinterpret_cast<float *>(c->f[OTBL_F_P]));
+    k_project<float><<<gp, 128, 0, c->stream>>>(c->dc, c->st, phi64, phi32, kr_split, c->f[OTBL_F_U],
+                                                c->f[OTBL_F_V], c->f[OTBL_F_W],
+                                                reinterpret_cast<float *>(c->f[OTBL_F_P]));
   else
-    k_project<double><<<gp, 128, 0, c->stream>>>(c->dc, c->st, phi, c->f[OTBL_F_U], c->f[OTBL_F_V],
-                                                 c->f[OTBL_F_W], c->f[OTBL_F_P]);
+    k_project<double><<<gp, 128, 0, c->stream>>>(c->dc, c->st, phi64, phi32, kr_split, c->f[OTBL_F_U],
+                                                 c->f[OTBL_F_V], c->f[OTBL_F_W], c->f[OTBL_F_P]);
   prof_end(c);
-  c->launches += 3;
+  c->launches += 1;
   return cudaGetLastError();
 }
 

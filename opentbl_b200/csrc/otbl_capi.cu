@@ -2,6 +2,7 @@
 // transfer and the stream-ordered orchestration of the kernels in
 // kernels.cu, following the call order of bl_1.F90:94-125.
 #include <algorithm>
+#include <cmath>
 #include <cstdlib>
 #include <cstdio>
 #include <cstring>
@@ -120,6 +121,20 @@ int check(otbl_ctx *c, cudaError_t e, const char *where) {
 
 }  // namespace
 
+// Mixed path: the first spanwise mode whose shifted Poisson y-system is
+// well enough conditioned for FP32 (kz^2 >= max|ayp(2,j)| / kPoisCond).
+static int pois_split(const otbl_config *cfg, const double *coef) {
+  otbl_coef_offsets o;
+  otbl_coef_layout(cfg->nx, cfg->ny, cfg->nz, &o);
+  const double *ayp = coef + o.off[OTBL_C_AYP], *kaz2 = coef + o.off[OTBL_C_KAZ2];
+  double amax = 0.0;
+  for (int j = 1; j <= cfg->ny - 1; ++j) amax = std::max(amax, std::fabs(ayp[(j - 1) * 3 + 1]));
+  const int nz2 = (2 * (cfg->nz / 3)) / 2 - 1;
+  int k = 0;
+  while (k <= nz2 && kaz2[k] < amax / kPoisCond) ++k;
+  return k;
+}
+
 extern "C" int otbl_ctx_create(const otbl_config *cfg, const double *coef, int device, otbl_ctx **out) {
   if (!cfg || !coef || !out) return OTBL_ERR_ARG;
   *out = nullptr;
@@ -182,6 +197,7 @@ extern "C" int otbl_ctx_create(const otbl_config *cfg, const double *coef, int d
     return fail(c, OTBL_ERR_CUDA, "coefficient upload failed");
   }
   c->mixed = cfg->precision == OTBL_PREC_MIXED;
+  c->pois_klo = pois_split(cfg, coef);
   c->dc = make_dcoef<double>(c->coef_dev, o, *cfg);
   c->dcf = make_dcoef<float>(nullptr, o, *cfg);
   if (c->mixed) {
@@ -208,6 +224,7 @@ extern "C" int otbl_ctx_create(const otbl_config *cfg, const double *coef, int d
       TRY(dalloc(c, &c->f[id], field_len(c, id)));
     }
   }
+  for (int id = 0; id < OTBL_F_COUNT; ++id) c->f_own[id] = c->f[id];
   TRY(dalloc(c, &c->u0, (size_t)ny + 1));
   TRY(dalloc(c, &c->v0, (size_t)ny + 1));
   TRY(dalloc(c, &c->um, (size_t)ny + 1));
@@ -243,6 +260,10 @@ extern "C" int otbl_ctx_create(const otbl_config *cfg, const double *coef, int d
   }
   TRY(dalloc(c, &w.twx, 2 * (size_t)n));
   TRY(dalloc(c, &w.twx2, 2 * (size_t)n));
+  if (c->mixed) {
+    TRY(dalloc(c, &w.twxf, 2 * (size_t)n));
+    TRY(dalloc(c, &w.twx2f, 2 * (size_t)n));
+  }
   TRY(dalloc(c, &w.vm_bits, (size_t)ny + 1));
   TRY(dalloc(c, &w.fac_u, 3 * (size_t)(ny + 4)));
   TRY(dalloc(c, &w.fac_v, 3 * (size_t)(ny + 4)));
@@ -256,11 +277,17 @@ extern "C" int otbl_ctx_create(const otbl_config *cfg, const double *coef, int d
   }
   TRY(dalloc(c, &w.gf, genflu_tab_doubles(ny)));
   TRY(dalloc(c, &w.pois_dinv, (size_t)nx * ny * (nz1 / 2)));
+  if (c->mixed) TRY(dalloc(c, &w.pois_dinvf, (size_t)nx * ny * (nz1 / 2)));
 #undef TRY
   if (!getenv("OTBL_NO_TMA")) {
     build_final_maps(c);
     build_x_maps(c);
     build_y_maps(c);
+  }
+  c->ydense = (cfg->options & OTBL_OPT_YDENSE) != 0;
+  if (c->ydense && check(c, ydense_prepare(c), "dense interpyy operator") != OTBL_OK) {
+    *out = c;
+    return OTBL_ERR_CUDA;
   }
   if (check(c, launch_twiddles(c), "twiddles") != OTBL_OK || check(c, launch_pois_lu(c), "pois_lu") != OTBL_OK ||
       check(c, launch_x_rows(c), "x rows") != OTBL_OK || check(c, launch_y_rows(c), "y rows") != OTBL_OK ||
@@ -284,9 +311,10 @@ extern "C" size_t otbl_ctx_bytes(const otbl_config *cfg) {
   b += 3 * (size_t)(ny + 1) * sizeof(double) + sizeof(DState);   // u0, v0, um, scalars
   b += 15 * lu * (mixed ? sizeof(float) : sizeof(double));       // intermediates
   b += 2 * (std::max(lu, (size_t)(ny + 2) * (nx - 1) * nz1) + 2 * lu) * sizeof(double);  // s1..s3, t1..t3
-  b += (4 * (size_t)M + 4 * (size_t)n) * sizeof(double) + (mixed ? 4 * (size_t)M * sizeof(float) : 0);
+  b += (4 * (size_t)M + 4 * (size_t)n) * sizeof(double) + (mixed ? (4 * (size_t)M + 4 * (size_t)n) * sizeof(float) : 0);
   b += (size_t)(ny + 1) * 8 + 6 * (size_t)(ny + 4) * sizeof(double) + genflu_tab_doubles(ny) * sizeof(double);
-  b += (size_t)nx * ny * (nz1 / 2) * sizeof(double);             // Poisson pivots
+  b += (size_t)nx * ny * (nz1 / 2) * (sizeof(double) + (mixed ? sizeof(float) : 0));  // Poisson pivots
+  if (cfg->options & OTBL_OPT_YDENSE) b += ydense_bytes(ny);     // dense interpyy operators
   b += (2 * 16 * (size_t)(ny + 2) + 4 * 16 * (size_t)nx + 2 * 8 * (size_t)ny) * sizeof(double);  // coefficient rows
   return b;
 }
@@ -295,7 +323,8 @@ extern "C" int otbl_ctx_rebind(otbl_ctx *c, const otbl_config *cfg, const double
   if (!c || !cfg || !coef) return OTBL_ERR_ARG;
   int st = otbl_config_check(cfg);
   if (st != OTBL_OK) return st;
-  if (cfg->nx != c->cfg.nx || cfg->ny != c->cfg.ny || cfg->nz != c->cfg.nz || cfg->precision != c->cfg.precision)
+  if (cfg->nx != c->cfg.nx || cfg->ny != c->cfg.ny || cfg->nz != c->cfg.nz || cfg->precision != c->cfg.precision ||
+      cfg->options != c->cfg.options)
     return OTBL_ERR_CONFIG;
   cudaSetDevice(c->device);
   OTBL_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
@@ -304,6 +333,7 @@ extern "C" int otbl_ctx_rebind(otbl_ctx *c, const otbl_config *cfg, const double
   const size_t ncoef = o.off[OTBL_C_COUNT];
   c->cfg = *cfg;
   c->coef_host.assign(coef, coef + ncoef);
+  c->pois_klo = pois_split(cfg, coef);
   OTBL_CUDA_TRY(c, cudaMemcpyAsync(c->coef_dev, coef, ncoef * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   OTBL_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   c->dc = make_dcoef<double>(c->coef_dev, o, *cfg);
@@ -315,6 +345,7 @@ extern "C" int otbl_ctx_rebind(otbl_ctx *c, const otbl_config *cfg, const double
     c->dcf = make_dcoef<float>(c->coef_dev_f, o, *cfg);
   }
   if (check(c, launch_pois_lu(c), "pois_lu") != OTBL_OK) return OTBL_ERR_CUDA;
+  if (c->ydense && check(c, ydense_prepare(c), "dense interpyy operator") != OTBL_OK) return OTBL_ERR_CUDA;
   if (check(c, launch_x_rows(c), "x rows") != OTBL_OK) return OTBL_ERR_CUDA;
   if (check(c, launch_y_rows(c), "y rows") != OTBL_OK) return OTBL_ERR_CUDA;
   OTBL_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
@@ -416,6 +447,23 @@ extern "C" int otbl_set_inflow(otbl_ctx *c, const double *u0, const double *v0, 
   return OTBL_OK;
 }
 
+// Maps the context's device error flag (first error wins) to a status and
+// its message.
+static int device_error(otbl_ctx *c, int code) {
+  switch (code) {
+    case OTBL_ERR_TIMEOUT:
+      c->err = "a device-side wait of a kernel timed out";
+      return OTBL_ERR_TIMEOUT;
+    case OTBL_DEVERR_GENFLU_GRID:
+      c->err = "genflu: the rescaled inflow grid could not be profiled (degenerate rescaling); "
+               "plane 1 holds the blended copy of plane xout";
+      return OTBL_ERR_NAN;
+    default:
+      c->err = "non-finite value in the CFL reduction (u, v, w maxima or dt)";
+      return OTBL_ERR_NAN;
+  }
+}
+
 extern "C" int otbl_get_inflow(otbl_ctx *c, double *um, otbl_inflow *s) {
   if (!c) return OTBL_ERR_ARG;
   cudaSetDevice(c->device);
@@ -439,11 +487,7 @@ extern "C" int otbl_get_inflow(otbl_ctx *c, double *um, otbl_inflow *s) {
     s->wmax = h.wmax;
     s->vmax = h.vmax;
   }
-  if (h.err) {
-    c->err = h.err == OTBL_ERR_TIMEOUT ? "a device-side wait of a kernel timed out"
-                                     : "non-finite value in the CFL reduction";
-    return h.err;
-  }
+  if (h.err) return device_error(c, h.err);
   return OTBL_OK;
 }
 
@@ -595,15 +639,91 @@ extern "C" int otbl_sync(otbl_ctx *c) {
   int err = 0;
   OTBL_CUDA_TRY(c, cudaMemcpyAsync(&err, &c->st->err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   OTBL_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-  if (err) {
-    c->err = err == OTBL_ERR_TIMEOUT ? "a device-side wait of a kernel timed out"
-                                     : "non-finite value in the CFL reduction";
-    return err;
+  if (err) return device_error(c, err);
+  return OTBL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// The reference's array surface: the state in the caller's device arrays.
+// Binding stores the pointers and re-encodes the TMA descriptors that name
+// state fields (host work only, no device synchronisation: launches already
+// issued keep the descriptors they were given).
+// ---------------------------------------------------------------------------
+static int bind_fields(otbl_ctx *c, double *const *ptr, const bool *use) {
+  bool changed = false;
+  for (int id = 0; id < OTBL_F_COUNT; ++id) {
+    if (!use[id]) continue;
+    double *q = ptr[id] ? ptr[id] : c->f_own[id];
+    if (q == c->f[id]) continue;
+    if (c->mixed) return fail(c, OTBL_ERR_CONFIG, "caller-owned state arrays need the FP64 path");
+    if (reinterpret_cast<uintptr_t>(q) % 16 != 0)
+      return fail(c, OTBL_ERR_ARG, "state arrays must be 16-byte aligned");
+    changed = true;
+  }
+  if (!changed) return OTBL_OK;
+  for (int id = 0; id < OTBL_F_COUNT; ++id)
+    if (use[id]) c->f[id] = ptr[id] ? ptr[id] : c->f_own[id];
+  if (!getenv("OTBL_NO_TMA")) {
+    build_final_maps(c);
+    build_x_maps(c);
+    build_y_maps(c);
   }
   return OTBL_OK;
 }
 
-extern "C" int otbl_chp2x(otbl_ctx *c, const double *plan, double *pen, int jee) {
+extern "C" int otbl_bind_state(otbl_ctx *c, double *u, double *v, double *w, double *p, double *rhsupa,
+                               double *rhsvpa, double *rhswpa) {
+  if (!c) return OTBL_ERR_ARG;
+  double *ptr[OTBL_F_COUNT] = {u, v, w, p, rhsupa, rhsvpa, rhswpa};
+  const bool use[OTBL_F_COUNT] = {true, true, true, true, true, true, true};
+  cudaSetDevice(c->device);
+  return bind_fields(c, ptr, use);
+}
+
+extern "C" int otbl_rhsp_arrays(otbl_ctx *c, double *u, double *v, double *w, double *p, double *rhsupa,
+                                double *rhsvpa, double *rhswpa, int m, int setstep) {
+  if (!c || !u || !v || !w || !p || !rhsupa || !rhsvpa || !rhswpa) return OTBL_ERR_ARG;
+  const int st = otbl_bind_state(c, u, v, w, p, rhsupa, rhsvpa, rhswpa);
+  return st != OTBL_OK ? st : otbl_rhsp(c, m, setstep);
+}
+
+extern "C" int otbl_outflow_correction_arrays(otbl_ctx *c, double *u, double *v, double *rhsupa) {
+  if (!c || !u || !v || !rhsupa) return OTBL_ERR_ARG;
+  double *ptr[OTBL_F_COUNT] = {u, v, nullptr, nullptr, rhsupa, nullptr, nullptr};
+  const bool use[OTBL_F_COUNT] = {true, true, false, false, true, false, false};
+  cudaSetDevice(c->device);
+  const int st = bind_fields(c, ptr, use);
+  return st != OTBL_OK ? st : otbl_outflow_correction(c);
+}
+
+extern "C" int otbl_pois_arrays(otbl_ctx *c, double *u, double *v, double *w, double *p, int m) {
+  if (!c || !u || !v || !w || !p) return OTBL_ERR_ARG;
+  double *ptr[OTBL_F_COUNT] = {u, v, w, p, nullptr, nullptr, nullptr};
+  const bool use[OTBL_F_COUNT] = {true, true, true, true, false, false, false};
+  cudaSetDevice(c->device);
+  const int st = bind_fields(c, ptr, use);
+  return st != OTBL_OK ? st : otbl_pois(c, m);
+}
+
+extern "C" int otbl_boun_arrays(otbl_ctx *c, double *u, double *v, double *w) {
+  if (!c || !u || !v || !w) return OTBL_ERR_ARG;
+  double *ptr[OTBL_F_COUNT] = {u, v, w, nullptr, nullptr, nullptr, nullptr};
+  const bool use[OTBL_F_COUNT] = {true, true, true, false, false, false, false};
+  cudaSetDevice(c->device);
+  const int st = bind_fields(c, ptr, use);
+  return st != OTBL_OK ? st : otbl_boun(c);
+}
+
+extern "C" int otbl_genflu_arrays(otbl_ctx *c, double *u, double *v, double *w) {
+  if (!c || !u || !v || !w) return OTBL_ERR_ARG;
+  double *ptr[OTBL_F_COUNT] = {u, v, w, nullptr, nullptr, nullptr, nullptr};
+  const bool use[OTBL_F_COUNT] = {true, true, true, false, false, false, false};
+  cudaSetDevice(c->device);
+  const int st = bind_fields(c, ptr, use);
+  return st != OTBL_OK ? st : otbl_genflu(c);
+}
+
+extern "C" int otbl_chp2x(otbl_ctx *c, double *pen, const double *plan, int jee) {
   if (!c || !plan || !pen || (jee != c->cfg.ny && jee != c->cfg.ny + 1)) return OTBL_ERR_ARG;
   cudaSetDevice(c->device);
   LAUNCH(c, launch_chp2x(c, plan, pen, jee, 1));
@@ -633,6 +753,29 @@ extern "C" int otbl_cosftx(otbl_ctx *c, double *cp, int nlines, int iopt) {
   return OTBL_OK;
 }
 
+extern "C" int otbl_interpyy(otbl_ctx *c, double *uy, double *wy, double *vy) {
+  if (!c || !uy || !wy || !vy) return OTBL_ERR_ARG;
+  cudaSetDevice(c->device);
+  LAUNCH(c, launch_interpy(c));
+  const size_t n = otbl_field_len(c->cfg.nx, c->cfg.ny, c->cfg.nz, 0);
+  void *src[3] = {c->w.uy, c->w.wy, c->w.vy};
+  double *dst[3] = {uy, wy, vy};
+  for (int f = 0; f < 3; ++f) {
+    if (c->mixed) {
+      std::vector<float> tmp(n);
+      OTBL_CUDA_TRY(c, cudaMemcpyAsync(tmp.data(), src[f], n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+      OTBL_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+      std::copy(tmp.begin(), tmp.end(), dst[f]);
+    } else {
+      OTBL_CUDA_TRY(c, cudaMemcpyAsync(dst[f], src[f], n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    }
+  }
+  OTBL_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  int err = 0;
+  OTBL_CUDA_TRY(c, cudaMemcpy(&err, &c->st->err, sizeof(int), cudaMemcpyDeviceToHost));
+  return err ? device_error(c, err) : OTBL_OK;
+}
+
 extern "C" int otbl_boun(otbl_ctx *c) {
   if (!c) return OTBL_ERR_ARG;
   cudaSetDevice(c->device);
@@ -655,11 +798,10 @@ extern "C" int otbl_genflu_noalloc(otbl_ctx *c, double *u, double *v, double *w,
   if (!c) return OTBL_ERR_ARG;
   if (!u || !v || !w || !u0 || !v0 || !um || !scal)
     return fail(c, OTBL_ERR_ARG, "otbl_genflu_noalloc: null device pointer");
-  if (genflu_tab_doubles(c->cfg.ny) > (size_t)OTBL_GENFLU_SCRATCH_MAX)
+  if (c->cfg.ny > kGenfluNoallocMaxNy)
     return fail(c, OTBL_ERR_CONFIG,
-                "otbl_genflu_noalloc: the tables, 3*(ny+1)+2 doubles, exceed OTBL_GENFLU_SCRATCH_MAX");
-  if (genflu_smem_bytes(c->cfg.ny) > 48 * 1024)
-    return fail(c, OTBL_ERR_CONFIG, "otbl_genflu_noalloc: ny too large for 48 KB of shared memory");
+                "otbl_genflu_noalloc: ny > 680 (its tables would exceed OTBL_GENFLU_SCRATCH_MAX or its "
+                "shared memory 48 KB)");
   OTBL_CUDA_TRY(c, cudaSetDevice(c->device));
   double *wk = nullptr;
   OTBL_CUDA_TRY(c, genflu_scratch_addr(c->device, &wk));

@@ -62,6 +62,7 @@ struct Work {
   float *twzf, *twz2f;         // the same rounded to FP32 (mixed path)
   double *twx;                 // x-DCT twiddles for the length nx-1 FFT
   double *twx2;                // exp(-i pi k/(2n)), k = 0..n-1
+  float *twxf, *twx2f;         // the same rounded to FP32 (mixed path)
   unsigned long long *vm_bits; // vm(j) maxima, j = 1..ny
   double *fac_u, *fac_v;       // implzy LU factors for the current dt (3*(ny+1))
   double *rowc;                // k_final_tb's per-row coefficients, [2][ny+2][16]
@@ -69,6 +70,7 @@ struct Work {
   void *yrowc;                 // k_interpy_t's per-row coefficients, [2][ny][8] (T)
   double *gf;                  // genflu tables (genflu_tab_doubles)
   double *pois_dinv;           // pivots of the (x-mode, kz) y-systems, [i][j][k]
+  float *pois_dinvf;           // the same rounded to FP32 (mixed path, modes >= kPoisLow)
 };
 
 // TMA descriptors (opaque 128-byte CUtensorMap objects) of the fields the
@@ -111,6 +113,14 @@ struct otbl_ctx {
   // [0] k_interpx, [1] k_difvisx, [2] k_interpy (one thread per line, so the
   // choice changes the schedule, never the arithmetic)
   int tune_bs[3] = {128, 128, 128};
+  // interpyy of the mixed path as a dense operator on the tensor cores
+  // (OTBL_OPT_YDENSE, k_ydense.cu): the operators' TF32 chunks on the device
+  // and, per input type and M-tile, the K-chunks [kb, ke) of their band
+  int pois_klo = 0;  // mixed path: spanwise modes k < pois_klo solve in FP64 (kPoisCond)
+  bool ydense = false;
+  uint32_t *yd_op = nullptr;
+  size_t yd_words_per_op = 0;
+  int yd_kb[2][2] = {{0, 0}, {0, 0}}, yd_ke[2][2] = {{0, 0}, {0, 0}};
   // TMA descriptors of the rhsp tail's inputs, per velocity component
   otbl::FinalMaps fmaps[3];
   bool fmaps_ok = false;
@@ -124,7 +134,8 @@ struct otbl_ctx {
   std::vector<double> coef_host;
   // state fields; on the mixed path p and the RHS history are stored as
   // float (f32[id]) behind the same pointer, u, v, w always as double
-  double *f[OTBL_F_COUNT];
+  double *f[OTBL_F_COUNT];      // the state the kernels use: own arrays or bound ones
+  double *f_own[OTBL_F_COUNT];  // the context's own state arrays (freed with it)
   bool f32[OTBL_F_COUNT] = {false, false, false, false, false, false, false};
   double *u0, *v0, *um;
   otbl::DState *st;
@@ -153,6 +164,20 @@ extern const char *const kProfNames[PK_COUNT];
 void prof_begin(otbl_ctx *c, int kind);
 void prof_end(otbl_ctx *c);
 }  // namespace otbl
+
+// Mixed path: the Poisson solve (x-DCTs, y-systems, phi) of a spanwise mode
+// k runs in FP32 only when its shifted y-system is well conditioned: kz^2 >=
+// max|ayp(2,j)| / kPoisCond, so that FP32 rounding of phi, amplified by the
+// y second difference (up to ~4/dy_wall^2 on the stretched grid), stays
+// below kPoisCond x 6e-8 of the mode's divergence. Lower modes run in FP64.
+// (FP32 from k = 4 up, tried first, left max|div u| ~1e-6 after the
+// projection at 1025x193x512: kappa(k = 4) ~ 1.6e5.)
+constexpr double kPoisCond = 1024.0;
+
+// Device error code written into the context's flag by genflu when the
+// rescaled inflow grid cannot be profiled; reported to callers as
+// OTBL_ERR_NAN with its own message (never returned as is).
+#define OTBL_DEVERR_GENFLU_GRID 0x105
 
 #define OTBL_CUDA_TRY(ctx, call)                                        \
   do {                                                                  \
@@ -204,15 +229,34 @@ cudaError_t launch_y_rows(otbl_ctx *c);
 bool build_y_maps(otbl_ctx *c);
 cudaError_t launch_twiddles(otbl_ctx *c);
 cudaError_t launch_pois_lu(otbl_ctx *c);
-cudaError_t launch_pois_solve(otbl_ctx *c, double *phi);
+// columns kr < kr_split solve in FP64 on phi64, the others in FP32 on phi32
+cudaError_t launch_pois_solve(otbl_ctx *c, double *phi64, float *phi32, int kr_split);
+cudaError_t launch_round_f32(otbl_ctx *c, const double *in, float *out, size_t n);
+// interpyy on the tensor cores (k_ydense.cu)
+cudaError_t ydense_prepare(otbl_ctx *c);
+cudaError_t launch_interpy_dense(otbl_ctx *c);
+size_t ydense_bytes(int ny);
 // standalone pieces
 cudaError_t launch_chp2x(otbl_ctx *c, const double *plan, double *pen, int jee, int to_pen);
 cudaError_t launch_fourxz(otbl_ctx *c, double *fou, double *phys, int iopt, int nlines);
 cudaError_t launch_cosftx(otbl_ctx *c, double *cpen, int nlines, int iopt);
 // genflu table scratch: fsca[2][ny+1] | kl[2][ny+1] (int) | ggg | ntop[2] (int)
-inline size_t genflu_tab_doubles(int ny) { return 3 * (size_t)(ny + 1) + 2; }
-// genflu on caller-owned buffers with the static table scratch (no allocation)
-size_t genflu_smem_bytes(int ny);
+constexpr size_t genflu_tab_doubles(int ny) { return 3 * (size_t)(ny + 1) + 2; }
+// dynamic shared memory of k_genflu_tab: ysca, www, yyy [2][ny+1], um(0..ny+1)
+// in doubles, kf, kh [2][ny+1] in ints, and slack
+constexpr size_t genflu_smem_bytes(int ny) {
+  return sizeof(double) * (6 * (size_t)(ny + 1) + (ny + 2)) + sizeof(int) * 4 * (size_t)(ny + 1) + 64;
+}
+// genflu on caller-owned buffers with the static table scratch (no
+// allocation). Its one limit: ny <= 680, where both the tables fit the
+// static array and k_genflu_tab's shared memory fits the 48 KB a launch gets
+// without opting in (at ny = 681 the tables still fit, the shared memory no
+// longer does).
+constexpr int kGenfluNoallocMaxNy = 680;
+static_assert(genflu_tab_doubles(kGenfluNoallocMaxNy) <= (size_t)OTBL_GENFLU_SCRATCH_MAX,
+              "genflu tables of the largest admitted ny exceed the static scratch");
+static_assert(genflu_smem_bytes(kGenfluNoallocMaxNy) <= 48 * 1024,
+              "genflu shared memory of the largest admitted ny exceeds 48 KB");
 cudaError_t genflu_scratch_addr(int device, double **p);
 cudaError_t launch_genflu_noalloc(otbl_ctx *c, double *wk, double *u, double *v, double *w, const double *u0,
                                   const double *v0, double *um, double *scal, int *err);

@@ -20,6 +20,8 @@ OTBL_BUSY = 7
 ERRORS = {1: "bad argument", 2: "bad configuration", 3: "out of device memory",
           4: "CUDA error", 5: "non-finite value", 6: "no CUDA device",
           8: "device wait timed out"}
+ERRORS_BY_NAME = {"ARG": 1, "CONFIG": 2, "OOM": 3, "CUDA": 4, "NAN": 5, "NODEV": 6, "BUSY": 7,
+                  "TIMEOUT": 8}
 FIELDS = ("u", "v", "w", "p", "rhsupa", "rhsvpa", "rhswpa")
 UTYPE = {"u": True, "v": False, "w": True, "p": False,
          "rhsupa": True, "rhsvpa": False, "rhswpa": True}
@@ -43,7 +45,7 @@ class OtblConfig(ctypes.Structure):
                 ("ax", ctypes.c_double), ("ay", ctypes.c_double),
                 ("az", ctypes.c_double), ("cfl", ctypes.c_double),
                 ("y_blend", ctypes.c_double), ("dt_fixed", ctypes.c_double),
-                ("precision", ctypes.c_int), ("reserved", ctypes.c_int)]
+                ("precision", ctypes.c_int), ("options", ctypes.c_int)]
 
 
 class OtblInflow(ctypes.Structure):
@@ -88,7 +90,14 @@ def _bind(L):
         "otbl_fourxz": ([P, P, P, I, I], I),
         "otbl_cosftx": ([P, P, I, I], I),
         "otbl_boun": ([P], I),
+        "otbl_interpyy": ([P, D, D, D], I),
         "otbl_genflu": ([P], I),
+        "otbl_bind_state": ([P] + [P] * 7, I),
+        "otbl_rhsp_arrays": ([P] + [P] * 7 + [I, I], I),
+        "otbl_outflow_correction_arrays": ([P, P, P, P], I),
+        "otbl_pois_arrays": ([P, P, P, P, P, I], I),
+        "otbl_boun_arrays": ([P, P, P, P], I),
+        "otbl_genflu_arrays": ([P, P, P, P], I),
         "otbl_launch_count": ([P], ctypes.c_longlong),
         "otbl_graph_create": ([ctypes.POINTER(P), I, I, ctypes.POINTER(P)], I),
         "otbl_graph_launch": ([P], I),
@@ -132,7 +141,7 @@ def dptr(a: np.ndarray):
 def make_config(cfg, re: float, xout: int) -> OtblConfig:
     return OtblConfig(cfg.nx, cfg.ny, cfg.nz, xout, cfg.xpose_round, cfg.dt_mode,
                       re, cfg.ax, 0.0, cfg.az, cfg.cfl, cfg.y_blend, cfg.dt_fixed,
-                      getattr(cfg, "precision", 0), 0)
+                      getattr(cfg, "precision", 0), getattr(cfg, "options", 0))
 
 
 def coef_compute(cfg, re: float, xout: int, y: np.ndarray, u0: np.ndarray) -> np.ndarray:

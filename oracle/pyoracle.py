@@ -25,7 +25,7 @@ class OtblConfig(ctypes.Structure):
                 ("ax", ctypes.c_double), ("ay", ctypes.c_double),
                 ("az", ctypes.c_double), ("cfl", ctypes.c_double),
                 ("y_blend", ctypes.c_double), ("dt_fixed", ctypes.c_double),
-                ("precision", ctypes.c_int), ("reserved", ctypes.c_int)]
+                ("precision", ctypes.c_int), ("options", ctypes.c_int)]
 
 
 class OtblInflow(ctypes.Structure):
@@ -102,7 +102,7 @@ UTYPE = {"u": True, "v": False, "w": True, "p": False,
 def make_config(cfg, re: float, xout: int) -> OtblConfig:
     return OtblConfig(cfg.nx, cfg.ny, cfg.nz, xout, cfg.xpose_round, cfg.dt_mode,
                       re, cfg.ax, 0.0, cfg.az, cfg.cfl, cfg.y_blend, cfg.dt_fixed,
-                      getattr(cfg, "precision", 0), 0)
+                      getattr(cfg, "precision", 0), getattr(cfg, "options", 0))
 
 
 def coef_count(cfg) -> int:

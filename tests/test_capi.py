@@ -120,3 +120,36 @@ def test_coefficients_are_host_only_and_deterministic():
     a = native.coef_compute(cfg, init["re"], init["xout"], init["y"], init["u0"])
     b = native.coef_compute(cfg, init["re"], init["xout"], init["y"], init["u0"])
     assert np.array_equal(a, b) and np.isfinite(a).all()
+
+
+def _driver():
+    from opentbl_b200 import build
+    if not os.path.exists(build.DRIVER):
+        build.build_driver()
+    return build.DRIVER
+
+
+def test_c_driver_without_gpu():
+    """csrc/otbl_driver.c drives the time loop through include/otbl.h alone.
+    Here (no GPU) it computes the coefficients and stops at context creation
+    with OTBL_ERR_NODEV (exit status 3): no CPU fallback."""
+    import subprocess
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present: the GPU test runs the driver")
+    r = subprocess.run([_driver()], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 3, (r.returncode, r.stdout, r.stderr)
+    assert "OTBL_ERR_NODEV" in r.stdout
+
+
+@pytest.mark.gpu
+def test_c_driver_on_gpu():
+    """The C driver on the GPU: three RK3 steps through the context API and
+    through the array surface on caller-owned arrays, bit-identical."""
+    import subprocess
+    r = subprocess.run([_driver(), "33", "41", "32", "3"], capture_output=True, text=True, timeout=300)
+    print(r.stdout)
+    assert r.returncode == 0, (r.returncode, r.stdout, r.stderr)
+    assert "bit-identical" in r.stdout
+    steps = [ln for ln in r.stdout.splitlines() if ln.startswith("step ")]
+    assert len(steps) == 3

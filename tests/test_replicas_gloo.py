@@ -88,6 +88,12 @@ def test_bench_reference_arm_under_torchrun():
               "cpu_baseline", "e2e"):
         assert k in d, k
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
-    assert d["steps"] == 1 and d["warmup"] == 1  # as asked (each is one substep)
+    assert d["steps"] == 1 and d["warmup"] == 1  # as asked (full RK3 steps)
+    # the same workload config as the GPU arm, and nothing of the product loaded
+    sys.path.insert(0, ROOT)
+    import bench
+    from opentbl_b200 import config
+    assert d["config"] == bench.workload_config(config.TINY, 2)
+    assert d["libraries_loaded"] == ["oracle/liboracle.so"], d["libraries_loaded"]
     assert d["cpu_baseline"]["kind"] == "port"
     assert d["e2e"]["h2d_bytes_per_step"] == 0

@@ -75,10 +75,14 @@ def test_genflu_noalloc_matches_genflu_two_calls():
         assert int(bufs["err"].cpu()[0]) == 0
 
 
-def test_genflu_noalloc_rejects_oversized_plane_and_nulls():
+@pytest.mark.parametrize("ny", [681, 700])
+def test_genflu_noalloc_rejects_oversized_plane_and_nulls(ny):
+    """ny = 681 still fits the tables (3*682+2 = 2048 doubles) but not 48 KB
+    of shared memory; ny = 700 fits neither. Both are refused before any
+    launch."""
     torch = pytest.importorskip("torch")
-    big = replace(config.SMALL, nx=9, ny=700, nz=32, name="tall-9x700x32")
-    assert 3 * (big.ny + 1) + 2 > SCRATCH_MAX
+    big = replace(config.SMALL, nx=9, ny=ny, nz=32, name=f"tall-9x{ny}x32")
+    assert 3 * (big.ny + 1) + 2 > SCRATCH_MAX or ny == 681
     init, coef = setup(big)
     g = Box(big, init, coef)
     fn = _bind(g.L)
