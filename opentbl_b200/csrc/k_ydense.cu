@@ -22,8 +22,12 @@
 // stages: the operator chunk (both M-tiles, both parts, 32 KB, stored in
 // global memory in the canonical K-major layout) arrives by one bulk copy
 // (cp.async.bulk, no tensor map, no multicast), the field chunk (16 rows x
-// 256 columns, FP64) is loaded, split and written in the canonical MN-major
-// layout by the threads. Thread 0 issues the MMAs and commits each stage to
+// 256 columns, FP64) is loaded, split and written by the threads in the
+// canonical K-major layout too, i.e. transposed on the way into shared
+// memory. (The field's natural order would be the MN-major operand form, but
+// kind::tf32 with B MN-major, no swizzle, left the accumulators at zero on
+// B200 in a one-MMA probe, while the K-major form was exact.) Thread 0 issues
+// the MMAs and commits each stage to
 // an mbarrier that releases it. Chunks in which an M-tile's rows of Mop are
 // below 2^-40 of its largest entry (the inverse of the diagonally dominant
 // tridiagonal decays geometrically away from the diagonal) are skipped for
@@ -59,9 +63,9 @@ constexpr uint64_t YD_WAIT_NS = 2000000000ull;  // 2 s
 __host__ __device__ constexpr int yd_a_off(int m, int k) {
   return (m & 7) * 16 + (m >> 3) * (YD_KC / 4 * 128) + (k >> 2) * 128 + (k & 3) * 4;
 }
-// canonical MN-major, no swizzle: element (n, k) of one part, k < 16
+// the field chunk in the same K-major form: element (n, k) of one part, k < 16
 __host__ __device__ constexpr int yd_b_off(int n, int k) {
-  return (n & 3) * 4 + (k & 7) * 16 + (n >> 2) * 128 + (k >> 3) * (YD_N / 4 * 128);
+  return (n & 7) * 16 + (n >> 3) * (YD_KC / 4 * 128) + (k >> 2) * 128 + (k & 3) * 4;
 }
 static_assert(yd_a_off(127, 15) + 4 == YD_A_PART, "A part layout");
 static_assert(yd_b_off(255, 15) + 4 == YD_B_PART, "B part layout");
@@ -72,9 +76,9 @@ __device__ __forceinline__ uint64_t yd_desc(uint32_t saddr, uint32_t lbo, uint32
   return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
          ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
 }
-// instruction descriptor, kind::tf32: F32 accumulator, A K-major, B MN-major
+// instruction descriptor, kind::tf32: F32 accumulator, A and B K-major
 constexpr uint32_t yd_idesc(int M, int N) {
-  return (1u << 4) | (2u << 7) | (2u << 10) | (0u << 15) | (1u << 16) | ((uint32_t)(N >> 3) << 17) |
+  return (1u << 4) | (2u << 7) | (2u << 10) | (0u << 15) | (0u << 16) | ((uint32_t)(N >> 3) << 17) |
          ((uint32_t)(M >> 4) << 24);
 }
 
@@ -182,27 +186,27 @@ __global__ void __launch_bounds__(YD_THREADS, 1) k_ydense(int nx, int ny, int nz
                     &bar_full[s]);
       }
       // the field chunk: rows k0..k0+15 x 256 columns, split into hi/lo.
-      // Item e = (row k = e % 16, column pair q = e / 16): the 16 threads of a
-      // row group write 16 rows of one 4-column group (conflict-free: the
-      // rows of an MN-major core matrix are consecutive 16-byte units).
+      // Item e = (column n = e % 256, rows k0+4g..k0+4g+3, g = e / 256): four
+      // loads of one column (a warp reads 32 consecutive columns of a row),
+      // one 16-byte store per part (8 consecutive lanes fill the 8 rows of a
+      // core matrix: conflict-free).
       const int k0 = kc * YD_KC;
-      for (int e = t; e < YD_KC * (YD_N / 2); e += YD_THREADS) {
-        const int k = e & (YD_KC - 1), q = e >> 4;  // column pair q: n = 2q, 2q+1
-        const int n = 2 * q, j = k0 + k;
+      for (int e = t; e < YD_N * (YD_KC / 4); e += YD_THREADS) {
+        const int n = e & (YD_N - 1), g = e / YD_N;
         const long cidx = c0 + n;
-        double x0 = 0.0, x1 = 0.0;
-        if (j < F.K && cidx < C) {  // nz1 is even: a pair never spans two planes
-          const long i = cidx / nz1, kr = cidx - i * nz1;
-          const double2 v = *reinterpret_cast<const double2 *>(F.in + ((size_t)i * F.K + j) * nz1 + kr);
-          x0 = v.x;
-          x1 = v.y;
+        const bool col_ok = cidx < C;
+        const long i = col_ok ? cidx / nz1 : 0, kr = col_ok ? cidx - i * nz1 : 0;
+        uint32_t hi[4], lo[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int j = k0 + 4 * g + q;
+          const double x = (col_ok && j < F.K) ? F.in[((size_t)i * F.K + j) * nz1 + kr] : 0.0;
+          hi[q] = yd_tf32((float)x);
+          lo[q] = yd_tf32((float)(x - (double)__uint_as_float(hi[q])));
         }
-        const uint32_t h0 = yd_tf32((float)x0), h1 = yd_tf32((float)x1);
-        const uint32_t l0 = yd_tf32((float)(x0 - (double)__uint_as_float(h0)));
-        const uint32_t l1 = yd_tf32((float)(x1 - (double)__uint_as_float(h1)));
-        const int off = yd_b_off(n, k);  // n even: n and n+1 share a 16-byte unit
-        *reinterpret_cast<uint2 *>(sb + off) = make_uint2(h0, h1);
-        *reinterpret_cast<uint2 *>(sb + YD_B_PART + off) = make_uint2(l0, l1);
+        const int off = yd_b_off(n, 4 * g);
+        *reinterpret_cast<uint4 *>(sb + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+        *reinterpret_cast<uint4 *>(sb + YD_B_PART + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
       }
       asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
       __syncthreads();
@@ -221,10 +225,10 @@ __global__ void __launch_bounds__(YD_THREADS, 1) k_ydense(int nx, int ny, int nz
             for (int ks = 0; ks < YD_KC / 8; ++ks) {
               const uint32_t ah = sa_u + (uint32_t)((mt * 2 + 0) * YD_A_PART + ks * 256);
               const uint32_t al = sa_u + (uint32_t)((mt * 2 + 1) * YD_A_PART + ks * 256);
-              const uint32_t bh = sb_u + (uint32_t)(ks * (YD_N / 4 * 128));
+              const uint32_t bh = sb_u + (uint32_t)(ks * 256);
               const uint32_t bl = bh + YD_B_PART;
               const uint64_t dah = yd_desc(ah, 128, YD_KC / 4 * 128), dal = yd_desc(al, 128, YD_KC / 4 * 128);
-              const uint64_t dbh = yd_desc(bh, YD_N / 4 * 128, 128), dbl = yd_desc(bl, YD_N / 4 * 128, 128);
+              const uint64_t dbh = yd_desc(bh, 128, YD_KC / 4 * 128), dbl = yd_desc(bl, 128, YD_KC / 4 * 128);
               const uint32_t first = (kc == F.kb[mt] && ks == 0) ? 0u : 1u;
               yd_mma(d, dah, dbh, IDESC, first);
               yd_mma(d, dah, dbl, IDESC, 1u);
