@@ -53,8 +53,10 @@ def peaks():
 # path stores the fields. FP64: the velocity u, v, w; FP32: the pressure p,
 # the RHS history rhs*pa, the x interpolants, the products and partial
 # right-hand sides, and the x-line right-hand sides. The divergence and phi
-# (four passes) hold the spanwise modes k < 4 in FP64 and the others in
-# FP32, so a fraction 4/(nz2+1) of those passes is FP64.
+# (four passes) hold the spanwise modes the Poisson solve keeps in FP64 (k
+# below the first mode with kz^2 >= max|ayp(2,j)| / 1024, the library's
+# conditioning rule: 35 of 170 at 1025x193x512) in FP64 and the others in
+# FP32.
 #   A  reads phi (div/phi), u, v, w (3 FP64), p (1 FP32);
 #      writes u, v, w (3 FP64), p, u_x, v_x, w_x (4 FP32)         6 + 5 + 1 div/phi
 #   B  reads u, v, w (3 FP64), u_x, v_x, w_x;
@@ -64,15 +66,32 @@ def peaks():
 #   D  reads 3 RHS, 3 RHS history, p (7 FP32), u, v, w (3 FP64);
 #      writes u, v, w (3 FP64), div, 3 RHS history (3 FP32)        6 + 10 + 1 div/phi
 #   P  reads div, writes phi                                        2 div/phi
-MIXED_MANIFEST = {"fp64_passes": 6 + 3 + 3 + 6, "fp32_passes": 5 + 9 + 9 + 10,
-                  "div_phi_passes": 4, "div_phi_fp64_modes": 4}
+MIXED_MANIFEST = {"fp64_passes": 6 + 3 + 3 + 6, "fp32_passes": 5 + 9 + 9 + 10, "div_phi_passes": 4}
+POIS_COND = 1024.0
 
 
-def mixed_passes(cfg):
+def pois_fp64_modes(cfg, coef) -> int:
+    """Spanwise modes whose Poisson solve the mixed path keeps in FP64."""
+    off = native.coef_offsets(cfg)
+    ayp = np.asarray(coef[off["AYP"]:off["AYP"] + 3 * cfg.ny])
+    amax = float(np.max(np.abs(ayp[1:3 * (cfg.ny - 1):3])))
+    kaz2 = np.asarray(coef[off["KAZ2"]:off["KAZ2"] + cfg.nz2 + 1])
+    k = 0
+    while k <= cfg.nz2 and kaz2[k] < amax / POIS_COND:
+        k += 1
+    return k
+
+
+def mixed_passes(cfg, fp64_modes: int):
     """(FP64 passes, FP32 passes) of the mixed substep for this box."""
-    f64 = min(MIXED_MANIFEST["div_phi_fp64_modes"], cfg.nz2 + 1) / (cfg.nz2 + 1)
+    f64 = min(fp64_modes, cfg.nz2 + 1) / (cfg.nz2 + 1)
     dp = MIXED_MANIFEST["div_phi_passes"]
     return (MIXED_MANIFEST["fp64_passes"] + dp * f64, MIXED_MANIFEST["fp32_passes"] + dp * (1 - f64))
+
+
+def mixed_substep_bytes(cfg, fp64_modes: int) -> float:
+    f64, f32 = mixed_passes(cfg, fp64_modes)
+    return (f64 + f32 / 2.0) * cfg.nx * (cfg.ny + 1) * cfg.nz1 * 8.0
 
 
 def algorithmic_bytes(cfg) -> dict:
@@ -93,7 +112,6 @@ def algorithmic_bytes(cfg) -> dict:
         "pois_bwd": 2 * V,
         "project": V + 2 * (2 * U + 2 * V),
         "substep_survey": 55.0 * U,
-        "substep_mixed": (mixed_passes(cfg)[0] + mixed_passes(cfg)[1] / 2.0) * U,
     }
 
 
@@ -339,10 +357,40 @@ def run_serve(device, args, ens):
     return out
 
 
-def run_mixed(cfg, init, coef, fbox, device, R, warm, K, fp64_ms_per_step):
+def time_mixed_box(mcfg, init, coef, device, R, warm, K):
+    """Device time (ms) of K RK3 steps after `warm` of a mixed-path box, and
+    its per-kernel-class ms per substep from one profiled step."""
+    import torch
+    b = Box(mcfg, init, coef, device=device)
+    b.autotune()
+    stream = torch.cuda.ExternalStream(b.stream, device=f"cuda:{device}")
+    for _ in range(warm):
+        b.advance(1)
+    b.sync()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    replicas.barrier(R)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(K):
+        b.advance(1)
+    ev1.record(stream)
+    ev1.synchronize()
+    ms = replicas.max_over_ranks(ev0.elapsed_time(ev1), R)
+    b.profile(True)
+    b.advance(1)
+    prof = b.profile_read()
+    b.profile(False)
+    b.close()
+    return ms, {k: round(v[0] / 3.0, 4) for k, v in prof.items()}
+
+
+def run_mixed(cfg, init, coef, fbox, device, R, warm, K, fp64_ms_per_step, ydense=True):
     """The mixed-precision path (OTBL_PREC_MIXED) on the same box: device
     time of K RK3 steps after `warm`, then its error against the FP64 path
-    after the same steps from the same initial state."""
+    after the same steps from the same initial state. With `ydense`, the
+    same path with interpyy as a dense operator on the tensor cores
+    (OTBL_OPT_YDENSE) is timed beside it."""
     import torch
     mcfg = cfgmod.replace(cfg, precision=1)
     mbox = Box(mcfg, init, coef, device=device)
@@ -372,7 +420,8 @@ def run_mixed(cfg, init, coef, fbox, device, R, warm, K, fp64_ms_per_step):
     mbox.profile(False)
     per_sub = {k: round(v[0] / 3.0, 4) for k, v in sorted(prof.items(), key=lambda t: -t[1][0])}
     peak, peak_kind = peaks()
-    ab = algorithmic_bytes(cfg)
+    kf64 = pois_fp64_modes(cfg, coef)
+    mbytes = mixed_substep_bytes(cfg, kf64)
     sub_s = ms / sub / 1e3
     # error against the FP64 path after the same number of steps
     nsteps = warm + K + 1
@@ -380,16 +429,23 @@ def run_mixed(cfg, init, coef, fbox, device, R, warm, K, fp64_ms_per_step):
     fbox.advance(nsteps)
     err = diag.compare(cfg, coef, mbox, fbox)
     mbox.close()
+    dense = None
+    if ydense and cfg.ny <= 256:
+        dms, dprof = time_mixed_box(cfgmod.replace(mcfg, options=1), init, coef, device, R, warm, K)
+        dense = {"ms_per_step": dms / K, "interpy_ms_per_substep": dprof.get("interpy"),
+                 "banded_interpy_ms_per_substep": per_sub.get("interpy"),
+                 "kernel": "k_ydense (tcgen05.mma kind::tf32, 3 products of the split operands)"}
     return {"value": value, "unit": UNIT, "ms_per_step": ms / K, "dtype": "f32 operators, f64 state",
             "speedup_vs_fp64": (fp64_ms_per_step / (ms / K)),
-            "substep_roofline": {"bytes_per_substep": ab["substep_mixed"],
-                                 "manifest": dict(MIXED_MANIFEST, passes_fp64_fp32=mixed_passes(cfg)),
-                                 "achieved": ab["substep_mixed"] / sub_s / 1e9, "peak": peak,
-                                 "unit": "GB/s", "frac": ab["substep_mixed"] / sub_s / 1e9 / peak,
+            "substep_roofline": {"bytes_per_substep": mbytes,
+                                 "manifest": dict(MIXED_MANIFEST, div_phi_fp64_modes=kf64,
+                                                  passes_fp64_fp32=mixed_passes(cfg, kf64)),
+                                 "achieved": mbytes / sub_s / 1e9, "peak": peak,
+                                 "unit": "GB/s", "frac": mbytes / sub_s / 1e9 / peak,
                                  "peak_kind": peak_kind},
             "kernels_ms_per_substep": per_sub,
             "err_vs_fp64": dict(steps=nsteps, **err), "clocks": clk.summary(),
-            "autotuned_cta_sizes": list(mtuned)}
+            "autotuned_cta_sizes": list(mtuned), "dense_interpyy": dense}
 
 
 def main():
@@ -402,6 +458,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-ydense", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--ensemble-steps", type=int, default=10)
     ap.add_argument("--no-serve", action="store_true")
@@ -513,7 +570,7 @@ def main():
 
     mixed = None
     if not args.no_mixed:
-        mixed = run_mixed(cfg, init, coef, box, local, R, warm, K, ms / K)
+        mixed = run_mixed(cfg, init, coef, box, local, R, warm, K, ms / K, ydense=not args.no_ydense)
 
     ens = None
     if not args.no_ensemble:

@@ -16,24 +16,41 @@
 // tcgen05.mma of kind::tf32) accumulate in FP32 in tensor memory, which gives
 // the FP32 accuracy of the mixed path's other operators.
 //
-// Kernel: persistent, one CTA of 128 threads per SM, tiles of N = 256
-// columns, both M-tiles of 128 output rows (TMEM columns 0..255 and
-// 256..511). K runs in chunks of 16 input rows through two shared-memory
-// stages: the operator chunk (both M-tiles, both parts, 32 KB, stored in
-// global memory in the canonical K-major layout) arrives by one bulk copy
-// (cp.async.bulk, no tensor map, no multicast), the field chunk (16 rows x
-// 256 columns, FP64) is loaded, split and written by the threads in the
-// canonical K-major layout too, i.e. transposed on the way into shared
-// memory. (The field's natural order would be the MN-major operand form, but
-// kind::tf32 with B MN-major, no swizzle, left the accumulators at zero on
-// B200 in a one-MMA probe, while the K-major form was exact.) Thread 0 issues
-// the MMAs and commits each stage to
-// an mbarrier that releases it. Chunks in which an M-tile's rows of Mop are
-// below 2^-40 of its largest entry (the inverse of the diagonally dominant
-// tridiagonal decays geometrically away from the diagonal) are skipped for
-// that M-tile. The epilogue reads the accumulators (tcgen05.ld) and stores
-// FP32. Every wait is bounded: on a timeout the CTA records
-// OTBL_ERR_TIMEOUT, stops, frees its tensor memory and returns.
+// Kernel: persistent, one CTA per SM, warp-specialised. A tile is one
+// plane i and NT consecutive spanwise columns kr (NT a multiple of 16, at
+// most 128, chosen so that nb = ceil(nz1/NT) tiles cover a plane); both
+// M-tiles of 128 output rows accumulate in tensor memory, in one of two
+// accumulator sets of 256 columns (set a: columns 256a + mt*NT ...), so that
+// the epilogue of one tile overlaps the MMAs of the next. K runs in chunks of
+// 16 input rows:
+//   warp 0, one lane: the field producer. Per chunk, a 3D TMA box of the
+//     FP64 field (NT columns x 16 rows x 1 plane; columns past nz1 and rows
+//     past K read as zero) into a ring of SF slots, which the converters
+//     release as soon as they have read it, so that many boxes are in flight.
+//   warp 10, one lane: the operator producer. Per chunk, the operator chunk
+//     (stored in global memory in the canonical K-major layout, 16 KB per
+//     M-tile for both parts; an M-tile's part only in the chunks of its band)
+//     by bulk copies (no tensor map) into a ring of SA slots, which the MMA
+//     completion releases. No multicast anywhere.
+//   warps 1-4: converters. Each FP64 value is split into hi/lo TF32 and
+//     written to one of NB operand buffers in the canonical K-major layout,
+//     i.e. transposed on the way. (The field's natural order would be the
+//     MN-major operand form, but kind::tf32 with B MN-major, no swizzle, left
+//     the accumulators at zero on B200 in a one-MMA probe, while the K-major
+//     form was exact.)
+//   warp 5, one lane: issues the MMAs and commits each chunk to the
+//     mbarriers that release its operator slot and operand buffer, and each
+//     tile to the one the epilogue waits on.
+//   warps 6-9: the epilogue, one TMEM lane quadrant each: tcgen05.ld of the
+//     accumulators, FP32 stores, then the tile's accumulator set is released.
+// Chunks in which an M-tile's rows of Mop are below 2^-40 of its largest
+// entry (the inverse of the diagonally dominant tridiagonal decays
+// geometrically away from the diagonal) are skipped for that M-tile. Every
+// wait is bounded: on a timeout the CTA records OTBL_ERR_TIMEOUT, every role
+// stops, the MMAs and copies in flight are waited for (bounded again), the
+// tensor memory is freed and the CTA returns.
+#include <cudaTypedefs.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -47,17 +64,23 @@ namespace otbl {
 
 namespace {
 
-constexpr int YD_N = 256;                      // columns per tile
 constexpr int YD_KC = 16;                      // input rows per K-chunk
-constexpr int YD_THREADS = 128;
+constexpr int YD_WARPS = 11;                   // 2 producers, 4 converters, MMA, 4 epilogue
+constexpr int YD_THREADS = 32 * YD_WARPS;
 constexpr int YD_A_PART = 128 * YD_KC * 4;     // one M-tile, one part: 8 KB
 constexpr int YD_A_CHUNK = 4 * YD_A_PART;      // 2 M-tiles x 2 parts: 32 KB
-constexpr int YD_B_PART = YD_N * YD_KC * 4;    // 16 KB
-constexpr int YD_B_CHUNK = 2 * YD_B_PART;      // hi, lo: 32 KB
-constexpr int YD_STAGE = YD_A_CHUNK + YD_B_CHUNK;
-constexpr int YD_SMEM = 2 * YD_STAGE + 2048;   // two stages, barriers, alignment slack
+constexpr int YD_SMEM_MAX = 227 * 1024;
+constexpr int YD_SA = 2;                       // operator ring slots
+constexpr int YD_NBUF = 4;                     // operand buffers (hi and lo parts)
+constexpr int YD_MAX_SF = 8;                   // field ring slots, at most
 constexpr uint32_t YD_TMEM_COLS = 512;
 constexpr uint64_t YD_WAIT_NS = 2000000000ull;  // 2 s
+
+// bytes of one field box and of one operand buffer (hi and lo parts) for
+// tiles of nt columns
+__host__ __device__ constexpr int yd_fp_bytes(int nt) { return nt * YD_KC * 8; }
+__host__ __device__ constexpr int yd_bbuf_bytes(int nt) { return 2 * nt * YD_KC * 4; }
+constexpr int YD_BAR_BYTES = 1024;
 
 // canonical K-major, no swizzle: element (m, k) of one M-tile part, k < 16
 __host__ __device__ constexpr int yd_a_off(int m, int k) {
@@ -68,7 +91,7 @@ __host__ __device__ constexpr int yd_b_off(int n, int k) {
   return (n & 7) * 16 + (n >> 3) * (YD_KC / 4 * 128) + (k >> 2) * 128 + (k & 3) * 4;
 }
 static_assert(yd_a_off(127, 15) + 4 == YD_A_PART, "A part layout");
-static_assert(yd_b_off(255, 15) + 4 == YD_B_PART, "B part layout");
+static_assert(yd_b_off(255, 15) + 4 == 256 * YD_KC * 4, "B part layout");
 
 // shared-memory matrix descriptor (sm_100): start, LBO, SBO in 16-byte
 // units, version 1, no swizzle
@@ -77,7 +100,7 @@ __device__ __forceinline__ uint64_t yd_desc(uint32_t saddr, uint32_t lbo, uint32
          ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
 }
 // instruction descriptor, kind::tf32: F32 accumulator, A and B K-major
-constexpr uint32_t yd_idesc(int M, int N) {
+__host__ __device__ constexpr uint32_t yd_idesc(int M, int N) {
   return (1u << 4) | (2u << 7) | (2u << 10) | (0u << 15) | (0u << 16) | ((uint32_t)(N >> 3) << 17) |
          ((uint32_t)(M >> 4) << 24);
 }
@@ -117,28 +140,73 @@ __device__ __forceinline__ void yd_tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) 
 
 }  // namespace
 
-struct YDenseField {
-  const double *in;  // K rows per plane
-  float *out;        // ny rows per plane
-  const uint32_t *op;  // operator chunks: [chunk][mt][part][YD_A_PART bytes]
-  int K;             // input rows per plane
-  int kb[2], ke[2];  // per M-tile, the chunks [kb, ke) that carry its band
-};
 struct YDenseArgs {
-  YDenseField f[3];
-  int nchunk;        // K-chunks (ceil(max K / 16))
-  int tiles;         // tiles per field
+  float *out[3];          // u, w, v interpolants, ny rows per plane
+  const uint32_t *op[3];  // each field's operator chunks: [chunk][mt][part][YD_A_PART bytes]
+  int kb[3][2], ke[3][2];  // per field and M-tile, the chunks [kb, ke) that carry its band
+  int c0[3], c1[3];       // per field, the chunks a tile runs through
+  int nt, nb, sf;         // tile columns, tiles per plane, field ring slots
+  int tiles;              // tiles per field: nx * nb
 };
 
-__global__ void __launch_bounds__(YD_THREADS, 1) k_ydense(int nx, int ny, int nz1, YDenseArgs a, int *err) {
+namespace {
+// the smem of the CTA, from a 1024-byte aligned base: SA operator slots, SF
+// field slots, YD_NBUF operand buffers (hi part, lo part), the barriers
+struct YdSmem {
+  unsigned char *base;
+  int nt, sf;
+  __device__ unsigned char *op(int s) const { return base + (size_t)s * YD_A_CHUNK; }
+  __device__ unsigned char *fp(int s) const { return op(YD_SA) + (size_t)s * yd_fp_bytes(nt); }
+  __device__ unsigned char *bb(int b) const { return fp(sf) + (size_t)b * yd_bbuf_bytes(nt); }
+  __device__ uint64_t *bars() const { return reinterpret_cast<uint64_t *>(bb(YD_NBUF)); }
+};
+// barrier slots
+enum {
+  YB_FPFULL = 0,                       // [YD_MAX_SF] field box landed (TMA bytes)
+  YB_FPEMPTY = YB_FPFULL + YD_MAX_SF,  // [YD_MAX_SF] converters read it (128 arrivals)
+  YB_OPFULL = YB_FPEMPTY + YD_MAX_SF,  // [YD_SA] operator chunk landed
+  YB_OPEMPTY = YB_OPFULL + YD_SA,      // [YD_SA] its MMAs completed
+  YB_BFULL = YB_OPEMPTY + YD_SA,       // [YD_NBUF] operand written (128 arrivals)
+  YB_BEMPTY = YB_BFULL + YD_NBUF,      // [YD_NBUF] its MMAs completed
+  YB_TFULL = YB_BEMPTY + YD_NBUF,      // [2] accumulator set complete
+  YB_TEMPTY = YB_TFULL + 2,            // [2] accumulator set read (128 arrivals)
+  YB_DRAIN = YB_TEMPTY + 2,
+  YB_COUNT
+};
+
+__device__ __forceinline__ bool yd_wait(uint64_t *bar, unsigned parity, volatile int *abort_flag, int *err) {
+  if (*abort_flag) return false;
+  if (mbar_wait_bounded(bar, parity, YD_WAIT_NS)) return true;
+  atomicExch(err, OTBL_ERR_TIMEOUT);
+  *abort_flag = 1;
+  return false;
+}
+__device__ __forceinline__ void yd_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+// after a timeout: the copies this thread issued into a ring of n slots
+// (issued = how many) land before the CTA leaves
+__device__ void yd_drain_ring(uint64_t *full, int n, unsigned issued) {
+  for (int s = 0; s < n; ++s) {
+    if (issued <= (unsigned)s) continue;
+    const unsigned last = issued - 1 - (unsigned)(((int)((issued - 1) % n) - s + n) % n);  // last q, q % n == s
+    mbar_wait_bounded(&full[s], (last / n) & 1, YD_WAIT_NS);
+  }
+}
+}  // namespace
+
+__global__ void __launch_bounds__(YD_THREADS, 1)
+    k_ydense(int nx, int ny, int nz1, YDenseArgs a, int *err, const __grid_constant__ YDenseMaps maps) {
   extern __shared__ __align__(1024) unsigned char ydsm[];
-  unsigned char *base = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(ydsm) + 1023) & ~(uintptr_t)1023);
-  uint64_t *bar_full = reinterpret_cast<uint64_t *>(base + 2 * YD_STAGE);  // [2]
-  uint64_t *bar_done = bar_full + 2;                                       // [2]
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bar_done + 2);
-  int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
+  YdSmem sm;
+  sm.base = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(ydsm) + 1023) & ~(uintptr_t)1023);
+  sm.nt = a.nt;
+  sm.sf = a.sf;
+  uint64_t *bar = sm.bars();
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bar + YB_COUNT);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
-  const long C = (long)nx * nz1;
+  const int NT = a.nt, SF = a.sf, total = 3 * a.tiles;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tmem_slot)),
@@ -146,11 +214,24 @@ __global__ void __launch_bounds__(YD_THREADS, 1) k_ydense(int nx, int ny, int nz
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
   }
-  if (t == 0) {
-    for (int s = 0; s < 2; ++s) {
-      mbar_init(&bar_full[s], 1);
-      mbar_init(&bar_done[s], 1);
+  if (t == 32) {
+    for (int s = 0; s < YD_MAX_SF; ++s) {
+      mbar_init(&bar[YB_FPFULL + s], 1);
+      mbar_init(&bar[YB_FPEMPTY + s], 128);
     }
+    for (int s = 0; s < YD_SA; ++s) {
+      mbar_init(&bar[YB_OPFULL + s], 1);
+      mbar_init(&bar[YB_OPEMPTY + s], 1);
+    }
+    for (int b = 0; b < YD_NBUF; ++b) {
+      mbar_init(&bar[YB_BFULL + b], 128);
+      mbar_init(&bar[YB_BEMPTY + b], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&bar[YB_TFULL + b], 1);
+      mbar_init(&bar[YB_TEMPTY + b], 128);
+    }
+    mbar_init(&bar[YB_DRAIN], 1);
     *abort_flag = 0;
     mbar_init_fence();
   }
@@ -158,139 +239,181 @@ __global__ void __launch_bounds__(YD_THREADS, 1) k_ydense(int nx, int ny, int nz
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   const uint32_t tmem = *tmem_slot;
-  constexpr uint32_t IDESC = yd_idesc(128, YD_N);
 
-  unsigned fills[2] = {0u, 0u};  // completed uses of each stage
-  int stage = 0;
-  const int total = 3 * a.tiles;
-  for (int tile = blockIdx.x; tile < total && !*abort_flag; tile += gridDim.x) {
-    const int fi = tile / a.tiles;
-    const YDenseField F = a.f[fi];
-    const long c0 = (long)(tile - fi * a.tiles) * YD_N;
-    const int nchunk = (F.K + YD_KC - 1) / YD_KC;
-    for (int kc = 0; kc < nchunk; ++kc) {
-      const int s = stage;
-      unsigned char *sa = base + s * YD_STAGE, *sb = sa + YD_A_CHUNK;
-      // the stage's previous MMAs must have read it before it is refilled
-      if (fills[s] > 0 && !mbar_wait_bounded(&bar_done[s], (fills[s] - 1) & 1, YD_WAIT_NS)) {
-        if (t == 0) {
-          atomicExch(err, OTBL_ERR_TIMEOUT);
-          *abort_flag = 1;
+  if (warp == 0) {
+    // ---- field producer ----
+    if (lane == 0) {
+      unsigned q = 0;
+      bool ok = true;
+      for (int tile = blockIdx.x; tile < total && ok && !*abort_flag; tile += gridDim.x) {
+        const int fi = tile / a.tiles, rem = tile - fi * a.tiles, i = rem / a.nb, b = rem - i * a.nb;
+        for (int kc = a.c0[fi]; kc < a.c1[fi]; ++kc, ++q) {
+          const int s = (int)(q % SF);
+          if (q >= (unsigned)SF && !yd_wait(&bar[YB_FPEMPTY + s], ((q / SF) - 1) & 1, abort_flag, err)) {
+            ok = false;
+            break;
+          }
+          mbar_arrive_expect_tx(&bar[YB_FPFULL + s], yd_fp_bytes(NT));
+          tma_load_3d(sm.fp(s), &maps.g[fi], b * NT, kc * YD_KC, i, &bar[YB_FPFULL + s]);
         }
       }
-      __syncthreads();
-      if (*abort_flag) break;
-      if (t == 0) {
-        mbar_arrive_expect_tx(&bar_full[s], YD_A_CHUNK);
-        yd_bulk_g2s(sa, reinterpret_cast<const unsigned char *>(F.op) + (size_t)kc * YD_A_CHUNK, YD_A_CHUNK,
-                    &bar_full[s]);
+      yd_drain_ring(&bar[YB_FPFULL], SF, q);
+    }
+  } else if (warp == 10) {
+    // ---- operator producer ----
+    if (lane == 0) {
+      unsigned q = 0;
+      bool ok = true;
+      for (int tile = blockIdx.x; tile < total && ok && !*abort_flag; tile += gridDim.x) {
+        const int fi = tile / a.tiles;
+        for (int kc = a.c0[fi]; kc < a.c1[fi]; ++kc, ++q) {
+          const int s = (int)(q % YD_SA);
+          if (q >= (unsigned)YD_SA && !yd_wait(&bar[YB_OPEMPTY + s], ((q / YD_SA) - 1) & 1, abort_flag, err)) {
+            ok = false;
+            break;
+          }
+          const bool m0 = kc >= a.kb[fi][0] && kc < a.ke[fi][0], m1 = kc >= a.kb[fi][1] && kc < a.ke[fi][1];
+          const unsigned char *opc = reinterpret_cast<const unsigned char *>(a.op[fi]) + (size_t)kc * YD_A_CHUNK;
+          if (m0 || m1) {
+            mbar_arrive_expect_tx(&bar[YB_OPFULL + s], (m0 + m1) * (YD_A_CHUNK / 2));
+            if (m0) yd_bulk_g2s(sm.op(s), opc, YD_A_CHUNK / 2, &bar[YB_OPFULL + s]);
+            if (m1) yd_bulk_g2s(sm.op(s) + YD_A_CHUNK / 2, opc + YD_A_CHUNK / 2, YD_A_CHUNK / 2, &bar[YB_OPFULL + s]);
+          } else {
+            yd_arrive(&bar[YB_OPFULL + s]);  // no part of this chunk is used
+          }
+        }
       }
-      // the field chunk: rows k0..k0+15 x 256 columns, split into hi/lo.
-      // Item e = (column n = e % 256, rows k0+4g..k0+4g+3, g = e / 256): four
-      // loads of one column (a warp reads 32 consecutive columns of a row),
-      // one 16-byte store per part (8 consecutive lanes fill the 8 rows of a
-      // core matrix: conflict-free).
-      const int k0 = kc * YD_KC;
-      for (int e = t; e < YD_N * (YD_KC / 4); e += YD_THREADS) {
-        const int n = e & (YD_N - 1), g = e / YD_N;
-        const long cidx = c0 + n;
-        const bool col_ok = cidx < C;
-        const long i = col_ok ? cidx / nz1 : 0, kr = col_ok ? cidx - i * nz1 : 0;
-        uint32_t hi[4], lo[4];
+      yd_drain_ring(&bar[YB_OPFULL], YD_SA, q);
+    }
+  } else if (warp <= 4) {
+    // ---- converters: FP64 box -> hi/lo TF32, K-major ----
+    const int ct = t - 32;
+    unsigned q = 0;
+    bool ok = true;
+    for (int tile = blockIdx.x; tile < total && ok && !*abort_flag; tile += gridDim.x) {
+      const int fi = tile / a.tiles;
+      for (int kc = a.c0[fi]; kc < a.c1[fi]; ++kc, ++q) {
+        const int s = (int)(q % SF), bs = (int)(q % YD_NBUF);
+        if (!yd_wait(&bar[YB_FPFULL + s], (q / SF) & 1, abort_flag, err) ||
+            (q >= YD_NBUF && !yd_wait(&bar[YB_BEMPTY + bs], ((q / YD_NBUF) - 1) & 1, abort_flag, err))) {
+          ok = false;
+          break;
+        }
+        const double *fp = reinterpret_cast<const double *>(sm.fp(s));
+        unsigned char *hi = sm.bb(bs), *lo = hi + NT * YD_KC * 4;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const int j = k0 + 4 * g + q;
-          const double x = (col_ok && j < F.K) ? F.in[((size_t)i * F.K + j) * nz1 + kr] : 0.0;
-          hi[q] = yd_tf32((float)x);
-          lo[q] = yd_tf32((float)(x - (double)__uint_as_float(hi[q])));
-        }
-        const int off = yd_b_off(n, 4 * g);
-        *reinterpret_cast<uint4 *>(sb + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-        *reinterpret_cast<uint4 *>(sb + YD_B_PART + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+        for (int g = 0; g < YD_KC / 4; ++g)
+          for (int n = ct; n < NT; n += 128) {
+            uint32_t h[4], l[4];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+              const double x = fp[(size_t)(4 * g + r) * NT + n];
+              h[r] = yd_tf32((float)x);
+              l[r] = yd_tf32((float)(x - (double)__uint_as_float(h[r])));
+            }
+            const int off = yd_b_off(n, 4 * g);
+            *reinterpret_cast<uint4 *>(hi + off) = make_uint4(h[0], h[1], h[2], h[3]);
+            *reinterpret_cast<uint4 *>(lo + off) = make_uint4(l[0], l[1], l[2], l[3]);
+          }
+        yd_arrive(&bar[YB_FPEMPTY + s]);  // the box has been read
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        yd_arrive(&bar[YB_BFULL + bs]);
       }
-      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-      __syncthreads();
-      if (t == 0) {
-        if (!mbar_wait_bounded(&bar_full[s], fills[s] & 1, YD_WAIT_NS)) {
-          atomicExch(err, OTBL_ERR_TIMEOUT);
-          *abort_flag = 1;
-        } else {
+    }
+  } else if (warp == 5) {
+    // ---- MMA issue ----
+    if (lane == 0) {
+      const uint32_t idesc = yd_idesc(128, NT);
+      unsigned q = 0, tl = 0;
+      bool ok = true;
+      for (int tile = blockIdx.x; tile < total && ok && !*abort_flag; tile += gridDim.x, ++tl) {
+        const int fi = tile / a.tiles, ab = (int)(tl & 1);
+        if (tl >= 2 && !yd_wait(&bar[YB_TEMPTY + ab], ((tl >> 1) - 1) & 1, abort_flag, err)) break;
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        for (int kc = a.c0[fi]; kc < a.c1[fi]; ++kc, ++q) {
+          const int so = (int)(q % YD_SA), bs = (int)(q % YD_NBUF);
+          if (!yd_wait(&bar[YB_OPFULL + so], (q / YD_SA) & 1, abort_flag, err) ||
+              !yd_wait(&bar[YB_BFULL + bs], (q / YD_NBUF) & 1, abort_flag, err)) {
+            ok = false;
+            break;
+          }
           asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-          const uint32_t sa_u = smem_u32(sa), sb_u = smem_u32(sb);
+          const uint32_t sa_u = smem_u32(sm.op(so)), sb_u = smem_u32(sm.bb(bs));
 #pragma unroll
           for (int mt = 0; mt < 2; ++mt) {
-            if (kc < F.kb[mt] || kc >= F.ke[mt]) continue;
-            const uint32_t d = tmem + (uint32_t)(mt * YD_N);
+            if (kc < a.kb[fi][mt] || kc >= a.ke[fi][mt]) continue;
+            const uint32_t d = tmem + (uint32_t)(ab * 256 + mt * NT);
 #pragma unroll
             for (int ks = 0; ks < YD_KC / 8; ++ks) {
               const uint32_t ah = sa_u + (uint32_t)((mt * 2 + 0) * YD_A_PART + ks * 256);
               const uint32_t al = sa_u + (uint32_t)((mt * 2 + 1) * YD_A_PART + ks * 256);
-              const uint32_t bh = sb_u + (uint32_t)(ks * 256);
-              const uint32_t bl = bh + YD_B_PART;
+              const uint32_t bh = sb_u + (uint32_t)(ks * 256), bl = bh + (uint32_t)(NT * YD_KC * 4);
               const uint64_t dah = yd_desc(ah, 128, YD_KC / 4 * 128), dal = yd_desc(al, 128, YD_KC / 4 * 128);
               const uint64_t dbh = yd_desc(bh, 128, YD_KC / 4 * 128), dbl = yd_desc(bl, 128, YD_KC / 4 * 128);
-              const uint32_t first = (kc == F.kb[mt] && ks == 0) ? 0u : 1u;
-              yd_mma(d, dah, dbh, IDESC, first);
-              yd_mma(d, dah, dbl, IDESC, 1u);
-              yd_mma(d, dal, dbh, IDESC, 1u);
+              const uint32_t first = (kc == a.kb[fi][mt] && ks == 0) ? 0u : 1u;
+              yd_mma(d, dah, dbh, idesc, first);
+              yd_mma(d, dah, dbl, idesc, 1u);
+              yd_mma(d, dal, dbh, idesc, 1u);
             }
           }
-          yd_commit(&bar_done[s]);
+          yd_commit(&bar[YB_OPEMPTY + so]);
+          yd_commit(&bar[YB_BEMPTY + bs]);
+        }
+        if (!ok) break;
+        yd_commit(&bar[YB_TFULL + ab]);
+      }
+      // every MMA issued has completed before the tensor memory is freed
+      yd_commit(&bar[YB_DRAIN]);
+      mbar_wait_bounded(&bar[YB_DRAIN], 0, YD_WAIT_NS);
+    }
+  } else {
+    // ---- epilogue: TMEM lane quadrant (warp % 4) ----
+    const int qd = warp & 3;
+    const bool vec4 = (nz1 & 3) == 0;
+    unsigned tl = 0;
+    for (int tile = blockIdx.x; tile < total && !*abort_flag; tile += gridDim.x, ++tl) {
+      const int fi = tile / a.tiles, rem = tile - fi * a.tiles, i = rem / a.nb, b = rem - i * a.nb;
+      const int ab = (int)(tl & 1);
+      if (!yd_wait(&bar[YB_TFULL + ab], (tl >> 1) & 1, abort_flag, err)) break;
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+      float *out = a.out[fi];
+#pragma unroll 1
+      for (int mt = 0; mt < 2; ++mt) {
+        const int r = mt * 128 + qd * 32 + lane;  // output row, 0-based
+        const bool band = a.ke[fi][mt] > a.kb[fi][mt];
+        float *orow = out + ((size_t)i * ny + (r < ny ? r : 0)) * nz1;
+        const uint32_t tbase = tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)(ab * 256 + mt * NT);
+#pragma unroll 1
+        for (int cb = 0; cb < NT; cb += 16) {
+          uint32_t v[16];
+          yd_tmem_ld16(tbase + (uint32_t)cb, v);
+          const int kr0 = b * NT + cb;
+          if (r < ny && kr0 < nz1) {
+            if (vec4) {
+#pragma unroll
+              for (int p = 0; p < 16; p += 4)
+                if (kr0 + p < nz1)
+                  *reinterpret_cast<float4 *>(orow + kr0 + p) =
+                      band ? make_float4(__uint_as_float(v[p]), __uint_as_float(v[p + 1]), __uint_as_float(v[p + 2]),
+                                         __uint_as_float(v[p + 3]))
+                           : make_float4(0.f, 0.f, 0.f, 0.f);
+            } else {
+#pragma unroll
+              for (int p = 0; p < 16; p += 2)
+                if (kr0 + p < nz1)
+                  *reinterpret_cast<float2 *>(orow + kr0 + p) =
+                      band ? make_float2(__uint_as_float(v[p]), __uint_as_float(v[p + 1])) : make_float2(0.f, 0.f);
+            }
+          }
         }
       }
-      fills[s] += 1;
-      stage ^= 1;
+      asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+      yd_arrive(&bar[YB_TEMPTY + ab]);
     }
-    __syncthreads();
-    if (*abort_flag) break;
-    // the last stage's commit covers every MMA of the tile
-    const int sl = stage ^ 1;
-    if (!mbar_wait_bounded(&bar_done[sl], (fills[sl] - 1) & 1, YD_WAIT_NS)) {
-      if (lane == 0) {
-        atomicExch(err, OTBL_ERR_TIMEOUT);
-        *abort_flag = 1;
-      }
-    }
-    __syncthreads();
-    if (*abort_flag) break;
-    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    // epilogue: warp w owns TMEM lanes 32w..32w+31 = output rows
-    for (int mt = 0; mt < 2; ++mt) {
-      const int r = mt * 128 + warp * 32 + lane;  // output row, 0-based
-      for (int cb = 0; cb < YD_N; cb += 16) {
-        uint32_t v[16];
-        yd_tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(mt * YD_N + cb), v);
-        if (r < ny && F.ke[mt] > F.kb[mt]) {
-#pragma unroll
-          for (int p = 0; p < 16; p += 2) {
-            const long cidx = c0 + cb + p;
-            if (cidx < C) {
-              const long i = cidx / nz1, kr = cidx - i * nz1;
-              *reinterpret_cast<float2 *>(F.out + ((size_t)i * ny + r) * nz1 + kr) =
-                  make_float2(__uint_as_float(v[p]), __uint_as_float(v[p + 1]));
-            }
-          }
-        } else if (r < ny) {  // an M-tile without any band: zero rows
-#pragma unroll
-          for (int p = 0; p < 16; p += 2) {
-            const long cidx = c0 + cb + p;
-            if (cidx < C) {
-              const long i = cidx / nz1, kr = cidx - i * nz1;
-              *reinterpret_cast<float2 *>(F.out + ((size_t)i * ny + r) * nz1 + kr) = make_float2(0.f, 0.f);
-            }
-          }
-        }
-      }
-    }
-    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-    __syncthreads();
   }
-  // drain: MMAs that may still be in flight before the memory is freed
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();
-  for (int s = 0; s < 2; ++s)
-    if (fills[s] > 0 && !*abort_flag) mbar_wait_bounded(&bar_done[s], (fills[s] - 1) & 1, YD_WAIT_NS);
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-  __syncthreads();
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(YD_TMEM_COLS) : "memory");
 }
@@ -414,27 +537,81 @@ size_t ydense_bytes(int ny) {
   return 2 * (size_t)nchunk * YD_A_CHUNK;
 }
 
+// tile columns: nb = ceil(nz1/128) tiles per plane of nt = nz1/nb columns
+// rounded up to 16 (the MMA's N); two M-tiles of nt columns make one of the
+// two 256-column accumulator sets
+static void ydense_tiling(int nz1, int *nt, int *nb) {
+  *nb = (nz1 + 127) / 128;
+  *nt = ((nz1 + *nb - 1) / *nb + 15) / 16 * 16;
+}
+
+// field ring slots that fit beside the operator ring and the operand buffers
+static int ydense_field_slots(int nt) {
+  const int room = YD_SMEM_MAX - 1024 - YD_SA * YD_A_CHUNK - YD_NBUF * yd_bbuf_bytes(nt) - YD_BAR_BYTES;
+  return std::min(YD_MAX_SF, room / yd_fp_bytes(nt));
+}
+
+static size_t ydense_smem(int nt, int sf) {
+  return 1024 + (size_t)YD_SA * YD_A_CHUNK + (size_t)sf * yd_fp_bytes(nt) + YD_NBUF * (size_t)yd_bbuf_bytes(nt) +
+         YD_BAR_BYTES;
+}
+
+void *tensor_map_encoder();
+
+bool build_ydense_maps(otbl_ctx *c) {
+  c->yd_maps_ok = false;
+  if (!c->ydense) return false;
+  const int nx = c->cfg.nx, ny = c->cfg.ny, nz1 = c->dc.nz1;
+  ydense_tiling(nz1, &c->yd_nt, &c->yd_nb);
+  auto fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(tensor_map_encoder());
+  if (!fn || (nz1 * 8) % 16 != 0) return false;
+  const double *in[3] = {c->f[OTBL_F_U], c->f[OTBL_F_W], c->f[OTBL_F_V]};
+  const int rows[3] = {ny + 1, ny + 1, ny};
+  for (int f = 0; f < 3; ++f) {
+    if (reinterpret_cast<uintptr_t>(in[f]) % 16 != 0) return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)nz1, (cuuint64_t)rows[f], (cuuint64_t)nx};
+    const cuuint64_t strides[2] = {(cuuint64_t)nz1 * 8, (cuuint64_t)rows[f] * nz1 * 8};
+    const cuuint32_t box[3] = {(cuuint32_t)c->yd_nt, (cuuint32_t)YD_KC, 1};
+    const cuuint32_t es[3] = {1, 1, 1};
+    if (fn(&c->yd_maps.g[f], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double *>(in[f]), dims, strides, box, es,
+           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return false;
+  }
+  c->yd_maps_ok = true;
+  return true;
+}
+
+// false when the dense path cannot run on this context (its TMA descriptors
+// could not be made); the caller then runs the banded interpyy
+bool ydense_ready(const otbl_ctx *c) { return c->ydense && c->yd_maps_ok && c->yd_op; }
+
 cudaError_t launch_interpy_dense(otbl_ctx *c) {
   cudaStream_t s = c->stream;
   const int nx = c->cfg.nx, ny = c->cfg.ny, nz1 = c->dc.nz1;
   YDenseArgs a;
-  const double *ins[3] = {c->f[OTBL_F_U], c->f[OTBL_F_W], c->f[OTBL_F_V]};
   void *outs[3] = {c->w.uy, c->w.wy, c->w.vy};
   const int which[3] = {0, 0, 1};
   for (int f = 0; f < 3; ++f) {
-    YDenseField &F = a.f[f];
-    F.in = ins[f];
-    F.out = static_cast<float *>(outs[f]);
-    F.op = c->yd_op + which[f] * c->yd_words_per_op;
-    F.K = which[f] == 0 ? ny + 1 : ny;
+    a.out[f] = static_cast<float *>(outs[f]);
+    a.op[f] = c->yd_op + which[f] * c->yd_words_per_op;
+    int c0 = 1 << 30, c1 = 0;
     for (int mt = 0; mt < 2; ++mt) {
-      F.kb[mt] = c->yd_kb[which[f]][mt];
-      F.ke[mt] = c->yd_ke[which[f]][mt];
+      a.kb[f][mt] = c->yd_kb[which[f]][mt];
+      a.ke[f][mt] = c->yd_ke[which[f]][mt];
+      if (a.ke[f][mt] > a.kb[f][mt]) {
+        c0 = std::min(c0, a.kb[f][mt]);
+        c1 = std::max(c1, a.ke[f][mt]);
+      }
     }
+    if (c1 == 0) c0 = 0;
+    a.c0[f] = c0;
+    a.c1[f] = c1;
   }
-  a.nchunk = (ny + 1 + YD_KC - 1) / YD_KC;
-  const long C = (long)nx * nz1;
-  a.tiles = (int)((C + YD_N - 1) / YD_N);
+  a.nt = c->yd_nt;
+  a.nb = c->yd_nb;
+  a.sf = ydense_field_slots(a.nt);
+  a.tiles = nx * a.nb;
   static int nsm = 0;
   if (nsm == 0) {
     int dev = 0;
@@ -443,8 +620,9 @@ cudaError_t launch_interpy_dense(otbl_ctx *c) {
     if (nsm <= 0) nsm = 148;
   }
   const int grid = std::min(3 * a.tiles, nsm);
-  cudaFuncSetAttribute(k_ydense, cudaFuncAttributeMaxDynamicSharedMemorySize, YD_SMEM);
-  k_ydense<<<grid, YD_THREADS, YD_SMEM, s>>>(nx, ny, nz1, a, &c->st->err);
+  const size_t smem = ydense_smem(a.nt, a.sf);
+  cudaFuncSetAttribute(k_ydense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_ydense<<<grid, YD_THREADS, smem, s>>>(nx, ny, nz1, a, &c->st->err, c->yd_maps);
   c->launches += 1;
   return cudaGetLastError();
 }

@@ -1027,7 +1027,7 @@ cudaError_t launch_interpy(otbl_ctx *c) {
   }
   const int ncol = c->cfg.nx * c->dc.nz1;
   prof_begin(c, PK_INTERPY);
-  if (c->ydense) {
+  if (ydense_ready(c)) {
     const cudaError_t e = launch_interpy_dense(c);
     prof_end(c);
     return e;

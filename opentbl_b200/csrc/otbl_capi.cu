@@ -289,6 +289,7 @@ extern "C" int otbl_ctx_create(const otbl_config *cfg, const double *coef, int d
     *out = c;
     return OTBL_ERR_CUDA;
   }
+  if (c->ydense && !getenv("OTBL_NO_TMA")) build_ydense_maps(c);
   if (check(c, launch_twiddles(c), "twiddles") != OTBL_OK || check(c, launch_pois_lu(c), "pois_lu") != OTBL_OK ||
       check(c, launch_x_rows(c), "x rows") != OTBL_OK || check(c, launch_y_rows(c), "y rows") != OTBL_OK ||
       check(c, cudaStreamSynchronize(c->stream), "init")) {
@@ -667,6 +668,7 @@ static int bind_fields(otbl_ctx *c, double *const *ptr, const bool *use) {
     build_final_maps(c);
     build_x_maps(c);
     build_y_maps(c);
+    build_ydense_maps(c);
   }
   return OTBL_OK;
 }

@@ -94,6 +94,12 @@ struct XMaps {
   CUtensorMap g[3], u[3], r[3];
 };
 
+// TMA descriptors of the dense interpyy's inputs (u, w, v): [nx][rows][nz1]
+// FP64, boxes of nt spanwise columns x 16 rows x 1 plane
+struct YDenseMaps {
+  CUtensorMap g[3];
+};
+
 }  // namespace otbl
 
 struct otbl_ctx {
@@ -113,14 +119,18 @@ struct otbl_ctx {
   // [0] k_interpx, [1] k_difvisx, [2] k_interpy (one thread per line, so the
   // choice changes the schedule, never the arithmetic)
   int tune_bs[3] = {128, 128, 128};
-  // interpyy of the mixed path as a dense operator on the tensor cores
-  // (OTBL_OPT_YDENSE, k_ydense.cu): the operators' TF32 chunks on the device
-  // and, per input type and M-tile, the K-chunks [kb, ke) of their band
   int pois_klo = 0;  // mixed path: spanwise modes k < pois_klo solve in FP64 (kPoisCond)
+  // interpyy of the mixed path as a dense operator on the tensor cores
+  // (OTBL_OPT_YDENSE, k_ydense.cu): the operators' TF32 chunks on the device,
+  // per input type and M-tile the K-chunks [kb, ke) of their band, the
+  // tiles' column count and the inputs' TMA descriptors
   bool ydense = false;
   uint32_t *yd_op = nullptr;
   size_t yd_words_per_op = 0;
   int yd_kb[2][2] = {{0, 0}, {0, 0}}, yd_ke[2][2] = {{0, 0}, {0, 0}};
+  int yd_nt = 0, yd_nb = 0;
+  otbl::YDenseMaps yd_maps;
+  bool yd_maps_ok = false;
   // TMA descriptors of the rhsp tail's inputs, per velocity component
   otbl::FinalMaps fmaps[3];
   bool fmaps_ok = false;
@@ -235,6 +245,8 @@ cudaError_t launch_round_f32(otbl_ctx *c, const double *in, float *out, size_t n
 // interpyy on the tensor cores (k_ydense.cu)
 cudaError_t ydense_prepare(otbl_ctx *c);
 cudaError_t launch_interpy_dense(otbl_ctx *c);
+bool build_ydense_maps(otbl_ctx *c);
+bool ydense_ready(const otbl_ctx *c);
 size_t ydense_bytes(int ny);
 // standalone pieces
 cudaError_t launch_chp2x(otbl_ctx *c, const double *plan, double *pen, int jee, int to_pen);

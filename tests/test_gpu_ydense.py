@@ -43,8 +43,11 @@ def _oracle_interpyy(cfg, o, fld, which):
     return out
 
 
-@pytest.mark.parametrize("name", ["TINY", "C1"])
+@pytest.mark.parametrize("name", ["TINY", "SMALL", "C1", "SLAB"])
 def test_ydense_interpolants_against_oracle(name):
+    """TINY, C1: one tile per plane (32 and 96 columns); SMALL: nz1 = 42,
+    not a multiple of 4; SLAB (257x193x512): two tiles of 176 columns per
+    plane, the second partly past nz1 = 340, and two M-tiles (ny = 193)."""
     cfg = getattr(config, name)
     init, coef = setup(cfg)
     g = Box(_dense(cfg), init, coef)
