@@ -195,7 +195,8 @@ def workload_config(cfg, ws):
     """The `config` of both arms' JSON lines (identical by construction)."""
     nz1 = 2 * (cfg.nz // 3)
     state = 8.0 * cfg.nx * nz1 * (4 * (cfg.ny + 1) + 3 * cfg.ny)
-    return {"workload": f"rk3_substep {cfg.name} fp64", "nx": cfg.nx, "ny": cfg.ny,
+    prec = "fp64" if getattr(cfg, "precision", 0) == 0 else "mixed"
+    return {"workload": f"rk3_substep {cfg.name} {prec}", "nx": cfg.nx, "ny": cfg.ny,
             "nz": cfg.nz, "substeps_per_step": 3,
             "l2": "inputs larger than L2 (state %.1f GB per box)" % (state / 1e9),
             "parallelism": f"replicas{ws}"}
@@ -357,12 +358,13 @@ def run_serve(device, args, ens):
     return out
 
 
-def time_mixed_box(mcfg, init, coef, device, R, warm, K):
+def time_mixed_box(mcfg, init, coef, device, R, warm, K, tune=True):
     """Device time (ms) of K RK3 steps after `warm` of a mixed-path box, and
     its per-kernel-class ms per substep from one profiled step."""
     import torch
     b = Box(mcfg, init, coef, device=device)
-    b.autotune()
+    if tune:
+        b.autotune()
     stream = torch.cuda.ExternalStream(b.stream, device=f"cuda:{device}")
     for _ in range(warm):
         b.advance(1)
@@ -385,7 +387,7 @@ def time_mixed_box(mcfg, init, coef, device, R, warm, K):
     return ms, {k: round(v[0] / 3.0, 4) for k, v in prof.items()}
 
 
-def run_mixed(cfg, init, coef, fbox, device, R, warm, K, fp64_ms_per_step, ydense=True):
+def run_mixed(cfg, init, coef, fbox, device, R, warm, K, fp64_ms_per_step, ydense=True, tune=True):
     """The mixed-precision path (OTBL_PREC_MIXED) on the same box: device
     time of K RK3 steps after `warm`, then its error against the FP64 path
     after the same steps from the same initial state. With `ydense`, the
@@ -394,7 +396,7 @@ def run_mixed(cfg, init, coef, fbox, device, R, warm, K, fp64_ms_per_step, ydens
     import torch
     mcfg = cfgmod.replace(cfg, precision=1)
     mbox = Box(mcfg, init, coef, device=device)
-    mtuned = mbox.autotune()
+    mtuned = mbox.autotune() if tune else None
     stream = torch.cuda.ExternalStream(mbox.stream, device=f"cuda:{device}")
     for _ in range(warm):
         mbox.advance(1)
@@ -431,7 +433,7 @@ def run_mixed(cfg, init, coef, fbox, device, R, warm, K, fp64_ms_per_step, ydens
     mbox.close()
     dense = None
     if ydense and cfg.ny <= 256:
-        dms, dprof = time_mixed_box(cfgmod.replace(mcfg, options=1), init, coef, device, R, warm, K)
+        dms, dprof = time_mixed_box(cfgmod.replace(mcfg, options=1), init, coef, device, R, warm, K, tune)
         dense = {"ms_per_step": dms / K, "interpy_ms_per_substep": dprof.get("interpy"),
                  "banded_interpy_ms_per_substep": per_sub.get("interpy"),
                  "kernel": "k_ydense (tcgen05.mma kind::tf32, 3 products of the split operands)"}
@@ -445,7 +447,7 @@ def run_mixed(cfg, init, coef, fbox, device, R, warm, K, fp64_ms_per_step, ydens
                                  "peak_kind": peak_kind},
             "kernels_ms_per_substep": per_sub,
             "err_vs_fp64": dict(steps=nsteps, **err), "clocks": clk.summary(),
-            "autotuned_cta_sizes": list(mtuned), "dense_interpyy": dense}
+            "autotuned_cta_sizes": list(mtuned) if mtuned else None, "dense_interpyy": dense}
 
 
 def main():
@@ -459,6 +461,10 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-ydense", action="store_true")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                    help="precision of the headline box (mixed: profiling runs of the mixed path alone)")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default CTA sizes (profiling runs: no tuning launches first)")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--ensemble-steps", type=int, default=10)
     ap.add_argument("--no-serve", action="store_true")
@@ -467,6 +473,9 @@ def main():
     ap.add_argument("--serve-load", type=float, default=0.7)
     args = ap.parse_args()
     cfg = getattr(cfgmod, args.config)
+    if args.precision == "mixed":
+        cfg = cfgmod.replace(cfg, precision=1)
+        args.no_mixed = True
     R = replicas.setup()
     ws, rank, local = R.world_size, R.rank, R.local_rank
     if args.impl == "reference":
@@ -477,7 +486,7 @@ def main():
     import torch
     torch.cuda.set_device(local)
     init, coef, box = build_box(cfg, local)
-    tuned = box.autotune()  # CTA sizes of the line kernels for this box
+    tuned = None if args.no_autotune else box.autotune()  # CTA sizes of the line kernels for this box
     stream = torch.cuda.ExternalStream(box.stream, device=f"cuda:{local}")
     warm = max(args.warmup, 0)
     K = max(args.steps, 1)
@@ -528,10 +537,13 @@ def main():
                 "algorithmic_bytes_per_launch": (ab[dom] / launches_dom) if dom in ab else None,
                 "launches_per_substep": launches_dom, "ms_per_substep": per_sub[dom],
                 "ms_per_launch": per_sub[dom] / launches_dom}
-    substep_roofline = {"bytes_per_substep": ab["substep_survey"], "ms_per_substep": sub_ms,
-                        "achieved": ab["substep_survey"] / (sub_ms / 1e3) / 1e9, "peak": peak,
-                        "unit": "GB/s", "frac": ab["substep_survey"] / (sub_ms / 1e3) / 1e9 / peak,
+    b_sub = ab["substep_survey"] if cfg.precision == 0 else mixed_substep_bytes(cfg, pois_fp64_modes(cfg, coef))
+    substep_roofline = {"bytes_per_substep": b_sub, "ms_per_substep": sub_ms,
+                        "achieved": b_sub / (sub_ms / 1e3) / 1e9, "peak": peak,
+                        "unit": "GB/s", "frac": b_sub / (sub_ms / 1e3) / 1e9 / peak,
                         "peak_kind": peak_kind}
+    if cfg.precision != 0:
+        roofline = None  # the per-kernel algorithmic bytes above count FP64 fields
     kernels = {k: round(v, 4) for k, v in sorted(per_sub.items(), key=lambda t: -t[1])}
 
     # ---- end to end through the public API with host buffers ----
@@ -570,7 +582,8 @@ def main():
 
     mixed = None
     if not args.no_mixed:
-        mixed = run_mixed(cfg, init, coef, box, local, R, warm, K, ms / K, ydense=not args.no_ydense)
+        mixed = run_mixed(cfg, init, coef, box, local, R, warm, K, ms / K, ydense=not args.no_ydense,
+                          tune=not args.no_autotune)
 
     ens = None
     if not args.no_ensemble:
@@ -596,8 +609,9 @@ def main():
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K,
                "warmup": warm, "ms_per_step": ms / K, "higher_is_better": True,
-               "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-               "config": workload_config(cfg, ws), "autotuned_cta_sizes": list(tuned),
+               "scaling": "weak", "vs_baseline": None,
+               "dtype": "f64" if cfg.precision == 0 else "f32 operators, f64 state", "data": "synthetic",
+               "config": workload_config(cfg, ws), "autotuned_cta_sizes": list(tuned) if tuned else None,
                "roofline": roofline, "substep_roofline": substep_roofline,
                "kernels_ms_per_substep": kernels,
                "kernels_note": "CUDA events around each kernel class in a separate profiled RK3 step "

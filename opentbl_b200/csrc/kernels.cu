@@ -972,8 +972,13 @@ using XTab = XTabT<double>;
 // CTA; T is the transform's arithmetic and phi's element type (FP64, or FP32
 // for the higher modes of the mixed path). The divergence itself is formed
 // in FP64 from the FP64 velocity.
+// With 512 threads both x-DCT kernels are bounded to 64 registers (two CTAs
+// per SM): at 66 registers the FP64 forward kernel of n = 1024 fits one CTA
+// per SM instead of two and took 1.18 instead of 0.83 ms per substep at
+// 1025x193x512. The 256-thread variants are not bounded (at 64 registers
+// they spill).
 template <typename T, int MB, int NT>
-__global__ void __launch_bounds__(NT) k_pois_fwd(DCoef c, XTabT<T> x, const double *__restrict__ u,
+__global__ void __launch_bounds__(NT, NT >= 512 ? 2 : 1) k_pois_fwd(DCoef c, XTabT<T> x, const double *__restrict__ u,
                                                  const double *__restrict__ v, const double *__restrict__ w,
                                                  T *__restrict__ phi, int kbeg, int kend) {
   using V = V2<T>;
@@ -1030,7 +1035,7 @@ __global__ void __launch_bounds__(NT) k_pois_fwd(DCoef c, XTabT<T> x, const doub
 
 // DCT-III along x (cosftx iopt=+1), in place on phi-hat, modes kbeg..kend
 template <typename T, int MB, int NT>
-__global__ void __launch_bounds__(NT) k_pois_bwd(DCoef c, XTabT<T> x, T *__restrict__ phi, int kbeg, int kend) {
+__global__ void __launch_bounds__(NT, NT >= 512 ? 2 : 1) k_pois_bwd(DCoef c, XTabT<T> x, T *__restrict__ phi, int kbeg, int kend) {
   using V = V2<T>;
   extern __shared__ __align__(16) unsigned char xsm_raw[];
   V *xsm = reinterpret_cast<V *>(xsm_raw);
