@@ -116,7 +116,8 @@ def algorithmic_bytes(cfg) -> dict:
 
 
 def read_traffic(kernel: str):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary."""
+    """DRAM bytes per substep of kernel class `kernel` at 1025x193x512, from
+    the committed ncu summary (profiles/dram_traffic.txt)."""
     p = os.path.join(ROOT, "profiles", "dram_traffic.txt")
     if not os.path.exists(p):
         return None
@@ -529,10 +530,13 @@ def main():
     launches_dom = prof[dom][1] / 3.0
     t_dom = per_sub[dom] / 1e3
     achieved = ab[dom] / t_dom / 1e9 if dom in ab else None
-    traffic = read_traffic(dom)
+    traffic_sub = read_traffic(dom) if cfg.name.startswith("C2") else None
     sub_ms = ms / sub
     roofline = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                "frac": (achieved / peak) if achieved else None,
+                "traffic": (traffic_sub / launches_dom) if traffic_sub else None,
+                "traffic_per_substep": traffic_sub,
+                "traffic_source": "profiles/dram_traffic_rk3_substep_SLAB.md (scaled by 1025/257)",
                 "peak_kind": peak_kind, "algorithmic_bytes_per_substep": ab.get(dom),
                 "algorithmic_bytes_per_launch": (ab[dom] / launches_dom) if dom in ab else None,
                 "launches_per_substep": launches_dom, "ms_per_substep": per_sub[dom],
