@@ -147,6 +147,45 @@ int otbl_get_inflow(otbl_ctx *ctx, double *um, otbl_inflow *st);
  * plane-1 branch's ener(1:3)). Zero before the first rhsp(m = 1). */
 int otbl_get_energies(otbl_ctx *ctx, double *ener);
 
+/* ---- one-point statistics, statsp (stotf.F90:51-291) ----
+ * otbl_statsp adds one sample of the one-point statistics of the context's
+ * current state to its accumulators, as rhsp does on its first substep when
+ * dostat is set (bl_1.F90:92, rhsp.F90:70-101): the x pre-pass (u
+ * interpolated to the half points in x and shifted by one plane, d/dx of it
+ * and of v and w; lip.f90:703-765, with the fd_ix/fd_dx operators), then per
+ * plane the interpolation onto the wall positions in y (interpy_new, fd_iy
+ * and fd_iyp) and the y derivatives (diffy_inplace, fd_dvdy), and the sums
+ * over the spanwise modes (cte = 1 for k = 0, 2 otherwise) and over the
+ * physical points of the triple products. Call it between substeps, where
+ * the reference sets dostat; it uses the context's line scratch and its
+ * stream, leaves the state unchanged, and synchronizes nothing. The
+ * accumulators (OTBL_NSTATS arrays of the reference's shape (ny, nx), column
+ * major: stat(j, i) at s*nx*ny + (i-1)*ny + (j-1)) are allocated on the
+ * first call (OTBL_NSTATS*nx*ny doubles, beyond otbl_ctx_bytes; from then
+ * on otbl_device_bytes counts them) and start at zero; otbl_get_stats
+ * copies them and the number of
+ * samples (the reference's totalcal, mod.F90:278) to the host
+ * (synchronizes); otbl_reset_stats zeroes them. The spectra, the two-point
+ * correlations and the instantaneous enstrophy field of statsp are not
+ * computed. On the mixed path the pressure is read from its FP32 storage;
+ * everything else is FP64 on both paths. */
+enum {
+  OTBL_ST_UA = 0, OTBL_ST_VA, OTBL_ST_WA, OTBL_ST_PM,          /* means (k = 0)      */
+  OTBL_ST_DUDX0, OTBL_ST_DVDX0, OTBL_ST_DWDX0,                /* mean gradients     */
+  OTBL_ST_DUDY0, OTBL_ST_DVDY0, OTBL_ST_DWDY0,
+  OTBL_ST_VORTXA, OTBL_ST_VORTYA, OTBL_ST_VORTZA,             /* mean vorticity     */
+  OTBL_ST_US, OTBL_ST_VS, OTBL_ST_WS, OTBL_ST_UV, OTBL_ST_UW, OTBL_ST_VW, /* stresses */
+  OTBL_ST_PUP, OTBL_ST_PVP, OTBL_ST_PP, OTBL_ST_PDUDX, OTBL_ST_PDUDY, /* pressure     */
+  OTBL_ST_PDVDX, OTBL_ST_PDVDY, OTBL_ST_PDWDZ,
+  OTBL_ST_VORTX, OTBL_ST_VORTY, OTBL_ST_VORTZ,                /* vorticity squares  */
+  OTBL_ST_DISPU, OTBL_ST_DISPV, OTBL_ST_DISPW, OTBL_ST_DISPUV, /* dissipation       */
+  OTBL_ST_U3, OTBL_ST_V3, OTBL_ST_U2V, OTBL_ST_V2U, OTBL_ST_W2V, OTBL_ST_W2U, /* triple */
+  OTBL_NSTATS
+};
+int otbl_statsp(otbl_ctx *ctx);                     /* stotf.F90:51       */
+int otbl_get_stats(otbl_ctx *ctx, double *stats_host, int *samples);
+int otbl_reset_stats(otbl_ctx *ctx);
+
 /* ---- the substep, bl_1.F90:94-125 ----
  * m = RK3 substep 1..3; setstep = 1 recomputes dt (adaptive mode). */
 int otbl_rhsp(otbl_ctx *ctx, int m, int setstep);   /* rhsp.F90:22        */

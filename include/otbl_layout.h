@@ -17,7 +17,10 @@
  * of OTBL_COEF_LIST. Each array keeps its Fortran column-major shape, e.g.
  * inxu(3,nx) occupies 3*nx doubles with inxu(r,i) at [(i-1)*3 + (r-1)], and
  * arrays with lower bound 0 (y(0:ny+1), dy(0:ny), ...) start at index 0.
- * The first block (SCAL) holds the scalars listed in OTBL_S_*.
+ * The first block (SCAL) holds the scalars listed in OTBL_S_*. The last five
+ * arrays (fd_dvdy, fd_dx, fd_ix, fd_iy, fd_iyp, each (8, n)) are the compact
+ * operators of the one-point statistics (coeft.f90:56-318); the substep does
+ * not read them.
  */
 #ifndef OTBL_LAYOUT_H
 #define OTBL_LAYOUT_H
@@ -42,7 +45,9 @@
   X(DCYU, 3 * (NY + 1)) X(DCYV, 3 * NY) X(COFCYU, 2 * NY) X(COFCYV, 2 * NY)   \
   X(DCBY, 16)                                                                 \
   X(VIYU, 3 * (NY + 1)) X(VIYV, 3 * NY) X(VYUI, 3 * (NY + 1)) X(VYVI, 3 * NY) \
-  X(COFVYU, 3 * NY) X(COFVYV, 3 * NY) X(COFVBY, 16) X(CCON, 8)
+  X(COFVYU, 3 * NY) X(COFVYV, 3 * NY) X(COFVBY, 16) X(CCON, 8)                \
+  X(FD_DVDY, 8 * NY) X(FD_DX, 8 * NX) X(FD_IX, 8 * NX) X(FD_IY, 8 * NY)       \
+  X(FD_IYP, 8 * NY)
 
 /* scalar slots inside the SCAL block */
 enum {

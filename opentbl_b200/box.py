@@ -190,6 +190,23 @@ class Box:
     def genflu(self):
         self._check(self.L.otbl_genflu(self.h), "otbl_genflu")
 
+    NSTATS = 40
+
+    def statsp(self):
+        """One sample of the one-point statistics of the current state into
+        the context's accumulators (statsp, stotf.F90:51-291)."""
+        self._check(self.L.otbl_statsp(self.h), "otbl_statsp")
+
+    def stats(self):
+        """(accumulators (NSTATS, nx, ny) in the order of OTBL_ST_*, samples)."""
+        out = np.zeros((self.NSTATS, self.cfg.nx, self.cfg.ny))
+        n = ctypes.c_int()
+        self._check(self.L.otbl_get_stats(self.h, native.dptr(out), ctypes.byref(n)), "otbl_get_stats")
+        return out, n.value
+
+    def reset_stats(self):
+        self._check(self.L.otbl_reset_stats(self.h), "otbl_reset_stats")
+
     def interpyy(self):
         """lip.f90:359-440 on the state's u, w, v: (uy, wy, vy), ny rows each."""
         shp = (self.cfg.nx, self.cfg.ny, self.cfg.nz1)

@@ -17,9 +17,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libotbl.so")
 DRIVER = os.path.join(HERE, "otbl_driver")
-SOURCES = ["kernels.cu", "k_xlines.cu", "k_ylines.cu", "k_ydense.cu", "otbl_capi.cu", "otbl_graph.cu",
-           "coef.cpp"]
-HEADERS = ["otbl_internal.cuh", "fft.cuh", "devcommon.cuh", "tma.cuh"]
+SOURCES = ["kernels.cu", "k_xlines.cu", "k_ylines.cu", "k_ydense.cu", "k_stats.cu", "otbl_capi.cu",
+           "otbl_graph.cu", "coef.cpp"]
+HEADERS = ["otbl_internal.cuh", "fft.cuh", "devcommon.cuh", "tma.cuh", "zline.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

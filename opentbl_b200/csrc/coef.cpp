@@ -12,8 +12,11 @@
 //   inlet_retheta bl_1.F90:372-396  inlet Re_theta and delta99
 //   magicnumber boun.f90:102-143    top transpiration vmagic(x)
 //   wavenumbers bl_1.F90:357-366    kaz = i*k/az, kaz2 = -kaz**2
-// The statistics-only arrays of coef (fd_*, l_weight, ldyy) are not built:
-// nothing on the substep reads them.
+//   fd_*        coeft.f90:56-318    the compact operators of the one-point
+//                                   statistics (statsp), which the substep
+//                                   itself does not read
+// The pressure-extrapolation weights of coef (l_weight, ldyy) are not built:
+// nothing here reads them.
 //
 // Output is the packed buffer described in include/otbl_layout.h, uploaded
 // to the device by otbl_ctx_create. Fortran semantics are kept where they
@@ -54,6 +57,187 @@ inline double cu(double a) { return a * a * a; }
 inline double p4(double a) {
   const double s = a * a;
   return s * s;
+}
+
+// x**5 as gfortran expands an integer power: x**3 * x**2
+inline double p5(double a) {
+  const double s = a * a;
+  return (s * a) * s;
+}
+
+// An (8, n) compact operator of the statistics: weights of the explicit
+// stencil in rows 1..5, the tridiagonal's sub-, main and super-diagonal in
+// rows 6..8 (coeft.f90:56-318).
+struct Op8 {
+  double *p;
+  double &operator()(int r, int j) const { return p[(size_t)(j - 1) * 8 + (r - 1)]; }
+  // the LU reorganisation done after each operator (coeft.f90:146-150,
+  // 188-192, 222-226, 304-316): eliminate from row j0 on, then invert the
+  // pivots of rows inv0..n
+  void factor(int n, int j0, int inv0) const {
+    const Op8 &c = *this;
+    for (int j = j0; j <= n; ++j) {
+      c(6, j) = c(6, j) / c(7, j - 1);
+      c(7, j) = c(7, j) - c(6, j) * c(8, j - 1);
+    }
+    for (int j = inv0; j <= n; ++j) c(7, j) = 1.0 / c(7, j);
+  }
+};
+
+// fd_dvdy, fd_dx, fd_ix, fd_iy, fd_iyp of coeft.f90:56-318, in the
+// Fortran's order of operations (negation, commuted sums b - c for -c+b and
+// the like change no bits)
+void fd_operators(int nx, int ny, double ax, double pi, const double *y, Op8 dv, Op8 dx, Op8 ix, Op8 iy,
+                  Op8 ip) {
+  std::vector<double> hv(ny + 2), hiv(ny + 2), ypv(ny + 2);
+  double *h = hv.data(), *hi = hiv.data(), *yp = ypv.data();  // (1:ny+1)
+  double a, b, c, d, e, f, g;
+
+  // d/dy at the v rows (non-uniform mesh), coeft.f90:56-150
+  for (int j = 1; j <= ny + 1; ++j) h[j] = y[j] - y[j - 1];
+  a = h[2], b = h[2] + h[3], c = h[2] + h[3] + h[4];
+  dv(1, 1) = -(a * b + a * c + 2 * b * c) / b / a / c;
+  dv(3, 1) = -(sq(a) * c / (b - c) / b / sq(a - b));
+  dv(4, 1) = sq(a) * b / c / sq(a - c) / (b - c);
+  dv(2, 1) = -(dv(1, 1) + dv(3, 1) + dv(4, 1));
+  dv(7, 1) = 1.0;
+  dv(8, 1) = b * c / (a - c) / (a - b);
+  dv(1, 2) = sq(a - b) * (a - c) * (a * b + 2 * a * c + 2 * b * c) / a / cu(b) / sq(c);
+  dv(2, 2) = 1 / a * (-3 * a * b + 2 * b * c + 5 * sq(a) - 4 * a * c) / (a - c) / (a - b);
+  dv(3, 2) = sq(a) * (a - c) * (-2 * a * c + 3 * a * b + 4 * b * c - 5 * sq(b)) / cu(b) / sq(b - c) / (a - b);
+  dv(4, 2) = -(dv(1, 2) + dv(2, 2) + dv(3, 2));
+  dv(6, 2) = -(sq(a - b) * (a - c) / c / sq(b));
+  dv(7, 2) = 1.0;
+  dv(8, 2) = sq(a) * (a - c) / (b - c) / sq(b);
+  for (int i = 3; i <= ny - 2; ++i) {
+    a = h[i - 1], b = h[i], c = h[i + 1], d = h[i + 2];
+    f = c + d, e = a + b;
+    const double qb = sq(b) + 2 * b * c + sq(c), qe = sq(e) - 2 * e * b + sq(b);
+    dv(1, i) = -(sq(c) * sq(b) * f / (f + e) / e / (sq(c) + 2 * c * e + sq(e)) / qe);
+    dv(2, i) = f / b * e * sq(c) *
+               (3 * c * b * f - 2 * c * f * e + 4 * sq(b) * c - 3 * b * e * c + 5 * sq(b) * f - 4 * b * e * f +
+                6 * cu(b) - 5 * e * sq(b)) /
+               (sq(f) + 2 * b * f + sq(b)) / (cu(b) + 3 * b * sq(c) + cu(c) + 3 * sq(b) * c) / qe;
+    dv(3, i) = (c * b * f - b * e * c - 2 * b * e * f + 2 * c * f * e) / f / b / e / c;
+    dv(4, i) = -((-3 * c * b * f - 2 * b * e * f + 3 * b * e * c + 4 * b * sq(c) - 5 * sq(c) * f - 4 * c * f * e +
+                  6 * cu(c) + 5 * sq(c) * e) *
+                 sq(b) / c * e * f / (sq(f) - 2 * f * c + sq(c)) /
+                 (3 * sq(e) * b * sq(c) + 6 * e * sq(b) * sq(c) + 6 * e * b * cu(c) + sq(e) * cu(b) + p5(c) +
+                  2 * p4(c) * e + cu(c) * sq(e) + 3 * sq(b) * cu(c) + cu(b) * sq(c) + 3 * b * p4(c) +
+                  2 * e * cu(b) * c + 3 * sq(e) * sq(b) * c));
+    dv(5, i) = -(dv(1, i) + dv(2, i) + dv(3, i) + dv(4, i));
+    dv(6, i) = -(e * sq(c) * f / (f + b) / qb / (b - e));
+    dv(7, i) = 1.0;
+    dv(8, i) = -(e * sq(b) * f / (c - f) / qb / (c + e));
+  }
+  a = h[ny - 2], b = h[ny - 1], c = h[ny];
+  f = a + b + c, e = b + c;
+  dv(1, ny - 1) = sq(c) * sq(c - e) / sq(f) / sq(f - e) / (c - f);
+  dv(3, ny - 1) = -((5 * sq(c) - 4 * f * c - 3 * c * e + 2 * f * e) / c / (c - f) / (c - e));
+  dv(4, ny - 1) = -(sq(c - e) * (c - f) * (2 * f * c + c * e + 2 * f * e) / c / sq(f) / cu(e));
+  dv(2, ny - 1) = -(dv(1, ny - 1) + dv(3, ny - 1) + dv(4, ny - 1));
+  dv(6, ny - 1) = -((c - f) * sq(c) / sq(e) / (f - e));
+  dv(7, ny - 1) = 1.0;
+  dv(8, ny - 1) = -(sq(c - e) * (c - f) / f / sq(e));
+  dv(1, ny) = sq(c) * e / sq(c - f) / (f - e) / f;
+  dv(2, ny) = -(sq(c) * f / e / sq(c - e) / (f - e));
+  dv(4, ny) = (f * c + c * e + 2 * f * e) / c / f / e;
+  dv(3, ny) = -(dv(1, ny) + dv(2, ny) + dv(4, ny));
+  dv(6, ny) = f * e / (c - f) / (c - e);
+  dv(7, ny) = 1.0;
+  dv.factor(ny, 2, 1);
+
+  // d/dx on the uniform x grid, coeft.f90:153-194: boundary rows 1, 2,
+  // nx-1, nx, the sixth-order interior scheme, weights divided by dx
+  {
+    const double r1[8] = {-37.0 / 12.0, 2.0 / 3.0, 3.0, -2.0 / 3.0, 1.0 / 12.0, 0.0, 1.0, 4.0};
+    const double r2[8] = {-43.0 / 96.0, -5.0 / 6.0, 9.0 / 8.0, 1.0 / 6.0, -1.0 / 96.0, 1.0 / 8.0, 1.0, 3.0 / 4.0};
+    const double rm[8] = {-1.0 / 36.0, -7.0 / 9.0, 0.0, 7.0 / 9.0, 1.0 / 36.0, 1.0 / 3.0, 1.0, 1.0 / 3.0};
+    const double rn1[8] = {1.0 / 96.0, -1.0 / 6.0, -9.0 / 8.0, 5.0 / 6.0, 43.0 / 96.0, 3.0 / 4.0, 1.0, 1.0 / 8.0};
+    const double rn[8] = {-1.0 / 12.0, 2.0 / 3.0, -3.0, -2.0 / 3.0, 37.0 / 12.0, 4.0, 1.0, 0.0};
+    for (int i = 1; i <= nx; ++i) {
+      const double *r = i == 1 ? r1 : (i == 2 ? r2 : (i == nx - 1 ? rn1 : (i == nx ? rn : rm)));
+      for (int k = 1; k <= 8; ++k) dx(k, i) = r[k - 1];
+    }
+    const double point0 = ax * pi / (nx + 1);
+    for (int i = 1; i <= nx; ++i)
+      for (int k = 1; k <= 5; ++k) dx(k, i) = dx(k, i) / point0;
+    dx.factor(nx, 2, 1);
+  }
+
+  // mid-point interpolation in x, coeft.f90:196-228
+  {
+    const double r1[8] = {5.0 / 24.0, 15.0 / 8.0, 5.0 / 8.0, -1.0 / 24.0, 0.0, 0.0, 1.0, 5.0 / 3.0};
+    const double rm[8] = {1.0 / 20.0, 3.0 / 4.0, 3.0 / 4.0, 1.0 / 20.0, 0.0, 3.0 / 10.0, 1.0, 3.0 / 10.0};
+    const double rn1[8] = {-1.0 / 84.0, 1.0 / 4.0, 5.0 / 4.0, 5.0 / 12.0, 0.0, 5.0 / 6.0, 1.0, 1.0 / 14.0};
+    const double rn[8] = {1.0 / 8.0, -7.0 / 8.0, 35.0 / 8.0, 35.0 / 8.0, 0.0, 7.0, 1.0, 0.0};
+    for (int i = 1; i <= nx; ++i) {
+      const double *r = i == 1 ? r1 : (i == nx - 1 ? rn1 : (i == nx ? rn : rm));
+      for (int k = 1; k <= 8; ++k) ix(k, i) = r[k - 1];
+    }
+    ix.factor(nx, 2, 1);
+  }
+
+  // mid-point interpolation in y onto the wall positions y(j): fd_iy for
+  // u and w (u-type rows at yp), fd_iyp for p, coeft.f90:231-318
+  for (int j = 1; j <= ny + 1; ++j) yp[j] = (y[j - 1] + y[j]) * 0.5;
+  for (int j = 1; j <= ny + 1; ++j) hi[j] = y[j] - y[j - 1];
+  for (int j = 2; j <= ny + 1; ++j) h[j] = yp[j] - yp[j - 1];
+  a = hi[2] / 2, b = a + h[3], c = b + h[4], d = c + h[5];
+  iy(1, 1) = -(c * b * d / (a - d) / (a - c) / (a - b));
+  iy(2, 1) = c * a * d / (b - d) / (b - c) / (a - b);
+  iy(3, 1) = -(b * a * d / (c - d) / (sq(c) - a * c - b * c + b * a));
+  iy(4, 1) = 1.0 - (iy(1, 1) + iy(2, 1) + iy(3, 1));
+  a = hi[3] / 2, b = a + h[4], c = b + h[5], d = c + h[6], e = hi[2] / 2;
+  iy(1, 2) = 2 * c * b * sq(a) * d / (e + d) / (e + c) / (b + e) / (2 * sq(a) + sq(e) + 3 * e * a);
+  iy(2, 2) = -(2 * c * b * e * d / (a - d) / (a - c) / (a - b) / (a + e));
+  iy(3, 2) = 2 * c * e * sq(a) * d / (b - d) / (b - c) /
+             (2 * sq(a) * e + 2 * sq(a) * b - 3 * a * sq(b) - 3 * a * e * b + cu(b) + e * sq(b));
+  iy(4, 2) = -(2 * sq(a) * b * e * d / (c - d) /
+               (3 * e * a * sq(c) - 2 * e * sq(a) * c - 3 * b * e * a * c - 2 * sq(a) * sq(c) + 2 * sq(a) * e * b +
+                3 * a * cu(c) + b * cu(c) - e * cu(c) + 2 * b * sq(a) * c - 3 * b * a * sq(c) + b * e * sq(c) -
+                p4(c)));
+  iy(7, 2) = 1.0;
+  iy(8, 2) = -(c * b * e * d / (2 * a + e) / (2 * a - d) / (2 * a - c) / (2 * a - b));
+  iy(5, 2) = (iy(7, 2) + iy(8, 2)) - (iy(1, 2) + iy(2, 2) + iy(3, 2) + iy(4, 2));
+  for (int j = 3; j <= ny - 1; ++j) {
+    a = hi[j + 1] / 2, b = a + h[j + 2], e = hi[j] / 2, f = e + h[j];
+    iy(1, j) = 4 * sq(e) * sq(a) * b / (b + f) /
+               (2 * sq(a) * sq(f) + p4(f) + 4 * sq(e) * sq(a) - 6 * sq(a) * e * f - 9 * e * a * sq(f) +
+                6 * sq(e) * a * f + 2 * sq(e) * sq(f) + 3 * a * cu(f) - 3 * e * cu(f));
+    iy(2, j) = -(4 * f * sq(a) * b / (b + e) / (a + e) / (e - f) / (2 * a + e));
+    iy(3, j) = -(4 * f * sq(e) * b / (a - b) / (a + f) / (2 * sq(e) + sq(a) + 3 * e * a));
+    iy(6, j) = -(f * b * sq(a) / (a + e) / (2 * e - f) / (b + 2 * e) / (a + 2 * e));
+    iy(7, j) = 1.0;
+    iy(8, j) = -(f * sq(e) * b / (2 * a - b) / (2 * a + f) / (2 * sq(a) + sq(e) + 3 * e * a));
+    iy(4, j) = (iy(6, j) + iy(7, j) + iy(8, j)) - (iy(1, j) + iy(2, j) + iy(3, j));
+  }
+  a = hi[ny + 1] / 2, e = hi[ny] / 2, f = e + h[ny], g = f + h[ny - 1];
+  const double top = 8 * cu(e) - 4 * g * sq(e) - 2 * f * a * e - 2 * g * e * a - 4 * f * sq(e) + g * a * f +
+                     4 * a * sq(e) + 2 * f * g * e;
+  iy(1, ny) = 2 * (4 * sq(e) + 2 * e * a - a * f - 2 * f * e) * sq(e) / (e - g) / (f - g) / g / (g + a);
+  iy(2, ny) = -(2 * (2 * e * a + 4 * sq(e) - a * g - 2 * g * e) * sq(e) / (e - f) / f /
+                (sq(f) + a * f - g * f - a * g));
+  iy(3, ny) = 2 * top / (cu(e) + a * sq(e) - f * sq(e) - g * sq(e) + g * a * f - g * e * a + f * g * e - f * a * e);
+  iy(4, ny) = 2 * (-2 * f * e - 2 * g * e + g * f + 4 * sq(e)) * sq(e) / (g + a) / (a + f) / (a + e) / a;
+  iy(6, ny) = 1.0;
+  iy(7, ny) = top / g / a / f;
+  for (size_t k = 0; k < 8 * (size_t)ny; ++k) ip.p[k] = iy.p[k];  // fd_iyp = fd_iy, then its top rows
+  a = hi[ny] / 2, e = hi[ny - 1] / 2, f = e + h[ny - 1];
+  ip(1, ny - 1) = 4 * sq(e) * sq(a) / (2 * a + f) / (a + f) / (2 * sq(e) + sq(f) - 3 * e * f);
+  ip(2, ny - 1) = -(4 * f * sq(a) / (3 * e * a + sq(e) + 2 * sq(a)) / (e - f));
+  ip(3, ny - 1) = 4 * sq(e) * f / (cu(a) + 2 * sq(e) * a + 3 * e * sq(a) + 2 * sq(e) * f + f * sq(a) + 3 * f * e * a);
+  ip(6, ny - 1) = -(f * sq(a) / (a + e) / (2 * e - f) / (2 * e + a));
+  ip(7, ny - 1) = 1.0;
+  ip(8, ny - 1) = sq(e) * f / (4 * cu(a) + 2 * sq(e) * a + 6 * e * sq(a) + 3 * f * e * a + sq(e) * f + 2 * f * sq(a));
+  e = hi[ny] / 2, f = e + h[ny], g = f + h[ny - 1];
+  ip(1, ny) = 2 * sq(e) * (2 * e - f) / (e - g) / (f - g) / g;
+  ip(2, ny) = -(2 * (2 * e - g) * sq(e) / (e - f) / f / (f - g));
+  ip(3, ny) = 2 * (4 * sq(e) + g * f - 2 * e * f - 2 * g * e) / (sq(e) - e * f + g * f - g * e);
+  ip(6, ny) = 1.0;
+  ip(7, ny) = (4 * sq(e) + g * f - 2 * e * f - 2 * g * e) / g / f;
+  ip.factor(ny, 3, 2);
+  iy.factor(ny, 3, 2);
 }
 
 // ludcmp, coeft.f90:1818-1883 (Numerical Recipes, implicit pivoting).
@@ -718,6 +902,9 @@ extern "C" int otbl_coef_compute(const otbl_config *cfg, const double *yin,
     for (int i = 2; i <= nx - 1; ++i) vm[i - 1] = (hm[i + 1] - hm[i - 1]) / (xm[i + 1] - xm[i - 1]);
     vm[nx - 1] = (hm[nx] - hm[nx - 1]) / (xm[nx] - xm[nx - 1]);
   }
+
+  fd_operators(nx, ny, ax, pi, y, Op8{P(OTBL_C_FD_DVDY)}, Op8{P(OTBL_C_FD_DX)}, Op8{P(OTBL_C_FD_IX)},
+               Op8{P(OTBL_C_FD_IY)}, Op8{P(OTBL_C_FD_IYP)});
 
   S[OTBL_S_RE] = re;
   S[OTBL_S_REX] = rex;

@@ -778,6 +778,36 @@ extern "C" int otbl_interpyy(otbl_ctx *c, double *uy, double *wy, double *vy) {
   return err ? device_error(c, err) : OTBL_OK;
 }
 
+extern "C" int otbl_statsp(otbl_ctx *c) {
+  if (!c) return OTBL_ERR_ARG;
+  cudaSetDevice(c->device);
+  LAUNCH(c, launch_statsp(c));
+  return OTBL_OK;
+}
+
+extern "C" int otbl_get_stats(otbl_ctx *c, double *host, int *samples) {
+  if (!c || !host) return OTBL_ERR_ARG;
+  cudaSetDevice(c->device);
+  const size_t n = (size_t)OTBL_NSTATS * c->cfg.nx * c->cfg.ny;
+  if (!c->stats) {
+    std::fill(host, host + n, 0.0);
+  } else {
+    OTBL_CUDA_TRY(c, cudaMemcpyAsync(host, c->stats, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    OTBL_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  }
+  if (samples) *samples = c->stats_samples;
+  return OTBL_OK;
+}
+
+extern "C" int otbl_reset_stats(otbl_ctx *c) {
+  if (!c) return OTBL_ERR_ARG;
+  cudaSetDevice(c->device);
+  if (c->stats)
+    OTBL_CUDA_TRY(c, cudaMemsetAsync(c->stats, 0, stats_bytes(c->cfg.nx, c->cfg.ny), c->stream));
+  c->stats_samples = 0;
+  return OTBL_OK;
+}
+
 extern "C" int otbl_boun(otbl_ctx *c) {
   if (!c) return OTBL_ERR_ARG;
   cudaSetDevice(c->device);

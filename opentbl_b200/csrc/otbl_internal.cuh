@@ -131,6 +131,10 @@ struct otbl_ctx {
   int yd_nt = 0, yd_nb = 0;
   otbl::YDenseMaps yd_maps;
   bool yd_maps_ok = false;
+  // one-point statistics (k_stats.cu): OTBL_NSTATS accumulators (ny, nx),
+  // allocated by the first otbl_statsp, and the number of samples in them
+  double *stats = nullptr;
+  int stats_samples = 0;
   // TMA descriptors of the rhsp tail's inputs, per velocity component
   otbl::FinalMaps fmaps[3];
   bool fmaps_ok = false;
@@ -247,6 +251,9 @@ cudaError_t ydense_prepare(otbl_ctx *c);
 cudaError_t launch_interpy_dense(otbl_ctx *c);
 bool build_ydense_maps(otbl_ctx *c);
 bool ydense_ready(const otbl_ctx *c);
+// one-point statistics, statsp (k_stats.cu)
+cudaError_t launch_statsp(otbl_ctx *c);
+size_t stats_bytes(int nx, int ny);
 size_t ydense_bytes(int ny);
 // standalone pieces
 cudaError_t launch_chp2x(otbl_ctx *c, const double *plan, double *pen, int jee, int to_pen);

@@ -32,7 +32,8 @@ COEF_NAMES = ("SCAL", "Y", "DY", "IDY", "IDYY", "DYMIN", "HY", "XG", "DX", "KAZ"
               "COFIVX", "INBX", "DCXU", "DCXV", "COFCXU", "COFCXV", "DCBX", "VIXU",
               "VIXV", "COFVXU", "COFVXV", "COFVBX", "INYU", "INYV", "COFIUY",
               "COFIVY", "INBY", "DCYU", "DCYV", "COFCYU", "COFCYV", "DCBY", "VIYU",
-              "VIYV", "VYUI", "VYVI", "COFVYU", "COFVYV", "COFVBY", "CCON")
+              "VIYV", "VYUI", "VYVI", "COFVYU", "COFVYV", "COFVBY", "CCON",
+              "FD_DVDY", "FD_DX", "FD_IX", "FD_IY", "FD_IYP")
 SCAL = dict(RE=0, REX=1, AX=2, AY=3, AZ=4, CFL=5, DX1=6, IDX=7, IDXX=8, DXMIN=9,
             DZMIN=10, DTRET=11, PI=12, UINF=13, RTHIN=14, DIN=15, YBLEND=16,
             RKC=20, RKD=23, RKCV=26, RKDV=29, NX=40, NY=41, NZ=42, XOUT=43)
@@ -92,6 +93,9 @@ def _bind(L):
         "otbl_boun": ([P], I),
         "otbl_interpyy": ([P, D, D, D], I),
         "otbl_genflu": ([P], I),
+        "otbl_statsp": ([P], I),
+        "otbl_get_stats": ([P, D, ctypes.POINTER(I)], I),
+        "otbl_reset_stats": ([P], I),
         "otbl_bind_state": ([P] + [P] * 7, I),
         "otbl_rhsp_arrays": ([P] + [P] * 7 + [I, I], I),
         "otbl_outflow_correction_arrays": ([P, P, P, P], I),

@@ -114,6 +114,20 @@ void orc_destroy(orc_box *b) {
   free(b);
 }
 
+/* read-only views for the statistics restatement (orc_stats.c) */
+int orc_box_dims(const orc_box *b, int *nx, int *ny, int *nz, int *xround) {
+  *nx = b->nx;
+  *ny = b->ny;
+  *nz = b->nz;
+  *xround = b->xround;
+  return 0;
+}
+const double *orc_box_coef(const orc_box *b, otbl_coef_offsets *o) {
+  *o = b->o;
+  return b->c;
+}
+const orc_fft *orc_box_zfft(const orc_box *b) { return b->fz; }
+
 double *orc_field(orc_box *b, int id) {
   return (id >= 0 && id < OTBL_F_COUNT) ? b->f[id] : NULL;
 }

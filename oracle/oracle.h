@@ -72,6 +72,14 @@ void orc_genflu(orc_box *b);
  * planes 2..nx are written, the rest set to 0) */
 void orc_divergence(orc_box *b, double *div);
 
+/* one-point statistics (orc_stats.c): statsp (stotf.F90:51-291) with the
+ * x pre-pass of rhsp (rhsp.F90:70-92) on the box's current state, added to
+ * acc (OTBL_NSTATS arrays (ny, nx), the order of OTBL_ST_*); and its
+ * compact operators on one line/column (op 0 interpx_new, 1 diffx, 2
+ * interpy_new for u, 3 for p, 4 diffy) */
+void orc_statsp(orc_box *b, double *acc);
+void orc_stats_operator(orc_box *b, int op, const double *in, double *out);
+
 /* operator-level entry points (lip.f90 / ffts.f90 / change.f90) */
 void orc_interpxx(orc_box *b, const double *gen, double *geni, int which,
                   int nlin);

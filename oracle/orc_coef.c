@@ -252,6 +252,255 @@ static void f_coefinv(double *a, int neq, int npter1) {
 #define T2(p, r, i) (p)[((i)-1) * 2 + (r)-1]
 #define MAT(p, nr, r, c) (p)[((c)-1) * (nr) + (r)-1]
 
+/* x**5 as gfortran expands an integer power: x**3 * x**2 */
+static double ipow5(double x) {
+  const double s = x * x;
+  return ((s * x) * s);
+}
+
+/* LU reorganisation of an (8, n) compact operator, coeft.f90:146-150 and
+ * its copies: from row j0 on, c6 /= c7(j-1), c7 -= c6 c8(j-1); then c7 is
+ * inverted on rows inv0..n */
+static void fd_lu(double *c, int n, int j0, int inv0) {
+#define C8(r, j) c[((j)-1) * 8 + (r)-1]
+  for (int j = j0; j <= n; ++j) {
+    C8(6, j) = C8(6, j) / C8(7, j - 1);
+    C8(7, j) = C8(7, j) - C8(6, j) * C8(8, j - 1);
+  }
+  for (int j = inv0; j <= n; ++j) C8(7, j) = 1.0 / C8(7, j);
+#undef C8
+}
+
+/* The compact operators of the one-point statistics, coeft.f90:56-318
+ * (Gamet et al.'s compact schemes on non-uniform meshes): fd_dvdy (d/dy at
+ * the v rows), fd_dx (d/dx), fd_ix (mid-point interpolation in x), fd_iy and
+ * fd_iyp (mid-point interpolation in y onto the wall positions, for u, w and
+ * for p). Each is (8, n): stencil weights in rows 1..5, the tridiagonal's
+ * sub-diagonal, diagonal and super-diagonal in rows 6..8, then LU-reorganised.
+ * Every expression keeps the Fortran's order of operations. */
+static void f_fd_operators(int nx, int ny, double ax, double pi, const double *y, double *fdvdy,
+                           double *fdx, double *fix, double *fiy, double *fiyp) {
+#define DV(r, j) fdvdy[((j)-1) * 8 + (r)-1]
+#define FX(r, i) fdx[((i)-1) * 8 + (r)-1]
+#define IX(r, i) fix[((i)-1) * 8 + (r)-1]
+#define IY(r, j) fiy[((j)-1) * 8 + (r)-1]
+#define IP(r, j) fiyp[((j)-1) * 8 + (r)-1]
+  double h[ny + 2], hi[ny + 2], yp[ny + 2]; /* h(1:ny+1), hi(1:ny+1), yp(1:ny+1) */
+  double a, b, c, d, e, f, g;
+
+  /* ---- d/dy, coeft.f90:56-150 ---- */
+  for (int j = 1; j <= ny + 1; ++j) h[j] = y[j] - y[j - 1];
+  a = h[2];
+  b = h[2] + h[3];
+  c = h[2] + h[3] + h[4];
+  DV(1, 1) = -(a * b + a * c + 2 * b * c) / b / a / c;
+  DV(3, 1) = -(ipow2(a) * c / (b - c) / b / ipow2(a - b));
+  DV(4, 1) = ipow2(a) * b / c / ipow2(a - c) / (b - c);
+  DV(2, 1) = -(DV(1, 1) + DV(3, 1) + DV(4, 1));
+  DV(7, 1) = 1.0;
+  DV(8, 1) = b * c / (a - c) / (a - b);
+  DV(1, 2) = ipow2(a - b) * (a - c) * (a * b + 2 * a * c + 2 * b * c) / a / ipow3(b) / ipow2(c);
+  DV(2, 2) = 1 / a * (-3 * a * b + 2 * b * c + 5 * ipow2(a) - 4 * a * c) / (a - c) / (a - b);
+  DV(3, 2) = ipow2(a) * (a - c) * (-2 * a * c + 3 * a * b + 4 * b * c - 5 * ipow2(b)) / ipow3(b) /
+             ipow2(b - c) / (a - b);
+  DV(4, 2) = -(DV(1, 2) + DV(2, 2) + DV(3, 2));
+  DV(6, 2) = -(ipow2(a - b) * (a - c) / c / ipow2(b));
+  DV(7, 2) = 1.0;
+  DV(8, 2) = ipow2(a) * (a - c) / (b - c) / ipow2(b);
+  for (int i = 3; i <= ny - 2; ++i) {
+    a = h[i - 1];
+    b = h[i];
+    c = h[i + 1];
+    d = h[i + 2];
+    f = c + d;
+    e = a + b;
+    DV(1, i) = -(ipow2(c) * ipow2(b) * f / (f + e) / e / (ipow2(c) + 2 * c * e + ipow2(e)) /
+                 (ipow2(e) - 2 * e * b + ipow2(b)));
+    DV(2, i) = f / b * e * ipow2(c) *
+               (3 * c * b * f - 2 * c * f * e + 4 * ipow2(b) * c - 3 * b * e * c + 5 * ipow2(b) * f -
+                4 * b * e * f + 6 * ipow3(b) - 5 * e * ipow2(b)) /
+               (ipow2(f) + 2 * b * f + ipow2(b)) /
+               (ipow3(b) + 3 * b * ipow2(c) + ipow3(c) + 3 * ipow2(b) * c) / (ipow2(e) - 2 * e * b + ipow2(b));
+    DV(3, i) = (c * b * f - b * e * c - 2 * b * e * f + 2 * c * f * e) / f / b / e / c;
+    DV(4, i) = -((-3 * c * b * f - 2 * b * e * f + 3 * b * e * c + 4 * b * ipow2(c) - 5 * ipow2(c) * f -
+                  4 * c * f * e + 6 * ipow3(c) + 5 * ipow2(c) * e) *
+                 ipow2(b) / c * e * f / (ipow2(f) - 2 * f * c + ipow2(c)) /
+                 (3 * ipow2(e) * b * ipow2(c) + 6 * e * ipow2(b) * ipow2(c) + 6 * e * b * ipow3(c) +
+                  ipow2(e) * ipow3(b) + ipow5(c) + 2 * ipow4(c) * e + ipow3(c) * ipow2(e) +
+                  3 * ipow2(b) * ipow3(c) + ipow3(b) * ipow2(c) + 3 * b * ipow4(c) + 2 * e * ipow3(b) * c +
+                  3 * ipow2(e) * ipow2(b) * c));
+    DV(5, i) = -(DV(1, i) + DV(2, i) + DV(3, i) + DV(4, i));
+    DV(6, i) = -(e * ipow2(c) * f / (f + b) / (ipow2(b) + 2 * b * c + ipow2(c)) / (b - e));
+    DV(7, i) = 1.0;
+    DV(8, i) = -(e * ipow2(b) * f / (c - f) / (ipow2(b) + 2 * b * c + ipow2(c)) / (c + e));
+  }
+  a = h[ny - 2];
+  b = h[ny - 1];
+  c = h[ny];
+  f = a + b + c;
+  e = b + c;
+  DV(1, ny - 1) = ipow2(c) * ipow2(c - e) / ipow2(f) / ipow2(f - e) / (c - f);
+  DV(3, ny - 1) = -((5 * ipow2(c) - 4 * f * c - 3 * c * e + 2 * f * e) / c / (c - f) / (c - e));
+  DV(4, ny - 1) = -(ipow2(c - e) * (c - f) * (2 * f * c + c * e + 2 * f * e) / c / ipow2(f) / ipow3(e));
+  DV(2, ny - 1) = -(DV(1, ny - 1) + DV(3, ny - 1) + DV(4, ny - 1));
+  DV(6, ny - 1) = -((c - f) * ipow2(c) / ipow2(e) / (f - e));
+  DV(7, ny - 1) = 1.0;
+  DV(8, ny - 1) = -(ipow2(c - e) * (c - f) / f / ipow2(e));
+  DV(1, ny) = ipow2(c) * e / ipow2(c - f) / (f - e) / f;
+  DV(2, ny) = -(ipow2(c) * f / e / ipow2(c - e) / (f - e));
+  DV(4, ny) = (f * c + c * e + 2 * f * e) / c / f / e;
+  DV(3, ny) = -(DV(1, ny) + DV(2, ny) + DV(4, ny));
+  DV(6, ny) = f * e / (c - f) / (c - e);
+  DV(7, ny) = 1.0;
+  fd_lu(fdvdy, ny, 2, 1);
+
+  /* ---- d/dx on the uniform x grid, coeft.f90:153-194 ---- */
+  FX(1, 1) = -37.0 / 12.0; FX(1, 2) = -43.0 / 96.0;
+  FX(2, 1) = 2.0 / 3.0;    FX(2, 2) = -5.0 / 6.0;
+  FX(3, 1) = 3.0;          FX(3, 2) = 9.0 / 8.0;
+  FX(4, 1) = -2.0 / 3.0;   FX(4, 2) = 1.0 / 6.0;
+  FX(5, 1) = 1.0 / 12.0;   FX(5, 2) = -1.0 / 96.0;
+  FX(7, 1) = 1.0;          FX(6, 2) = 1.0 / 8.0;
+  FX(8, 1) = 4.0;          FX(7, 2) = 1.0;
+  FX(8, 2) = 3.0 / 4.0;
+  for (int i = 3; i <= nx - 2; ++i) {
+    FX(1, i) = -1.0 / 36.0;
+    FX(2, i) = -7.0 / 9.0;
+    FX(3, i) = 0.0;
+    FX(4, i) = 7.0 / 9.0;
+    FX(5, i) = 1.0 / 36.0;
+    FX(6, i) = 1.0 / 3.0;
+    FX(7, i) = 1.0;
+    FX(8, i) = 1.0 / 3.0;
+  }
+  FX(1, nx - 1) = 1.0 / 96.0;  FX(1, nx) = -1.0 / 12.0;
+  FX(2, nx - 1) = -1.0 / 6.0;  FX(2, nx) = 2.0 / 3.0;
+  FX(3, nx - 1) = -9.0 / 8.0;  FX(3, nx) = -3.0;
+  FX(4, nx - 1) = 5.0 / 6.0;   FX(4, nx) = -2.0 / 3.0;
+  FX(5, nx - 1) = 43.0 / 96.0; FX(5, nx) = 37.0 / 12.0;
+  FX(6, nx - 1) = 3.0 / 4.0;   FX(6, nx) = 4.0;
+  FX(7, nx - 1) = 1.0;         FX(7, nx) = 1.0;
+  FX(8, nx - 1) = 1.0 / 8.0;
+  const double point0 = ax * pi / (nx + 1);
+  for (int i = 1; i <= nx; ++i)
+    for (int r = 1; r <= 5; ++r) FX(r, i) = FX(r, i) / point0;
+  fd_lu(fdx, nx, 2, 1);
+
+  /* ---- mid-point interpolation in x, coeft.f90:196-228 ---- */
+  IX(1, 1) = 5.0 / 24.0;   IX(1, nx - 1) = -1.0 / 84.0;
+  IX(2, 1) = 15.0 / 8.0;   IX(2, nx - 1) = 1.0 / 4.0;
+  IX(3, 1) = 5.0 / 8.0;    IX(3, nx - 1) = 5.0 / 4.0;
+  IX(4, 1) = -1.0 / 24.0;  IX(4, nx - 1) = 5.0 / 12.0;
+  IX(7, 1) = 1.0;          IX(6, nx - 1) = 5.0 / 6.0;
+  IX(8, 1) = 5.0 / 3.0;    IX(7, nx - 1) = 1.0;
+  IX(8, nx - 1) = 1.0 / 14.0;
+  for (int i = 2; i <= nx - 2; ++i) {
+    IX(1, i) = 1.0 / 20.0;
+    IX(2, i) = 3.0 / 4.0;
+    IX(3, i) = 3.0 / 4.0;
+    IX(4, i) = 1.0 / 20.0;
+    IX(6, i) = 3.0 / 10.0;
+    IX(7, i) = 1.0;
+    IX(8, i) = 3.0 / 10.0;
+  }
+  IX(1, nx) = 1.0 / 8.0;
+  IX(2, nx) = -7.0 / 8.0;
+  IX(3, nx) = 35.0 / 8.0;
+  IX(4, nx) = 35.0 / 8.0;
+  IX(6, nx) = 7.0;
+  IX(7, nx) = 1.0;
+  fd_lu(fix, nx, 2, 1);
+
+  /* ---- mid-point interpolation in y onto the wall positions, for u, w
+   * (fd_iy) and p (fd_iyp), coeft.f90:231-318 ---- */
+  for (int j = 1; j <= ny + 1; ++j) yp[j] = (y[j - 1] + y[j]) * 0.5;
+  for (int j = 1; j <= ny + 1; ++j) hi[j] = y[j] - y[j - 1];
+  for (int j = 2; j <= ny + 1; ++j) h[j] = yp[j] - yp[j - 1];
+  a = hi[2] / 2;
+  b = a + h[3];
+  c = b + h[4];
+  d = c + h[5];
+  IY(1, 1) = -(c * b * d / (a - d) / (a - c) / (a - b));
+  IY(2, 1) = c * a * d / (b - d) / (b - c) / (a - b);
+  IY(3, 1) = -(b * a * d / (c - d) / (ipow2(c) - a * c - b * c + b * a));
+  IY(4, 1) = 1.0 - (IY(1, 1) + IY(2, 1) + IY(3, 1));
+  a = hi[3] / 2;
+  b = a + h[4];
+  c = b + h[5];
+  d = c + h[6];
+  e = hi[2] / 2;
+  IY(1, 2) = 2 * c * b * ipow2(a) * d / (e + d) / (e + c) / (b + e) / (2 * ipow2(a) + ipow2(e) + 3 * e * a);
+  IY(2, 2) = -(2 * c * b * e * d / (a - d) / (a - c) / (a - b) / (a + e));
+  IY(3, 2) = 2 * c * e * ipow2(a) * d / (b - d) / (b - c) /
+             (2 * ipow2(a) * e + 2 * ipow2(a) * b - 3 * a * ipow2(b) - 3 * a * e * b + ipow3(b) + e * ipow2(b));
+  IY(4, 2) = -(2 * ipow2(a) * b * e * d / (c - d) /
+               (3 * e * a * ipow2(c) - 2 * e * ipow2(a) * c - 3 * b * e * a * c - 2 * ipow2(a) * ipow2(c) +
+                2 * ipow2(a) * e * b + 3 * a * ipow3(c) + b * ipow3(c) - e * ipow3(c) + 2 * b * ipow2(a) * c -
+                3 * b * a * ipow2(c) + b * e * ipow2(c) - ipow4(c)));
+  IY(7, 2) = 1.0;
+  IY(8, 2) = -(c * b * e * d / (2 * a + e) / (2 * a - d) / (2 * a - c) / (2 * a - b));
+  IY(5, 2) = (IY(7, 2) + IY(8, 2)) - (IY(1, 2) + IY(2, 2) + IY(3, 2) + IY(4, 2));
+  for (int j = 3; j <= ny - 1; ++j) {
+    a = hi[j + 1] / 2;
+    b = a + h[j + 2];
+    e = hi[j] / 2;
+    f = e + h[j];
+    IY(1, j) = 4 * ipow2(e) * ipow2(a) * b / (b + f) /
+               (2 * ipow2(a) * ipow2(f) + ipow4(f) + 4 * ipow2(e) * ipow2(a) - 6 * ipow2(a) * e * f -
+                9 * e * a * ipow2(f) + 6 * ipow2(e) * a * f + 2 * ipow2(e) * ipow2(f) + 3 * a * ipow3(f) -
+                3 * e * ipow3(f));
+    IY(2, j) = -(4 * f * ipow2(a) * b / (b + e) / (a + e) / (e - f) / (2 * a + e));
+    IY(3, j) = -(4 * f * ipow2(e) * b / (a - b) / (a + f) / (2 * ipow2(e) + ipow2(a) + 3 * e * a));
+    IY(6, j) = -(f * b * ipow2(a) / (a + e) / (2 * e - f) / (b + 2 * e) / (a + 2 * e));
+    IY(7, j) = 1.0;
+    IY(8, j) = -(f * ipow2(e) * b / (2 * a - b) / (2 * a + f) / (2 * ipow2(a) + ipow2(e) + 3 * e * a));
+    IY(4, j) = (IY(6, j) + IY(7, j) + IY(8, j)) - (IY(1, j) + IY(2, j) + IY(3, j));
+  }
+  a = hi[ny + 1] / 2;
+  e = hi[ny] / 2;
+  f = e + h[ny];
+  g = f + h[ny - 1];
+  {
+    const double n3 = 8 * ipow3(e) - 4 * g * ipow2(e) - 2 * f * a * e - 2 * g * e * a - 4 * f * ipow2(e) +
+                      g * a * f + 4 * a * ipow2(e) + 2 * f * g * e;
+    IY(1, ny) = 2 * (4 * ipow2(e) + 2 * e * a - a * f - 2 * f * e) * ipow2(e) / (e - g) / (f - g) / g / (g + a);
+    IY(2, ny) = -(2 * (2 * e * a + 4 * ipow2(e) - a * g - 2 * g * e) * ipow2(e) / (e - f) / f /
+                  (ipow2(f) + a * f - g * f - a * g));
+    IY(3, ny) = 2 * n3 /
+                (ipow3(e) + a * ipow2(e) - f * ipow2(e) - g * ipow2(e) + g * a * f - g * e * a + f * g * e - f * a * e);
+    IY(4, ny) = 2 * (-2 * f * e - 2 * g * e + g * f + 4 * ipow2(e)) * ipow2(e) / (g + a) / (a + f) / (a + e) / a;
+    IY(6, ny) = 1.0;
+    IY(7, ny) = n3 / g / a / f;
+  }
+  memcpy(fiyp, fiy, sizeof(double) * 8 * (size_t)ny);
+  a = hi[ny] / 2;
+  e = hi[ny - 1] / 2;
+  f = e + h[ny - 1];
+  IP(1, ny - 1) = 4 * ipow2(e) * ipow2(a) / (2 * a + f) / (a + f) / (2 * ipow2(e) + ipow2(f) - 3 * e * f);
+  IP(2, ny - 1) = -(4 * f * ipow2(a) / (3 * e * a + ipow2(e) + 2 * ipow2(a)) / (e - f));
+  IP(3, ny - 1) = 4 * ipow2(e) * f /
+                  (ipow3(a) + 2 * ipow2(e) * a + 3 * e * ipow2(a) + 2 * ipow2(e) * f + f * ipow2(a) + 3 * f * e * a);
+  IP(6, ny - 1) = -(f * ipow2(a) / (a + e) / (2 * e - f) / (2 * e + a));
+  IP(7, ny - 1) = 1.0;
+  IP(8, ny - 1) = ipow2(e) * f /
+                  (4 * ipow3(a) + 2 * ipow2(e) * a + 6 * e * ipow2(a) + 3 * f * e * a + ipow2(e) * f + 2 * f * ipow2(a));
+  e = hi[ny] / 2;
+  f = e + h[ny];
+  g = f + h[ny - 1];
+  IP(1, ny) = 2 * ipow2(e) * (2 * e - f) / (e - g) / (f - g) / g;
+  IP(2, ny) = -(2 * (2 * e - g) * ipow2(e) / (e - f) / f / (f - g));
+  IP(3, ny) = 2 * (4 * ipow2(e) + g * f - 2 * e * f - 2 * g * e) / (ipow2(e) - e * f + g * f - g * e);
+  IP(6, ny) = 1.0;
+  IP(7, ny) = (4 * ipow2(e) + g * f - 2 * e * f - 2 * g * e) / g / f;
+  fd_lu(fiyp, ny, 3, 2);
+  fd_lu(fiy, ny, 3, 2);
+#undef DV
+#undef FX
+#undef IX
+#undef IY
+#undef IP
+}
+
 int orc_coef_compute(const otbl_config *cfg, const double *yin, const double *u0in,
                      double *out) {
   if (!cfg || !yin || !u0in || !out) return OTBL_ERR_ARG;
@@ -711,6 +960,9 @@ int orc_coef_compute(const otbl_config *cfg, const double *yin, const double *u0
     for (i = 2; i <= nx - 1; ++i) VMAGIC(i) = (hm[i + 1] - hm[i - 1]) / (xm[i + 1] - xm[i - 1]);
     VMAGIC(nx) = (hm[nx] - hm[nx - 1]) / (xm[nx] - xm[nx - 1]);
   }
+
+  f_fd_operators(nx, ny, ax, pi, y, out + lay.off[OTBL_C_FD_DVDY], out + lay.off[OTBL_C_FD_DX],
+                 out + lay.off[OTBL_C_FD_IX], out + lay.off[OTBL_C_FD_IY], out + lay.off[OTBL_C_FD_IYP]);
 
   S[OTBL_S_RE] = re;
   S[OTBL_S_REX] = rex;

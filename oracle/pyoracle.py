@@ -85,6 +85,8 @@ def lib():
         L.orc_c2r_line.argtypes = [P, ctypes.c_int, ctypes.c_int, D, D, D]
         L.orc_r2c_line.argtypes = [P, ctypes.c_int, ctypes.c_int, D, D, D]
         L.orc_dct_line.argtypes = [P, ctypes.c_int, D, ctypes.c_int, D]
+        L.orc_statsp.argtypes = [P, D]
+        L.orc_stats_operator.argtypes = [P, ctypes.c_int, D, D]
         _lib = L
     return _lib
 
@@ -112,7 +114,8 @@ def coef_count(cfg) -> int:
             nz2 + 1, nx - 1, 3 * ny, nx, 3 * nx, 3 * nx, 2 * nx, 2 * nx, 16, 3 * nx, 3 * nx,
             2 * nx, 2 * nx, 20, 3 * nx, 3 * nx, 3 * nx, 3 * nx, 16, 3 * ny, 3 * ny, 2 * ny,
             2 * ny, 16, 3 * (ny + 1), 3 * ny, 2 * ny, 2 * ny, 16, 3 * (ny + 1), 3 * ny,
-            3 * (ny + 1), 3 * ny, 3 * ny, 3 * ny, 16, 8]
+            3 * (ny + 1), 3 * ny, 3 * ny, 3 * ny, 16, 8,
+            8 * ny, 8 * nx, 8 * nx, 8 * ny, 8 * ny]
     return int(sum(lens))
 
 
@@ -194,6 +197,25 @@ class OracleBox:
         st = self.L.orc_advance(self.h, nsteps)
         if st != 0:
             raise RuntimeError(f"oracle advance failed: {st}")
+
+    NSTATS = 40
+
+    def statsp(self, acc: np.ndarray | None = None) -> np.ndarray:
+        """Adds one sample of statsp (stotf.F90:51-291) of the current state
+        to acc, (NSTATS, nx, ny) (the reference's (ny, nx) per statistic),
+        and returns it."""
+        c = self.cfg
+        if acc is None:
+            acc = np.zeros((self.NSTATS, c.nx, c.ny))
+        self.L.orc_statsp(self.h, dptr(acc))
+        return acc
+
+    def stats_operator(self, op: int, line: np.ndarray, n_out: int) -> np.ndarray:
+        """One line/column through a statistics operator: 0 interpx_new, 1
+        diffx, 2 interpy_new (u), 3 interpy_new (p), 4 diffy."""
+        out = np.zeros(n_out)
+        self.L.orc_stats_operator(self.h, op, dptr(np.ascontiguousarray(line, dtype=np.float64)), dptr(out))
+        return out
 
     def divergence(self):
         c = self.cfg
