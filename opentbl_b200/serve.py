@@ -9,9 +9,12 @@ in chunks of RK3 steps, each chunk one CUDA graph launch, so the kernels of
 all admitted requests overlap on the device. Slots are kept when their
 request finishes and re-bound (otbl_ctx_rebind) to the next request of the
 same grid size and precision; idle slots of other sizes are released when
-memory is needed. New slots are created (device allocation, coefficient
-upload, autotuning) on a background host thread, so the loop keeps feeding
-the running requests meanwhile. The host loop never blocks on the device:
+memory is needed. A slot is prepared for its request on a background host
+thread (a new context: device allocation, coefficient upload, autotuning;
+or an idle one re-bound: the request's coefficients and initial fields
+uploaded on the slot's stream; then the capture of its chunk's CUDA graph),
+so the loop keeps feeding the running requests meanwhile. The host loop
+never blocks on the device:
 it polls each slot (otbl_query / otbl_graph_query) and issues the next chunk
 when the last one has finished.
 
@@ -171,40 +174,46 @@ class Server:
                 return True
         return False
 
-    def _create(self, req: Request, init: dict, need: int, key) -> "_Slot":
-        """Runs on the creation thread: a new context for req, autotuned (or
-        given the CTA sizes already picked for its grid size)."""
+    def _prepare(self, req: Request, init: dict, slot: "_Slot | None", need: int, key):
+        """Runs on the preparation thread: a new context for req, autotuned
+        (or given the CTA sizes already picked for its grid size), or the
+        idle `slot` re-bound to req; then the CUDA graph of its chunk."""
         t = time.perf_counter()
-        box = Box(req.cfg, init, device=self.device)
-        if self.autotune:
-            if key in self.tuning:
-                box.set_tuning(self.tuning[key])
-            else:
-                self.tuning[key] = box.autotune()
-        self.stats["create_s"] += time.perf_counter() - t
-        return _Slot(box, need)
+        if slot is None:
+            box = Box(req.cfg, init, device=self.device)
+            if self.autotune:
+                if key in self.tuning:
+                    box.set_tuning(self.tuning[key])
+                else:
+                    self.tuning[key] = box.autotune()
+            slot = _Slot(box, need)
+            self.stats["create_s"] += time.perf_counter() - t
+        else:
+            slot.box.rebind(req.cfg, init)
+            self.stats["rebind_s"] += time.perf_counter() - t
+        t = time.perf_counter()
+        slot.chunk = min(self.chunk, req.steps)
+        slot.graph = Graph([slot.box], slot.chunk) if req.steps >= slot.chunk else None
+        self.stats["capture_s"] += time.perf_counter() - t
+        return slot
 
     def _acquire(self, req: Request, init: dict):
-        """A slot for the request at the head of the queue: an idle slot of
-        its grid size re-bound at once, or a new one created in the
-        background (None until it is ready, or while memory is short)."""
+        """A slot for the request at the head of the queue, prepared in the
+        background: an idle slot of its grid size re-bound, or a new one
+        (None until it is ready, or while memory is short)."""
         key = size_key(req.cfg)
         if self.pending is not None:
-            preq, fut = self.pending
+            preq, fut, created = self.pending
             if preq is not req or not fut.done():
                 return None
             self.pending = None
-            s = fut.result()
-            self.stats["created"] += 1
-            return s
+            self.stats["created" if created else "reused"] += 1
+            return fut.result()
         lst = self.idle.get(key)
         if lst:
-            t = time.perf_counter()
             s = lst.pop()
-            s.box.rebind(req.cfg, init)
-            self.stats["reused"] += 1
-            self.stats["rebind_s"] += time.perf_counter() - t
-            return s
+            self.pending = (req, self.creator.submit(self._prepare, req, init, s, s.nbytes, key), False)
+            return None
         need = self._bytes(req.cfg, init)
         while self.used + need > self.budget and self._evict_one():
             pass
@@ -212,7 +221,7 @@ class Server:
             return None
         self.used += need
         self.stats["peak_bytes"] = max(self.stats["peak_bytes"], self.used)
-        self.pending = (req, self.creator.submit(self._create, req, init, need, key))
+        self.pending = (req, self.creator.submit(self._prepare, req, init, None, need, key), True)
         return None
 
     def _issue(self, s: _Slot):
@@ -273,10 +282,6 @@ class Server:
                 queue.popleft()
                 s.req = req
                 s.remaining = req.steps
-                s.chunk = min(self.chunk, req.steps)
-                t = time.perf_counter()
-                s.graph = Graph([s.box], s.chunk) if req.steps >= s.chunk else None
-                self.stats["capture_s"] += time.perf_counter() - t
                 s.admitted = time.perf_counter() - t0
                 active.append(s)
                 self._issue(s)
