@@ -153,16 +153,36 @@ __global__ void __launch_bounds__(128) k_products(DCoef c, ZTabT<T> z, ProdArgs<
 // Register layout L: lane t holds complex element n = t + 32 m in v[m],
 // m < E = M/32. Passes: radix 8 (Ns = 1), radix 8 (Ns = 8), radix R3
 // (Ns = 64); the first reads L, the last writes L, the two in between go
-// through a per-warp shared buffer whose index i is stored at i + i/8, which
-// makes every pass conflict-free. The arithmetic is warp_fft's, operation
-// for operation.
+// through a per-warp shared buffer. Its element i is stored at i + i/8 for
+// 16-byte (FP64) elements and at i ^ ((i/8) mod 16) for 8-byte (FP32) ones,
+// which makes every exchange of the three passes conflict-free for its
+// element size (a bank model of the access patterns: the FP32 buffer at
+// i + i/8 needed 160 wavefronts per transform where 96 is the minimum, and
+// ncu showed 15 M of its 42 M shared wavefronts as conflicts at
+// 257x193x512). The real-to-complex post-step takes the mirrored element
+// Z[M-k] from the lane that holds it by warp shuffles instead of a round
+// trip through the buffer. The arithmetic is warp_fft's, operation for
+// operation.
 // ---------------------------------------------------------------------------
 template <int M>
 struct ZPlan {
   static constexpr int E = M / 32;
   static constexpr int R3 = 4;  // 256 = 8 x 8 x 4
 };
-__device__ __forceinline__ int zpad(int i) { return i + (i >> 3); }
+template <typename V>
+__device__ __forceinline__ int zpad(int i) {
+  if constexpr (sizeof(V) == 16)
+    return i + (i >> 3);
+  else
+    return i ^ ((i >> 3) & 15);
+}
+template <typename V>
+__device__ __forceinline__ V shfl_cx(V v, int src) {
+  V r;
+  r.x = __shfl_sync(0xffffffffu, v.x, src);
+  r.y = __shfl_sync(0xffffffffu, v.y, src);
+  return r;
+}
 
 // inverse (SIGN = +1) or forward (SIGN = -1) FFT of a line in layout L
 template <int M, int SIGN, typename V>
@@ -178,7 +198,7 @@ __device__ __forceinline__ void zfft_regs(V (&L)[M / 32], V *buf, const V *__res
     dft_small<8, SIGN>(v);
     const int j = t + 32 * it;
 #pragma unroll
-    for (int r = 0; r < 8; ++r) buf[zpad(j * 8 + r)] = v[r];
+    for (int r = 0; r < 8; ++r) buf[zpad<V>(j * 8 + r)] = v[r];
   }
   __syncwarp();
   // pass B: radix 8, Ns = 8
@@ -188,7 +208,7 @@ __device__ __forceinline__ void zfft_regs(V (&L)[M / 32], V *buf, const V *__res
     for (int it = 0; it < IA; ++it) {
       const int j = t + 32 * it;
 #pragma unroll
-      for (int r = 0; r < 8; ++r) v[it][r] = buf[zpad(j + r * (M / 8))];
+      for (int r = 0; r < 8; ++r) v[it][r] = buf[zpad<V>(j + r * (M / 8))];
     }
     __syncwarp();
 #pragma unroll
@@ -203,7 +223,7 @@ __device__ __forceinline__ void zfft_regs(V (&L)[M / 32], V *buf, const V *__res
       dft_small<8, SIGN>(v[it]);
       const int base = (j / 8) * 64 + k;
 #pragma unroll
-      for (int r = 0; r < 8; ++r) buf[zpad(base + r * 8)] = v[it][r];
+      for (int r = 0; r < 8; ++r) buf[zpad<V>(base + r * 8)] = v[it][r];
     }
   }
   __syncwarp();
@@ -215,7 +235,7 @@ __device__ __forceinline__ void zfft_regs(V (&L)[M / 32], V *buf, const V *__res
     for (int it = 0; it < IC; ++it) {
       const int j = t + 32 * it;
 #pragma unroll
-      for (int r = 0; r < R3; ++r) v[it][r] = buf[zpad(j + r * (M / R3))];
+      for (int r = 0; r < R3; ++r) v[it][r] = buf[zpad<V>(j + r * (M / R3))];
     }
     __syncwarp();
 #pragma unroll
@@ -271,18 +291,19 @@ __device__ __forceinline__ void zr2c_regs(const ZTabT<T> &z, V2<T> (&L)[M / 32],
   using V = V2<T>;
   constexpr int E = M / 32;
   zfft_regs<M, -1>(L, buf, z.tw, t);
-  __syncwarp();
-#pragma unroll
-  for (int m = 0; m < E; ++m) buf[zpad(t + 32 * m)] = L[m];
-  __syncwarp();
   const int nz2 = z.nz2;
   const T dnf = T(1) / (T)z.nz;
 #pragma unroll
   for (int m = 0; m < E; ++m) {
+    // Z[(M - k) mod M], k = t + 32 m: element (32 - t) + 32 (E - 1 - m), held
+    // by lane 32 - t in L[E - 1 - m] for t >= 1; element 32 ((E - m) mod E),
+    // this lane's own L[(E - m) mod E], for t = 0
+    const V other = shfl_cx(L[E - 1 - m], (32 - t) & 31);
+    const V zm = t == 0 ? L[(E - m) % E] : other;
     const int k = t + 32 * m;
     if (k <= nz2) {
       const V zk = L[m];
-      const V zc = cconj(buf[zpad((M - k) & (M - 1))]);
+      const V zc = cconj(zm);
       const V e = cmake<V>(T(0.5) * (zk.x + zc.x), T(0.5) * (zk.y + zc.y));
       const V d = csub(zk, zc);
       const V o = cmake<V>(T(0.5) * d.y, T(-0.5) * d.x);  // -i d / 2
