@@ -81,6 +81,11 @@ MED = BoxConfig(nx=513, ny=193, nz=256, lx=40.0, ly=10.0, lz=8.0,
 # device, for profiling captures
 SLAB = BoxConfig(nx=257, ny=193, nz=512, lx=20.0, ly=10.0, lz=10.0,
                  re_theta=1000.0, profile="musker", name="SLAB-257x193x512")
+# the x extent of the 1025x193x512 box with a quarter of its rows (the x-line
+# and x-DCT kernels take the code path of the full box, n = 1024): fields of
+# 139 MB, about 3.6 GB on the device, for profiling captures
+STRIP = BoxConfig(nx=1025, ny=49, nz=512, lx=80.0, ly=10.0, lz=10.0,
+                  re_theta=1000.0, profile="musker", name="STRIP-1025x49x512")
 # small box for tests and smoke runs
 TINY = BoxConfig(nx=33, ny=41, nz=32, lx=12.0, ly=6.0, lz=4.0, dy_wall=0.02,
                  re_theta=300.0, profile="blasius", y_blend=1.5,

@@ -243,10 +243,39 @@ __device__ __forceinline__ void block_fft(V *buf, int n, const V *__restrict__ t
   while (rem % 5 == 0) { block_pass<5, SIGN, NB>(buf, n, Ns, tw); Ns *= 5; rem /= 5; }
 }
 
-// Padded shared-memory index for the line FFTs below: one double2 of padding
-// every 8, which turns the radix-8, Ns = 1 write stride of 8 elements (128
-// bytes, a 32-way bank conflict) into 9.
-__device__ __forceinline__ int xpad(int i) { return i + (i >> 3); }
+// Shared-memory index of element i of a line for the line FFTs below.
+// 16-byte (FP64) elements: one element of padding every 8, which turns the
+// radix-8, Ns = 1 write stride of 8 elements (128 bytes, a 32-way bank
+// conflict) into 9. 8-byte (FP32) elements: i ^ ((i / 8) mod 16), a
+// permutation inside each block of 128 elements that keeps every run of 16
+// consecutive elements on distinct banks and sends the stride-8 writes to 16
+// distinct bank pairs (the padding of the FP64 layout leaves two of every 16
+// consecutive FP32 elements on one bank pair).
+template <typename V>
+__host__ __device__ __forceinline__ int xpad(int i) {
+  if constexpr (sizeof(V) == 16)
+    return i + (i >> 3);
+  else
+    return i ^ ((i >> 3) & 15);
+}
+
+// Line stride (elements) of MB lines of n elements in the layout of xpad:
+// the first index past a line, rounded up so that the MB lines start P / MB
+// elements apart modulo the P elements of a 128-byte bank row (P = 8 for
+// FP64, 16 for FP32), which spreads the MB lines of one plane row, loaded and
+// stored by consecutive threads, over distinct banks. For n = 1024, MB = 4 a
+// bank model of the x-DCT kernels' accesses gives 3200 wavefronts per CTA
+// for FP32 (6208 with the FP64 layout and an odd stride; 2816 minimum) and
+// 6272 for FP64 (7040 with an odd stride; 5632 minimum).
+template <typename V>
+__host__ __device__ __forceinline__ int xline_ld(int n, int MB) {
+  if constexpr (sizeof(V) == 16) {
+    const int b = xpad<V>(n - 1) + 1;
+    return b + (((8 / MB - b) % 8) + 8) % 8;
+  } else {
+    return ((n + 15) / 16) * 16 + 16 / MB;
+  }
+}
 
 // Stockham pass as stockham_pass, on a padded line, by the G threads (rank t)
 // that own this line; every thread of the CTA runs the same passes on its own
@@ -261,7 +290,7 @@ __device__ __forceinline__ void stockham_pass_pad(V *buf, int M, int Ns, const V
     const int j = t + it * G;
     if (j < nit) {
 #pragma unroll
-      for (int r = 0; r < R; ++r) v[it][r] = buf[xpad(j + r * nit)];
+      for (int r = 0; r < R; ++r) v[it][r] = buf[xpad<V>(j + r * nit)];
     }
   }
   __syncthreads();
@@ -281,7 +310,7 @@ __device__ __forceinline__ void stockham_pass_pad(V *buf, int M, int Ns, const V
       dft_small<R, SIGN>(v[it]);
       const int base = (j / Ns) * Ns * R + k;
 #pragma unroll
-      for (int r = 0; r < R; ++r) buf[xpad(base + r * Ns)] = v[it][r];
+      for (int r = 0; r < R; ++r) buf[xpad<V>(base + r * Ns)] = v[it][r];
     }
   }
   __syncthreads();

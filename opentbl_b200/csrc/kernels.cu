@@ -921,10 +921,11 @@ using XTab = XTabT<double>;
 // The x-line transforms of pois: MB spanwise modes of one row j per CTA of
 // 256 threads. The loads and stores walk the planes with the MB modes of a
 // plane on consecutive threads (MB x 16 contiguous bytes per plane row); the
-// MB complex lines of length n = nx-1 sit in padded shared memory (line
-// stride xpad(n) | 1, odd, so that the MB lines of one plane fall in
-// different banks) and are transformed together, 256/MB threads per line.
-// MB is chosen per n so that n * MB <= 4096 (n = 1024: 4 modes, 74 KB).
+// MB complex lines of length n = nx-1 sit in shared memory in the layout of
+// xpad (line stride xline_ld, which puts the MB lines of one plane on
+// different banks) and are transformed together, NT/MB threads per line.
+// MB is chosen per n so that n * MB <= 4096 (n = 1024: 4 modes, 74 KB in
+// FP64, 33 KB in FP32).
 
 // divergence (pois.f90:41-54) + DCT-II along x (cosftx iopt=-1); output
 // phi-hat in plane layout (v-type, plane i = x-mode index + 2). Mode 0 made
@@ -944,7 +945,7 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 2 : 1) k_pois_fwd(DCoef c, XTa
   using V = V2<T>;
   extern __shared__ __align__(16) unsigned char xsm_raw[];
   V *xsm = reinterpret_cast<V *>(xsm_raw);
-  const int n = x.n, ld = xpad(n) | 1, ny = c.ny, nz1 = c.nz1, xr = c.xround;
+  const int n = x.n, ld = xline_ld<V>(n, MB), ny = c.ny, nz1 = c.nz1, xr = c.xround;
   const int j = blockIdx.y + 1;
   const int k0 = kbeg + blockIdx.x * MB;
   const size_t PU = (size_t)(ny + 1) * nz1, PV = (size_t)ny * nz1;
@@ -971,7 +972,7 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 2 : 1) k_pois_fwd(DCoef c, XTa
       val.y = (T)rnd(im, xr);
     }
     const int dst = (tt & 1) ? n - 1 - (tt >> 1) : (tt >> 1);
-    xsm[l * ld + xpad(dst)] = val;
+    xsm[l * ld + xpad<V>(dst)] = val;
   }
   __syncthreads();
   {
@@ -983,7 +984,7 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 2 : 1) k_pois_fwd(DCoef c, XTa
     const int l = e % MB, kk = e / MB;
     const int k = k0 + l;
     if (k > kend) continue;
-    const V Vv = xsm[l * ld + xpad(kk)], Vm = xsm[l * ld + xpad(kk == 0 ? 0 : n - kk)];
+    const V Vv = xsm[l * ld + xpad<V>(kk)], Vm = xsm[l * ld + xpad<V>(kk == 0 ? 0 : n - kk)];
     const V wq = __ldg(x.tw2 + kk);
     const V y = cadd(cmul(wq, Vv), cmul(cconj(wq), Vm));
     V out;
@@ -999,7 +1000,7 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 2 : 1) k_pois_bwd(DCoef c, XTa
   using V = V2<T>;
   extern __shared__ __align__(16) unsigned char xsm_raw[];
   V *xsm = reinterpret_cast<V *>(xsm_raw);
-  const int n = x.n, ld = xpad(n) | 1, ny = c.ny, nz1 = c.nz1, xr = c.xround;
+  const int n = x.n, ld = xline_ld<V>(n, MB), ny = c.ny, nz1 = c.nz1, xr = c.xround;
   const int j = blockIdx.y + 1;
   const int k0 = kbeg + blockIdx.x * MB;
   const size_t PV = (size_t)ny * nz1;
@@ -1026,7 +1027,7 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 2 : 1) k_pois_bwd(DCoef c, XTa
       d.y = Y.y - Ym.x;
       val = cmul(cconj(__ldg(x.tw2 + kk)), d);
     }
-    xsm[l * ld + xpad(kk)] = val;
+    xsm[l * ld + xpad<V>(kk)] = val;
   }
   __syncthreads();
   {
@@ -1037,7 +1038,7 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 2 : 1) k_pois_bwd(DCoef c, XTa
     const int l = e % MB, tt = e / MB;
     const int k = k0 + l;
     if (k > kend) continue;
-    const V Vv = xsm[l * ld + xpad((tt & 1) ? n - 1 - (tt >> 1) : (tt >> 1))];
+    const V Vv = xsm[l * ld + xpad<V>((tt & 1) ? n - 1 - (tt >> 1) : (tt >> 1))];
     // mode 0 is real (pois.f90:102): its imaginary pencil is identically zero
     // in the reference's real transforms, while the complex line transform
     // used here leaves rounding-level values there
@@ -1048,39 +1049,63 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 2 : 1) k_pois_bwd(DCoef c, XTa
   }
 }
 
-// projection, pois.f90:144-162; one thread per (i >= 2, j, kr). phi holds
-// the columns kr < kr_split in FP64 (phi64) and the others in FP32 (phi32,
-// the mixed path's higher spanwise modes); the update is FP64.
+// projection, pois.f90:144-162; one thread per (i >= 2, j, spanwise mode k),
+// the mode's two components kr = 2k, 2k+1 together (16-byte velocity and
+// 8- or 16-byte phi and p accesses; the w update of one component takes the
+// other component's phi, pof = +-1 in the reference). phi holds the modes
+// 2k < kr_split in FP64 (phi64) and the others in FP32 (phi32, the mixed
+// path's higher spanwise modes); the update is FP64, operation for operation
+// the reference's per-component statements.
 template <typename TP>
-__global__ void __launch_bounds__(128) k_project(DCoef c, const DState *st, const double *__restrict__ phi64,
+__global__ void __launch_bounds__(256) k_project(DCoef c, const DState *st, const double *__restrict__ phi64,
                                                  const float *__restrict__ phi32, int kr_split, double *u,
                                                  double *v, double *w, TP *p) {
-  const int kr = blockIdx.x * blockDim.x + threadIdx.x;
-  if (kr >= c.nz1) return;
-  const int j = blockIdx.y + 1, i = blockIdx.z + 2;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int nx = c.nx, ny = c.ny, nz1 = c.nz1;
+  if (2 * k >= nz1) return;
+  const int j = blockIdx.y + 1, i = blockIdx.z + 2;
   const size_t PU = (size_t)(ny + 1) * nz1, PV = (size_t)ny * nz1;
-  const int k = kr >> 1, odd = kr & 1, pof = odd ? -1 : 1;
   const double kz = c.kaz[k];
-  const size_t base = (size_t)(i - 1) * PV + kr;  // phi(j, i) at base + (j-1)*nz1
-  const bool lo = kr < kr_split;                  // kr and kr + pof are one mode
-  auto F = [&](long off) { return lo ? phi64[(long)base + off] : (double)phi32[(long)base + off]; };
+  const size_t base = (size_t)(i - 1) * PV + 2 * k;  // phi(j, i) at base + (j-1)*nz1
+  const bool lo = 2 * k < kr_split;
+  auto F = [&](size_t off) -> double2 {
+    if (lo) return *reinterpret_cast<const double2 *>(phi64 + base + off);
+    const float2 f = *reinterpret_cast<const float2 *>(phi32 + base + off);
+    return make_double2((double)f.x, (double)f.y);
+  };
+  using VP = V2<TP>;
+  double2 f1 = make_double2(0.0, 0.0);
+  if (j <= ny - 1) f1 = F((size_t)(j - 1) * nz1);
   if (j >= 2) {
-    const double fm = F((long)(j - 2) * nz1);
-    TP *pq = p + (size_t)(i - 1) * PV + (size_t)(j - 1) * nz1 + kr;
-    *pq = (TP)(st->varstep * fm + (double)*pq);
-    const double q = F((long)(j - 2) * nz1 + pof);
-    const double kf = odd ? kz * q : -kz * q;
-    double *wq = w + (size_t)(i - 1) * PU + (size_t)(j - 1) * nz1 + kr;
-    *wq = *wq - kf;
-  }
-  if (j >= 2 && j <= ny - 1) {
-    double *vq = v + (size_t)(i - 1) * PV + (size_t)(j - 1) * nz1 + kr;
-    *vq = *vq - c.idyy[j - 1] * (F((long)(j - 1) * nz1) - F((long)(j - 2) * nz1));
+    const double2 fm = F((size_t)(j - 2) * nz1);
+    VP *pq = reinterpret_cast<VP *>(p + (size_t)(i - 1) * PV + (size_t)(j - 1) * nz1 + 2 * k);
+    const VP p0 = *pq;
+    VP p1;
+    p1.x = (TP)(st->varstep * fm.x + (double)p0.x);
+    p1.y = (TP)(st->varstep * fm.y + (double)p0.y);
+    *pq = p1;
+    double2 *wq = reinterpret_cast<double2 *>(w + (size_t)(i - 1) * PU + (size_t)(j - 1) * nz1 + 2 * k);
+    double2 wv = *wq;
+    wv.x = wv.x - -kz * fm.y;
+    wv.y = wv.y - kz * fm.x;
+    *wq = wv;
+    if (j <= ny - 1) {
+      const double dy = c.idyy[j - 1];
+      double2 *vq = reinterpret_cast<double2 *>(v + (size_t)(i - 1) * PV + (size_t)(j - 1) * nz1 + 2 * k);
+      double2 vv = *vq;
+      vv.x = vv.x - dy * (f1.x - fm.x);
+      vv.y = vv.y - dy * (f1.y - fm.y);
+      *vq = vv;
+    }
   }
   if (j <= ny - 1 && i <= nx - 1) {
-    double *uq = u + (size_t)(i - 1) * PU + (size_t)j * nz1 + kr;
-    *uq = *uq - c.S[OTBL_S_IDXX] * (F((long)PV + (long)(j - 1) * nz1) - F((long)(j - 1) * nz1));
+    const double2 f2 = F(PV + (size_t)(j - 1) * nz1);
+    const double idxx = c.S[OTBL_S_IDXX];
+    double2 *uq = reinterpret_cast<double2 *>(u + (size_t)(i - 1) * PU + (size_t)j * nz1 + 2 * k);
+    double2 uv = *uq;
+    uv.x = uv.x - idxx * (f2.x - f1.x);
+    uv.y = uv.y - idxx * (f2.y - f1.y);
+    *uq = uv;
   }
 }
 
@@ -1184,7 +1209,6 @@ __global__ void k_twiddles(double2 *tw, int n, double2 *tw2, int n2, int mode2) 
   }
 }
 
-static inline int xpad_host(int i) { return i + (i >> 3); }
 #ifndef OTBL_POIS_NT
 #define OTBL_POIS_NT 512
 #endif
@@ -1473,7 +1497,7 @@ static void pois_xdct(otbl_ctx *c, bool fwd, T *phi, int kbeg, int kend) {
   const int ny = c->cfg.ny, n = c->cfg.nx - 1;
   // modes per CTA: n * MB <= 4096 and at most 8
   const int MB = n <= 512 ? 8 : (n <= 1024 ? 4 : (n <= 2048 ? 2 : 1));
-  const size_t smem = (size_t)MB * (xpad_host(n) | 1) * sizeof(V2<T>);
+  const size_t smem = (size_t)MB * xline_ld<V2<T>>(n, MB) * sizeof(V2<T>);
   const dim3 gx((kend - kbeg + 1 + MB - 1) / MB, ny - 1);
   // threads per CTA: 512 when the CTA holds 2048-4096 points (fewer items
   // and registers per thread, the same barriers), else 256
@@ -1525,14 +1549,16 @@ cudaError_t launch_pois(otbl_ctx *c, int m) {
   pois_xdct<double>(c, false, phi64, 0, klo - 1);
   if (klo <= nz2) pois_xdct<float>(c, false, phi32, klo, nz2);
   prof_end(c);
-  dim3 gp((nz1 + 127) / 128, ny, nx - 1);
+  // one thread per complex mode: 170 modes of nz = 512 in one CTA of 192
+  const int nmodes = nz1 / 2, pt = std::min(256, (nmodes + 31) / 32 * 32);
+  dim3 gp((nmodes + pt - 1) / pt, ny, nx - 1);
   prof_begin(c, PK_PROJECT);
   if (c->f32[OTBL_F_P])
-    k_project<float><<<gp, 128, 0, c->stream>>>(c->dc, c->st, phi64, phi32, kr_split, c->f[OTBL_F_U],
+    k_project<float><<<gp, pt, 0, c->stream>>>(c->dc, c->st, phi64, phi32, kr_split, c->f[OTBL_F_U],
                                                 c->f[OTBL_F_V], c->f[OTBL_F_W],
                                                 reinterpret_cast<float *>(c->f[OTBL_F_P]));
   else
-    k_project<double><<<gp, 128, 0, c->stream>>>(c->dc, c->st, phi64, phi32, kr_split, c->f[OTBL_F_U],
+    k_project<double><<<gp, pt, 0, c->stream>>>(c->dc, c->st, phi64, phi32, kr_split, c->f[OTBL_F_U],
                                                  c->f[OTBL_F_V], c->f[OTBL_F_W], c->f[OTBL_F_P]);
   prof_end(c);
   c->launches += 1;
