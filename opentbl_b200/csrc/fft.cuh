@@ -333,4 +333,21 @@ __device__ __forceinline__ void block_fft_lines(V *buf, int n, const V *__restri
   while (rem % 5 == 0) { stockham_pass_pad<5, SIGN, I5>(buf, n, Ns, tw, t, G); Ns *= 5; rem /= 5; }
 }
 
+// block_fft_lines for a length N = 2^a known at compile time: the same
+// passes in the same order (8s, 4s, 2s), each with its constant stride. Inside
+// the persistent x-DCT kernels' tile loop the run-time form needs more than
+// the 128 registers a 512-thread CTA may hold (ptxas: 0.1-2 KB of spills per
+// thread with the run-time length, none with this one).
+template <int SIGN, int NT, int N, int NS = 1, typename V>
+__device__ __forceinline__ void block_fft_lines_n(V *buf, const V *__restrict__ tw, int t, int G) {
+  constexpr int rem = N / NS;
+  if constexpr (rem > 1) {
+    static_assert(rem % 2 == 0, "power-of-two lengths only");
+    constexpr int R = rem % 8 == 0 ? 8 : (rem % 4 == 0 ? 4 : 2);
+    constexpr int MAXIT = (4096 / R + NT - 1) / NT;
+    stockham_pass_pad<R, SIGN, MAXIT>(buf, N, NS, tw, t, G);
+    block_fft_lines_n<SIGN, NT, N, NS * R>(buf, tw, t, G);
+  }
+}
+
 }  // namespace otbl

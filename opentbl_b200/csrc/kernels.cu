@@ -25,6 +25,7 @@
 // REAL4 rounding of the transposed payload (OTBL_XPOSE_FP32) is applied at
 // exactly the loads/stores where the reference transposes.
 #include <cfloat>
+#include <cudaTypedefs.h>
 #include <mutex>
 #include <algorithm>
 #include <type_traits>
@@ -32,6 +33,7 @@
 #include "devcommon.cuh"
 #include "fft.cuh"
 #include "otbl_internal.cuh"
+#include "tma.cuh"
 #include "zline.cuh"
 
 namespace otbl {
@@ -1049,6 +1051,231 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 2 : 1) k_pois_bwd(DCoef c, XTa
   }
 }
 
+// TMA-fed persistent forms of the two x-DCT kernels, for the power-of-two
+// line lengths N = 256..2048. One CTA per SM (two for the FP32 backward
+// transform) walks the tiles q = blockIdx.x + m gridDim.x, a tile being row j
+// and MB spanwise modes (k-group fastest, so the CTAs at work share rows and
+// the v row pair of a tile meets its neighbour's in L2). The loads are TMA
+// boxes issued by thread 0 and counted on mbarriers, the waits bounded
+// (OTBL_ERR_TIMEOUT, after draining the copies in flight); the next tile's
+// data arrive while this tile's FFT runs, which the one-shot kernels above
+// leave to other CTAs' warps (measured there: long-scoreboard stalls 15 per
+// issue in the forward, 7 in the backward transform, DRAM at 30% and 9% of
+// its peak on a 1025x49x512 box). Arithmetic: k_pois_fwd's and k_pois_bwd's,
+// operation for operation.
+
+// spanwise modes per x-DCT CTA: n * MB <= 4096 and at most 8
+__host__ __device__ constexpr int pois_mb(int n) { return n <= 512 ? 8 : (n <= 1024 ? 4 : (n <= 2048 ? 2 : 1)); }
+
+template <int MB>
+struct PoisChunk {
+  static constexpr int CP = MB >= 8 ? 64 : 128;  // planes per chunk
+  static constexpr int RW = 2 * MB;              // kr of a row segment
+  static constexpr int UB = ((CP + 1) * RW * 8 + 127) / 128 * 128;
+  static constexpr int VB = CP * 2 * RW * 8, WB = CP * RW * 8;
+  static constexpr int CH = UB + VB + WB;  // chunk stride in the ring (bytes)
+  static constexpr unsigned TX = (unsigned)((CP + 1) * RW * 8 + VB + WB);
+};
+
+// forward: the tile's velocity rows stream through a ring of S chunks of CP
+// planes (u row j over CP + 1 planes, v rows j - 1 and j, w row j); thread 0
+// refills a slot at the first CTA barrier after its chunk was read, so S
+// chunks are in flight through the FFT
+template <typename T, int N>
+__global__ void __launch_bounds__(512, 1) k_pois_fwd_t(DCoef c, XTabT<T> x, const __grid_constant__ PoisMaps maps,
+                                                      T *__restrict__ phi, int kbeg, int kend, int S, int *err) {
+  using V = V2<T>;
+  constexpr int MB = pois_mb(N), NT = 512, n = N;
+  using P = PoisChunk<MB>;
+  extern __shared__ __align__(128) unsigned char pxraw[];
+  const int ld = xline_ld<V>(n, MB), ny = c.ny, nz1 = c.nz1, xr = c.xround;
+  V *xsm = reinterpret_cast<V *>(pxraw + (size_t)S * P::CH);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(pxraw + (size_t)S * P::CH +
+                                               ((size_t)MB * ld * sizeof(V) + 15) / 16 * 16);
+  const int t = threadIdx.x;
+  const int nkg = (kend - kbeg) / MB + 1, ntile = nkg * (ny - 1);
+  const int mine = (int)blockIdx.x < ntile ? (ntile - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  const int NC = (n + P::CP - 1) / P::CP, G = mine * NC;
+  const size_t PV = (size_t)ny * nz1;
+  int issued = 0;  // thread 0's count of chunks issued
+  auto issue_upto = [&](int h_end) {
+    for (; issued < h_end && issued < G; ++issued) {
+      const int h = issued, sl = h % S, q = (int)blockIdx.x + (h / NC) * (int)gridDim.x;
+      const int j = q / nkg + 1, k0 = kbeg + (q % nkg) * MB, tt0 = (h % NC) * P::CP;
+      unsigned char *b = pxraw + (size_t)sl * P::CH;
+      mbar_arrive_expect_tx(&bar[sl], P::TX);
+      tma_load_3d(b, &maps.u, 2 * k0, j, tt0, &bar[sl]);
+      tma_load_3d(b + P::UB, &maps.v, 2 * k0, j - 1, tt0 + 1, &bar[sl]);
+      tma_load_3d(b + P::UB + P::VB, &maps.w, 2 * k0, j, tt0 + 1, &bar[sl]);
+    }
+  };
+  if (t == 0) {
+    for (int sl = 0; sl < S; ++sl) mbar_init(&bar[sl], 1);
+    mbar_init_fence();
+  }
+  __syncthreads();
+  if (t == 0) issue_upto(S);
+  const double idx = c.S[OTBL_S_IDX];
+  int g = 0;
+  for (int m = 0; m < mine; ++m) {
+    const int q = (int)blockIdx.x + m * (int)gridDim.x;
+    const int j = q / nkg + 1, k0 = kbeg + (q % nkg) * MB;
+    const double idy = c.idy[j];
+    for (int cc = 0; cc < NC; ++cc, ++g) {
+      const int sl = g % S;
+      const bool ok = mbar_wait_bounded(&bar[sl], (unsigned)((g / S) & 1), 2000000000ull);
+      if (__syncthreads_or(!ok)) {
+        if (t == 0) {
+          atomicExch(err, OTBL_ERR_TIMEOUT);
+          for (int h = g; h < issued; ++h) mbar_wait_bounded(&bar[h % S], (unsigned)((h / S) & 1), 200000000ull);
+        }
+        return;
+      }
+      if (t == 0) issue_upto(g + S);  // chunks before g are consumed
+      const unsigned char *b = pxraw + (size_t)sl * P::CH;
+      const double *us = reinterpret_cast<const double *>(b);
+      const double *vs = reinterpret_cast<const double *>(b + P::UB);
+      const double *ws = reinterpret_cast<const double *>(b + P::UB + P::VB);
+      const int tt0 = cc * P::CP;
+      for (int e = t; e < P::CP * MB; e += NT) {
+        const int l = e % MB, pl = e / MB, tt = tt0 + pl;
+        if (tt >= n) continue;
+        const int k = k0 + l;
+        V val;
+        val.x = 0;
+        val.y = 0;
+        if (k <= kend) {
+          const double kz = c.kaz[k];
+          const double2 wv = *reinterpret_cast<const double2 *>(ws + pl * P::RW + 2 * l);
+          const double2 v1 = *reinterpret_cast<const double2 *>(vs + (2 * pl + 1) * P::RW + 2 * l);
+          const double2 v0 = *reinterpret_cast<const double2 *>(vs + (2 * pl) * P::RW + 2 * l);
+          const double2 ua = *reinterpret_cast<const double2 *>(us + (pl + 1) * P::RW + 2 * l);
+          const double2 ub = *reinterpret_cast<const double2 *>(us + pl * P::RW + 2 * l);
+          double re = -kz * wv.y + (v1.x - v0.x) * idy;
+          double im = kz * wv.x + (v1.y - v0.y) * idy;
+          re = re + idx * (ua.x - ub.x);
+          im = im + idx * (ua.y - ub.y);
+          val.x = (T)rnd(re, xr);
+          val.y = (T)rnd(im, xr);
+        }
+        const int dst = (tt & 1) ? n - 1 - (tt >> 1) : (tt >> 1);
+        xsm[l * ld + xpad<V>(dst)] = val;
+      }
+    }
+    __syncthreads();  // the tile's lines are complete and its chunks read
+    if (t == 0) issue_upto(g + S);
+    {
+      constexpr int GL = NT / MB;
+      block_fft_lines_n<-1, NT, N>(xsm + (t / GL) * ld, x.tw, t % GL, GL);
+    }
+    const T dnf = (T)(1.0 / (double)n);
+    for (int e = t; e < n * MB; e += NT) {
+      const int l = e % MB, kk = e / MB;
+      const int k = k0 + l;
+      if (k > kend) continue;
+      const V Vv = xsm[l * ld + xpad<V>(kk)], Vm = xsm[l * ld + xpad<V>(kk == 0 ? 0 : n - kk)];
+      const V wq = __ldg(x.tw2 + kk);
+      const V y = cadd(cmul(wq, Vv), cmul(cconj(wq), Vm));
+      V out;
+      out.x = (T)rnd((double)(dnf * y.x), xr);
+      out.y = k == 0 ? (T)0 : (T)rnd((double)(dnf * y.y), xr);
+      *reinterpret_cast<V *>(phi + (size_t)(kk + 1) * PV + (size_t)(j - 1) * nz1 + 2 * k) = out;
+    }
+  }
+}
+
+// backward: the tile's phi-hat row (planes 1..n, min(256, n) per box) lands
+// in one of two line buffers while the other tile's FFT runs
+template <typename T, int N, int MINB>
+__global__ void __launch_bounds__(512, MINB) k_pois_bwd_t(DCoef c, XTabT<T> x, const __grid_constant__ PoisMaps maps,
+                                                         T *__restrict__ phi, int kbeg, int kend, int *err) {
+  using V = V2<T>;
+  constexpr int MB = pois_mb(N), NT = 512, RW = 2 * MB, n = N;
+  constexpr int BZ = n < 256 ? n : 256, NBX = (n + BZ - 1) / BZ;
+  extern __shared__ __align__(128) unsigned char pxraw[];
+  const int ld = xline_ld<V>(n, MB), ny = c.ny, nz1 = c.nz1, xr = c.xround;
+  const unsigned TX = (unsigned)(NBX * BZ * RW * sizeof(T));
+  const size_t RB = ((size_t)TX + 127) / 128 * 128;
+  V *xsm = reinterpret_cast<V *>(pxraw + 2 * RB);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(pxraw + 2 * RB + ((size_t)MB * ld * sizeof(V) + 15) / 16 * 16);
+  const CUtensorMap *mp = sizeof(T) == 8 ? &maps.phi64 : &maps.phi32;
+  const int t = threadIdx.x;
+  const int nkg = (kend - kbeg) / MB + 1, ntile = nkg * (ny - 1);
+  const int mine = (int)blockIdx.x < ntile ? (ntile - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  const size_t PV = (size_t)ny * nz1;
+  auto issue = [&](int m) {
+    const int q = (int)blockIdx.x + m * (int)gridDim.x;
+    const int j = q / nkg + 1, k0 = kbeg + (q % nkg) * MB;
+    unsigned char *b = pxraw + (size_t)(m & 1) * RB;
+    mbar_arrive_expect_tx(&bar[m & 1], TX);
+    for (int z = 0; z < NBX; ++z)
+      tma_load_3d(b + (size_t)z * BZ * RW * sizeof(T), mp, 2 * k0, j - 1, 1 + z * BZ, &bar[m & 1]);
+  };
+  if (t == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_init_fence();
+  }
+  __syncthreads();
+  if (t == 0 && mine > 0) issue(0);
+  for (int m = 0; m < mine; ++m) {
+    const int q = (int)blockIdx.x + m * (int)gridDim.x;
+    const int j = q / nkg + 1, k0 = kbeg + (q % nkg) * MB;
+    // the other buffer was read by the previous tile's pre-step, before its FFT
+    if (t == 0 && m + 1 < mine) issue(m + 1);
+    const bool ok = mbar_wait_bounded(&bar[m & 1], (unsigned)((m >> 1) & 1), 2000000000ull);
+    if (__syncthreads_or(!ok)) {
+      if (t == 0) {
+        atomicExch(err, OTBL_ERR_TIMEOUT);
+        mbar_wait_bounded(&bar[m & 1], (unsigned)((m >> 1) & 1), 200000000ull);
+        if (m + 1 < mine) mbar_wait_bounded(&bar[(m + 1) & 1], (unsigned)(((m + 1) >> 1) & 1), 200000000ull);
+      }
+      return;
+    }
+    const T *raw = reinterpret_cast<const T *>(pxraw + (size_t)(m & 1) * RB);
+    for (int e = t; e < n * MB; e += NT) {
+      const int l = e % MB, kk = e / MB;
+      const int k = k0 + l;
+      V val;
+      val.x = 0;
+      val.y = 0;
+      if (k <= kend) {
+        const V qv = *reinterpret_cast<const V *>(raw + kk * RW + 2 * l);
+        V Y, Ym;
+        Y.x = (T)rnd((double)qv.x, xr);
+        Y.y = (T)rnd((double)qv.y, xr);
+        Ym.x = 0;
+        Ym.y = 0;
+        if (kk > 0) {
+          const V qm = *reinterpret_cast<const V *>(raw + (n - kk) * RW + 2 * l);
+          Ym.x = (T)rnd((double)qm.x, xr);
+          Ym.y = (T)rnd((double)qm.y, xr);
+        }
+        V d;  // Y - i Ym
+        d.x = Y.x + Ym.y;
+        d.y = Y.y - Ym.x;
+        val = cmul(cconj(__ldg(x.tw2 + kk)), d);
+      }
+      xsm[l * ld + xpad<V>(kk)] = val;
+    }
+    __syncthreads();
+    {
+      constexpr int GL = NT / MB;
+      block_fft_lines_n<1, NT, N>(xsm + (t / GL) * ld, x.tw, t % GL, GL);
+    }
+    for (int e = t; e < n * MB; e += NT) {
+      const int l = e % MB, tt = e / MB;
+      const int k = k0 + l;
+      if (k > kend) continue;
+      const V Vv = xsm[l * ld + xpad<V>((tt & 1) ? n - 1 - (tt >> 1) : (tt >> 1))];
+      V out;
+      out.x = (T)rnd((double)((T)0.5 * Vv.x), xr);
+      out.y = k == 0 ? (T)0 : (T)rnd((double)((T)0.5 * Vv.y), xr);
+      *reinterpret_cast<V *>(phi + (size_t)(tt + 1) * PV + (size_t)(j - 1) * nz1 + 2 * k) = out;
+    }
+  }
+}
+
 // projection, pois.f90:144-162; one thread per (i >= 2, j, spanwise mode k),
 // the mode's two components kr = 2k, 2k+1 together (16-byte velocity and
 // 8- or 16-byte phi and p accesses; the w update of one component takes the
@@ -1489,14 +1716,115 @@ cudaError_t launch_outflow(otbl_ctx *c) {
   return cudaGetLastError();
 }
 
+// 3D map [planes][rows][nz1] of esz-byte elements, boxes of bx x by x bz
+static bool encode_pois(CUtensorMap *m, const void *base, size_t esz, int nz1, int rows, int planes, int bx, int by,
+                        int bz) {
+  auto fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(tensor_map_encoder());
+  if (!fn || !base || ((uintptr_t)base) % 16 != 0 || ((size_t)nz1 * esz) % 16 != 0 || ((size_t)bx * esz) % 16 != 0)
+    return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)nz1, (cuuint64_t)rows, (cuuint64_t)planes};
+  const cuuint64_t strides[2] = {(cuuint64_t)nz1 * esz, (cuuint64_t)rows * nz1 * esz};
+  const cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, (cuuint32_t)bz};
+  const cuuint32_t es[3] = {1, 1, 1};
+  const CUtensorMapDataType dt = esz == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  return fn(m, dt, 3, const_cast<void *>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+bool build_pois_maps(otbl_ctx *c) {
+  const int nx = c->cfg.nx, ny = c->cfg.ny, nz1 = c->dc.nz1, n = nx - 1;
+  const int MB = pois_mb(n), CP = MB >= 8 ? 64 : 128, BZ = std::min(256, n);
+  c->pmaps_vel = encode_pois(&c->pmaps.u, c->f[OTBL_F_U], 8, nz1, ny + 1, nx, 2 * MB, 1, CP + 1) &&
+                 encode_pois(&c->pmaps.v, c->f[OTBL_F_V], 8, nz1, ny, nx, 2 * MB, 2, CP) &&
+                 encode_pois(&c->pmaps.w, c->f[OTBL_F_W], 8, nz1, ny + 1, nx, 2 * MB, 1, CP);
+  c->pmaps_phi64 = encode_pois(&c->pmaps.phi64, c->w.s2, 8, nz1, ny, nx, 2 * MB, 1, BZ);
+  c->pmaps_phi32 = c->mixed && encode_pois(&c->pmaps.phi32, c->w.s3, 4, nz1, ny, nx, 2 * MB, 1, BZ);
+  return c->pmaps_vel && c->pmaps_phi64;
+}
+
+static int sm_count() {
+  static int nsm = 0;
+  if (nsm == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (nsm <= 0) nsm = 148;
+  }
+  return nsm;
+}
+
+// The TMA-fed x-DCT pass when its descriptors exist, n is 256, 512, 1024 or
+// 2048 and the boxes are aligned (the first kr of an FP32 box on a 16-byte
+// boundary); false leaves the pass to pois_xdct's one-shot kernels
+// (OTBL_POIS_ONESHOT=1 forces them).
+template <typename T>
+static bool pois_xdct_t(otbl_ctx *c, bool fwd, T *phi, int kbeg, int kend) {
+  constexpr bool F64 = sizeof(T) == 8;
+  const int ny = c->cfg.ny, n = c->cfg.nx - 1, MB = pois_mb(n);
+  if (getenv("OTBL_POIS_ONESHOT")) return false;
+  if (fwd && !c->pmaps_vel) return false;
+  if (!fwd && !(F64 ? c->pmaps_phi64 : c->pmaps_phi32)) return false;
+  if (!fwd && !F64 && (kbeg % 2 != 0 || MB < 2)) return false;
+  if ((void *)phi != (F64 ? (void *)c->w.s2 : (void *)c->w.s3)) return false;
+  using V = V2<T>;
+  const size_t xs = ((size_t)MB * xline_ld<V>(n, MB) * sizeof(V) + 15) / 16 * 16;
+  const int ntile = ((kend - kbeg) / MB + 1) * (ny - 1);
+  const int smax = 232448;  // dynamic shared memory per CTA (227 KB)
+  XTabT<T> xt;
+  if constexpr (F64)
+    xt = xtab(c);
+  else
+    xt = xtabf(c);
+  int *err = &c->st->err;
+  if (fwd) {
+    auto go = [&](auto kern, int ch) {
+      const int S = std::min(6, (int)((smax - xs - 64) / ch));
+      if (S < 2) return false;
+      const size_t smem = (size_t)S * ch + xs + 8 * (size_t)S;
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      kern<<<std::min(ntile, sm_count()), 512, smem, c->stream>>>(c->dc, xt, c->pmaps, phi, kbeg, kend, S, err);
+      return true;
+    };
+    switch (n) {
+      case 256: return go(k_pois_fwd_t<T, 256>, PoisChunk<pois_mb(256)>::CH);
+      case 512: return go(k_pois_fwd_t<T, 512>, PoisChunk<pois_mb(512)>::CH);
+      case 1024: return go(k_pois_fwd_t<T, 1024>, PoisChunk<pois_mb(1024)>::CH);
+      case 2048: return go(k_pois_fwd_t<T, 2048>, PoisChunk<pois_mb(2048)>::CH);
+      default: return false;
+    }
+  }
+  const int BZ = std::min(256, n), NBX = (n + BZ - 1) / BZ;
+  const size_t rb = ((size_t)NBX * BZ * 2 * MB * sizeof(T) + 127) / 128 * 128;
+  const size_t smem = 2 * rb + xs + 16;
+  if (smem > (size_t)smax) return false;
+  constexpr int MINB = F64 ? 1 : 2;
+  auto go = [&](auto kern) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const int per = smem * 2 + 2048 <= 233472 ? MINB : 1;  // CTAs per SM that fit
+    kern<<<std::min(ntile, per * sm_count()), 512, smem, c->stream>>>(c->dc, xt, c->pmaps, phi, kbeg, kend, err);
+    return true;
+  };
+  switch (n) {
+    case 256: return go(k_pois_bwd_t<T, 256, MINB>);
+    case 512: return go(k_pois_bwd_t<T, 512, MINB>);
+    case 1024: return go(k_pois_bwd_t<T, 1024, MINB>);
+    case 2048: return go(k_pois_bwd_t<T, 2048, MINB>);
+    default: return false;
+  }
+}
+
 // One x-DCT pass (forward: divergence + DCT-II; backward: DCT-III) over the
 // spanwise modes kbeg..kend in T, MB modes per CTA.
 template <typename T>
 static void pois_xdct(otbl_ctx *c, bool fwd, T *phi, int kbeg, int kend) {
   if (kend < kbeg) return;
+  if (pois_xdct_t<T>(c, fwd, phi, kbeg, kend)) {
+    c->launches += 1;
+    return;
+  }
   const int ny = c->cfg.ny, n = c->cfg.nx - 1;
-  // modes per CTA: n * MB <= 4096 and at most 8
-  const int MB = n <= 512 ? 8 : (n <= 1024 ? 4 : (n <= 2048 ? 2 : 1));
+  const int MB = pois_mb(n);
   const size_t smem = (size_t)MB * xline_ld<V2<T>>(n, MB) * sizeof(V2<T>);
   const dim3 gx((kend - kbeg + 1 + MB - 1) / MB, ny - 1);
   // threads per CTA: 512 when the CTA holds 2048-4096 points (fewer items

@@ -283,6 +283,7 @@ extern "C" int otbl_ctx_create(const otbl_config *cfg, const double *coef, int d
     build_final_maps(c);
     build_x_maps(c);
     build_y_maps(c);
+    build_pois_maps(c);
   }
   c->ydense = (cfg->options & OTBL_OPT_YDENSE) != 0;
   if (c->ydense && check(c, ydense_prepare(c), "dense interpyy operator") != OTBL_OK) {
@@ -669,6 +670,7 @@ static int bind_fields(otbl_ctx *c, double *const *ptr, const bool *use) {
     build_x_maps(c);
     build_y_maps(c);
     build_ydense_maps(c);
+    build_pois_maps(c);
   }
   return OTBL_OK;
 }

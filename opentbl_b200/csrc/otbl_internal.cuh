@@ -100,6 +100,14 @@ struct YDenseMaps {
   CUtensorMap g[3];
 };
 
+// TMA descriptors of pois' x-DCT kernels (k_pois_fwd_t, k_pois_bwd_t):
+// the velocity [nx][rows][nz1] FP64 in boxes of 2 MB kr x rows x planes (u:
+// 1 row x CP + 1 planes, v: 2 rows x CP, w: 1 row x CP) and phi-hat [nx][ny]
+// [nz1] in FP64 and FP32, boxes of 2 MB kr x 1 row x min(256, nx - 1) planes
+struct PoisMaps {
+  CUtensorMap u, v, w, phi64, phi32;
+};
+
 }  // namespace otbl
 
 struct otbl_ctx {
@@ -142,6 +150,8 @@ struct otbl_ctx {
   bool xmaps_ok = false;
   otbl::YMaps ymi;       // k_interpy_t
   bool ymaps_ok = false;
+  otbl::PoisMaps pmaps;  // k_pois_fwd_t / k_pois_bwd_t
+  bool pmaps_vel = false, pmaps_phi64 = false, pmaps_phi32 = false;
   int mixed;                // cfg.precision == OTBL_PREC_MIXED
   double *coef_dev;
   float *coef_dev_f;
@@ -250,6 +260,7 @@ cudaError_t launch_round_f32(otbl_ctx *c, const double *in, float *out, size_t n
 cudaError_t ydense_prepare(otbl_ctx *c);
 cudaError_t launch_interpy_dense(otbl_ctx *c);
 bool build_ydense_maps(otbl_ctx *c);
+bool build_pois_maps(otbl_ctx *c);
 bool ydense_ready(const otbl_ctx *c);
 // one-point statistics, statsp (k_stats.cu)
 cudaError_t launch_statsp(otbl_ctx *c);
