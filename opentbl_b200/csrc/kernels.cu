@@ -1093,7 +1093,9 @@ __global__ void __launch_bounds__(512, 1) k_pois_fwd_t(DCoef c, XTabT<T> x, cons
   uint64_t *bar = reinterpret_cast<uint64_t *>(pxraw + (size_t)S * P::CH +
                                                ((size_t)MB * ld * sizeof(V) + 15) / 16 * 16);
   const int t = threadIdx.x;
-  const int nkg = (kend - kbeg) / MB + 1, ntile = nkg * (ny - 1);
+  // tiles start at an even mode (a 16-byte box origin for FP32 kr); modes
+  // below kbeg are computed as zeros and not stored
+  const int kb0 = kbeg & ~1, nkg = (kend - kb0) / MB + 1, ntile = nkg * (ny - 1);
   const int mine = (int)blockIdx.x < ntile ? (ntile - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
   const int NC = (n + P::CP - 1) / P::CP, G = mine * NC;
   const size_t PV = (size_t)ny * nz1;
@@ -1101,7 +1103,7 @@ __global__ void __launch_bounds__(512, 1) k_pois_fwd_t(DCoef c, XTabT<T> x, cons
   auto issue_upto = [&](int h_end) {
     for (; issued < h_end && issued < G; ++issued) {
       const int h = issued, sl = h % S, q = (int)blockIdx.x + (h / NC) * (int)gridDim.x;
-      const int j = q / nkg + 1, k0 = kbeg + (q % nkg) * MB, tt0 = (h % NC) * P::CP;
+      const int j = q / nkg + 1, k0 = kb0 + (q % nkg) * MB, tt0 = (h % NC) * P::CP;
       unsigned char *b = pxraw + (size_t)sl * P::CH;
       mbar_arrive_expect_tx(&bar[sl], P::TX);
       tma_load_3d(b, &maps.u, 2 * k0, j, tt0, &bar[sl]);
@@ -1119,7 +1121,7 @@ __global__ void __launch_bounds__(512, 1) k_pois_fwd_t(DCoef c, XTabT<T> x, cons
   int g = 0;
   for (int m = 0; m < mine; ++m) {
     const int q = (int)blockIdx.x + m * (int)gridDim.x;
-    const int j = q / nkg + 1, k0 = kbeg + (q % nkg) * MB;
+    const int j = q / nkg + 1, k0 = kb0 + (q % nkg) * MB;
     const double idy = c.idy[j];
     for (int cc = 0; cc < NC; ++cc, ++g) {
       const int sl = g % S;
@@ -1144,7 +1146,7 @@ __global__ void __launch_bounds__(512, 1) k_pois_fwd_t(DCoef c, XTabT<T> x, cons
         V val;
         val.x = 0;
         val.y = 0;
-        if (k <= kend) {
+        if (k >= kbeg && k <= kend) {
           const double kz = c.kaz[k];
           const double2 wv = *reinterpret_cast<const double2 *>(ws + pl * P::RW + 2 * l);
           const double2 v1 = *reinterpret_cast<const double2 *>(vs + (2 * pl + 1) * P::RW + 2 * l);
@@ -1172,7 +1174,7 @@ __global__ void __launch_bounds__(512, 1) k_pois_fwd_t(DCoef c, XTabT<T> x, cons
     for (int e = t; e < n * MB; e += NT) {
       const int l = e % MB, kk = e / MB;
       const int k = k0 + l;
-      if (k > kend) continue;
+      if (k < kbeg || k > kend) continue;
       const V Vv = xsm[l * ld + xpad<V>(kk)], Vm = xsm[l * ld + xpad<V>(kk == 0 ? 0 : n - kk)];
       const V wq = __ldg(x.tw2 + kk);
       const V y = cadd(cmul(wq, Vv), cmul(cconj(wq), Vm));
@@ -1200,12 +1202,14 @@ __global__ void __launch_bounds__(512, MINB) k_pois_bwd_t(DCoef c, XTabT<T> x, c
   uint64_t *bar = reinterpret_cast<uint64_t *>(pxraw + 2 * RB + ((size_t)MB * ld * sizeof(V) + 15) / 16 * 16);
   const CUtensorMap *mp = sizeof(T) == 8 ? &maps.phi64 : &maps.phi32;
   const int t = threadIdx.x;
-  const int nkg = (kend - kbeg) / MB + 1, ntile = nkg * (ny - 1);
+  // tiles start at an even mode (a 16-byte box origin for FP32 kr); modes
+  // below kbeg are computed as zeros and not stored
+  const int kb0 = kbeg & ~1, nkg = (kend - kb0) / MB + 1, ntile = nkg * (ny - 1);
   const int mine = (int)blockIdx.x < ntile ? (ntile - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
   const size_t PV = (size_t)ny * nz1;
   auto issue = [&](int m) {
     const int q = (int)blockIdx.x + m * (int)gridDim.x;
-    const int j = q / nkg + 1, k0 = kbeg + (q % nkg) * MB;
+    const int j = q / nkg + 1, k0 = kb0 + (q % nkg) * MB;
     unsigned char *b = pxraw + (size_t)(m & 1) * RB;
     mbar_arrive_expect_tx(&bar[m & 1], TX);
     for (int z = 0; z < NBX; ++z)
@@ -1220,7 +1224,7 @@ __global__ void __launch_bounds__(512, MINB) k_pois_bwd_t(DCoef c, XTabT<T> x, c
   if (t == 0 && mine > 0) issue(0);
   for (int m = 0; m < mine; ++m) {
     const int q = (int)blockIdx.x + m * (int)gridDim.x;
-    const int j = q / nkg + 1, k0 = kbeg + (q % nkg) * MB;
+    const int j = q / nkg + 1, k0 = kb0 + (q % nkg) * MB;
     // the other buffer was read by the previous tile's pre-step, before its FFT
     if (t == 0 && m + 1 < mine) issue(m + 1);
     const bool ok = mbar_wait_bounded(&bar[m & 1], (unsigned)((m >> 1) & 1), 2000000000ull);
@@ -1239,7 +1243,7 @@ __global__ void __launch_bounds__(512, MINB) k_pois_bwd_t(DCoef c, XTabT<T> x, c
       V val;
       val.x = 0;
       val.y = 0;
-      if (k <= kend) {
+      if (k >= kbeg && k <= kend) {
         const V qv = *reinterpret_cast<const V *>(raw + kk * RW + 2 * l);
         V Y, Ym;
         Y.x = (T)rnd((double)qv.x, xr);
@@ -1266,7 +1270,7 @@ __global__ void __launch_bounds__(512, MINB) k_pois_bwd_t(DCoef c, XTabT<T> x, c
     for (int e = t; e < n * MB; e += NT) {
       const int l = e % MB, tt = e / MB;
       const int k = k0 + l;
-      if (k > kend) continue;
+      if (k < kbeg || k > kend) continue;
       const V Vv = xsm[l * ld + xpad<V>((tt & 1) ? n - 1 - (tt >> 1) : (tt >> 1))];
       V out;
       out.x = (T)rnd((double)((T)0.5 * Vv.x), xr);
@@ -1754,9 +1758,8 @@ static int sm_count() {
   return nsm;
 }
 
-// The TMA-fed x-DCT pass when its descriptors exist, n is 256, 512, 1024 or
-// 2048 and the boxes are aligned (the first kr of an FP32 box on a 16-byte
-// boundary); false leaves the pass to pois_xdct's one-shot kernels
+// The TMA-fed x-DCT pass when its descriptors exist and n is 256, 512, 1024
+// or 2048; false leaves the pass to pois_xdct's one-shot kernels
 // (OTBL_POIS_ONESHOT=1 forces them).
 template <typename T>
 static bool pois_xdct_t(otbl_ctx *c, bool fwd, T *phi, int kbeg, int kend) {
@@ -1765,11 +1768,11 @@ static bool pois_xdct_t(otbl_ctx *c, bool fwd, T *phi, int kbeg, int kend) {
   if (getenv("OTBL_POIS_ONESHOT")) return false;
   if (fwd && !c->pmaps_vel) return false;
   if (!fwd && !(F64 ? c->pmaps_phi64 : c->pmaps_phi32)) return false;
-  if (!fwd && !F64 && (kbeg % 2 != 0 || MB < 2)) return false;
+  if (!fwd && !F64 && MB < 2) return false;
   if ((void *)phi != (F64 ? (void *)c->w.s2 : (void *)c->w.s3)) return false;
   using V = V2<T>;
   const size_t xs = ((size_t)MB * xline_ld<V>(n, MB) * sizeof(V) + 15) / 16 * 16;
-  const int ntile = ((kend - kbeg) / MB + 1) * (ny - 1);
+  const int ntile = ((kend - (kbeg & ~1)) / MB + 1) * (ny - 1);
   const int smax = 232448;  // dynamic shared memory per CTA (227 KB)
   XTabT<T> xt;
   if constexpr (F64)
