@@ -335,15 +335,17 @@ __device__ __forceinline__ double regs_absmax(const V (&a)[E]) {
 }
 
 // CTAs per SM bound: FP64 unbounded (252 registers, 4.49 ms per substep at
-// 1025x193x512; 5.02 at >= 3 CTAs with spills), FP32 >= 3 CTAs (168
-// registers, 2.62 ms; 3.16 unbounded at 185). A variant with two warps per
-// line (4 elements per thread, radix-4 passes, named barriers) measured
-// slower in both precisions (4.92 and 3.61 ms) and was dropped.
+// 1025x193x512; 5.02 at >= 3 CTAs with spills), FP32 >= 4 CTAs (126-128
+// registers, 36 bytes of spills in part 0; 2.29-2.30 ms per substep against
+// 2.34-2.43 at >= 3 CTAs and 162-168 registers, after the exchange buffer's
+// swizzle; 3.16 unbounded before it). A variant with two warps per line (4
+// elements per thread, radix-4 passes, named barriers) measured slower in
+// both precisions (4.92 and 3.61 ms) and was dropped.
 #ifndef OTBL_PR_MB_D
 #define OTBL_PR_MB_D 1
 #endif
 #ifndef OTBL_PR_MB_F
-#define OTBL_PR_MB_F 3
+#define OTBL_PR_MB_F 4
 #endif
 template <int M, typename T, int PART>
 __global__ void __launch_bounds__(128, std::is_same<T, double>::value ? OTBL_PR_MB_D : OTBL_PR_MB_F)

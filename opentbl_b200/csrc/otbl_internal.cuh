@@ -195,7 +195,10 @@ void prof_end(otbl_ctx *c);
 // y second difference (up to ~4/dy_wall^2 on the stretched grid), stays
 // below kPoisCond x 6e-8 of the mode's divergence. Lower modes run in FP64.
 // (FP32 from k = 4 up, tried first, left max|div u| ~1e-6 after the
-// projection at 1025x193x512: kappa(k = 4) ~ 1.6e5.)
+// projection at 1025x193x512: kappa(k = 4) ~ 1.6e5. Measured there after 100
+// RK3 steps, against the 1e-10 gate: bound 1024, FP32 from k = 35, 7e-13;
+// 4096, from k = 18, 2.3e-10; 16384, from k = 9, 1.0e-7. The two looser
+// bounds saved 0.1-0.2 ms per mixed step.)
 constexpr double kPoisCond = 1024.0;
 
 // Device error code written into the context's flag by genflu when the
