@@ -149,13 +149,15 @@ __global__ void __launch_bounds__(128) k_products(DCoef c, ZTabT<T> z, ProdArgs<
 }
 
 // ---------------------------------------------------------------------------
-// k_products for M = nz/2 = 256 (nz = 512): the transforms and products of
-// k_products with each line kept in registers between the inverse
-// transform's last Stockham pass and the forward transform's first one.
-// Register layout L: lane t holds complex element n = t + 32 m in v[m],
-// m < E = M/32. Passes: radix 8 (Ns = 1), radix 8 (Ns = 8), radix R3
-// (Ns = 64); the first reads L, the last writes L, the two in between go
-// through a per-warp shared buffer. Its element i is stored at i + i/8 for
+// k_products for M = nz/2 = 256 or 128 (nz = 512, 256): the transforms and
+// products of k_products with each line kept in registers between the
+// inverse transform's last Stockham pass and the forward transform's first
+// one. Register layout L: lane t holds complex element n = t + 32 m in v[m],
+// m < E = M/32. Passes: radix E (Ns = 1; its butterflies' inputs j + 32 r are
+// one lane's registers), radix 8 (Ns = E), radix 4 (Ns = 8 E = M/4); the
+// first reads L, the last writes L, the two in between go through a per-warp
+// shared buffer. M = 256: radices 8, 8, 4, warp_fft's order; M = 128: 4, 8,
+// 4 (warp_fft's 8, 8, 2 would need eight register inputs per butterfly). Its element i is stored at i + i/8 for
 // 16-byte (FP64) elements and at i ^ ((i/8) mod 16) for 8-byte (FP32) ones,
 // which makes every exchange of the three passes conflict-free for its
 // element size (a bank model of the access patterns: the FP32 buffer at
@@ -163,13 +165,14 @@ __global__ void __launch_bounds__(128) k_products(DCoef c, ZTabT<T> z, ProdArgs<
 // ncu showed 15 M of its 42 M shared wavefronts as conflicts at
 // 257x193x512). The real-to-complex post-step takes the mirrored element
 // Z[M-k] from the lane that holds it by warp shuffles instead of a round
-// trip through the buffer. The arithmetic is warp_fft's, operation for
-// operation.
+// trip through the buffer. For M = 256 the arithmetic is warp_fft's,
+// operation for operation.
 // ---------------------------------------------------------------------------
 template <int M>
 struct ZPlan {
+  static_assert(M == 256 || M == 128, "register transforms for M = 128, 256");
   static constexpr int E = M / 32;
-  static constexpr int R3 = 4;  // 256 = 8 x 8 x 4
+  static constexpr int R3 = 4;  // M = E x 8 x 4
 };
 template <typename V>
 __device__ __forceinline__ int zpad(int i) {
@@ -190,46 +193,49 @@ __device__ __forceinline__ V shfl_cx(V v, int src) {
 template <int M, int SIGN, typename V>
 __device__ __forceinline__ void zfft_regs(V (&L)[M / 32], V *buf, const V *__restrict__ tw, int t) {
   constexpr int E = M / 32, R3 = ZPlan<M>::R3;
-  constexpr int IA = E / 8;  // radix-8 items per lane in the first two passes
-  // pass A: radix 8, Ns = 1, input from registers
+  // pass A: radix E, Ns = 1, input from registers (inputs t + 32 r)
+  {
+    V v[E];
 #pragma unroll
-  for (int it = 0; it < IA; ++it) {
-    V v[8];
+    for (int r = 0; r < E; ++r) v[r] = L[r];
+    dft_small<E, SIGN>(v);
 #pragma unroll
-    for (int r = 0; r < 8; ++r) v[r] = L[it + r * IA];
-    dft_small<8, SIGN>(v);
-    const int j = t + 32 * it;
-#pragma unroll
-    for (int r = 0; r < 8; ++r) buf[zpad<V>(j * 8 + r)] = v[r];
+    for (int r = 0; r < E; ++r) buf[zpad<V>(t * E + r)] = v[r];
   }
   __syncwarp();
-  // pass B: radix 8, Ns = 8
+  // pass B: radix 8, Ns = E (M / 8 butterflies: IB per lane, or the first
+  // M / 8 lanes)
   {
-    V v[IA][8];
+    constexpr int NB = M / 8, IB = (NB + 31) / 32;
+    V v[IB][8];
 #pragma unroll
-    for (int it = 0; it < IA; ++it) {
+    for (int it = 0; it < IB; ++it) {
       const int j = t + 32 * it;
+      if (j < NB) {
 #pragma unroll
-      for (int r = 0; r < 8; ++r) v[it][r] = buf[zpad<V>(j + r * (M / 8))];
+        for (int r = 0; r < 8; ++r) v[it][r] = buf[zpad<V>(j + r * NB)];
+      }
     }
     __syncwarp();
 #pragma unroll
-    for (int it = 0; it < IA; ++it) {
-      const int j = t + 32 * it, k = j % 8;
+    for (int it = 0; it < IB; ++it) {
+      const int j = t + 32 * it, k = j % E;
+      if (j < NB) {
 #pragma unroll
-      for (int r = 1; r < 8; ++r) {
-        V w = __ldg(&tw[r * k * (M / 64)]);
-        if (SIGN > 0) w.y = -w.y;
-        v[it][r] = cmul(v[it][r], w);
+        for (int r = 1; r < 8; ++r) {
+          V w = __ldg(&tw[r * k * (M / (8 * E))]);
+          if (SIGN > 0) w.y = -w.y;
+          v[it][r] = cmul(v[it][r], w);
+        }
+        dft_small<8, SIGN>(v[it]);
+        const int base = (j / E) * (8 * E) + k;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) buf[zpad<V>(base + r * E)] = v[it][r];
       }
-      dft_small<8, SIGN>(v[it]);
-      const int base = (j / 8) * 64 + k;
-#pragma unroll
-      for (int r = 0; r < 8; ++r) buf[zpad<V>(base + r * 8)] = v[it][r];
     }
   }
   __syncwarp();
-  // pass C: radix R3, Ns = 64 (= M/R3), output to registers
+  // pass C: radix R3, Ns = M / R3, output to registers
   {
     constexpr int IC = (M / R3) / 32;
     V v[IC][R3];
@@ -242,7 +248,7 @@ __device__ __forceinline__ void zfft_regs(V (&L)[M / 32], V *buf, const V *__res
     __syncwarp();
 #pragma unroll
     for (int it = 0; it < IC; ++it) {
-      const int j = t + 32 * it;  // k = j mod 64 = j, twiddle stride M/(64 R3) = 1
+      const int j = t + 32 * it;  // k = j mod (M / R3) = j, twiddle stride M/(Ns R3) = 1
 #pragma unroll
       for (int r = 1; r < R3; ++r) {
         V w = __ldg(&tw[r * j]);
@@ -1565,14 +1571,23 @@ static cudaError_t products_t(otbl_ctx *c, int setstep, int part, const ZTabT<T>
   // part 0: all planes, rows 1..ny+1; part 2: all planes, rows 1..ny;
   // part 1: planes 2..nx-1, rows 1..ny
   const dim3 g((c->cfg.ny + (part == 0 ? 1 : 0) + 3) / 4, c->cfg.nx - (part == 1 ? 2 : 0));
-  if (M == 256) {
+  if (M == 256 || M == 128) {
     const size_t smem = (size_t)4 * (M + M / 8) * sizeof(V2<T>);
-    if (part == 0)
-      k_products_r<256, T, 0><<<g, 128, smem, c->stream>>>(c->dc, z, a);
-    else if (part == 1)
-      k_products_r<256, T, 1><<<g, 128, smem, c->stream>>>(c->dc, z, a);
-    else
-      k_products_r<256, T, 2><<<g, 128, smem, c->stream>>>(c->dc, z, a);
+    if (M == 256) {
+      if (part == 0)
+        k_products_r<256, T, 0><<<g, 128, smem, c->stream>>>(c->dc, z, a);
+      else if (part == 1)
+        k_products_r<256, T, 1><<<g, 128, smem, c->stream>>>(c->dc, z, a);
+      else
+        k_products_r<256, T, 2><<<g, 128, smem, c->stream>>>(c->dc, z, a);
+    } else {
+      if (part == 0)
+        k_products_r<128, T, 0><<<g, 128, smem, c->stream>>>(c->dc, z, a);
+      else if (part == 1)
+        k_products_r<128, T, 1><<<g, 128, smem, c->stream>>>(c->dc, z, a);
+      else
+        k_products_r<128, T, 2><<<g, 128, smem, c->stream>>>(c->dc, z, a);
+    }
   } else {
     const size_t smem = (size_t)4 * 3 * M * sizeof(V2<T>);
     auto k = part == 0 ? k_products<T, 0> : (part == 1 ? k_products<T, 1> : k_products<T, 2>);
