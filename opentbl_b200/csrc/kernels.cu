@@ -149,15 +149,17 @@ __global__ void __launch_bounds__(128) k_products(DCoef c, ZTabT<T> z, ProdArgs<
 }
 
 // ---------------------------------------------------------------------------
-// k_products for M = nz/2 = 256 or 128 (nz = 512, 256): the transforms and
+// k_products for M = nz/2 = 32..256 (nz = 64..512): the transforms and
 // products of k_products with each line kept in registers between the
 // inverse transform's last Stockham pass and the forward transform's first
 // one. Register layout L: lane t holds complex element n = t + 32 m in v[m],
 // m < E = M/32. Passes: radix E (Ns = 1; its butterflies' inputs j + 32 r are
-// one lane's registers), radix 8 (Ns = E), radix 4 (Ns = 8 E = M/4); the
-// first reads L, the last writes L, the two in between go through a per-warp
-// shared buffer. M = 256: radices 8, 8, 4, warp_fft's order; M = 128: 4, 8,
-// 4 (warp_fft's 8, 8, 2 would need eight register inputs per butterfly). Its element i is stored at i + i/8 for
+// one lane's registers; a copy for E = 1), radix 8 (Ns = E), radix 4 (Ns =
+// 8 E = M/4); the first reads L, the last writes L (for M < 128 through the
+// buffer, its outputs not being in layout L), the two in between go through
+// a per-warp shared buffer. M = 256: radices 8, 8, 4, warp_fft's order;
+// M = 128: 4, 8, 4, M = 64: 2, 8, 4, M = 32: 8, 4 (warp_fft's order would
+// need eight register inputs per butterfly). Its element i is stored at i + i/8 for
 // 16-byte (FP64) elements and at i ^ ((i/8) mod 16) for 8-byte (FP32) ones,
 // which makes every exchange of the three passes conflict-free for its
 // element size (a bank model of the access patterns: the FP32 buffer at
@@ -170,7 +172,7 @@ __global__ void __launch_bounds__(128) k_products(DCoef c, ZTabT<T> z, ProdArgs<
 // ---------------------------------------------------------------------------
 template <int M>
 struct ZPlan {
-  static_assert(M == 256 || M == 128, "register transforms for M = 128, 256");
+  static_assert(M == 256 || M == 128 || M == 64 || M == 32, "register transforms for M = 32..256");
   static constexpr int E = M / 32;
   static constexpr int R3 = 4;  // M = E x 8 x 4
 };
@@ -193,12 +195,13 @@ __device__ __forceinline__ V shfl_cx(V v, int src) {
 template <int M, int SIGN, typename V>
 __device__ __forceinline__ void zfft_regs(V (&L)[M / 32], V *buf, const V *__restrict__ tw, int t) {
   constexpr int E = M / 32, R3 = ZPlan<M>::R3;
-  // pass A: radix E, Ns = 1, input from registers (inputs t + 32 r)
+  // pass A: radix E, Ns = 1, input from registers (inputs t + 32 r; a copy
+  // for E = 1)
   {
     V v[E];
 #pragma unroll
     for (int r = 0; r < E; ++r) v[r] = L[r];
-    dft_small<E, SIGN>(v);
+    if constexpr (E > 1) dft_small<E, SIGN>(v);
 #pragma unroll
     for (int r = 0; r < E; ++r) buf[zpad<V>(t * E + r)] = v[r];
   }
@@ -221,11 +224,13 @@ __device__ __forceinline__ void zfft_regs(V (&L)[M / 32], V *buf, const V *__res
     for (int it = 0; it < IB; ++it) {
       const int j = t + 32 * it, k = j % E;
       if (j < NB) {
+        if constexpr (E > 1) {  // Ns = 1 has no twiddles
 #pragma unroll
-        for (int r = 1; r < 8; ++r) {
-          V w = __ldg(&tw[r * k * (M / (8 * E))]);
-          if (SIGN > 0) w.y = -w.y;
-          v[it][r] = cmul(v[it][r], w);
+          for (int r = 1; r < 8; ++r) {
+            V w = __ldg(&tw[r * k * (M / (8 * E))]);
+            if (SIGN > 0) w.y = -w.y;
+            v[it][r] = cmul(v[it][r], w);
+          }
         }
         dft_small<8, SIGN>(v[it]);
         const int base = (j / E) * (8 * E) + k;
@@ -235,29 +240,45 @@ __device__ __forceinline__ void zfft_regs(V (&L)[M / 32], V *buf, const V *__res
     }
   }
   __syncwarp();
-  // pass C: radix R3, Ns = M / R3, output to registers
+  // pass C: radix R3, Ns = M / R3, output to registers (for M < 128, whose
+  // outputs j + r M/R3 are not in layout L, through the buffer)
   {
-    constexpr int IC = (M / R3) / 32;
+    constexpr int NC = M / R3, IC = (NC + 31) / 32;
     V v[IC][R3];
 #pragma unroll
     for (int it = 0; it < IC; ++it) {
       const int j = t + 32 * it;
+      if (j < NC) {
 #pragma unroll
-      for (int r = 0; r < R3; ++r) v[it][r] = buf[zpad<V>(j + r * (M / R3))];
+        for (int r = 0; r < R3; ++r) v[it][r] = buf[zpad<V>(j + r * NC)];
+      }
     }
     __syncwarp();
 #pragma unroll
     for (int it = 0; it < IC; ++it) {
       const int j = t + 32 * it;  // k = j mod (M / R3) = j, twiddle stride M/(Ns R3) = 1
+      if (j < NC) {
 #pragma unroll
-      for (int r = 1; r < R3; ++r) {
-        V w = __ldg(&tw[r * j]);
-        if (SIGN > 0) w.y = -w.y;
-        v[it][r] = cmul(v[it][r], w);
+        for (int r = 1; r < R3; ++r) {
+          V w = __ldg(&tw[r * j]);
+          if (SIGN > 0) w.y = -w.y;
+          v[it][r] = cmul(v[it][r], w);
+        }
+        dft_small<R3, SIGN>(v[it]);
+#pragma unroll
+        for (int r = 0; r < R3; ++r) {
+          if constexpr (NC >= 32)
+            L[it + r * IC] = v[it][r];
+          else
+            buf[zpad<V>(j + r * NC)] = v[it][r];
+        }
       }
-      dft_small<R3, SIGN>(v[it]);
+    }
+    if constexpr (NC < 32) {
+      __syncwarp();
 #pragma unroll
-      for (int r = 0; r < R3; ++r) L[it + r * IC] = v[it][r];
+      for (int m = 0; m < E; ++m) L[m] = buf[zpad<V>(t + 32 * m)];
+      __syncwarp();
     }
   }
 }
@@ -1571,23 +1592,26 @@ static cudaError_t products_t(otbl_ctx *c, int setstep, int part, const ZTabT<T>
   // part 0: all planes, rows 1..ny+1; part 2: all planes, rows 1..ny;
   // part 1: planes 2..nx-1, rows 1..ny
   const dim3 g((c->cfg.ny + (part == 0 ? 1 : 0) + 3) / 4, c->cfg.nx - (part == 1 ? 2 : 0));
-  if (M == 256 || M == 128) {
+  // the register-pipelined transforms for M = 32..256; other M (and
+  // OTBL_PRODUCTS_SMEM=1) the shared-memory kernel
+  if ((M == 32 || M == 64 || M == 128 || M == 256) && !getenv("OTBL_PRODUCTS_SMEM")) {
     const size_t smem = (size_t)4 * (M + M / 8) * sizeof(V2<T>);
-    if (M == 256) {
+    auto go = [&](auto k0, auto k1, auto k2) {
       if (part == 0)
-        k_products_r<256, T, 0><<<g, 128, smem, c->stream>>>(c->dc, z, a);
+        k0<<<g, 128, smem, c->stream>>>(c->dc, z, a);
       else if (part == 1)
-        k_products_r<256, T, 1><<<g, 128, smem, c->stream>>>(c->dc, z, a);
+        k1<<<g, 128, smem, c->stream>>>(c->dc, z, a);
       else
-        k_products_r<256, T, 2><<<g, 128, smem, c->stream>>>(c->dc, z, a);
-    } else {
-      if (part == 0)
-        k_products_r<128, T, 0><<<g, 128, smem, c->stream>>>(c->dc, z, a);
-      else if (part == 1)
-        k_products_r<128, T, 1><<<g, 128, smem, c->stream>>>(c->dc, z, a);
-      else
-        k_products_r<128, T, 2><<<g, 128, smem, c->stream>>>(c->dc, z, a);
-    }
+        k2<<<g, 128, smem, c->stream>>>(c->dc, z, a);
+    };
+    if (M == 256)
+      go(k_products_r<256, T, 0>, k_products_r<256, T, 1>, k_products_r<256, T, 2>);
+    else if (M == 128)
+      go(k_products_r<128, T, 0>, k_products_r<128, T, 1>, k_products_r<128, T, 2>);
+    else if (M == 64)
+      go(k_products_r<64, T, 0>, k_products_r<64, T, 1>, k_products_r<64, T, 2>);
+    else
+      go(k_products_r<32, T, 0>, k_products_r<32, T, 1>, k_products_r<32, T, 2>);
   } else {
     const size_t smem = (size_t)4 * 3 * M * sizeof(V2<T>);
     auto k = part == 0 ? k_products<T, 0> : (part == 1 ? k_products<T, 1> : k_products<T, 2>);

@@ -63,16 +63,17 @@ def test_mixed_one_substep(name):
     assert max(other[n] for n in ("rhsupa", "rhsvpa", "rhswpa")) <= 1e-4
 
 
-def test_mixed_register_products_nz256():
-    """nz = 256: the FP32 products in the register-pipelined transforms of
-    M = 128 (radices 4, 8, 4), one substep against the FP64 oracle."""
-    cfg = replace(config.TINY, nx=17, nz=256, name="wide-17x41x256")
+@pytest.mark.parametrize("nz", [256, 128, 64])
+def test_mixed_register_products(nz):
+    """nz = 64..256: the FP32 products in the register-pipelined transforms
+    of M = 32..128, one substep against the FP64 oracle."""
+    cfg = replace(config.TINY, nx=17, nz=nz, name=f"wide-17x41x{nz}")
     init, coef = setup(cfg)
     g = Box(_mixed(cfg), init, coef)
     o = oracle_box(cfg, init)
     g.substep(1, True)
     o.substep(1, 1)
-    r = _report("wide-17x41x256 mixed, 1 substep", g, o, cfg, coef)
+    r = _report(f"{cfg.name} mixed, 1 substep", g, o, cfg, coef)
     assert r["vel_rel_l2"] <= 1e-7
     assert rel_l2(g.field("p"), o.field("p")) <= 1e-5
 

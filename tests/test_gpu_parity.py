@@ -184,11 +184,10 @@ def test_long_lines(cfg):
     assert max(e.values()) <= 1e-11, e
 
 
-@pytest.mark.parametrize("nz", [512, 256])
+@pytest.mark.parametrize("nz", [512, 256, 128, 64])
 def test_register_products_path(nz):
-    """nz = 512 and 256 (M = nz/2 = 256, 128) run the register-pipelined
-    spanwise transforms of k_products; one substep and one step against the
-    oracle."""
+    """nz = 64..512 (M = nz/2 = 32..256) run the register-pipelined spanwise
+    transforms of k_products; one substep and one step against the oracle."""
     cfg = replace(config.TINY, nx=17, nz=nz, name=f"wide-17x41x{nz}")
     g, o, init, coef = _pair(cfg)
     g.substep(1, True)
