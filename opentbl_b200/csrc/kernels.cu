@@ -365,7 +365,10 @@ __device__ __forceinline__ double regs_absmax(const V (&a)[E]) {
 // 1025x193x512; 5.02 at >= 3 CTAs with spills), FP32 >= 4 CTAs (126-128
 // registers, 36 bytes of spills in part 0; 2.29-2.30 ms per substep against
 // 2.34-2.43 at >= 3 CTAs and 162-168 registers, after the exchange buffer's
-// swizzle; 3.16 unbounded before it). A variant with two warps per line (4
+// swizzle; 3.16 unbounded before it). M < 256: FP32 >= 5 CTAs (M = 128: 96
+// registers, 0.69 against 0.72 ms per substep at 513x193x256 at 111); FP64
+// unbounded (M = 128: 152-168 registers, three CTAs; four at 128 registers
+// took 1.10-1.11 against 1.08-1.10 ms). A variant with two warps per line (4
 // elements per thread, radix-4 passes, named barriers) measured slower in
 // both precisions (4.92 and 3.61 ms) and was dropped.
 #ifndef OTBL_PR_MB_D
@@ -375,7 +378,7 @@ __device__ __forceinline__ double regs_absmax(const V (&a)[E]) {
 #define OTBL_PR_MB_F 4
 #endif
 template <int M, typename T, int PART>
-__global__ void __launch_bounds__(128, std::is_same<T, double>::value ? OTBL_PR_MB_D : OTBL_PR_MB_F)
+__global__ void __launch_bounds__(128, std::is_same<T, double>::value ? OTBL_PR_MB_D : (M < 256 ? 5 : OTBL_PR_MB_F))
     k_products_r(DCoef c, ZTabT<T> z, ProdArgs<T> a) {
   using V = V2<T>;
   extern __shared__ __align__(16) unsigned char smraw[];
