@@ -1791,15 +1791,19 @@ bool build_pois_maps(otbl_ctx *c) {
   return c->pmaps_vel && c->pmaps_phi64;
 }
 
+// SMs of the current device (the persistent x-DCT grids; any grid size is
+// correct, the count only spreads the tiles), cached per device ordinal
 static int sm_count() {
-  static int nsm = 0;
-  if (nsm == 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    if (nsm <= 0) nsm = 148;
+  constexpr int kDevs = 64;
+  static int nsm[kDevs] = {0};  // the same value if two host threads race
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kDevs) return 148;
+  if (nsm[dev] == 0) {
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+    nsm[dev] = n;
   }
-  return nsm;
+  return nsm[dev];
 }
 
 // The TMA-fed x-DCT pass when its descriptors exist and n is 256, 512, 1024
