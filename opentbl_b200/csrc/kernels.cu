@@ -159,13 +159,13 @@ __global__ void __launch_bounds__(128) k_products(DCoef c, ZTabT<T> z, ProdArgs<
 // buffer, its outputs not being in layout L), the two in between go through
 // a per-warp shared buffer. M = 256: radices 8, 8, 4, warp_fft's order;
 // M = 128: 4, 8, 4, M = 64: 2, 8, 4, M = 32: 8, 4 (warp_fft's order would
-// need eight register inputs per butterfly). Its element i is stored at i + i/8 for
-// 16-byte (FP64) elements and at i ^ ((i/8) mod 16) for 8-byte (FP32) ones,
-// which makes every exchange of the three passes conflict-free for its
-// element size (a bank model of the access patterns: the FP32 buffer at
-// i + i/8 needed 160 wavefronts per transform where 96 is the minimum, and
-// ncu showed 15 M of its 42 M shared wavefronts as conflicts at
-// 257x193x512). The real-to-complex post-step takes the mirrored element
+// need eight register inputs per butterfly). The buffer's element i is
+// stored at i + i/8 for 16-byte (FP64) elements and at i ^ ((i/8) mod 16)
+// for 8-byte (FP32) ones, which at M = 256 makes every exchange of the three
+// passes conflict-free for its element size (a bank model of the access
+// patterns: the FP32 buffer at i + i/8 needed 160 wavefronts per transform
+// where 96 is the minimum, and ncu showed 15 M of its 42 M shared wavefronts
+// as conflicts at 257x193x512; 0.4 M with the swizzle). The real-to-complex post-step takes the mirrored element
 // Z[M-k] from the lane that holds it by warp shuffles instead of a round
 // trip through the buffer. For M = 256 the arithmetic is warp_fft's,
 // operation for operation.
